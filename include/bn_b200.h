@@ -1,0 +1,184 @@
+/*
+ * bn_b200.h -- C ABI of the B200 (sm_100a) backend for the Braverman-Newman
+ * trapdoored-matrix scoring path of sacs-epfl/secure-vector-search.
+ *
+ * This is the drop-in boundary.  In the reference, the scorers reach the GPU
+ * through `HandleInner::Gpu(Box<FlatGpuState>)` (scorer-bntm/src/lib.rs:118-127)
+ * and `HandleInner::Gpu(Box<IvfGpuState>)` (scorer-bntm/src/ivf.rs:108-117);
+ * every entry point below names the method it replaces.  Conventions:
+ *
+ *   - plain C types, host pointers unless a name starts with d_ (device);
+ *   - every field element is a canonical residue mod p = 2^61 - 1, n = 1024;
+ *   - every call returns BN_OK (0) or a negative status; bn_last_error()
+ *     then describes the failure (thread-local string), mirroring the
+ *     reference's GpuError (gpu/mod.rs:97-110);
+ *   - handles are thread-safe: calls on one handle are serialised on its
+ *     own CUDA stream, calls on distinct handles run concurrently;
+ *   - host buffers are only borrowed for the duration of a call.
+ */
+#ifndef BN_B200_H
+#define BN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BN_ABI_VERSION 1
+
+/* Status codes (GpuError, gpu/mod.rs:97-110; BnTmError, lib.rs:178-196). */
+#define BN_OK 0
+#define BN_EINVAL (-1)       /* bad argument or shape (e.g. n != 1024, k > 1024)   */
+#define BN_ECUDA (-2)        /* CUDA runtime failure      (GpuError::Driver)         */
+#define BN_EBUDGET (-3)      /* payload exceeds budget    (GpuError::BudgetTooSmall) */
+#define BN_ENODEV (-4)       /* no usable CUDA device                                */
+#define BN_EUNSUPPORTED (-5) /* handle lacks the client state this call needs       */
+
+#define BN_TOPK_MAX 1024
+
+/* Last error message of the calling thread ("" when none). */
+const char* bn_last_error(void);
+/* Build description: ABI version, target architecture, compiler. */
+const char* bn_build_info(void);
+/* Number of visible CUDA devices (0 without a GPU). */
+int bn_device_count(int* out);
+
+typedef struct bn_ctx bn_ctx;
+typedef struct bn_flat bn_flat;
+typedef struct bn_ivf bn_ivf;
+typedef struct bn_plan bn_plan;
+
+/* Sparse {-1,0,+1} matrix in CSR form: rowptr has rows+1 entries, idx holds
+ * sorted column indices, sign holds +1/-1 (crypto.rs:168-186 SparseMatrix). */
+typedef struct bn_sparse_csr {
+    const uint64_t* rowptr;
+    const uint32_t* idx;
+    const int8_t* sign;
+} bn_sparse_csr;
+
+/* ---------------------------------------------------------------- context
+ * Replaces the process-wide cudarc context + PTX module (gpu/mod.rs:169-200)
+ * and the VRAM budget resolution (scorer-gpu-common/src/budget.rs:132-150):
+ * vram_budget_bytes = 0 takes 80 % of the device's free memory. */
+int bn_ctx_create(int device, uint64_t vram_budget_bytes, bn_ctx** out);
+int bn_ctx_destroy(bn_ctx* ctx);
+/* Budget, bytes currently held by handles, high-water mark
+ * (FlatGpuState::{vram_budget_bytes, peak_vram_bytes}, gpu/mod.rs:334-340). */
+int bn_ctx_memory(const bn_ctx* ctx, uint64_t* budget_bytes, uint64_t* used_bytes, uint64_t* peak_bytes);
+
+/* ---------------------------------------------------------------- flat
+ * FlatGpuState::build (gpu/mod.rs:300-332).  m_enc is m x n, a_l and h are
+ * m x n1, all row-major host arrays; the corpus is uploaded eagerly and stays
+ * resident (the reference uploads lazily through its LRU store). */
+int bn_flat_build(bn_ctx* ctx, const uint64_t* m_enc, const uint64_t* a_l, const uint64_t* h, uint64_t m,
+                  uint32_t n, uint32_t n1, bn_flat** out);
+/* Client-side state for on-device decode: L (n x n1 row-major), the
+ * plaintext M (m x n row-major) and S (crypto.rs:353-392 EncryptedCluster
+ * fields l_subspace/m_plain/s_mat).  Needed by bn_flat_query. */
+int bn_flat_attach_client(bn_flat* h, const uint64_t* l_subspace, const uint64_t* m_plain, bn_sparse_csr s_mat);
+/* Encrypt on the device and build in one step (crypto.rs:405-478 +
+ * gpu/mod.rs:300-332): M_enc = M + H L^T + S and AL = M L are computed
+ * from the quantised plaintext m_q (m x n), L, H and S; the client state is
+ * attached as by bn_flat_attach_client. */
+int bn_flat_build_from_plain(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1,
+                             const uint64_t* l_subspace, const uint64_t* h, bn_sparse_csr s_mat, bn_flat** out);
+int bn_flat_destroy(bn_flat* h);
+int bn_flat_info(const bn_flat* h, uint64_t* rows, uint64_t* device_bytes);
+/* Device-resident m_enc (row-major m x 1024) of a flat handle. */
+int bn_flat_device_m_enc(const bn_flat* h, const uint64_t** d_m_enc);
+
+/* FlatGpuState::compute_products (gpu/mod.rs:362-379): r = M_enc v_enc. */
+int bn_flat_compute_products(bn_flat* h, const uint64_t* v_enc, uint64_t* r);
+/* Batched compute_products (crypto.rs:782-828): r is B x m. */
+int bn_flat_compute_products_batch(bn_flat* h, const uint64_t* v_encs, uint32_t B, uint64_t* r);
+/* FlatGpuState::decode_dense_terms (gpu/mod.rs:390-408): AL g + H lt_venc. */
+int bn_flat_decode_dense_terms(bn_flat* h, const uint64_t* g, const uint64_t* lt_venc, uint64_t* out);
+/* verify_response (crypto.rs:1013-1046) on the device for a claimed r.
+ * v_seed is the seed of the verification RNG, i.e. domain_separate(q_seed,
+ * "protocol2") in the reference (lib.rs:422).  *failed_trial = -1 when
+ * every trial passes, else the first failing trial.  ur/zv (nullable, length
+ * trials) receive both sides of every trial. */
+int bn_flat_verify(bn_flat* h, const uint64_t* r, const uint64_t* v_enc, const uint8_t v_seed[32], uint32_t trials,
+                   int32_t* failed_trial, uint64_t* ur, uint64_t* zv);
+/* Whole server + client path of BnTmScorer::score / score_batch
+ * (lib.rs:326-475, 522-624) for B encoded queries: scan, fused-launch
+ * Protocol 2, decode, fp_to_signed and top-k, all on the device.
+ *   v_enc  B x n, g  B x n1
+ *   T      query b has t_nnz[b] entries starting at sum(t_nnz[0..b)) in
+ *          t_idx (column) / t_sign (+1/-1)
+ *   v_seeds B x 32 bytes (nullable when trials == 0)
+ * Outputs: ids/scores B x k (score desc, id asc; n_hits[b] = min(k, m)
+ * valid), failed_trial[b] (nullable; -1 = verified or not run), r_out and
+ * mv_out (nullable, B x m: scan residues and decoded residues). */
+int bn_flat_query(bn_flat* h, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                  const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds, uint32_t trials, uint32_t k,
+                  uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed_trial, uint64_t* r_out,
+                  uint64_t* mv_out);
+
+/* Prepared, device-resident form of bn_flat_query for a fixed (B, trials,
+ * k): bn_plan_enqueue only enqueues kernels on `stream` (no host work, no
+ * allocation, no synchronisation), so it can be captured in a CUDA graph.
+ *   d_v_enc B x 1024 u64, d_g B x n1 u64,
+ *   d_t     B x 1024 u32 entries (col | 0x80000000 for -1), d_t_nnz B,
+ *   d_v_seeds B x 32 bytes, outputs d_ids/d_scores B x k, d_n B,
+ *   d_failed B (-1 = pass).  All device pointers. */
+int bn_flat_plan(bn_flat* h, uint32_t B, uint32_t trials, uint32_t k, bn_plan** out);
+int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v_enc, const uint64_t* d_g, const uint32_t* d_t,
+                    const uint32_t* d_t_nnz, const uint8_t* d_v_seeds, uint32_t* d_ids, int64_t* d_scores,
+                    uint32_t* d_n, int32_t* d_failed, void* stream);
+/* Scan-only enqueue of the same plan: d_r (B x m) = M_enc v_enc. */
+int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v_enc, uint64_t* d_r, void* stream);
+int bn_plan_destroy(bn_plan* p);
+
+/* ---------------------------------------------------------------- IVF
+ * IvfGpuState::build (gpu/mod.rs:423-474) over a device-resident CSR of the
+ * inverted lists: list c owns rows [list_offsets[c], list_offsets[c+1]) of
+ * the concatenated m_enc / a_l / h arrays; ids[row] is the global vector id
+ * (ivf-index IvfIndex::clusters membership). */
+int bn_ivf_build(bn_ctx* ctx, uint32_t nlist, const uint64_t* list_offsets, const uint32_t* ids, const uint64_t* m_enc,
+                 const uint64_t* a_l, const uint64_t* h, uint32_t n, uint32_t n1, bn_ivf** out);
+int bn_ivf_attach_client(bn_ivf* h, const uint64_t* l_subspace, const uint64_t* m_plain, bn_sparse_csr s_mat);
+/* Device encryption of every list (crypto.rs:405-478 per cluster,
+ * ivf.rs:627-653) followed by bn_ivf_build + bn_ivf_attach_client.  h and
+ * s_mat are the concatenation of the per-list H / S (each list with its own
+ * h_seed, ivf.rs:258-264). */
+int bn_ivf_build_from_plain(bn_ctx* ctx, uint32_t nlist, const uint64_t* list_offsets, const uint32_t* ids,
+                            const uint64_t* m_q, uint32_t n, uint32_t n1, const uint64_t* l_subspace,
+                            const uint64_t* h, bn_sparse_csr s_mat, bn_ivf** out);
+int bn_ivf_destroy(bn_ivf* h);
+int bn_ivf_info(const bn_ivf* h, uint64_t* rows, uint64_t* device_bytes);
+/* IvfGpuState::compute_products (gpu/mod.rs:506-536).  *m_out = list size;
+ * 0 (and nothing written) for an empty or out-of-range list, the
+ * reference's Ok(None). */
+int bn_ivf_compute_products(bn_ivf* h, uint32_t ci, const uint64_t* v_enc, uint64_t* r, uint64_t* m_out);
+/* IvfGpuState::decode_dense_terms (gpu/mod.rs:542-577). */
+int bn_ivf_decode_dense_terms(bn_ivf* h, uint32_t ci, const uint64_t* g, const uint64_t* lt_venc, uint64_t* out,
+                              uint64_t* m_out);
+/* verify_response for one list and a claimed r (ivf.rs:791-806). */
+int bn_ivf_verify(bn_ivf* h, uint32_t ci, const uint64_t* r, const uint64_t* v_enc, const uint8_t v_seed[32],
+                  uint32_t trials, int32_t* failed_trial, uint64_t* ur, uint64_t* zv);
+/* BnTmIvfScorer::score / score_batch (ivf.rs:746-927, 1199-1366) for B
+ * queries with nprobe routed lists each (probes B x nprobe, in probe
+ * order): every probed list of every query is scanned, verified, decoded
+ * and ranked in one persistent launch per stage.  Inputs as in
+ * bn_flat_query.  failed_cluster[b]/failed_trial[b] (nullable) name the
+ * first probed list (probe order) whose verification failed, -1 if none. */
+int bn_ivf_query(bn_ivf* h, uint32_t B, uint32_t nprobe, const uint32_t* probes, const uint64_t* v_enc,
+                 const uint64_t* g, const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz,
+                 const uint8_t* v_seeds, uint32_t trials, uint32_t k, uint32_t* ids, int64_t* scores, uint32_t* n_hits,
+                 int32_t* failed_cluster, int32_t* failed_trial);
+
+/* ---------------------------------------------------------------- keygen
+ * encrypt_cluster (crypto.rs:405-478) on the device with host in/out:
+ * m_enc = m_q + H L^T + S, a_l = m_q L.  Used to cross-check the device
+ * encryption against a CPU restatement. */
+int bn_encrypt_cluster(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1,
+                       const uint64_t* l_subspace, const uint64_t* h, bn_sparse_csr s_mat, uint64_t* m_enc,
+                       uint64_t* a_l);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BN_B200_H */

@@ -1,0 +1,63 @@
+/*
+ * bn_host.h -- host-side (client) half of the BN path, in C++ above the
+ * device ABI of bn_b200.h: key generation, quantisation and query encoding,
+ * with the reference's exact RNG consumption so that the device sees the
+ * same M_enc / v_enc the reference CPU scorer would build.
+ *
+ * Each function names the reference function it restates
+ * (scorer-bntm/src/crypto.rs, lib.rs, ivf.rs).  All are CPU-only and need no
+ * GPU; the device entry points are in bn_b200.h.
+ */
+#ifndef BN_HOST_H
+#define BN_HOST_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* params.rs:179-181 mu = n^(eps-1); crypto.rs:210-211 32-bit threshold. */
+double bn_host_mu(void);
+/* params.rs:198-205 (3 trials for p = 2^61 - 1). */
+uint32_t bn_host_default_trials(void);
+
+/* crypto.rs:142-150 domain_separate(seed, tag). */
+void bn_host_domain_separate(const uint8_t seed[32], const char* tag, uint8_t out[32]);
+/* ivf.rs:258-264 derive_h_seed(upload_seed, cluster_idx). */
+void bn_host_derive_h_seed(uint64_t upload_seed, uint64_t cluster_idx, uint8_t out[32]);
+
+/* crypto.rs:235-238 generate_subspace: L, n x n1 row-major. */
+void bn_host_generate_subspace(const uint8_t key_seed[32], uint32_t n, uint32_t n1, uint64_t* L);
+/* crypto.rs:258-270 regenerate_h_s: H (m x n1) then S row by row (CSR).
+ * Returns nnz(S), or -(needed) when s_cap is too small. */
+int64_t bn_host_regenerate_h_s(const uint8_t h_seed[32], uint64_t m, uint32_t n, uint32_t n1, uint64_t* H,
+                               uint64_t* s_rowptr, uint32_t* s_idx, int8_t* s_sign, uint64_t s_cap);
+/* Per-list regenerate_h_s for an IVF index (ivf.rs:627-653): list c uses
+ * derive_h_seed(upload_seed, c); outputs are the concatenation in list order
+ * (rows list_offsets[c]..list_offsets[c+1]).  Lists run in parallel. */
+int64_t bn_host_regenerate_h_s_lists(uint64_t upload_seed, uint32_t nlist, const uint64_t* list_offsets, uint32_t n,
+                                     uint32_t n1, uint64_t* H, uint64_t* s_rowptr, uint32_t* s_idx, int8_t* s_sign,
+                                     uint64_t s_cap);
+
+/* crypto.rs:105-122 quantise_vector over `count` vectors of dimension d
+ * (d <= n), zero-padded to n: out is count x n. */
+void bn_host_quantise(const float* v, uint64_t count, uint32_t d, uint32_t n, uint64_t q, uint64_t* out);
+
+/* crypto.rs:508-553 encode_query with ChaCha20Rng::from_seed(q_seed):
+ * writes v_enc (n), g (n1), T (t_idx/t_sign, room for n) and returns |T|. */
+uint32_t bn_host_encode_query(const uint64_t* v_q, const uint64_t* L, uint32_t n, uint32_t n1,
+                              const uint8_t q_seed[32], uint64_t* v_enc, uint64_t* g, uint32_t* t_idx,
+                              int8_t* t_sign);
+
+/* ivf-index/src/ivf.rs:150-164 probe_route: the nprobe nearest centroids
+ * by f32 L2 (scalar, in dimension order), ties by lower index.  Queries
+ * run in parallel; out is count x min(nprobe, nlist). */
+void bn_host_probe_route(const float* centroids, uint32_t nlist, uint32_t d, const float* queries, uint64_t count,
+                         uint32_t nprobe, uint32_t* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BN_HOST_H */

@@ -1,0 +1,464 @@
+"""ctypes bindings of the C ABI in include/bn_b200.h (libbn_b200.so).
+
+The product path: every call lands in the sm_100a library; there is no
+Python or CPU fallback.  Loading fails loudly when the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbn_b200.so")
+N = 1024
+P = (1 << 61) - 1
+TOPK_MAX = 1024
+
+BN_OK, BN_EINVAL, BN_ECUDA, BN_EBUDGET, BN_ENODEV, BN_EUNSUPPORTED = 0, -1, -2, -3, -4, -5
+_NAMES = {BN_EINVAL: "EINVAL", BN_ECUDA: "ECUDA", BN_EBUDGET: "EBUDGET", BN_ENODEV: "ENODEV",
+          BN_EUNSUPPORTED: "EUNSUPPORTED"}
+
+
+class BnError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"{LIB_PATH} is not built; run `python secure-vector-search_b200/build.py`")
+lib = C.CDLL(LIB_PATH)
+
+vp = C.c_void_p
+u32, u64, i32 = C.c_uint32, C.c_uint64, C.c_int32
+
+
+class SparseCsr(C.Structure):
+    _fields_ = [("rowptr", vp), ("idx", vp), ("sign", vp)]
+
+
+_SIGS = {
+    "bn_last_error": (C.c_char_p, []),
+    "bn_build_info": (C.c_char_p, []),
+    "bn_device_count": (C.c_int, [vp]),
+    "bn_ctx_create": (C.c_int, [C.c_int, u64, vp]),
+    "bn_ctx_destroy": (C.c_int, [vp]),
+    "bn_ctx_memory": (C.c_int, [vp, vp, vp, vp]),
+    "bn_flat_build": (C.c_int, [vp, vp, vp, vp, u64, u32, u32, vp]),
+    "bn_flat_attach_client": (C.c_int, [vp, vp, vp, SparseCsr]),
+    "bn_flat_build_from_plain": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, vp]),
+    "bn_flat_destroy": (C.c_int, [vp]),
+    "bn_flat_info": (C.c_int, [vp, vp, vp]),
+    "bn_flat_device_m_enc": (C.c_int, [vp, vp]),
+    "bn_flat_compute_products": (C.c_int, [vp, vp, vp]),
+    "bn_flat_compute_products_batch": (C.c_int, [vp, vp, u32, vp]),
+    "bn_flat_decode_dense_terms": (C.c_int, [vp, vp, vp, vp]),
+    "bn_flat_verify": (C.c_int, [vp, vp, vp, vp, u32, vp, vp, vp]),
+    "bn_flat_query": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp, vp]),
+    "bn_flat_plan": (C.c_int, [vp, u32, u32, u32, vp]),
+    "bn_plan_enqueue": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "bn_plan_enqueue_scan": (C.c_int, [vp, vp, vp, vp]),
+    "bn_plan_destroy": (C.c_int, [vp]),
+    "bn_ivf_build": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, u32, u32, vp]),
+    "bn_ivf_attach_client": (C.c_int, [vp, vp, vp, SparseCsr]),
+    "bn_ivf_build_from_plain": (C.c_int, [vp, u32, vp, vp, vp, u32, u32, vp, vp, SparseCsr, vp]),
+    "bn_ivf_destroy": (C.c_int, [vp]),
+    "bn_ivf_info": (C.c_int, [vp, vp, vp]),
+    "bn_ivf_compute_products": (C.c_int, [vp, u32, vp, vp, vp]),
+    "bn_ivf_decode_dense_terms": (C.c_int, [vp, u32, vp, vp, vp, vp]),
+    "bn_ivf_verify": (C.c_int, [vp, u32, vp, vp, vp, u32, vp, vp, vp]),
+    "bn_ivf_query": (C.c_int, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
+    "bn_encrypt_cluster": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, vp, vp]),
+}
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def last_error() -> str:
+    return lib.bn_last_error().decode()
+
+
+def check(rc: int):
+    if rc != BN_OK:
+        raise BnError(rc, last_error())
+
+
+def ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    return a.ctypes.data_as(vp)
+
+
+def _u64(a):
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def _csr(rowptr, idx, sign):
+    rowptr, idx, sign = _u64(rowptr), np.ascontiguousarray(idx, np.uint32), np.ascontiguousarray(sign, np.int8)
+    keep = (rowptr, idx, sign)
+    return SparseCsr(ptr(rowptr), ptr(idx) if idx.size else None, ptr(sign) if sign.size else None), keep
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    check(lib.bn_device_count(C.byref(n)))
+    return n.value
+
+
+def build_info() -> str:
+    return lib.bn_build_info().decode()
+
+
+class Context:
+    """bn_ctx: a device and its memory budget (gpu/mod.rs:169-200, budget.rs:132-150)."""
+
+    def __init__(self, device: int = 0, vram_budget_bytes: int = 0):
+        self.h = None
+        h = vp()
+        check(lib.bn_ctx_create(device, vram_budget_bytes, C.byref(h)))
+        self.h = h
+
+    def memory(self):
+        b, u, p = u64(), u64(), u64()
+        check(lib.bn_ctx_memory(self.h, C.byref(b), C.byref(u), C.byref(p)))
+        return b.value, u.value, p.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.bn_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def _t_concat(enc_list):
+    """Concatenate per-query sparse T (idx, sign) lists."""
+    nnz = np.array([len(t[0]) for t in enc_list], np.uint32)
+    idx = np.concatenate([np.asarray(t[0], np.uint32) for t in enc_list]) if len(enc_list) else np.zeros(0, np.uint32)
+    sign = np.concatenate([np.asarray(t[1], np.int8) for t in enc_list]) if len(enc_list) else np.zeros(0, np.int8)
+    return idx, sign, nnz
+
+
+class Flat:
+    """bn_flat: a resident flat corpus (FlatGpuState, gpu/mod.rs:279-409)."""
+
+    def __init__(self, ctx: Context, handle, m: int, n1: int):
+        self.ctx, self.h, self.m, self.n1 = ctx, handle, m, n1
+
+    @classmethod
+    def build(cls, ctx, m_enc, a_l, h, m, n1=128):
+        m_enc, a_l, h = _u64(m_enc), _u64(a_l), _u64(h)
+        out = vp()
+        check(lib.bn_flat_build(ctx.h, ptr(m_enc), ptr(a_l), ptr(h), m, N, n1, C.byref(out)))
+        return cls(ctx, out, m, n1)
+
+    @classmethod
+    def build_from_plain(cls, ctx, m_q, m, L, H, s_rowptr, s_idx, s_sign, n1=128):
+        m_q, L, H = _u64(m_q), _u64(L), _u64(H)
+        csr, keep = _csr(s_rowptr, s_idx, s_sign)
+        out = vp()
+        check(lib.bn_flat_build_from_plain(ctx.h, ptr(m_q), m, N, n1, ptr(L), ptr(H), csr, C.byref(out)))
+        return cls(ctx, out, m, n1)
+
+    def attach_client(self, L, m_plain, s_rowptr, s_idx, s_sign):
+        L, m_plain = _u64(L), _u64(m_plain)
+        csr, keep = _csr(s_rowptr, s_idx, s_sign)
+        check(lib.bn_flat_attach_client(self.h, ptr(L), ptr(m_plain), csr))
+
+    def info(self):
+        rows, b = u64(), u64()
+        check(lib.bn_flat_info(self.h, C.byref(rows), C.byref(b)))
+        return rows.value, b.value
+
+    def device_m_enc(self) -> int:
+        p = vp()
+        check(lib.bn_flat_device_m_enc(self.h, C.byref(p)))
+        return p.value
+
+    def compute_products(self, v_enc) -> np.ndarray:
+        v = _u64(v_enc)
+        r = np.zeros(max(self.m, 1), np.uint64)
+        check(lib.bn_flat_compute_products(self.h, ptr(v), ptr(r)))
+        return r[: self.m]
+
+    def compute_products_batch(self, v_encs) -> np.ndarray:
+        v = _u64(v_encs).reshape(-1, N)
+        r = np.zeros((v.shape[0], max(self.m, 1)), np.uint64)
+        check(lib.bn_flat_compute_products_batch(self.h, ptr(v), v.shape[0], ptr(r)))
+        return r[:, : self.m]
+
+    def decode_dense_terms(self, g, lt_venc) -> np.ndarray:
+        g, lt = _u64(g), _u64(lt_venc)
+        out = np.zeros(max(self.m, 1), np.uint64)
+        check(lib.bn_flat_decode_dense_terms(self.h, ptr(g), ptr(lt), ptr(out)))
+        return out[: self.m]
+
+    def verify(self, r, v_enc, v_seed: bytes, trials: int):
+        r, v = _u64(r), _u64(v_enc)
+        seed = np.frombuffer(bytes(v_seed), np.uint8).copy()
+        f = i32(0)
+        ur = np.zeros(max(trials, 1), np.uint64)
+        zv = np.zeros(max(trials, 1), np.uint64)
+        check(lib.bn_flat_verify(self.h, ptr(r) if r.size else None, ptr(v), ptr(seed), trials, C.byref(f), ptr(ur),
+                                 ptr(zv)))
+        ran = trials if f.value < 0 else f.value + 1
+        return f.value, ur[:ran], zv[:ran]
+
+    def query(self, v_enc, g, t_list, v_seeds, trials, k, want_r=False, want_mv=False):
+        """t_list: per query (idx array, sign array).  v_seeds: list of 32-byte seeds or None."""
+        v = _u64(v_enc).reshape(-1, N)
+        B = v.shape[0]
+        gg = _u64(g).reshape(B, self.n1)
+        ti, ts, tn = _t_concat(t_list)
+        seeds = None if v_seeds is None else np.frombuffer(b"".join(bytes(s) for s in v_seeds), np.uint8).copy()
+        kk = max(k, 1)
+        ids = np.zeros((B, kk), np.uint32)
+        sc = np.zeros((B, kk), np.int64)
+        nh = np.zeros(B, np.uint32)
+        fl = np.zeros(B, np.int32)
+        r = np.zeros((B, max(self.m, 1)), np.uint64) if want_r else None
+        mv = np.zeros((B, max(self.m, 1)), np.uint64) if want_mv else None
+        check(lib.bn_flat_query(self.h, B, ptr(v), ptr(gg), ptr(ti) if ti.size else None, ptr(ts) if ts.size else None,
+                                ptr(tn), ptr(seeds), trials, k, ptr(ids), ptr(sc), ptr(nh), ptr(fl), ptr(r), ptr(mv)))
+        hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
+        return hits, fl, (r[:, : self.m] if want_r else None), (mv[:, : self.m] if want_mv else None)
+
+    def plan(self, B: int, trials: int, k: int) -> "Plan":
+        out = vp()
+        check(lib.bn_flat_plan(self.h, B, trials, k, C.byref(out)))
+        return Plan(self, out, B, trials, k)
+
+    def close(self):
+        if self.h:
+            lib.bn_flat_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Plan:
+    """bn_plan: enqueue-only form of Flat.query over device buffers (graph-capturable)."""
+
+    def __init__(self, flat, handle, B, trials, k):
+        self.flat, self.h, self.B, self.trials, self.k = flat, handle, B, trials, k
+
+    def enqueue(self, d_v, d_g, d_t, d_t_nnz, d_seeds, d_ids, d_scores, d_n, d_failed, stream: int):
+        check(lib.bn_plan_enqueue(self.h, d_v, d_g, d_t, d_t_nnz, d_seeds, d_ids, d_scores, d_n, d_failed, stream))
+
+    def enqueue_scan(self, d_v, d_r, stream: int):
+        check(lib.bn_plan_enqueue_scan(self.h, d_v, d_r, stream))
+
+    def close(self):
+        if self.h:
+            lib.bn_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Ivf:
+    """bn_ivf: resident inverted lists in CSR form (IvfGpuState, gpu/mod.rs:423-578)."""
+
+    def __init__(self, ctx, handle, offsets, n1):
+        self.ctx, self.h, self.offsets, self.n1 = ctx, handle, np.asarray(offsets, np.uint64), n1
+        self.nlist = len(offsets) - 1
+
+    @classmethod
+    def build(cls, ctx, offsets, ids, m_enc, a_l, h, n1=128):
+        off = _u64(offsets)
+        ids = np.ascontiguousarray(ids, np.uint32)
+        m_enc, a_l, h = _u64(m_enc), _u64(a_l), _u64(h)
+        out = vp()
+        check(lib.bn_ivf_build(ctx.h, len(off) - 1, ptr(off), ptr(ids), ptr(m_enc), ptr(a_l), ptr(h), N, n1,
+                               C.byref(out)))
+        return cls(ctx, out, off, n1)
+
+    @classmethod
+    def build_from_plain(cls, ctx, offsets, ids, m_q, L, H, s_rowptr, s_idx, s_sign, n1=128):
+        off = _u64(offsets)
+        ids = np.ascontiguousarray(ids, np.uint32)
+        m_q, L, H = _u64(m_q), _u64(L), _u64(H)
+        csr, keep = _csr(s_rowptr, s_idx, s_sign)
+        out = vp()
+        check(lib.bn_ivf_build_from_plain(ctx.h, len(off) - 1, ptr(off), ptr(ids), ptr(m_q), N, n1, ptr(L), ptr(H),
+                                          csr, C.byref(out)))
+        return cls(ctx, out, off, n1)
+
+    def attach_client(self, L, m_plain, s_rowptr, s_idx, s_sign):
+        L, m_plain = _u64(L), _u64(m_plain)
+        csr, keep = _csr(s_rowptr, s_idx, s_sign)
+        check(lib.bn_ivf_attach_client(self.h, ptr(L), ptr(m_plain), csr))
+
+    def compute_products(self, ci, v_enc):
+        v = _u64(v_enc)
+        m = int(self.offsets[ci + 1] - self.offsets[ci]) if ci < self.nlist else 0
+        r = np.zeros(max(m, 1), np.uint64)
+        mo = u64()
+        check(lib.bn_ivf_compute_products(self.h, ci, ptr(v), ptr(r), C.byref(mo)))
+        return None if mo.value == 0 else r[: mo.value]
+
+    def decode_dense_terms(self, ci, g, lt):
+        g, lt = _u64(g), _u64(lt)
+        m = int(self.offsets[ci + 1] - self.offsets[ci]) if ci < self.nlist else 0
+        out = np.zeros(max(m, 1), np.uint64)
+        mo = u64()
+        check(lib.bn_ivf_decode_dense_terms(self.h, ci, ptr(g), ptr(lt), ptr(out), C.byref(mo)))
+        return None if mo.value == 0 else out[: mo.value]
+
+    def verify(self, ci, r, v_enc, v_seed, trials):
+        r, v = _u64(r), _u64(v_enc)
+        seed = np.frombuffer(bytes(v_seed), np.uint8).copy()
+        f = i32(0)
+        ur = np.zeros(max(trials, 1), np.uint64)
+        zv = np.zeros(max(trials, 1), np.uint64)
+        check(lib.bn_ivf_verify(self.h, ci, ptr(r) if r.size else None, ptr(v), ptr(seed), trials, C.byref(f),
+                                ptr(ur), ptr(zv)))
+        ran = trials if f.value < 0 else f.value + 1
+        return f.value, ur[:ran], zv[:ran]
+
+    def query(self, probes, v_enc, g, t_list, v_seeds, trials, k):
+        pr = np.ascontiguousarray(probes, np.uint32)
+        B, nprobe = pr.shape
+        v = _u64(v_enc).reshape(B, N)
+        gg = _u64(g).reshape(B, self.n1)
+        ti, ts, tn = _t_concat(t_list)
+        seeds = None if v_seeds is None else np.frombuffer(b"".join(bytes(s) for s in v_seeds), np.uint8).copy()
+        kk = max(k, 1)
+        ids = np.zeros((B, kk), np.uint32)
+        sc = np.zeros((B, kk), np.int64)
+        nh = np.zeros(B, np.uint32)
+        fc = np.zeros(B, np.int32)
+        ft = np.zeros(B, np.int32)
+        check(lib.bn_ivf_query(self.h, B, nprobe, ptr(pr), ptr(v), ptr(gg), ptr(ti) if ti.size else None,
+                               ptr(ts) if ts.size else None, ptr(tn), ptr(seeds), trials, k, ptr(ids), ptr(sc),
+                               ptr(nh), ptr(fc), ptr(ft)))
+        hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
+        return hits, fc, ft
+
+    def close(self):
+        if self.h:
+            lib.bn_ivf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def encrypt_cluster(ctx, m_q, m, L, H, s_rowptr, s_idx, s_sign, n1=128):
+    m_q, L, H = _u64(m_q), _u64(L), _u64(H)
+    csr, keep = _csr(s_rowptr, s_idx, s_sign)
+    m_enc = np.zeros(max(m * N, 1), np.uint64)
+    al = np.zeros(max(m * n1, 1), np.uint64)
+    check(lib.bn_encrypt_cluster(ctx.h, ptr(m_q), m, N, n1, ptr(L), ptr(H), csr, ptr(m_enc), ptr(al)))
+    return m_enc[: m * N], al[: m * n1]
+
+
+# ---------------------------------------------------------------- host side (include/bn_host.h)
+_HOST_SIGS = {
+    "bn_host_mu": (C.c_double, []),
+    "bn_host_default_trials": (u32, []),
+    "bn_host_domain_separate": (None, [vp, C.c_char_p, vp]),
+    "bn_host_derive_h_seed": (None, [u64, u64, vp]),
+    "bn_host_generate_subspace": (None, [vp, u32, u32, vp]),
+    "bn_host_regenerate_h_s": (C.c_int64, [vp, u64, u32, u32, vp, vp, vp, vp, u64]),
+    "bn_host_regenerate_h_s_lists": (C.c_int64, [u64, u32, vp, u32, u32, vp, vp, vp, vp, u64]),
+    "bn_host_quantise": (None, [vp, u64, u32, u32, u64, vp]),
+    "bn_host_encode_query": (u32, [vp, vp, u32, u32, vp, vp, vp, vp, vp]),
+    "bn_host_probe_route": (None, [vp, u32, u32, vp, u64, u32, vp]),
+}
+for _name, (_res, _args) in _HOST_SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def _seed_arr(s) -> np.ndarray:
+    a = np.frombuffer(bytes(s), np.uint8).copy()
+    assert a.size == 32
+    return a
+
+
+def host_domain_separate(seed: bytes, tag: str = "protocol2") -> bytes:
+    out = np.zeros(32, np.uint8)
+    lib.bn_host_domain_separate(ptr(_seed_arr(seed)), tag.encode(), ptr(out))
+    return out.tobytes()
+
+
+def host_derive_h_seed(upload_seed: int, ci: int) -> bytes:
+    out = np.zeros(32, np.uint8)
+    lib.bn_host_derive_h_seed(upload_seed, ci, ptr(out))
+    return out.tobytes()
+
+
+def host_generate_subspace(key_seed: bytes, n1: int = 128) -> np.ndarray:
+    L = np.zeros(N * n1, np.uint64)
+    lib.bn_host_generate_subspace(ptr(_seed_arr(key_seed)), N, n1, ptr(L))
+    return L
+
+
+def host_regenerate_h_s(h_seed: bytes, m: int, n1: int = 128):
+    H = np.zeros(max(m * n1, 1), np.uint64)
+    rowptr = np.zeros(m + 1, np.uint64)
+    cap = max(m * 160, 1024)
+    while True:
+        idx = np.zeros(cap, np.uint32)
+        sign = np.zeros(cap, np.int8)
+        nnz = lib.bn_host_regenerate_h_s(ptr(_seed_arr(h_seed)), m, N, n1, ptr(H), ptr(rowptr), ptr(idx), ptr(sign), cap)
+        if nnz >= 0:
+            return H[: m * n1], rowptr, idx[:nnz], sign[:nnz]
+        cap = -nnz
+
+
+def host_regenerate_h_s_lists(upload_seed: int, offsets, n1: int = 128):
+    off = _u64(offsets)
+    rows = int(off[-1])
+    H = np.zeros(max(rows * n1, 1), np.uint64)
+    rowptr = np.zeros(rows + 1, np.uint64)
+    cap = max(rows * 160, 1024)
+    while True:
+        idx = np.zeros(cap, np.uint32)
+        sign = np.zeros(cap, np.int8)
+        nnz = lib.bn_host_regenerate_h_s_lists(upload_seed, len(off) - 1, ptr(off), N, n1, ptr(H), ptr(rowptr),
+                                               ptr(idx), ptr(sign), cap)
+        if nnz >= 0:
+            return H[: rows * n1], rowptr, idx[:nnz], sign[:nnz]
+        cap = -nnz
+
+
+def host_quantise(v, q: int = 1 << 20) -> np.ndarray:
+    v = np.ascontiguousarray(v, np.float32)
+    if v.ndim == 1:
+        v = v[None]
+    out = np.zeros((v.shape[0], N), np.uint64)
+    lib.bn_host_quantise(ptr(v), v.shape[0], v.shape[1], N, q, ptr(out))
+    return out
+
+
+def host_encode_query(v_q, L, q_seed: bytes, n1: int = 128):
+    v_q, L = _u64(v_q), _u64(L)
+    v_enc = np.zeros(N, np.uint64)
+    g = np.zeros(n1, np.uint64)
+    ti = np.zeros(N, np.uint32)
+    ts = np.zeros(N, np.int8)
+    c = lib.bn_host_encode_query(ptr(v_q), ptr(L), N, n1, ptr(_seed_arr(q_seed)), ptr(v_enc), ptr(g), ptr(ti), ptr(ts))
+    return v_enc, g, ti[:c].copy(), ts[:c].copy()
+
+
+def host_probe_route(centroids, queries, nprobe: int) -> np.ndarray:
+    c = np.ascontiguousarray(centroids, np.float32)
+    q = np.ascontiguousarray(queries, np.float32)
+    if q.ndim == 1:
+        q = q[None]
+    np_ = min(nprobe, c.shape[0])
+    out = np.zeros((q.shape[0], np_), np.uint32)
+    lib.bn_host_probe_route(ptr(c), c.shape[0], c.shape[1], ptr(q), q.shape[0], nprobe, ptr(out))
+    return out

@@ -1,0 +1,1226 @@
+// bn_capi.cu -- implementation of the C ABI declared in include/bn_b200.h.
+//
+// Replaces the cudarc glue of the reference (scorer-bntm/src/gpu/mod.rs):
+// instead of one synchronous H2D + launch + D2H per query and per probed
+// list on the default stream (gpu/mod.rs:584-614), a query batch is packed
+// into one pinned staging copy, the whole pipeline (scan, Protocol 2,
+// decode, top-k) is enqueued on the handle's own stream, and one D2H brings
+// back only the ranked hits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bn_b200.h"
+#include "bn_kernels.cuh"
+
+using namespace bn;
+
+// ------------------------------------------------------------------ errors
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CU(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return fail(BN_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));     \
+    } while (0)
+
+#define TRY(call)                    \
+    do {                             \
+        int rc_ = (call);            \
+        if (rc_ != BN_OK) return rc_; \
+    } while (0)
+
+inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+}  // namespace
+
+// ------------------------------------------------------------------ context
+struct bn_ctx {
+    int device = 0;
+    int num_sms = 148;
+    uint64_t budget = 0, used = 0, peak = 0;
+    std::mutex mu;
+};
+
+namespace {
+
+// Device allocation accounted against the context budget.
+struct DevMem {
+    bn_ctx* ctx = nullptr;
+    void* p = nullptr;
+    uint64_t bytes = 0;
+
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+    ~DevMem() { release(); }
+
+    void release() {
+        if (p) {
+            cudaFree(p);
+            std::lock_guard<std::mutex> g(ctx->mu);
+            ctx->used -= bytes;
+        }
+        p = nullptr;
+        bytes = 0;
+    }
+    int alloc(bn_ctx* c, uint64_t b) {
+        release();
+        ctx = c;
+        if (b == 0) return BN_OK;
+        {
+            std::lock_guard<std::mutex> g(c->mu);
+            if (c->used + b > c->budget)
+                return fail(BN_EBUDGET, "cluster payload %llu bytes exceeds budget %llu bytes (%llu bytes in use)",
+                            (unsigned long long)b, (unsigned long long)c->budget, (unsigned long long)c->used);
+            c->used += b;
+            c->peak = std::max(c->peak, c->used);
+        }
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            std::lock_guard<std::mutex> g(c->mu);
+            c->used -= b;
+            p = nullptr;
+            return fail(BN_ECUDA, "cudaMalloc(%llu): %s", (unsigned long long)b, cudaGetErrorString(e));
+        }
+        bytes = b;
+        return BN_OK;
+    }
+    // Grow-only reallocation (contents not kept).
+    int reserve(bn_ctx* c, uint64_t b) { return (p && bytes >= b) ? BN_OK : alloc(c, b); }
+    template <class T>
+    T* at(uint64_t off = 0) const {
+        return reinterpret_cast<T*>(static_cast<char*>(p) + off);
+    }
+};
+
+struct PinnedMem {
+    void* p = nullptr;
+    uint64_t bytes = 0;
+    ~PinnedMem() {
+        if (p) cudaFreeHost(p);
+    }
+    int reserve(uint64_t b) {
+        if (p && bytes >= b) return BN_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        CU(cudaMallocHost(&p, b));
+        bytes = b;
+        return BN_OK;
+    }
+    template <class T>
+    T* at(uint64_t off = 0) const {
+        return reinterpret_cast<T*>(static_cast<char*>(p) + off);
+    }
+};
+
+// Bump allocator computing sub-buffer offsets (256-byte aligned).
+struct Layout {
+    uint64_t off = 0;
+    template <class T>
+    uint64_t take(uint64_t count) {
+        off = align_up(off, 256);
+        uint64_t o = off;
+        off += count * sizeof(T);
+        return o;
+    }
+};
+
+// Resident corpus: a flat cluster, or all IVF lists concatenated.
+struct Corpus {
+    uint64_t rows = 0;
+    uint32_t n = N, n1 = 128;
+    DevMem m_enc, al_cm, h_cm;
+    bool client = false;
+    DevMem L, mp_cm, s_ell, s_off, s_w, ids;
+
+    uint64_t bytes() const {
+        return m_enc.bytes + al_cm.bytes + h_cm.bytes + L.bytes + mp_cm.bytes + s_ell.bytes + s_off.bytes + s_w.bytes +
+               ids.bytes;
+    }
+};
+
+int check_shape(uint32_t n, uint32_t n1) {
+    if (n != N) return fail(BN_EINVAL, "dimension too large: n = %u, this backend is built for n = %u", n, N);
+    if (!(n1 == 64 || n1 == 128 || n1 == 256 || n1 == 512))
+        return fail(BN_EINVAL, "n1 = %u is not 1024 >> k for k in 1..=4 (params.rs:102-120)", n1);
+    return BN_OK;
+}
+
+// Row-major host [rows][cols] -> device column-major [cols][rows].
+int upload_colmajor(bn_ctx* ctx, const uint64_t* host, uint64_t rows, uint32_t cols, DevMem& dst, cudaStream_t s) {
+    TRY(dst.alloc(ctx, rows * cols * 8));
+    if (rows == 0) return BN_OK;
+    uint64_t chunk = std::max<uint64_t>(32, (256ull << 20) / (cols * 8ull));
+    chunk = std::min(chunk, rows);
+    DevMem tmp;
+    TRY(tmp.alloc(ctx, chunk * cols * 8));
+    for (uint64_t r0 = 0; r0 < rows; r0 += chunk) {
+        uint64_t cr = std::min(chunk, rows - r0);
+        CU(cudaMemcpyAsync(tmp.p, host + r0 * cols, cr * cols * 8, cudaMemcpyHostToDevice, s));
+        launch_transpose_u64(tmp.at<uint64_t>(), cr, cols, dst.at<uint64_t>() + r0, rows, s);
+        CU(cudaStreamSynchronize(s));
+    }
+    CU(cudaGetLastError());
+    return BN_OK;
+}
+
+// Device row-major -> device column-major (whole array).
+int device_colmajor(bn_ctx* ctx, const uint64_t* d_src, uint64_t rows, uint32_t cols, DevMem& dst, cudaStream_t s) {
+    TRY(dst.alloc(ctx, rows * cols * 8));
+    if (rows) launch_transpose_u64(d_src, rows, cols, dst.at<uint64_t>(), rows, s);
+    CU(cudaGetLastError());
+    return BN_OK;
+}
+
+int upload_sparse_ell(bn_ctx* ctx, bn_sparse_csr S, uint64_t rows, Corpus& c, cudaStream_t s) {
+    const uint64_t slices = (rows + 31) / 32;
+    std::vector<uint16_t> w(std::max<uint64_t>(slices, 1), 0);
+    std::vector<uint32_t> off(std::max<uint64_t>(slices, 1), 0);
+    uint64_t total = 0;
+    for (uint64_t sl = 0; sl < slices; ++sl) {
+        uint64_t mx = 0;
+        for (uint64_t i = sl * 32; i < std::min(rows, sl * 32 + 32); ++i) {
+            if (S.rowptr[i + 1] < S.rowptr[i]) return fail(BN_EINVAL, "s_mat.rowptr is not monotone at row %llu", (unsigned long long)i);
+            mx = std::max<uint64_t>(mx, S.rowptr[i + 1] - S.rowptr[i]);
+        }
+        if (mx > N) return fail(BN_EINVAL, "s_mat row with %llu entries exceeds n", (unsigned long long)mx);
+        w[sl] = (uint16_t)mx;
+        off[sl] = (uint32_t)total;
+        total += mx * 32;
+        if (total > 0xffffffffull) return fail(BN_EINVAL, "s_mat too large for the sliced-ELL layout");
+    }
+    const uint64_t nnz = rows ? S.rowptr[rows] : 0;
+    for (uint64_t e = 0; e < nnz; ++e)
+        if (S.idx[e] >= N || (S.sign[e] != 1 && S.sign[e] != -1))
+            return fail(BN_EINVAL, "s_mat entry %llu is not (col < n, sign +-1)", (unsigned long long)e);
+    TRY(c.s_ell.alloc(ctx, std::max<uint64_t>(total, 1) * 2));
+    TRY(c.s_off.alloc(ctx, off.size() * 4));
+    TRY(c.s_w.alloc(ctx, w.size() * 2));
+    CU(cudaMemcpyAsync(c.s_off.p, off.data(), off.size() * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c.s_w.p, w.data(), w.size() * 2, cudaMemcpyHostToDevice, s));
+    if (rows) {
+        DevMem rp, ix, sg;
+        TRY(rp.alloc(ctx, (rows + 1) * 8));
+        TRY(ix.alloc(ctx, std::max<uint64_t>(nnz, 1) * 4));
+        TRY(sg.alloc(ctx, std::max<uint64_t>(nnz, 1)));
+        CU(cudaMemcpyAsync(rp.p, S.rowptr, (rows + 1) * 8, cudaMemcpyHostToDevice, s));
+        if (nnz) {
+            CU(cudaMemcpyAsync(ix.p, S.idx, nnz * 4, cudaMemcpyHostToDevice, s));
+            CU(cudaMemcpyAsync(sg.p, S.sign, nnz, cudaMemcpyHostToDevice, s));
+        }
+        launch_csr_to_ell(rp.at<uint64_t>(), ix.at<uint32_t>(), sg.at<int8_t>(), rows, c.s_off.at<uint32_t>(),
+                          c.s_w.at<uint16_t>(), c.s_ell.at<uint16_t>(), s);
+        CU(cudaGetLastError());
+        CU(cudaStreamSynchronize(s));
+    }
+    return BN_OK;
+}
+
+int validate_residues(const uint64_t* a, uint64_t count, const char* what) {
+    for (uint64_t i = 0; i < count; ++i)
+        if (a[i] >= P) return fail(BN_EINVAL, "%s[%llu] = %llu is not a canonical residue mod 2^61-1", what,
+                                   (unsigned long long)i, (unsigned long long)a[i]);
+    return BN_OK;
+}
+
+int attach_client(bn_ctx* ctx, Corpus& c, const uint64_t* L, const uint64_t* m_plain, bn_sparse_csr S, cudaStream_t s) {
+    if (!L || !m_plain || (c.rows && (!S.rowptr || (S.rowptr[c.rows] && (!S.idx || !S.sign)))))
+        return fail(BN_EINVAL, "attach_client: l_subspace, m_plain and s_mat are required");
+    TRY(validate_residues(L, (uint64_t)N * c.n1, "l_subspace"));
+    TRY(c.L.alloc(ctx, (uint64_t)N * c.n1 * 8));
+    CU(cudaMemcpyAsync(c.L.p, L, (uint64_t)N * c.n1 * 8, cudaMemcpyHostToDevice, s));
+    TRY(upload_colmajor(ctx, m_plain, c.rows, N, c.mp_cm, s));
+    TRY(upload_sparse_ell(ctx, S, c.rows, c, s));
+    CU(cudaStreamSynchronize(s));
+    c.client = true;
+    return BN_OK;
+}
+
+// Device encryption: m_enc = m_q + H L^T + S (row-major, stays on device in
+// `m_enc`), AL = m_q L (row-major in `al_rm`).  crypto.rs:405-478.
+int device_encrypt(bn_ctx* ctx, const uint64_t* d_mq, uint64_t rows, uint32_t n1, const uint64_t* d_L,
+                   const uint64_t* d_H, bn_sparse_csr S, DevMem& m_enc, DevMem& al_rm, cudaStream_t s) {
+    TRY(m_enc.alloc(ctx, rows * N * 8));
+    TRY(al_rm.alloc(ctx, rows * n1 * 8));
+    if (!rows) return BN_OK;
+    // H L^T + M, K = n1
+    launch_gemm_abt(d_H, d_L, d_mq, rows, N, n1, m_enc.at<uint64_t>(), s);
+    CU(cudaGetLastError());
+    {
+        const uint64_t nnz = S.rowptr[rows];
+        DevMem rp, ix, sg;
+        TRY(rp.alloc(ctx, (rows + 1) * 8));
+        TRY(ix.alloc(ctx, std::max<uint64_t>(nnz, 1) * 4));
+        TRY(sg.alloc(ctx, std::max<uint64_t>(nnz, 1)));
+        CU(cudaMemcpyAsync(rp.p, S.rowptr, (rows + 1) * 8, cudaMemcpyHostToDevice, s));
+        if (nnz) {
+            CU(cudaMemcpyAsync(ix.p, S.idx, nnz * 4, cudaMemcpyHostToDevice, s));
+            CU(cudaMemcpyAsync(sg.p, S.sign, nnz, cudaMemcpyHostToDevice, s));
+        }
+        launch_apply_sparse(rp.at<uint64_t>(), ix.at<uint32_t>(), sg.at<int8_t>(), rows, N, m_enc.at<uint64_t>(), s);
+        CU(cudaGetLastError());
+        CU(cudaStreamSynchronize(s));
+    }
+    // AL = M L: B operand is L^T (n1 x n), K = n
+    DevMem lt;
+    TRY(lt.alloc(ctx, (uint64_t)n1 * N * 8));
+    launch_transpose_u64(d_L, N, n1, lt.at<uint64_t>(), N, s);
+    launch_gemm_abt(d_mq, lt.at<uint64_t>(), nullptr, rows, n1, N, al_rm.at<uint64_t>(), s);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(s));
+    return BN_OK;
+}
+
+int check_plain_inputs(const uint64_t* m_q, uint64_t rows, const uint64_t* L, const uint64_t* H, uint32_t n1,
+                       bn_sparse_csr S) {
+    if ((rows && (!m_q || !H || !S.rowptr)) || !L) return fail(BN_EINVAL, "null input array");
+    TRY(validate_residues(m_q, rows * N, "m_q"));
+    TRY(validate_residues(L, (uint64_t)N * n1, "l_subspace"));
+    TRY(validate_residues(H, rows * n1, "h"));
+    if (rows && S.rowptr[rows] && (!S.idx || !S.sign)) return fail(BN_EINVAL, "s_mat arrays are null");
+    for (uint64_t e = 0; rows && e < S.rowptr[rows]; ++e)
+        if (S.idx[e] >= N || (S.sign[e] != 1 && S.sign[e] != -1)) return fail(BN_EINVAL, "bad s_mat entry %llu", (unsigned long long)e);
+    return BN_OK;
+}
+
+// Encrypt on device and fill a corpus (server + client state).
+int build_corpus_from_plain(bn_ctx* ctx, Corpus& c, const uint64_t* m_q, uint64_t rows, uint32_t n1, const uint64_t* L,
+                            const uint64_t* H, bn_sparse_csr S, cudaStream_t s) {
+    c.rows = rows;
+    c.n1 = n1;
+    DevMem d_mq, d_L, d_H, al_rm;
+    TRY(d_mq.alloc(ctx, rows * N * 8));
+    TRY(d_L.alloc(ctx, (uint64_t)N * n1 * 8));
+    TRY(d_H.alloc(ctx, rows * n1 * 8));
+    if (rows) {
+        CU(cudaMemcpyAsync(d_mq.p, m_q, rows * N * 8, cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(d_H.p, H, rows * n1 * 8, cudaMemcpyHostToDevice, s));
+    }
+    CU(cudaMemcpyAsync(d_L.p, L, (uint64_t)N * n1 * 8, cudaMemcpyHostToDevice, s));
+    TRY(device_encrypt(ctx, d_mq.at<uint64_t>(), rows, n1, d_L.at<uint64_t>(), d_H.at<uint64_t>(), S, c.m_enc, al_rm, s));
+    TRY(device_colmajor(ctx, al_rm.at<uint64_t>(), rows, n1, c.al_cm, s));
+    TRY(device_colmajor(ctx, d_H.at<uint64_t>(), rows, n1, c.h_cm, s));
+    TRY(device_colmajor(ctx, d_mq.at<uint64_t>(), rows, N, c.mp_cm, s));
+    CU(cudaStreamSynchronize(s));
+    TRY(c.L.alloc(ctx, (uint64_t)N * n1 * 8));
+    CU(cudaMemcpyAsync(c.L.p, L, (uint64_t)N * n1 * 8, cudaMemcpyHostToDevice, s));
+    TRY(upload_sparse_ell(ctx, S, rows, c, s));
+    CU(cudaStreamSynchronize(s));
+    c.client = true;
+    return BN_OK;
+}
+
+// ------------------------------------------------------------------ pipeline
+struct Meta {  // device pointers
+    const ScanSeg* segs;
+    const uint64_t* seg_blk;
+    uint32_t nseg;
+    uint64_t total_blocks;
+    const VerifySeg* vsegs;
+    uint32_t nvseg;
+    const DecodeQuery* dq;
+};
+struct Scratch {  // device pointers
+    QLimb* limbs;
+    uint64_t* x;
+    uint64_t* r;
+    uint64_t* z_part;
+    uint64_t* ur_part;
+    uint32_t* flags;
+    uint64_t* ur;
+    uint64_t* zv;
+    TopkScratch topk;
+};
+struct Inputs {
+    const uint64_t* v;
+    const uint64_t* g;
+    const uint32_t* t;
+    const uint32_t* t_nnz;
+    const uint8_t* seeds;
+};
+struct Outputs {
+    uint32_t* ids;
+    int64_t* scores;
+    uint32_t* n;
+    int32_t* vfailed;  // per verify segment
+    uint64_t* mv;      // nullable
+};
+
+struct HostMeta {
+    std::vector<ScanSeg> segs;
+    std::vector<uint64_t> seg_blk;
+    std::vector<VerifySeg> vsegs;
+    std::vector<DecodeQuery> dq;
+    std::vector<uint32_t> seg_cluster;  // IVF: list id of each segment
+    uint64_t total_out = 0, max_rows = 0;
+};
+
+void finish_meta(HostMeta& hm) {
+    hm.seg_blk.assign(hm.segs.size() + 1, 0);
+    for (size_t i = 0; i < hm.segs.size(); ++i)
+        hm.seg_blk[i + 1] = hm.seg_blk[i] + (hm.segs[i].rows + SCAN_ROWS - 1) / SCAN_ROWS;
+}
+
+void flat_meta(uint64_t m, uint32_t B, HostMeta& hm) {
+    hm = HostMeta();
+    for (uint32_t b = 0; b < B; ++b) {
+        hm.segs.push_back(ScanSeg{0, (uint64_t)b * m, (uint32_t)m, b});
+        hm.vsegs.push_back(VerifySeg{0, (uint64_t)b * m, (uint32_t)m, b});
+        hm.dq.push_back(DecodeQuery{b, 1});
+    }
+    hm.total_out = (uint64_t)B * m;
+    hm.max_rows = m;
+    finish_meta(hm);
+}
+
+struct Sizes {
+    uint32_t B, n1, trials, k, ctas;
+    uint64_t total_out, nseg, nvseg;
+    FreivaldsPlan fp;
+};
+
+int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms) {
+    uint64_t by_rows = (max_rows_per_query + 8191) / 8192;
+    uint64_t by_sms = std::max<uint64_t>(1, (uint64_t)sms * 8 / std::max<uint32_t>(B, 1));
+    return (int)std::max<uint64_t>(1, std::min(by_rows, by_sms));
+}
+
+// Offsets of every device buffer of one pipeline run.
+struct RunLayout {
+    // inputs (contiguous from 0 -> one H2D)
+    uint64_t v, g, t, t_nnz, seeds, segs, seg_blk, vsegs, dq, in_end;
+    // outputs (contiguous -> one D2H)
+    uint64_t ids, scores, n, vfailed, ur, zv, out_begin, out_end;
+    // internal
+    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, total;
+};
+
+RunLayout make_layout(const Sizes& z, bool want_mv) {
+    Layout L;
+    RunLayout o{};
+    o.v = L.take<uint64_t>((uint64_t)z.B * N);
+    o.g = L.take<uint64_t>((uint64_t)z.B * z.n1);
+    o.t = L.take<uint32_t>((uint64_t)z.B * N);
+    o.t_nnz = L.take<uint32_t>(z.B);
+    o.seeds = L.take<uint8_t>((uint64_t)z.B * 32);
+    o.segs = L.take<ScanSeg>(z.nseg);
+    o.seg_blk = L.take<uint64_t>(z.nseg + 1);
+    o.vsegs = L.take<VerifySeg>(z.nvseg);
+    o.dq = L.take<DecodeQuery>(z.B);
+    o.in_end = L.off;
+    o.ids = L.take<uint32_t>((uint64_t)z.B * std::max<uint32_t>(z.k, 1));
+    o.out_begin = o.ids;
+    o.scores = L.take<int64_t>((uint64_t)z.B * std::max<uint32_t>(z.k, 1));
+    o.n = L.take<uint32_t>(z.B);
+    o.vfailed = L.take<int32_t>(std::max<uint64_t>(z.nvseg, 1));
+    o.ur = L.take<uint64_t>(std::max<uint64_t>(z.nvseg * z.trials, 1));
+    o.zv = L.take<uint64_t>(std::max<uint64_t>(z.nvseg * z.trials, 1));
+    o.out_end = L.off;
+    o.limbs = L.take<QLimb>((uint64_t)z.B * N);
+    o.x = L.take<uint64_t>((uint64_t)z.B * z.n1);
+    o.r = L.take<uint64_t>(std::max<uint64_t>(z.total_out, 1));
+    o.mv = want_mv ? L.take<uint64_t>(std::max<uint64_t>(z.total_out, 1)) : 0;
+    o.z_part = L.take<uint64_t>(z.trials ? (uint64_t)z.nvseg * z.fp.chunks * z.trials * N : 1);
+    o.ur_part = L.take<uint64_t>(z.trials ? (uint64_t)z.nvseg * z.fp.chunks * z.trials : 1);
+    o.flags = L.take<uint32_t>(1);
+    const uint64_t cand = (uint64_t)z.B * z.ctas * std::max<uint32_t>(z.k, 1);
+    o.cand_s = L.take<int64_t>(cand);
+    o.cand_i = L.take<uint32_t>(cand);
+    o.cand_n = L.take<uint32_t>((uint64_t)z.B * z.ctas);
+    o.total = L.off;
+    return o;
+}
+
+int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m, const Inputs& in, const Scratch& sc,
+                     const Outputs& out, cudaStream_t s) {
+    launch_query_limbs(in.v, z.B, sc.limbs, s);
+    launch_scan(c.m_enc.at<uint64_t>(), sc.limbs, m.segs, m.seg_blk, m.nseg, m.total_blocks, sc.r, ctx->num_sms, s);
+    if (z.trials) {
+        CU(cudaMemsetAsync(sc.flags, 0, 4, s));
+        launch_freivalds(c.m_enc.at<uint64_t>(), sc.r, m.vsegs, m.nvseg, reinterpret_cast<const ChaChaKey*>(in.seeds),
+                         z.trials, z.fp, sc.z_part, sc.ur_part, sc.flags, s);
+        launch_freivalds_finish(sc.z_part, sc.ur_part, in.v, m.vsegs, m.nvseg, z.trials, z.fp, sc.ur, sc.zv,
+                                out.vfailed, s);
+    } else {
+        CU(cudaMemsetAsync(out.vfailed, 0xff, std::max<uint64_t>(m.nvseg, 1) * 4, s));
+    }
+    if (z.k) {
+        launch_lt_times_v(c.L.at<uint64_t>(), c.n1, in.v, z.B, sc.x, s);
+        launch_decode_topk(sc.r, c.al_cm.at<uint64_t>(), c.h_cm.at<uint64_t>(), c.mp_cm.at<uint64_t>(),
+                           c.s_ell.at<uint16_t>(), c.s_off.at<uint32_t>(), c.s_w.at<uint16_t>(),
+                           c.ids.p ? c.ids.at<uint32_t>() : nullptr, c.rows, c.n1, m.segs, m.dq, z.B, in.v, in.g, sc.x,
+                           in.t, in.t_nnz, z.k, (int)z.ctas, sc.topk, out.mv, out.ids, out.scores, out.n, s);
+    } else {
+        CU(cudaMemsetAsync(out.n, 0, (uint64_t)z.B * 4, s));
+    }
+    CU(cudaGetLastError());
+    return BN_OK;
+}
+
+// Handle-side state shared by flat and IVF.
+struct Engine {
+    bn_ctx* ctx = nullptr;
+    Corpus c;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    DevMem ws;
+    PinnedMem host;
+};
+
+int engine_init(Engine& e, bn_ctx* ctx) {
+    e.ctx = ctx;
+    CU(cudaSetDevice(ctx->device));
+    CU(cudaStreamCreateWithFlags(&e.stream, cudaStreamNonBlocking));
+    return BN_OK;
+}
+
+void engine_free(Engine& e) {
+    if (e.stream) {
+        cudaStreamSynchronize(e.stream);
+        cudaStreamDestroy(e.stream);
+    }
+}
+
+// Host-buffer query: pack, one H2D, pipeline, one D2H, sync.
+int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+              const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds, uint32_t trials, uint32_t k,
+              uint32_t* ids, int64_t* scores, uint32_t* n_hits, std::vector<int32_t>& vfailed, uint64_t* r_out,
+              uint64_t* mv_out) {
+    Corpus& c = e.c;
+    if (!c.client) return fail(BN_EUNSUPPORTED, "this handle has no client state (attach_client was not called)");
+    if (k > BN_TOPK_MAX) return fail(BN_EINVAL, "k = %u exceeds BN_TOPK_MAX = %d", k, BN_TOPK_MAX);
+    if (B > 65535) return fail(BN_EINVAL, "B = %u exceeds 65535 queries per call", B);
+    if (trials && !v_seeds) return fail(BN_EINVAL, "v_seeds is required when trials > 0");
+    if (!v_enc || !g || !t_nnz) return fail(BN_EINVAL, "null query input");
+    uint64_t t_total = 0;
+    for (uint32_t b = 0; b < B; ++b) {
+        if (t_nnz[b] > N) return fail(BN_EINVAL, "t_nnz[%u] = %u exceeds n", b, t_nnz[b]);
+        t_total += t_nnz[b];
+    }
+    if (t_total && (!t_idx || !t_sign)) return fail(BN_EINVAL, "t_idx / t_sign are null");
+    TRY(validate_residues(v_enc, (uint64_t)B * N, "v_enc"));
+    TRY(validate_residues(g, (uint64_t)B * c.n1, "g"));
+
+    uint64_t max_q_rows = 0;
+    for (auto& d : hm.dq) {
+        uint64_t rsum = 0;
+        for (uint32_t s = d.seg0; s < d.seg0 + d.nseg; ++s) rsum += hm.segs[s].rows;
+        max_q_rows = std::max(max_q_rows, rsum);
+    }
+    Sizes z{B, c.n1, trials, k, (uint32_t)pick_ctas(max_q_rows, B, e.ctx->num_sms), hm.total_out, hm.segs.size(),
+            hm.vsegs.size(), plan_freivalds(std::max<uint64_t>(hm.max_rows, 1), (uint32_t)std::max<size_t>(hm.vsegs.size(), 1), e.ctx->num_sms)};
+    const RunLayout o = make_layout(z, mv_out != nullptr);
+    TRY(e.ws.reserve(e.ctx, o.total));
+    TRY(e.host.reserve(o.out_end));
+
+    // pack inputs
+    char* h = e.host.at<char>();
+    memcpy(h + o.v, v_enc, (uint64_t)B * N * 8);
+    memcpy(h + o.g, g, (uint64_t)B * c.n1 * 8);
+    uint32_t* ht = reinterpret_cast<uint32_t*>(h + o.t);
+    uint64_t tp = 0;
+    for (uint32_t b = 0; b < B; ++b) {
+        for (uint32_t i = 0; i < t_nnz[b]; ++i, ++tp) {
+            if (t_idx[tp] >= N || (t_sign[tp] != 1 && t_sign[tp] != -1))
+                return fail(BN_EINVAL, "T entry %llu is not (col < n, sign +-1)", (unsigned long long)tp);
+            ht[(uint64_t)b * N + i] = t_idx[tp] | (t_sign[tp] < 0 ? 0x80000000u : 0u);
+        }
+    }
+    memcpy(h + o.t_nnz, t_nnz, (uint64_t)B * 4);
+    if (v_seeds) memcpy(h + o.seeds, v_seeds, (uint64_t)B * 32);
+    else memset(h + o.seeds, 0, (uint64_t)B * 32);
+    memcpy(h + o.segs, hm.segs.data(), hm.segs.size() * sizeof(ScanSeg));
+    memcpy(h + o.seg_blk, hm.seg_blk.data(), hm.seg_blk.size() * 8);
+    memcpy(h + o.vsegs, hm.vsegs.data(), hm.vsegs.size() * sizeof(VerifySeg));
+    memcpy(h + o.dq, hm.dq.data(), hm.dq.size() * sizeof(DecodeQuery));
+
+    CU(cudaSetDevice(e.ctx->device));
+    char* d = e.ws.at<char>();
+    CU(cudaMemcpyAsync(d, h, o.in_end, cudaMemcpyHostToDevice, e.stream));
+    Meta m{reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk), (uint32_t)hm.segs.size(),
+           hm.seg_blk.back(), reinterpret_cast<VerifySeg*>(d + o.vsegs), (uint32_t)hm.vsegs.size(),
+           reinterpret_cast<DecodeQuery*>(d + o.dq)};
+    Inputs in{reinterpret_cast<uint64_t*>(d + o.v), reinterpret_cast<uint64_t*>(d + o.g),
+              reinterpret_cast<uint32_t*>(d + o.t), reinterpret_cast<uint32_t*>(d + o.t_nnz),
+              reinterpret_cast<uint8_t*>(d + o.seeds)};
+    Scratch sc{reinterpret_cast<QLimb*>(d + o.limbs), reinterpret_cast<uint64_t*>(d + o.x),
+               reinterpret_cast<uint64_t*>(d + o.r), reinterpret_cast<uint64_t*>(d + o.z_part),
+               reinterpret_cast<uint64_t*>(d + o.ur_part), reinterpret_cast<uint32_t*>(d + o.flags),
+               reinterpret_cast<uint64_t*>(d + o.ur), reinterpret_cast<uint64_t*>(d + o.zv),
+               TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
+                           reinterpret_cast<uint32_t*>(d + o.cand_n)}};
+    Outputs out{reinterpret_cast<uint32_t*>(d + o.ids), reinterpret_cast<int64_t*>(d + o.scores),
+                reinterpret_cast<uint32_t*>(d + o.n), reinterpret_cast<int32_t*>(d + o.vfailed),
+                mv_out ? reinterpret_cast<uint64_t*>(d + o.mv) : nullptr};
+    if (hm.segs.empty()) {
+        CU(cudaMemsetAsync(out.n, 0, (uint64_t)B * 4, e.stream));
+    } else {
+        TRY(enqueue_pipeline(e.ctx, c, z, m, in, sc, out, e.stream));
+    }
+    CU(cudaMemcpyAsync(h + o.out_begin, d + o.out_begin, o.out_end - o.out_begin, cudaMemcpyDeviceToHost, e.stream));
+    if (r_out && hm.total_out)
+        CU(cudaMemcpyAsync(r_out, d + o.r, hm.total_out * 8, cudaMemcpyDeviceToHost, e.stream));
+    if (mv_out && hm.total_out)
+        CU(cudaMemcpyAsync(mv_out, d + o.mv, hm.total_out * 8, cudaMemcpyDeviceToHost, e.stream));
+    CU(cudaStreamSynchronize(e.stream));
+
+    const uint32_t ks = std::max<uint32_t>(k, 1);
+    const uint32_t* hid = reinterpret_cast<uint32_t*>(h + o.ids);
+    const int64_t* hsc = reinterpret_cast<int64_t*>(h + o.scores);
+    const uint32_t* hn = reinterpret_cast<uint32_t*>(h + o.n);
+    for (uint32_t b = 0; b < B; ++b) {
+        const uint32_t nh = hm.segs.empty() ? 0 : hn[b];
+        if (n_hits) n_hits[b] = nh;
+        if (k) {
+            if (ids) memcpy(ids + (uint64_t)b * k, hid + (uint64_t)b * ks, (uint64_t)nh * 4);
+            if (scores) memcpy(scores + (uint64_t)b * k, hsc + (uint64_t)b * ks, (uint64_t)nh * 8);
+        }
+    }
+    vfailed.assign(hm.vsegs.size(), -1);
+    if (!hm.vsegs.empty()) memcpy(vfailed.data(), h + o.vfailed, hm.vsegs.size() * 4);
+    return BN_OK;
+}
+
+// Verify a claimed r for one contiguous row range.
+int run_verify(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* r, const uint64_t* v_enc, const uint8_t* seed,
+               uint32_t trials, int32_t* failed_trial, uint64_t* ur, uint64_t* zv) {
+    if (!failed_trial || !v_enc || !seed || (rows && !r)) return fail(BN_EINVAL, "null argument");
+    TRY(validate_residues(r, rows, "r"));
+    TRY(validate_residues(v_enc, N, "v_enc"));
+    if (trials == 0 || rows == 0) {
+        // the reference's loop body never runs: every (zero) trial passes;
+        // with m = 0 both sides are the empty sum.
+        *failed_trial = -1;
+        for (uint32_t t = 0; t < trials; ++t) { if (ur) ur[t] = 0; if (zv) zv[t] = 0; }
+        return BN_OK;
+    }
+    FreivaldsPlan fp = plan_freivalds(rows, 1, e.ctx->num_sms);
+    Layout L;
+    const uint64_t o_r = L.take<uint64_t>(rows), o_v = L.take<uint64_t>(N), o_seed = L.take<uint8_t>(32),
+                   o_vs = L.take<VerifySeg>(1), in_end = L.off;
+    const uint64_t o_fail = L.take<int32_t>(1), o_ur = L.take<uint64_t>(trials), o_zv = L.take<uint64_t>(trials),
+                   out_end = L.off;
+    const uint64_t o_zp = L.take<uint64_t>((uint64_t)fp.chunks * trials * N), o_urp = L.take<uint64_t>((uint64_t)fp.chunks * trials),
+                   o_flags = L.take<uint32_t>(1);
+    TRY(e.ws.reserve(e.ctx, L.off));
+    TRY(e.host.reserve(out_end));
+    char* h = e.host.at<char>();
+    memcpy(h + o_r, r, rows * 8);
+    memcpy(h + o_v, v_enc, N * 8);
+    memcpy(h + o_seed, seed, 32);
+    VerifySeg vs{row0, 0, (uint32_t)rows, 0};
+    memcpy(h + o_vs, &vs, sizeof vs);
+    char* d = e.ws.at<char>();
+    CU(cudaSetDevice(e.ctx->device));
+    CU(cudaMemcpyAsync(d, h, in_end, cudaMemcpyHostToDevice, e.stream));
+    CU(cudaMemsetAsync(d + o_flags, 0, 4, e.stream));
+    launch_freivalds(e.c.m_enc.at<uint64_t>(), reinterpret_cast<uint64_t*>(d + o_r), reinterpret_cast<VerifySeg*>(d + o_vs),
+                     1, reinterpret_cast<ChaChaKey*>(d + o_seed), trials, fp, reinterpret_cast<uint64_t*>(d + o_zp),
+                     reinterpret_cast<uint64_t*>(d + o_urp), reinterpret_cast<uint32_t*>(d + o_flags), e.stream);
+    launch_freivalds_finish(reinterpret_cast<uint64_t*>(d + o_zp), reinterpret_cast<uint64_t*>(d + o_urp),
+                            reinterpret_cast<uint64_t*>(d + o_v), reinterpret_cast<VerifySeg*>(d + o_vs), 1, trials, fp,
+                            reinterpret_cast<uint64_t*>(d + o_ur), reinterpret_cast<uint64_t*>(d + o_zv),
+                            reinterpret_cast<int32_t*>(d + o_fail), e.stream);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(h + o_fail, d + o_fail, out_end - o_fail, cudaMemcpyDeviceToHost, e.stream));
+    CU(cudaStreamSynchronize(e.stream));
+    *failed_trial = *reinterpret_cast<int32_t*>(h + o_fail);
+    const uint32_t ran = *failed_trial < 0 ? trials : (uint32_t)*failed_trial + 1;
+    for (uint32_t t = 0; t < trials; ++t) {
+        if (ur) ur[t] = t < ran ? reinterpret_cast<uint64_t*>(h + o_ur)[t] : 0;
+        if (zv) zv[t] = t < ran ? reinterpret_cast<uint64_t*>(h + o_zv)[t] : 0;
+    }
+    return BN_OK;
+}
+
+// Scan rows [row0, row0+rows) against B queries; r is B x rows (host).
+int run_scan(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* v_encs, uint32_t B, uint64_t* r) {
+    if (!v_encs || (rows && B && !r)) return fail(BN_EINVAL, "null argument");
+    TRY(validate_residues(v_encs, (uint64_t)B * N, "v_enc"));
+    if (!rows || !B) return BN_OK;
+    HostMeta hm;
+    for (uint32_t b = 0; b < B; ++b) hm.segs.push_back(ScanSeg{row0, (uint64_t)b * rows, (uint32_t)rows, b});
+    finish_meta(hm);
+    Layout L;
+    const uint64_t o_v = L.take<uint64_t>((uint64_t)B * N), o_s = L.take<ScanSeg>(B), o_b = L.take<uint64_t>(B + 1), in_end = L.off;
+    const uint64_t o_l = L.take<QLimb>((uint64_t)B * N), o_r = L.take<uint64_t>((uint64_t)B * rows);
+    TRY(e.ws.reserve(e.ctx, L.off));
+    TRY(e.host.reserve(in_end));
+    char* h = e.host.at<char>();
+    memcpy(h + o_v, v_encs, (uint64_t)B * N * 8);
+    memcpy(h + o_s, hm.segs.data(), B * sizeof(ScanSeg));
+    memcpy(h + o_b, hm.seg_blk.data(), (B + 1) * 8ull);
+    char* d = e.ws.at<char>();
+    CU(cudaSetDevice(e.ctx->device));
+    CU(cudaMemcpyAsync(d, h, in_end, cudaMemcpyHostToDevice, e.stream));
+    launch_query_limbs(reinterpret_cast<uint64_t*>(d + o_v), B, reinterpret_cast<QLimb*>(d + o_l), e.stream);
+    launch_scan(e.c.m_enc.at<uint64_t>(), reinterpret_cast<QLimb*>(d + o_l), reinterpret_cast<ScanSeg*>(d + o_s),
+                reinterpret_cast<uint64_t*>(d + o_b), B, hm.seg_blk.back(), reinterpret_cast<uint64_t*>(d + o_r),
+                e.ctx->num_sms, e.stream);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(r, d + o_r, (uint64_t)B * rows * 8, cudaMemcpyDeviceToHost, e.stream));
+    CU(cudaStreamSynchronize(e.stream));
+    return BN_OK;
+}
+
+int run_dense_terms(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* g, const uint64_t* lt, uint64_t* out) {
+    if (!g || !lt || (rows && !out)) return fail(BN_EINVAL, "null argument");
+    TRY(validate_residues(g, e.c.n1, "g"));
+    TRY(validate_residues(lt, e.c.n1, "lt_venc"));
+    if (!rows) return BN_OK;
+    Layout L;
+    const uint64_t o_g = L.take<uint64_t>(e.c.n1), o_x = L.take<uint64_t>(e.c.n1), in_end = L.off, o_o = L.take<uint64_t>(rows);
+    TRY(e.ws.reserve(e.ctx, L.off));
+    TRY(e.host.reserve(in_end));
+    char* h = e.host.at<char>();
+    memcpy(h + o_g, g, e.c.n1 * 8ull);
+    memcpy(h + o_x, lt, e.c.n1 * 8ull);
+    char* d = e.ws.at<char>();
+    CU(cudaSetDevice(e.ctx->device));
+    CU(cudaMemcpyAsync(d, h, in_end, cudaMemcpyHostToDevice, e.stream));
+    // column-major arrays: the list's rows are a contiguous slice of each column
+    launch_dense_terms(e.c.al_cm.at<uint64_t>() + row0, e.c.h_cm.at<uint64_t>() + row0, rows, e.c.n1,
+                       reinterpret_cast<uint64_t*>(d + o_g), reinterpret_cast<uint64_t*>(d + o_x),
+                       reinterpret_cast<uint64_t*>(d + o_o), e.stream);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(out, d + o_o, rows * 8, cudaMemcpyDeviceToHost, e.stream));
+    CU(cudaStreamSynchronize(e.stream));
+    return BN_OK;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ handles
+struct bn_flat {
+    Engine e;
+    uint64_t m = 0;
+};
+
+struct bn_ivf {
+    Engine e;
+    uint32_t nlist = 0;
+    std::vector<uint64_t> offsets;
+};
+
+struct bn_plan {
+    bn_flat* h = nullptr;
+    Sizes z{};
+    RunLayout o{};
+    DevMem ws;
+    uint32_t nseg = 0;
+    uint64_t total_blocks = 0;
+};
+
+extern "C" {
+
+const char* bn_last_error(void) { return g_err.c_str(); }
+
+const char* bn_build_info(void) {
+    static char buf[256];
+    snprintf(buf, sizeof buf, "bn_b200 abi=%d arch=sm_100a cuda=%d.%d n=%u", BN_ABI_VERSION, CUDART_VERSION / 1000,
+             (CUDART_VERSION % 1000) / 10, N);
+    return buf;
+}
+
+int bn_device_count(int* out) {
+    if (!out) return fail(BN_EINVAL, "null out");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    *out = n;
+    return BN_OK;
+}
+
+int bn_ctx_create(int device, uint64_t vram_budget_bytes, bn_ctx** out) {
+    if (!out) return fail(BN_EINVAL, "null out");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(BN_ENODEV, "no CUDA device is visible");
+    }
+    if (device < 0 || device >= count) return fail(BN_EINVAL, "device %d out of range (%d visible)", device, count);
+    CU(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CU(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10) return fail(BN_ENODEV, "device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+    size_t free_b = 0, total_b = 0;
+    CU(cudaMemGetInfo(&free_b, &total_b));
+    auto* c = new bn_ctx();
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    c->budget = vram_budget_bytes ? vram_budget_bytes : (uint64_t)(free_b * 0.8);
+    *out = c;
+    return BN_OK;
+}
+
+int bn_ctx_destroy(bn_ctx* ctx) {
+    delete ctx;
+    return BN_OK;
+}
+
+int bn_ctx_memory(const bn_ctx* ctx, uint64_t* budget, uint64_t* used, uint64_t* peak) {
+    if (!ctx) return fail(BN_EINVAL, "null ctx");
+    auto* c = const_cast<bn_ctx*>(ctx);
+    std::lock_guard<std::mutex> g(c->mu);
+    if (budget) *budget = c->budget;
+    if (used) *used = c->used;
+    if (peak) *peak = c->peak;
+    return BN_OK;
+}
+
+// ---------------------------------------------------------------- flat
+int bn_flat_build(bn_ctx* ctx, const uint64_t* m_enc, const uint64_t* a_l, const uint64_t* h, uint64_t m, uint32_t n,
+                  uint32_t n1, bn_flat** out) {
+    if (!ctx || !out) return fail(BN_EINVAL, "null argument");
+    *out = nullptr;
+    TRY(check_shape(n, n1));
+    if (m > 0xffffffffull) return fail(BN_EINVAL, "cluster size must fit in u32");
+    if (m && (!m_enc || !a_l || !h)) return fail(BN_EINVAL, "null corpus array");
+    TRY(validate_residues(m_enc, m * N, "m_enc"));
+    TRY(validate_residues(a_l, m * n1, "a_l"));
+    TRY(validate_residues(h, m * n1, "h"));
+    auto* f = new bn_flat();
+    int rc = engine_init(f->e, ctx);
+    if (rc == BN_OK) {
+        Corpus& c = f->e.c;
+        c.rows = m;
+        c.n1 = n1;
+        f->m = m;
+        rc = c.m_enc.alloc(ctx, m * N * 8);
+        if (rc == BN_OK && m) {
+            cudaError_t er = cudaMemcpyAsync(c.m_enc.p, m_enc, m * N * 8, cudaMemcpyHostToDevice, f->e.stream);
+            if (er != cudaSuccess) rc = fail(BN_ECUDA, "upload m_enc: %s", cudaGetErrorString(er));
+        }
+        if (rc == BN_OK) rc = upload_colmajor(ctx, a_l, m, n1, c.al_cm, f->e.stream);
+        if (rc == BN_OK) rc = upload_colmajor(ctx, h, m, n1, c.h_cm, f->e.stream);
+        if (rc == BN_OK && cudaStreamSynchronize(f->e.stream) != cudaSuccess) rc = fail(BN_ECUDA, "upload sync failed");
+    }
+    if (rc != BN_OK) {
+        engine_free(f->e);
+        delete f;
+        return rc;
+    }
+    *out = f;
+    return BN_OK;
+}
+
+int bn_flat_attach_client(bn_flat* f, const uint64_t* L, const uint64_t* m_plain, bn_sparse_csr s_mat) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    std::lock_guard<std::mutex> g(f->e.mu);
+    CU(cudaSetDevice(f->e.ctx->device));
+    TRY(validate_residues(m_plain, f->m * N, "m_plain"));
+    return attach_client(f->e.ctx, f->e.c, L, m_plain, s_mat, f->e.stream);
+}
+
+int bn_flat_build_from_plain(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1, const uint64_t* L,
+                             const uint64_t* H, bn_sparse_csr S, bn_flat** out) {
+    if (!ctx || !out) return fail(BN_EINVAL, "null argument");
+    *out = nullptr;
+    TRY(check_shape(n, n1));
+    if (m > 0xffffffffull) return fail(BN_EINVAL, "cluster size must fit in u32");
+    TRY(check_plain_inputs(m_q, m, L, H, n1, S));
+    auto* f = new bn_flat();
+    int rc = engine_init(f->e, ctx);
+    f->m = m;
+    if (rc == BN_OK) rc = build_corpus_from_plain(ctx, f->e.c, m_q, m, n1, L, H, S, f->e.stream);
+    if (rc != BN_OK) {
+        engine_free(f->e);
+        delete f;
+        return rc;
+    }
+    *out = f;
+    return BN_OK;
+}
+
+int bn_flat_destroy(bn_flat* f) {
+    if (!f) return BN_OK;
+    engine_free(f->e);
+    delete f;
+    return BN_OK;
+}
+
+int bn_flat_info(const bn_flat* f, uint64_t* rows, uint64_t* bytes) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    if (rows) *rows = f->m;
+    if (bytes) *bytes = f->e.c.bytes();
+    return BN_OK;
+}
+
+int bn_flat_device_m_enc(const bn_flat* f, const uint64_t** d) {
+    if (!f || !d) return fail(BN_EINVAL, "null argument");
+    *d = f->e.c.m_enc.at<uint64_t>();
+    return BN_OK;
+}
+
+int bn_flat_compute_products(bn_flat* f, const uint64_t* v_enc, uint64_t* r) {
+    return bn_flat_compute_products_batch(f, v_enc, 1, r);
+}
+
+int bn_flat_compute_products_batch(bn_flat* f, const uint64_t* v_encs, uint32_t B, uint64_t* r) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    std::lock_guard<std::mutex> g(f->e.mu);
+    return run_scan(f->e, 0, f->m, v_encs, B, r);
+}
+
+int bn_flat_decode_dense_terms(bn_flat* f, const uint64_t* g, const uint64_t* lt, uint64_t* out) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    std::lock_guard<std::mutex> gd(f->e.mu);
+    return run_dense_terms(f->e, 0, f->m, g, lt, out);
+}
+
+int bn_flat_verify(bn_flat* f, const uint64_t* r, const uint64_t* v_enc, const uint8_t v_seed[32], uint32_t trials,
+                   int32_t* failed_trial, uint64_t* ur, uint64_t* zv) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    std::lock_guard<std::mutex> g(f->e.mu);
+    return run_verify(f->e, 0, f->m, r, v_enc, v_seed, trials, failed_trial, ur, zv);
+}
+
+int bn_flat_query(bn_flat* f, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                  const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds, uint32_t trials, uint32_t k,
+                  uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed_trial, uint64_t* r_out,
+                  uint64_t* mv_out) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    if (B == 0) return BN_OK;
+    std::lock_guard<std::mutex> gd(f->e.mu);
+    HostMeta hm;
+    if (f->m) flat_meta(f->m, B, hm);
+    else {
+        for (uint32_t b = 0; b < B; ++b) hm.dq.push_back(DecodeQuery{0, 0});
+        finish_meta(hm);
+    }
+    std::vector<int32_t> vf;
+    TRY(run_query(f->e, hm, B, v_enc, g, t_idx, t_sign, t_nnz, v_seeds, trials, k, ids, scores, n_hits, vf, r_out, mv_out));
+    if (failed_trial)
+        for (uint32_t b = 0; b < B; ++b) failed_trial[b] = f->m ? vf[b] : -1;
+    return BN_OK;
+}
+
+int bn_flat_plan(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, bn_plan** out) {
+    if (!f || !out) return fail(BN_EINVAL, "null argument");
+    *out = nullptr;
+    if (!B || B > 65535) return fail(BN_EINVAL, "B must be in 1..=65535");
+    if (!f->m) return fail(BN_EINVAL, "empty corpus");
+    if (k > BN_TOPK_MAX) return fail(BN_EINVAL, "k = %u exceeds BN_TOPK_MAX", k);
+    if (k && !f->e.c.client) return fail(BN_EUNSUPPORTED, "this handle has no client state");
+    std::lock_guard<std::mutex> gd(f->e.mu);
+    HostMeta hm;
+    flat_meta(f->m, B, hm);
+    auto* p = new bn_plan();
+    p->h = f;
+    p->z = Sizes{B, f->e.c.n1, trials, k, (uint32_t)pick_ctas(f->m, B, f->e.ctx->num_sms), hm.total_out, hm.segs.size(),
+                 hm.vsegs.size(), plan_freivalds(f->m, B, f->e.ctx->num_sms)};
+    p->o = make_layout(p->z, false);
+    p->nseg = (uint32_t)hm.segs.size();
+    p->total_blocks = hm.seg_blk.back();
+    int rc = p->ws.alloc(f->e.ctx, p->o.total);
+    if (rc == BN_OK) {
+        std::vector<char> h(p->o.in_end, 0);
+        memcpy(h.data() + p->o.segs, hm.segs.data(), hm.segs.size() * sizeof(ScanSeg));
+        memcpy(h.data() + p->o.seg_blk, hm.seg_blk.data(), hm.seg_blk.size() * 8);
+        memcpy(h.data() + p->o.vsegs, hm.vsegs.data(), hm.vsegs.size() * sizeof(VerifySeg));
+        memcpy(h.data() + p->o.dq, hm.dq.data(), hm.dq.size() * sizeof(DecodeQuery));
+        if (cudaMemcpy(p->ws.p, h.data(), p->o.in_end, cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = fail(BN_ECUDA, "plan metadata upload failed");
+    }
+    if (rc != BN_OK) {
+        delete p;
+        return rc;
+    }
+    *out = p;
+    return BN_OK;
+}
+
+int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v, const uint64_t* d_g, const uint32_t* d_t, const uint32_t* d_t_nnz,
+                    const uint8_t* d_seeds, uint32_t* d_ids, int64_t* d_scores, uint32_t* d_n, int32_t* d_failed,
+                    void* stream) {
+    if (!p) return fail(BN_EINVAL, "null plan");
+    if (!d_v || (p->z.k && (!d_g || !d_t || !d_t_nnz || !d_ids || !d_scores || !d_n)) || (p->z.trials && !d_seeds) || !d_failed)
+        return fail(BN_EINVAL, "null device pointer");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char* d = p->ws.at<char>();
+    const RunLayout& o = p->o;
+    Meta m{reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk), p->nseg, p->total_blocks,
+           reinterpret_cast<VerifySeg*>(d + o.vsegs), p->nseg, reinterpret_cast<DecodeQuery*>(d + o.dq)};
+    Inputs in{d_v, d_g, d_t, d_t_nnz, d_seeds};
+    Scratch sc{reinterpret_cast<QLimb*>(d + o.limbs), reinterpret_cast<uint64_t*>(d + o.x),
+               reinterpret_cast<uint64_t*>(d + o.r), reinterpret_cast<uint64_t*>(d + o.z_part),
+               reinterpret_cast<uint64_t*>(d + o.ur_part), reinterpret_cast<uint32_t*>(d + o.flags),
+               reinterpret_cast<uint64_t*>(d + o.ur), reinterpret_cast<uint64_t*>(d + o.zv),
+               TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
+                           reinterpret_cast<uint32_t*>(d + o.cand_n)}};
+    Outputs out{d_ids, d_scores, d_n, d_failed, nullptr};
+    return enqueue_pipeline(p->h->e.ctx, p->h->e.c, p->z, m, in, sc, out, s);
+}
+
+int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v, uint64_t* d_r, void* stream) {
+    if (!p || !d_v || !d_r) return fail(BN_EINVAL, "null argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char* d = p->ws.at<char>();
+    const RunLayout& o = p->o;
+    launch_query_limbs(d_v, p->z.B, reinterpret_cast<QLimb*>(d + o.limbs), s);
+    launch_scan(p->h->e.c.m_enc.at<uint64_t>(), reinterpret_cast<QLimb*>(d + o.limbs),
+                reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk), p->nseg,
+                p->total_blocks, d_r, p->h->e.ctx->num_sms, s);
+    CU(cudaGetLastError());
+    return BN_OK;
+}
+
+int bn_plan_destroy(bn_plan* p) {
+    delete p;
+    return BN_OK;
+}
+
+// ---------------------------------------------------------------- IVF
+static int check_offsets(uint32_t nlist, const uint64_t* off) {
+    if (!off) return fail(BN_EINVAL, "null list_offsets");
+    if (off[0] != 0) return fail(BN_EINVAL, "list_offsets[0] must be 0");
+    for (uint32_t c = 0; c < nlist; ++c) {
+        if (off[c + 1] < off[c]) return fail(BN_EINVAL, "list_offsets not monotone at %u", c);
+        if (off[c + 1] - off[c] > 0xffffffffull) return fail(BN_EINVAL, "list %u larger than 2^32 rows", c);
+    }
+    return BN_OK;
+}
+
+int bn_ivf_build(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const uint32_t* ids, const uint64_t* m_enc,
+                 const uint64_t* a_l, const uint64_t* h, uint32_t n, uint32_t n1, bn_ivf** out) {
+    if (!ctx || !out) return fail(BN_EINVAL, "null argument");
+    *out = nullptr;
+    TRY(check_shape(n, n1));
+    TRY(check_offsets(nlist, off));
+    const uint64_t rows = off[nlist];
+    if (rows && (!ids || !m_enc || !a_l || !h)) return fail(BN_EINVAL, "null corpus array");
+    TRY(validate_residues(m_enc, rows * N, "m_enc"));
+    TRY(validate_residues(a_l, rows * n1, "a_l"));
+    TRY(validate_residues(h, rows * n1, "h"));
+    auto* v = new bn_ivf();
+    int rc = engine_init(v->e, ctx);
+    v->nlist = nlist;
+    v->offsets.assign(off, off + nlist + 1);
+    Corpus& c = v->e.c;
+    c.rows = rows;
+    c.n1 = n1;
+    if (rc == BN_OK) rc = c.m_enc.alloc(ctx, rows * N * 8);
+    if (rc == BN_OK && rows && cudaMemcpy(c.m_enc.p, m_enc, rows * N * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = fail(BN_ECUDA, "upload m_enc failed");
+    if (rc == BN_OK) rc = c.ids.alloc(ctx, std::max<uint64_t>(rows, 1) * 4);
+    if (rc == BN_OK && rows && cudaMemcpy(c.ids.p, ids, rows * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = fail(BN_ECUDA, "upload ids failed");
+    if (rc == BN_OK) rc = upload_colmajor(ctx, a_l, rows, n1, c.al_cm, v->e.stream);
+    if (rc == BN_OK) rc = upload_colmajor(ctx, h, rows, n1, c.h_cm, v->e.stream);
+    if (rc != BN_OK) {
+        engine_free(v->e);
+        delete v;
+        return rc;
+    }
+    *out = v;
+    return BN_OK;
+}
+
+int bn_ivf_attach_client(bn_ivf* v, const uint64_t* L, const uint64_t* m_plain, bn_sparse_csr s_mat) {
+    if (!v) return fail(BN_EINVAL, "null handle");
+    std::lock_guard<std::mutex> g(v->e.mu);
+    CU(cudaSetDevice(v->e.ctx->device));
+    TRY(validate_residues(m_plain, v->e.c.rows * N, "m_plain"));
+    return attach_client(v->e.ctx, v->e.c, L, m_plain, s_mat, v->e.stream);
+}
+
+int bn_ivf_build_from_plain(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const uint32_t* ids, const uint64_t* m_q,
+                            uint32_t n, uint32_t n1, const uint64_t* L, const uint64_t* H, bn_sparse_csr S,
+                            bn_ivf** out) {
+    if (!ctx || !out) return fail(BN_EINVAL, "null argument");
+    *out = nullptr;
+    TRY(check_shape(n, n1));
+    TRY(check_offsets(nlist, off));
+    const uint64_t rows = off[nlist];
+    if (rows && !ids) return fail(BN_EINVAL, "null ids");
+    TRY(check_plain_inputs(m_q, rows, L, H, n1, S));
+    auto* v = new bn_ivf();
+    int rc = engine_init(v->e, ctx);
+    v->nlist = nlist;
+    v->offsets.assign(off, off + nlist + 1);
+    if (rc == BN_OK) rc = build_corpus_from_plain(ctx, v->e.c, m_q, rows, n1, L, H, S, v->e.stream);
+    if (rc == BN_OK) rc = v->e.c.ids.alloc(ctx, std::max<uint64_t>(rows, 1) * 4);
+    if (rc == BN_OK && rows && cudaMemcpy(v->e.c.ids.p, ids, rows * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = fail(BN_ECUDA, "upload ids failed");
+    if (rc != BN_OK) {
+        engine_free(v->e);
+        delete v;
+        return rc;
+    }
+    *out = v;
+    return BN_OK;
+}
+
+int bn_ivf_destroy(bn_ivf* v) {
+    if (!v) return BN_OK;
+    engine_free(v->e);
+    delete v;
+    return BN_OK;
+}
+
+int bn_ivf_info(const bn_ivf* v, uint64_t* rows, uint64_t* bytes) {
+    if (!v) return fail(BN_EINVAL, "null handle");
+    if (rows) *rows = v->e.c.rows;
+    if (bytes) *bytes = v->e.c.bytes();
+    return BN_OK;
+}
+
+int bn_ivf_compute_products(bn_ivf* v, uint32_t ci, const uint64_t* v_enc, uint64_t* r, uint64_t* m_out) {
+    if (!v || !m_out) return fail(BN_EINVAL, "null argument");
+    *m_out = 0;
+    if (ci >= v->nlist) return BN_OK;
+    const uint64_t row0 = v->offsets[ci], m = v->offsets[ci + 1] - row0;
+    if (!m) return BN_OK;
+    std::lock_guard<std::mutex> g(v->e.mu);
+    TRY(run_scan(v->e, row0, m, v_enc, 1, r));
+    *m_out = m;
+    return BN_OK;
+}
+
+int bn_ivf_decode_dense_terms(bn_ivf* v, uint32_t ci, const uint64_t* g, const uint64_t* lt, uint64_t* out,
+                              uint64_t* m_out) {
+    if (!v || !m_out) return fail(BN_EINVAL, "null argument");
+    *m_out = 0;
+    if (ci >= v->nlist) return BN_OK;
+    const uint64_t row0 = v->offsets[ci], m = v->offsets[ci + 1] - row0;
+    if (!m) return BN_OK;
+    std::lock_guard<std::mutex> gd(v->e.mu);
+    // dense_terms_kernel walks columns with stride = its row count, so give
+    // it a compact copy of this list's AL / H columns.
+    Engine& e = v->e;
+    const uint32_t n1 = e.c.n1;
+    DevMem al, hh;
+    TRY(al.alloc(e.ctx, m * n1 * 8));
+    TRY(hh.alloc(e.ctx, m * n1 * 8));
+    CU(cudaMemcpy2DAsync(al.p, m * 8, e.c.al_cm.at<uint64_t>() + row0, e.c.rows * 8, m * 8, n1, cudaMemcpyDeviceToDevice, e.stream));
+    CU(cudaMemcpy2DAsync(hh.p, m * 8, e.c.h_cm.at<uint64_t>() + row0, e.c.rows * 8, m * 8, n1, cudaMemcpyDeviceToDevice, e.stream));
+    TRY(validate_residues(g, n1, "g"));
+    TRY(validate_residues(lt, n1, "lt_venc"));
+    Layout L;
+    const uint64_t o_g = L.take<uint64_t>(n1), o_x = L.take<uint64_t>(n1), in_end = L.off, o_o = L.take<uint64_t>(m);
+    TRY(e.ws.reserve(e.ctx, L.off));
+    TRY(e.host.reserve(in_end));
+    char* h = e.host.at<char>();
+    memcpy(h + o_g, g, n1 * 8ull);
+    memcpy(h + o_x, lt, n1 * 8ull);
+    char* d = e.ws.at<char>();
+    CU(cudaMemcpyAsync(d, h, in_end, cudaMemcpyHostToDevice, e.stream));
+    launch_dense_terms(al.at<uint64_t>(), hh.at<uint64_t>(), m, n1, reinterpret_cast<uint64_t*>(d + o_g),
+                       reinterpret_cast<uint64_t*>(d + o_x), reinterpret_cast<uint64_t*>(d + o_o), e.stream);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(out, d + o_o, m * 8, cudaMemcpyDeviceToHost, e.stream));
+    CU(cudaStreamSynchronize(e.stream));
+    *m_out = m;
+    return BN_OK;
+}
+
+int bn_ivf_verify(bn_ivf* v, uint32_t ci, const uint64_t* r, const uint64_t* v_enc, const uint8_t v_seed[32],
+                  uint32_t trials, int32_t* failed_trial, uint64_t* ur, uint64_t* zv) {
+    if (!v) return fail(BN_EINVAL, "null handle");
+    if (ci >= v->nlist) return fail(BN_EINVAL, "list %u out of range", ci);
+    std::lock_guard<std::mutex> g(v->e.mu);
+    const uint64_t row0 = v->offsets[ci], m = v->offsets[ci + 1] - row0;
+    return run_verify(v->e, row0, m, r, v_enc, v_seed, trials, failed_trial, ur, zv);
+}
+
+int bn_ivf_query(bn_ivf* v, uint32_t B, uint32_t nprobe, const uint32_t* probes, const uint64_t* v_enc, const uint64_t* g,
+                 const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds,
+                 uint32_t trials, uint32_t k, uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed_cluster,
+                 int32_t* failed_trial) {
+    if (!v) return fail(BN_EINVAL, "null handle");
+    if (B == 0) return BN_OK;
+    if (nprobe && !probes) return fail(BN_EINVAL, "null probes");
+    std::lock_guard<std::mutex> gd(v->e.mu);
+    HostMeta hm;
+    uint64_t out = 0;
+    for (uint32_t b = 0; b < B; ++b) {
+        const uint32_t seg0 = (uint32_t)hm.segs.size();
+        for (uint32_t p = 0; p < nprobe; ++p) {
+            const uint32_t ci = probes[(uint64_t)b * nprobe + p];
+            if (ci >= v->nlist) return fail(BN_EINVAL, "probe %u of query %u names list %u of %u", p, b, ci, v->nlist);
+            const uint64_t row0 = v->offsets[ci], m = v->offsets[ci + 1] - row0;
+            if (!m) continue;  // ivf.rs:787-789 skips empty clusters
+            hm.segs.push_back(ScanSeg{row0, out, (uint32_t)m, b});
+            hm.vsegs.push_back(VerifySeg{row0, out, (uint32_t)m, b});
+            hm.seg_cluster.push_back(ci);
+            hm.max_rows = std::max(hm.max_rows, m);
+            out += m;
+        }
+        hm.dq.push_back(DecodeQuery{seg0, (uint32_t)hm.segs.size() - seg0});
+    }
+    hm.total_out = out;
+    finish_meta(hm);
+    std::vector<int32_t> vf;
+    TRY(run_query(v->e, hm, B, v_enc, g, t_idx, t_sign, t_nnz, v_seeds, trials, k, ids, scores, n_hits, vf, nullptr, nullptr));
+    for (uint32_t b = 0; b < B; ++b) {
+        int32_t fc = -1, ft = -1;
+        const DecodeQuery& dq = hm.dq[b];
+        for (uint32_t s = dq.seg0; s < dq.seg0 + dq.nseg; ++s)
+            if (vf[s] >= 0) {
+                fc = (int32_t)hm.seg_cluster[s];
+                ft = vf[s];
+                break;
+            }
+        if (failed_cluster) failed_cluster[b] = fc;
+        if (failed_trial) failed_trial[b] = ft;
+    }
+    return BN_OK;
+}
+
+// ---------------------------------------------------------------- keygen
+int bn_encrypt_cluster(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1, const uint64_t* L,
+                       const uint64_t* H, bn_sparse_csr S, uint64_t* m_enc, uint64_t* a_l) {
+    if (!ctx) return fail(BN_EINVAL, "null ctx");
+    TRY(check_shape(n, n1));
+    TRY(check_plain_inputs(m_q, m, L, H, n1, S));
+    if (m && (!m_enc || !a_l)) return fail(BN_EINVAL, "null output");
+    if (!m) return BN_OK;
+    CU(cudaSetDevice(ctx->device));
+    cudaStream_t s;
+    CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int rc = BN_OK;
+    {
+        DevMem d_mq, d_L, d_H, enc, al;
+        rc = d_mq.alloc(ctx, m * N * 8);
+        if (rc == BN_OK) rc = d_L.alloc(ctx, (uint64_t)N * n1 * 8);
+        if (rc == BN_OK) rc = d_H.alloc(ctx, m * n1 * 8);
+        if (rc == BN_OK) {
+            cudaMemcpyAsync(d_mq.p, m_q, m * N * 8, cudaMemcpyHostToDevice, s);
+            cudaMemcpyAsync(d_L.p, L, (uint64_t)N * n1 * 8, cudaMemcpyHostToDevice, s);
+            cudaMemcpyAsync(d_H.p, H, m * n1 * 8, cudaMemcpyHostToDevice, s);
+            rc = device_encrypt(ctx, d_mq.at<uint64_t>(), m, n1, d_L.at<uint64_t>(), d_H.at<uint64_t>(), S, enc, al, s);
+        }
+        if (rc == BN_OK) {
+            cudaMemcpyAsync(m_enc, enc.p, m * N * 8, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(a_l, al.p, m * n1 * 8, cudaMemcpyDeviceToHost, s);
+            cudaError_t e = cudaStreamSynchronize(s);
+            if (e != cudaSuccess) rc = fail(BN_ECUDA, "encrypt: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaStreamDestroy(s);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,756 @@
+// bn_kernels.cu -- CUDA-core kernels of the BN path for sm_100a.
+//
+// scan_kernel       r = M_enc . v (crypto.rs:561-626 / kernels.cu:100-178),
+//                   streamed row-major with 128-bit non-allocating loads;
+//                   one work item = 4 rows x 1024 columns, split over four
+//                   warps (a quarter row each); per element 6 IMAD.WIDE
+//                   into three 64-bit limb accumulators, no carries, no
+//                   per-product fold; a transposed warp reduction and one
+//                   fold per row at the end.
+// freivalds_kernel  Protocol 2 (crypto.rs:1013-1046): u drawn on device from
+//                   the ChaCha20 keystream by index, z_t = u_t^T M_enc and
+//                   u_t . r partials per row chunk.
+// decode_topk       decode_scores (crypto.rs:901-940) + fp_to_signed + top-k
+//                   (lib.rs:452-469) in one pass over the client arrays.
+// gemm_abt          keygen-side F_p GEMMs (crypto.rs:419-467).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bn_kernels.cuh"
+
+namespace bn {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ uint4 ldg_stream(const uint4* p) {
+    uint4 v;
+    asm("ld.global.nc.L1::no_allocate.L2::256B.v4.u32 {%0,%1,%2,%3}, [%4];"
+        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+        : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ void named_bar(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+__device__ __forceinline__ uint64_t mac(uint64_t acc, uint32_t a, uint32_t b) {
+    return acc + (uint64_t)a * (uint64_t)b;
+}
+
+// ------------------------------------------------------------------ limbs
+__global__ void query_limbs_kernel(const uint64_t* __restrict__ v, uint64_t total, QLimb* __restrict__ out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    uint64_t x = v[i];
+    Limbs3 b = limbs(x), c = limbs_hi(x);
+    out[i] = QLimb{b.b0, b.b1, b.b2, c.b0, c.b1, c.b2, 0u, 0u};
+}
+
+// ------------------------------------------------------------------ scan
+constexpr int SCAN_GROUPS = 3;                 // 4-warp groups per CTA
+constexpr int SCAN_THREADS = 128 * SCAN_GROUPS;
+
+__device__ __forceinline__ uint32_t find_seg(const uint64_t* __restrict__ seg_blk, uint32_t nseg, uint32_t hint,
+                                             uint64_t blk) {
+    if (blk >= seg_blk[hint] && blk < seg_blk[hint + 1]) return hint;
+    uint32_t lo = 0, hi = nseg;  // find last s with seg_blk[s] <= blk
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (seg_blk[mid] <= blk) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(SCAN_THREADS, 1)
+scan_kernel(const uint64_t* __restrict__ m_enc, const QLimb* __restrict__ qlimbs, const ScanSeg* __restrict__ segs,
+            const uint64_t* __restrict__ seg_blk, uint32_t nseg, uint64_t total_blocks, uint64_t* __restrict__ r) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int group = warp >> 2, wq = warp & 3;
+    __shared__ unsigned long long red[2][SCAN_GROUPS][4][SCAN_ROWS][3];
+
+    uint32_t b0[8], b1[8], b2[8], c0[8], c1[8], c2[8];
+    uint32_t cur_q = 0xffffffffu, seg = 0;
+    int parity = 0;
+    const bool hi16 = (lane & 16) != 0, hi8 = (lane & 8) != 0;
+
+    for (uint64_t blk = (uint64_t)blockIdx.x * SCAN_GROUPS + group; blk < total_blocks;
+         blk += (uint64_t)gridDim.x * SCAN_GROUPS) {
+        seg = find_seg(seg_blk, nseg, seg, blk);
+        const ScanSeg sg = segs[seg];
+        const uint64_t local = (blk - seg_blk[seg]) * SCAN_ROWS;
+        const uint64_t left = (uint64_t)sg.rows - local;
+        const int nrows = left < (uint64_t)SCAN_ROWS ? (int)left : SCAN_ROWS;
+        if (sg.query != cur_q) {
+            cur_q = sg.query;
+            const QLimb* ql = qlimbs + (uint64_t)cur_q * N + wq * 256 + 2 * lane;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const QLimb q = ql[64 * k + e];
+                    b0[2 * k + e] = q.b0; b1[2 * k + e] = q.b1; b2[2 * k + e] = q.b2;
+                    c0[2 * k + e] = q.c0; c1[2 * k + e] = q.c1; c2[2 * k + e] = q.c2;
+                }
+        }
+        const uint4* base = reinterpret_cast<const uint4*>(m_enc + (sg.row0 + local) * N) + wq * 128 + lane;
+
+        uint64_t acc[SCAN_ROWS][3];
+#pragma unroll
+        for (int rr = 0; rr < SCAN_ROWS; ++rr) {
+            uint64_t a0 = 0, a1 = 0, a2 = 0;
+            if (rr < nrows) {
+                const uint4* rp = base + (uint64_t)rr * (N / 2);
+                uint4 x[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) x[k] = ldg_stream(rp + 32 * k);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int e0 = 2 * k, e1 = 2 * k + 1;
+                    a0 = mac(mac(a0, x[k].x, b0[e0]), x[k].y, c0[e0]);
+                    a1 = mac(mac(a1, x[k].x, b1[e0]), x[k].y, c1[e0]);
+                    a2 = mac(mac(a2, x[k].x, b2[e0]), x[k].y, c2[e0]);
+                    a0 = mac(mac(a0, x[k].z, b0[e1]), x[k].w, c0[e1]);
+                    a1 = mac(mac(a1, x[k].z, b1[e1]), x[k].w, c1[e1]);
+                    a2 = mac(mac(a2, x[k].z, b2[e1]), x[k].w, c2[e1]);
+                }
+            }
+            acc[rr][0] = a0; acc[rr][1] = a1; acc[rr][2] = a2;
+        }
+
+        // Transposed reduction: 4 rows x 3 accumulators over 32 lanes.  Each
+        // accumulator stays below 2^64 over the whole row (1024 products of
+        // < 2^53.2 each), so plain adds suffice.
+        uint64_t w[2][3];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                uint64_t send = hi16 ? acc[q][a] : acc[q + 2][a];
+                uint64_t keep = hi16 ? acc[q + 2][a] : acc[q][a];
+                w[q][a] = keep + __shfl_xor_sync(FULL, send, 16);
+            }
+        uint64_t xs[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            uint64_t send = hi8 ? w[0][a] : w[1][a];
+            uint64_t keep = hi8 ? w[1][a] : w[0][a];
+            xs[a] = keep + __shfl_xor_sync(FULL, send, 8);
+        }
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) xs[a] += __shfl_xor_sync(FULL, xs[a], off);
+        // lane L now holds row (L >> 3) of this warp's quarter.
+        if ((lane & 7) == 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) red[parity][group][wq][lane >> 3][a] = xs[a];
+        }
+        named_bar(1 + group, 128);
+        if (wq == 0 && lane < nrows) {
+            uint64_t s[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                s[a] = red[parity][group][0][lane][a] + red[parity][group][1][lane][a] +
+                       red[parity][group][2][lane][a] + red[parity][group][3][lane][a];
+            r[sg.out0 + local + lane] = combine3(s[0], s[1], s[2]);
+        }
+        parity ^= 1;
+    }
+}
+
+// ------------------------------------------------------------------ Freivalds
+constexpr int FV_THREADS = 256;
+constexpr int FV_TILE = 32;
+
+template <int TMAX>
+__global__ void __launch_bounds__(FV_THREADS)
+freivalds_kernel(const uint64_t* __restrict__ m_enc, const uint64_t* __restrict__ r, const VerifySeg* __restrict__ vsegs,
+                 const ChaChaKey* __restrict__ keys, uint32_t t_base, uint32_t t_cnt, uint32_t trials,
+                 uint32_t chunks, uint32_t chunk_rows, uint64_t* __restrict__ z_part, uint64_t* __restrict__ ur_part,
+                 uint32_t* __restrict__ flags, uint32_t seg_base) {
+    const uint32_t seg = seg_base + blockIdx.z, chunk = blockIdx.y;
+    const uint32_t j = blockIdx.x * FV_THREADS + threadIdx.x;
+    const VerifySeg vs = vsegs[seg];
+    const uint64_t row_begin = (uint64_t)chunk * chunk_rows;
+    const uint64_t row_end = min((uint64_t)vs.rows, row_begin + chunk_rows);
+    const ChaChaKey key = keys[vs.query];
+
+    __shared__ uint32_t ul[FV_TILE][TMAX][6];
+    __shared__ uint64_t uraw[TMAX][FV_TILE];
+
+    uint64_t acc[TMAX][3];
+#pragma unroll
+    for (int t = 0; t < TMAX; ++t) acc[t][0] = acc[t][1] = acc[t][2] = 0;
+    uint64_t urp = 0;
+    uint32_t since_fold = 0;
+    const uint32_t gen_t = threadIdx.x >> 3, gen_b = threadIdx.x & 7;
+
+    for (uint64_t tile = row_begin; tile < row_end; tile += FV_TILE) {
+        const uint32_t nt = (uint32_t)min((uint64_t)FV_TILE, row_end - tile);
+        __syncthreads();
+        if (gen_t < t_cnt) {
+            const uint64_t first = (uint64_t)(t_base + gen_t) * vs.rows + tile;  // draw index of row `tile`
+            const uint64_t blk = first / 8 + gen_b;
+            if (blk * 8 < first + nt) {
+                uint32_t w[16];
+                chacha20_block(key, blk, w);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const uint64_t idx = blk * 8 + q;
+                    if (idx >= first && idx < first + nt) {
+                        uint64_t x = ((uint64_t)w[2 * q] | ((uint64_t)w[2 * q + 1] << 32)) & P;
+                        if (x == P) { atomicOr(flags, 1u); x = 0; }
+                        const uint32_t ii = (uint32_t)(idx - first);
+                        Limbs3 b = limbs(x), c = limbs_hi(x);
+                        ul[ii][gen_t][0] = b.b0; ul[ii][gen_t][1] = b.b1; ul[ii][gen_t][2] = b.b2;
+                        ul[ii][gen_t][3] = c.b0; ul[ii][gen_t][4] = c.b1; ul[ii][gen_t][5] = c.b2;
+                        uraw[gen_t][ii] = x;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        const uint64_t* mp = m_enc + (vs.row0 + tile) * N + j;
+        for (uint32_t ii = 0; ii < nt; ++ii) {
+            const uint64_t mv = __ldg(mp + (uint64_t)ii * N);
+            const uint32_t mlo = (uint32_t)mv, mhi = (uint32_t)(mv >> 32);
+#pragma unroll
+            for (int t = 0; t < TMAX; ++t) {
+                if (t < (int)t_cnt) {
+                    const uint32_t* u = ul[ii][t];
+                    acc[t][0] = mac(mac(acc[t][0], mlo, u[0]), mhi, u[3]);
+                    acc[t][1] = mac(mac(acc[t][1], mlo, u[1]), mhi, u[4]);
+                    acc[t][2] = mac(mac(acc[t][2], mlo, u[2]), mhi, u[5]);
+                }
+            }
+        }
+        if (blockIdx.x == 0 && threadIdx.x < t_cnt) {
+            for (uint32_t ii = 0; ii < nt; ++ii)
+                urp = add_mod(urp, mul_mod(uraw[threadIdx.x][ii], r[vs.r0 + tile + ii]));
+        }
+        since_fold += nt;
+        if (since_fold >= 480) {  // 512 more rows would still fit below 2^63
+#pragma unroll
+            for (int t = 0; t < TMAX; ++t) { acc[t][0] = fold(acc[t][0]); acc[t][1] = fold(acc[t][1]); acc[t][2] = fold(acc[t][2]); }
+            since_fold = 0;
+        }
+    }
+    const uint64_t slot = (uint64_t)seg * chunks + chunk;
+#pragma unroll
+    for (int t = 0; t < TMAX; ++t)
+        if (t < (int)t_cnt) z_part[(slot * trials + t_base + t) * N + j] = combine3(acc[t][0], acc[t][1], acc[t][2]);
+    if (blockIdx.x == 0 && threadIdx.x < t_cnt) ur_part[slot * trials + t_base + threadIdx.x] = urp;
+}
+
+__device__ __forceinline__ uint64_t block_sum_mod(uint64_t v, uint64_t* sh) {
+    // 256 threads
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = add_mod(v, __shfl_xor_sync(FULL, v, off));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    if (lane == 0) sh[warp] = v;
+    __syncthreads();
+    uint64_t t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = add_mod(t, sh[w]);
+    return t;
+}
+
+__global__ void __launch_bounds__(256)
+freivalds_finish_kernel(const uint64_t* __restrict__ z_part, const uint64_t* __restrict__ ur_part,
+                        const uint64_t* __restrict__ v_enc, const VerifySeg* __restrict__ vsegs, uint32_t trials,
+                        uint32_t chunks, uint64_t* __restrict__ ur, uint64_t* __restrict__ zv,
+                        int32_t* __restrict__ failed) {
+    const uint32_t seg = blockIdx.x;
+    const VerifySeg vs = vsegs[seg];
+    const uint64_t* v = v_enc + (uint64_t)vs.query * N;
+    __shared__ uint64_t sh[32];
+    int32_t fail = -1;
+    for (uint32_t t = 0; t < trials; ++t) {
+        uint64_t part = 0;
+        for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
+            uint64_t z = 0;
+            for (uint32_t c = 0; c < chunks; ++c) z = add_mod(z, z_part[(((uint64_t)seg * chunks + c) * trials + t) * N + j]);
+            part = add_mod(part, mul_mod(z, v[j]));
+        }
+        const uint64_t zvt = block_sum_mod(part, sh);
+        if (threadIdx.x == 0) {
+            uint64_t urt = 0;
+            for (uint32_t c = 0; c < chunks; ++c) urt = add_mod(urt, ur_part[((uint64_t)seg * chunks + c) * trials + t]);
+            ur[(uint64_t)seg * trials + t] = urt;
+            zv[(uint64_t)seg * trials + t] = zvt;
+            if (fail < 0 && urt != zvt) fail = (int32_t)t;
+        }
+    }
+    if (threadIdx.x == 0) failed[seg] = fail;
+}
+
+// ------------------------------------------------------------------ L^T v
+__global__ void lt_times_v_kernel(const uint64_t* __restrict__ L, uint32_t n1, const uint64_t* __restrict__ v,
+                                  uint64_t* __restrict__ x) {
+    const uint32_t q = blockIdx.x;
+    for (uint32_t k = threadIdx.x; k < n1; k += blockDim.x) {
+        uint64_t acc = 0;
+        for (uint32_t j = 0; j < N; ++j) acc = add_mod(acc, mul_mod(L[(uint64_t)j * n1 + k], v[(uint64_t)q * N + j]));
+        x[(uint64_t)q * n1 + k] = acc;
+    }
+}
+
+// ------------------------------------------------------------------ decode
+// Dot of a column-major row with a vector whose limbs sit in shared memory.
+__device__ __forceinline__ uint64_t cm_dot(const uint64_t* __restrict__ a_cm, uint64_t rows, uint64_t row,
+                                           const uint32_t (*vl)[6], uint32_t n1) {
+    uint64_t a0 = 0, a1 = 0, a2 = 0;
+    for (uint32_t k = 0; k < n1; ++k) {
+        const uint64_t x = __ldg(a_cm + (uint64_t)k * rows + row);
+        const uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
+        a0 = mac(mac(a0, lo, vl[k][0]), hi, vl[k][3]);
+        a1 = mac(mac(a1, lo, vl[k][1]), hi, vl[k][4]);
+        a2 = mac(mac(a2, lo, vl[k][2]), hi, vl[k][5]);
+    }
+    return combine3(a0, a1, a2);
+}
+
+__global__ void dense_terms_kernel(const uint64_t* __restrict__ al_cm, const uint64_t* __restrict__ h_cm, uint64_t rows,
+                                   uint32_t n1, const uint64_t* __restrict__ g, const uint64_t* __restrict__ x,
+                                   uint64_t* __restrict__ out) {
+    __shared__ uint32_t gl[512][6], xl[512][6];
+    for (uint32_t k = threadIdx.x; k < n1; k += blockDim.x) {
+        Limbs3 b = limbs(g[k]), c = limbs_hi(g[k]);
+        gl[k][0] = b.b0; gl[k][1] = b.b1; gl[k][2] = b.b2; gl[k][3] = c.b0; gl[k][4] = c.b1; gl[k][5] = c.b2;
+        b = limbs(x[k]); c = limbs_hi(x[k]);
+        xl[k][0] = b.b0; xl[k][1] = b.b1; xl[k][2] = b.b2; xl[k][3] = c.b0; xl[k][4] = c.b1; xl[k][5] = c.b2;
+    }
+    __syncthreads();
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = add_mod(cm_dot(al_cm, rows, i, gl, n1), cm_dot(h_cm, rows, i, xl, n1));
+}
+
+constexpr int DT_THREADS = 256;
+constexpr int CAND_CAP = 2048;
+
+__device__ __forceinline__ bool better(int64_t s1, uint32_t i1, int64_t s2, uint32_t i2) {
+    return s1 > s2 || (s1 == s2 && i1 < i2);
+}
+
+// In-place bitonic sort of n (power of two) entries, best first.
+__device__ void bitonic_best_first(int64_t* s, uint32_t* id, int n) {
+    for (int size = 2; size <= n; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < n / 2; i += blockDim.x) {
+                const int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const bool sw = up ? better(s[hi], id[hi], s[lo], id[lo]) : better(s[lo], id[lo], s[hi], id[hi]);
+                if (sw) {
+                    int64_t ts = s[lo]; s[lo] = s[hi]; s[hi] = ts;
+                    uint32_t ti = id[lo]; id[lo] = id[hi]; id[hi] = ti;
+                }
+            }
+        }
+    __syncthreads();
+}
+
+// Candidate buffer of one CTA: entries better than the current k-th best
+// are appended; when the buffer nears capacity it is sorted and cut to k.
+struct TopkBuf {
+    int64_t s[CAND_CAP];
+    uint32_t id[CAND_CAP];
+    int cnt;
+    int64_t thr_s;
+    uint32_t thr_i;
+    int have_thr;
+};
+
+__device__ void topk_compact(TopkBuf& b, int k) {
+    __syncthreads();
+    const int cnt = b.cnt;
+    int n = 1;
+    while (n < cnt) n <<= 1;
+    for (int i = cnt + threadIdx.x; i < n; i += blockDim.x) { b.s[i] = INT64_MIN; b.id[i] = 0xffffffffu; }
+    bitonic_best_first(b.s, b.id, n);
+    if (threadIdx.x == 0) {
+        if (cnt >= k) {
+            b.cnt = k;
+            b.thr_s = b.s[k - 1];
+            b.thr_i = b.id[k - 1];
+            b.have_thr = 1;
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void topk_offer(TopkBuf& b, bool valid, int64_t s, uint32_t id, int64_t thr_s, uint32_t thr_i,
+                                           int have_thr) {
+    if (valid && (!have_thr || better(s, id, thr_s, thr_i))) {
+        const int pos = atomicAdd(&b.cnt, 1);
+        b.s[pos] = s;
+        b.id[pos] = id;
+    }
+}
+
+__device__ __forceinline__ uint32_t find_query_seg(const ScanSeg* __restrict__ segs, uint32_t seg0, uint32_t nseg,
+                                                   uint64_t r_idx) {
+    uint32_t lo = seg0, hi = seg0 + nseg;  // last s with segs[s].out0 <= r_idx
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (segs[mid].out0 <= r_idx) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(DT_THREADS)
+decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ al_cm, const uint64_t* __restrict__ h_cm,
+                   const uint64_t* __restrict__ mp_cm, const uint16_t* __restrict__ s_ell,
+                   const uint32_t* __restrict__ s_off, const uint16_t* __restrict__ s_w,
+                   const uint32_t* __restrict__ ids, uint64_t total_rows, uint32_t n1, const ScanSeg* __restrict__ segs,
+                   const DecodeQuery* __restrict__ queries, const uint64_t* __restrict__ vv,
+                   const uint64_t* __restrict__ gg, const uint64_t* __restrict__ xx,
+                   const uint32_t* __restrict__ t_ent, const uint32_t* __restrict__ t_nnz, uint32_t k,
+                   int64_t* __restrict__ cand_s, uint32_t* __restrict__ cand_i, uint32_t* __restrict__ cand_n,
+                   uint64_t* __restrict__ mv_out) {
+    const uint32_t q = blockIdx.y;
+    const DecodeQuery dq = queries[q];
+    if (dq.nseg == 0) {  // every probed list of this query was empty
+        if (threadIdx.x == 0) cand_n[(uint64_t)q * gridDim.x + blockIdx.x] = 0;
+        return;
+    }
+    extern __shared__ uint32_t dyn_limbs[];
+    uint32_t(*gl)[6] = reinterpret_cast<uint32_t(*)[6]>(dyn_limbs);
+    uint32_t(*xl)[6] = reinterpret_cast<uint32_t(*)[6]>(dyn_limbs + 6 * n1);
+    __shared__ uint64_t vs[N];
+    __shared__ uint32_t tl[N];
+    __shared__ TopkBuf buf;
+    const uint32_t tn = min(t_nnz[q], (uint32_t)N);
+    for (uint32_t kk = threadIdx.x; kk < n1; kk += blockDim.x) {
+        const uint64_t gv = gg[(uint64_t)q * n1 + kk], xv = xx[(uint64_t)q * n1 + kk];
+        Limbs3 b = limbs(gv), c = limbs_hi(gv);
+        gl[kk][0] = b.b0; gl[kk][1] = b.b1; gl[kk][2] = b.b2; gl[kk][3] = c.b0; gl[kk][4] = c.b1; gl[kk][5] = c.b2;
+        b = limbs(xv); c = limbs_hi(xv);
+        xl[kk][0] = b.b0; xl[kk][1] = b.b1; xl[kk][2] = b.b2; xl[kk][3] = c.b0; xl[kk][4] = c.b1; xl[kk][5] = c.b2;
+    }
+    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) vs[j] = vv[(uint64_t)q * N + j];
+    for (uint32_t c = threadIdx.x; c < tn; c += blockDim.x) tl[c] = t_ent[(uint64_t)q * N + c];
+    if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
+    __syncthreads();
+
+    const uint64_t rbase = segs[dq.seg0].out0;
+    const ScanSeg last = segs[dq.seg0 + dq.nseg - 1];
+    const uint64_t qrows = last.out0 + last.rows - rbase;
+    const uint64_t per = (qrows + gridDim.x - 1) / gridDim.x;
+    const uint64_t v_begin = (uint64_t)blockIdx.x * per;
+    const uint64_t v_end = min(qrows, v_begin + per);
+
+    for (uint64_t tile = v_begin; tile < v_end; tile += DT_THREADS) {
+        const uint64_t vrow = tile + threadIdx.x;
+        const bool valid = vrow < v_end;
+        int64_t score = 0;
+        uint32_t id = 0;
+        if (valid) {
+            const uint64_t ridx = rbase + vrow;
+            const uint32_t sidx = find_query_seg(segs, dq.seg0, dq.nseg, ridx);
+            const ScanSeg sg = segs[sidx];
+            const uint64_t grow = sg.row0 + (ridx - sg.out0);
+            // M v' = AL G + M T
+            const uint64_t al_g = cm_dot(al_cm, total_rows, grow, gl, n1);
+            uint64_t m_t = 0;
+            for (uint32_t c = 0; c < tn; ++c) {
+                const uint32_t e = tl[c];
+                const uint64_t x = __ldg(mp_cm + (uint64_t)(e & 0x3ffu) * total_rows + grow);
+                m_t = (e >> 31) ? sub_mod(m_t, x) : add_mod(m_t, x);
+            }
+            // M' v_enc = H (L^T v_enc) + S v_enc
+            const uint64_t h_x = cm_dot(h_cm, total_rows, grow, xl, n1);
+            const uint64_t slice = grow >> 5;
+            const uint32_t sl = (uint32_t)(grow & 31);
+            const uint32_t off = s_off[slice], wdt = s_w[slice];
+            uint64_t s_v = 0;
+            for (uint32_t c = 0; c < wdt; ++c) {
+                const uint16_t e = __ldg(s_ell + off + (uint64_t)c * 32 + sl);
+                if (e != 0xffffu) s_v = (e & 0x8000u) ? sub_mod(s_v, vs[e & 0x3ffu]) : add_mod(s_v, vs[e & 0x3ffu]);
+            }
+            const uint64_t mv = sub_mod(sub_mod(r[ridx], add_mod(al_g, m_t)), add_mod(h_x, s_v));
+            if (mv_out) mv_out[ridx] = mv;
+            score = to_signed(mv);
+            id = ids ? ids[grow] : (uint32_t)grow;
+        }
+        const int64_t ts = buf.thr_s;
+        const uint32_t ti = buf.thr_i;
+        const int ht = buf.have_thr;
+        topk_offer(buf, valid, score, id, ts, ti, ht);
+        __syncthreads();
+        if (buf.cnt > CAND_CAP - DT_THREADS) topk_compact(buf, (int)k);
+    }
+    topk_compact(buf, (int)k);
+    const int keep = min(buf.cnt, (int)k);
+    const uint64_t slot = (uint64_t)q * gridDim.x + blockIdx.x;
+    for (int i = threadIdx.x; i < keep; i += blockDim.x) {
+        cand_s[slot * k + i] = buf.s[i];
+        cand_i[slot * k + i] = buf.id[i];
+    }
+    if (threadIdx.x == 0) cand_n[slot] = (uint32_t)keep;
+}
+
+__global__ void __launch_bounds__(DT_THREADS)
+topk_merge_kernel(const int64_t* __restrict__ cand_s, const uint32_t* __restrict__ cand_i,
+                  const uint32_t* __restrict__ cand_n, uint32_t ctas, uint32_t k, uint32_t* __restrict__ out_ids,
+                  int64_t* __restrict__ out_scores, uint32_t* __restrict__ out_n) {
+    const uint32_t q = blockIdx.x;
+    __shared__ TopkBuf buf;
+    if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
+    __syncthreads();
+    const uint64_t total = (uint64_t)ctas * k;
+    for (uint64_t tile = 0; tile < total; tile += DT_THREADS) {
+        const uint64_t e = tile + threadIdx.x;
+        bool valid = false;
+        int64_t s = 0;
+        uint32_t id = 0;
+        if (e < total) {
+            const uint32_t c = (uint32_t)(e / k), i = (uint32_t)(e % k);
+            const uint64_t slot = (uint64_t)q * ctas + c;
+            if (i < cand_n[slot]) { valid = true; s = cand_s[slot * k + i]; id = cand_i[slot * k + i]; }
+        }
+        const int64_t ts = buf.thr_s;
+        const uint32_t ti = buf.thr_i;
+        const int ht = buf.have_thr;
+        topk_offer(buf, valid, s, id, ts, ti, ht);
+        __syncthreads();
+        if (buf.cnt > CAND_CAP - DT_THREADS) topk_compact(buf, (int)k);
+    }
+    topk_compact(buf, (int)k);
+    const int keep = min(buf.cnt, (int)k);
+    for (int i = threadIdx.x; i < keep; i += blockDim.x) {
+        out_ids[(uint64_t)q * k + i] = buf.id[i];
+        out_scores[(uint64_t)q * k + i] = buf.s[i];
+    }
+    if (threadIdx.x == 0) out_n[q] = (uint32_t)keep;
+}
+
+// ------------------------------------------------------------------ keygen GEMM
+constexpr int GT = 64;   // output tile
+constexpr int GK = 16;   // K chunk
+
+__global__ void __launch_bounds__(256)
+gemm_abt_kernel(const uint64_t* __restrict__ A, const uint64_t* __restrict__ B, const uint64_t* __restrict__ D,
+                uint64_t rows, uint32_t cols, uint32_t K, uint64_t* __restrict__ C) {
+    __shared__ uint64_t As[GT][GK + 1];
+    __shared__ uint32_t Bs[GK][GT][6];
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const uint64_t row0 = (uint64_t)blockIdx.x * GT;
+    const uint32_t col0 = blockIdx.y * GT;
+    uint64_t acc[4][4][3];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = acc[a][b][2] = 0;
+    for (uint32_t kk = 0; kk < K; kk += GK) {
+        for (int e = threadIdx.x; e < GT * GK; e += 256) {
+            const int rr = e / GK, k = e % GK;
+            const uint64_t gr = row0 + rr;
+            As[rr][k] = gr < rows ? A[gr * K + kk + k] : 0;
+            const uint32_t gc = col0 + rr;
+            const uint64_t bv = gc < cols ? B[(uint64_t)gc * K + kk + k] : 0;
+            Limbs3 lb = limbs(bv), lc = limbs_hi(bv);
+            Bs[k][rr][0] = lb.b0; Bs[k][rr][1] = lb.b1; Bs[k][rr][2] = lb.b2;
+            Bs[k][rr][3] = lc.b0; Bs[k][rr][4] = lc.b1; Bs[k][rr][5] = lc.b2;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int k = 0; k < GK; ++k) {
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const uint64_t m = As[ty + 16 * a][k];
+                const uint32_t lo = (uint32_t)m, hi = (uint32_t)(m >> 32);
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const uint32_t* l = Bs[k][tx + 16 * b];
+                    acc[a][b][0] = mac(mac(acc[a][b][0], lo, l[0]), hi, l[3]);
+                    acc[a][b][1] = mac(mac(acc[a][b][1], lo, l[1]), hi, l[4]);
+                    acc[a][b][2] = mac(mac(acc[a][b][2], lo, l[2]), hi, l[5]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const uint64_t gr = row0 + ty + 16 * a;
+            const uint32_t gc = col0 + tx + 16 * b;
+            if (gr < rows && gc < cols) {
+                uint64_t v = combine3(acc[a][b][0], acc[a][b][1], acc[a][b][2]);
+                if (D) v = add_mod(v, D[gr * cols + gc]);
+                C[gr * cols + gc] = v;
+            }
+        }
+}
+
+__global__ void apply_sparse_kernel(const uint64_t* __restrict__ rowptr, const uint32_t* __restrict__ idx,
+                                    const int8_t* __restrict__ sign, uint64_t rows, uint32_t cols,
+                                    uint64_t* __restrict__ C) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x)
+        for (uint64_t c = rowptr[i]; c < rowptr[i + 1]; ++c) {
+            uint64_t* p = C + i * cols + idx[c];
+            *p = sign[c] > 0 ? add_mod(*p, 1) : sub_mod(*p, 1);
+        }
+}
+
+__global__ void transpose_u64_kernel(const uint64_t* __restrict__ in, uint64_t rows, uint32_t cols,
+                                     uint64_t* __restrict__ out, uint64_t out_ld) {
+    __shared__ uint64_t t[32][33];
+    const uint64_t r0 = (uint64_t)blockIdx.x * 32;
+    const uint32_t c0 = blockIdx.y * 32;
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const uint64_t r = r0 + yy;
+        const uint32_t c = c0 + threadIdx.x;
+        t[yy][threadIdx.x] = (r < rows && c < cols) ? in[r * cols + c] : 0;
+    }
+    __syncthreads();
+    for (int yy = threadIdx.y; yy < 32; yy += blockDim.y) {
+        const uint32_t c = c0 + yy;
+        const uint64_t r = r0 + threadIdx.x;
+        if (r < rows && c < cols) out[(uint64_t)c * out_ld + r] = t[threadIdx.x][yy];
+    }
+}
+
+__global__ void csr_to_ell_kernel(const uint64_t* __restrict__ rowptr, const uint32_t* __restrict__ idx,
+                                  const int8_t* __restrict__ sign, uint64_t rows, const uint32_t* __restrict__ s_off,
+                                  const uint16_t* __restrict__ s_w, uint16_t* __restrict__ ell) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t slice = i >> 5;
+        const uint32_t sl = (uint32_t)(i & 31), off = s_off[slice], w = s_w[slice];
+        const uint64_t b = rowptr[i], e = rowptr[i + 1];
+        for (uint32_t c = 0; c < w; ++c) {
+            uint16_t v = 0xffffu;
+            if (b + c < e) v = (uint16_t)(idx[b + c] | (sign[b + c] < 0 ? 0x8000u : 0u));
+            ell[off + (uint64_t)c * 32 + sl] = v;
+        }
+    }
+}
+
+inline unsigned grid_for(uint64_t n, unsigned threads, unsigned cap = 65535u * 16u) {
+    uint64_t g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+void launch_query_limbs(const uint64_t* d_v, uint32_t nq, QLimb* d_limbs, cudaStream_t s) {
+    const uint64_t total = (uint64_t)nq * N;
+    query_limbs_kernel<<<grid_for(total, 256), 256, 0, s>>>(d_v, total, d_limbs);
+}
+
+void launch_scan(const uint64_t* d_m_enc, const QLimb* d_limbs, const ScanSeg* d_segs, const uint64_t* d_seg_blk,
+                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, cudaStream_t s) {
+    if (total_blocks == 0) return;
+    uint64_t want = (total_blocks + SCAN_GROUPS - 1) / SCAN_GROUPS;
+    unsigned grid = (unsigned)(want < (uint64_t)num_sms ? want : (uint64_t)num_sms);
+    scan_kernel<<<grid, SCAN_THREADS, 0, s>>>(d_m_enc, d_limbs, d_segs, d_seg_blk, nseg, total_blocks, d_r);
+}
+
+FreivaldsPlan plan_freivalds(uint64_t max_rows, uint32_t nseg, int num_sms) {
+    // aim for ~2 waves of 4-column-block CTAs over all segments
+    uint64_t target_ctas = (uint64_t)num_sms * 4;
+    uint64_t per_seg = target_ctas / (4ull * (nseg ? nseg : 1));
+    if (per_seg < 1) per_seg = 1;
+    uint64_t chunk_rows = (max_rows + per_seg - 1) / per_seg;
+    chunk_rows = ((chunk_rows + FV_TILE - 1) / FV_TILE) * FV_TILE;
+    if (chunk_rows < FV_TILE) chunk_rows = FV_TILE;
+    uint64_t chunks = (max_rows + chunk_rows - 1) / chunk_rows;
+    if (chunks < 1) chunks = 1;
+    return FreivaldsPlan{(uint32_t)chunks, (uint32_t)chunk_rows};
+}
+
+void launch_freivalds(const uint64_t* d_m_enc, const uint64_t* d_r, const VerifySeg* d_vsegs, uint32_t nseg,
+                      const ChaChaKey* d_keys, uint32_t trials, FreivaldsPlan plan, uint64_t* d_z_part,
+                      uint64_t* d_ur_part, uint32_t* d_flags, cudaStream_t s) {
+    for (uint32_t s0 = 0; s0 < nseg; s0 += 65535u) {
+        const uint32_t ns = nseg - s0 < 65535u ? nseg - s0 : 65535u;
+        dim3 grid(N / FV_THREADS, plan.chunks, ns);
+        for (uint32_t t0 = 0; t0 < trials;) {
+            const uint32_t left = trials - t0;
+            if (left > 8) {
+                const uint32_t c = left < 24 ? left : 24;
+                freivalds_kernel<24><<<grid, FV_THREADS, 0, s>>>(d_m_enc, d_r, d_vsegs, d_keys, t0, c, trials, plan.chunks,
+                                                                 plan.chunk_rows, d_z_part, d_ur_part, d_flags, s0);
+                t0 += c;
+            } else if (left > 4) {
+                freivalds_kernel<8><<<grid, FV_THREADS, 0, s>>>(d_m_enc, d_r, d_vsegs, d_keys, t0, left, trials,
+                                                                plan.chunks, plan.chunk_rows, d_z_part, d_ur_part, d_flags, s0);
+                t0 += left;
+            } else {
+                freivalds_kernel<4><<<grid, FV_THREADS, 0, s>>>(d_m_enc, d_r, d_vsegs, d_keys, t0, left, trials,
+                                                                plan.chunks, plan.chunk_rows, d_z_part, d_ur_part, d_flags, s0);
+                t0 += left;
+            }
+        }
+    }
+}
+
+void launch_freivalds_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint64_t* d_v_enc,
+                             const VerifySeg* d_vsegs, uint32_t nseg, uint32_t trials, FreivaldsPlan plan,
+                             uint64_t* d_ur, uint64_t* d_zv, int32_t* d_failed, cudaStream_t s) {
+    freivalds_finish_kernel<<<nseg, 256, 0, s>>>(d_z_part, d_ur_part, d_v_enc, d_vsegs, trials, plan.chunks, d_ur, d_zv,
+                                                 d_failed);
+}
+
+void launch_lt_times_v(const uint64_t* d_L, uint32_t n1, const uint64_t* d_v, uint32_t nq, uint64_t* d_x,
+                       cudaStream_t s) {
+    lt_times_v_kernel<<<nq, 128, 0, s>>>(d_L, n1, d_v, d_x);
+}
+
+void launch_dense_terms(const uint64_t* d_al_cm, const uint64_t* d_h_cm, uint64_t rows, uint32_t n1,
+                        const uint64_t* d_g, const uint64_t* d_x, uint64_t* d_out, cudaStream_t s) {
+    dense_terms_kernel<<<grid_for(rows, 256, 148 * 8), 256, 0, s>>>(d_al_cm, d_h_cm, rows, n1, d_g, d_x, d_out);
+}
+
+void launch_decode_topk(const uint64_t* d_r, const uint64_t* d_al_cm, const uint64_t* d_h_cm, const uint64_t* d_mp_cm,
+                        const uint16_t* d_s_ell, const uint32_t* d_s_off, const uint16_t* d_s_w, const uint32_t* d_ids,
+                        uint64_t total_rows, uint32_t n1, const ScanSeg* d_segs, const DecodeQuery* d_q, uint32_t nq,
+                        const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
+                        const uint32_t* d_t_nnz, uint32_t k, int ctas_per_query, TopkScratch scratch,
+                        uint64_t* d_mv_out, uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n,
+                        cudaStream_t s) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(decode_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 6 * 4 * 512);
+        attr_set = true;
+    }
+    dim3 grid(ctas_per_query, nq);
+    decode_topk_kernel<<<grid, DT_THREADS, 2 * 6 * 4 * n1, s>>>(d_r, d_al_cm, d_h_cm, d_mp_cm, d_s_ell, d_s_off, d_s_w, d_ids,
+                                                   total_rows, n1, d_segs, d_q, d_v, d_g, d_x, d_t, d_t_nnz, k,
+                                                   scratch.cand_s, scratch.cand_i, scratch.cand_n, d_mv_out);
+    topk_merge_kernel<<<nq, DT_THREADS, 0, s>>>(scratch.cand_s, scratch.cand_i, scratch.cand_n, ctas_per_query, k,
+                                                d_out_ids, d_out_scores, d_out_n);
+}
+
+void launch_gemm_abt(const uint64_t* d_A, const uint64_t* d_B, const uint64_t* d_D, uint64_t rows, uint32_t cols,
+                     uint32_t K, uint64_t* d_C, cudaStream_t s) {
+    dim3 grid((unsigned)((rows + GT - 1) / GT), (cols + GT - 1) / GT);
+    gemm_abt_kernel<<<grid, 256, 0, s>>>(d_A, d_B, d_D, rows, cols, K, d_C);
+}
+
+void launch_apply_sparse(const uint64_t* d_rowptr, const uint32_t* d_idx, const int8_t* d_sign, uint64_t rows,
+                         uint32_t cols, uint64_t* d_C, cudaStream_t s) {
+    apply_sparse_kernel<<<grid_for(rows, 256, 148 * 16), 256, 0, s>>>(d_rowptr, d_idx, d_sign, rows, cols, d_C);
+}
+
+void launch_transpose_u64(const uint64_t* d_in, uint64_t rows, uint32_t cols, uint64_t* d_out, uint64_t out_ld,
+                          cudaStream_t s) {
+    dim3 grid((unsigned)((rows + 31) / 32), (cols + 31) / 32);
+    transpose_u64_kernel<<<grid, dim3(32, 8), 0, s>>>(d_in, rows, cols, d_out, out_ld);
+}
+
+void launch_csr_to_ell(const uint64_t* d_rowptr, const uint32_t* d_idx, const int8_t* d_sign, uint64_t rows,
+                       const uint32_t* d_s_off, const uint16_t* d_s_w, uint16_t* d_s_ell, cudaStream_t s) {
+    csr_to_ell_kernel<<<grid_for(rows, 256, 148 * 16), 256, 0, s>>>(d_rowptr, d_idx, d_sign, rows, d_s_off, d_s_w, d_s_ell);
+}
+
+}  // namespace bn

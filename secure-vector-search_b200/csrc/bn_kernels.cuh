@@ -1,0 +1,130 @@
+// bn_kernels.cuh -- launchers for the BN device kernels (sm_100a).
+//
+// Device data layout (one flat corpus, or the concatenation of all IVF
+// lists in list order):
+//   m_enc   u64 [rows][1024]   row-major, 8 KiB per row   (server state)
+//   al_cm   u64 [128][rows]    AL, column-major           (client state)
+//   h_cm    u64 [128][rows]    H,  column-major
+//   mp_cm   u64 [1024][rows]   plaintext M, column-major  (M*T column sums)
+//   s_ell   u16 sliced-ELL of S: 32-row slices, entry = col | 0x8000 for -1,
+//           0xFFFF = padding; s_off[slice] = u32 offset of the slice's data,
+//           s_w[slice] = width
+//   ids     u32 [rows]         global vector id of each row (IVF), or null
+// Column-major client arrays make the decode's thread-per-row reads
+// coalesced; the row-major m_enc makes the scan's warp-per-row reads
+// coalesced.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bn_chacha.cuh"
+#include "bn_fp.cuh"
+
+namespace bn {
+
+// Per-query operand limbs for the scan: v = b0 + b1 2^21 + b2 2^42 and the
+// same split of v * 2^32 mod p (c0..c2), padded to 32 bytes.
+struct QLimb {
+    uint32_t b0, b1, b2, c0, c1, c2, pad0, pad1;
+};
+
+// A contiguous run of rows scanned against one query; r lands at out0.
+struct ScanSeg {
+    uint64_t row0;
+    uint64_t out0;
+    uint32_t rows;
+    uint32_t query;
+};
+
+// Rows per work item of the scan (one group of four warps).
+constexpr int SCAN_ROWS = 4;
+
+// Freivalds: per (segment, trial group) the u stream is ChaCha20Rng keyed
+// by v_seed; u_t[i] is draw number t*m_seg + i of that stream (crypto.rs:
+// 1026-1027).  Bit 0 of *flags is set if a draw hit the rejected value p
+// (probability 2^-61 per draw), meaning later draws of the reference
+// stream would be shifted by one.
+struct VerifySeg {
+    uint64_t row0;   // first row in m_enc
+    uint64_t r0;     // first r value of this segment
+    uint32_t rows;   // m of the list / flat corpus
+    uint32_t query;  // index into v_enc / keys arrays
+};
+
+void launch_query_limbs(const uint64_t* d_v, uint32_t nq, QLimb* d_limbs, cudaStream_t s);
+
+// Segment scan: r[out0 + i] = sum_j m_enc[row0 + i][j] * v[query][j] mod p.
+// seg_blk: exclusive prefix sum over ceil(rows / SCAN_ROWS), nseg + 1 entries.
+void launch_scan(const uint64_t* d_m_enc, const QLimb* d_limbs, const ScanSeg* d_segs, const uint64_t* d_seg_blk,
+                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, cudaStream_t s);
+
+// Freivalds partial sums for one segment list.  z_part: [nseg][chunks][T][1024],
+// ur_part: [nseg][chunks][T].  chunk_rows: rows per chunk (multiple of 32).
+struct FreivaldsPlan {
+    uint32_t chunks;      // per segment
+    uint32_t chunk_rows;
+};
+FreivaldsPlan plan_freivalds(uint64_t max_rows, uint32_t nseg, int num_sms);
+void launch_freivalds(const uint64_t* d_m_enc, const uint64_t* d_r, const VerifySeg* d_vsegs, uint32_t nseg,
+                      const ChaChaKey* d_keys, uint32_t trials, FreivaldsPlan plan, uint64_t* d_z_part,
+                      uint64_t* d_ur_part, uint32_t* d_flags, cudaStream_t s);
+// Per segment: ur[t], zv[t], first failing trial (-1 if none).
+void launch_freivalds_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint64_t* d_v_enc,
+                             const VerifySeg* d_vsegs, uint32_t nseg, uint32_t trials, FreivaldsPlan plan,
+                             uint64_t* d_ur, uint64_t* d_zv, int32_t* d_failed, cudaStream_t s);
+
+// x = L^T v for nq queries: L is [1024][n1] row-major, x is [nq][n1].
+void launch_lt_times_v(const uint64_t* d_L, uint32_t n1, const uint64_t* d_v, uint32_t nq, uint64_t* d_x,
+                       cudaStream_t s);
+
+// Dense decode terms only: out[i] = AL_i . g + H_i . x (FlatGpuState::
+// decode_dense_terms, gpu/mod.rs:390-408).
+void launch_dense_terms(const uint64_t* d_al_cm, const uint64_t* d_h_cm, uint64_t rows, uint32_t n1,
+                        const uint64_t* d_g, const uint64_t* d_x, uint64_t* d_out, cudaStream_t s);
+
+// Per-query segment range for decode + rank.  Query q's operands sit at
+// fixed strides: v_enc at q*1024, g and x at q*n1, T entries at q*1024
+// (t_nnz[q] of them, entry = col | 0x80000000 for -1).
+struct DecodeQuery {
+    uint32_t seg0;     // first segment of this query in the segment array
+    uint32_t nseg;
+};
+
+// Top-k candidate lists.
+constexpr int TOPK_MAX = 1024;
+constexpr int DECODE_CTAS_PER_QUERY_MAX = 148;
+
+struct TopkScratch {
+    int64_t* cand_s;    // [nq][ctas][k]
+    uint32_t* cand_i;
+    uint32_t* cand_n;   // [nq][ctas]
+};
+
+// Decode + fp_to_signed + per-CTA top-k for every query, then a merge into
+// out_ids/out_scores [nq][k] (score desc, id asc) and out_n [nq].
+// r is indexed like the scan output (segment out0).  mv_out (nullable)
+// receives the decoded residues at the same offsets.
+void launch_decode_topk(const uint64_t* d_r, const uint64_t* d_al_cm, const uint64_t* d_h_cm, const uint64_t* d_mp_cm,
+                        const uint16_t* d_s_ell, const uint32_t* d_s_off, const uint16_t* d_s_w, const uint32_t* d_ids,
+                        uint64_t total_rows, uint32_t n1, const ScanSeg* d_segs, const DecodeQuery* d_q, uint32_t nq,
+                        const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
+                        const uint32_t* d_t_nnz, uint32_t k, int ctas_per_query, TopkScratch scratch,
+                        uint64_t* d_mv_out, uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n,
+                        cudaStream_t s);
+
+// Keygen-side dense F_p GEMM: C[i][j] = sum_k A[i][k] * B[j][k]  (A: rows x K,
+// B: cols x K, both row-major), optionally C += D (same shape, row-major).
+// K must be a multiple of 16 and at most 1024.
+void launch_gemm_abt(const uint64_t* d_A, const uint64_t* d_B, const uint64_t* d_D, uint64_t rows, uint32_t cols,
+                     uint32_t K, uint64_t* d_C, cudaStream_t s);
+// Applies a CSR {-1,+1} matrix: C[i][idx] +-= 1 (mod p).
+void launch_apply_sparse(const uint64_t* d_rowptr, const uint32_t* d_idx, const int8_t* d_sign, uint64_t rows,
+                         uint32_t cols, uint64_t* d_C, cudaStream_t s);
+// Row-major [rows][cols] -> column-major: out[c * out_ld + r].
+void launch_transpose_u64(const uint64_t* d_in, uint64_t rows, uint32_t cols, uint64_t* d_out, uint64_t out_ld,
+                          cudaStream_t s);
+// CSR -> sliced ELL (see layout note above); s_off/s_w computed on host.
+void launch_csr_to_ell(const uint64_t* d_rowptr, const uint32_t* d_idx, const int8_t* d_sign, uint64_t rows,
+                       const uint32_t* d_s_off, const uint16_t* d_s_w, uint16_t* d_s_ell, cudaStream_t s);
+
+}  // namespace bn
