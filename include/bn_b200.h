@@ -130,6 +130,10 @@ int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v_enc, const uint64_t* d_g, co
                     uint32_t* d_n, int32_t* d_failed, void* stream);
 /* Scan-only enqueue of the same plan: d_r (B x m) = M_enc v_enc. */
 int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v_enc, uint64_t* d_r, void* stream);
+/* Device flags of the last enqueue of this plan (0 = healthy; non-zero when
+ * a bounded device-side wait timed out and the outputs must be discarded).
+ * Synchronous: call after the enqueued work has completed. */
+int bn_plan_status(bn_plan* p, uint32_t* device_flags);
 int bn_plan_destroy(bn_plan* p);
 
 /* ---------------------------------------------------------------- IVF

@@ -60,6 +60,7 @@ _SIGS = {
     "bn_flat_plan": (C.c_int, [vp, u32, u32, u32, vp]),
     "bn_plan_enqueue": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "bn_plan_enqueue_scan": (C.c_int, [vp, vp, vp, vp]),
+    "bn_plan_status": (C.c_int, [vp, vp]),
     "bn_plan_destroy": (C.c_int, [vp]),
     "bn_ivf_build": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, u32, u32, vp]),
     "bn_ivf_attach_client": (C.c_int, [vp, vp, vp, SparseCsr]),
@@ -255,6 +256,11 @@ class Plan:
 
     def enqueue_scan(self, d_v, d_r, stream: int):
         check(lib.bn_plan_enqueue_scan(self.h, d_v, d_r, stream))
+
+    def status(self) -> int:
+        f = u32(0)
+        check(lib.bn_plan_status(self.h, C.byref(f)))
+        return f.value
 
     def close(self):
         if self.h:

@@ -348,6 +348,7 @@ struct Scratch {  // device pointers
     uint64_t* ur;
     uint64_t* zv;
     TopkScratch topk;
+    uint32_t* err;  // device pipeline timeout flags
 };
 struct Inputs {
     const uint64_t* v;
@@ -398,7 +399,7 @@ struct Sizes {
 };
 
 int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms) {
-    uint64_t by_rows = (max_rows_per_query + 8191) / 8192;
+    uint64_t by_rows = (max_rows_per_query + 255) / 256;
     uint64_t by_sms = std::max<uint64_t>(1, (uint64_t)sms * 8 / std::max<uint32_t>(B, 1));
     return (int)std::max<uint64_t>(1, std::min(by_rows, by_sms));
 }
@@ -408,7 +409,7 @@ struct RunLayout {
     // inputs (contiguous from 0 -> one H2D)
     uint64_t v, g, t, t_nnz, seeds, segs, seg_blk, vsegs, dq, in_end;
     // outputs (contiguous -> one D2H)
-    uint64_t ids, scores, n, vfailed, ur, zv, out_begin, out_end;
+    uint64_t ids, scores, n, vfailed, ur, zv, err, out_begin, out_end;
     // internal
     uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, total;
 };
@@ -433,6 +434,7 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
     o.vfailed = L.take<int32_t>(std::max<uint64_t>(z.nvseg, 1));
     o.ur = L.take<uint64_t>(std::max<uint64_t>(z.nvseg * z.trials, 1));
     o.zv = L.take<uint64_t>(std::max<uint64_t>(z.nvseg * z.trials, 1));
+    o.err = L.take<uint32_t>(1);
     o.out_end = L.off;
     o.limbs = L.take<QLimb>((uint64_t)z.B * N);
     o.x = L.take<uint64_t>((uint64_t)z.B * z.n1);
@@ -451,8 +453,10 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
 
 int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m, const Inputs& in, const Scratch& sc,
                      const Outputs& out, cudaStream_t s) {
+    CU(cudaMemsetAsync(sc.err, 0, 4, s));
     launch_query_limbs(in.v, z.B, sc.limbs, s);
-    launch_scan(c.m_enc.at<uint64_t>(), sc.limbs, m.segs, m.seg_blk, m.nseg, m.total_blocks, sc.r, ctx->num_sms, s);
+    launch_scan(c.m_enc.at<uint64_t>(), sc.limbs, m.segs, m.seg_blk, m.nseg, m.total_blocks, sc.r, ctx->num_sms, sc.err,
+                s);
     if (z.trials) {
         CU(cudaMemsetAsync(sc.flags, 0, 4, s));
         launch_freivalds(c.m_enc.at<uint64_t>(), sc.r, m.vsegs, m.nvseg, reinterpret_cast<const ChaChaKey*>(in.seeds),
@@ -566,12 +570,14 @@ int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const 
                reinterpret_cast<uint64_t*>(d + o.ur_part), reinterpret_cast<uint32_t*>(d + o.flags),
                reinterpret_cast<uint64_t*>(d + o.ur), reinterpret_cast<uint64_t*>(d + o.zv),
                TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
-                           reinterpret_cast<uint32_t*>(d + o.cand_n)}};
+                           reinterpret_cast<uint32_t*>(d + o.cand_n)},
+               reinterpret_cast<uint32_t*>(d + o.err)};
     Outputs out{reinterpret_cast<uint32_t*>(d + o.ids), reinterpret_cast<int64_t*>(d + o.scores),
                 reinterpret_cast<uint32_t*>(d + o.n), reinterpret_cast<int32_t*>(d + o.vfailed),
                 mv_out ? reinterpret_cast<uint64_t*>(d + o.mv) : nullptr};
     if (hm.segs.empty()) {
         CU(cudaMemsetAsync(out.n, 0, (uint64_t)B * 4, e.stream));
+        CU(cudaMemsetAsync(sc.err, 0, 4, e.stream));
     } else {
         TRY(enqueue_pipeline(e.ctx, c, z, m, in, sc, out, e.stream));
     }
@@ -581,6 +587,8 @@ int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const 
     if (mv_out && hm.total_out)
         CU(cudaMemcpyAsync(mv_out, d + o.mv, hm.total_out * 8, cudaMemcpyDeviceToHost, e.stream));
     CU(cudaStreamSynchronize(e.stream));
+    if (const uint32_t ev = *reinterpret_cast<uint32_t*>(h + o.err))
+        return fail(BN_ECUDA, "a device pipeline wait timed out (flags 0x%x); results discarded", ev);
 
     const uint32_t ks = std::max<uint32_t>(k, 1);
     const uint32_t* hid = reinterpret_cast<uint32_t*>(h + o.ids);
@@ -662,8 +670,9 @@ int run_scan(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* v_encs, ui
     Layout L;
     const uint64_t o_v = L.take<uint64_t>((uint64_t)B * N), o_s = L.take<ScanSeg>(B), o_b = L.take<uint64_t>(B + 1), in_end = L.off;
     const uint64_t o_l = L.take<QLimb>((uint64_t)B * N), o_r = L.take<uint64_t>((uint64_t)B * rows);
+    const uint64_t o_e = L.take<uint32_t>(1);
     TRY(e.ws.reserve(e.ctx, L.off));
-    TRY(e.host.reserve(in_end));
+    TRY(e.host.reserve(std::max<uint64_t>(in_end, 4)));
     char* h = e.host.at<char>();
     memcpy(h + o_v, v_encs, (uint64_t)B * N * 8);
     memcpy(h + o_s, hm.segs.data(), B * sizeof(ScanSeg));
@@ -671,13 +680,17 @@ int run_scan(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* v_encs, ui
     char* d = e.ws.at<char>();
     CU(cudaSetDevice(e.ctx->device));
     CU(cudaMemcpyAsync(d, h, in_end, cudaMemcpyHostToDevice, e.stream));
+    CU(cudaMemsetAsync(d + o_e, 0, 4, e.stream));
     launch_query_limbs(reinterpret_cast<uint64_t*>(d + o_v), B, reinterpret_cast<QLimb*>(d + o_l), e.stream);
     launch_scan(e.c.m_enc.at<uint64_t>(), reinterpret_cast<QLimb*>(d + o_l), reinterpret_cast<ScanSeg*>(d + o_s),
                 reinterpret_cast<uint64_t*>(d + o_b), B, hm.seg_blk.back(), reinterpret_cast<uint64_t*>(d + o_r),
-                e.ctx->num_sms, e.stream);
+                e.ctx->num_sms, reinterpret_cast<uint32_t*>(d + o_e), e.stream);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(r, d + o_r, (uint64_t)B * rows * 8, cudaMemcpyDeviceToHost, e.stream));
+    uint32_t ev = 0;
+    CU(cudaMemcpyAsync(&ev, d + o_e, 4, cudaMemcpyDeviceToHost, e.stream));
     CU(cudaStreamSynchronize(e.stream));
+    if (ev) return fail(BN_ECUDA, "a device pipeline wait timed out (flags 0x%x); results discarded", ev);
     return BN_OK;
 }
 
@@ -969,7 +982,8 @@ int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v, const uint64_t* d_g, const 
                reinterpret_cast<uint64_t*>(d + o.ur_part), reinterpret_cast<uint32_t*>(d + o.flags),
                reinterpret_cast<uint64_t*>(d + o.ur), reinterpret_cast<uint64_t*>(d + o.zv),
                TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
-                           reinterpret_cast<uint32_t*>(d + o.cand_n)}};
+                           reinterpret_cast<uint32_t*>(d + o.cand_n)},
+               reinterpret_cast<uint32_t*>(d + o.err)};
     Outputs out{d_ids, d_scores, d_n, d_failed, nullptr};
     return enqueue_pipeline(p->h->e.ctx, p->h->e.c, p->z, m, in, sc, out, s);
 }
@@ -979,11 +993,18 @@ int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v, uint64_t* d_r, void* s
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     char* d = p->ws.at<char>();
     const RunLayout& o = p->o;
+    CU(cudaMemsetAsync(d + o.err, 0, 4, s));
     launch_query_limbs(d_v, p->z.B, reinterpret_cast<QLimb*>(d + o.limbs), s);
     launch_scan(p->h->e.c.m_enc.at<uint64_t>(), reinterpret_cast<QLimb*>(d + o.limbs),
                 reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk), p->nseg,
-                p->total_blocks, d_r, p->h->e.ctx->num_sms, s);
+                p->total_blocks, d_r, p->h->e.ctx->num_sms, reinterpret_cast<uint32_t*>(d + o.err), s);
     CU(cudaGetLastError());
+    return BN_OK;
+}
+
+int bn_plan_status(bn_plan* p, uint32_t* device_flags) {
+    if (!p || !device_flags) return fail(BN_EINVAL, "null argument");
+    CU(cudaMemcpy(device_flags, p->ws.at<char>() + p->o.err, 4, cudaMemcpyDeviceToHost));
     return BN_OK;
 }
 

@@ -50,7 +50,7 @@ __global__ void query_limbs_kernel(const uint64_t* __restrict__ v, uint64_t tota
 }
 
 // ------------------------------------------------------------------ scan
-constexpr int SCAN_GROUPS = 3;                 // 4-warp groups per CTA
+constexpr int SCAN_GROUPS = 4;                 // 4-warp groups per CTA
 constexpr int SCAN_THREADS = 128 * SCAN_GROUPS;
 
 __device__ __forceinline__ uint32_t find_seg(const uint64_t* __restrict__ seg_blk, uint32_t nseg, uint32_t hint,
@@ -156,6 +156,202 @@ scan_kernel(const uint64_t* __restrict__ m_enc, const QLimb* __restrict__ qlimbs
                 s[a] = red[parity][group][0][lane][a] + red[parity][group][1][lane][a] +
                        red[parity][group][2][lane][a] + red[parity][group][3][lane][a];
             r[sg.out0 + local + lane] = combine3(s[0], s[1], s[2]);
+        }
+        parity ^= 1;
+    }
+}
+
+// ------------------------------------------------------------------ scan, TMA pipeline
+// One producer warp streams each 4-row block (up to 32 KiB, contiguous in
+// m_enc) into a ring of shared-memory stages with a single cp.async.bulk;
+// four consumer groups of four warps take the stages round-robin.  Every
+// mbarrier wait is bounded: on timeout the CTA records an error in *err
+// and stops, so a lost completion cannot hang the GPU.
+constexpr int TS_STAGES = 6;
+constexpr int TS_GROUPS = 4;
+constexpr int TS_CONSUMERS = 32 * 4 * TS_GROUPS;   // 512
+constexpr int TS_THREADS = TS_CONSUMERS + 32;      // + producer warp
+constexpr uint32_t TS_STAGE_BYTES = SCAN_ROWS * N * 8;  // 32 KiB
+constexpr long long WAIT_CYCLES = 2000000000ll;    // ~1 s at 1.9 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: true when the phase with `parity` completed.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - t0 > WAIT_CYCLES) return false;
+    return true;
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+struct ScanBlock {
+    uint64_t row0;  // first m_enc row
+    uint64_t out0;  // first r slot
+    int nrows;
+    uint32_t query;
+};
+__device__ __forceinline__ ScanBlock scan_block(const ScanSeg* __restrict__ segs, const uint64_t* __restrict__ seg_blk,
+                                                uint32_t nseg, uint32_t& hint, uint64_t blk) {
+    hint = find_seg(seg_blk, nseg, hint, blk);
+    const ScanSeg sg = segs[hint];
+    const uint64_t local = (blk - seg_blk[hint]) * SCAN_ROWS;
+    const uint64_t left = (uint64_t)sg.rows - local;
+    return ScanBlock{sg.row0 + local, sg.out0 + local, left < (uint64_t)SCAN_ROWS ? (int)left : SCAN_ROWS, sg.query};
+}
+
+__global__ void __launch_bounds__(TS_THREADS, 1)
+scan_tma_kernel(const uint64_t* __restrict__ m_enc, const QLimb* __restrict__ qlimbs, const ScanSeg* __restrict__ segs,
+                const uint64_t* __restrict__ seg_blk, uint32_t nseg, uint64_t total_blocks, uint64_t* __restrict__ r,
+                uint32_t* __restrict__ err) {
+    extern __shared__ __align__(1024) unsigned char ts_smem[];
+    uint4* stage_base = reinterpret_cast<uint4*>(ts_smem);
+    __shared__ uint64_t full_bar[TS_STAGES], empty_bar[TS_STAGES];
+    __shared__ unsigned long long red[2][TS_GROUPS][4][SCAN_ROWS][3];
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TS_STAGES; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 4);
+        }
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const uint64_t nblk = total_blocks > blockIdx.x ? (total_blocks - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+
+    if (warp == TS_CONSUMERS / 32) {  // ---------------- producer warp
+        if (lane == 0) {
+            uint32_t hint = 0;
+            uint64_t i = 0;
+            for (; i < nblk; ++i) {
+                const int s = (int)(i % TS_STAGES);
+                if (i >= TS_STAGES && !mbar_wait(&empty_bar[s], (uint32_t)(((i / TS_STAGES) - 1) & 1))) {
+                    abort_flag = 1;
+                    atomicOr(err, 1u);
+                    break;
+                }
+                if (abort_flag) break;
+                const ScanBlock b = scan_block(segs, seg_blk, nseg, hint, blockIdx.x + i * gridDim.x);
+                const uint32_t bytes = (uint32_t)b.nrows * N * 8;
+                mbar_expect_tx(&full_bar[s], bytes);
+                bulk_g2s(stage_base + (uint64_t)s * (TS_STAGE_BYTES / 16), m_enc + b.row0 * N, bytes, &full_bar[s]);
+            }
+            // drain: no bulk copy may still be writing shared memory at exit
+            for (uint64_t j = (i > TS_STAGES ? i - TS_STAGES : 0); j < i; ++j)
+                mbar_wait(&full_bar[j % TS_STAGES], (uint32_t)((j / TS_STAGES) & 1));
+        }
+        return;
+    }
+
+    // ---------------------------------------------------- consumer groups
+    const int group = warp >> 2, wq = warp & 3;
+    const bool hi16 = (lane & 16) != 0, hi8 = (lane & 8) != 0;
+    uint32_t b0[8], b1[8], b2[8], c0[8], c1[8], c2[8];
+    uint32_t cur_q = 0xffffffffu, hint = 0;
+    int parity = 0;
+    for (uint64_t i = group; i < nblk; i += TS_GROUPS) {
+        const int s = (int)(i % TS_STAGES);
+        const ScanBlock b = scan_block(segs, seg_blk, nseg, hint, blockIdx.x + i * gridDim.x);
+        if (b.query != cur_q) {
+            cur_q = b.query;
+            const QLimb* ql = qlimbs + (uint64_t)cur_q * N + wq * 256 + 2 * lane;
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    const QLimb q = ql[64 * k + e];
+                    b0[2 * k + e] = q.b0; b1[2 * k + e] = q.b1; b2[2 * k + e] = q.b2;
+                    c0[2 * k + e] = q.c0; c1[2 * k + e] = q.c1; c2[2 * k + e] = q.c2;
+                }
+        }
+        const bool ok = mbar_wait(&full_bar[s], (uint32_t)((i / TS_STAGES) & 1));
+        if (!ok) { abort_flag = 1; atomicOr(err, 2u); }
+        uint64_t acc[SCAN_ROWS][3];
+        const uint4* base = stage_base + (uint64_t)s * (TS_STAGE_BYTES / 16) + wq * 128 + lane;
+#pragma unroll
+        for (int rr = 0; rr < SCAN_ROWS; ++rr) {
+            uint64_t a0 = 0, a1 = 0, a2 = 0;
+            if (ok && rr < b.nrows) {
+                const uint4* rp = base + rr * (N / 2);
+                uint4 x[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) x[k] = rp[32 * k];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int e0 = 2 * k, e1 = 2 * k + 1;
+                    a0 = mac(mac(a0, x[k].x, b0[e0]), x[k].y, c0[e0]);
+                    a1 = mac(mac(a1, x[k].x, b1[e0]), x[k].y, c1[e0]);
+                    a2 = mac(mac(a2, x[k].x, b2[e0]), x[k].y, c2[e0]);
+                    a0 = mac(mac(a0, x[k].z, b0[e1]), x[k].w, c0[e1]);
+                    a1 = mac(mac(a1, x[k].z, b1[e1]), x[k].w, c1[e1]);
+                    a2 = mac(mac(a2, x[k].z, b2[e1]), x[k].w, c2[e1]);
+                }
+            }
+            acc[rr][0] = a0; acc[rr][1] = a1; acc[rr][2] = a2;
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty_bar[s]);  // this warp is done with the stage
+        uint64_t w[2][3];
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                uint64_t send = hi16 ? acc[q][a] : acc[q + 2][a];
+                uint64_t keep = hi16 ? acc[q + 2][a] : acc[q][a];
+                w[q][a] = keep + __shfl_xor_sync(FULL, send, 16);
+            }
+        uint64_t xs[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            uint64_t send = hi8 ? w[0][a] : w[1][a];
+            uint64_t keep = hi8 ? w[1][a] : w[0][a];
+            xs[a] = keep + __shfl_xor_sync(FULL, send, 8);
+        }
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) xs[a] += __shfl_xor_sync(FULL, xs[a], off);
+        if ((lane & 7) == 0) {
+#pragma unroll
+            for (int a = 0; a < 3; ++a) red[parity][group][wq][lane >> 3][a] = xs[a];
+        }
+        named_bar(1 + group, 128);
+        if (abort_flag) break;  // read after the barrier: uniform across the group
+        if (wq == 0 && lane < b.nrows) {
+            uint64_t t[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+                t[a] = red[parity][group][0][lane][a] + red[parity][group][1][lane][a] +
+                       red[parity][group][2][lane][a] + red[parity][group][3][lane][a];
+            r[b.out0 + lane] = combine3(t[0], t[1], t[2]);
         }
         parity ^= 1;
     }
@@ -304,6 +500,7 @@ __global__ void lt_times_v_kernel(const uint64_t* __restrict__ L, uint32_t n1, c
 __device__ __forceinline__ uint64_t cm_dot(const uint64_t* __restrict__ a_cm, uint64_t rows, uint64_t row,
                                            const uint32_t (*vl)[6], uint32_t n1) {
     uint64_t a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll 8
     for (uint32_t k = 0; k < n1; ++k) {
         const uint64_t x = __ldg(a_cm + (uint64_t)k * rows + row);
         const uint32_t lo = (uint32_t)x, hi = (uint32_t)(x >> 32);
@@ -457,6 +654,7 @@ decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ 
             // M v' = AL G + M T
             const uint64_t al_g = cm_dot(al_cm, total_rows, grow, gl, n1);
             uint64_t m_t = 0;
+#pragma unroll 4
             for (uint32_t c = 0; c < tn; ++c) {
                 const uint32_t e = tl[c];
                 const uint64_t x = __ldg(mp_cm + (uint64_t)(e & 0x3ffu) * total_rows + grow);
@@ -468,6 +666,7 @@ decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ 
             const uint32_t sl = (uint32_t)(grow & 31);
             const uint32_t off = s_off[slice], wdt = s_w[slice];
             uint64_t s_v = 0;
+#pragma unroll 4
             for (uint32_t c = 0; c < wdt; ++c) {
                 const uint16_t e = __ldg(s_ell + off + (uint64_t)c * 32 + sl);
                 if (e != 0xffffu) s_v = (e & 0x8000u) ? sub_mod(s_v, vs[e & 0x3ffu]) : add_mod(s_v, vs[e & 0x3ffu]);
@@ -648,11 +847,16 @@ void launch_query_limbs(const uint64_t* d_v, uint32_t nq, QLimb* d_limbs, cudaSt
 }
 
 void launch_scan(const uint64_t* d_m_enc, const QLimb* d_limbs, const ScanSeg* d_segs, const uint64_t* d_seg_blk,
-                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, cudaStream_t s) {
+                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, uint32_t* d_err, cudaStream_t s) {
     if (total_blocks == 0) return;
-    uint64_t want = (total_blocks + SCAN_GROUPS - 1) / SCAN_GROUPS;
-    unsigned grid = (unsigned)(want < (uint64_t)num_sms ? want : (uint64_t)num_sms);
-    scan_kernel<<<grid, SCAN_THREADS, 0, s>>>(d_m_enc, d_limbs, d_segs, d_seg_blk, nseg, total_blocks, d_r);
+    static bool attr_set = false;
+    const int smem = TS_STAGES * TS_STAGE_BYTES;
+    if (!attr_set) {
+        cudaFuncSetAttribute(scan_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr_set = true;
+    }
+    unsigned grid = (unsigned)(total_blocks < (uint64_t)num_sms ? total_blocks : (uint64_t)num_sms);
+    scan_tma_kernel<<<grid, TS_THREADS, smem, s>>>(d_m_enc, d_limbs, d_segs, d_seg_blk, nseg, total_blocks, d_r, d_err);
 }
 
 FreivaldsPlan plan_freivalds(uint64_t max_rows, uint32_t nseg, int num_sms) {

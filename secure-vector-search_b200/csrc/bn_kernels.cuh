@@ -55,8 +55,10 @@ void launch_query_limbs(const uint64_t* d_v, uint32_t nq, QLimb* d_limbs, cudaSt
 
 // Segment scan: r[out0 + i] = sum_j m_enc[row0 + i][j] * v[query][j] mod p.
 // seg_blk: exclusive prefix sum over ceil(rows / SCAN_ROWS), nseg + 1 entries.
+// d_err (device u32): bit 0/1 set if a pipeline wait timed out (the scan
+// result is then invalid); the kernel never waits without a bound.
 void launch_scan(const uint64_t* d_m_enc, const QLimb* d_limbs, const ScanSeg* d_segs, const uint64_t* d_seg_blk,
-                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, cudaStream_t s);
+                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, uint32_t* d_err, cudaStream_t s);
 
 // Freivalds partial sums for one segment list.  z_part: [nseg][chunks][T][1024],
 // ur_part: [nseg][chunks][T].  chunk_rows: rows per chunk (multiple of 32).
