@@ -37,6 +37,13 @@ extern "C" {
 #define BN_EUNSUPPORTED (-5) /* handle lacks the client state this call needs       */
 
 #define BN_TOPK_MAX 1024
+#define BN_MAX_TRIALS 64 /* Protocol 2 trials per call */
+
+/* Protocol 2 engines (bn_ctx_set_engine).  Both compute z_t = u_t^T M_enc
+ * exactly; TENSOR runs it as a u8-limb GEMM on tcgen05 tensor cores,
+ * CUDA_CORE as 64-bit limb multiply-adds on the CUDA cores. */
+#define BN_ENGINE_TENSOR 0
+#define BN_ENGINE_CUDA_CORE 1
 
 /* Last error message of the calling thread ("" when none). */
 const char* bn_last_error(void);
@@ -64,6 +71,10 @@ typedef struct bn_sparse_csr {
  * vram_budget_bytes = 0 takes 80 % of the device's free memory. */
 int bn_ctx_create(int device, uint64_t vram_budget_bytes, bn_ctx** out);
 int bn_ctx_destroy(bn_ctx* ctx);
+/* Selects the Protocol 2 engine used by later calls on this context's
+ * handles (default BN_ENGINE_TENSOR).  No counterpart in the reference, whose
+ * verification runs on the host (lib.rs:419-437). */
+int bn_ctx_set_engine(bn_ctx* ctx, int engine);
 /* Budget, bytes currently held by handles, high-water mark
  * (FlatGpuState::{vram_budget_bytes, peak_vram_bytes}, gpu/mod.rs:334-340). */
 int bn_ctx_memory(const bn_ctx* ctx, uint64_t* budget_bytes, uint64_t* used_bytes, uint64_t* peak_bytes);

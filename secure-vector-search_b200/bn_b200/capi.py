@@ -17,6 +17,7 @@ P = (1 << 61) - 1
 TOPK_MAX = 1024
 
 BN_OK, BN_EINVAL, BN_ECUDA, BN_EBUDGET, BN_ENODEV, BN_EUNSUPPORTED = 0, -1, -2, -3, -4, -5
+ENGINE_TENSOR, ENGINE_CUDA_CORE = 0, 1
 _NAMES = {BN_EINVAL: "EINVAL", BN_ECUDA: "ECUDA", BN_EBUDGET: "EBUDGET", BN_ENODEV: "ENODEV",
           BN_EUNSUPPORTED: "EUNSUPPORTED"}
 
@@ -46,6 +47,7 @@ _SIGS = {
     "bn_ctx_create": (C.c_int, [C.c_int, u64, vp]),
     "bn_ctx_destroy": (C.c_int, [vp]),
     "bn_ctx_memory": (C.c_int, [vp, vp, vp, vp]),
+    "bn_ctx_set_engine": (C.c_int, [vp, C.c_int]),
     "bn_flat_build": (C.c_int, [vp, vp, vp, vp, u64, u32, u32, vp]),
     "bn_flat_attach_client": (C.c_int, [vp, vp, vp, SparseCsr]),
     "bn_flat_build_from_plain": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, vp]),
@@ -124,6 +126,9 @@ class Context:
         h = vp()
         check(lib.bn_ctx_create(device, vram_budget_bytes, C.byref(h)))
         self.h = h
+
+    def set_engine(self, engine: int):
+        check(lib.bn_ctx_set_engine(self.h, engine))
 
     def memory(self):
         b, u, p = u64(), u64(), u64()

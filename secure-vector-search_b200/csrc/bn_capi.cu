@@ -18,6 +18,7 @@
 
 #include "bn_b200.h"
 #include "bn_kernels.cuh"
+#include "bn_tc.cuh"
 
 using namespace bn;
 
@@ -54,6 +55,7 @@ inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
 struct bn_ctx {
     int device = 0;
     int num_sms = 148;
+    int engine = BN_ENGINE_TENSOR;  // Protocol 2 engine
     uint64_t budget = 0, used = 0, peak = 0;
     std::mutex mu;
 };
@@ -150,12 +152,20 @@ struct Corpus {
     DevMem m_enc, al_cm, h_cm;
     bool client = false;
     DevMem L, mp_cm, s_ell, s_off, s_w, ids;
+    CUtensorMap tmap_m;  // m_enc as bytes {8192, rows}, 128x128 boxes, 128-byte swizzle
 
     uint64_t bytes() const {
         return m_enc.bytes + al_cm.bytes + h_cm.bytes + L.bytes + mp_cm.bytes + s_ell.bytes + s_off.bytes + s_w.bytes +
                ids.bytes;
     }
 };
+
+int corpus_tmap(Corpus& c) {
+    if (!c.rows) return BN_OK;
+    cudaError_t e = make_tmap_u8(&c.tmap_m, c.m_enc.p, (uint64_t)N * 8, c.rows, TC_ROWS, TC_ROWS);
+    if (e != cudaSuccess) return fail(BN_ECUDA, "tensor map of m_enc: %s", cudaGetErrorString(e));
+    return BN_OK;
+}
 
 int check_shape(uint32_t n, uint32_t n1) {
     if (n != N) return fail(BN_EINVAL, "dimension too large: n = %u, this backend is built for n = %u", n, N);
@@ -316,6 +326,7 @@ int build_corpus_from_plain(bn_ctx* ctx, Corpus& c, const uint64_t* m_q, uint64_
     }
     CU(cudaMemcpyAsync(d_L.p, L, (uint64_t)N * n1 * 8, cudaMemcpyHostToDevice, s));
     TRY(device_encrypt(ctx, d_mq.at<uint64_t>(), rows, n1, d_L.at<uint64_t>(), d_H.at<uint64_t>(), S, c.m_enc, al_rm, s));
+    TRY(corpus_tmap(c));
     TRY(device_colmajor(ctx, al_rm.at<uint64_t>(), rows, n1, c.al_cm, s));
     TRY(device_colmajor(ctx, d_H.at<uint64_t>(), rows, n1, c.h_cm, s));
     TRY(device_colmajor(ctx, d_mq.at<uint64_t>(), rows, N, c.mp_cm, s));
@@ -329,7 +340,14 @@ int build_corpus_from_plain(bn_ctx* ctx, Corpus& c, const uint64_t* m_q, uint64_
 }
 
 // ------------------------------------------------------------------ pipeline
-struct Meta {  // device pointers
+constexpr uint32_t MAX_TRIALS = 64;  // Protocol 2 trials per call
+
+struct TcMaps {  // host-side tensor maps of the U buffer, one per pass of <= 20 trials
+    CUtensorMap u[(MAX_TRIALS + TC_MAX_TRIALS - 1) / TC_MAX_TRIALS];
+};
+inline uint32_t pass_rows(uint32_t t_cnt) { return 8 * ((t_cnt + 1) & ~1u); }
+
+struct Meta {  // device pointers (+ host tensor maps)
     const ScanSeg* segs;
     const uint64_t* seg_blk;
     uint32_t nseg;
@@ -337,6 +355,13 @@ struct Meta {  // device pointers
     const VerifySeg* vsegs;
     uint32_t nvseg;
     const DecodeQuery* dq;
+    const TcBlock* tc_blocks;
+    uint32_t nblocks;
+    const TcPanel* tc_panels;
+    uint32_t npanels;
+    const uint32_t* seg_panel0;
+    const uint32_t* seg_block0;
+    const TcMaps* maps;
 };
 struct Scratch {  // device pointers
     QLimb* limbs;
@@ -349,6 +374,7 @@ struct Scratch {  // device pointers
     uint64_t* zv;
     TopkScratch topk;
     uint32_t* err;  // device pipeline timeout flags
+    uint8_t* u_buf;
 };
 struct Inputs {
     const uint64_t* v;
@@ -371,6 +397,9 @@ struct HostMeta {
     std::vector<VerifySeg> vsegs;
     std::vector<DecodeQuery> dq;
     std::vector<uint32_t> seg_cluster;  // IVF: list id of each segment
+    std::vector<TcBlock> blocks;        // 128-row blocks of every verify segment
+    std::vector<TcPanel> panels;        // 4096-row panels of every verify segment
+    std::vector<uint32_t> seg_block0, seg_panel0;
     uint64_t total_out = 0, max_rows = 0;
 };
 
@@ -378,6 +407,21 @@ void finish_meta(HostMeta& hm) {
     hm.seg_blk.assign(hm.segs.size() + 1, 0);
     for (size_t i = 0; i < hm.segs.size(); ++i)
         hm.seg_blk[i + 1] = hm.seg_blk[i] + (hm.segs[i].rows + SCAN_ROWS - 1) / SCAN_ROWS;
+    hm.blocks.clear();
+    hm.panels.clear();
+    hm.seg_block0.assign(hm.vsegs.size() + 1, 0);
+    hm.seg_panel0.assign(hm.vsegs.size() + 1, 0);
+    for (uint32_t s = 0; s < hm.vsegs.size(); ++s) {
+        const VerifySeg& v = hm.vsegs[s];
+        hm.seg_block0[s] = (uint32_t)hm.blocks.size();
+        hm.seg_panel0[s] = (uint32_t)hm.panels.size();
+        for (uint32_t i0 = 0; i0 < v.rows; i0 += TC_ROWS) hm.blocks.push_back(TcBlock{s, i0});
+        for (uint32_t p0 = 0; p0 < v.rows; p0 += TC_PANEL_ROWS)
+            hm.panels.push_back(TcPanel{v.row0 + p0, std::min<uint32_t>(TC_PANEL_ROWS, v.rows - p0),
+                                        hm.seg_block0[s] + p0 / TC_ROWS, s, 0});
+    }
+    hm.seg_block0.back() = (uint32_t)hm.blocks.size();
+    hm.seg_panel0.back() = (uint32_t)hm.panels.size();
 }
 
 void flat_meta(uint64_t m, uint32_t B, HostMeta& hm) {
@@ -394,8 +438,9 @@ void flat_meta(uint64_t m, uint32_t B, HostMeta& hm) {
 
 struct Sizes {
     uint32_t B, n1, trials, k, ctas;
-    uint64_t total_out, nseg, nvseg;
-    FreivaldsPlan fp;
+    uint64_t total_out, nseg, nvseg, nblocks, npanels;
+    FreivaldsPlan fp;  // CUDA-core engine
+    int engine;        // BN_ENGINE_*
 };
 
 int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms) {
@@ -407,11 +452,11 @@ int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms) {
 // Offsets of every device buffer of one pipeline run.
 struct RunLayout {
     // inputs (contiguous from 0 -> one H2D)
-    uint64_t v, g, t, t_nnz, seeds, segs, seg_blk, vsegs, dq, in_end;
+    uint64_t v, g, t, t_nnz, seeds, segs, seg_blk, vsegs, dq, tc_blocks, tc_panels, seg_panel0, seg_block0, in_end;
     // outputs (contiguous -> one D2H)
     uint64_t ids, scores, n, vfailed, ur, zv, err, out_begin, out_end;
     // internal
-    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, total;
+    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, total;
 };
 
 RunLayout make_layout(const Sizes& z, bool want_mv) {
@@ -426,6 +471,10 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
     o.seg_blk = L.take<uint64_t>(z.nseg + 1);
     o.vsegs = L.take<VerifySeg>(z.nvseg);
     o.dq = L.take<DecodeQuery>(z.B);
+    o.tc_blocks = L.take<TcBlock>(z.nblocks);
+    o.tc_panels = L.take<TcPanel>(z.npanels);
+    o.seg_panel0 = L.take<uint32_t>(z.nvseg + 1);
+    o.seg_block0 = L.take<uint32_t>(z.nvseg + 1);
     o.in_end = L.off;
     o.ids = L.take<uint32_t>((uint64_t)z.B * std::max<uint32_t>(z.k, 1));
     o.out_begin = o.ids;
@@ -440,15 +489,29 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
     o.x = L.take<uint64_t>((uint64_t)z.B * z.n1);
     o.r = L.take<uint64_t>(std::max<uint64_t>(z.total_out, 1));
     o.mv = want_mv ? L.take<uint64_t>(std::max<uint64_t>(z.total_out, 1)) : 0;
-    o.z_part = L.take<uint64_t>(z.trials ? (uint64_t)z.nvseg * z.fp.chunks * z.trials * N : 1);
-    o.ur_part = L.take<uint64_t>(z.trials ? (uint64_t)z.nvseg * z.fp.chunks * z.trials : 1);
+    const bool tc = z.engine == BN_ENGINE_TENSOR;
+    const uint64_t zp = !z.trials ? 1 : tc ? z.npanels * z.trials * N : (uint64_t)z.nvseg * z.fp.chunks * z.trials * N;
+    const uint64_t up = !z.trials ? 1 : tc ? z.nblocks * z.trials : (uint64_t)z.nvseg * z.fp.chunks * z.trials;
+    o.z_part = L.take<uint64_t>(std::max<uint64_t>(zp, 1));
+    o.ur_part = L.take<uint64_t>(std::max<uint64_t>(up, 1));
     o.flags = L.take<uint32_t>(1);
     const uint64_t cand = (uint64_t)z.B * z.ctas * std::max<uint32_t>(z.k, 1);
     o.cand_s = L.take<int64_t>(cand);
     o.cand_i = L.take<uint32_t>(cand);
     o.cand_n = L.take<uint32_t>((uint64_t)z.B * z.ctas);
-    o.total = L.off;
+    o.u_buf = (tc && z.trials) ? L.take<uint8_t>(std::max<uint64_t>(z.nblocks, 1) * pass_rows(TC_MAX_TRIALS) * TC_ROWS) : 0;
+    o.total = L.off + 1024;
     return o;
+}
+
+int make_tc_maps(const Sizes& z, const uint8_t* d_u, TcMaps& maps) {
+    if (z.engine != BN_ENGINE_TENSOR || !z.trials || !z.nblocks) return BN_OK;
+    for (uint32_t t0 = 0, ps = 0; t0 < z.trials; t0 += TC_MAX_TRIALS, ++ps) {
+        const uint32_t nr = pass_rows(std::min<uint32_t>(TC_MAX_TRIALS, z.trials - t0));
+        cudaError_t e = make_tmap_u8(&maps.u[ps], d_u, TC_ROWS, z.nblocks * (uint64_t)nr, TC_ROWS, nr);
+        if (e != cudaSuccess) return fail(BN_ECUDA, "tensor map for the Freivalds draws: %s", cudaGetErrorString(e));
+    }
+    return BN_OK;
 }
 
 int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m, const Inputs& in, const Scratch& sc,
@@ -459,10 +522,23 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
                 s);
     if (z.trials) {
         CU(cudaMemsetAsync(sc.flags, 0, 4, s));
-        launch_freivalds(c.m_enc.at<uint64_t>(), sc.r, m.vsegs, m.nvseg, reinterpret_cast<const ChaChaKey*>(in.seeds),
-                         z.trials, z.fp, sc.z_part, sc.ur_part, sc.flags, s);
-        launch_freivalds_finish(sc.z_part, sc.ur_part, in.v, m.vsegs, m.nvseg, z.trials, z.fp, sc.ur, sc.zv,
-                                out.vfailed, s);
+        const ChaChaKey* keys = reinterpret_cast<const ChaChaKey*>(in.seeds);
+        if (z.engine == BN_ENGINE_TENSOR) {
+            for (uint32_t t0 = 0, ps = 0; t0 < z.trials; t0 += TC_MAX_TRIALS, ++ps) {
+                const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, z.trials - t0), nr = pass_rows(tc);
+                launch_tc_ugen(m.vsegs, m.tc_blocks, m.nblocks, keys, sc.r, t0, tc, nr, sc.u_buf, sc.ur_part, z.trials,
+                               sc.flags, s);
+                launch_tc_freivalds(c.tmap_m, m.maps->u[ps], m.tc_panels, m.npanels, t0, tc, nr, z.trials, sc.z_part,
+                                    sc.err, ctx->num_sms, s);
+            }
+            launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, in.v, m.vsegs, m.nvseg, z.trials, sc.ur,
+                             sc.zv, out.vfailed, s);
+        } else {
+            launch_freivalds(c.m_enc.at<uint64_t>(), sc.r, m.vsegs, m.nvseg, keys, z.trials, z.fp, sc.z_part, sc.ur_part,
+                             sc.flags, s);
+            launch_freivalds_finish(sc.z_part, sc.ur_part, in.v, m.vsegs, m.nvseg, z.trials, z.fp, sc.ur, sc.zv,
+                                    out.vfailed, s);
+        }
     } else {
         CU(cudaMemsetAsync(out.vfailed, 0xff, std::max<uint64_t>(m.nvseg, 1) * 4, s));
     }
@@ -477,6 +553,34 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
     }
     CU(cudaGetLastError());
     return BN_OK;
+}
+
+Meta meta_at(char* d, const RunLayout& o, const HostMeta& hm, const TcMaps* maps) {
+    return Meta{reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk),
+                (uint32_t)hm.segs.size(), hm.seg_blk.empty() ? 0 : hm.seg_blk.back(),
+                reinterpret_cast<VerifySeg*>(d + o.vsegs), (uint32_t)hm.vsegs.size(),
+                reinterpret_cast<DecodeQuery*>(d + o.dq), reinterpret_cast<TcBlock*>(d + o.tc_blocks),
+                (uint32_t)hm.blocks.size(), reinterpret_cast<TcPanel*>(d + o.tc_panels), (uint32_t)hm.panels.size(),
+                reinterpret_cast<uint32_t*>(d + o.seg_panel0), reinterpret_cast<uint32_t*>(d + o.seg_block0), maps};
+}
+Scratch scratch_at(char* d, const RunLayout& o) {
+    return Scratch{reinterpret_cast<QLimb*>(d + o.limbs), reinterpret_cast<uint64_t*>(d + o.x),
+                   reinterpret_cast<uint64_t*>(d + o.r), reinterpret_cast<uint64_t*>(d + o.z_part),
+                   reinterpret_cast<uint64_t*>(d + o.ur_part), reinterpret_cast<uint32_t*>(d + o.flags),
+                   reinterpret_cast<uint64_t*>(d + o.ur), reinterpret_cast<uint64_t*>(d + o.zv),
+                   TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
+                               reinterpret_cast<uint32_t*>(d + o.cand_n)},
+                   reinterpret_cast<uint32_t*>(d + o.err), reinterpret_cast<uint8_t*>(d + o.u_buf)};
+}
+void pack_meta(char* h, const RunLayout& o, const HostMeta& hm) {
+    memcpy(h + o.segs, hm.segs.data(), hm.segs.size() * sizeof(ScanSeg));
+    memcpy(h + o.seg_blk, hm.seg_blk.data(), hm.seg_blk.size() * 8);
+    memcpy(h + o.vsegs, hm.vsegs.data(), hm.vsegs.size() * sizeof(VerifySeg));
+    memcpy(h + o.dq, hm.dq.data(), hm.dq.size() * sizeof(DecodeQuery));
+    memcpy(h + o.tc_blocks, hm.blocks.data(), hm.blocks.size() * sizeof(TcBlock));
+    memcpy(h + o.tc_panels, hm.panels.data(), hm.panels.size() * sizeof(TcPanel));
+    memcpy(h + o.seg_panel0, hm.seg_panel0.data(), hm.seg_panel0.size() * 4);
+    memcpy(h + o.seg_block0, hm.seg_block0.data(), hm.seg_block0.size() * 4);
 }
 
 // Handle-side state shared by flat and IVF.
@@ -503,6 +607,20 @@ void engine_free(Engine& e) {
     }
 }
 
+Sizes sizes_for(const Engine& e, const HostMeta& hm, uint32_t B, uint32_t trials, uint32_t k) {
+    uint64_t max_q_rows = 0;
+    for (auto& d : hm.dq) {
+        uint64_t rsum = 0;
+        for (uint32_t s = d.seg0; s < d.seg0 + d.nseg; ++s) rsum += hm.segs[s].rows;
+        max_q_rows = std::max(max_q_rows, rsum);
+    }
+    return Sizes{B, e.c.n1, trials, k, (uint32_t)pick_ctas(max_q_rows, B, e.ctx->num_sms), hm.total_out,
+                 hm.segs.size(), hm.vsegs.size(), hm.blocks.size(), hm.panels.size(),
+                 plan_freivalds(std::max<uint64_t>(hm.max_rows, 1), (uint32_t)std::max<size_t>(hm.vsegs.size(), 1),
+                                e.ctx->num_sms),
+                 e.ctx->engine};
+}
+
 // Host-buffer query: pack, one H2D, pipeline, one D2H, sync.
 int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
               const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds, uint32_t trials, uint32_t k,
@@ -512,6 +630,7 @@ int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const 
     if (!c.client) return fail(BN_EUNSUPPORTED, "this handle has no client state (attach_client was not called)");
     if (k > BN_TOPK_MAX) return fail(BN_EINVAL, "k = %u exceeds BN_TOPK_MAX = %d", k, BN_TOPK_MAX);
     if (B > 65535) return fail(BN_EINVAL, "B = %u exceeds 65535 queries per call", B);
+    if (trials > MAX_TRIALS) return fail(BN_EINVAL, "trials = %u exceeds %u", trials, MAX_TRIALS);
     if (trials && !v_seeds) return fail(BN_EINVAL, "v_seeds is required when trials > 0");
     if (!v_enc || !g || !t_nnz) return fail(BN_EINVAL, "null query input");
     uint64_t t_total = 0;
@@ -523,17 +642,13 @@ int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const 
     TRY(validate_residues(v_enc, (uint64_t)B * N, "v_enc"));
     TRY(validate_residues(g, (uint64_t)B * c.n1, "g"));
 
-    uint64_t max_q_rows = 0;
-    for (auto& d : hm.dq) {
-        uint64_t rsum = 0;
-        for (uint32_t s = d.seg0; s < d.seg0 + d.nseg; ++s) rsum += hm.segs[s].rows;
-        max_q_rows = std::max(max_q_rows, rsum);
-    }
-    Sizes z{B, c.n1, trials, k, (uint32_t)pick_ctas(max_q_rows, B, e.ctx->num_sms), hm.total_out, hm.segs.size(),
-            hm.vsegs.size(), plan_freivalds(std::max<uint64_t>(hm.max_rows, 1), (uint32_t)std::max<size_t>(hm.vsegs.size(), 1), e.ctx->num_sms)};
+    const Sizes z = sizes_for(e, hm, B, trials, k);
     const RunLayout o = make_layout(z, mv_out != nullptr);
     TRY(e.ws.reserve(e.ctx, o.total));
     TRY(e.host.reserve(o.out_end));
+    char* d = e.ws.at<char>();
+    TcMaps maps;
+    TRY(make_tc_maps(z, reinterpret_cast<uint8_t*>(d + o.u_buf), maps));
 
     // pack inputs
     char* h = e.host.at<char>();
@@ -551,27 +666,15 @@ int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const 
     memcpy(h + o.t_nnz, t_nnz, (uint64_t)B * 4);
     if (v_seeds) memcpy(h + o.seeds, v_seeds, (uint64_t)B * 32);
     else memset(h + o.seeds, 0, (uint64_t)B * 32);
-    memcpy(h + o.segs, hm.segs.data(), hm.segs.size() * sizeof(ScanSeg));
-    memcpy(h + o.seg_blk, hm.seg_blk.data(), hm.seg_blk.size() * 8);
-    memcpy(h + o.vsegs, hm.vsegs.data(), hm.vsegs.size() * sizeof(VerifySeg));
-    memcpy(h + o.dq, hm.dq.data(), hm.dq.size() * sizeof(DecodeQuery));
+    pack_meta(h, o, hm);
 
     CU(cudaSetDevice(e.ctx->device));
-    char* d = e.ws.at<char>();
     CU(cudaMemcpyAsync(d, h, o.in_end, cudaMemcpyHostToDevice, e.stream));
-    Meta m{reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk), (uint32_t)hm.segs.size(),
-           hm.seg_blk.back(), reinterpret_cast<VerifySeg*>(d + o.vsegs), (uint32_t)hm.vsegs.size(),
-           reinterpret_cast<DecodeQuery*>(d + o.dq)};
+    const Meta m = meta_at(d, o, hm, &maps);
     Inputs in{reinterpret_cast<uint64_t*>(d + o.v), reinterpret_cast<uint64_t*>(d + o.g),
               reinterpret_cast<uint32_t*>(d + o.t), reinterpret_cast<uint32_t*>(d + o.t_nnz),
               reinterpret_cast<uint8_t*>(d + o.seeds)};
-    Scratch sc{reinterpret_cast<QLimb*>(d + o.limbs), reinterpret_cast<uint64_t*>(d + o.x),
-               reinterpret_cast<uint64_t*>(d + o.r), reinterpret_cast<uint64_t*>(d + o.z_part),
-               reinterpret_cast<uint64_t*>(d + o.ur_part), reinterpret_cast<uint32_t*>(d + o.flags),
-               reinterpret_cast<uint64_t*>(d + o.ur), reinterpret_cast<uint64_t*>(d + o.zv),
-               TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
-                           reinterpret_cast<uint32_t*>(d + o.cand_n)},
-               reinterpret_cast<uint32_t*>(d + o.err)};
+    const Scratch sc = scratch_at(d, o);
     Outputs out{reinterpret_cast<uint32_t*>(d + o.ids), reinterpret_cast<int64_t*>(d + o.scores),
                 reinterpret_cast<uint32_t*>(d + o.n), reinterpret_cast<int32_t*>(d + o.vfailed),
                 mv_out ? reinterpret_cast<uint64_t*>(d + o.mv) : nullptr};
@@ -607,10 +710,11 @@ int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const 
     return BN_OK;
 }
 
-// Verify a claimed r for one contiguous row range.
+// Verify a claimed r for one contiguous row range (Protocol 2 only).
 int run_verify(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* r, const uint64_t* v_enc, const uint8_t* seed,
                uint32_t trials, int32_t* failed_trial, uint64_t* ur, uint64_t* zv) {
     if (!failed_trial || !v_enc || !seed || (rows && !r)) return fail(BN_EINVAL, "null argument");
+    if (trials > MAX_TRIALS) return fail(BN_EINVAL, "trials = %u exceeds %u", trials, MAX_TRIALS);
     TRY(validate_residues(r, rows, "r"));
     TRY(validate_residues(v_enc, N, "v_enc"));
     if (trials == 0 || rows == 0) {
@@ -620,41 +724,57 @@ int run_verify(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* r, const
         for (uint32_t t = 0; t < trials; ++t) { if (ur) ur[t] = 0; if (zv) zv[t] = 0; }
         return BN_OK;
     }
-    FreivaldsPlan fp = plan_freivalds(rows, 1, e.ctx->num_sms);
-    Layout L;
-    const uint64_t o_r = L.take<uint64_t>(rows), o_v = L.take<uint64_t>(N), o_seed = L.take<uint8_t>(32),
-                   o_vs = L.take<VerifySeg>(1), in_end = L.off;
-    const uint64_t o_fail = L.take<int32_t>(1), o_ur = L.take<uint64_t>(trials), o_zv = L.take<uint64_t>(trials),
-                   out_end = L.off;
-    const uint64_t o_zp = L.take<uint64_t>((uint64_t)fp.chunks * trials * N), o_urp = L.take<uint64_t>((uint64_t)fp.chunks * trials),
-                   o_flags = L.take<uint32_t>(1);
-    TRY(e.ws.reserve(e.ctx, L.off));
-    TRY(e.host.reserve(out_end));
+    HostMeta hm;
+    hm.vsegs.push_back(VerifySeg{row0, 0, (uint32_t)rows, 0});
+    hm.max_rows = rows;
+    finish_meta(hm);
+    Sizes z{1, e.c.n1, trials, 0, 1, rows, 0, 1, hm.blocks.size(), hm.panels.size(),
+            plan_freivalds(rows, 1, e.ctx->num_sms), e.ctx->engine};
+    const RunLayout o = make_layout(z, false);
+    TRY(e.ws.reserve(e.ctx, o.total));
+    TRY(e.host.reserve(o.out_end));
     char* h = e.host.at<char>();
-    memcpy(h + o_r, r, rows * 8);
-    memcpy(h + o_v, v_enc, N * 8);
-    memcpy(h + o_seed, seed, 32);
-    VerifySeg vs{row0, 0, (uint32_t)rows, 0};
-    memcpy(h + o_vs, &vs, sizeof vs);
     char* d = e.ws.at<char>();
+    TcMaps maps;
+    TRY(make_tc_maps(z, reinterpret_cast<uint8_t*>(d + o.u_buf), maps));
+    memcpy(h + o.v, v_enc, N * 8);
+    memcpy(h + o.seeds, seed, 32);
+    pack_meta(h, o, hm);
     CU(cudaSetDevice(e.ctx->device));
-    CU(cudaMemcpyAsync(d, h, in_end, cudaMemcpyHostToDevice, e.stream));
-    CU(cudaMemsetAsync(d + o_flags, 0, 4, e.stream));
-    launch_freivalds(e.c.m_enc.at<uint64_t>(), reinterpret_cast<uint64_t*>(d + o_r), reinterpret_cast<VerifySeg*>(d + o_vs),
-                     1, reinterpret_cast<ChaChaKey*>(d + o_seed), trials, fp, reinterpret_cast<uint64_t*>(d + o_zp),
-                     reinterpret_cast<uint64_t*>(d + o_urp), reinterpret_cast<uint32_t*>(d + o_flags), e.stream);
-    launch_freivalds_finish(reinterpret_cast<uint64_t*>(d + o_zp), reinterpret_cast<uint64_t*>(d + o_urp),
-                            reinterpret_cast<uint64_t*>(d + o_v), reinterpret_cast<VerifySeg*>(d + o_vs), 1, trials, fp,
-                            reinterpret_cast<uint64_t*>(d + o_ur), reinterpret_cast<uint64_t*>(d + o_zv),
-                            reinterpret_cast<int32_t*>(d + o_fail), e.stream);
+    CU(cudaMemcpyAsync(d, h, o.in_end, cudaMemcpyHostToDevice, e.stream));
+    CU(cudaMemcpyAsync(d + o.r, r, rows * 8, cudaMemcpyHostToDevice, e.stream));
+    const Meta m = meta_at(d, o, hm, &maps);
+    const Scratch sc = scratch_at(d, o);
+    const ChaChaKey* keys = reinterpret_cast<const ChaChaKey*>(d + o.seeds);
+    const uint64_t* dv = reinterpret_cast<uint64_t*>(d + o.v);
+    int32_t* dfail = reinterpret_cast<int32_t*>(d + o.vfailed);
+    CU(cudaMemsetAsync(sc.flags, 0, 4, e.stream));
+    CU(cudaMemsetAsync(sc.err, 0, 4, e.stream));
+    if (z.engine == BN_ENGINE_TENSOR) {
+        for (uint32_t t0 = 0, ps = 0; t0 < trials; t0 += TC_MAX_TRIALS, ++ps) {
+            const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, trials - t0), nr = pass_rows(tc);
+            launch_tc_ugen(m.vsegs, m.tc_blocks, m.nblocks, keys, sc.r, t0, tc, nr, sc.u_buf, sc.ur_part, trials,
+                           sc.flags, e.stream);
+            launch_tc_freivalds(e.c.tmap_m, maps.u[ps], m.tc_panels, m.npanels, t0, tc, nr, trials, sc.z_part, sc.err,
+                                e.ctx->num_sms, e.stream);
+        }
+        launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, dv, m.vsegs, 1, trials, sc.ur, sc.zv, dfail,
+                         e.stream);
+    } else {
+        launch_freivalds(e.c.m_enc.at<uint64_t>(), sc.r, m.vsegs, 1, keys, trials, z.fp, sc.z_part, sc.ur_part, sc.flags,
+                         e.stream);
+        launch_freivalds_finish(sc.z_part, sc.ur_part, dv, m.vsegs, 1, trials, z.fp, sc.ur, sc.zv, dfail, e.stream);
+    }
     CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(h + o_fail, d + o_fail, out_end - o_fail, cudaMemcpyDeviceToHost, e.stream));
+    CU(cudaMemcpyAsync(h + o.out_begin, d + o.out_begin, o.out_end - o.out_begin, cudaMemcpyDeviceToHost, e.stream));
     CU(cudaStreamSynchronize(e.stream));
-    *failed_trial = *reinterpret_cast<int32_t*>(h + o_fail);
+    if (const uint32_t ev = *reinterpret_cast<uint32_t*>(h + o.err))
+        return fail(BN_ECUDA, "a device pipeline wait timed out (flags 0x%x); results discarded", ev);
+    *failed_trial = *reinterpret_cast<int32_t*>(h + o.vfailed);
     const uint32_t ran = *failed_trial < 0 ? trials : (uint32_t)*failed_trial + 1;
     for (uint32_t t = 0; t < trials; ++t) {
-        if (ur) ur[t] = t < ran ? reinterpret_cast<uint64_t*>(h + o_ur)[t] : 0;
-        if (zv) zv[t] = t < ran ? reinterpret_cast<uint64_t*>(h + o_zv)[t] : 0;
+        if (ur) ur[t] = t < ran ? reinterpret_cast<uint64_t*>(h + o.ur)[t] : 0;
+        if (zv) zv[t] = t < ran ? reinterpret_cast<uint64_t*>(h + o.zv)[t] : 0;
     }
     return BN_OK;
 }
@@ -738,8 +858,8 @@ struct bn_plan {
     Sizes z{};
     RunLayout o{};
     DevMem ws;
-    uint32_t nseg = 0;
-    uint64_t total_blocks = 0;
+    HostMeta hm;
+    TcMaps maps;
 };
 
 extern "C" {
@@ -793,6 +913,13 @@ int bn_ctx_destroy(bn_ctx* ctx) {
     return BN_OK;
 }
 
+int bn_ctx_set_engine(bn_ctx* ctx, int engine) {
+    if (!ctx) return fail(BN_EINVAL, "null ctx");
+    if (engine != BN_ENGINE_TENSOR && engine != BN_ENGINE_CUDA_CORE) return fail(BN_EINVAL, "unknown engine %d", engine);
+    ctx->engine = engine;
+    return BN_OK;
+}
+
 int bn_ctx_memory(const bn_ctx* ctx, uint64_t* budget, uint64_t* used, uint64_t* peak) {
     if (!ctx) return fail(BN_EINVAL, "null ctx");
     auto* c = const_cast<bn_ctx*>(ctx);
@@ -826,6 +953,7 @@ int bn_flat_build(bn_ctx* ctx, const uint64_t* m_enc, const uint64_t* a_l, const
             cudaError_t er = cudaMemcpyAsync(c.m_enc.p, m_enc, m * N * 8, cudaMemcpyHostToDevice, f->e.stream);
             if (er != cudaSuccess) rc = fail(BN_ECUDA, "upload m_enc: %s", cudaGetErrorString(er));
         }
+        if (rc == BN_OK) rc = corpus_tmap(c);
         if (rc == BN_OK) rc = upload_colmajor(ctx, a_l, m, n1, c.al_cm, f->e.stream);
         if (rc == BN_OK) rc = upload_colmajor(ctx, h, m, n1, c.h_cm, f->e.stream);
         if (rc == BN_OK && cudaStreamSynchronize(f->e.stream) != cudaSuccess) rc = fail(BN_ECUDA, "upload sync failed");
@@ -936,24 +1064,19 @@ int bn_flat_plan(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, bn_plan** 
     if (!B || B > 65535) return fail(BN_EINVAL, "B must be in 1..=65535");
     if (!f->m) return fail(BN_EINVAL, "empty corpus");
     if (k > BN_TOPK_MAX) return fail(BN_EINVAL, "k = %u exceeds BN_TOPK_MAX", k);
+    if (trials > MAX_TRIALS) return fail(BN_EINVAL, "trials = %u exceeds %u", trials, MAX_TRIALS);
     if (k && !f->e.c.client) return fail(BN_EUNSUPPORTED, "this handle has no client state");
     std::lock_guard<std::mutex> gd(f->e.mu);
-    HostMeta hm;
-    flat_meta(f->m, B, hm);
     auto* p = new bn_plan();
     p->h = f;
-    p->z = Sizes{B, f->e.c.n1, trials, k, (uint32_t)pick_ctas(f->m, B, f->e.ctx->num_sms), hm.total_out, hm.segs.size(),
-                 hm.vsegs.size(), plan_freivalds(f->m, B, f->e.ctx->num_sms)};
+    flat_meta(f->m, B, p->hm);
+    p->z = sizes_for(f->e, p->hm, B, trials, k);
     p->o = make_layout(p->z, false);
-    p->nseg = (uint32_t)hm.segs.size();
-    p->total_blocks = hm.seg_blk.back();
     int rc = p->ws.alloc(f->e.ctx, p->o.total);
+    if (rc == BN_OK) rc = make_tc_maps(p->z, reinterpret_cast<uint8_t*>(p->ws.at<char>() + p->o.u_buf), p->maps);
     if (rc == BN_OK) {
         std::vector<char> h(p->o.in_end, 0);
-        memcpy(h.data() + p->o.segs, hm.segs.data(), hm.segs.size() * sizeof(ScanSeg));
-        memcpy(h.data() + p->o.seg_blk, hm.seg_blk.data(), hm.seg_blk.size() * 8);
-        memcpy(h.data() + p->o.vsegs, hm.vsegs.data(), hm.vsegs.size() * sizeof(VerifySeg));
-        memcpy(h.data() + p->o.dq, hm.dq.data(), hm.dq.size() * sizeof(DecodeQuery));
+        pack_meta(h.data(), p->o, p->hm);
         if (cudaMemcpy(p->ws.p, h.data(), p->o.in_end, cudaMemcpyHostToDevice) != cudaSuccess)
             rc = fail(BN_ECUDA, "plan metadata upload failed");
     }
@@ -973,17 +1096,9 @@ int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v, const uint64_t* d_g, const 
         return fail(BN_EINVAL, "null device pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     char* d = p->ws.at<char>();
-    const RunLayout& o = p->o;
-    Meta m{reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk), p->nseg, p->total_blocks,
-           reinterpret_cast<VerifySeg*>(d + o.vsegs), p->nseg, reinterpret_cast<DecodeQuery*>(d + o.dq)};
+    const Meta m = meta_at(d, p->o, p->hm, &p->maps);
     Inputs in{d_v, d_g, d_t, d_t_nnz, d_seeds};
-    Scratch sc{reinterpret_cast<QLimb*>(d + o.limbs), reinterpret_cast<uint64_t*>(d + o.x),
-               reinterpret_cast<uint64_t*>(d + o.r), reinterpret_cast<uint64_t*>(d + o.z_part),
-               reinterpret_cast<uint64_t*>(d + o.ur_part), reinterpret_cast<uint32_t*>(d + o.flags),
-               reinterpret_cast<uint64_t*>(d + o.ur), reinterpret_cast<uint64_t*>(d + o.zv),
-               TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
-                           reinterpret_cast<uint32_t*>(d + o.cand_n)},
-               reinterpret_cast<uint32_t*>(d + o.err)};
+    const Scratch sc = scratch_at(d, p->o);
     Outputs out{d_ids, d_scores, d_n, d_failed, nullptr};
     return enqueue_pipeline(p->h->e.ctx, p->h->e.c, p->z, m, in, sc, out, s);
 }
@@ -996,8 +1111,9 @@ int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v, uint64_t* d_r, void* s
     CU(cudaMemsetAsync(d + o.err, 0, 4, s));
     launch_query_limbs(d_v, p->z.B, reinterpret_cast<QLimb*>(d + o.limbs), s);
     launch_scan(p->h->e.c.m_enc.at<uint64_t>(), reinterpret_cast<QLimb*>(d + o.limbs),
-                reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk), p->nseg,
-                p->total_blocks, d_r, p->h->e.ctx->num_sms, reinterpret_cast<uint32_t*>(d + o.err), s);
+                reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk),
+                (uint32_t)p->hm.segs.size(), p->hm.seg_blk.back(), d_r, p->h->e.ctx->num_sms,
+                reinterpret_cast<uint32_t*>(d + o.err), s);
     CU(cudaGetLastError());
     return BN_OK;
 }
@@ -1045,6 +1161,7 @@ int bn_ivf_build(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const uint32_
     if (rc == BN_OK) rc = c.m_enc.alloc(ctx, rows * N * 8);
     if (rc == BN_OK && rows && cudaMemcpy(c.m_enc.p, m_enc, rows * N * 8, cudaMemcpyHostToDevice) != cudaSuccess)
         rc = fail(BN_ECUDA, "upload m_enc failed");
+    if (rc == BN_OK) rc = corpus_tmap(c);
     if (rc == BN_OK) rc = c.ids.alloc(ctx, std::max<uint64_t>(rows, 1) * 4);
     if (rc == BN_OK && rows && cudaMemcpy(c.ids.p, ids, rows * 4, cudaMemcpyHostToDevice) != cudaSuccess)
         rc = fail(BN_ECUDA, "upload ids failed");

@@ -1,11 +1,11 @@
 // bn_kernels.cu -- CUDA-core kernels of the BN path for sm_100a.
 //
-// scan_kernel       r = M_enc . v (crypto.rs:561-626 / kernels.cu:100-178),
-//                   streamed row-major with 128-bit non-allocating loads;
-//                   one work item = 4 rows x 1024 columns, split over four
-//                   warps (a quarter row each); per element 6 IMAD.WIDE
-//                   into three 64-bit limb accumulators, no carries, no
-//                   per-product fold; a transposed warp reduction and one
+// scan_tma_kernel   r = M_enc . v (crypto.rs:561-626 / kernels.cu:100-178),
+//                   4-row blocks streamed into shared memory by one bulk
+//                   copy each; one work item = 4 rows x 1024 columns split
+//                   over four warps (a quarter row each); per element 6
+//                   IMAD.WIDE into three 64-bit limb accumulators, no carries,
+//                   no per-product fold; a transposed warp reduction and one
 //                   fold per row at the end.
 // freivalds_kernel  Protocol 2 (crypto.rs:1013-1046): u drawn on device from
 //                   the ChaCha20 keystream by index, z_t = u_t^T M_enc and
@@ -23,14 +23,6 @@ namespace bn {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-
-__device__ __forceinline__ uint4 ldg_stream(const uint4* p) {
-    uint4 v;
-    asm("ld.global.nc.L1::no_allocate.L2::256B.v4.u32 {%0,%1,%2,%3}, [%4];"
-        : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-        : "l"(p));
-    return v;
-}
 
 __device__ __forceinline__ void named_bar(int id, int threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
@@ -50,8 +42,6 @@ __global__ void query_limbs_kernel(const uint64_t* __restrict__ v, uint64_t tota
 }
 
 // ------------------------------------------------------------------ scan
-constexpr int SCAN_GROUPS = 4;                 // 4-warp groups per CTA
-constexpr int SCAN_THREADS = 128 * SCAN_GROUPS;
 
 __device__ __forceinline__ uint32_t find_seg(const uint64_t* __restrict__ seg_blk, uint32_t nseg, uint32_t hint,
                                              uint64_t blk) {
@@ -62,103 +52,6 @@ __device__ __forceinline__ uint32_t find_seg(const uint64_t* __restrict__ seg_bl
         if (seg_blk[mid] <= blk) lo = mid; else hi = mid;
     }
     return lo;
-}
-
-__global__ void __launch_bounds__(SCAN_THREADS, 1)
-scan_kernel(const uint64_t* __restrict__ m_enc, const QLimb* __restrict__ qlimbs, const ScanSeg* __restrict__ segs,
-            const uint64_t* __restrict__ seg_blk, uint32_t nseg, uint64_t total_blocks, uint64_t* __restrict__ r) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int group = warp >> 2, wq = warp & 3;
-    __shared__ unsigned long long red[2][SCAN_GROUPS][4][SCAN_ROWS][3];
-
-    uint32_t b0[8], b1[8], b2[8], c0[8], c1[8], c2[8];
-    uint32_t cur_q = 0xffffffffu, seg = 0;
-    int parity = 0;
-    const bool hi16 = (lane & 16) != 0, hi8 = (lane & 8) != 0;
-
-    for (uint64_t blk = (uint64_t)blockIdx.x * SCAN_GROUPS + group; blk < total_blocks;
-         blk += (uint64_t)gridDim.x * SCAN_GROUPS) {
-        seg = find_seg(seg_blk, nseg, seg, blk);
-        const ScanSeg sg = segs[seg];
-        const uint64_t local = (blk - seg_blk[seg]) * SCAN_ROWS;
-        const uint64_t left = (uint64_t)sg.rows - local;
-        const int nrows = left < (uint64_t)SCAN_ROWS ? (int)left : SCAN_ROWS;
-        if (sg.query != cur_q) {
-            cur_q = sg.query;
-            const QLimb* ql = qlimbs + (uint64_t)cur_q * N + wq * 256 + 2 * lane;
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-#pragma unroll
-                for (int e = 0; e < 2; ++e) {
-                    const QLimb q = ql[64 * k + e];
-                    b0[2 * k + e] = q.b0; b1[2 * k + e] = q.b1; b2[2 * k + e] = q.b2;
-                    c0[2 * k + e] = q.c0; c1[2 * k + e] = q.c1; c2[2 * k + e] = q.c2;
-                }
-        }
-        const uint4* base = reinterpret_cast<const uint4*>(m_enc + (sg.row0 + local) * N) + wq * 128 + lane;
-
-        uint64_t acc[SCAN_ROWS][3];
-#pragma unroll
-        for (int rr = 0; rr < SCAN_ROWS; ++rr) {
-            uint64_t a0 = 0, a1 = 0, a2 = 0;
-            if (rr < nrows) {
-                const uint4* rp = base + (uint64_t)rr * (N / 2);
-                uint4 x[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) x[k] = ldg_stream(rp + 32 * k);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int e0 = 2 * k, e1 = 2 * k + 1;
-                    a0 = mac(mac(a0, x[k].x, b0[e0]), x[k].y, c0[e0]);
-                    a1 = mac(mac(a1, x[k].x, b1[e0]), x[k].y, c1[e0]);
-                    a2 = mac(mac(a2, x[k].x, b2[e0]), x[k].y, c2[e0]);
-                    a0 = mac(mac(a0, x[k].z, b0[e1]), x[k].w, c0[e1]);
-                    a1 = mac(mac(a1, x[k].z, b1[e1]), x[k].w, c1[e1]);
-                    a2 = mac(mac(a2, x[k].z, b2[e1]), x[k].w, c2[e1]);
-                }
-            }
-            acc[rr][0] = a0; acc[rr][1] = a1; acc[rr][2] = a2;
-        }
-
-        // Transposed reduction: 4 rows x 3 accumulators over 32 lanes.  Each
-        // accumulator stays below 2^64 over the whole row (1024 products of
-        // < 2^53.2 each), so plain adds suffice.
-        uint64_t w[2][3];
-#pragma unroll
-        for (int q = 0; q < 2; ++q)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                uint64_t send = hi16 ? acc[q][a] : acc[q + 2][a];
-                uint64_t keep = hi16 ? acc[q + 2][a] : acc[q][a];
-                w[q][a] = keep + __shfl_xor_sync(FULL, send, 16);
-            }
-        uint64_t xs[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            uint64_t send = hi8 ? w[0][a] : w[1][a];
-            uint64_t keep = hi8 ? w[1][a] : w[0][a];
-            xs[a] = keep + __shfl_xor_sync(FULL, send, 8);
-        }
-#pragma unroll
-        for (int off = 4; off > 0; off >>= 1)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) xs[a] += __shfl_xor_sync(FULL, xs[a], off);
-        // lane L now holds row (L >> 3) of this warp's quarter.
-        if ((lane & 7) == 0) {
-#pragma unroll
-            for (int a = 0; a < 3; ++a) red[parity][group][wq][lane >> 3][a] = xs[a];
-        }
-        named_bar(1 + group, 128);
-        if (wq == 0 && lane < nrows) {
-            uint64_t s[3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-                s[a] = red[parity][group][0][lane][a] + red[parity][group][1][lane][a] +
-                       red[parity][group][2][lane][a] + red[parity][group][3][lane][a];
-            r[sg.out0 + local + lane] = combine3(s[0], s[1], s[2]);
-        }
-        parity ^= 1;
-    }
 }
 
 // ------------------------------------------------------------------ scan, TMA pipeline

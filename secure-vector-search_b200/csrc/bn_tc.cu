@@ -1,0 +1,417 @@
+// bn_tc.cu -- Protocol 2 (crypto.rs:1013-1046) on the 5th-generation tensor
+// cores: z_t = u_t^T M_enc for up to 20 trials per pass as an exact u8 GEMM
+// (tcgen05.mma kind::i8, s32 accumulators in TMEM), fed by TMA, drained by
+// four epilogue warps that recombine the byte limbs modulo p = 2^61 - 1.
+//
+// Roles per CTA (one CTA per SM, persistent over 4096-row panels):
+//   warp 0  TMA producer: per 128-row stage, S boxes of 128 rows x 128 bytes
+//           of M_enc (S strips of 16 columns) + the 8T x 128 U tile
+//   warp 1  MMA issuer: per stage S x 4 tcgen05.mma (M=128, N=8T, K=32),
+//           tcgen05.commit frees the stage; after the panel's last stage a
+//           commit hands the TMEM accumulators to the epilogue
+//   warps 2-5 epilogue: tcgen05.ld, limb recombination, z partials to HBM
+// Every mbarrier wait is bounded; on timeout the CTA flags *err and winds
+// down (waits for its own copies and MMAs, frees TMEM) instead of hanging.
+#include <cudaTypedefs.h>
+
+#include "bn_tc.cuh"
+
+namespace bn {
+
+namespace {
+
+constexpr unsigned FULLMASK = 0xffffffffu;
+constexpr long long TC_WAIT_CYCLES = 2000000000ll;  // ~1 s
+
+__device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void bar_init(uint64_t* b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!bar_try(b, parity))
+        if (clock64() - t0 > TC_WAIT_CYCLES) return false;
+    return true;
+}
+__device__ __forceinline__ void bar_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(uint64_t* b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* b) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            su32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(su32(b))
+        : "memory");
+}
+__device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: 128-byte swizzle, sm_100 version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3fff) | ((uint64_t)((lbo >> 4) & 0x3fff) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3fff) << 32) | (1ull << 46) | (2ull << 61);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc)
+        : "memory");
+}
+__device__ __forceinline__ void mma_commit(uint64_t* b) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(b)) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
+          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// ------------------------------------------------------------------ u draws
+constexpr int UG_THREADS = 256;
+
+__global__ void __launch_bounds__(UG_THREADS)
+tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ blocks, const ChaChaKey* __restrict__ keys,
+               const uint64_t* __restrict__ r, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows,
+               uint8_t* __restrict__ u_out, uint64_t* __restrict__ ur_part, uint32_t trials_total,
+               uint32_t* __restrict__ flags) {
+    const uint32_t blk = blockIdx.x;
+    const TcBlock tb = blocks[blk];
+    const VerifySeg vs = vsegs[tb.seg];
+    const uint32_t here = min((uint32_t)TC_ROWS, vs.rows - tb.i0);
+    const ChaChaKey key = keys[vs.query];
+    __shared__ uint64_t us[TC_MAX_TRIALS][TC_ROWS];
+
+    // draws: 128 consecutive indices per trial span at most 17 keystream blocks
+    for (uint32_t item = threadIdx.x; item < t_cnt * 17; item += blockDim.x) {
+        const uint32_t tl = item / 17, bi = item % 17;
+        const uint64_t first = (uint64_t)(t_base + tl) * vs.rows + tb.i0;
+        const uint64_t kb = first / 8 + bi;
+        if (kb * 8 >= first + TC_ROWS) continue;
+        uint32_t w[16];
+        chacha20_block(key, kb, w);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint64_t idx = kb * 8 + q;
+            if (idx >= first && idx < first + TC_ROWS) {
+                const uint32_t ii = (uint32_t)(idx - first);
+                uint64_t x = ((uint64_t)w[2 * q] | ((uint64_t)w[2 * q + 1] << 32)) & P;
+                if (ii >= here) x = 0;  // rows past the segment end
+                else if (x == P) { atomicOr(flags, 1u); x = 0; }
+                us[tl][ii] = x;
+            }
+        }
+    }
+    __syncthreads();
+    // U tile image: row (t, b) holds byte b of u_t[i] for the 128 rows i
+    uint8_t* dst = u_out + (uint64_t)blk * n_rows * TC_ROWS;
+    for (uint32_t c = threadIdx.x; c < n_rows * (TC_ROWS / 16); c += blockDim.x) {
+        const uint32_t row = c / (TC_ROWS / 16), ch = c % (TC_ROWS / 16);
+        const uint32_t tl = row / 8, b = row % 8;
+        uint32_t wv[4] = {0, 0, 0, 0};
+        if (tl < t_cnt) {
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const uint32_t byte = (uint32_t)(us[tl][ch * 16 + q] >> (8 * b)) & 0xffu;
+                wv[q >> 2] |= byte << (8 * (q & 3));
+            }
+        }
+        reinterpret_cast<uint4*>(dst + (uint64_t)row * TC_ROWS)[ch] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+    }
+    // u_t . r over this block's rows
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (uint32_t tl = warp; tl < t_cnt; tl += blockDim.x / 32) {
+        uint64_t acc = 0;
+        for (uint32_t ii = lane; ii < here; ii += 32) acc = add_mod(acc, mul_mod(us[tl][ii], r[vs.r0 + tb.i0 + ii]));
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc = add_mod(acc, __shfl_xor_sync(FULLMASK, acc, off));
+        if (lane == 0) ur_part[(uint64_t)blk * trials_total + t_base + tl] = acc;
+    }
+}
+
+// ------------------------------------------------------------------ GEMM + drain
+constexpr int TC_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr uint32_t STRIP_BYTES = TC_ROWS * 128;  // one 128x128 M box
+
+template <int S>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constant__ CUtensorMap tmap_u,
+                    const TcPanel* __restrict__ panels, uint32_t npanels, uint32_t t_base, uint32_t t_cnt,
+                    uint32_t n_rows, uint32_t trials_total, uint32_t stages, uint32_t stage_bytes,
+                    uint64_t* __restrict__ z_part, uint32_t* __restrict__ err) {
+    extern __shared__ uint8_t tc_dyn[];
+    __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    const uint32_t base = (su32(tc_dyn) + 1023u) & ~1023u;  // 1024-byte aligned stage ring
+    uint8_t* ring = tc_dyn + (base - su32(tc_dyn));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t u_off = S * STRIP_BYTES;
+    const uint32_t u_bytes = n_rows * TC_ROWS;
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < stages; ++s) {
+            bar_init(&full_b[s], 1);
+            bar_init(&empty_b[s], 1);
+        }
+        bar_init(&accf_b, 1);
+        bar_init(&acce_b, 4);
+        bar_init(&done_b, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_s)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tmem = tmem_base_s;
+    const uint32_t groups = (64 + S - 1) / S;
+
+    if (warp == 0) {
+        // ---------------------------------------------------------- TMA producer
+        if (lane == 0) {
+            uint64_t it = 0;
+            bool stop = false;
+            for (uint32_t p = blockIdx.x; p < npanels && !stop; p += gridDim.x) {
+                const TcPanel pn = panels[p];
+                const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
+                for (uint32_t g = 0; g < groups && !stop; ++g) {
+                    const uint32_t sg = min((uint32_t)S, 64u - g * S);
+                    for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
+                        const uint32_t st = (uint32_t)(it % stages);
+                        if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1))) {
+                            abort_s = 1;
+                            atomicOr(err, 4u);
+                            stop = true;
+                            break;
+                        }
+                        if (abort_s) { stop = true; break; }
+                        uint8_t* sb = ring + (uint64_t)st * stage_bytes;
+                        bar_expect_tx(&full_b[st], sg * STRIP_BYTES + u_bytes);
+                        for (uint32_t s = 0; s < sg; ++s)
+                            tma_2d(sb + s * STRIP_BYTES, &tmap_m, (int)((g * S + s) * 128), (int)(pn.row0 + rb * TC_ROWS),
+                                   &full_b[st]);
+                        tma_2d(sb + u_off, &tmap_u, 0, (int)((pn.rb0 + rb) * n_rows), &full_b[st]);
+                    }
+                }
+            }
+            // no copy may still be landing in shared memory when the CTA exits
+            for (uint64_t j = it > stages ? it - stages : 0; j < it; ++j)
+                bar_wait(&full_b[j % stages], (uint32_t)((j / stages) & 1));
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = (2u << 4) | (1u << 15) | ((n_rows >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+            uint64_t it = 0, gc = 0;
+            bool stop = false;
+            for (uint32_t p = blockIdx.x; p < npanels && !stop; p += gridDim.x) {
+                const TcPanel pn = panels[p];
+                const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
+                for (uint32_t g = 0; g < groups && !stop; ++g, ++gc) {
+                    const uint32_t sg = min((uint32_t)S, 64u - g * S);
+                    if (gc > 0 && !bar_wait(&acce_b, (uint32_t)((gc - 1) & 1))) {
+                        abort_s = 1;
+                        atomicOr(err, 8u);
+                        stop = true;
+                        break;
+                    }
+                    tc_after();
+                    for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
+                        const uint32_t st = (uint32_t)(it % stages);
+                        if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
+                            abort_s = 1;
+                            atomicOr(err, 8u);
+                            stop = true;
+                            break;
+                        }
+                        tc_after();
+                        const uint32_t sb = base + st * stage_bytes;
+                        for (uint32_t s = 0; s < sg; ++s)
+#pragma unroll
+                            for (uint32_t ks = 0; ks < TC_ROWS / 32; ++ks) {
+                                const uint64_t a = sdesc(sb + s * STRIP_BYTES + ks * 4096u, STRIP_BYTES, 1024);
+                                const uint64_t b = sdesc(sb + u_off + ks * 32u, 16, 1024);
+                                mma_i8(tmem + s * n_rows, a, b, idesc, (rb | ks) != 0);
+                            }
+                        mma_commit(&empty_b[st]);  // stage reusable once these MMAs have read it
+                    }
+                    if (stop) break;
+                    mma_commit(&accf_b);  // accumulators complete for this group
+                }
+            }
+            mma_commit(&done_b);
+            bar_wait(&done_b, 0);  // every issued MMA has finished before TMEM is freed
+        }
+    } else {
+        // ---------------------------------------------------------- epilogue
+        const uint32_t q = (uint32_t)(warp & 3);          // TMEM lane quarter of this warp
+        const uint32_t lane_c = q * 32 + lane;            // byte column within the strip
+        const uint32_t jl = lane_c >> 3, a = lane_c & 7;
+        const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+        uint64_t gc = 0;
+        bool stop = false;
+        for (uint32_t p = blockIdx.x; p < npanels && !stop; p += gridDim.x) {
+            for (uint32_t g = 0; g < groups; ++g, ++gc) {
+                const uint32_t sg = min((uint32_t)S, 64u - g * S);
+                const bool ok = bar_wait(&accf_b, (uint32_t)(gc & 1));
+                if (!ok) { abort_s = 1; atomicOr(err, 16u); }
+                __syncwarp();
+                if (!ok || abort_s) { stop = true; break; }
+                tc_after();
+                for (uint32_t s = 0; s < sg; ++s) {
+                    const uint32_t j = (g * S + s) * 16 + jl;
+                    for (uint32_t c0 = 0; c0 < n_rows; c0 += 16) {
+                        uint32_t v[16];
+                        tmem_ld16(tmem + ((q * 32) << 16) + s * n_rows + c0, v);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const uint32_t t = c0 / 8 + h;
+                            uint64_t lo = 0, hi = 0;
+#pragma unroll
+                            for (int b = 0; b < 4; ++b) {
+                                lo += (uint64_t)v[8 * h + b] << (8 * b);
+                                hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
+                            }
+                            uint64_t zc = canon(rotl61(lo, w1) + rotl61(hi, w2));  // (lo + hi 2^32) 2^(8a) mod p
+                            zc += __shfl_xor_sync(FULLMASK, zc, 1);
+                            zc += __shfl_xor_sync(FULLMASK, zc, 2);
+                            zc += __shfl_xor_sync(FULLMASK, zc, 4);
+                            if (a == 0 && t < t_cnt)
+                                z_part[((uint64_t)p * trials_total + t_base + t) * N + j] = canon(zc);
+                        }
+                    }
+                }
+                tc_before();
+                __syncwarp();
+                if (lane == 0) bar_arrive(&acce_b);
+            }
+        }
+    }
+    tc_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+    }
+}
+
+__global__ void __launch_bounds__(256)
+tc_finish_kernel(const uint64_t* __restrict__ z_part, const uint64_t* __restrict__ ur_part,
+                 const uint32_t* __restrict__ seg_panel0, const uint32_t* __restrict__ seg_block0,
+                 const uint64_t* __restrict__ v_enc, const VerifySeg* __restrict__ vsegs, uint32_t trials,
+                 uint64_t* __restrict__ ur, uint64_t* __restrict__ zv, int32_t* __restrict__ failed) {
+    const uint32_t seg = blockIdx.x;
+    const VerifySeg vs = vsegs[seg];
+    const uint64_t* v = v_enc + (uint64_t)vs.query * N;
+    const uint32_t p0 = seg_panel0[seg], p1 = seg_panel0[seg + 1];
+    const uint32_t b0 = seg_block0[seg], b1 = seg_block0[seg + 1];
+    __shared__ uint64_t sh[8];
+    int32_t fail = -1;
+    for (uint32_t t = 0; t < trials; ++t) {
+        uint64_t part = 0;
+        for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
+            uint64_t z = 0;
+            for (uint32_t p = p0; p < p1; ++p) z = add_mod(z, z_part[((uint64_t)p * trials + t) * N + j]);
+            part = add_mod(part, mul_mod(z, v[j]));
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) part = add_mod(part, __shfl_xor_sync(FULLMASK, part, off));
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = part;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint64_t zvt = 0, urt = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) zvt = add_mod(zvt, sh[w]);
+            for (uint32_t b = b0; b < b1; ++b) urt = add_mod(urt, ur_part[(uint64_t)b * trials + t]);
+            ur[(uint64_t)seg * trials + t] = urt;
+            zv[(uint64_t)seg * trials + t] = zvt;
+            if (fail < 0 && urt != zvt) fail = (int32_t)t;
+        }
+    }
+    if (threadIdx.x == 0) failed[seg] = fail;
+}
+
+}  // namespace
+
+cudaError_t make_tmap_u8(CUtensorMap* map, const void* base, uint64_t inner_bytes, uint64_t rows, uint32_t box_inner,
+                         uint32_t box_rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+        if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn) return e != cudaSuccess ? e : cudaErrorNotSupported;
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[2] = {inner_bytes, rows};
+    const cuuint64_t strides[1] = {inner_bytes};
+    const cuuint32_t box[2] = {box_inner, box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+void launch_tc_ugen(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const ChaChaKey* d_keys,
+                    const uint64_t* d_r, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint8_t* d_u,
+                    uint64_t* d_ur_part, uint32_t trials_total, uint32_t* d_flags, cudaStream_t s) {
+    if (!nblocks) return;
+    tc_ugen_kernel<<<nblocks, UG_THREADS, 0, s>>>(d_vsegs, d_blocks, d_keys, d_r, t_base, t_cnt, n_rows, d_u, d_ur_part,
+                                                  trials_total, d_flags);
+}
+
+void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
+                         uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
+                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s) {
+    if (!npanels) return;
+    const int S = n_rows <= 128 ? 4 : 3;
+    const uint32_t stage_bytes = (uint32_t)S * STRIP_BYTES + ((n_rows * TC_ROWS + 1023u) & ~1023u);
+    uint32_t stages = (220u * 1024u) / stage_bytes;
+    stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
+    const int smem = (int)(stages * stage_bytes + 1024);
+    const unsigned grid = npanels < (uint32_t)num_sms ? npanels : (unsigned)num_sms;
+    if (S == 4) {
+        cudaFuncSetAttribute(tc_freivalds_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        tc_freivalds_kernel<4><<<grid, TC_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, t_base, t_cnt, n_rows,
+                                                              trials_total, stages, stage_bytes, d_z_part, d_err);
+    } else {
+        cudaFuncSetAttribute(tc_freivalds_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        tc_freivalds_kernel<3><<<grid, TC_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, t_base, t_cnt, n_rows,
+                                                              trials_total, stages, stage_bytes, d_z_part, d_err);
+    }
+}
+
+void launch_tc_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint32_t* d_seg_panel0,
+                      const uint32_t* d_seg_block0, const uint64_t* d_v_enc, const VerifySeg* d_vsegs, uint32_t nseg,
+                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, int32_t* d_failed, cudaStream_t s) {
+    if (!nseg) return;
+    tc_finish_kernel<<<nseg, 256, 0, s>>>(d_z_part, d_ur_part, d_seg_panel0, d_seg_block0, d_v_enc, d_vsegs, trials,
+                                          d_ur, d_zv, d_failed);
+}
+
+}  // namespace bn

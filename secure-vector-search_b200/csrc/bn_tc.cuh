@@ -1,0 +1,69 @@
+// bn_tc.cuh -- tensor-core (tcgen05, kind::i8) kernels of the BN path.
+//
+// Protocol 2 on tensor cores.  With M_enc viewed as bytes Mb[i][c]
+// (c = 8j + a, a = byte a of the u64 element j) and the Freivalds draws as
+// bytes Ub[i][(t,b)] (byte b of u_t[i]),
+//     z_t[j] = sum_i u_t[i] M[i][j] = sum_{a,b} 2^(8(a+b)) D[8j+a][(t,b)],
+//     D      = Mb^T Ub                      (exact u8 x u8 -> s32 GEMM),
+// so the 61-bit F_p products become one integer GEMM on the tensor cores
+// followed by a cheap limb recombination mod p.  The M_enc tile that TMA
+// brings into shared memory (128 rows x 128 bytes, 128-byte swizzle) is the
+// MMA's A operand read MN-major; the U tile is the K-major B operand.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bn_chacha.cuh"
+#include "bn_kernels.cuh"
+
+namespace bn {
+
+constexpr int TC_ROWS = 128;         // rows (K) per stage
+constexpr int TC_PANEL_ROWS = 4096;  // rows accumulated in TMEM before a drain (4096 * 255^2 < 2^31)
+constexpr int TC_MAX_TRIALS = 20;    // per pass: N = 8 * trials_padded <= 160
+
+// One panel of a verify segment: rows [row0, row0 + rows) of m_enc, whose U
+// tiles start at row block `rb0` of the U buffer.
+struct TcPanel {
+    uint64_t row0;
+    uint32_t rows;
+    uint32_t rb0;
+    uint32_t seg;
+    uint32_t pad;
+};
+
+// Row block of the U generator: 128 rows of segment `seg` starting at local row `i0`.
+struct TcBlock {
+    uint32_t seg;
+    uint32_t i0;
+};
+
+// Encodes the 2-D tensor maps (driver entry point; no -lcuda needed).
+// Returns cudaSuccess or the failure.
+cudaError_t make_tmap_u8(CUtensorMap* map, const void* base, uint64_t inner_bytes, uint64_t rows, uint32_t box_inner,
+                         uint32_t box_rows);
+
+// u generation: for each row block, U tile bytes [(t,b)][128 rows] (K-major
+// B operand image, un-swizzled; TMA applies the swizzle) for trials
+// [t_base, t_base + t_cnt), padded with zero rows up to n_rows = 8 * t_pad,
+// and u_t . r partial sums per block.  *flags bit 0: a draw hit p.
+void launch_tc_ugen(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const ChaChaKey* d_keys,
+                    const uint64_t* d_r, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint8_t* d_u,
+                    uint64_t* d_ur_part, uint32_t trials_total, uint32_t* d_flags, cudaStream_t s);
+
+// The GEMM + drain: z_part[panel][t_base + t][j] (canonical residues) for
+// t < t_cnt.  tmap_m: m_enc bytes {8192, rows}, box {128, 128}, swizzle 128B;
+// tmap_u: U bytes {128, nblocks * n_rows}, box {128, n_rows}, swizzle 128B.
+// *err: bit 2/3/4 set when a bounded pipeline wait timed out.
+void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
+                         uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
+                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s);
+
+// Per segment: z_t = sum of its panels' partials, zv_t = z_t . v, ur_t =
+// sum of its blocks' partials; failed = first t with ur_t != zv_t or -1.
+void launch_tc_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint32_t* d_seg_panel0,
+                      const uint32_t* d_seg_block0, const uint64_t* d_v_enc, const VerifySeg* d_vsegs, uint32_t nseg,
+                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, int32_t* d_failed, cudaStream_t s);
+
+}  // namespace bn

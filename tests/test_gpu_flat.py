@@ -71,10 +71,21 @@ def test_decode_dense_terms(ctx, m):
     assert [int(v) for v in f.decode_dense_terms(g, x)] == want
 
 
-@pytest.mark.parametrize("trials", [1, 3, 20, 29])
-def test_verify_honest_matches_oracle(ctx, trials):
+@pytest.fixture(params=["tensor", "cuda_core"])
+def engine(request, ctx):
     c = capi()
-    M, L, cl = cluster(777, 21, uniform=True)
+    ctx.set_engine(c.ENGINE_TENSOR if request.param == "tensor" else c.ENGINE_CUDA_CORE)
+    yield request.param
+    ctx.set_engine(c.ENGINE_TENSOR)
+
+
+@pytest.mark.parametrize("m,trials", [(777, 1), (777, 3), (777, 20), (777, 29), (4097, 16), (10000, 17), (1, 5)])
+def test_verify_honest_matches_oracle(ctx, engine, m, trials):
+    """Protocol 2 on both engines: every trial's (u.r, (u^T M).v) pair is
+    bit-equal to the oracle's; panel and row-block boundaries, multi-pass
+    trial counts and both strip widths are covered."""
+    c = capi()
+    M, L, cl = cluster(m, 21 + m, uniform=True)
     f = c.Flat.build(ctx, cl.m_enc, cl.a_l, cl.h_mat, cl.m)
     enc = O.encode_query(uniform_fp(N, 22), L, bytes([23]) * 32)
     r = O.matvec(cl.m_enc, cl.m, N, enc.v_enc)
@@ -85,8 +96,22 @@ def test_verify_honest_matches_oracle(ctx, trials):
     assert np.array_equal(urg, uro) and np.array_equal(zvg, zvo)
 
 
+def test_verify_extreme_residues_tensor(ctx):
+    """All-(p-1) matrix: the largest byte limbs in every position."""
+    c = capi()
+    m = 4500
+    m_enc = np.full((m, N), P - 1, np.uint64)
+    v = np.full(N, P - 1, np.uint64)
+    f = c.Flat.build(ctx, m_enc, np.zeros(m * 128, np.uint64), np.zeros(m * 128, np.uint64), m)
+    r = O.matvec(m_enc, m, N, v)
+    seed = bytes([77]) * 32
+    fo, uro, zvo = O.verify_response(r, m_enc, m, N, v, 20, seed)
+    fg, urg, zvg = f.verify(r, v, seed, 20)
+    assert fo == fg == -1 and np.array_equal(urg, uro) and np.array_equal(zvg, zvo)
+
+
 @pytest.mark.parametrize("pos", [0, 400, 776])
-def test_verify_detects_tampered_response(ctx, pos):
+def test_verify_detects_tampered_response(ctx, engine, pos):
     """crypto.rs:1445-1474: r[pos] += 1 is rejected at trial 0."""
     c = capi()
     M, L, cl = cluster(777, 31, uniform=True)
@@ -115,8 +140,8 @@ def _oracle_query(M, L, cl, v, qs, trials, k):
     return f, ids, sc, r, mv, enc
 
 
-@pytest.mark.parametrize("m,trials,k", [(2000, 3, 10), (1, 0, 10), (513, 20, 100), (300, 3, 1024)])
-def test_query_matches_oracle(ctx, m, trials, k):
+@pytest.mark.parametrize("m,trials,k", [(2000, 3, 10), (1, 0, 10), (513, 20, 100), (300, 3, 1024), (9000, 20, 10)])
+def test_query_matches_oracle(ctx, engine, m, trials, k):
     """Whole BnTmScorer::score path (lib.rs:326-475): r, decoded Mv, top-k
     ids and scores, and the Freivalds bit, for several queries at once."""
     M, L, cl = cluster(m, 100 + m)

@@ -56,8 +56,16 @@ def test_decode_dense_terms_per_list(case, ivf):
         assert [int(t) for t in ivf.decode_dense_terms(ci, g, x)] == want
 
 
+@pytest.fixture(params=["tensor", "cuda_core"])
+def engine(request, ctx):
+    c = capi()
+    ctx.set_engine(c.ENGINE_TENSOR if request.param == "tensor" else c.ENGINE_CUDA_CORE)
+    yield request.param
+    ctx.set_engine(c.ENGINE_TENSOR)
+
+
 @pytest.mark.parametrize("trials", [0, 3, 20])
-def test_query_matches_oracle(case, ivf, trials):
+def test_query_matches_oracle(case, ivf, engine, trials):
     rng = np.random.default_rng(trials)
     B, nprobe, k = 5, 4, 25
     probes = np.stack([rng.permutation(case.nlist)[:nprobe] for _ in range(B)]).astype(np.uint32)
@@ -94,7 +102,7 @@ def test_all_lists_probed_single_list_equals_flat(ctx):
     assert np.array_equal(hi[0][0], hf[0][0]) and np.array_equal(hi[0][1], hf[0][1])
 
 
-def test_verify_tampered_list(case, ivf):
+def test_verify_tampered_list(case, ivf, engine):
     ci = 7
     cl = case.clusters[ci]
     enc = O.encode_query(int8_matrix(1, 768, 12)[0], case.L, bytes([13]) * 32)
