@@ -378,13 +378,22 @@ freivalds_finish_kernel(const uint64_t* __restrict__ z_part, const uint64_t* __r
 }
 
 // ------------------------------------------------------------------ L^T v
-__global__ void lt_times_v_kernel(const uint64_t* __restrict__ L, uint32_t n1, const uint64_t* __restrict__ v,
-                                  uint64_t* __restrict__ x) {
+__global__ void __launch_bounds__(1024)
+lt_times_v_kernel(const uint64_t* __restrict__ L, uint32_t n1, const uint64_t* __restrict__ v, uint64_t* __restrict__ x) {
+    // 1024 threads: column k = tid % n1, j-slice tid / n1; slices combined in shared memory
     const uint32_t q = blockIdx.x;
-    for (uint32_t k = threadIdx.x; k < n1; k += blockDim.x) {
-        uint64_t acc = 0;
-        for (uint32_t j = 0; j < N; ++j) acc = add_mod(acc, mul_mod(L[(uint64_t)j * n1 + k], v[(uint64_t)q * N + j]));
-        x[(uint64_t)q * n1 + k] = acc;
+    const uint32_t k = threadIdx.x % n1, slices = blockDim.x / n1, sl = threadIdx.x / n1;
+    __shared__ uint64_t part[1024];
+    uint64_t acc = 0;
+    if (sl < slices)
+        for (uint32_t j = sl; j < N; j += slices)
+            acc = add_mod(acc, mul_mod(L[(uint64_t)j * n1 + k], v[(uint64_t)q * N + j]));
+    part[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x < n1) {
+        uint64_t s = 0;
+        for (uint32_t i = 0; i < slices; ++i) s = add_mod(s, part[i * n1 + threadIdx.x]);
+        x[(uint64_t)q * n1 + threadIdx.x] = s;
     }
 }
 
@@ -800,7 +809,7 @@ void launch_freivalds_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part
 
 void launch_lt_times_v(const uint64_t* d_L, uint32_t n1, const uint64_t* d_v, uint32_t nq, uint64_t* d_x,
                        cudaStream_t s) {
-    lt_times_v_kernel<<<nq, 128, 0, s>>>(d_L, n1, d_v, d_x);
+    lt_times_v_kernel<<<nq, (1024 / n1) * n1, 0, s>>>(d_L, n1, d_v, d_x);
 }
 
 void launch_dense_terms(const uint64_t* d_al_cm, const uint64_t* d_h_cm, uint64_t rows, uint32_t n1,

@@ -195,10 +195,11 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
         if (lane == 0) {
             uint64_t it = 0;
             bool stop = false;
-            for (uint32_t p = blockIdx.x; p < npanels && !stop; p += gridDim.x) {
+            for (uint32_t item = blockIdx.x; item < npanels * groups && !stop; item += gridDim.x) {
+                const uint32_t p = item / groups, g = item % groups;
                 const TcPanel pn = panels[p];
                 const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
-                for (uint32_t g = 0; g < groups && !stop; ++g) {
+                {
                     const uint32_t sg = min((uint32_t)S, 64u - g * S);
                     for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                         const uint32_t st = (uint32_t)(it % stages);
@@ -228,10 +229,11 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
             const uint32_t idesc = (2u << 4) | (1u << 15) | ((n_rows >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
             uint64_t it = 0, gc = 0;
             bool stop = false;
-            for (uint32_t p = blockIdx.x; p < npanels && !stop; p += gridDim.x) {
+            for (uint32_t item = blockIdx.x; item < npanels * groups && !stop; item += gridDim.x, ++gc) {
+                const uint32_t p = item / groups, g = item % groups;
                 const TcPanel pn = panels[p];
                 const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
-                for (uint32_t g = 0; g < groups && !stop; ++g, ++gc) {
+                {
                     const uint32_t sg = min((uint32_t)S, 64u - g * S);
                     if (gc > 0 && !bar_wait(&acce_b, (uint32_t)((gc - 1) & 1))) {
                         abort_s = 1;
@@ -274,8 +276,9 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
         const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
         uint64_t gc = 0;
         bool stop = false;
-        for (uint32_t p = blockIdx.x; p < npanels && !stop; p += gridDim.x) {
-            for (uint32_t g = 0; g < groups; ++g, ++gc) {
+        for (uint32_t item = blockIdx.x; item < npanels * groups && !stop; item += gridDim.x, ++gc) {
+            const uint32_t p = item / groups, g = item % groups;
+            {
                 const uint32_t sg = min((uint32_t)S, 64u - g * S);
                 const bool ok = bar_wait(&accf_b, (uint32_t)(gc & 1));
                 if (!ok) { abort_s = 1; atomicOr(err, 16u); }
@@ -319,40 +322,54 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
     }
 }
 
+__device__ __forceinline__ uint64_t block_sum_mod256(uint64_t v, uint64_t* sh) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = add_mod(v, __shfl_xor_sync(FULLMASK, v, off));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint64_t t = 0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = add_mod(t, sh[w]);
+    return t;
+}
+
+// One CTA per (trial, segment): zv = (sum over panels of z) . v, ur = sum over blocks.
 __global__ void __launch_bounds__(256)
 tc_finish_kernel(const uint64_t* __restrict__ z_part, const uint64_t* __restrict__ ur_part,
                  const uint32_t* __restrict__ seg_panel0, const uint32_t* __restrict__ seg_block0,
                  const uint64_t* __restrict__ v_enc, const VerifySeg* __restrict__ vsegs, uint32_t trials,
-                 uint64_t* __restrict__ ur, uint64_t* __restrict__ zv, int32_t* __restrict__ failed) {
-    const uint32_t seg = blockIdx.x;
+                 uint64_t* __restrict__ ur, uint64_t* __restrict__ zv) {
+    const uint32_t t = blockIdx.x, seg = blockIdx.y;
     const VerifySeg vs = vsegs[seg];
     const uint64_t* v = v_enc + (uint64_t)vs.query * N;
     const uint32_t p0 = seg_panel0[seg], p1 = seg_panel0[seg + 1];
     const uint32_t b0 = seg_block0[seg], b1 = seg_block0[seg + 1];
     __shared__ uint64_t sh[8];
-    int32_t fail = -1;
-    for (uint32_t t = 0; t < trials; ++t) {
-        uint64_t part = 0;
-        for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
-            uint64_t z = 0;
-            for (uint32_t p = p0; p < p1; ++p) z = add_mod(z, z_part[((uint64_t)p * trials + t) * N + j]);
-            part = add_mod(part, mul_mod(z, v[j]));
-        }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) part = add_mod(part, __shfl_xor_sync(FULLMASK, part, off));
-        __syncthreads();
-        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = part;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            uint64_t zvt = 0, urt = 0;
-            for (int w = 0; w < (int)(blockDim.x >> 5); ++w) zvt = add_mod(zvt, sh[w]);
-            for (uint32_t b = b0; b < b1; ++b) urt = add_mod(urt, ur_part[(uint64_t)b * trials + t]);
-            ur[(uint64_t)seg * trials + t] = urt;
-            zv[(uint64_t)seg * trials + t] = zvt;
-            if (fail < 0 && urt != zvt) fail = (int32_t)t;
-        }
+    uint64_t part = 0;
+    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
+        uint64_t z = 0;
+        for (uint32_t p = p0; p < p1; ++p) z = add_mod(z, z_part[((uint64_t)p * trials + t) * N + j]);
+        part = add_mod(part, mul_mod(z, v[j]));
     }
-    if (threadIdx.x == 0) failed[seg] = fail;
+    const uint64_t zvt = block_sum_mod256(part, sh);
+    uint64_t u = 0;
+    for (uint32_t b = b0 + threadIdx.x; b < b1; b += blockDim.x) u = add_mod(u, ur_part[(uint64_t)b * trials + t]);
+    const uint64_t urt = block_sum_mod256(u, sh);
+    if (threadIdx.x == 0) {
+        ur[(uint64_t)seg * trials + t] = urt;
+        zv[(uint64_t)seg * trials + t] = zvt;
+    }
+}
+
+__global__ void tc_decide_kernel(const uint64_t* __restrict__ ur, const uint64_t* __restrict__ zv, uint32_t nseg,
+                                 uint32_t trials, int32_t* __restrict__ failed) {
+    const uint32_t seg = blockIdx.x * blockDim.x + threadIdx.x;
+    if (seg >= nseg) return;
+    int32_t f = -1;
+    for (uint32_t t = 0; t < trials && f < 0; ++t)
+        if (ur[(uint64_t)seg * trials + t] != zv[(uint64_t)seg * trials + t]) f = (int32_t)t;
+    failed[seg] = f;
 }
 
 }  // namespace
@@ -394,7 +411,8 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
     uint32_t stages = (220u * 1024u) / stage_bytes;
     stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
     const int smem = (int)(stages * stage_bytes + 1024);
-    const unsigned grid = npanels < (uint32_t)num_sms ? npanels : (unsigned)num_sms;
+    const uint32_t items = npanels * ((64 + S - 1) / S);
+    const unsigned grid = items < (uint32_t)num_sms ? items : (unsigned)num_sms;
     if (S == 4) {
         cudaFuncSetAttribute(tc_freivalds_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         tc_freivalds_kernel<4><<<grid, TC_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, t_base, t_cnt, n_rows,
@@ -409,9 +427,14 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
 void launch_tc_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint32_t* d_seg_panel0,
                       const uint32_t* d_seg_block0, const uint64_t* d_v_enc, const VerifySeg* d_vsegs, uint32_t nseg,
                       uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, int32_t* d_failed, cudaStream_t s) {
-    if (!nseg) return;
-    tc_finish_kernel<<<nseg, 256, 0, s>>>(d_z_part, d_ur_part, d_seg_panel0, d_seg_block0, d_v_enc, d_vsegs, trials,
-                                          d_ur, d_zv, d_failed);
+    if (!nseg || !trials) return;
+    for (uint32_t s0 = 0; s0 < nseg; s0 += 65535u) {  // grid.y limit
+        const uint32_t ns = nseg - s0 < 65535u ? nseg - s0 : 65535u;
+        tc_finish_kernel<<<dim3(trials, ns), 256, 0, s>>>(d_z_part, d_ur_part, d_seg_panel0 + s0, d_seg_block0 + s0,
+                                                          d_v_enc, d_vsegs + s0, trials, d_ur + (uint64_t)s0 * trials,
+                                                          d_zv + (uint64_t)s0 * trials);
+    }
+    tc_decide_kernel<<<(nseg + 127) / 128, 128, 0, s>>>(d_ur, d_zv, nseg, trials, d_failed);
 }
 
 }  // namespace bn
