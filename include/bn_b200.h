@@ -113,6 +113,21 @@ int bn_flat_decode_dense_terms(bn_flat* h, const uint64_t* g, const uint64_t* lt
  * trials) receive both sides of every trial. */
 int bn_flat_verify(bn_flat* h, const uint64_t* r, const uint64_t* v_enc, const uint8_t v_seed[32], uint32_t trials,
                    int32_t* failed_trial, uint64_t* ur, uint64_t* zv);
+/* Allocation-free form of bn_flat_verify over device buffers, enqueued on
+ * `stream` (no synchronisation).  No counterpart in the reference.  For
+ * callers that cannot allocate device memory while scoring: services that
+ * pre-reserve their whole memory budget and must not fail an allocation
+ * mid-request, and latency-critical threads for which cudaMalloc / cudaFree
+ * could synchronise the device.  Its scratch is a fixed array of about
+ * 3 MiB in the library, held on every GPU that loads it until exit; trials
+ * must be in 1..=BN_NOALLOC_MAX_TRIALS.  All calls share that array: calls
+ * that overlap on the GPU race, so serialise them.  The first call on a
+ * device resolves the array's address; make it outside stream capture.
+ *   d_r m, d_v_enc 1024, d_v_seed 32 bytes; outputs d_failed_trial (1),
+ *   d_ur / d_zv (trials) as in bn_flat_verify. */
+#define BN_NOALLOC_MAX_TRIALS 24
+int bn_flat_verify_noalloc(bn_flat* h, const uint64_t* d_r, const uint64_t* d_v_enc, const uint8_t* d_v_seed,
+                           uint32_t trials, int32_t* d_failed_trial, uint64_t* d_ur, uint64_t* d_zv, void* stream);
 /* Whole server + client path of BnTmScorer::score / score_batch
  * (lib.rs:326-475, 522-624) for B encoded queries: scan, fused-launch
  * Protocol 2, decode, fp_to_signed and top-k, all on the device.

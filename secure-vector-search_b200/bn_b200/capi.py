@@ -58,6 +58,7 @@ _SIGS = {
     "bn_flat_compute_products_batch": (C.c_int, [vp, vp, u32, vp]),
     "bn_flat_decode_dense_terms": (C.c_int, [vp, vp, vp, vp]),
     "bn_flat_verify": (C.c_int, [vp, vp, vp, vp, u32, vp, vp, vp]),
+    "bn_flat_verify_noalloc": (C.c_int, [vp, vp, vp, vp, u32, vp, vp, vp, vp]),
     "bn_flat_query": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp, vp]),
     "bn_flat_plan": (C.c_int, [vp, u32, u32, u32, vp]),
     "bn_plan_enqueue": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),

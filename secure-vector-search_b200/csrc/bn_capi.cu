@@ -1140,6 +1140,18 @@ static int check_offsets(uint32_t nlist, const uint64_t* off) {
     return BN_OK;
 }
 
+// Internal hooks for bn_noalloc.cu (not part of the public header).
+int bn_internal_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
+int bn_internal_flat_view(const bn_flat* f, int* device, const uint64_t** d_m_enc, uint64_t* rows, int* num_sms) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    *device = f->e.ctx->device;
+    *d_m_enc = f->e.c.m_enc.at<uint64_t>();
+    *rows = f->m;
+    *num_sms = f->e.ctx->num_sms;
+    return BN_OK;
+}
+
 int bn_ivf_build(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const uint32_t* ids, const uint64_t* m_enc,
                  const uint64_t* a_l, const uint64_t* h, uint32_t n, uint32_t n1, bn_ivf** out) {
     if (!ctx || !out) return fail(BN_EINVAL, "null argument");

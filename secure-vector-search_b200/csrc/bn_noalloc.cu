@@ -1,0 +1,132 @@
+// bn_noalloc.cu -- Protocol 2 verification that allocates nothing.
+//
+// bn_flat_verify_noalloc runs the same Freivalds computation as
+// bn_flat_verify with the CUDA-core engine, but every byte of scratch it
+// needs lives in the file-scope array below, which the CUDA runtime creates
+// when the library is loaded on a device.  It exists for callers that
+// cannot allocate device memory while they score:
+//   - services that pre-reserve their whole device-memory budget at start-up
+//     (the reference's VRAM budget model, scorer-gpu-common/src/budget.rs)
+//     and must not fail an allocation under memory pressure mid-request;
+//   - latency-critical request threads, where cudaMalloc / cudaFree may
+//     synchronise the device and stall every stream in flight.
+//
+// Limits: at most BN_NOALLOC_MAX_TRIALS trials and the row chunking below
+// (the array holds 16 chunks x 24 trials x 1024 z partials, ~3 MiB per GPU,
+// kept until the process exits).  Every call shares the one array, so calls
+// that overlap on the GPU (two streams, or two threads) race and corrupt
+// each other's partial sums: serialise them.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <mutex>
+
+#include "bn_b200.h"
+#include "bn_kernels.cuh"
+
+using namespace bn;
+
+namespace {
+
+constexpr uint32_t NOALLOC_CHUNKS = 16;
+constexpr uint32_t NOALLOC_TRIALS = BN_NOALLOC_MAX_TRIALS;
+
+// Layout: z partials | u.r partials | rejection flags | segment descriptor.
+constexpr size_t Z_WORDS = (size_t)NOALLOC_CHUNKS * NOALLOC_TRIALS * N;
+constexpr size_t UR_WORDS = (size_t)NOALLOC_CHUNKS * NOALLOC_TRIALS;
+constexpr size_t SCRATCH_BYTES = (Z_WORDS + UR_WORDS) * 8 + 256 + 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SCRATCH_BYTES];
+
+// Clears what must start at zero and writes this call's segment descriptor.
+__global__ void noalloc_init_kernel(uint32_t rows) {
+    uint32_t* flags = reinterpret_cast<uint32_t*>(g_noalloc_scratch + (Z_WORDS + UR_WORDS) * 8);
+    VerifySeg* vseg = reinterpret_cast<VerifySeg*>(g_noalloc_scratch + (Z_WORDS + UR_WORDS) * 8 + 256);
+    *flags = 0;
+    *vseg = VerifySeg{0, 0, rows, 0};
+}
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_mu;
+void* g_scratch_ptr[MAX_DEVICES] = {nullptr};
+
+thread_local char g_msg[512];
+
+}  // namespace
+
+// Defined in bn_capi.cu: records a message for bn_last_error().
+extern "C" int bn_internal_set_error(int code, const char* msg);
+// Defined in bn_capi.cu: the device and device-resident m_enc of a flat handle.
+extern "C" int bn_internal_flat_view(const bn_flat* h, int* device, const uint64_t** d_m_enc, uint64_t* rows,
+                                     int* num_sms);
+
+extern "C" int bn_flat_verify_noalloc(bn_flat* h, const uint64_t* d_r, const uint64_t* d_v_enc,
+                                      const uint8_t* d_v_seed, uint32_t trials, int32_t* d_failed_trial,
+                                      uint64_t* d_ur, uint64_t* d_zv, void* stream) {
+    if (!h || !d_r || !d_v_enc || !d_v_seed || !d_failed_trial || !d_ur || !d_zv)
+        return bn_internal_set_error(BN_EINVAL, "bn_flat_verify_noalloc: null argument");
+    if (trials == 0 || trials > NOALLOC_TRIALS) {
+        snprintf(g_msg, sizeof g_msg, "bn_flat_verify_noalloc: trials = %u is outside 1..=%u (static scratch limit)",
+                 trials, NOALLOC_TRIALS);
+        return bn_internal_set_error(BN_EINVAL, g_msg);
+    }
+    int device = 0, sms = 0;
+    const uint64_t* m_enc = nullptr;
+    uint64_t rows = 0;
+    int rc = bn_internal_flat_view(h, &device, &m_enc, &rows, &sms);
+    if (rc != BN_OK) return rc;
+    if (rows == 0 || rows > 0xffffffffull)
+        return bn_internal_set_error(BN_EINVAL, "bn_flat_verify_noalloc: the corpus must have 1..2^32-1 rows");
+    if (device < 0 || device >= MAX_DEVICES) return bn_internal_set_error(BN_EINVAL, "device index out of range");
+
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        snprintf(g_msg, sizeof g_msg, "cudaSetDevice: %s", cudaGetErrorString(e));
+        return bn_internal_set_error(BN_ECUDA, g_msg);
+    }
+    void* base = nullptr;
+    {
+        // One-time set-up per device: the array's device address.  Do this
+        // first call outside any stream capture.
+        std::lock_guard<std::mutex> g(g_mu);
+        if (!g_scratch_ptr[device]) {
+            e = cudaGetSymbolAddress(&g_scratch_ptr[device], g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                g_scratch_ptr[device] = nullptr;
+                snprintf(g_msg, sizeof g_msg, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+                return bn_internal_set_error(BN_ECUDA, g_msg);
+            }
+        }
+        base = g_scratch_ptr[device];
+    }
+
+    // Fit the rows into at most NOALLOC_CHUNKS chunks of 32-row multiples.
+    FreivaldsPlan plan = plan_freivalds(rows, 1, sms);
+    if (plan.chunks > NOALLOC_CHUNKS) {
+        uint64_t cr = (rows + NOALLOC_CHUNKS - 1) / NOALLOC_CHUNKS;
+        cr = (cr + 31) / 32 * 32;
+        plan.chunk_rows = (uint32_t)cr;
+        plan.chunks = (uint32_t)((rows + cr - 1) / cr);
+    }
+
+    unsigned char* sb = static_cast<unsigned char*>(base);
+    uint64_t* z_part = reinterpret_cast<uint64_t*>(sb);
+    uint64_t* ur_part = z_part + Z_WORDS;
+    uint32_t* flags = reinterpret_cast<uint32_t*>(sb + (Z_WORDS + UR_WORDS) * 8);
+    VerifySeg* vseg = reinterpret_cast<VerifySeg*>(sb + (Z_WORDS + UR_WORDS) * 8 + 256);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+
+    // The array keeps the previous call's contents: reset the rejection flag
+    // and write this call's segment descriptor on the stream.  The z and u.r
+    // partials are fully overwritten by the kernels below.
+    noalloc_init_kernel<<<1, 1, 0, s>>>((uint32_t)rows);
+    launch_freivalds(m_enc, d_r, vseg, 1, reinterpret_cast<const ChaChaKey*>(d_v_seed), trials, plan, z_part, ur_part,
+                     flags, s);
+    launch_freivalds_finish(z_part, ur_part, d_v_enc, vseg, 1, trials, plan, d_ur, d_zv, d_failed_trial, s);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        snprintf(g_msg, sizeof g_msg, "bn_flat_verify_noalloc launch: %s", cudaGetErrorString(e));
+        return bn_internal_set_error(BN_ECUDA, g_msg);
+    }
+    return BN_OK;
+}
