@@ -375,6 +375,7 @@ struct Scratch {  // device pointers
     TopkScratch topk;
     uint32_t* err;  // device pipeline timeout flags
     uint8_t* u_buf;
+    uint64_t* r_part;  // fused pass: per strip-group partial dots
 };
 struct Inputs {
     const uint64_t* v;
@@ -456,7 +457,7 @@ struct RunLayout {
     // outputs (contiguous -> one D2H)
     uint64_t ids, scores, n, vfailed, ur, zv, err, out_begin, out_end;
     // internal
-    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, total;
+    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, r_part, total;
 };
 
 RunLayout make_layout(const Sizes& z, bool want_mv) {
@@ -500,6 +501,10 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
     o.cand_i = L.take<uint32_t>(cand);
     o.cand_n = L.take<uint32_t>((uint64_t)z.B * z.ctas);
     o.u_buf = (tc && z.trials) ? L.take<uint8_t>(std::max<uint64_t>(z.nblocks, 1) * pass_rows(TC_MAX_TRIALS) * TC_ROWS) : 0;
+    o.r_part = (tc && z.trials)
+                   ? L.take<uint64_t>((uint64_t)tc_groups(pass_rows(std::min<uint32_t>(TC_MAX_TRIALS, z.trials))) *
+                                      std::max<uint64_t>(z.total_out, 1))
+                   : 0;
     o.total = L.off + 1024;
     return o;
 }
@@ -518,29 +523,41 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
                      const Outputs& out, cudaStream_t s) {
     CU(cudaMemsetAsync(sc.err, 0, 4, s));
     launch_query_limbs(in.v, z.B, sc.limbs, s);
-    launch_scan(c.m_enc.at<uint64_t>(), sc.limbs, m.segs, m.seg_blk, m.nseg, m.total_blocks, sc.r, ctx->num_sms, sc.err,
-                s);
-    if (z.trials) {
+    const ChaChaKey* keys = reinterpret_cast<const ChaChaKey*>(in.seeds);
+    if (z.trials && z.engine == BN_ENGINE_TENSOR) {
+        // One pass over m_enc yields r and the first <= 20 trials' z (tensor
+        // cores); later passes of 20 trials reuse the now-known r.
         CU(cudaMemsetAsync(sc.flags, 0, 4, s));
-        const ChaChaKey* keys = reinterpret_cast<const ChaChaKey*>(in.seeds);
-        if (z.engine == BN_ENGINE_TENSOR) {
-            for (uint32_t t0 = 0, ps = 0; t0 < z.trials; t0 += TC_MAX_TRIALS, ++ps) {
-                const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, z.trials - t0), nr = pass_rows(tc);
+        for (uint32_t t0 = 0, ps = 0; t0 < z.trials; t0 += TC_MAX_TRIALS, ++ps) {
+            const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, z.trials - t0), nr = pass_rows(tc);
+            if (ps == 0) {
+                launch_tc_ugen(m.vsegs, m.tc_blocks, m.nblocks, keys, nullptr, t0, tc, nr, sc.u_buf, sc.ur_part,
+                               z.trials, sc.flags, s);
+                launch_tc_fused(c.tmap_m, m.maps->u[ps], m.tc_panels, m.npanels, m.vsegs, sc.limbs, tc, nr, z.trials,
+                                sc.z_part, sc.r_part, z.total_out, sc.err, ctx->num_sms, s);
+                launch_tc_rreduce(m.vsegs, m.tc_blocks, m.nblocks, sc.r_part, z.total_out, tc_groups(nr), sc.u_buf, tc,
+                                  nr, z.trials, sc.r, sc.ur_part, s);
+            } else {
                 launch_tc_ugen(m.vsegs, m.tc_blocks, m.nblocks, keys, sc.r, t0, tc, nr, sc.u_buf, sc.ur_part, z.trials,
                                sc.flags, s);
                 launch_tc_freivalds(c.tmap_m, m.maps->u[ps], m.tc_panels, m.npanels, t0, tc, nr, z.trials, sc.z_part,
                                     sc.err, ctx->num_sms, s);
             }
-            launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, in.v, m.vsegs, m.nvseg, z.trials, sc.ur,
-                             sc.zv, out.vfailed, s);
-        } else {
+        }
+        launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, in.v, m.vsegs, m.nvseg, z.trials, sc.ur,
+                         sc.zv, out.vfailed, s);
+    } else {
+        launch_scan(c.m_enc.at<uint64_t>(), sc.limbs, m.segs, m.seg_blk, m.nseg, m.total_blocks, sc.r, ctx->num_sms,
+                    sc.err, s);
+        if (z.trials) {
+            CU(cudaMemsetAsync(sc.flags, 0, 4, s));
             launch_freivalds(c.m_enc.at<uint64_t>(), sc.r, m.vsegs, m.nvseg, keys, z.trials, z.fp, sc.z_part, sc.ur_part,
                              sc.flags, s);
             launch_freivalds_finish(sc.z_part, sc.ur_part, in.v, m.vsegs, m.nvseg, z.trials, z.fp, sc.ur, sc.zv,
                                     out.vfailed, s);
+        } else {
+            CU(cudaMemsetAsync(out.vfailed, 0xff, std::max<uint64_t>(m.nvseg, 1) * 4, s));
         }
-    } else {
-        CU(cudaMemsetAsync(out.vfailed, 0xff, std::max<uint64_t>(m.nvseg, 1) * 4, s));
     }
     if (z.k) {
         launch_lt_times_v(c.L.at<uint64_t>(), c.n1, in.v, z.B, sc.x, s);
@@ -570,7 +587,8 @@ Scratch scratch_at(char* d, const RunLayout& o) {
                    reinterpret_cast<uint64_t*>(d + o.ur), reinterpret_cast<uint64_t*>(d + o.zv),
                    TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
                                reinterpret_cast<uint32_t*>(d + o.cand_n)},
-                   reinterpret_cast<uint32_t*>(d + o.err), reinterpret_cast<uint8_t*>(d + o.u_buf)};
+                   reinterpret_cast<uint32_t*>(d + o.err), reinterpret_cast<uint8_t*>(d + o.u_buf),
+                   reinterpret_cast<uint64_t*>(d + o.r_part)};
 }
 void pack_meta(char* h, const RunLayout& o, const HostMeta& hm) {
     memcpy(h + o.segs, hm.segs.data(), hm.segs.size() * sizeof(ScanSeg));

@@ -21,6 +21,9 @@ constexpr uint32_t N = 1024;          // ring dimension, params.rs:89-91
 constexpr uint32_t LIMB_BITS = 21;    // v = b0 + b1*2^21 + b2*2^42
 constexpr uint32_t LIMB_MASK = (1u << LIMB_BITS) - 1;
 
+// 64-bit accumulate of a 32 x 32 -> 64 product (one IMAD.WIDE.U32).
+BN_HD uint64_t mac(uint64_t acc, uint32_t a, uint32_t b) { return acc + (uint64_t)a * (uint64_t)b; }
+
 // One Mersenne fold: x (< 2^64) -> congruent value < 2^61 + 8.
 BN_HD uint64_t fold(uint64_t x) { return (x & P) + (x >> 61); }
 

@@ -28,10 +28,6 @@ __device__ __forceinline__ void named_bar(int id, int threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 
-__device__ __forceinline__ uint64_t mac(uint64_t acc, uint32_t a, uint32_t b) {
-    return acc + (uint64_t)a * (uint64_t)b;
-}
-
 // ------------------------------------------------------------------ limbs
 __global__ void query_limbs_kernel(const uint64_t* __restrict__ v, uint64_t total, QLimb* __restrict__ out) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -126,6 +122,7 @@ scan_tma_kernel(const uint64_t* __restrict__ m_enc, const QLimb* __restrict__ ql
     __shared__ uint64_t full_bar[TS_STAGES], empty_bar[TS_STAGES];
     __shared__ unsigned long long red[2][TS_GROUPS][4][SCAN_ROWS][3];
     __shared__ volatile int abort_flag;
+    __shared__ volatile int group_stop[2][TS_GROUPS];  // per-iteration snapshot, double-buffered
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -236,8 +233,11 @@ scan_tma_kernel(const uint64_t* __restrict__ m_enc, const QLimb* __restrict__ ql
 #pragma unroll
             for (int a = 0; a < 3; ++a) red[parity][group][wq][lane >> 3][a] = xs[a];
         }
+        // Stop decision: one snapshot per group and iteration, written before
+        // the barrier and read after it, so the four warps agree.
+        if (wq == 0 && lane == 0) group_stop[parity][group] = abort_flag;
         named_bar(1 + group, 128);
-        if (abort_flag) break;  // read after the barrier: uniform across the group
+        if (group_stop[parity][group]) break;
         if (wq == 0 && lane < b.nrows) {
             uint64_t t[3];
 #pragma unroll
@@ -501,6 +501,34 @@ __device__ __forceinline__ uint32_t find_query_seg(const ScanSeg* __restrict__ s
     return lo;
 }
 
+// Two rows per thread: every broadcast limb load serves both rows.
+__device__ __forceinline__ void cm_dot2(const uint64_t* __restrict__ a_cm, uint64_t rows, uint64_t row0, uint64_t row1,
+                                        bool has1, const uint4* __restrict__ vl, uint32_t n1, uint64_t& out0,
+                                        uint64_t& out1) {
+    uint64_t a0 = 0, a1 = 0, a2 = 0, e0 = 0, e1 = 0, e2 = 0;
+    const uint64_t* p0 = a_cm + row0;
+    const uint64_t* p1 = a_cm + (has1 ? row1 : row0);
+#pragma unroll 4
+    for (uint32_t k = 0; k < n1; ++k) {
+        const uint64_t x = __ldg(p0 + (uint64_t)k * rows);
+        const uint64_t y = __ldg(p1 + (uint64_t)k * rows);
+        const uint4 l0 = vl[2 * k], l1 = vl[2 * k + 1];  // {b0,b1,b2,c0}, {c1,c2,-,-}
+        const uint32_t xl = (uint32_t)x, xh = (uint32_t)(x >> 32), yl = (uint32_t)y, yh = (uint32_t)(y >> 32);
+        a0 = mac(mac(a0, xl, l0.x), xh, l0.w);
+        a1 = mac(mac(a1, xl, l0.y), xh, l1.x);
+        a2 = mac(mac(a2, xl, l0.z), xh, l1.y);
+        e0 = mac(mac(e0, yl, l0.x), yh, l0.w);
+        e1 = mac(mac(e1, yl, l0.y), yh, l1.x);
+        e2 = mac(mac(e2, yl, l0.z), yh, l1.y);
+    }
+    out0 = combine3(a0, a1, a2);
+    out1 = combine3(e0, e1, e2);
+}
+
+// Sum of +-x (sign in bit 31 of the entry) over a gathered column list,
+// folded lazily: every term is < 2^61, three terms fit below 2^63.
+__device__ __forceinline__ uint64_t signed_term(uint64_t x, bool neg) { return neg ? P - x : x; }
+
 __global__ void __launch_bounds__(DT_THREADS)
 decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ al_cm, const uint64_t* __restrict__ h_cm,
                    const uint64_t* __restrict__ mp_cm, const uint16_t* __restrict__ s_ell,
@@ -517,9 +545,9 @@ decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ 
         if (threadIdx.x == 0) cand_n[(uint64_t)q * gridDim.x + blockIdx.x] = 0;
         return;
     }
-    extern __shared__ uint32_t dyn_limbs[];
-    uint32_t(*gl)[6] = reinterpret_cast<uint32_t(*)[6]>(dyn_limbs);
-    uint32_t(*xl)[6] = reinterpret_cast<uint32_t(*)[6]>(dyn_limbs + 6 * n1);
+    extern __shared__ uint4 dyn_limbs[];
+    uint4* gl = dyn_limbs;           // 2 x uint4 per k
+    uint4* xl = dyn_limbs + 2 * n1;
     __shared__ uint64_t vs[N];
     __shared__ uint32_t tl[N];
     __shared__ TopkBuf buf;
@@ -527,9 +555,11 @@ decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ 
     for (uint32_t kk = threadIdx.x; kk < n1; kk += blockDim.x) {
         const uint64_t gv = gg[(uint64_t)q * n1 + kk], xv = xx[(uint64_t)q * n1 + kk];
         Limbs3 b = limbs(gv), c = limbs_hi(gv);
-        gl[kk][0] = b.b0; gl[kk][1] = b.b1; gl[kk][2] = b.b2; gl[kk][3] = c.b0; gl[kk][4] = c.b1; gl[kk][5] = c.b2;
+        gl[2 * kk] = make_uint4(b.b0, b.b1, b.b2, c.b0);
+        gl[2 * kk + 1] = make_uint4(c.b1, c.b2, 0u, 0u);
         b = limbs(xv); c = limbs_hi(xv);
-        xl[kk][0] = b.b0; xl[kk][1] = b.b1; xl[kk][2] = b.b2; xl[kk][3] = c.b0; xl[kk][4] = c.b1; xl[kk][5] = c.b2;
+        xl[2 * kk] = make_uint4(b.b0, b.b1, b.b2, c.b0);
+        xl[2 * kk + 1] = make_uint4(c.b1, c.b2, 0u, 0u);
     }
     for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) vs[j] = vv[(uint64_t)q * N + j];
     for (uint32_t c = threadIdx.x; c < tn; c += blockDim.x) tl[c] = t_ent[(uint64_t)q * N + c];
@@ -542,48 +572,77 @@ decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ 
     const uint64_t per = (qrows + gridDim.x - 1) / gridDim.x;
     const uint64_t v_begin = (uint64_t)blockIdx.x * per;
     const uint64_t v_end = min(qrows, v_begin + per);
+    const bool one_seg = dq.nseg == 1;
 
-    for (uint64_t tile = v_begin; tile < v_end; tile += DT_THREADS) {
-        const uint64_t vrow = tile + threadIdx.x;
-        const bool valid = vrow < v_end;
-        int64_t score = 0;
-        uint32_t id = 0;
-        if (valid) {
-            const uint64_t ridx = rbase + vrow;
-            const uint32_t sidx = find_query_seg(segs, dq.seg0, dq.nseg, ridx);
-            const ScanSeg sg = segs[sidx];
-            const uint64_t grow = sg.row0 + (ridx - sg.out0);
-            // M v' = AL G + M T
-            const uint64_t al_g = cm_dot(al_cm, total_rows, grow, gl, n1);
+    for (uint64_t tile = v_begin; tile < v_end; tile += 2 * DT_THREADS) {
+        uint64_t vrow[2], grow[2], ridx[2];
+        bool valid[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            vrow[h] = tile + threadIdx.x + (uint64_t)h * DT_THREADS;
+            valid[h] = vrow[h] < v_end;
+            ridx[h] = rbase + (valid[h] ? vrow[h] : v_begin);
+            const ScanSeg sg = segs[one_seg ? dq.seg0 : find_query_seg(segs, dq.seg0, dq.nseg, ridx[h])];
+            grow[h] = sg.row0 + (ridx[h] - sg.out0);
+        }
+        uint64_t al_g0 = 0, al_g1 = 0, h_x0 = 0, h_x1 = 0;
+        if (valid[0]) {
+            cm_dot2(al_cm, total_rows, grow[0], grow[1], valid[1], gl, n1, al_g0, al_g1);
+            cm_dot2(h_cm, total_rows, grow[0], grow[1], valid[1], xl, n1, h_x0, h_x1);
+        }
+        int64_t score[2] = {0, 0};
+        uint32_t id[2] = {0, 0};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (!valid[h]) continue;
+            const uint64_t gr = grow[h];
+            // M T: signed column sums, lazily folded
             uint64_t m_t = 0;
-#pragma unroll 4
-            for (uint32_t c = 0; c < tn; ++c) {
+            uint32_t c = 0;
+            for (; c + 3 <= tn; c += 3) {
+                const uint32_t e0 = tl[c], e1 = tl[c + 1], e2 = tl[c + 2];
+                const uint64_t x0 = __ldg(mp_cm + (uint64_t)(e0 & 0x3ffu) * total_rows + gr);
+                const uint64_t x1 = __ldg(mp_cm + (uint64_t)(e1 & 0x3ffu) * total_rows + gr);
+                const uint64_t x2 = __ldg(mp_cm + (uint64_t)(e2 & 0x3ffu) * total_rows + gr);
+                m_t = fold(m_t) + signed_term(x0, e0 >> 31) + signed_term(x1, e1 >> 31) + signed_term(x2, e2 >> 31);
+            }
+            for (; c < tn; ++c) {
                 const uint32_t e = tl[c];
-                const uint64_t x = __ldg(mp_cm + (uint64_t)(e & 0x3ffu) * total_rows + grow);
-                m_t = (e >> 31) ? sub_mod(m_t, x) : add_mod(m_t, x);
+                m_t = fold(m_t) + signed_term(__ldg(mp_cm + (uint64_t)(e & 0x3ffu) * total_rows + gr), e >> 31);
             }
-            // M' v_enc = H (L^T v_enc) + S v_enc
-            const uint64_t h_x = cm_dot(h_cm, total_rows, grow, xl, n1);
-            const uint64_t slice = grow >> 5;
-            const uint32_t sl = (uint32_t)(grow & 31);
-            const uint32_t off = s_off[slice], wdt = s_w[slice];
+            m_t = canon(m_t);
+            // S v_enc over this row's sliced-ELL entries
+            const uint64_t slice = gr >> 5;
+            const uint32_t sl = (uint32_t)(gr & 31), off = s_off[slice], wdt = s_w[slice];
             uint64_t s_v = 0;
-#pragma unroll 4
-            for (uint32_t c = 0; c < wdt; ++c) {
-                const uint16_t e = __ldg(s_ell + off + (uint64_t)c * 32 + sl);
-                if (e != 0xffffu) s_v = (e & 0x8000u) ? sub_mod(s_v, vs[e & 0x3ffu]) : add_mod(s_v, vs[e & 0x3ffu]);
+            uint32_t cc = 0;
+            for (; cc + 3 <= wdt; cc += 3) {
+                const uint16_t f0 = __ldg(s_ell + off + (uint64_t)cc * 32 + sl);
+                const uint16_t f1 = __ldg(s_ell + off + (uint64_t)(cc + 1) * 32 + sl);
+                const uint16_t f2 = __ldg(s_ell + off + (uint64_t)(cc + 2) * 32 + sl);
+                const uint64_t y0 = f0 == 0xffffu ? 0 : signed_term(vs[f0 & 0x3ffu], f0 & 0x8000u);
+                const uint64_t y1 = f1 == 0xffffu ? 0 : signed_term(vs[f1 & 0x3ffu], f1 & 0x8000u);
+                const uint64_t y2 = f2 == 0xffffu ? 0 : signed_term(vs[f2 & 0x3ffu], f2 & 0x8000u);
+                s_v = fold(s_v) + y0 + y1 + y2;
             }
-            const uint64_t mv = sub_mod(sub_mod(r[ridx], add_mod(al_g, m_t)), add_mod(h_x, s_v));
-            if (mv_out) mv_out[ridx] = mv;
-            score = to_signed(mv);
-            id = ids ? ids[grow] : (uint32_t)grow;
+            for (; cc < wdt; ++cc) {
+                const uint16_t f = __ldg(s_ell + off + (uint64_t)cc * 32 + sl);
+                s_v = fold(s_v) + (f == 0xffffu ? 0 : signed_term(vs[f & 0x3ffu], f & 0x8000u));
+            }
+            s_v = canon(s_v);
+            const uint64_t alg = h ? al_g1 : al_g0, hx = h ? h_x1 : h_x0;
+            const uint64_t mv = sub_mod(sub_mod(r[ridx[h]], add_mod(alg, m_t)), add_mod(hx, s_v));
+            if (mv_out) mv_out[ridx[h]] = mv;
+            score[h] = to_signed(mv);
+            id[h] = ids ? ids[gr] : (uint32_t)gr;
         }
         const int64_t ts = buf.thr_s;
         const uint32_t ti = buf.thr_i;
         const int ht = buf.have_thr;
-        topk_offer(buf, valid, score, id, ts, ti, ht);
+        topk_offer(buf, valid[0], score[0], id[0], ts, ti, ht);
+        topk_offer(buf, valid[1], score[1], id[1], ts, ti, ht);
         __syncthreads();
-        if (buf.cnt > CAND_CAP - DT_THREADS) topk_compact(buf, (int)k);
+        if (buf.cnt > CAND_CAP - 2 * DT_THREADS) topk_compact(buf, (int)k);
     }
     topk_compact(buf, (int)k);
     const int keep = min(buf.cnt, (int)k);
@@ -826,11 +885,11 @@ void launch_decode_topk(const uint64_t* d_r, const uint64_t* d_al_cm, const uint
                         cudaStream_t s) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(decode_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 6 * 4 * 512);
+        cudaFuncSetAttribute(decode_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 32 * 512);
         attr_set = true;
     }
     dim3 grid(ctas_per_query, nq);
-    decode_topk_kernel<<<grid, DT_THREADS, 2 * 6 * 4 * n1, s>>>(d_r, d_al_cm, d_h_cm, d_mp_cm, d_s_ell, d_s_off, d_s_w, d_ids,
+    decode_topk_kernel<<<grid, DT_THREADS, 2 * 32 * n1, s>>>(d_r, d_al_cm, d_h_cm, d_mp_cm, d_s_ell, d_s_off, d_s_w, d_ids,
                                                    total_rows, n1, d_segs, d_q, d_v, d_g, d_x, d_t, d_t_nnz, k,
                                                    scratch.cand_s, scratch.cand_i, scratch.cand_n, d_mv_out);
     topk_merge_kernel<<<nq, DT_THREADS, 0, s>>>(scratch.cand_s, scratch.cand_i, scratch.cand_n, ctas_per_query, k,

@@ -135,7 +135,8 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
         }
         reinterpret_cast<uint4*>(dst + (uint64_t)row * TC_ROWS)[ch] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
     }
-    // u_t . r over this block's rows
+    // u_t . r over this block's rows (skipped when r is not known yet)
+    if (!r) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (uint32_t tl = warp; tl < t_cnt; tl += blockDim.x / 32) {
         uint64_t acc = 0;
@@ -322,6 +323,286 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
     }
 }
 
+// ------------------------------------------------------------------ fused scan + Protocol 2
+// Same pipeline as tc_freivalds_kernel, plus six scan warps that read each
+// shared-memory stage too: for the stage's 128 rows and the group's S strips
+// (16 u64 columns per strip) they form the partial dot products with the
+// query on the CUDA cores, so r = M_enc v comes out of the same single read
+// of M_enc as z = U^T M_enc.  A stage is recycled only after the MMA commit
+// and all six scan warps have released it.  r partials land per strip group
+// in r_part[group][r index]; tc_rreduce_kernel sums them.
+constexpr int FU_SCAN_WARPS = 6;
+constexpr int FU_THREADS = TC_THREADS + 32 * FU_SCAN_WARPS;  // 384
+
+template <int S>
+__global__ void __launch_bounds__(FU_THREADS, 1)
+tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constant__ CUtensorMap tmap_u,
+                const TcPanel* __restrict__ panels, uint32_t npanels, const VerifySeg* __restrict__ vsegs,
+                const QLimb* __restrict__ qlimbs, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
+                uint32_t stages, uint32_t stage_bytes, uint64_t* __restrict__ z_part, uint64_t* __restrict__ r_part,
+                uint64_t r_stride, uint32_t* __restrict__ err) {
+    extern __shared__ uint8_t tc_dyn[];
+    __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b;
+    __shared__ uint64_t red[S][TC_ROWS];
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+    __shared__ volatile int scan_stop;
+
+    const uint32_t base = (su32(tc_dyn) + 1023u) & ~1023u;
+    uint8_t* ring = tc_dyn + (base - su32(tc_dyn));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t u_off = S * STRIP_BYTES;
+    const uint32_t u_bytes = n_rows * TC_ROWS;
+    const uint32_t groups = (64 + S - 1) / S;
+    const uint32_t items = npanels * groups;
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < stages; ++s) {
+            bar_init(&full_b[s], 1);
+            bar_init(&empty_b[s], 1 + FU_SCAN_WARPS);
+        }
+        bar_init(&accf_b, 1);
+        bar_init(&acce_b, 4);
+        bar_init(&done_b, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_s)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tmem = tmem_base_s;
+
+    if (warp == 0) {
+        if (lane == 0) {  // ------------------------------------------ TMA producer
+            uint64_t it = 0;
+            bool stop = false;
+            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
+                const uint32_t p = item / groups, g = item % groups;
+                const TcPanel pn = panels[p];
+                const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
+                const uint32_t sg = min((uint32_t)S, 64u - g * S);
+                for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
+                    const uint32_t st = (uint32_t)(it % stages);
+                    if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1))) {
+                        abort_s = 1;
+                        atomicOr(err, 4u);
+                        stop = true;
+                        break;
+                    }
+                    if (abort_s) { stop = true; break; }
+                    uint8_t* sb = ring + (uint64_t)st * stage_bytes;
+                    bar_expect_tx(&full_b[st], sg * STRIP_BYTES + u_bytes);
+                    for (uint32_t s = 0; s < sg; ++s)
+                        tma_2d(sb + s * STRIP_BYTES, &tmap_m, (int)((g * S + s) * 128), (int)(pn.row0 + rb * TC_ROWS),
+                               &full_b[st]);
+                    tma_2d(sb + u_off, &tmap_u, 0, (int)((pn.rb0 + rb) * n_rows), &full_b[st]);
+                }
+            }
+            for (uint64_t j = it > stages ? it - stages : 0; j < it; ++j)
+                bar_wait(&full_b[j % stages], (uint32_t)((j / stages) & 1));
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // ------------------------------------------ MMA issuer
+            const uint32_t idesc = (2u << 4) | (1u << 15) | ((n_rows >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+            uint64_t it = 0, gc = 0;
+            bool stop = false;
+            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x, ++gc) {
+                const uint32_t p = item / groups, g = item % groups;
+                const TcPanel pn = panels[p];
+                const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
+                const uint32_t sg = min((uint32_t)S, 64u - g * S);
+                if (gc > 0 && !bar_wait(&acce_b, (uint32_t)((gc - 1) & 1))) {
+                    abort_s = 1;
+                    atomicOr(err, 8u);
+                    break;
+                }
+                tc_after();
+                for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
+                    const uint32_t st = (uint32_t)(it % stages);
+                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
+                        abort_s = 1;
+                        atomicOr(err, 8u);
+                        stop = true;
+                        break;
+                    }
+                    tc_after();
+                    const uint32_t sb = base + st * stage_bytes;
+                    for (uint32_t s = 0; s < sg; ++s)
+#pragma unroll
+                        for (uint32_t ks = 0; ks < TC_ROWS / 32; ++ks) {
+                            const uint64_t a = sdesc(sb + s * STRIP_BYTES + ks * 4096u, STRIP_BYTES, 1024);
+                            const uint64_t b = sdesc(sb + u_off + ks * 32u, 16, 1024);
+                            mma_i8(tmem + s * n_rows, a, b, idesc, (rb | ks) != 0);
+                        }
+                    mma_commit(&empty_b[st]);
+                }
+                if (stop) break;
+                mma_commit(&accf_b);
+            }
+            mma_commit(&done_b);
+            bar_wait(&done_b, 0);
+        }
+    } else if (warp < 6) {
+        // ---------------------------------------------------------- TMEM epilogue (z)
+        const uint32_t q = (uint32_t)(warp & 3);
+        const uint32_t lane_c = q * 32 + lane;
+        const uint32_t jl = lane_c >> 3, a = lane_c & 7;
+        const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+        uint64_t gc = 0;
+        for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, ++gc) {
+            const uint32_t p = item / groups, g = item % groups;
+            const uint32_t sg = min((uint32_t)S, 64u - g * S);
+            const bool ok = bar_wait(&accf_b, (uint32_t)(gc & 1));
+            if (!ok) { abort_s = 1; atomicOr(err, 16u); }
+            __syncwarp();
+            if (!ok || abort_s) break;
+            tc_after();
+            for (uint32_t s = 0; s < sg; ++s) {
+                const uint32_t j = (g * S + s) * 16 + jl;
+                for (uint32_t c0 = 0; c0 < n_rows; c0 += 16) {
+                    uint32_t v[16];
+                    tmem_ld16(tmem + ((q * 32) << 16) + s * n_rows + c0, v);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t t = c0 / 8 + h;
+                        uint64_t lo = 0, hi = 0;
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            lo += (uint64_t)v[8 * h + b] << (8 * b);
+                            hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
+                        }
+                        uint64_t zc = canon(rotl61(lo, w1) + rotl61(hi, w2));
+                        zc += __shfl_xor_sync(FULLMASK, zc, 1);
+                        zc += __shfl_xor_sync(FULLMASK, zc, 2);
+                        zc += __shfl_xor_sync(FULLMASK, zc, 4);
+                        if (a == 0 && t < t_cnt) z_part[((uint64_t)p * trials_total + t) * N + j] = canon(zc);
+                    }
+                }
+            }
+            tc_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(&acce_b);
+        }
+    } else {
+        // ---------------------------------------------------------- scan warps (r)
+        const uint32_t sw = (uint32_t)(warp - 6);
+        // S = 3: six warps = 3 strips x 2 halves of 64 rows; S = 4: warps 0-3
+        // take one strip of 128 rows each, warps 4-5 only keep the barrier count.
+        const uint32_t my_s = S == 3 ? sw % 3 : sw, half = S == 3 ? sw / 3 : 0;
+        const uint32_t rows_per_warp = S == 3 ? 64 : 128;
+        uint32_t lb0[16], lb1[16], lb2[16], lc0[16], lc1[16], lc2[16];
+        uint64_t it = 0;
+        bool stop = false;
+        for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
+            const uint32_t p = item / groups, g = item % groups;
+            const TcPanel pn = panels[p];
+            const VerifySeg vs = vsegs[pn.seg];
+            const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
+            const uint32_t sg = min((uint32_t)S, 64u - g * S);
+            const uint64_t r0 = vs.r0 + (pn.row0 - vs.row0);  // r index of the panel's first row
+            const bool active = my_s < sg;
+            if (active) {
+                const QLimb* ql = qlimbs + (uint64_t)vs.query * N + (g * S + my_s) * 16;
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const QLimb l = ql[e];
+                    lb0[e] = l.b0; lb1[e] = l.b1; lb2[e] = l.b2; lc0[e] = l.c0; lc1[e] = l.c1; lc2[e] = l.c2;
+                }
+            }
+            for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
+                const uint32_t st = (uint32_t)(it % stages);
+                const bool ok = bar_wait(&full_b[st], (uint32_t)((it / stages) & 1));
+                if (!ok) { abort_s = 1; atomicOr(err, 32u); }
+                if (ok && active) {
+                    const uint8_t* box = ring + (uint64_t)st * stage_bytes + my_s * STRIP_BYTES;
+                    for (uint32_t rr = half * rows_per_warp + lane; rr < (half + 1) * rows_per_warp; rr += 32) {
+                        uint64_t a0 = 0, a1 = 0, a2 = 0;
+                        const uint8_t* row = box + rr * 128;
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) {  // 16-byte chunk c holds elements 2c, 2c+1
+                            const uint4 x = *reinterpret_cast<const uint4*>(row + ((c ^ (rr & 7)) << 4));
+                            a0 = mac(mac(a0, x.x, lb0[2 * c]), x.y, lc0[2 * c]);
+                            a1 = mac(mac(a1, x.x, lb1[2 * c]), x.y, lc1[2 * c]);
+                            a2 = mac(mac(a2, x.x, lb2[2 * c]), x.y, lc2[2 * c]);
+                            a0 = mac(mac(a0, x.z, lb0[2 * c + 1]), x.w, lc0[2 * c + 1]);
+                            a1 = mac(mac(a1, x.z, lb1[2 * c + 1]), x.w, lc1[2 * c + 1]);
+                            a2 = mac(mac(a2, x.z, lb2[2 * c + 1]), x.w, lc2[2 * c + 1]);
+                        }
+                        red[my_s][rr] = combine3(a0, a1, a2);
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) bar_arrive(&empty_b[st]);
+                // combine the group's strips for this stage's rows; the stop
+                // decision is a snapshot taken before the barrier, so all six
+                // warps see the same value and leave together
+                if (sw == 0 && lane == 0) scan_stop = abort_s;
+                asm volatile("bar.sync 1, %0;" ::"r"(32 * FU_SCAN_WARPS) : "memory");
+                if (scan_stop) { stop = true; break; }
+                for (uint32_t rr = sw * 32 + lane; rr < TC_ROWS; rr += 32 * FU_SCAN_WARPS) {
+                    const uint32_t lr = rb * TC_ROWS + rr;
+                    if (lr < pn.rows) {
+                        uint64_t acc = 0;
+                        for (uint32_t s = 0; s < sg; ++s) acc = add_mod(acc, red[s][rr]);
+                        r_part[(uint64_t)g * r_stride + r0 + lr] = acc;
+                    }
+                }
+                asm volatile("bar.sync 1, %0;" ::"r"(32 * FU_SCAN_WARPS) : "memory");
+            }
+        }
+    }
+    tc_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+    }
+}
+
+// r[i] = sum over strip groups of r_part, then u_t . r for this pass's draws
+// rebuilt from their byte image (one CTA per 128-row block).
+__global__ void __launch_bounds__(TC_ROWS)
+tc_rreduce_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ blocks,
+                  const uint64_t* __restrict__ r_part, uint64_t r_stride, uint32_t groups,
+                  const uint8_t* __restrict__ u_img, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
+                  uint64_t* __restrict__ r, uint64_t* __restrict__ ur_part) {
+    const uint32_t blk = blockIdx.x;
+    const TcBlock tb = blocks[blk];
+    const VerifySeg vs = vsegs[tb.seg];
+    const uint32_t i = threadIdx.x;
+    const bool valid = tb.i0 + i < vs.rows;
+    const uint64_t ri = vs.r0 + tb.i0 + i;
+    uint64_t rv = 0;
+    if (valid) {
+        for (uint32_t g = 0; g < groups; ++g) rv = add_mod(rv, r_part[(uint64_t)g * r_stride + ri]);
+        r[ri] = rv;
+    }
+    __shared__ uint64_t sh[TC_ROWS / 32];
+    const uint8_t* img = u_img + (uint64_t)blk * n_rows * TC_ROWS;
+    for (uint32_t t = 0; t < t_cnt; ++t) {
+        uint64_t u = 0;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) u |= (uint64_t)img[(uint64_t)(8 * t + b) * TC_ROWS + i] << (8 * b);
+        uint64_t part = valid ? mul_mod(u, rv) : 0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) part = add_mod(part, __shfl_xor_sync(FULLMASK, part, off));
+        __syncthreads();
+        if ((i & 31) == 0) sh[i >> 5] = part;
+        __syncthreads();
+        if (i == 0) {
+            uint64_t tot = 0;
+            for (int w = 0; w < TC_ROWS / 32; ++w) tot = add_mod(tot, sh[w]);
+            ur_part[(uint64_t)blk * trials_total + t] = tot;
+        }
+    }
+}
+
 __device__ __forceinline__ uint64_t block_sum_mod256(uint64_t v, uint64_t* sh) {
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) v = add_mod(v, __shfl_xor_sync(FULLMASK, v, off));
@@ -422,6 +703,39 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
         tc_freivalds_kernel<3><<<grid, TC_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, t_base, t_cnt, n_rows,
                                                               trials_total, stages, stage_bytes, d_z_part, d_err);
     }
+}
+
+void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels, uint32_t npanels,
+                     const VerifySeg* d_vsegs, const QLimb* d_limbs, uint32_t t_cnt, uint32_t n_rows,
+                     uint32_t trials_total, uint64_t* d_z_part, uint64_t* d_r_part, uint64_t r_stride,
+                     uint32_t* d_err, int num_sms, cudaStream_t s) {
+    if (!npanels) return;
+    const int S = n_rows <= 128 ? 4 : 3;
+    const uint32_t stage_bytes = (uint32_t)S * STRIP_BYTES + ((n_rows * TC_ROWS + 1023u) & ~1023u);
+    uint32_t stages = (216u * 1024u) / stage_bytes;
+    stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
+    const int smem = (int)(stages * stage_bytes + 1024);
+    const uint32_t items = npanels * ((64 + S - 1) / S);
+    const unsigned grid = items < (uint32_t)num_sms ? items : (unsigned)num_sms;
+    if (S == 4) {
+        cudaFuncSetAttribute(tc_fused_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        tc_fused_kernel<4><<<grid, FU_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, d_vsegs, d_limbs, t_cnt,
+                                                          n_rows, trials_total, stages, stage_bytes, d_z_part, d_r_part,
+                                                          r_stride, d_err);
+    } else {
+        cudaFuncSetAttribute(tc_fused_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        tc_fused_kernel<3><<<grid, FU_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, d_vsegs, d_limbs, t_cnt,
+                                                          n_rows, trials_total, stages, stage_bytes, d_z_part, d_r_part,
+                                                          r_stride, d_err);
+    }
+}
+
+void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const uint64_t* d_r_part,
+                       uint64_t r_stride, uint32_t groups, const uint8_t* d_u, uint32_t t_cnt, uint32_t n_rows,
+                       uint32_t trials_total, uint64_t* d_r, uint64_t* d_ur_part, cudaStream_t s) {
+    if (!nblocks) return;
+    tc_rreduce_kernel<<<nblocks, TC_ROWS, 0, s>>>(d_vsegs, d_blocks, d_r_part, r_stride, groups, d_u, t_cnt, n_rows,
+                                                  trials_total, d_r, d_ur_part);
 }
 
 void launch_tc_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint32_t* d_seg_panel0,

@@ -60,6 +60,21 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
                          uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
                          uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s);
 
+// Fused single pass over m_enc for the first <= 20 trials: z_part as above
+// plus r_part[group][r index] (S-strip group partial dots with the query,
+// r_stride = total r entries, groups = ceil(64 / S) with S = 4 when
+// n_rows <= 128 else 3), to be summed by launch_tc_rreduce.
+void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels, uint32_t npanels,
+                     const VerifySeg* d_vsegs, const QLimb* d_limbs, uint32_t t_cnt, uint32_t n_rows,
+                     uint32_t trials_total, uint64_t* d_z_part, uint64_t* d_r_part, uint64_t r_stride,
+                     uint32_t* d_err, int num_sms, cudaStream_t s);
+inline uint32_t tc_groups(uint32_t n_rows) { return n_rows <= 128 ? 16u : 22u; }
+// r = sum of the group partials, and u_t . r partials for the pass's trials
+// from the U byte image.
+void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const uint64_t* d_r_part,
+                       uint64_t r_stride, uint32_t groups, const uint8_t* d_u, uint32_t t_cnt, uint32_t n_rows,
+                       uint32_t trials_total, uint64_t* d_r, uint64_t* d_ur_part, cudaStream_t s);
+
 // Per segment: z_t = sum of its panels' partials, zv_t = z_t . v, ur_t =
 // sum of its blocks' partials; failed = first t with ur_t != zv_t or -1.
 void launch_tc_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint32_t* d_seg_panel0,
