@@ -376,6 +376,7 @@ struct Scratch {  // device pointers
     uint32_t* err;  // device pipeline timeout flags
     uint8_t* u_buf;
     uint64_t* r_part;  // fused pass: per strip-group partial dots
+    uint64_t* zv_chunks;
 };
 struct Inputs {
     const uint64_t* v;
@@ -446,7 +447,7 @@ struct Sizes {
 
 int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms) {
     uint64_t by_rows = (max_rows_per_query + 255) / 256;
-    uint64_t by_sms = std::max<uint64_t>(1, (uint64_t)sms * 8 / std::max<uint32_t>(B, 1));
+    uint64_t by_sms = std::max<uint64_t>(1, (uint64_t)sms * 4 / std::max<uint32_t>(B, 1));
     return (int)std::max<uint64_t>(1, std::min(by_rows, by_sms));
 }
 
@@ -457,7 +458,7 @@ struct RunLayout {
     // outputs (contiguous -> one D2H)
     uint64_t ids, scores, n, vfailed, ur, zv, err, out_begin, out_end;
     // internal
-    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, r_part, total;
+    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, r_part, zv_chunks, total;
 };
 
 RunLayout make_layout(const Sizes& z, bool want_mv) {
@@ -505,6 +506,7 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
                    ? L.take<uint64_t>((uint64_t)tc_groups(pass_rows(std::min<uint32_t>(TC_MAX_TRIALS, z.trials))) *
                                       std::max<uint64_t>(z.total_out, 1))
                    : 0;
+    o.zv_chunks = L.take<uint64_t>(std::max<uint64_t>(z.nvseg * z.trials * 8, 1));
     o.total = L.off + 1024;
     return o;
 }
@@ -545,7 +547,7 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
             }
         }
         launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, in.v, m.vsegs, m.nvseg, z.trials, sc.ur,
-                         sc.zv, out.vfailed, s);
+                         sc.zv, sc.zv_chunks, out.vfailed, s);
     } else {
         launch_scan(c.m_enc.at<uint64_t>(), sc.limbs, m.segs, m.seg_blk, m.nseg, m.total_blocks, sc.r, ctx->num_sms,
                     sc.err, s);
@@ -588,7 +590,7 @@ Scratch scratch_at(char* d, const RunLayout& o) {
                    TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
                                reinterpret_cast<uint32_t*>(d + o.cand_n)},
                    reinterpret_cast<uint32_t*>(d + o.err), reinterpret_cast<uint8_t*>(d + o.u_buf),
-                   reinterpret_cast<uint64_t*>(d + o.r_part)};
+                   reinterpret_cast<uint64_t*>(d + o.r_part), reinterpret_cast<uint64_t*>(d + o.zv_chunks)};
 }
 void pack_meta(char* h, const RunLayout& o, const HostMeta& hm) {
     memcpy(h + o.segs, hm.segs.data(), hm.segs.size() * sizeof(ScanSeg));
@@ -776,8 +778,8 @@ int run_verify(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* r, const
             launch_tc_freivalds(e.c.tmap_m, maps.u[ps], m.tc_panels, m.npanels, t0, tc, nr, trials, sc.z_part, sc.err,
                                 e.ctx->num_sms, e.stream);
         }
-        launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, dv, m.vsegs, 1, trials, sc.ur, sc.zv, dfail,
-                         e.stream);
+        launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, dv, m.vsegs, 1, trials, sc.ur, sc.zv,
+                         sc.zv_chunks, dfail, e.stream);
     } else {
         launch_freivalds(e.c.m_enc.at<uint64_t>(), sc.r, m.vsegs, 1, keys, trials, z.fp, sc.z_part, sc.ur_part, sc.flags,
                          e.stream);

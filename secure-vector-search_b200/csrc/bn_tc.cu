@@ -85,7 +85,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 }
 
 // ------------------------------------------------------------------ u draws
-constexpr int UG_THREADS = 256;
+constexpr int UG_THREADS = 352;  // >= 20 trials x 17 keystream blocks: one block per thread
+constexpr int UG_PAD = TC_ROWS + TC_ROWS / 16;  // one pad word per 16 keeps lanes off shared banks
+__device__ __forceinline__ uint32_t ug_idx(uint32_t i) { return i + (i >> 4); }
 
 __global__ void __launch_bounds__(UG_THREADS)
 tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ blocks, const ChaChaKey* __restrict__ keys,
@@ -97,7 +99,7 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
     const VerifySeg vs = vsegs[tb.seg];
     const uint32_t here = min((uint32_t)TC_ROWS, vs.rows - tb.i0);
     const ChaChaKey key = keys[vs.query];
-    __shared__ uint64_t us[TC_MAX_TRIALS][TC_ROWS];
+    __shared__ uint64_t us[TC_MAX_TRIALS][UG_PAD];
 
     // draws: 128 consecutive indices per trial span at most 17 keystream blocks
     for (uint32_t item = threadIdx.x; item < t_cnt * 17; item += blockDim.x) {
@@ -115,32 +117,38 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
                 uint64_t x = ((uint64_t)w[2 * q] | ((uint64_t)w[2 * q + 1] << 32)) & P;
                 if (ii >= here) x = 0;  // rows past the segment end
                 else if (x == P) { atomicOr(flags, 1u); x = 0; }
-                us[tl][ii] = x;
+                us[tl][ug_idx(ii)] = x;
             }
         }
     }
     __syncthreads();
-    // U tile image: row (t, b) holds byte b of u_t[i] for the 128 rows i
+    // U tile image: row (t, b) holds byte b of u_t[i] for the 128 rows i.
+    // Thread (t, chunk) reads its 16 draws once and writes all 8 byte rows.
     uint8_t* dst = u_out + (uint64_t)blk * n_rows * TC_ROWS;
-    for (uint32_t c = threadIdx.x; c < n_rows * (TC_ROWS / 16); c += blockDim.x) {
-        const uint32_t row = c / (TC_ROWS / 16), ch = c % (TC_ROWS / 16);
-        const uint32_t tl = row / 8, b = row % 8;
-        uint32_t wv[4] = {0, 0, 0, 0};
-        if (tl < t_cnt) {
+    for (uint32_t c = threadIdx.x; c < t_cnt * (TC_ROWS / 16); c += blockDim.x) {
+        const uint32_t tl = c / (TC_ROWS / 16), ch = c % (TC_ROWS / 16);
+        uint64_t x[16];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                const uint32_t byte = (uint32_t)(us[tl][ch * 16 + q] >> (8 * b)) & 0xffu;
-                wv[q >> 2] |= byte << (8 * (q & 3));
-            }
+        for (int q = 0; q < 16; ++q) x[q] = us[tl][ug_idx(ch * 16 + q)];
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            uint32_t wv[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int q = 0; q < 16; ++q) wv[q >> 2] |= (uint32_t)((x[q] >> (8 * b)) & 0xffu) << (8 * (q & 3));
+            reinterpret_cast<uint4*>(dst + (uint64_t)(tl * 8 + b) * TC_ROWS)[ch] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
         }
-        reinterpret_cast<uint4*>(dst + (uint64_t)row * TC_ROWS)[ch] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+    }
+    for (uint32_t c = threadIdx.x; c < (n_rows - 8 * t_cnt) * (TC_ROWS / 16); c += blockDim.x) {  // zero pad rows
+        const uint32_t row = 8 * t_cnt + c / (TC_ROWS / 16), ch = c % (TC_ROWS / 16);
+        reinterpret_cast<uint4*>(dst + (uint64_t)row * TC_ROWS)[ch] = make_uint4(0, 0, 0, 0);
     }
     // u_t . r over this block's rows (skipped when r is not known yet)
     if (!r) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (uint32_t tl = warp; tl < t_cnt; tl += blockDim.x / 32) {
         uint64_t acc = 0;
-        for (uint32_t ii = lane; ii < here; ii += 32) acc = add_mod(acc, mul_mod(us[tl][ii], r[vs.r0 + tb.i0 + ii]));
+        for (uint32_t ii = lane; ii < here; ii += 32)
+            acc = add_mod(acc, mul_mod(us[tl][ug_idx(ii)], r[vs.r0 + tb.i0 + ii]));
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) acc = add_mod(acc, __shfl_xor_sync(FULLMASK, acc, off));
         if (lane == 0) ur_part[(uint64_t)blk * trials_total + t_base + tl] = acc;
@@ -281,10 +289,9 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
             const uint32_t p = item / groups, g = item % groups;
             {
                 const uint32_t sg = min((uint32_t)S, 64u - g * S);
-                const bool ok = bar_wait(&accf_b, (uint32_t)(gc & 1));
-                if (!ok) { abort_s = 1; atomicOr(err, 16u); }
-                __syncwarp();
-                if (!ok || abort_s) { stop = true; break; }
+                const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b, (uint32_t)(gc & 1)));  // warp-uniform
+                if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
+                if (__any_sync(FULLMASK, !ok || abort_s)) { stop = true; break; }
                 tc_after();
                 for (uint32_t s = 0; s < sg; ++s) {
                     const uint32_t j = (g * S + s) * 16 + jl;
@@ -331,8 +338,8 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
 // of M_enc as z = U^T M_enc.  A stage is recycled only after the MMA commit
 // and all six scan warps have released it.  r partials land per strip group
 // in r_part[group][r index]; tc_rreduce_kernel sums them.
-constexpr int FU_SCAN_WARPS = 6;
-constexpr int FU_THREADS = TC_THREADS + 32 * FU_SCAN_WARPS;  // 384
+constexpr int FU_SCAN_WARPS = 4;
+constexpr int FU_THREADS = TC_THREADS + 32 * FU_SCAN_WARPS;  // 320
 
 template <int S>
 __global__ void __launch_bounds__(FU_THREADS, 1)
@@ -343,7 +350,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 uint64_t r_stride, uint32_t* __restrict__ err) {
     extern __shared__ uint8_t tc_dyn[];
     __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b;
-    __shared__ uint64_t red[S][TC_ROWS];
+    __shared__ QLimb qsm[64];  // the current strip group's query limbs (scan warps)
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
     __shared__ volatile int scan_stop;
@@ -458,10 +465,9 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
         for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, ++gc) {
             const uint32_t p = item / groups, g = item % groups;
             const uint32_t sg = min((uint32_t)S, 64u - g * S);
-            const bool ok = bar_wait(&accf_b, (uint32_t)(gc & 1));
-            if (!ok) { abort_s = 1; atomicOr(err, 16u); }
-            __syncwarp();
-            if (!ok || abort_s) break;
+            const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b, (uint32_t)(gc & 1)));  // warp-uniform
+            if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
+            if (__any_sync(FULLMASK, !ok || abort_s)) break;
             tc_after();
             for (uint32_t s = 0; s < sg; ++s) {
                 const uint32_t j = (g * S + s) * 16 + jl;
@@ -491,69 +497,59 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
         }
     } else {
         // ---------------------------------------------------------- scan warps (r)
+        // Four warps, one lane per stage row: lane reads its row's S strips
+        // (16 u64 each, 128-byte swizzled) and dots them with the group's
+        // query limbs, broadcast from shared memory.  No barrier per stage:
+        // each lane writes its row's partial for this strip group directly.
         const uint32_t sw = (uint32_t)(warp - 6);
-        // S = 3: six warps = 3 strips x 2 halves of 64 rows; S = 4: warps 0-3
-        // take one strip of 128 rows each, warps 4-5 only keep the barrier count.
-        const uint32_t my_s = S == 3 ? sw % 3 : sw, half = S == 3 ? sw / 3 : 0;
-        const uint32_t rows_per_warp = S == 3 ? 64 : 128;
-        uint32_t lb0[16], lb1[16], lb2[16], lc0[16], lc1[16], lc2[16];
         uint64_t it = 0;
-        bool stop = false;
-        for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
+        for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
             const uint32_t p = item / groups, g = item % groups;
             const TcPanel pn = panels[p];
             const VerifySeg vs = vsegs[pn.seg];
             const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
             const uint32_t sg = min((uint32_t)S, 64u - g * S);
             const uint64_t r0 = vs.r0 + (pn.row0 - vs.row0);  // r index of the panel's first row
-            const bool active = my_s < sg;
-            if (active) {
-                const QLimb* ql = qlimbs + (uint64_t)vs.query * N + (g * S + my_s) * 16;
-#pragma unroll
-                for (int e = 0; e < 16; ++e) {
-                    const QLimb l = ql[e];
-                    lb0[e] = l.b0; lb1[e] = l.b1; lb2[e] = l.b2; lc0[e] = l.c0; lc1[e] = l.c1; lc2[e] = l.c2;
-                }
-            }
+            // this group's limbs: elements (g*S + s)*16 + e, s < sg.  Barrier A
+            // also publishes the stop snapshot taken before it, so every scan
+            // warp takes the same exit decision (the next snapshot is written
+            // only after barrier B, which all warps pass after reading it).
+            if (sw == 0 && lane == 0) scan_stop = abort_s;
+            asm volatile("bar.sync 1, %0;" ::"r"(32 * FU_SCAN_WARPS) : "memory");  // A
+            if (scan_stop) break;
+            for (uint32_t e = threadIdx.x - 32 * 6; e < sg * 16; e += 32 * FU_SCAN_WARPS)
+                qsm[e] = qlimbs[(uint64_t)vs.query * N + g * S * 16 + e];
+            asm volatile("bar.sync 1, %0;" ::"r"(32 * FU_SCAN_WARPS) : "memory");  // B
             for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                 const uint32_t st = (uint32_t)(it % stages);
-                const bool ok = bar_wait(&full_b[st], (uint32_t)((it / stages) & 1));
-                if (!ok) { abort_s = 1; atomicOr(err, 32u); }
-                if (ok && active) {
-                    const uint8_t* box = ring + (uint64_t)st * stage_bytes + my_s * STRIP_BYTES;
-                    for (uint32_t rr = half * rows_per_warp + lane; rr < (half + 1) * rows_per_warp; rr += 32) {
-                        uint64_t a0 = 0, a1 = 0, a2 = 0;
-                        const uint8_t* row = box + rr * 128;
+                const bool ok = __all_sync(FULLMASK, bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)));
+                if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 32u); }
+                const uint32_t rr = sw * 32 + lane;  // stage row
+                uint64_t a0 = 0, a1 = 0, a2 = 0, e0 = 0, e1 = 0, e2 = 0;
+                if (ok) {
+                    const uint8_t* sb = ring + (uint64_t)st * stage_bytes;
+                    for (uint32_t s = 0; s < sg; ++s) {
+                        const uint8_t* row = sb + s * STRIP_BYTES + rr * 128;
+                        const QLimb* ql = qsm + s * 16;
 #pragma unroll
                         for (int c = 0; c < 8; ++c) {  // 16-byte chunk c holds elements 2c, 2c+1
                             const uint4 x = *reinterpret_cast<const uint4*>(row + ((c ^ (rr & 7)) << 4));
-                            a0 = mac(mac(a0, x.x, lb0[2 * c]), x.y, lc0[2 * c]);
-                            a1 = mac(mac(a1, x.x, lb1[2 * c]), x.y, lc1[2 * c]);
-                            a2 = mac(mac(a2, x.x, lb2[2 * c]), x.y, lc2[2 * c]);
-                            a0 = mac(mac(a0, x.z, lb0[2 * c + 1]), x.w, lc0[2 * c + 1]);
-                            a1 = mac(mac(a1, x.z, lb1[2 * c + 1]), x.w, lc1[2 * c + 1]);
-                            a2 = mac(mac(a2, x.z, lb2[2 * c + 1]), x.w, lc2[2 * c + 1]);
+                            const QLimb l0 = ql[2 * c], l1 = ql[2 * c + 1];
+                            a0 = mac(mac(a0, x.x, l0.b0), x.y, l0.c0);
+                            a1 = mac(mac(a1, x.x, l0.b1), x.y, l0.c1);
+                            a2 = mac(mac(a2, x.x, l0.b2), x.y, l0.c2);
+                            e0 = mac(mac(e0, x.z, l1.b0), x.w, l1.c0);
+                            e1 = mac(mac(e1, x.z, l1.b1), x.w, l1.c1);
+                            e2 = mac(mac(e2, x.z, l1.b2), x.w, l1.c2);
                         }
-                        red[my_s][rr] = combine3(a0, a1, a2);
                     }
                 }
                 __syncwarp();
-                if (lane == 0) bar_arrive(&empty_b[st]);
-                // combine the group's strips for this stage's rows; the stop
-                // decision is a snapshot taken before the barrier, so all six
-                // warps see the same value and leave together
-                if (sw == 0 && lane == 0) scan_stop = abort_s;
-                asm volatile("bar.sync 1, %0;" ::"r"(32 * FU_SCAN_WARPS) : "memory");
-                if (scan_stop) { stop = true; break; }
-                for (uint32_t rr = sw * 32 + lane; rr < TC_ROWS; rr += 32 * FU_SCAN_WARPS) {
-                    const uint32_t lr = rb * TC_ROWS + rr;
-                    if (lr < pn.rows) {
-                        uint64_t acc = 0;
-                        for (uint32_t s = 0; s < sg; ++s) acc = add_mod(acc, red[s][rr]);
-                        r_part[(uint64_t)g * r_stride + r0 + lr] = acc;
-                    }
-                }
-                asm volatile("bar.sync 1, %0;" ::"r"(32 * FU_SCAN_WARPS) : "memory");
+                if (lane == 0) bar_arrive(&empty_b[st]);  // this warp is done with the stage
+                if (!ok) break;  // abort_s is set; the next barrier A turns it into a uniform exit
+                const uint32_t lr = rb * TC_ROWS + rr;
+                // at most 64 elements per row and group: every accumulator < 2^59
+                if (lr < pn.rows) r_part[(uint64_t)g * r_stride + r0 + lr] = combine3(a0 + e0, a1 + e1, a2 + e2);
             }
         }
     }
@@ -583,8 +579,9 @@ tc_rreduce_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict
         for (uint32_t g = 0; g < groups; ++g) rv = add_mod(rv, r_part[(uint64_t)g * r_stride + ri]);
         r[ri] = rv;
     }
-    __shared__ uint64_t sh[TC_ROWS / 32];
+    __shared__ uint64_t sh[TC_MAX_TRIALS][TC_ROWS / 32];
     const uint8_t* img = u_img + (uint64_t)blk * n_rows * TC_ROWS;
+    const int warp = i >> 5, lane = i & 31;
     for (uint32_t t = 0; t < t_cnt; ++t) {
         uint64_t u = 0;
 #pragma unroll
@@ -592,14 +589,13 @@ tc_rreduce_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict
         uint64_t part = valid ? mul_mod(u, rv) : 0;
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) part = add_mod(part, __shfl_xor_sync(FULLMASK, part, off));
-        __syncthreads();
-        if ((i & 31) == 0) sh[i >> 5] = part;
-        __syncthreads();
-        if (i == 0) {
-            uint64_t tot = 0;
-            for (int w = 0; w < TC_ROWS / 32; ++w) tot = add_mod(tot, sh[w]);
-            ur_part[(uint64_t)blk * trials_total + t] = tot;
-        }
+        if (lane == 0) sh[t][warp] = part;
+    }
+    __syncthreads();
+    if (i < t_cnt) {
+        uint64_t tot = 0;
+        for (int w = 0; w < TC_ROWS / 32; ++w) tot = add_mod(tot, sh[i][w]);
+        ur_part[(uint64_t)blk * trials_total + i] = tot;
     }
 }
 
@@ -615,41 +611,52 @@ __device__ __forceinline__ uint64_t block_sum_mod256(uint64_t v, uint64_t* sh) {
     return t;
 }
 
-// One CTA per (trial, segment): zv = (sum over panels of z) . v, ur = sum over blocks.
-__global__ void __launch_bounds__(256)
+// CTA (trial t, y, segment): y < 8 sums z over the segment's panels for the
+// 128 columns [128y, 128y+128) and writes that chunk's share of z_t . v;
+// y == 8 sums the u_t . r partials of the segment's row blocks.
+constexpr int FIN_CHUNKS = N / 128;
+
+__global__ void __launch_bounds__(128)
 tc_finish_kernel(const uint64_t* __restrict__ z_part, const uint64_t* __restrict__ ur_part,
                  const uint32_t* __restrict__ seg_panel0, const uint32_t* __restrict__ seg_block0,
                  const uint64_t* __restrict__ v_enc, const VerifySeg* __restrict__ vsegs, uint32_t trials,
-                 uint64_t* __restrict__ ur, uint64_t* __restrict__ zv) {
-    const uint32_t t = blockIdx.x, seg = blockIdx.y;
-    const VerifySeg vs = vsegs[seg];
-    const uint64_t* v = v_enc + (uint64_t)vs.query * N;
-    const uint32_t p0 = seg_panel0[seg], p1 = seg_panel0[seg + 1];
-    const uint32_t b0 = seg_block0[seg], b1 = seg_block0[seg + 1];
-    __shared__ uint64_t sh[8];
+                 uint64_t* __restrict__ ur, uint64_t* __restrict__ zv_chunks) {
+    const uint32_t t = blockIdx.x, y = blockIdx.y, seg = blockIdx.z;
+    __shared__ uint64_t sh[4];
     uint64_t part = 0;
-    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
+    if (y < FIN_CHUNKS) {
+        const VerifySeg vs = vsegs[seg];
+        const uint32_t j = y * 128 + threadIdx.x;
+        const uint32_t p0 = seg_panel0[seg], p1 = seg_panel0[seg + 1];
         uint64_t z = 0;
         for (uint32_t p = p0; p < p1; ++p) z = add_mod(z, z_part[((uint64_t)p * trials + t) * N + j]);
-        part = add_mod(part, mul_mod(z, v[j]));
+        part = mul_mod(z, v_enc[(uint64_t)vs.query * N + j]);
+    } else {
+        const uint32_t b0 = seg_block0[seg], b1 = seg_block0[seg + 1];
+        for (uint32_t b = b0 + threadIdx.x; b < b1; b += blockDim.x) part = add_mod(part, ur_part[(uint64_t)b * trials + t]);
     }
-    const uint64_t zvt = block_sum_mod256(part, sh);
-    uint64_t u = 0;
-    for (uint32_t b = b0 + threadIdx.x; b < b1; b += blockDim.x) u = add_mod(u, ur_part[(uint64_t)b * trials + t]);
-    const uint64_t urt = block_sum_mod256(u, sh);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) part = add_mod(part, __shfl_xor_sync(FULLMASK, part, off));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = part;
+    __syncthreads();
     if (threadIdx.x == 0) {
-        ur[(uint64_t)seg * trials + t] = urt;
-        zv[(uint64_t)seg * trials + t] = zvt;
+        const uint64_t tot = add_mod(add_mod(sh[0], sh[1]), add_mod(sh[2], sh[3]));
+        if (y < FIN_CHUNKS) zv_chunks[((uint64_t)seg * trials + t) * FIN_CHUNKS + y] = tot;
+        else ur[(uint64_t)seg * trials + t] = tot;
     }
 }
 
-__global__ void tc_decide_kernel(const uint64_t* __restrict__ ur, const uint64_t* __restrict__ zv, uint32_t nseg,
-                                 uint32_t trials, int32_t* __restrict__ failed) {
+__global__ void tc_decide_kernel(const uint64_t* __restrict__ ur, const uint64_t* __restrict__ zv_chunks,
+                                 uint32_t nseg, uint32_t trials, uint64_t* __restrict__ zv, int32_t* __restrict__ failed) {
     const uint32_t seg = blockIdx.x * blockDim.x + threadIdx.x;
     if (seg >= nseg) return;
     int32_t f = -1;
-    for (uint32_t t = 0; t < trials && f < 0; ++t)
-        if (ur[(uint64_t)seg * trials + t] != zv[(uint64_t)seg * trials + t]) f = (int32_t)t;
+    for (uint32_t t = 0; t < trials; ++t) {
+        uint64_t z = 0;
+        for (int c = 0; c < FIN_CHUNKS; ++c) z = add_mod(z, zv_chunks[((uint64_t)seg * trials + t) * FIN_CHUNKS + c]);
+        zv[(uint64_t)seg * trials + t] = z;
+        if (f < 0 && ur[(uint64_t)seg * trials + t] != z) f = (int32_t)t;
+    }
     failed[seg] = f;
 }
 
@@ -740,15 +747,18 @@ void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32
 
 void launch_tc_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint32_t* d_seg_panel0,
                       const uint32_t* d_seg_block0, const uint64_t* d_v_enc, const VerifySeg* d_vsegs, uint32_t nseg,
-                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, int32_t* d_failed, cudaStream_t s) {
+                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, uint64_t* d_zv_chunks, int32_t* d_failed,
+                      cudaStream_t s) {
     if (!nseg || !trials) return;
-    for (uint32_t s0 = 0; s0 < nseg; s0 += 65535u) {  // grid.y limit
+    // zv chunk partials go to the z_part tail region reserved by the caller
+    uint64_t* zv_chunks = d_zv_chunks;
+    for (uint32_t s0 = 0; s0 < nseg; s0 += 65535u) {  // grid.z limit
         const uint32_t ns = nseg - s0 < 65535u ? nseg - s0 : 65535u;
-        tc_finish_kernel<<<dim3(trials, ns), 256, 0, s>>>(d_z_part, d_ur_part, d_seg_panel0 + s0, d_seg_block0 + s0,
-                                                          d_v_enc, d_vsegs + s0, trials, d_ur + (uint64_t)s0 * trials,
-                                                          d_zv + (uint64_t)s0 * trials);
+        tc_finish_kernel<<<dim3(trials, FIN_CHUNKS + 1, ns), 128, 0, s>>>(
+            d_z_part, d_ur_part, d_seg_panel0 + s0, d_seg_block0 + s0, d_v_enc, d_vsegs + s0, trials,
+            d_ur + (uint64_t)s0 * trials, zv_chunks + (uint64_t)s0 * trials * FIN_CHUNKS);
     }
-    tc_decide_kernel<<<(nseg + 127) / 128, 128, 0, s>>>(d_ur, d_zv, nseg, trials, d_failed);
+    tc_decide_kernel<<<(nseg + 127) / 128, 128, 0, s>>>(d_ur, zv_chunks, nseg, trials, d_zv, d_failed);
 }
 
 }  // namespace bn

@@ -77,8 +77,10 @@ void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32
 
 // Per segment: z_t = sum of its panels' partials, zv_t = z_t . v, ur_t =
 // sum of its blocks' partials; failed = first t with ur_t != zv_t or -1.
+// d_zv_chunks: scratch of nseg * trials * 8 words (per 128-column share of zv).
 void launch_tc_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint32_t* d_seg_panel0,
                       const uint32_t* d_seg_block0, const uint64_t* d_v_enc, const VerifySeg* d_vsegs, uint32_t nseg,
-                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, int32_t* d_failed, cudaStream_t s);
+                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, uint64_t* d_zv_chunks, int32_t* d_failed,
+                      cudaStream_t s);
 
 }  // namespace bn
