@@ -162,6 +162,48 @@ int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v_enc, uint64_t* d_r, voi
 int bn_plan_status(bn_plan* p, uint32_t* device_flags);
 int bn_plan_destroy(bn_plan* p);
 
+/* ---------------------------------------------------------------- block scoring
+ * B queries per launch as tensor-core integer GEMMs over byte-planar copies of
+ * the corpus: compute_products_batch (crypto.rs:782-828) + decode_scores
+ * (crypto.rs:901-940) + top-k (lib.rs:452-469) for the whole block, with
+ * Protocol 2 applied PER BLOCK: one 32-byte block seed, trial t's draws u_t
+ * (draw t*m + i of ChaCha20Rng(block_seed), as verify_response draws them,
+ * crypto.rs:1021-1036) shared by the block's queries, and query q accepted
+ * iff u_t . r_q == (u_t^T M_enc) . v_q for every t.  No counterpart in the
+ * reference, which verifies each query with its own seed (the per-query
+ * entry points above keep that behaviour); the block form costs one pass of
+ * M_enc per block instead of one per query.
+ * Needs the client state with m_plain entries and S entries in [-128, 127]
+ * (int8-quantised corpora; BN_EUNSUPPORTED otherwise).  The byte-planar
+ * copies take 8 * (1024 + 2 * n1) + 2048 + 8 bytes per row of device memory,
+ * built on first use or by bn_flat_block_prepare. */
+#define BN_BLOCK_AUTOTUNE 1u /* bn_flat_block_plan: time the GEMM tilings on this corpus, keep the fastest */
+int bn_flat_block_prepare(bn_flat* h);
+/* Plan for blocks of exactly B queries (1..=8192).  Enqueue-only afterwards
+ * (CUDA-graph capturable), like bn_flat_plan. */
+int bn_flat_block_plan(bn_flat* h, uint32_t B, uint32_t trials, uint32_t k, uint32_t flags, bn_plan** out);
+/* Chosen configuration: {W rows per tile (queries x 8), pipeline stages,
+ * work order (0 = W tile fastest), K panel of the u . r GEMM}. */
+int bn_plan_block_config(const bn_plan* p, uint32_t config[4]);
+/* Device buffers as bn_plan_enqueue, with one 32-byte d_block_seed.
+ * bn_plan_status reports bit 8 when a T column sum left [-128, 127]. */
+int bn_plan_enqueue_block(bn_plan* p, const uint64_t* d_v_enc, const uint64_t* d_g, const uint32_t* d_t,
+                          const uint32_t* d_t_nnz, const uint8_t* d_block_seed, uint32_t* d_ids, int64_t* d_scores,
+                          uint32_t* d_n, int32_t* d_failed, void* stream);
+/* Host buffers, inputs and outputs as bn_flat_query (failed_trial[q] = first
+ * failing trial of query q under the block seed, -1 if accepted); mv_out
+ * (nullable) receives the decoded residues B x m. */
+int bn_flat_query_block(bn_flat* h, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                        const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t block_seed[32], uint32_t trials,
+                        uint32_t k, uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed_trial,
+                        uint64_t* mv_out);
+/* Protocol 2 over claimed responses r (B x m) with the block seed:
+ * failed_trial[q], and ur / zv (nullable, trials x B, [t][q]) = u_t . r_q and
+ * z_t . v_q. */
+int bn_flat_verify_block(bn_flat* h, uint32_t B, const uint64_t* r, const uint64_t* v_enc,
+                         const uint8_t block_seed[32], uint32_t trials, int32_t* failed_trial, uint64_t* ur,
+                         uint64_t* zv);
+
 /* ---------------------------------------------------------------- IVF
  * IvfGpuState::build (gpu/mod.rs:423-474) over a device-resident CSR of the
  * inverted lists: list c owns rows [list_offsets[c], list_offsets[c+1]) of

@@ -18,6 +18,7 @@ TOPK_MAX = 1024
 
 BN_OK, BN_EINVAL, BN_ECUDA, BN_EBUDGET, BN_ENODEV, BN_EUNSUPPORTED = 0, -1, -2, -3, -4, -5
 ENGINE_TENSOR, ENGINE_CUDA_CORE = 0, 1
+BLOCK_AUTOTUNE = 1
 _NAMES = {BN_EINVAL: "EINVAL", BN_ECUDA: "ECUDA", BN_EBUDGET: "EBUDGET", BN_ENODEV: "ENODEV",
           BN_EUNSUPPORTED: "EUNSUPPORTED"}
 
@@ -65,6 +66,12 @@ _SIGS = {
     "bn_plan_enqueue_scan": (C.c_int, [vp, vp, vp, vp]),
     "bn_plan_status": (C.c_int, [vp, vp]),
     "bn_plan_destroy": (C.c_int, [vp]),
+    "bn_flat_block_prepare": (C.c_int, [vp]),
+    "bn_flat_block_plan": (C.c_int, [vp, u32, u32, u32, u32, vp]),
+    "bn_plan_block_config": (C.c_int, [vp, vp]),
+    "bn_plan_enqueue_block": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "bn_flat_query_block": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
+    "bn_flat_verify_block": (C.c_int, [vp, u32, vp, vp, vp, u32, vp, vp, vp]),
     "bn_ivf_build": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, u32, u32, vp]),
     "bn_ivf_attach_client": (C.c_int, [vp, vp, vp, SparseCsr]),
     "bn_ivf_build_from_plain": (C.c_int, [vp, u32, vp, vp, vp, u32, u32, vp, vp, SparseCsr, vp]),
@@ -242,6 +249,44 @@ class Flat:
         check(lib.bn_flat_plan(self.h, B, trials, k, C.byref(out)))
         return Plan(self, out, B, trials, k)
 
+    # ---- block scoring: B queries per launch, Protocol 2 with one seed per block
+    def block_prepare(self):
+        check(lib.bn_flat_block_prepare(self.h))
+
+    def block_plan(self, B: int, trials: int, k: int, autotune: bool = False) -> "Plan":
+        out = vp()
+        check(lib.bn_flat_block_plan(self.h, B, trials, k, BLOCK_AUTOTUNE if autotune else 0, C.byref(out)))
+        return Plan(self, out, B, trials, k, block=True)
+
+    def query_block(self, v_enc, g, t_list, block_seed, trials, k, want_mv=False):
+        v = _u64(v_enc).reshape(-1, N)
+        B = v.shape[0]
+        gg = _u64(g).reshape(B, self.n1)
+        ti, ts, tn = _t_concat(t_list)
+        seed = None if block_seed is None else np.frombuffer(bytes(block_seed), np.uint8).copy()
+        kk = max(k, 1)
+        ids = np.zeros((B, kk), np.uint32)
+        sc = np.zeros((B, kk), np.int64)
+        nh = np.zeros(B, np.uint32)
+        fl = np.zeros(B, np.int32)
+        mv = np.zeros((B, max(self.m, 1)), np.uint64) if want_mv else None
+        check(lib.bn_flat_query_block(self.h, B, ptr(v), ptr(gg), ptr(ti) if ti.size else None,
+                                      ptr(ts) if ts.size else None, ptr(tn), ptr(seed), trials, k, ptr(ids), ptr(sc),
+                                      ptr(nh), ptr(fl), ptr(mv)))
+        hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
+        return hits, fl, (mv[:, : self.m] if want_mv else None)
+
+    def verify_block(self, r, v_enc, block_seed, trials):
+        r = _u64(r).reshape(-1, self.m)
+        v = _u64(v_enc).reshape(-1, N)
+        B = r.shape[0]
+        seed = np.frombuffer(bytes(block_seed), np.uint8).copy()
+        fl = np.zeros(B, np.int32)
+        ur = np.zeros((max(trials, 1), B), np.uint64)
+        zv = np.zeros((max(trials, 1), B), np.uint64)
+        check(lib.bn_flat_verify_block(self.h, B, ptr(r), ptr(v), ptr(seed), trials, ptr(fl), ptr(ur), ptr(zv)))
+        return fl, ur[:trials], zv[:trials]
+
     def close(self):
         if self.h:
             lib.bn_flat_destroy(self.h)
@@ -254,11 +299,18 @@ class Flat:
 class Plan:
     """bn_plan: enqueue-only form of Flat.query over device buffers (graph-capturable)."""
 
-    def __init__(self, flat, handle, B, trials, k):
-        self.flat, self.h, self.B, self.trials, self.k = flat, handle, B, trials, k
+    def __init__(self, flat, handle, B, trials, k, block=False):
+        self.flat, self.h, self.B, self.trials, self.k, self.block = flat, handle, B, trials, k, block
 
     def enqueue(self, d_v, d_g, d_t, d_t_nnz, d_seeds, d_ids, d_scores, d_n, d_failed, stream: int):
-        check(lib.bn_plan_enqueue(self.h, d_v, d_g, d_t, d_t_nnz, d_seeds, d_ids, d_scores, d_n, d_failed, stream))
+        """Per-query plans: d_seeds holds B seeds.  Block plans: d_seeds is the one block seed."""
+        fn = lib.bn_plan_enqueue_block if self.block else lib.bn_plan_enqueue
+        check(fn(self.h, d_v, d_g, d_t, d_t_nnz, d_seeds, d_ids, d_scores, d_n, d_failed, stream))
+
+    def block_config(self):
+        cfg = np.zeros(4, np.uint32)
+        check(lib.bn_plan_block_config(self.h, ptr(cfg)))
+        return {"w_tile": int(cfg[0]), "stages": int(cfg[1]), "order": int(cfg[2]), "k_panel": int(cfg[3])}
 
     def enqueue_scan(self, d_v, d_r, stream: int):
         check(lib.bn_plan_enqueue_scan(self.h, d_v, d_r, stream))

@@ -1,0 +1,463 @@
+// bn_batch.cu -- tensor-core block scoring: the byte-planar u8/s8 GEMM with
+// F_p recombination epilogues, and the layout / operand builders around it.
+//
+// bgemm_kernel roles per CTA (one CTA per SM, persistent over work items;
+// an item is 128 A rows x w_tile W rows x one K panel):
+//   warp 0    TMA producer: per 128-byte K step, the A box (128 rows) and the
+//             W box (w_tile rows) into a ring of shared-memory stages
+//   warp 1    MMA issuer: 4 x tcgen05.mma (M=128, N=w_tile, K=32) per stage
+//             into one of two TMEM accumulators (double-buffered across
+//             items), tcgen05.commit frees the stage / hands over the item
+//   warps 2-5 epilogue: tcgen05.ld, byte-weight recombination mod p, stores
+// Every mbarrier wait is bounded; on timeout the CTA sets *err and winds down
+// (waits for its own copies and MMAs, frees TMEM) instead of hanging.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+
+#include "bn_batch.cuh"
+#include "bn_fp.cuh"
+#include "bn_tcgen05.cuh"
+
+namespace bn {
+
+namespace {
+
+using namespace tcg;
+
+constexpr int BG_THREADS = 192;
+
+struct ItemIdx {
+    uint32_t kp, ta, tw;
+};
+__device__ __forceinline__ ItemIdx item_idx(const BgParams& p, uint32_t item) {
+    const uint32_t per = p.a_tiles * p.w_tiles;
+    const uint32_t kp = item / per, rem = item % per;
+    if (p.order_a_fast) return ItemIdx{kp, rem % p.a_tiles, rem / p.a_tiles};
+    return ItemIdx{kp, rem / p.w_tiles, rem % p.w_tiles};
+}
+
+__global__ void __launch_bounds__(BG_THREADS, 1)
+bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CUtensorMap tmap_w,
+             const BgParams p, uint32_t stages, uint32_t stage_bytes, uint32_t* __restrict__ err) {
+    extern __shared__ uint8_t bg_dyn[];
+    __shared__ uint64_t full_b[BG_MAX_STAGES], empty_b[BG_MAX_STAGES], accf_b[2], acce_b[2], done_b;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    const uint32_t base = (su32(bg_dyn) + 1023u) & ~1023u;  // 1024-byte aligned ring (128-byte swizzle atoms)
+    uint8_t* ring = bg_dyn + (base - su32(bg_dyn));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr uint32_t A_BYTES = BG_AROWS * BG_KSTEP;
+    const uint32_t w_bytes = p.w_tile * BG_KSTEP;
+    const uint32_t kpanels = (p.k_bytes + p.k_panel - 1) / p.k_panel;
+    const uint32_t items = kpanels * p.a_tiles * p.w_tiles;
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < stages; ++s) {
+            bar_init(&full_b[s], 1);
+            bar_init(&empty_b[s], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            bar_init(&accf_b[b], 1);
+            bar_init(&acce_b[b], 4);
+        }
+        bar_init(&done_b, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_s)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tmem = tmem_base_s;
+
+    if (warp == 0) {
+        if (lane == 0) {  // ---------------------------------------------- TMA producer
+            uint64_t it = 0;
+            bool stop = false;
+            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
+                const ItemIdx ix = item_idx(p, item);
+                const uint32_t k0 = ix.kp * p.k_panel, k1 = min(p.k_bytes, k0 + p.k_panel);
+                for (uint32_t k = k0; k < k1; k += BG_KSTEP, ++it) {
+                    const uint32_t st = (uint32_t)(it % stages);
+                    if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1))) {
+                        abort_s = 1;
+                        atomicOr(err, 4u);
+                        stop = true;
+                        break;
+                    }
+                    if (abort_s) { stop = true; break; }
+                    uint8_t* sb = ring + (uint64_t)st * stage_bytes;
+                    bar_expect_tx(&full_b[st], A_BYTES + w_bytes);
+                    tma_2d(sb, &tmap_a, (int)k, (int)(ix.ta * BG_AROWS), &full_b[st]);
+                    tma_2d(sb + A_BYTES, &tmap_w, (int)k, (int)(ix.tw * p.w_tile), &full_b[st]);
+                }
+            }
+            // no copy may still be landing in shared memory when the CTA exits
+            for (uint64_t j = it > stages ? it - stages : 0; j < it; ++j)
+                bar_wait(&full_b[j % stages], (uint32_t)((j / stages) & 1));
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // ---------------------------------------------- MMA issuer
+            const uint32_t sgn = p.mode == BG_S8 ? 1u : 0u;
+            const uint32_t idesc = (2u << 4) | (sgn << 7) | (sgn << 10) | ((p.w_tile >> 3) << 17) |
+                                   ((uint32_t)(BG_AROWS >> 4) << 24);
+            uint64_t it = 0, n = 0;
+            bool stop = false;
+            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x, ++n) {
+                const ItemIdx ix = item_idx(p, item);
+                const uint32_t buf = (uint32_t)(n & 1), use = (uint32_t)(n >> 1);
+                if (use > 0 && !bar_wait(&acce_b[buf], (use - 1) & 1)) {
+                    abort_s = 1;
+                    atomicOr(err, 8u);
+                    break;
+                }
+                tc_after();
+                const uint32_t d = tmem + buf * 256u;
+                const uint32_t k0 = ix.kp * p.k_panel, k1 = min(p.k_bytes, k0 + p.k_panel);
+                bool first = true;
+                for (uint32_t k = k0; k < k1; k += BG_KSTEP, ++it) {
+                    const uint32_t st = (uint32_t)(it % stages);
+                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
+                        abort_s = 1;
+                        atomicOr(err, 8u);
+                        stop = true;
+                        break;
+                    }
+                    tc_after();
+                    const uint32_t sa = base + st * stage_bytes, sw = sa + A_BYTES;
+#pragma unroll
+                    for (uint32_t ks = 0; ks < BG_KSTEP / 32; ++ks)
+                        mma_i8(d, sdesc(sa + ks * 32u, 16, 1024), sdesc(sw + ks * 32u, 16, 1024), idesc,
+                               (first && ks == 0) ? 0u : 1u);
+                    first = false;
+                    mma_commit(&empty_b[st]);  // stage reusable once these MMAs have read it
+                }
+                if (stop) break;
+                mma_commit(&accf_b[buf]);  // accumulator complete for this item
+            }
+            mma_commit(&done_b);
+            bar_wait(&done_b, 0);  // every issued MMA has finished before TMEM is freed
+        }
+    } else {
+        // -------------------------------------------------------------- epilogue
+        const uint32_t q = (uint32_t)(warp & 3);  // TMEM lane quarter of this warp
+        uint64_t n = 0;
+        for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, ++n) {
+            const uint32_t buf = (uint32_t)(n & 1), use = (uint32_t)(n >> 1);
+            const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b[buf], use & 1));  // warp-uniform
+            if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
+            if (__any_sync(FULLMASK, !ok || abort_s)) break;
+            tc_after();
+            const ItemIdx ix = item_idx(p, item);
+            const uint32_t taddr = tmem + ((q * 32u) << 16) + buf * 256u;
+            const uint32_t ybase = ix.tw * p.w_tile / 8;
+            if (p.mode == BG_PLANAR) {
+                const uint32_t a = lane & 7;
+                const uint32_t x = ix.ta * (BG_AROWS / 8) + q * 4 + (lane >> 3);
+                const uint32_t x4 = ix.ta * (BG_AROWS / 8) + q * 4;  // first x of this warp
+                const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+                uint64_t* out = p.out + (uint64_t)ix.kp * p.out_pstride;
+                for (uint32_t c0 = 0; c0 < p.w_tile; c0 += 16) {
+                    uint32_t v[16];
+                    tmem_ld16(taddr + c0, v);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t y = ybase + c0 / 8 + h;
+                        uint64_t lo = 0, hi = 0;
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            lo += (uint64_t)v[8 * h + b] << (8 * b);
+                            hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
+                        }
+                        uint64_t f = canon(rotl61(lo, w1) + rotl61(hi, w2));  // (lo + hi 2^32) 2^(8a) mod p
+                        f += __shfl_xor_sync(FULLMASK, f, 1);
+                        f += __shfl_xor_sync(FULLMASK, f, 2);
+                        f += __shfl_xor_sync(FULLMASK, f, 4);
+                        f = canon(f);
+                        uint32_t packed = (uint32_t)((f >> (8 * a)) & 0xffu) << (8 * (lane >> 3));
+                        packed |= __shfl_xor_sync(FULLMASK, packed, 8);
+                        packed |= __shfl_xor_sync(FULLMASK, packed, 16);
+                        if (y < p.y_count) {
+                            if (a == 0 && x < p.x_count) {
+                                uint64_t* dst = out + (uint64_t)y * p.out_ld + x;
+                                *dst = p.accumulate ? add_mod(*dst, f) : f;
+                            }
+                            if (p.planar_out && lane < 8 && x4 < p.x_count)
+                                *reinterpret_cast<uint32_t*>(p.planar_out + ((uint64_t)y * 8 + lane) * p.planar_ld + x4) =
+                                    packed;
+                        }
+                    }
+                }
+            } else {
+                const uint32_t x = ix.ta * BG_AROWS + q * 32 + lane;
+                const bool xv = x < p.x_count;
+                const uint64_t corr = xv ? p.corr[x] : 0;
+                for (uint32_t c0 = 0; c0 < p.w_tile; c0 += 16) {
+                    uint32_t v[16];
+                    tmem_ld16(taddr + c0, v);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t y = ybase + c0 / 8 + h;
+                        int64_t lo = 0, hi = 0;
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            lo += (int64_t)(int32_t)v[8 * h + b] * (int64_t)(1ll << (8 * b));
+                            hi += (int64_t)(int32_t)v[8 * h + 4 + b] * (int64_t)(1ll << (8 * b));
+                        }
+                        const uint64_t lr = lo < 0 ? (uint64_t)(lo + (int64_t)P) : (uint64_t)lo;
+                        const uint64_t hr = hi < 0 ? (uint64_t)(hi + (int64_t)P) : (uint64_t)hi;
+                        const uint64_t f = add_mod(canon(lr + rotl61(hr, 32)), corr);
+                        if (xv && y < p.y_count) {
+                            uint64_t* dst = p.out + (uint64_t)y * p.out_ld + x;
+                            *dst = sub_mod(*dst, f);
+                        }
+                    }
+                }
+            }
+            tc_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(&acce_b[buf]);
+        }
+    }
+    tc_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------ layouts and operands
+__global__ void planar_rows_kernel(const uint64_t* __restrict__ src, uint64_t rows, uint32_t k, uint64_t src_ld,
+                                   int negate, uint8_t* __restrict__ dst, uint64_t dst_ld, uint32_t col0) {
+    const uint32_t chunks = k / 16;
+    const uint64_t total = rows * chunks;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = e / chunks;
+        const uint32_t jc = (uint32_t)(e % chunks);
+        uint64_t x[16];
+        const uint64_t* s = src + i * src_ld + jc * 16;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            const uint64_t y = s[t];
+            x[t] = negate ? (y == 0 ? 0 : P - y) : y;
+        }
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int t = 0; t < 16; ++t) w[t >> 2] |= (uint32_t)((x[t] >> (8 * a)) & 0xffu) << (8 * (t & 3));
+            *reinterpret_cast<uint4*>(dst + (i * 8 + a) * dst_ld + col0 + jc * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+}
+
+__global__ void planar_cm_kernel(const uint64_t* __restrict__ src_cm, uint64_t rows, uint32_t k,
+                                 uint8_t* __restrict__ dst, uint64_t dst_ld, uint32_t col0) {
+    const uint32_t chunks = k / 16;
+    const uint64_t total = rows * chunks;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t jc = (uint32_t)(e / rows);
+        const uint64_t i = e % rows;  // consecutive threads: consecutive rows (coalesced column reads)
+        uint64_t x[16];
+#pragma unroll
+        for (int t = 0; t < 16; ++t) x[t] = src_cm[(uint64_t)(jc * 16 + t) * rows + i];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+            for (int t = 0; t < 16; ++t) w[t >> 2] |= (uint32_t)((x[t] >> (8 * a)) & 0xffu) << (8 * (t & 3));
+            *reinterpret_cast<uint4*>(dst + (i * 8 + a) * dst_ld + col0 + jc * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+    }
+}
+
+__global__ void ms8_m_kernel(const uint64_t* __restrict__ mp_cm, uint64_t rows, int8_t* __restrict__ dst,
+                             uint32_t* __restrict__ bad) {
+    const uint32_t chunks = N / 16;
+    const uint64_t total = rows * chunks;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t jc = (uint32_t)(e / rows);
+        const uint64_t i = e % rows;
+        uint32_t w[4] = {0, 0, 0, 0};
+        bool out_of_range = false;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            const int64_t sv = to_signed(mp_cm[(uint64_t)(jc * 16 + t) * rows + i]);
+            out_of_range |= sv < -128 || sv > 127;
+            w[t >> 2] |= (uint32_t)((uint8_t)(int8_t)sv) << (8 * (t & 3));
+        }
+        if (out_of_range) atomicOr(bad, 1u);
+        *reinterpret_cast<uint4*>(dst + i * (2 * N) + jc * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+__global__ void ms8_s_kernel(const uint16_t* __restrict__ s_ell, const uint32_t* __restrict__ s_off,
+                             const uint16_t* __restrict__ s_w, uint64_t rows, int8_t* __restrict__ dst,
+                             uint64_t* __restrict__ corr, uint32_t* __restrict__ bad) {
+    const uint64_t c_mod = canon(0x0101010101010101ull);  // sum_b 2^(8b)
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x) {
+        int8_t* row = dst + i * (2 * N) + N;
+        for (uint32_t c = 0; c < N / 16; ++c) reinterpret_cast<uint4*>(row)[c] = make_uint4(0, 0, 0, 0);
+        const uint64_t slice = i >> 5;
+        const uint32_t sl = (uint32_t)(i & 31), off = s_off[slice], wdt = s_w[slice];
+        int rs = 0;
+        for (uint32_t cc = 0; cc < wdt; ++cc) {
+            const uint16_t f = s_ell[off + (uint64_t)cc * 32 + sl];
+            if (f == 0xffffu) continue;
+            const int sgn = (f & 0x8000u) ? -1 : 1;
+            const int nv = (int)row[f & 0x3ffu] + sgn;
+            if (nv < -128 || nv > 127) atomicOr(bad, 1u);
+            row[f & 0x3ffu] = (int8_t)nv;
+            rs += sgn;
+        }
+        const uint64_t m = mul_mod((uint64_t)(128 * (rs < 0 ? -rs : rs)), c_mod);
+        corr[i] = rs < 0 ? (m ? P - m : 0) : m;
+    }
+}
+
+__global__ void w_tv_kernel(const uint64_t* __restrict__ v, uint32_t nq, int8_t* __restrict__ dst) {
+    const uint32_t chunks = N / 16;
+    const uint64_t total = (uint64_t)nq * 8 * chunks;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t qb = e / chunks;
+        const uint32_t jc = (uint32_t)(e % chunks);
+        const uint32_t q = (uint32_t)(qb >> 3), b = (uint32_t)(qb & 7);
+        int8_t* row = dst + qb * (2 * N);
+        reinterpret_cast<uint4*>(row)[jc] = make_uint4(0, 0, 0, 0);  // T part (b = 0 filled below)
+        uint32_t w[4] = {0, 0, 0, 0};
+#pragma unroll
+        for (int t = 0; t < 16; ++t) {
+            const int byte = (int)((v[(uint64_t)q * N + jc * 16 + t] >> (8 * b)) & 0xffu) - 128;
+            w[t >> 2] |= (uint32_t)((uint8_t)(int8_t)byte) << (8 * (t & 3));
+        }
+        reinterpret_cast<uint4*>(row + N)[jc] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+__global__ void w_t_kernel(const uint32_t* __restrict__ t_ent, const uint32_t* __restrict__ t_nnz, uint32_t nq,
+                           int8_t* __restrict__ dst, uint32_t* __restrict__ bad) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    int8_t* row = dst + (uint64_t)q * 8 * (2 * N);  // row (q, b = 0)
+    const uint32_t tn = min(t_nnz[q], (uint32_t)N);
+    for (uint32_t c = 0; c < tn; ++c) {
+        const uint32_t e = t_ent[(uint64_t)q * N + c];
+        const int nv = (int)row[e & 0x3ffu] + ((e >> 31) ? -1 : 1);
+        if (nv < -128 || nv > 127) atomicOr(bad, 2u);
+        row[e & 0x3ffu] = (int8_t)nv;
+    }
+}
+
+__global__ void zsum_kernel(const uint64_t* __restrict__ z_part, uint32_t npanels, uint32_t t_base,
+                            uint32_t trials_total, uint64_t* __restrict__ z) {
+    const uint32_t t = t_base + blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    uint64_t acc = 0;
+    for (uint32_t pn = 0; pn < npanels; ++pn) acc = add_mod(acc, z_part[((uint64_t)pn * trials_total + t) * N + j]);
+    z[(uint64_t)t * N + j] = acc;
+}
+
+__global__ void __launch_bounds__(128) zv_kernel(const uint64_t* __restrict__ z, const uint64_t* __restrict__ v,
+                                                 uint32_t nq, uint64_t* __restrict__ zv) {
+    const uint32_t q = blockIdx.x, t = blockIdx.y;
+    __shared__ uint64_t sh[4];
+    uint64_t acc = 0;
+    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x)
+        acc = add_mod(acc, mul_mod(z[(uint64_t)t * N + j], v[(uint64_t)q * N + j]));
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc = add_mod(acc, __shfl_xor_sync(0xffffffffu, acc, off));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) zv[(uint64_t)t * nq + q] = add_mod(add_mod(sh[0], sh[1]), add_mod(sh[2], sh[3]));
+}
+
+__global__ void ur_decide_kernel(const uint64_t* __restrict__ ur_part, uint32_t kpanels, uint32_t trials, uint32_t nq,
+                                 const uint64_t* __restrict__ zv, uint64_t* __restrict__ ur, int32_t* __restrict__ failed) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    int32_t f = -1;
+    for (uint32_t t = 0; t < trials; ++t) {
+        uint64_t acc = 0;
+        for (uint32_t kp = 0; kp < kpanels; ++kp) acc = add_mod(acc, ur_part[((uint64_t)kp * trials + t) * nq + q]);
+        if (ur) ur[(uint64_t)t * nq + q] = acc;
+        if (f < 0 && acc != zv[(uint64_t)t * nq + q]) f = (int32_t)t;
+    }
+    failed[q] = f;
+}
+
+unsigned grid_for(uint64_t work, unsigned threads, unsigned cap) {
+    const uint64_t g = (work + threads - 1) / threads;
+    return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+}  // namespace
+
+uint32_t bgemm_stage_bytes(uint32_t w_tile) { return BG_AROWS * BG_KSTEP + ((w_tile * BG_KSTEP + 1023u) & ~1023u); }
+
+void launch_bgemm(const CUtensorMap& tmap_a, const CUtensorMap& tmap_w, const BgParams& p, uint32_t stages, int ctas,
+                  uint32_t* d_err, cudaStream_t s) {
+    const uint32_t kpanels = (p.k_bytes + p.k_panel - 1) / p.k_panel;
+    const uint64_t items = (uint64_t)kpanels * p.a_tiles * p.w_tiles;
+    if (!items) return;
+    const uint32_t stage_bytes = bgemm_stage_bytes(p.w_tile);
+    // at least half the SM's shared memory: one CTA per SM, so the second
+    // never waits in tcgen05.alloc for the first one's 512 TMEM columns
+    const int smem = (int)std::max<uint32_t>(stages * stage_bytes + 1024, 116u * 1024u);
+    cudaFuncSetAttribute(bgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const unsigned grid = items < (uint64_t)ctas ? (unsigned)items : (unsigned)ctas;
+    bgemm_kernel<<<grid, BG_THREADS, smem, s>>>(tmap_a, tmap_w, p, stages, stage_bytes, d_err);
+}
+
+void launch_planar_rows(const uint64_t* d_src, uint64_t rows, uint32_t k, uint64_t src_ld, int negate, uint8_t* d_dst,
+                        uint64_t dst_ld, uint32_t col0, cudaStream_t s) {
+    if (!rows) return;
+    planar_rows_kernel<<<grid_for(rows * (k / 16), 256, 148 * 16), 256, 0, s>>>(d_src, rows, k, src_ld, negate, d_dst,
+                                                                              dst_ld, col0);
+}
+
+void launch_planar_cm(const uint64_t* d_src_cm, uint64_t rows, uint32_t k, uint8_t* d_dst, uint64_t dst_ld,
+                      uint32_t col0, cudaStream_t s) {
+    if (!rows) return;
+    planar_cm_kernel<<<grid_for(rows * (k / 16), 256, 148 * 16), 256, 0, s>>>(d_src_cm, rows, k, d_dst, dst_ld, col0);
+}
+
+void launch_ms8(const uint64_t* d_mp_cm, const uint16_t* d_s_ell, const uint32_t* d_s_off, const uint16_t* d_s_w,
+                uint64_t rows, int8_t* d_dst, uint64_t* d_corr, uint32_t* d_bad, cudaStream_t s) {
+    if (!rows) return;
+    ms8_m_kernel<<<grid_for(rows * (N / 16), 256, 148 * 16), 256, 0, s>>>(d_mp_cm, rows, d_dst, d_bad);
+    ms8_s_kernel<<<grid_for(rows, 128, 148 * 16), 128, 0, s>>>(d_s_ell, d_s_off, d_s_w, rows, d_dst, d_corr, d_bad);
+}
+
+void launch_w_tv(const uint64_t* d_v, const uint32_t* d_t, const uint32_t* d_t_nnz, uint32_t nq, int8_t* d_dst,
+                 uint32_t* d_bad, cudaStream_t s) {
+    if (!nq) return;
+    w_tv_kernel<<<grid_for((uint64_t)nq * 8 * (N / 16), 256, 148 * 8), 256, 0, s>>>(d_v, nq, d_dst);
+    w_t_kernel<<<(nq + 127) / 128, 128, 0, s>>>(d_t, d_t_nnz, nq, d_dst, d_bad);
+}
+
+void launch_zsum(const uint64_t* d_z_part, uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t trials_total,
+                 uint64_t* d_z, cudaStream_t s) {
+    if (!t_cnt) return;
+    zsum_kernel<<<dim3(N / 256, t_cnt), 256, 0, s>>>(d_z_part, npanels, t_base, trials_total, d_z);
+}
+
+void launch_zv(const uint64_t* d_z, const uint64_t* d_v, uint32_t trials, uint32_t nq, uint64_t* d_zv, cudaStream_t s) {
+    if (!trials || !nq) return;
+    zv_kernel<<<dim3(nq, trials), 128, 0, s>>>(d_z, d_v, nq, d_zv);
+}
+
+void launch_ur_decide(const uint64_t* d_ur_part, uint32_t kpanels, uint32_t trials, uint32_t nq, const uint64_t* d_zv,
+                      uint64_t* d_ur, int32_t* d_failed, cudaStream_t s) {
+    if (!nq) return;
+    ur_decide_kernel<<<(nq + 127) / 128, 128, 0, s>>>(d_ur_part, kpanels, trials, nq, d_zv, d_ur, d_failed);
+}
+
+}  // namespace bn

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "bn_b200.h"
+#include "bn_internal.cuh"
 #include "bn_kernels.cuh"
 #include "bn_tc.cuh"
 
@@ -25,8 +26,9 @@ using namespace bn;
 // ------------------------------------------------------------------ errors
 namespace {
 thread_local std::string g_err;
+}  // namespace
 
-int fail(int code, const char* fmt, ...) {
+int bn::api::fail(int code, const char* fmt, ...) {
     char buf[1024];
     va_list ap;
     va_start(ap, fmt);
@@ -36,129 +38,9 @@ int fail(int code, const char* fmt, ...) {
     return code;
 }
 
-#define CU(call)                                                                                    \
-    do {                                                                                            \
-        cudaError_t e_ = (call);                                                                    \
-        if (e_ != cudaSuccess) return fail(BN_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));     \
-    } while (0)
-
-#define TRY(call)                    \
-    do {                             \
-        int rc_ = (call);            \
-        if (rc_ != BN_OK) return rc_; \
-    } while (0)
-
-inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
-}  // namespace
-
-// ------------------------------------------------------------------ context
-struct bn_ctx {
-    int device = 0;
-    int num_sms = 148;
-    int engine = BN_ENGINE_TENSOR;  // Protocol 2 engine
-    uint64_t budget = 0, used = 0, peak = 0;
-    std::mutex mu;
-};
+using namespace bn::api;
 
 namespace {
-
-// Device allocation accounted against the context budget.
-struct DevMem {
-    bn_ctx* ctx = nullptr;
-    void* p = nullptr;
-    uint64_t bytes = 0;
-
-    DevMem() = default;
-    DevMem(const DevMem&) = delete;
-    DevMem& operator=(const DevMem&) = delete;
-    ~DevMem() { release(); }
-
-    void release() {
-        if (p) {
-            cudaFree(p);
-            std::lock_guard<std::mutex> g(ctx->mu);
-            ctx->used -= bytes;
-        }
-        p = nullptr;
-        bytes = 0;
-    }
-    int alloc(bn_ctx* c, uint64_t b) {
-        release();
-        ctx = c;
-        if (b == 0) return BN_OK;
-        {
-            std::lock_guard<std::mutex> g(c->mu);
-            if (c->used + b > c->budget)
-                return fail(BN_EBUDGET, "cluster payload %llu bytes exceeds budget %llu bytes (%llu bytes in use)",
-                            (unsigned long long)b, (unsigned long long)c->budget, (unsigned long long)c->used);
-            c->used += b;
-            c->peak = std::max(c->peak, c->used);
-        }
-        cudaError_t e = cudaMalloc(&p, b);
-        if (e != cudaSuccess) {
-            std::lock_guard<std::mutex> g(c->mu);
-            c->used -= b;
-            p = nullptr;
-            return fail(BN_ECUDA, "cudaMalloc(%llu): %s", (unsigned long long)b, cudaGetErrorString(e));
-        }
-        bytes = b;
-        return BN_OK;
-    }
-    // Grow-only reallocation (contents not kept).
-    int reserve(bn_ctx* c, uint64_t b) { return (p && bytes >= b) ? BN_OK : alloc(c, b); }
-    template <class T>
-    T* at(uint64_t off = 0) const {
-        return reinterpret_cast<T*>(static_cast<char*>(p) + off);
-    }
-};
-
-struct PinnedMem {
-    void* p = nullptr;
-    uint64_t bytes = 0;
-    ~PinnedMem() {
-        if (p) cudaFreeHost(p);
-    }
-    int reserve(uint64_t b) {
-        if (p && bytes >= b) return BN_OK;
-        if (p) cudaFreeHost(p);
-        p = nullptr;
-        bytes = 0;
-        CU(cudaMallocHost(&p, b));
-        bytes = b;
-        return BN_OK;
-    }
-    template <class T>
-    T* at(uint64_t off = 0) const {
-        return reinterpret_cast<T*>(static_cast<char*>(p) + off);
-    }
-};
-
-// Bump allocator computing sub-buffer offsets (256-byte aligned).
-struct Layout {
-    uint64_t off = 0;
-    template <class T>
-    uint64_t take(uint64_t count) {
-        off = align_up(off, 256);
-        uint64_t o = off;
-        off += count * sizeof(T);
-        return o;
-    }
-};
-
-// Resident corpus: a flat cluster, or all IVF lists concatenated.
-struct Corpus {
-    uint64_t rows = 0;
-    uint32_t n = N, n1 = 128;
-    DevMem m_enc, al_cm, h_cm;
-    bool client = false;
-    DevMem L, mp_cm, s_ell, s_off, s_w, ids;
-    CUtensorMap tmap_m;  // m_enc as bytes {8192, rows}, 128x128 boxes, 128-byte swizzle
-
-    uint64_t bytes() const {
-        return m_enc.bytes + al_cm.bytes + h_cm.bytes + L.bytes + mp_cm.bytes + s_ell.bytes + s_off.bytes + s_w.bytes +
-               ids.bytes;
-    }
-};
 
 int corpus_tmap(Corpus& c) {
     if (!c.rows) return BN_OK;
@@ -603,16 +485,6 @@ void pack_meta(char* h, const RunLayout& o, const HostMeta& hm) {
     memcpy(h + o.seg_block0, hm.seg_block0.data(), hm.seg_block0.size() * 4);
 }
 
-// Handle-side state shared by flat and IVF.
-struct Engine {
-    bn_ctx* ctx = nullptr;
-    Corpus c;
-    cudaStream_t stream = nullptr;
-    std::mutex mu;
-    DevMem ws;
-    PinnedMem host;
-};
-
 int engine_init(Engine& e, bn_ctx* ctx) {
     e.ctx = ctx;
     CU(cudaSetDevice(ctx->device));
@@ -861,18 +733,6 @@ int run_dense_terms(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* g, 
 
 }  // namespace
 
-// ------------------------------------------------------------------ handles
-struct bn_flat {
-    Engine e;
-    uint64_t m = 0;
-};
-
-struct bn_ivf {
-    Engine e;
-    uint32_t nlist = 0;
-    std::vector<uint64_t> offsets;
-};
-
 struct bn_plan {
     bn_flat* h = nullptr;
     Sizes z{};
@@ -880,6 +740,10 @@ struct bn_plan {
     DevMem ws;
     HostMeta hm;
     TcMaps maps;
+    BlockPlan* block = nullptr;  // set for block plans (bn_flat_block_plan)
+    ~bn_plan() {
+        if (block) block_plan_free(block);
+    }
 };
 
 extern "C" {
@@ -1112,6 +976,7 @@ int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v, const uint64_t* d_g, const 
                     const uint8_t* d_seeds, uint32_t* d_ids, int64_t* d_scores, uint32_t* d_n, int32_t* d_failed,
                     void* stream) {
     if (!p) return fail(BN_EINVAL, "null plan");
+    if (p->block) return fail(BN_EINVAL, "block plan: use bn_plan_enqueue_block");
     if (!d_v || (p->z.k && (!d_g || !d_t || !d_t_nnz || !d_ids || !d_scores || !d_n)) || (p->z.trials && !d_seeds) || !d_failed)
         return fail(BN_EINVAL, "null device pointer");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1125,6 +990,7 @@ int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v, const uint64_t* d_g, const 
 
 int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v, uint64_t* d_r, void* stream) {
     if (!p || !d_v || !d_r) return fail(BN_EINVAL, "null argument");
+    if (p->block) return fail(BN_EINVAL, "block plan: use bn_plan_enqueue_block");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     char* d = p->ws.at<char>();
     const RunLayout& o = p->o;
@@ -1140,8 +1006,93 @@ int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v, uint64_t* d_r, void* s
 
 int bn_plan_status(bn_plan* p, uint32_t* device_flags) {
     if (!p || !device_flags) return fail(BN_EINVAL, "null argument");
+    if (p->block) return block_plan_status(p->block, device_flags);
     CU(cudaMemcpy(device_flags, p->ws.at<char>() + p->o.err, 4, cudaMemcpyDeviceToHost));
     return BN_OK;
+}
+
+int bn_flat_block_prepare(bn_flat* f) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    if (!f->m) return fail(BN_EINVAL, "empty corpus");
+    return block_prepare(f);
+}
+
+int bn_flat_block_plan(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint32_t flags, bn_plan** out) {
+    if (!f || !out) return fail(BN_EINVAL, "null argument");
+    flags &= BN_BLOCK_AUTOTUNE;
+    *out = nullptr;
+    BlockPlan* b = nullptr;
+    TRY(block_plan_create(f, B, trials, k, flags, &b));
+    auto* p = new bn_plan();
+    p->h = f;
+    p->block = b;
+    *out = p;
+    return BN_OK;
+}
+
+int bn_plan_block_config(const bn_plan* p, uint32_t config[4]) {
+    if (!p || !config) return fail(BN_EINVAL, "null argument");
+    if (!p->block) return fail(BN_EINVAL, "not a block plan");
+    block_plan_config(p->block, config);
+    return BN_OK;
+}
+
+int bn_plan_enqueue_block(bn_plan* p, const uint64_t* d_v, const uint64_t* d_g, const uint32_t* d_t,
+                          const uint32_t* d_t_nnz, const uint8_t* d_block_seed, uint32_t* d_ids, int64_t* d_scores,
+                          uint32_t* d_n, int32_t* d_failed, void* stream) {
+    if (!p) return fail(BN_EINVAL, "null plan");
+    if (!p->block) return fail(BN_EINVAL, "not a block plan: use bn_plan_enqueue");
+    return block_enqueue(*p->block, d_v, d_g, d_t, d_t_nnz, d_block_seed, d_ids, d_scores, d_n, d_failed,
+                         static_cast<cudaStream_t>(stream), nullptr);
+}
+
+static int cached_block_plan(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint32_t flags, BlockPlan** out) {
+    if (f->block_cache && f->cache_B == B && f->cache_trials == trials && f->cache_k == k && f->cache_flags == flags) {
+        *out = f->block_cache;
+        return BN_OK;
+    }
+    if (f->block_cache) {
+        block_plan_free(f->block_cache);
+        f->block_cache = nullptr;
+    }
+    TRY(block_plan_create(f, B, trials, k, flags, &f->block_cache));
+    f->cache_flags = flags;
+    f->cache_B = B;
+    f->cache_trials = trials;
+    f->cache_k = k;
+    *out = f->block_cache;
+    return BN_OK;
+}
+
+int bn_flat_query_block(bn_flat* f, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                        const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* block_seed, uint32_t trials,
+                        uint32_t k, uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed_trial,
+                        uint64_t* mv_out) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    if (B == 0) return BN_OK;
+    if (!v_enc || !g || !t_nnz || (trials && !block_seed)) return fail(BN_EINVAL, "null query input");
+    TRY(validate_residues(v_enc, (uint64_t)B * N, "v_enc"));
+    TRY(validate_residues(g, (uint64_t)B * f->e.c.n1, "g"));
+    uint64_t t_total = 0;
+    for (uint32_t q = 0; q < B; ++q) t_total += t_nnz[q];
+    if (t_total && (!t_idx || !t_sign)) return fail(BN_EINVAL, "t_idx / t_sign are null");
+    std::lock_guard<std::mutex> gd(f->block_mu);
+    BlockPlan* b = nullptr;
+    TRY(cached_block_plan(f, B, trials, k, 0, &b));
+    return block_query_host(*b, v_enc, g, t_idx, t_sign, t_nnz, block_seed, ids, scores, n_hits, failed_trial, mv_out);
+}
+
+int bn_flat_verify_block(bn_flat* f, uint32_t B, const uint64_t* r, const uint64_t* v_enc, const uint8_t* block_seed,
+                         uint32_t trials, int32_t* failed_trial, uint64_t* ur, uint64_t* zv) {
+    if (!f || !r || !v_enc || !block_seed || !failed_trial) return fail(BN_EINVAL, "null argument");
+    if (B == 0) return BN_OK;
+    if (trials == 0) return fail(BN_EINVAL, "trials must be >= 1");
+    TRY(validate_residues(v_enc, (uint64_t)B * N, "v_enc"));
+    TRY(validate_residues(r, (uint64_t)B * f->m, "r"));
+    std::lock_guard<std::mutex> gd(f->block_mu);
+    BlockPlan* b = nullptr;
+    TRY(cached_block_plan(f, B, trials, 0, BLOCK_VERIFY_ONLY, &b));
+    return block_verify_host(*b, r, v_enc, block_seed, failed_trial, ur, zv);
 }
 
 int bn_plan_destroy(bn_plan* p) {

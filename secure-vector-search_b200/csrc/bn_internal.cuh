@@ -1,0 +1,206 @@
+// bn_internal.cuh -- library-internal types shared by the translation units
+// behind the C ABI (bn_capi.cu, bn_block.cu): the context, budget-accounted
+// device memory, the resident corpus and the flat / IVF handles.
+#pragma once
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bn_b200.h"
+#include "bn_kernels.cuh"
+
+// ------------------------------------------------------------------ context
+struct bn_ctx {
+    int device = 0;
+    int num_sms = 148;
+    int engine = BN_ENGINE_TENSOR;  // Protocol 2 engine
+    uint64_t budget = 0, used = 0, peak = 0;
+    std::mutex mu;
+};
+
+namespace bn {
+namespace api {
+
+// Records the message for bn_last_error() (thread-local) and returns code.
+int fail(int code, const char* fmt, ...);
+
+#define CU(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess) return ::bn::api::fail(BN_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+#define TRY(call)                    \
+    do {                             \
+        int rc_ = (call);            \
+        if (rc_ != BN_OK) return rc_; \
+    } while (0)
+
+inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+
+
+// Device allocation accounted against the context budget.
+struct DevMem {
+    bn_ctx* ctx = nullptr;
+    void* p = nullptr;
+    uint64_t bytes = 0;
+
+    DevMem() = default;
+    DevMem(const DevMem&) = delete;
+    DevMem& operator=(const DevMem&) = delete;
+    ~DevMem() { release(); }
+
+    void release() {
+        if (p) {
+            cudaFree(p);
+            std::lock_guard<std::mutex> g(ctx->mu);
+            ctx->used -= bytes;
+        }
+        p = nullptr;
+        bytes = 0;
+    }
+    int alloc(bn_ctx* c, uint64_t b) {
+        release();
+        ctx = c;
+        if (b == 0) return BN_OK;
+        {
+            std::lock_guard<std::mutex> g(c->mu);
+            if (c->used + b > c->budget)
+                return fail(BN_EBUDGET, "cluster payload %llu bytes exceeds budget %llu bytes (%llu bytes in use)",
+                            (unsigned long long)b, (unsigned long long)c->budget, (unsigned long long)c->used);
+            c->used += b;
+            c->peak = std::max(c->peak, c->used);
+        }
+        cudaError_t e = cudaMalloc(&p, b);
+        if (e != cudaSuccess) {
+            std::lock_guard<std::mutex> g(c->mu);
+            c->used -= b;
+            p = nullptr;
+            return fail(BN_ECUDA, "cudaMalloc(%llu): %s", (unsigned long long)b, cudaGetErrorString(e));
+        }
+        bytes = b;
+        return BN_OK;
+    }
+    // Grow-only reallocation (contents not kept).
+    int reserve(bn_ctx* c, uint64_t b) { return (p && bytes >= b) ? BN_OK : alloc(c, b); }
+    template <class T>
+    T* at(uint64_t off = 0) const {
+        return reinterpret_cast<T*>(static_cast<char*>(p) + off);
+    }
+};
+
+struct PinnedMem {
+    void* p = nullptr;
+    uint64_t bytes = 0;
+    ~PinnedMem() {
+        if (p) cudaFreeHost(p);
+    }
+    int reserve(uint64_t b) {
+        if (p && bytes >= b) return BN_OK;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+        CU(cudaMallocHost(&p, b));
+        bytes = b;
+        return BN_OK;
+    }
+    template <class T>
+    T* at(uint64_t off = 0) const {
+        return reinterpret_cast<T*>(static_cast<char*>(p) + off);
+    }
+};
+
+// Bump allocator computing sub-buffer offsets (256-byte aligned).
+struct Layout {
+    uint64_t off = 0;
+    template <class T>
+    uint64_t take(uint64_t count) {
+        off = align_up(off, 256);
+        uint64_t o = off;
+        off += count * sizeof(T);
+        return o;
+    }
+};
+
+// Resident corpus: a flat cluster, or all IVF lists concatenated.
+struct Corpus {
+    uint64_t rows = 0;
+    uint32_t n = N, n1 = 128;
+    DevMem m_enc, al_cm, h_cm;
+    bool client = false;
+    DevMem L, mp_cm, s_ell, s_off, s_w, ids;
+    CUtensorMap tmap_m;  // m_enc as bytes {8192, rows}, 128x128 boxes, 128-byte swizzle
+
+    // Byte-planar operands of block scoring (built on first use, see
+    // bn_block.cu): m_enc planes [rows*8][1024], [AL | H] planes
+    // [rows*8][k_alh], [M | S] as signed bytes [rows][2048], corr[rows].
+    bool block_ready = false;
+    DevMem mp8, alh8, ms8, corr;
+    uint32_t k_alh = 0;
+    CUtensorMap tmap_mp, tmap_alh, tmap_ms;
+
+    uint64_t bytes() const {
+        return m_enc.bytes + al_cm.bytes + h_cm.bytes + L.bytes + mp_cm.bytes + s_ell.bytes + s_off.bytes + s_w.bytes +
+               ids.bytes + mp8.bytes + alh8.bytes + ms8.bytes + corr.bytes;
+    }
+};
+
+// Handle-side state shared by flat and IVF.
+struct Engine {
+    bn_ctx* ctx = nullptr;
+    Corpus c;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    DevMem ws;
+    PinnedMem host;
+};
+
+// Block scoring (bn_block.cu).
+struct BlockPlan;
+void block_plan_free(BlockPlan* b);
+
+}  // namespace api
+}  // namespace bn
+
+// ------------------------------------------------------------------ handles
+struct bn_flat {
+    bn::api::Engine e;
+    uint64_t m = 0;
+    // block plan cached by the host-buffer block entry points
+    bn::api::BlockPlan* block_cache = nullptr;
+    uint32_t cache_B = 0, cache_trials = 0, cache_k = 0, cache_flags = 0;
+    std::mutex block_mu;
+    ~bn_flat() {
+        if (block_cache) bn::api::block_plan_free(block_cache);
+    }
+};
+
+struct bn_ivf {
+    bn::api::Engine e;
+    uint32_t nlist = 0;
+    std::vector<uint64_t> offsets;
+};
+
+
+namespace bn {
+namespace api {
+int block_prepare(bn_flat* f);
+constexpr uint32_t BLOCK_VERIFY_ONLY = 1u << 31;  // internal block_plan_create flag
+int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint32_t flags, BlockPlan** out);
+void block_plan_config(const BlockPlan* b, uint32_t cfg[4]);
+int block_plan_status(BlockPlan* b, uint32_t* flags);
+int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const uint32_t* d_t, const uint32_t* d_tn,
+                  const uint8_t* d_seed, uint32_t* d_ids, int64_t* d_scores, uint32_t* d_n, int32_t* d_failed,
+                  cudaStream_t s, uint64_t* d_mv_out);
+int block_query_host(BlockPlan& b, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                     const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed, uint32_t* ids, int64_t* scores,
+                     uint32_t* n_hits, int32_t* failed, uint64_t* mv_out);
+int block_verify_host(BlockPlan& b, const uint64_t* r, const uint64_t* v_enc, const uint8_t* seed, int32_t* failed,
+                      uint64_t* ur, uint64_t* zv);
+}  // namespace api
+}  // namespace bn

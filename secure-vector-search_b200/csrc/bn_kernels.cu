@@ -689,6 +689,53 @@ topk_merge_kernel(const int64_t* __restrict__ cand_s, const uint32_t* __restrict
     if (threadIdx.x == 0) out_n[q] = (uint32_t)keep;
 }
 
+// Top-k of precomputed residues: query q's row scores are to_signed(
+// mv[q * ld + i]) for i < rows, ids[i] (or i).  Same per-CTA candidate
+// buffers as decode_topk_kernel, merged by topk_merge_kernel.
+__global__ void __launch_bounds__(DT_THREADS)
+topk_rows_kernel(const uint64_t* __restrict__ mv, uint64_t ld, uint64_t rows, const uint32_t* __restrict__ ids,
+                 uint32_t k, int64_t* __restrict__ cand_s, uint32_t* __restrict__ cand_i,
+                 uint32_t* __restrict__ cand_n) {
+    const uint32_t q = blockIdx.y;
+    __shared__ TopkBuf buf;
+    if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
+    __syncthreads();
+    const uint64_t per = ((rows + gridDim.x - 1) / gridDim.x + 1) & ~1ull;
+    const uint64_t v_begin = min(rows, (uint64_t)blockIdx.x * per);
+    const uint64_t v_end = min(rows, v_begin + per);
+    const uint64_t* src = mv + (uint64_t)q * ld;
+    for (uint64_t tile = v_begin; tile < v_end; tile += 2 * DT_THREADS) {
+        const uint64_t i0 = tile + 2 * threadIdx.x;
+        bool valid[2] = {i0 < v_end, i0 + 1 < v_end};
+        int64_t sc[2] = {0, 0};
+        uint32_t id[2] = {0, 0};
+        if (valid[1]) {  // v_begin and per are even: the pair is 16-byte aligned
+            const ulonglong2 w = *reinterpret_cast<const ulonglong2*>(src + i0);
+            sc[0] = to_signed(w.x);
+            sc[1] = to_signed(w.y);
+        } else if (valid[0]) {
+            sc[0] = to_signed(src[i0]);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) id[h] = valid[h] ? (ids ? ids[i0 + h] : (uint32_t)(i0 + h)) : 0;
+        const int64_t ts = buf.thr_s;
+        const uint32_t ti = buf.thr_i;
+        const int ht = buf.have_thr;
+        topk_offer(buf, valid[0], sc[0], id[0], ts, ti, ht);
+        topk_offer(buf, valid[1], sc[1], id[1], ts, ti, ht);
+        __syncthreads();
+        if (buf.cnt > CAND_CAP - 2 * DT_THREADS) topk_compact(buf, (int)k);
+    }
+    topk_compact(buf, (int)k);
+    const int keep = min(buf.cnt, (int)k);
+    const uint64_t slot = (uint64_t)q * gridDim.x + blockIdx.x;
+    for (int i = threadIdx.x; i < keep; i += blockDim.x) {
+        cand_s[slot * k + i] = buf.s[i];
+        cand_i[slot * k + i] = buf.id[i];
+    }
+    if (threadIdx.x == 0) cand_n[slot] = (uint32_t)keep;
+}
+
 // ------------------------------------------------------------------ keygen GEMM
 constexpr int GT = 64;   // output tile
 constexpr int GK = 16;   // K chunk
@@ -892,6 +939,16 @@ void launch_decode_topk(const uint64_t* d_r, const uint64_t* d_al_cm, const uint
     decode_topk_kernel<<<grid, DT_THREADS, 2 * 32 * n1, s>>>(d_r, d_al_cm, d_h_cm, d_mp_cm, d_s_ell, d_s_off, d_s_w, d_ids,
                                                    total_rows, n1, d_segs, d_q, d_v, d_g, d_x, d_t, d_t_nnz, k,
                                                    scratch.cand_s, scratch.cand_i, scratch.cand_n, d_mv_out);
+    topk_merge_kernel<<<nq, DT_THREADS, 0, s>>>(scratch.cand_s, scratch.cand_i, scratch.cand_n, ctas_per_query, k,
+                                                d_out_ids, d_out_scores, d_out_n);
+}
+
+void launch_topk_rows(const uint64_t* d_mv, uint64_t ld, uint64_t rows, uint32_t nq, const uint32_t* d_ids, uint32_t k,
+                      int ctas_per_query, TopkScratch scratch, uint32_t* d_out_ids, int64_t* d_out_scores,
+                      uint32_t* d_out_n, cudaStream_t s) {
+    if (!nq) return;
+    topk_rows_kernel<<<dim3(ctas_per_query, nq), DT_THREADS, 0, s>>>(d_mv, ld, rows, d_ids, k, scratch.cand_s,
+                                                                   scratch.cand_i, scratch.cand_n);
     topk_merge_kernel<<<nq, DT_THREADS, 0, s>>>(scratch.cand_s, scratch.cand_i, scratch.cand_n, ctas_per_query, k,
                                                 d_out_ids, d_out_scores, d_out_n);
 }

@@ -15,74 +15,13 @@
 #include <cudaTypedefs.h>
 
 #include "bn_tc.cuh"
+#include "bn_tcgen05.cuh"
 
 namespace bn {
 
 namespace {
 
-constexpr unsigned FULLMASK = 0xffffffffu;
-constexpr long long TC_WAIT_CYCLES = 2000000000ll;  // ~1 s
-
-__device__ __forceinline__ uint32_t su32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
-
-__device__ __forceinline__ void bar_init(uint64_t* b, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(su32(b)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity) {
-    const long long t0 = clock64();
-    while (!bar_try(b, parity))
-        if (clock64() - t0 > TC_WAIT_CYCLES) return false;
-    return true;
-}
-__device__ __forceinline__ void bar_arrive(uint64_t* b) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
-}
-__device__ __forceinline__ void bar_expect_tx(uint64_t* b, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* b) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-            su32(dst)),
-        "l"(map), "r"(x), "r"(y), "r"(su32(b))
-        : "memory");
-}
-__device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// Shared-memory matrix descriptor: 128-byte swizzle, sm_100 version 1.
-__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((saddr >> 4) & 0x3fff) | ((uint64_t)((lbo >> 4) & 0x3fff) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3fff) << 32) | (1ull << 46) | (2ull << 61);
-}
-
-__device__ __forceinline__ void mma_i8(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(d),
-        "l"(a), "l"(b), "r"(idesc), "r"(acc)
-        : "memory");
-}
-__device__ __forceinline__ void mma_commit(uint64_t* b) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(su32(b)) : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
+using namespace tcg;
 
 // ------------------------------------------------------------------ u draws
 constexpr int UG_THREADS = 352;  // >= 20 trials x 17 keystream blocks: one block per thread
@@ -92,8 +31,8 @@ __device__ __forceinline__ uint32_t ug_idx(uint32_t i) { return i + (i >> 4); }
 __global__ void __launch_bounds__(UG_THREADS)
 tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ blocks, const ChaChaKey* __restrict__ keys,
                const uint64_t* __restrict__ r, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows,
-               uint8_t* __restrict__ u_out, uint64_t* __restrict__ ur_part, uint32_t trials_total,
-               uint32_t* __restrict__ flags) {
+               uint8_t* __restrict__ u_out, uint64_t u_row_pitch, uint64_t* __restrict__ ur_part,
+               uint32_t trials_total, uint32_t* __restrict__ flags) {
     const uint32_t blk = blockIdx.x;
     const TcBlock tb = blocks[blk];
     const VerifySeg vs = vsegs[tb.seg];
@@ -124,7 +63,10 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
     __syncthreads();
     // U tile image: row (t, b) holds byte b of u_t[i] for the 128 rows i.
     // Thread (t, chunk) reads its 16 draws once and writes all 8 byte rows.
-    uint8_t* dst = u_out + (uint64_t)blk * n_rows * TC_ROWS;
+    // per-block image: rows of 128 bytes, blocks n_rows * 128 apart; flat
+    // image: rows u_row_pitch apart, this block at byte column r0 + i0
+    const uint64_t pitch = u_row_pitch ? u_row_pitch : TC_ROWS;
+    uint8_t* dst = u_row_pitch ? u_out + vs.r0 + tb.i0 : u_out + (uint64_t)blk * n_rows * TC_ROWS;
     for (uint32_t c = threadIdx.x; c < t_cnt * (TC_ROWS / 16); c += blockDim.x) {
         const uint32_t tl = c / (TC_ROWS / 16), ch = c % (TC_ROWS / 16);
         uint64_t x[16];
@@ -135,12 +77,12 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
             uint32_t wv[4] = {0, 0, 0, 0};
 #pragma unroll
             for (int q = 0; q < 16; ++q) wv[q >> 2] |= (uint32_t)((x[q] >> (8 * b)) & 0xffu) << (8 * (q & 3));
-            reinterpret_cast<uint4*>(dst + (uint64_t)(tl * 8 + b) * TC_ROWS)[ch] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+            reinterpret_cast<uint4*>(dst + (uint64_t)(tl * 8 + b) * pitch)[ch] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
         }
     }
     for (uint32_t c = threadIdx.x; c < (n_rows - 8 * t_cnt) * (TC_ROWS / 16); c += blockDim.x) {  // zero pad rows
         const uint32_t row = 8 * t_cnt + c / (TC_ROWS / 16), ch = c % (TC_ROWS / 16);
-        reinterpret_cast<uint4*>(dst + (uint64_t)row * TC_ROWS)[ch] = make_uint4(0, 0, 0, 0);
+        reinterpret_cast<uint4*>(dst + (uint64_t)row * pitch)[ch] = make_uint4(0, 0, 0, 0);
     }
     // u_t . r over this block's rows (skipped when r is not known yet)
     if (!r) return;
@@ -164,7 +106,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constant__ CUtensorMap tmap_u,
                     const TcPanel* __restrict__ panels, uint32_t npanels, uint32_t t_base, uint32_t t_cnt,
                     uint32_t n_rows, uint32_t trials_total, uint32_t stages, uint32_t stage_bytes,
-                    uint64_t* __restrict__ z_part, uint32_t* __restrict__ err) {
+                    uint64_t* __restrict__ z_part, uint32_t* __restrict__ err, int u_flat) {
     extern __shared__ uint8_t tc_dyn[];
     __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b;
     __shared__ uint32_t tmem_base_s;
@@ -224,7 +166,10 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
                         for (uint32_t s = 0; s < sg; ++s)
                             tma_2d(sb + s * STRIP_BYTES, &tmap_m, (int)((g * S + s) * 128), (int)(pn.row0 + rb * TC_ROWS),
                                    &full_b[st]);
-                        tma_2d(sb + u_off, &tmap_u, 0, (int)((pn.rb0 + rb) * n_rows), &full_b[st]);
+                        if (u_flat)
+                            tma_2d(sb + u_off, &tmap_u, (int)((pn.rb0 + rb) * TC_ROWS), 0, &full_b[st]);
+                        else
+                            tma_2d(sb + u_off, &tmap_u, 0, (int)((pn.rb0 + rb) * n_rows), &full_b[st]);
                     }
                 }
             }
@@ -599,18 +544,6 @@ tc_rreduce_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict
     }
 }
 
-__device__ __forceinline__ uint64_t block_sum_mod256(uint64_t v, uint64_t* sh) {
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) v = add_mod(v, __shfl_xor_sync(FULLMASK, v, off));
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-    __syncthreads();
-    uint64_t t = 0;
-    if (threadIdx.x == 0)
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = add_mod(t, sh[w]);
-    return t;
-}
-
 // CTA (trial t, y, segment): y < 8 sums z over the segment's panels for the
 // 128 columns [128y, 128y+128) and writes that chunk's share of z_t . v;
 // y == 8 sums the u_t . r partials of the segment's row blocks.
@@ -684,15 +617,16 @@ cudaError_t make_tmap_u8(CUtensorMap* map, const void* base, uint64_t inner_byte
 
 void launch_tc_ugen(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const ChaChaKey* d_keys,
                     const uint64_t* d_r, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint8_t* d_u,
-                    uint64_t* d_ur_part, uint32_t trials_total, uint32_t* d_flags, cudaStream_t s) {
+                    uint64_t* d_ur_part, uint32_t trials_total, uint32_t* d_flags, cudaStream_t s,
+                    uint64_t u_row_pitch) {
     if (!nblocks) return;
-    tc_ugen_kernel<<<nblocks, UG_THREADS, 0, s>>>(d_vsegs, d_blocks, d_keys, d_r, t_base, t_cnt, n_rows, d_u, d_ur_part,
-                                                  trials_total, d_flags);
+    tc_ugen_kernel<<<nblocks, UG_THREADS, 0, s>>>(d_vsegs, d_blocks, d_keys, d_r, t_base, t_cnt, n_rows, d_u,
+                                                  u_row_pitch, d_ur_part, trials_total, d_flags);
 }
 
 void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
                          uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
-                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s) {
+                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s, int u_flat) {
     if (!npanels) return;
     const int S = n_rows <= 128 ? 4 : 3;
     const uint32_t stage_bytes = (uint32_t)S * STRIP_BYTES + ((n_rows * TC_ROWS + 1023u) & ~1023u);
@@ -704,11 +638,11 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
     if (S == 4) {
         cudaFuncSetAttribute(tc_freivalds_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         tc_freivalds_kernel<4><<<grid, TC_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, t_base, t_cnt, n_rows,
-                                                              trials_total, stages, stage_bytes, d_z_part, d_err);
+                                                              trials_total, stages, stage_bytes, d_z_part, d_err, u_flat);
     } else {
         cudaFuncSetAttribute(tc_freivalds_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         tc_freivalds_kernel<3><<<grid, TC_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, t_base, t_cnt, n_rows,
-                                                              trials_total, stages, stage_bytes, d_z_part, d_err);
+                                                              trials_total, stages, stage_bytes, d_z_part, d_err, u_flat);
     }
 }
 

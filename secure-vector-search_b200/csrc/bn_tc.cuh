@@ -48,17 +48,23 @@ cudaError_t make_tmap_u8(CUtensorMap* map, const void* base, uint64_t inner_byte
 // B operand image, un-swizzled; TMA applies the swizzle) for trials
 // [t_base, t_base + t_cnt), padded with zero rows up to n_rows = 8 * t_pad,
 // and u_t . r partial sums per block.  *flags bit 0: a draw hit p.
+// u_row_pitch = 0: per-block images (block b at d_u + b * n_rows * 128);
+// otherwise one flat image, row (t,b) at d_u + (t*8+b) * u_row_pitch and the
+// draw for r index x at byte column x (x = segment r0 + row).
 void launch_tc_ugen(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const ChaChaKey* d_keys,
                     const uint64_t* d_r, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint8_t* d_u,
-                    uint64_t* d_ur_part, uint32_t trials_total, uint32_t* d_flags, cudaStream_t s);
+                    uint64_t* d_ur_part, uint32_t trials_total, uint32_t* d_flags, cudaStream_t s,
+                    uint64_t u_row_pitch = 0);
 
 // The GEMM + drain: z_part[panel][t_base + t][j] (canonical residues) for
 // t < t_cnt.  tmap_m: m_enc bytes {8192, rows}, box {128, 128}, swizzle 128B;
-// tmap_u: U bytes {128, nblocks * n_rows}, box {128, n_rows}, swizzle 128B.
+// tmap_u: U bytes {128, nblocks * n_rows}, box {128, n_rows}, swizzle 128B
+// (u_flat = 0), or the flat image {row pitch, n_rows}, box {128, n_rows}
+// (u_flat = 1; panel rb0 = first row / 128).
 // *err: bit 2/3/4 set when a bounded pipeline wait timed out.
 void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
                          uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
-                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s);
+                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s, int u_flat = 0);
 
 // Fused single pass over m_enc for the first <= 20 trials: z_part as above
 // plus r_part[group][r index] (S-strip group partial dots with the query,
