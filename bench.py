@@ -4,9 +4,12 @@ Default workload (one GPU): flat corpus N = 1,000,000, d = 768 (padded to
 n = 1024), int8 data mapped into F_p and BN-encrypted, one query per step
 with Protocol 2 (Freivalds, 20 trials) fused into the same launch sequence,
 then on-device decode and top-10.  A step = one query through the whole
-server + client path.
+server + client path.  After it, block scoring (B = 8, 32, 128, 512 queries per
+launch as tensor-core GEMMs with Protocol 2 per block) is timed on the same
+corpus and reported under "block" in the same JSON line.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--block-sizes 8,32,128,512]
 
 --impl reference times the reference's CPU path (the CPU restatement under
 oracle/) on the host cores over a bounded sample of the same workload.
@@ -269,9 +272,121 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     }
     plans["full"].close()
     plans["noverify"].close()
+    if args.block_sizes:
+        res["block"] = run_block(args, flat, L, seed, dev, stream, res["value"], dist)
     flat.close()
     ctx.close()
     return res
+
+
+def run_block(args, flat, L, seed, dev, stream, single_qps, dist):
+    """Block scoring (B queries per launch, tensor-core GEMMs, Protocol 2 per
+    block): each timed step is one CUDA-graph replay of G consecutive blocks
+    with distinct inputs; ~10,240 queries per block size (bounded)."""
+    import torch
+
+    from bn_b200 import capi
+
+    d, k, trials = 768, 10, args.trials
+    sizes = [int(b) for b in args.block_sizes.split(",") if b]
+    pool = max(sizes) * 4
+    qv = to_residues(synth_int8(pool, d, seed + 2000))
+    encs = [capi.host_encode_query(qv[i], L, capi.host_derive_h_seed(seed ^ 0x424C4B, i)) for i in range(pool)]
+    t_arr = np.zeros((pool, N_DIM), np.uint32)
+    tn = np.zeros(pool, np.uint32)
+    for i, (ve, g, ti, ts) in enumerate(encs):
+        tn[i] = ti.size
+        t_arr[i, : ti.size] = ti | np.where(ts < 0, np.uint32(0x80000000), np.uint32(0))
+    d_v = torch.from_numpy(np.stack([e[0] for e in encs]).view(np.int64)).to(dev)
+    d_g = torch.from_numpy(np.stack([e[1] for e in encs]).view(np.int64)).to(dev)
+    d_t = torch.from_numpy(t_arr.view(np.int32)).to(dev)
+    d_tn = torch.from_numpy(tn.view(np.int32)).to(dev)
+    seeds = torch.from_numpy(np.frombuffer(b"".join(bytes([j + 1]) * 32 for j in range(8)), np.uint8).copy()).to(dev)
+    d_ids = torch.zeros((pool, k), dtype=torch.int32, device=dev)
+    d_sc = torch.zeros((pool, k), dtype=torch.int64, device=dev)
+    d_n = torch.zeros(pool, dtype=torch.int32, device=dev)
+    d_f = torch.full((pool,), 7, dtype=torch.int32, device=dev)
+    flat.block_prepare()
+    out = {"trials": trials, "k": k, "freivalds": "one seed per block, every query checked", "per_B": {}}
+    peak_tops = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak_tops = 2.0 * float(json.load(f)["bf16_tflops"])  # dense int8 rate = 2x dense bf16 on sm_100
+    except (OSError, KeyError, ValueError):
+        peak_tops = 2.0 * 1590.0
+    best = None
+    for B in sizes:
+        plan = flat.block_plan(B, trials, k, autotune=True)
+        cfg = plan.block_config()
+        G = max(1, min(4, pool // B))
+        reps = max(args.warmup + 1, min(10240 // B, 1280) // G)
+
+        def ptrs(j):
+            o = j * B
+            return (d_v[o].data_ptr(), d_g[o].data_ptr(), d_t[o].data_ptr(), d_tn[o : o + 1].data_ptr(),
+                    seeds[32 * j : 32 * (j + 1)].data_ptr(), d_ids[o].data_ptr(), d_sc[o].data_ptr(),
+                    d_n[o : o + 1].data_ptr(), d_f[o : o + 1].data_ptr())
+
+        with torch.cuda.stream(stream):
+            for j in range(G):
+                plan.enqueue(*ptrs(j), stream.cuda_stream)
+        stream.synchronize()
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            for j in range(G):
+                plan.enqueue(*ptrs(j), torch.cuda.current_stream().cuda_stream)
+        for _ in range(args.warmup):
+            graph.replay()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(reps):
+            graph.replay()
+        ev1.record()
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        del graph
+        status = plan.status()
+        fl = d_f[: G * B].cpu().numpy()
+        assert status == 0 and np.all(fl == -1), "block verification failed on honest responses"
+        nq = reps * G * B
+        qps = (dist.get_world_size() if dist else 1) * nq / (ms / 1e3)
+        macs = flat.m * 8 * 8 * B * N_DIM  # byte-planar r = M_enc v GEMM
+        gemm_tops = 2 * macs / (cfg["tuned_scan_ms"] / 1e3) / 1e12 if cfg["tuned_scan_ms"] else None
+        out["per_B"][str(B)] = {"qps": qps, "ms_per_block": ms / (reps * G), "queries_timed": nq, "graph_blocks": G,
+                                "tiling": {kk: cfg[kk] for kk in ("w_tile", "stages", "order", "k_panel")},
+                                "scan_gemm_ms": cfg["tuned_scan_ms"], "scan_gemm_tops": gemm_tops}
+        if best is None or qps > best[1]:
+            best = (B, qps, gemm_tops)
+        plan.close()
+    out["best"] = {"B": best[0], "qps": best[1], "vs_single_query": best[1] / single_qps}
+    if best[2]:
+        out["roofline"] = {"kernel": f"bgemm r = M_enc v (B={best[0]})", "bound": "tensor", "achieved": best[2],
+                           "peak": peak_tops, "unit": "TOP/s int8", "frac": best[2] / peak_tops,
+                           "peak_source": "2 x measured dense bf16 (int8 tensor rate on sm_100)"}
+    # e2e through the C ABI with host buffers (pack + H2D + block pipeline + D2H of hits)
+    B = 32 if 32 in sizes else sizes[0]
+    vb = np.stack([e[0] for e in encs[:B]])
+    gb = np.stack([e[1] for e in encs[:B]])
+    tb = [(e[2], e[3]) for e in encs[:B]]
+    for _ in range(2):
+        flat.query_block(vb, gb, tb, bytes([1]) * 32, trials, k)
+    reps = 20
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        hits, fl, _ = flat.query_block(vb, gb, tb, bytes([1]) * 32, trials, k)
+    e2e_s = (time.perf_counter() - t0) / reps
+    assert np.all(fl == -1)
+    h2d = B * (N_DIM * 8 + 128 * 8 + 4 * N_DIM + 4) + 32
+    out["e2e"] = {"B": B, "value": B / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+                  "d2h_bytes_per_step": B * (k * 12 + 8)}
+    return out
 
 
 def main():
@@ -283,6 +398,8 @@ def main():
     ap.add_argument("--rows", type=int, default=1_000_000)
     ap.add_argument("--trials", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--block-sizes", default="8,32,128,512",
+                    help="block scoring sizes B to time after the single-query metric ('' to skip)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

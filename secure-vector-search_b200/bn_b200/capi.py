@@ -68,7 +68,7 @@ _SIGS = {
     "bn_plan_destroy": (C.c_int, [vp]),
     "bn_flat_block_prepare": (C.c_int, [vp]),
     "bn_flat_block_plan": (C.c_int, [vp, u32, u32, u32, u32, vp]),
-    "bn_plan_block_config": (C.c_int, [vp, vp]),
+    "bn_plan_block_config": (C.c_int, [vp, vp, vp]),
     "bn_plan_enqueue_block": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "bn_flat_query_block": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
     "bn_flat_verify_block": (C.c_int, [vp, u32, vp, vp, vp, u32, vp, vp, vp]),
@@ -309,8 +309,10 @@ class Plan:
 
     def block_config(self):
         cfg = np.zeros(4, np.uint32)
-        check(lib.bn_plan_block_config(self.h, ptr(cfg)))
-        return {"w_tile": int(cfg[0]), "stages": int(cfg[1]), "order": int(cfg[2]), "k_panel": int(cfg[3])}
+        ms = np.zeros(2, np.float32)
+        check(lib.bn_plan_block_config(self.h, ptr(cfg), ptr(ms)))
+        return {"w_tile": int(cfg[0]), "stages": int(cfg[1]), "order": int(cfg[2]), "k_panel": int(cfg[3]),
+                "tuned_scan_ms": float(ms[0]), "tuned_ur_ms": float(ms[1])}
 
     def enqueue_scan(self, d_v, d_r, stream: int):
         check(lib.bn_plan_enqueue_scan(self.h, d_v, d_r, stream))

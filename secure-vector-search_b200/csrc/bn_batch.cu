@@ -185,10 +185,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         packed |= __shfl_xor_sync(FULLMASK, packed, 8);
                         packed |= __shfl_xor_sync(FULLMASK, packed, 16);
                         if (y < p.y_count) {
-                            if (a == 0 && x < p.x_count) {
-                                uint64_t* dst = out + (uint64_t)y * p.out_ld + x;
-                                *dst = p.accumulate ? add_mod(*dst, f) : f;
-                            }
+                            if (a == 0 && x < p.x_count) out[(uint64_t)y * p.out_ld + x] = f;
                             if (p.planar_out && lane < 8 && x4 < p.x_count)
                                 *reinterpret_cast<uint32_t*>(p.planar_out + ((uint64_t)y * 8 + lane) * p.planar_ld + x4) =
                                     packed;
@@ -214,10 +211,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         const uint64_t lr = lo < 0 ? (uint64_t)(lo + (int64_t)P) : (uint64_t)lo;
                         const uint64_t hr = hi < 0 ? (uint64_t)(hi + (int64_t)P) : (uint64_t)hi;
                         const uint64_t f = add_mod(canon(lr + rotl61(hr, 32)), corr);
-                        if (xv && y < p.y_count) {
-                            uint64_t* dst = p.out + (uint64_t)y * p.out_ld + x;
-                            *dst = sub_mod(*dst, f);
-                        }
+                        if (xv && y < p.y_count) p.out[(uint64_t)y * p.out_ld + x] = f;
                     }
                 }
             }

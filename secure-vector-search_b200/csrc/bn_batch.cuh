@@ -27,11 +27,11 @@ constexpr uint32_t BG_MAX_KPANEL = 16384;  // K bytes summed in s32 before a dra
 
 enum BgMode : int {
     // u8 x u8; A rows (x, a), W rows (y, b); f(x, y) = sum 2^(8(a+b)) D mod p.
-    // out[kp * out_pstride + y * out_ld + x] = f (accumulate = 0) or += f.
+    // out[kp * out_pstride + y * out_ld + x] = f.
     // planar_out (nullable): byte a of f at planar_out[(y * 8 + a) * planar_ld + x].
     BG_PLANAR = 0,
     // s8 x s8; A rows x, W rows (y, b); f(x, y) = sum_b 2^(8b) D mod p.
-    // out[y * out_ld + x] -= f + corr[x].
+    // out[y * out_ld + x] = f + corr[x].
     BG_S8 = 1,
 };
 
@@ -47,7 +47,6 @@ struct BgParams {
     uint64_t* out;
     uint64_t out_ld;
     uint64_t out_pstride;  // per K panel (PLANAR)
-    int accumulate;
     const uint64_t* corr;  // S8
     uint8_t* planar_out;   // PLANAR, nullable
     uint64_t planar_ld;

@@ -38,10 +38,11 @@ struct BlockPlan {
     uint32_t nblocks = 0, npanels = 0;  // U row blocks, z panels (4096 rows)
     // tuned GEMM configuration
     uint32_t w_tile = 256, stages = 4, order = 0, k_panel4 = 16384;
+    float tuned_ms[2] = {0.f, 0.f};  // autotuner's best G1 and G4 launch times
     int topk_ctas = 1;
     // workspace
     DevMem ws;
-    uint64_t o_err, o_bad, o_vseg, o_blocks, o_panels, o_vp, o_gx, o_tv, o_x, o_r, o_rp, o_ub, o_zpart, o_z, o_zv,
+    uint64_t o_err, o_bad, o_vseg, o_blocks, o_panels, o_vp, o_gx, o_tv, o_x, o_r, o_f2, o_f3, o_rp, o_ub, o_zpart, o_z, o_zv,
         o_urpart, o_ur, o_fail, o_cs, o_ci, o_cn, o_in, o_in_v, o_in_g, o_in_t, o_in_tn, o_in_seed, o_out_ids,
         o_out_sc, o_out_n, o_out_end;
     CUtensorMap tm_vp, tm_gx, tm_tv, tm_rp, tm_ub;
@@ -176,6 +177,7 @@ int autotune(BlockPlan& b, cudaStream_t s) {
     b.w_tile = bw;
     b.stages = bs;
     b.order = bo;
+    b.tuned_ms[0] = best / 2;  // two timed launches per candidate
     if (rc == BN_OK && b.trials) {  // K panel of the u . r GEMM
         float bestk = 1e30f;
         uint32_t bk = b.k_panel4;
@@ -209,6 +211,7 @@ int autotune(BlockPlan& b, cudaStream_t s) {
             if (ms < bestk) { bestk = ms; bk = kp; }
         }
         b.k_panel4 = bk;
+        b.tuned_ms[1] = bestk / 2;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -265,7 +268,9 @@ int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint3
     b->o_gx = L.take<uint8_t>(8ull * qb * c.k_alh);
     b->o_tv = L.take<uint8_t>(8ull * qb * 2 * N);
     b->o_x = L.take<uint64_t>(qb * c.n1);
-    b->o_r = L.take<uint64_t>((uint64_t)B * b->nld);
+    b->o_r = L.take<uint64_t>((uint64_t)B * b->nld);    // r = M_enc v
+    b->o_f2 = L.take<uint64_t>(qb * b->nld);             // -(AL g + H x)
+    b->o_f3 = L.take<uint64_t>(qb * b->nld);             // M T + S v   (Mv = r + f2 - f3)
     b->o_rp = L.take<uint8_t>(8ull * B * b->npad);
     b->o_ub = L.take<uint8_t>(trials ? (uint64_t)b->n_rows * b->npad : 0);
     b->o_zpart = L.take<uint64_t>(trials ? (uint64_t)b->npanels * tt * N : 0);
@@ -327,11 +332,15 @@ int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint3
     return BN_OK;
 }
 
-void block_plan_config(const BlockPlan* b, uint32_t cfg[4]) {
+void block_plan_config(const BlockPlan* b, uint32_t cfg[4], float tuned_ms[2]) {
     cfg[0] = b->w_tile;
     cfg[1] = b->stages;
     cfg[2] = b->order;
     cfg[3] = b->k_panel4;
+    if (tuned_ms) {
+        tuned_ms[0] = b->tuned_ms[0];
+        tuned_ms[1] = b->tuned_ms[1];
+    }
 }
 
 int block_plan_status(BlockPlan* b, uint32_t* flags) {
@@ -384,7 +393,7 @@ static void enqueue_verify(BlockPlan& b, const uint64_t* d_v, const uint8_t* d_s
 
 int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const uint32_t* d_t, const uint32_t* d_tn,
                   const uint8_t* d_seed, uint32_t* d_ids, int64_t* d_scores, uint32_t* d_n, int32_t* d_failed,
-                  cudaStream_t s, uint64_t* d_mv_out) {
+                  cudaStream_t s, bool want_mv) {
     if (b.verify_only) return fail(BN_EINVAL, "verification-only block plan");
     if (!d_v || !d_g || !d_t || !d_tn || !d_failed || (b.trials && !d_seed) || (b.k && (!d_ids || !d_scores || !d_n)))
         return fail(BN_EINVAL, "null device pointer");
@@ -399,6 +408,7 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     uint64_t* x = reinterpret_cast<uint64_t*>(d + b.o_x);
     uint64_t* r = reinterpret_cast<uint64_t*>(d + b.o_r);
     uint8_t* rp = reinterpret_cast<uint8_t*>(d + b.o_rp);
+    if (b.k == 0 && !d_ids) d_ids = reinterpret_cast<uint32_t*>(d + b.o_out_ids);  // unused when k = 0
     // operands of this block
     launch_planar_rows(d_v, b.B, N, N, 0, vp, N, 0, s);
     launch_lt_times_v(c.L.at<uint64_t>(), c.n1, d_v, b.B, x, s);
@@ -410,13 +420,13 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     p.out = r;
     p.planar_out = rp;
     launch_bgemm(c.tmap_mp, b.tm_vp, p, b.stages, sms, err, s);
-    // G2: r += -(AL g + H x)
+    // G2: f2 = -(AL g + H x)
     p.k_bytes = c.k_alh;
     p.k_panel = c.k_alh;
-    p.accumulate = 1;
+    p.out = reinterpret_cast<uint64_t*>(d + b.o_f2);
     p.planar_out = nullptr;
     launch_bgemm(c.tmap_alh, b.tm_gx, p, b.stages, sms, err, s);
-    // G3: r -= M T + S v  ->  r = Mv
+    // G3: f3 = M T + S v
     BgParams q{};
     q.mode = BG_S8;
     q.a_tiles = (uint32_t)((c.rows + BG_AROWS - 1) / BG_AROWS);
@@ -426,20 +436,23 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     q.k_panel = 2 * N;
     q.x_count = (uint32_t)c.rows;
     q.y_count = b.B;
-    q.out = r;
+    q.out = reinterpret_cast<uint64_t*>(d + b.o_f3);
     q.out_ld = b.nld;
     q.corr = c.corr.at<uint64_t>();
     q.order_a_fast = (int)b.order;
     launch_bgemm(c.tmap_ms, b.tm_tv, q, b.stages, sms, err, s);
-    if (b.k) {
+    // Mv = r + f2 - f3 (written over f3 when asked for), fp_to_signed, top-k
+    if (b.k || want_mv) {
         TopkScratch ts{reinterpret_cast<int64_t*>(d + b.o_cs), reinterpret_cast<uint32_t*>(d + b.o_ci),
                        reinterpret_cast<uint32_t*>(d + b.o_cn)};
-        launch_topk_rows(r, b.nld, c.rows, b.B, nullptr, b.k, b.topk_ctas, ts, d_ids, d_scores, d_n, s);
+        const bool own = b.k == 0;  // only the residues wanted: ranks go to the plan's own buffers
+        launch_topk_rows(r, reinterpret_cast<uint64_t*>(d + b.o_f2), reinterpret_cast<uint64_t*>(d + b.o_f3), b.nld,
+                         c.rows, b.B, nullptr, own ? 1u : b.k, b.topk_ctas, ts,
+                         own ? reinterpret_cast<uint32_t*>(d + b.o_out_ids) : d_ids,
+                         own ? reinterpret_cast<int64_t*>(d + b.o_out_sc) : d_scores,
+                         own ? reinterpret_cast<uint32_t*>(d + b.o_out_n) : d_n,
+                         want_mv ? reinterpret_cast<uint64_t*>(d + b.o_f3) : nullptr, s);
     }
-    if (d_mv_out)
-        for (uint32_t q2 = 0; q2 < b.B; ++q2)
-            CU(cudaMemcpyAsync(d_mv_out + (uint64_t)q2 * c.rows, r + (uint64_t)q2 * b.nld, c.rows * 8,
-                               cudaMemcpyDeviceToDevice, s));
     if (b.trials) enqueue_verify(b, d_v, d_seed, d_failed, s);
     else CU(cudaMemsetAsync(d_failed, 0xff, (uint64_t)b.B * 4, s));
     CU(cudaGetLastError());
@@ -479,13 +492,13 @@ int block_query_host(BlockPlan& b, const uint64_t* v_enc, const uint64_t* g, con
                       reinterpret_cast<uint32_t*>(d + b.o_in_t), reinterpret_cast<uint32_t*>(d + b.o_in_tn),
                       reinterpret_cast<uint8_t*>(d + b.o_in_seed), reinterpret_cast<uint32_t*>(d + b.o_out_ids),
                       reinterpret_cast<int64_t*>(d + b.o_out_sc), reinterpret_cast<uint32_t*>(d + b.o_out_n),
-                      reinterpret_cast<int32_t*>(d + b.o_fail), s, nullptr));
+                      reinterpret_cast<int32_t*>(d + b.o_fail), s, mv_out != nullptr));
     int32_t* hf = reinterpret_cast<int32_t*>(h + (b.o_out_end - b.o_in));
     CU(cudaMemcpyAsync(at(b.o_out_ids), d + b.o_out_ids, b.o_out_end - b.o_out_ids, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(hf, d + b.o_fail, (uint64_t)B * 4, cudaMemcpyDeviceToHost, s));
     if (mv_out)
         for (uint32_t q = 0; q < B; ++q)
-            CU(cudaMemcpyAsync(mv_out + (uint64_t)q * c.rows, d + b.o_r + (uint64_t)q * b.nld * 8, c.rows * 8,
+            CU(cudaMemcpyAsync(mv_out + (uint64_t)q * c.rows, d + b.o_f3 + (uint64_t)q * b.nld * 8, c.rows * 8,
                                cudaMemcpyDeviceToHost, s));
     uint32_t flags[2] = {0, 0};
     CU(cudaMemcpyAsync(flags, d + b.o_err, 8, cudaMemcpyDeviceToHost, s));

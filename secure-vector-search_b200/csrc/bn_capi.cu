@@ -1030,10 +1030,10 @@ int bn_flat_block_plan(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint
     return BN_OK;
 }
 
-int bn_plan_block_config(const bn_plan* p, uint32_t config[4]) {
+int bn_plan_block_config(const bn_plan* p, uint32_t config[4], float tuned_ms[2]) {
     if (!p || !config) return fail(BN_EINVAL, "null argument");
     if (!p->block) return fail(BN_EINVAL, "not a block plan");
-    block_plan_config(p->block, config);
+    block_plan_config(p->block, config, tuned_ms);
     return BN_OK;
 }
 
@@ -1043,7 +1043,7 @@ int bn_plan_enqueue_block(bn_plan* p, const uint64_t* d_v, const uint64_t* d_g, 
     if (!p) return fail(BN_EINVAL, "null plan");
     if (!p->block) return fail(BN_EINVAL, "not a block plan: use bn_plan_enqueue");
     return block_enqueue(*p->block, d_v, d_g, d_t, d_t_nnz, d_block_seed, d_ids, d_scores, d_n, d_failed,
-                         static_cast<cudaStream_t>(stream), nullptr);
+                         static_cast<cudaStream_t>(stream), false);
 }
 
 static int cached_block_plan(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint32_t flags, BlockPlan** out) {

@@ -689,13 +689,16 @@ topk_merge_kernel(const int64_t* __restrict__ cand_s, const uint32_t* __restrict
     if (threadIdx.x == 0) out_n[q] = (uint32_t)keep;
 }
 
-// Top-k of precomputed residues: query q's row scores are to_signed(
-// mv[q * ld + i]) for i < rows, ids[i] (or i).  Same per-CTA candidate
-// buffers as decode_topk_kernel, merged by topk_merge_kernel.
+// Top-k of residues combined on the fly: query q's row i scores
+// to_signed(a + b - c) (b, c nullable) with a = ra[q * ld + i] etc., ids[i]
+// (or i); mv_out (nullable) receives the combined residues at the same
+// offsets.  Same per-CTA candidate buffers as decode_topk_kernel, merged by
+// topk_merge_kernel.
 __global__ void __launch_bounds__(DT_THREADS)
-topk_rows_kernel(const uint64_t* __restrict__ mv, uint64_t ld, uint64_t rows, const uint32_t* __restrict__ ids,
-                 uint32_t k, int64_t* __restrict__ cand_s, uint32_t* __restrict__ cand_i,
-                 uint32_t* __restrict__ cand_n) {
+topk_rows_kernel(const uint64_t* __restrict__ ra, const uint64_t* __restrict__ rb, const uint64_t* __restrict__ rc,
+                 uint64_t ld, uint64_t rows, const uint32_t* __restrict__ ids, uint32_t k,
+                 int64_t* __restrict__ cand_s, uint32_t* __restrict__ cand_i, uint32_t* __restrict__ cand_n,
+                 uint64_t* __restrict__ mv_out) {
     const uint32_t q = blockIdx.y;
     __shared__ TopkBuf buf;
     if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
@@ -703,21 +706,37 @@ topk_rows_kernel(const uint64_t* __restrict__ mv, uint64_t ld, uint64_t rows, co
     const uint64_t per = ((rows + gridDim.x - 1) / gridDim.x + 1) & ~1ull;
     const uint64_t v_begin = min(rows, (uint64_t)blockIdx.x * per);
     const uint64_t v_end = min(rows, v_begin + per);
-    const uint64_t* src = mv + (uint64_t)q * ld;
+    const uint64_t base = (uint64_t)q * ld;
     for (uint64_t tile = v_begin; tile < v_end; tile += 2 * DT_THREADS) {
         const uint64_t i0 = tile + 2 * threadIdx.x;
-        bool valid[2] = {i0 < v_end, i0 + 1 < v_end};
-        int64_t sc[2] = {0, 0};
-        uint32_t id[2] = {0, 0};
-        if (valid[1]) {  // v_begin and per are even: the pair is 16-byte aligned
-            const ulonglong2 w = *reinterpret_cast<const ulonglong2*>(src + i0);
-            sc[0] = to_signed(w.x);
-            sc[1] = to_signed(w.y);
-        } else if (valid[0]) {
-            sc[0] = to_signed(src[i0]);
+        const bool valid[2] = {i0 < v_end, i0 + 1 < v_end};
+        uint64_t mv[2] = {0, 0};
+        if (valid[0]) {  // v_begin, per and ld are even: the pair is 16-byte aligned and inside the row of ld
+            const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(ra + base + i0);
+            mv[0] = x.x;
+            mv[1] = x.y;
+            if (rb) {
+                const ulonglong2 y = *reinterpret_cast<const ulonglong2*>(rb + base + i0);
+                mv[0] = add_mod(mv[0], y.x);
+                mv[1] = add_mod(mv[1], y.y);
+            }
+            if (rc) {
+                const ulonglong2 z = *reinterpret_cast<const ulonglong2*>(rc + base + i0);
+                mv[0] = sub_mod(mv[0], z.x);
+                mv[1] = sub_mod(mv[1], z.y);
+            }
+            if (mv_out) {
+                mv_out[base + i0] = mv[0];
+                if (valid[1]) mv_out[base + i0 + 1] = mv[1];
+            }
         }
+        int64_t sc[2];
+        uint32_t id[2];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) id[h] = valid[h] ? (ids ? ids[i0 + h] : (uint32_t)(i0 + h)) : 0;
+        for (int h = 0; h < 2; ++h) {
+            sc[h] = to_signed(mv[h]);
+            id[h] = valid[h] ? (ids ? ids[i0 + h] : (uint32_t)(i0 + h)) : 0;
+        }
         const int64_t ts = buf.thr_s;
         const uint32_t ti = buf.thr_i;
         const int ht = buf.have_thr;
@@ -943,12 +962,13 @@ void launch_decode_topk(const uint64_t* d_r, const uint64_t* d_al_cm, const uint
                                                 d_out_ids, d_out_scores, d_out_n);
 }
 
-void launch_topk_rows(const uint64_t* d_mv, uint64_t ld, uint64_t rows, uint32_t nq, const uint32_t* d_ids, uint32_t k,
-                      int ctas_per_query, TopkScratch scratch, uint32_t* d_out_ids, int64_t* d_out_scores,
-                      uint32_t* d_out_n, cudaStream_t s) {
+void launch_topk_rows(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_c, uint64_t ld, uint64_t rows,
+                      uint32_t nq, const uint32_t* d_ids, uint32_t k, int ctas_per_query, TopkScratch scratch,
+                      uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n, uint64_t* d_mv_out,
+                      cudaStream_t s) {
     if (!nq) return;
-    topk_rows_kernel<<<dim3(ctas_per_query, nq), DT_THREADS, 0, s>>>(d_mv, ld, rows, d_ids, k, scratch.cand_s,
-                                                                   scratch.cand_i, scratch.cand_n);
+    topk_rows_kernel<<<dim3(ctas_per_query, nq), DT_THREADS, 0, s>>>(d_a, d_b, d_c, ld, rows, d_ids, k, scratch.cand_s,
+                                                                   scratch.cand_i, scratch.cand_n, d_mv_out);
     topk_merge_kernel<<<nq, DT_THREADS, 0, s>>>(scratch.cand_s, scratch.cand_i, scratch.cand_n, ctas_per_query, k,
                                                 d_out_ids, d_out_scores, d_out_n);
 }

@@ -114,11 +114,13 @@ void launch_decode_topk(const uint64_t* d_r, const uint64_t* d_al_cm, const uint
                         uint64_t* d_mv_out, uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n,
                         cudaStream_t s);
 
-// Top-k over precomputed residues mv[q * ld + i] (i < rows; ld even), ranked
-// by to_signed, ids[i] or i; outputs as launch_decode_topk.
-void launch_topk_rows(const uint64_t* d_mv, uint64_t ld, uint64_t rows, uint32_t nq, const uint32_t* d_ids, uint32_t k,
-                      int ctas_per_query, TopkScratch scratch, uint32_t* d_out_ids, int64_t* d_out_scores,
-                      uint32_t* d_out_n, cudaStream_t s);
+// Top-k over residues combined on the fly, mv = a + b - c at [q * ld + i]
+// (i < rows; ld even; b, c nullable), ranked by to_signed, ids[i] or i;
+// outputs as launch_decode_topk; d_mv_out (nullable) receives mv.
+void launch_topk_rows(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_c, uint64_t ld, uint64_t rows,
+                      uint32_t nq, const uint32_t* d_ids, uint32_t k, int ctas_per_query, TopkScratch scratch,
+                      uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n, uint64_t* d_mv_out,
+                      cudaStream_t s);
 
 // Keygen-side dense F_p GEMM: C[i][j] = sum_k A[i][k] * B[j][k]  (A: rows x K,
 // B: cols x K, both row-major), optionally C += D (same shape, row-major).
