@@ -8,7 +8,7 @@
 //   warp 1    MMA issuer: 4 x tcgen05.mma (M=128, N=w_tile, K=32) per stage
 //             into one of two TMEM accumulators (double-buffered across
 //             items), tcgen05.commit frees the stage / hands over the item
-//   warps 2-5 epilogue: tcgen05.ld, byte-weight recombination mod p, stores
+//   warps 2-9 epilogue: tcgen05.ld, byte-weight recombination mod p, stores
 // Every mbarrier wait is bounded; on timeout the CTA sets *err and winds down
 // (waits for its own copies and MMAs, frees TMEM) instead of hanging.
 #include <cudaTypedefs.h>
@@ -25,7 +25,8 @@ namespace {
 
 using namespace tcg;
 
-constexpr int BG_THREADS = 192;
+constexpr int BG_EPI_WARPS = 8;
+constexpr int BG_THREADS = 64 + 32 * BG_EPI_WARPS;  // TMA warp, MMA warp, epilogue warps
 
 struct ItemIdx {
     uint32_t kp, ta, tw;
@@ -37,21 +38,42 @@ __device__ __forceinline__ ItemIdx item_idx(const BgParams& p, uint32_t item) {
     return ItemIdx{kp, rem / p.w_tiles, rem % p.w_tiles};
 }
 
+// The j-th work item of this CTA.  Streaming mode: global items blockIdx.x +
+// j * gridDim.x.  A-resident mode: this CTA owns A tiles blockIdx.x + t *
+// gridDim.x and visits every W tile of each (j = t * w_tiles + tw).
+__device__ __forceinline__ bool item_at(const BgParams& p, uint32_t items, uint32_t j, ItemIdx& ix) {
+    if (p.a_resident) {
+        const uint32_t ta = blockIdx.x + (j / p.w_tiles) * gridDim.x;
+        if (ta >= p.a_tiles) return false;
+        ix = ItemIdx{0, ta, j % p.w_tiles};
+        return true;
+    }
+    const uint32_t item = blockIdx.x + j * gridDim.x;
+    if (item >= items) return false;
+    ix = item_idx(p, item);
+    return true;
+}
+
 __global__ void __launch_bounds__(BG_THREADS, 1)
 bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CUtensorMap tmap_w,
              const BgParams p, uint32_t stages, uint32_t stage_bytes, uint32_t* __restrict__ err) {
     extern __shared__ uint8_t bg_dyn[];
     __shared__ uint64_t full_b[BG_MAX_STAGES], empty_b[BG_MAX_STAGES], accf_b[2], acce_b[2], done_b;
+    __shared__ uint64_t afull_b[BG_MAX_ASLOTS], aempty_b[BG_MAX_ASLOTS];  // A-resident slots
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
 
-    const uint32_t base = (su32(bg_dyn) + 1023u) & ~1023u;  // 1024-byte aligned ring (128-byte swizzle atoms)
-    uint8_t* ring = bg_dyn + (base - su32(bg_dyn));
+    // 1024-byte aligned (128-byte swizzle atoms): [A slots (A-resident)] [stage ring]
+    const uint32_t sbase = (su32(bg_dyn) + 1023u) & ~1023u;
+    uint8_t* sptr = bg_dyn + (sbase - su32(bg_dyn));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr uint32_t A_BYTES = BG_AROWS * BG_KSTEP;
     const uint32_t w_bytes = p.w_tile * BG_KSTEP;
     const uint32_t kpanels = (p.k_bytes + p.k_panel - 1) / p.k_panel;
     const uint32_t items = kpanels * p.a_tiles * p.w_tiles;
+    const uint32_t a_slots = p.a_resident ? p.k_bytes / BG_KSTEP : 0;
+    const uint32_t base = sbase + a_slots * A_BYTES;  // stage ring
+    uint8_t* ring = sptr + a_slots * A_BYTES;
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < stages; ++s) {
@@ -60,7 +82,11 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
         }
         for (int b = 0; b < 2; ++b) {
             bar_init(&accf_b[b], 1);
-            bar_init(&acce_b[b], 4);
+            bar_init(&acce_b[b], BG_EPI_WARPS);
+        }
+        for (uint32_t k = 0; k < a_slots; ++k) {
+            bar_init(&afull_b[k], 1);
+            bar_init(&aempty_b[k], 1);
         }
         bar_init(&done_b, 1);
         abort_s = 0;
@@ -79,12 +105,31 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
 
     if (warp == 0) {
         if (lane == 0) {  // ---------------------------------------------- TMA producer
+            // stage ring: A + W boxes per K step (streaming) or W boxes only
+            // (A-resident: the A tile's K slices stay in their slots for all
+            // W tiles of the tile and are reloaded for the next one once the
+            // MMAs of its last item have read them)
             uint64_t it = 0;
+            uint32_t t_last = 0xffffffffu;
             bool stop = false;
-            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
-                const ItemIdx ix = item_idx(p, item);
+            ItemIdx ix;
+            for (uint32_t j = 0; !stop && item_at(p, items, j, ix); ++j) {
+                const uint32_t t = a_slots ? j / p.w_tiles : 0;
+                const bool load_a = a_slots && ix.tw == 0;
                 const uint32_t k0 = ix.kp * p.k_panel, k1 = min(p.k_bytes, k0 + p.k_panel);
                 for (uint32_t k = k0; k < k1; k += BG_KSTEP, ++it) {
+                    const uint32_t ks = (k - k0) / BG_KSTEP;
+                    if (load_a) {
+                        if (t > 0 && !bar_wait(&aempty_b[ks], (t - 1) & 1)) {
+                            abort_s = 1;
+                            atomicOr(err, 4u);
+                            stop = true;
+                            break;
+                        }
+                        bar_expect_tx(&afull_b[ks], A_BYTES);
+                        tma_2d(sptr + ks * A_BYTES, &tmap_a, (int)k, (int)(ix.ta * BG_AROWS), &afull_b[ks]);
+                        t_last = t;
+                    }
                     const uint32_t st = (uint32_t)(it % stages);
                     if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1))) {
                         abort_s = 1;
@@ -94,14 +139,21 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     }
                     if (abort_s) { stop = true; break; }
                     uint8_t* sb = ring + (uint64_t)st * stage_bytes;
-                    bar_expect_tx(&full_b[st], A_BYTES + w_bytes);
-                    tma_2d(sb, &tmap_a, (int)k, (int)(ix.ta * BG_AROWS), &full_b[st]);
-                    tma_2d(sb + A_BYTES, &tmap_w, (int)k, (int)(ix.tw * p.w_tile), &full_b[st]);
+                    if (a_slots) {
+                        bar_expect_tx(&full_b[st], w_bytes);
+                        tma_2d(sb, &tmap_w, (int)k, (int)(ix.tw * p.w_tile), &full_b[st]);
+                    } else {
+                        bar_expect_tx(&full_b[st], A_BYTES + w_bytes);
+                        tma_2d(sb, &tmap_a, (int)k, (int)(ix.ta * BG_AROWS), &full_b[st]);
+                        tma_2d(sb + A_BYTES, &tmap_w, (int)k, (int)(ix.tw * p.w_tile), &full_b[st]);
+                    }
                 }
             }
             // no copy may still be landing in shared memory when the CTA exits
             for (uint64_t j = it > stages ? it - stages : 0; j < it; ++j)
                 bar_wait(&full_b[j % stages], (uint32_t)((j / stages) & 1));
+            if (t_last != 0xffffffffu)
+                for (uint32_t k = 0; k < a_slots; ++k) bar_wait(&afull_b[k], t_last & 1);
         }
     } else if (warp == 1) {
         if (lane == 0) {  // ---------------------------------------------- MMA issuer
@@ -110,8 +162,10 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                                    ((uint32_t)(BG_AROWS >> 4) << 24);
             uint64_t it = 0, n = 0;
             bool stop = false;
-            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x, ++n) {
-                const ItemIdx ix = item_idx(p, item);
+            ItemIdx ix;
+            for (uint32_t j = 0; !stop && item_at(p, items, j, ix); ++j, ++n) {
+                const uint32_t t = a_slots ? j / p.w_tiles : 0;
+                const bool last_of_a = a_slots && ix.tw == p.w_tiles - 1;
                 const uint32_t buf = (uint32_t)(n & 1), use = (uint32_t)(n >> 1);
                 if (use > 0 && !bar_wait(&acce_b[buf], (use - 1) & 1)) {
                     abort_s = 1;
@@ -124,20 +178,24 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 bool first = true;
                 for (uint32_t k = k0; k < k1; k += BG_KSTEP, ++it) {
                     const uint32_t st = (uint32_t)(it % stages);
-                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
+                    const uint32_t ks = (k - k0) / BG_KSTEP;
+                    if ((a_slots && !bar_wait(&afull_b[ks], t & 1)) || !bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) ||
+                        abort_s) {
                         abort_s = 1;
                         atomicOr(err, 8u);
                         stop = true;
                         break;
                     }
                     tc_after();
-                    const uint32_t sa = base + st * stage_bytes, sw = sa + A_BYTES;
+                    const uint32_t sa = a_slots ? sbase + ks * A_BYTES : base + st * stage_bytes;
+                    const uint32_t sw = a_slots ? base + st * stage_bytes : sa + A_BYTES;
 #pragma unroll
-                    for (uint32_t ks = 0; ks < BG_KSTEP / 32; ++ks)
-                        mma_i8(d, sdesc(sa + ks * 32u, 16, 1024), sdesc(sw + ks * 32u, 16, 1024), idesc,
-                               (first && ks == 0) ? 0u : 1u);
+                    for (uint32_t kk = 0; kk < BG_KSTEP / 32; ++kk)
+                        mma_i8(d, sdesc(sa + kk * 32u, 16, 1024), sdesc(sw + kk * 32u, 16, 1024), idesc,
+                               (first && kk == 0) ? 0u : 1u);
                     first = false;
-                    mma_commit(&empty_b[st]);  // stage reusable once these MMAs have read it
+                    mma_commit(&empty_b[st]);                // stage reusable once these MMAs have read it
+                    if (last_of_a) mma_commit(&aempty_b[ks]);  // A slot reusable for the next A tile
                 }
                 if (stop) break;
                 mma_commit(&accf_b[buf]);  // accumulator complete for this item
@@ -147,24 +205,78 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
         }
     } else {
         // -------------------------------------------------------------- epilogue
-        const uint32_t q = (uint32_t)(warp & 3);  // TMEM lane quarter of this warp
+        // 8 warps: warp w reads TMEM lane quarter w % 4 and every other
+        // 64-column chunk (half = (w - 2) / 4) of each item.
+        const uint32_t q = (uint32_t)(warp & 3);
+        const uint32_t half = (uint32_t)(warp - 2) >> 2;
         uint64_t n = 0;
-        for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, ++n) {
+        ItemIdx ix;
+        for (uint32_t j = 0; item_at(p, items, j, ix); ++j, ++n) {
             const uint32_t buf = (uint32_t)(n & 1), use = (uint32_t)(n >> 1);
             const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b[buf], use & 1));  // warp-uniform
             if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
             if (__any_sync(FULLMASK, !ok || abort_s)) break;
             tc_after();
-            const ItemIdx ix = item_idx(p, item);
             const uint32_t taddr = tmem + ((q * 32u) << 16) + buf * 256u;
             const uint32_t ybase = ix.tw * p.w_tile / 8;
+            const uint32_t wide = p.w_tile & ~63u;  // columns handled in 64-column chunks
             if (p.mode == BG_PLANAR) {
-                const uint32_t a = lane & 7;
-                const uint32_t x = ix.ta * (BG_AROWS / 8) + q * 4 + (lane >> 3);
+                const uint32_t a = lane & 7, xi = lane >> 3;
                 const uint32_t x4 = ix.ta * (BG_AROWS / 8) + q * 4;  // first x of this warp
+                const uint32_t x = x4 + xi;
                 const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
                 uint64_t* out = p.out + (uint64_t)ix.kp * p.out_pstride;
-                for (uint32_t c0 = 0; c0 < p.w_tile; c0 += 16) {
+                for (uint32_t c0 = 64 * half; c0 < wide; c0 += 128) {
+                    uint32_t v[64];
+                    tmem_ld64(taddr + c0, v);
+                    uint64_t part[8];  // (lo + hi 2^32) 2^(8a) mod p for the chunk's 8 y
+#pragma unroll
+                    for (int yy = 0; yy < 8; ++yy) {
+                        uint64_t lo = 0, hi = 0;
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            lo += (uint64_t)v[8 * yy + b] << (8 * b);
+                            hi += (uint64_t)v[8 * yy + 4 + b] << (8 * b);
+                        }
+                        part[yy] = canon(rotl61(lo, w1) + rotl61(hi, w2));
+                    }
+                    // butterfly over the 8 lanes of one x: each level halves the
+                    // y values a lane carries; lane a ends with y = a
+                    const bool b2 = (a & 4) != 0, b1 = (a & 2) != 0, b0 = (a & 1) != 0;
+                    uint64_t k4[4], k2[2];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        k4[i] = (b2 ? part[i + 4] : part[i]) + __shfl_xor_sync(FULLMASK, b2 ? part[i] : part[i + 4], 4);
+#pragma unroll
+                    for (int i = 0; i < 2; ++i)
+                        k2[i] = (b1 ? k4[i + 2] : k4[i]) + __shfl_xor_sync(FULLMASK, b1 ? k4[i] : k4[i + 2], 2);
+                    const uint64_t f =
+                        canon((b0 ? k2[1] : k2[0]) + __shfl_xor_sync(FULLMASK, b0 ? k2[0] : k2[1], 1));  // < 8p
+                    const uint32_t y = ybase + c0 / 8 + a;
+                    if (y < p.y_count && x < p.x_count) out[(uint64_t)y * p.out_ld + x] = f;
+                    if (p.planar_out) {
+                        // 4 x 8 byte transpose across the lanes of one y: lane
+                        // (xi, a) ends with planes 4(xi&1) + 2(xi>>1) + {0, 1}
+                        // of f(x4..x4+3, y) as two 32-bit words
+                        const bool e0 = (xi & 1) != 0, e1 = (xi & 2) != 0;
+                        const uint32_t flo = (uint32_t)f, fhi = (uint32_t)(f >> 32);
+                        const uint32_t keep1 = e0 ? fhi : flo;
+                        const uint32_t recv1 = __shfl_xor_sync(FULLMASK, e0 ? flo : fhi, 8);
+                        const uint32_t ev = e0 ? recv1 : keep1, od = e0 ? keep1 : recv1;
+                        const uint32_t pa = __byte_perm(ev, od, 0x5140), pb = __byte_perm(ev, od, 0x7362);
+                        const uint32_t keep2 = e1 ? pb : pa;
+                        const uint32_t recv2 = __shfl_xor_sync(FULLMASK, e1 ? pa : pb, 16);
+                        const uint32_t p0 = e1 ? recv2 : keep2, p1 = e1 ? keep2 : recv2;
+                        if (y < p.y_count && x4 < p.x_count) {
+                            const uint32_t plane = 4 * (xi & 1) + 2 * (xi >> 1);
+                            uint8_t* dst = p.planar_out + ((uint64_t)y * 8 + plane) * p.planar_ld + x4;
+                            *reinterpret_cast<uint32_t*>(dst) = __byte_perm(p0, p1, 0x5410);
+                            *reinterpret_cast<uint32_t*>(dst + p.planar_ld) = __byte_perm(p0, p1, 0x7632);
+                        }
+                    }
+                }
+                // remaining columns (w_tile not a multiple of 64): 16 at a time
+                for (uint32_t c0 = wide + 16 * half; c0 < p.w_tile; c0 += 32) {
                     uint32_t v[16];
                     tmem_ld16(taddr + c0, v);
 #pragma unroll
@@ -176,19 +288,19 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                             lo += (uint64_t)v[8 * h + b] << (8 * b);
                             hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
                         }
-                        uint64_t f = canon(rotl61(lo, w1) + rotl61(hi, w2));  // (lo + hi 2^32) 2^(8a) mod p
+                        uint64_t f = canon(rotl61(lo, w1) + rotl61(hi, w2));
                         f += __shfl_xor_sync(FULLMASK, f, 1);
                         f += __shfl_xor_sync(FULLMASK, f, 2);
                         f += __shfl_xor_sync(FULLMASK, f, 4);
                         f = canon(f);
-                        uint32_t packed = (uint32_t)((f >> (8 * a)) & 0xffu) << (8 * (lane >> 3));
+                        uint32_t packed = (uint32_t)((f >> (8 * a)) & 0xffu) << (8 * xi);
                         packed |= __shfl_xor_sync(FULLMASK, packed, 8);
                         packed |= __shfl_xor_sync(FULLMASK, packed, 16);
                         if (y < p.y_count) {
                             if (a == 0 && x < p.x_count) out[(uint64_t)y * p.out_ld + x] = f;
                             if (p.planar_out && lane < 8 && x4 < p.x_count)
-                                *reinterpret_cast<uint32_t*>(p.planar_out + ((uint64_t)y * 8 + lane) * p.planar_ld + x4) =
-                                    packed;
+                                *reinterpret_cast<uint32_t*>(p.planar_out + ((uint64_t)y * 8 + lane) * p.planar_ld +
+                                                             x4) = packed;
                         }
                     }
                 }
@@ -196,12 +308,28 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 const uint32_t x = ix.ta * BG_AROWS + q * 32 + lane;
                 const bool xv = x < p.x_count;
                 const uint64_t corr = xv ? p.corr[x] : 0;
-                for (uint32_t c0 = 0; c0 < p.w_tile; c0 += 16) {
+                for (uint32_t c0 = 64 * half; c0 < wide; c0 += 128) {
+                    uint32_t v[64];
+                    tmem_ld64(taddr + c0, v);
+#pragma unroll
+                    for (int yy = 0; yy < 8; ++yy) {
+                        int64_t lo = 0, hi = 0;
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            lo += (int64_t)(int32_t)v[8 * yy + b] * (int64_t)(1ll << (8 * b));
+                            hi += (int64_t)(int32_t)v[8 * yy + 4 + b] * (int64_t)(1ll << (8 * b));
+                        }
+                        const uint64_t lr = lo < 0 ? (uint64_t)(lo + (int64_t)P) : (uint64_t)lo;
+                        const uint64_t hr = hi < 0 ? (uint64_t)(hi + (int64_t)P) : (uint64_t)hi;
+                        const uint32_t y = ybase + c0 / 8 + yy;
+                        if (xv && y < p.y_count) p.out[(uint64_t)y * p.out_ld + x] = add_mod(canon(lr + rotl61(hr, 32)), corr);
+                    }
+                }
+                for (uint32_t c0 = wide + 16 * half; c0 < p.w_tile; c0 += 32) {
                     uint32_t v[16];
                     tmem_ld16(taddr + c0, v);
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
-                        const uint32_t y = ybase + c0 / 8 + h;
                         int64_t lo = 0, hi = 0;
 #pragma unroll
                         for (int b = 0; b < 4; ++b) {
@@ -210,8 +338,8 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         }
                         const uint64_t lr = lo < 0 ? (uint64_t)(lo + (int64_t)P) : (uint64_t)lo;
                         const uint64_t hr = hi < 0 ? (uint64_t)(hi + (int64_t)P) : (uint64_t)hi;
-                        const uint64_t f = add_mod(canon(lr + rotl61(hr, 32)), corr);
-                        if (xv && y < p.y_count) p.out[(uint64_t)y * p.out_ld + x] = f;
+                        const uint32_t y = ybase + c0 / 8 + h;
+                        if (xv && y < p.y_count) p.out[(uint64_t)y * p.out_ld + x] = add_mod(canon(lr + rotl61(hr, 32)), corr);
                     }
                 }
             }
@@ -394,19 +522,27 @@ unsigned grid_for(uint64_t work, unsigned threads, unsigned cap) {
 
 }  // namespace
 
-uint32_t bgemm_stage_bytes(uint32_t w_tile) { return BG_AROWS * BG_KSTEP + ((w_tile * BG_KSTEP + 1023u) & ~1023u); }
+uint32_t bgemm_stage_bytes(uint32_t w_tile, bool a_resident) {
+    return (a_resident ? 0u : (uint32_t)(BG_AROWS * BG_KSTEP)) + ((w_tile * BG_KSTEP + 1023u) & ~1023u);
+}
+
+uint32_t bgemm_smem_bytes(const BgParams& p, uint32_t stages) {
+    const uint32_t a = p.a_resident ? (p.k_bytes / BG_KSTEP) * BG_AROWS * BG_KSTEP : 0u;
+    return a + stages * bgemm_stage_bytes(p.w_tile, p.a_resident != 0) + 1024u;
+}
 
 void launch_bgemm(const CUtensorMap& tmap_a, const CUtensorMap& tmap_w, const BgParams& p, uint32_t stages, int ctas,
                   uint32_t* d_err, cudaStream_t s) {
     const uint32_t kpanels = (p.k_bytes + p.k_panel - 1) / p.k_panel;
     const uint64_t items = (uint64_t)kpanels * p.a_tiles * p.w_tiles;
     if (!items) return;
-    const uint32_t stage_bytes = bgemm_stage_bytes(p.w_tile);
+    const uint32_t stage_bytes = bgemm_stage_bytes(p.w_tile, p.a_resident != 0);
     // at least half the SM's shared memory: one CTA per SM, so the second
     // never waits in tcgen05.alloc for the first one's 512 TMEM columns
-    const int smem = (int)std::max<uint32_t>(stages * stage_bytes + 1024, 116u * 1024u);
+    const int smem = (int)std::max<uint32_t>(bgemm_smem_bytes(p, stages), 116u * 1024u);
     cudaFuncSetAttribute(bgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    const unsigned grid = items < (uint64_t)ctas ? (unsigned)items : (unsigned)ctas;
+    const uint64_t units = p.a_resident ? p.a_tiles : items;
+    const unsigned grid = units < (uint64_t)ctas ? (unsigned)units : (unsigned)ctas;
     bgemm_kernel<<<grid, BG_THREADS, smem, s>>>(tmap_a, tmap_w, p, stages, stage_bytes, d_err);
 }
 

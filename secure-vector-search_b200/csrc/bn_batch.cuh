@@ -23,6 +23,8 @@ namespace bn {
 constexpr int BG_AROWS = 128;              // A rows per work item (TMEM lanes)
 constexpr int BG_KSTEP = 128;              // K bytes per pipeline stage (one 128-byte swizzle atom)
 constexpr int BG_MAX_STAGES = 6;
+constexpr int BG_MAX_ASLOTS = 8;           // A-resident mode: K <= 8 * 128 bytes
+constexpr uint32_t BG_MAX_SMEM = 232448;   // dynamic shared memory per CTA on sm_100
 constexpr uint32_t BG_MAX_KPANEL = 16384;  // K bytes summed in s32 before a drain: 16384 * 255^2 < 2^31
 
 enum BgMode : int {
@@ -51,14 +53,18 @@ struct BgParams {
     uint8_t* planar_out;   // PLANAR, nullable
     uint64_t planar_ld;
     int order_a_fast;      // work order: 0 = W tile fastest, 1 = A tile fastest
+    int a_resident;        // keep each A tile (all of K, one K panel) in shared memory across its W tiles
 };
 
 // tmap_a: A bytes {k_bytes, A rows}, box {128, 128}; tmap_w: W bytes
 // {k_bytes, W rows}, box {128, w_tile}; both 128-byte swizzle.  stages in
 // [2, BG_MAX_STAGES].  *err: bit 2/3/4 set when a bounded wait timed out.
+// A-resident mode needs k_panel == k_bytes <= BG_MAX_ASLOTS * 128 and
+// bgemm_smem_bytes(p, stages) <= BG_MAX_SMEM.
 void launch_bgemm(const CUtensorMap& tmap_a, const CUtensorMap& tmap_w, const BgParams& p, uint32_t stages, int ctas,
                   uint32_t* d_err, cudaStream_t s);
-uint32_t bgemm_stage_bytes(uint32_t w_tile);
+uint32_t bgemm_stage_bytes(uint32_t w_tile, bool a_resident);
+uint32_t bgemm_smem_bytes(const BgParams& p, uint32_t stages);
 
 // Byte planes of a row-major u64 matrix: dst[(i*8 + a) * dst_ld + col0 + j] =
 // byte a of (negate ? p - src : src)[i * src_ld + j], j < k (k % 16 == 0).

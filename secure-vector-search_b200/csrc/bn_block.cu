@@ -37,7 +37,7 @@ struct BlockPlan {
     uint32_t t_pass = 0, n_rows = 0;   // trials per Freivalds pass, U rows (8 * even trials)
     uint32_t nblocks = 0, npanels = 0;  // U row blocks, z panels (4096 rows)
     // tuned GEMM configuration
-    uint32_t w_tile = 256, stages = 4, order = 0, k_panel4 = 16384;
+    uint32_t w_tile = 256, stages = 4, order = 0, a_res = 0, k_panel4 = 16384;
     float tuned_ms[2] = {0.f, 0.f};  // autotuner's best G1 and G4 launch times
     int topk_ctas = 1;
     // workspace
@@ -55,9 +55,18 @@ namespace {
 
 uint32_t kpanels_of(const BlockPlan& b) { return (uint32_t)((b.npad + b.k_panel4 - 1) / b.k_panel4); }
 
-uint32_t stages_for(uint32_t w_tile) {
-    const uint32_t s = (220u * 1024u) / bgemm_stage_bytes(w_tile);
-    return std::max<uint32_t>(2, std::min<uint32_t>(BG_MAX_STAGES, s));
+// Most pipeline stages whose shared memory fits (0 when even 2 do not).
+uint32_t stages_for(const BgParams& p) {
+    for (uint32_t st = BG_MAX_STAGES; st >= 2; --st)
+        if (bgemm_smem_bytes(p, st) + 1024 <= BG_MAX_SMEM) return st;
+    return 0;
+}
+
+// The u . r GEMM's stage count (W = the U planes, streaming A).
+uint32_t stages_u(uint32_t n_rows) {
+    BgParams p{};
+    p.w_tile = n_rows;
+    return stages_for(p);
 }
 
 int tmap(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uint32_t box_rows, const char* what) {
@@ -121,6 +130,7 @@ BgParams g1_params(const BlockPlan& b, const Corpus& c) {
     p.y_count = b.B;
     p.out_ld = b.nld;
     p.order_a_fast = (int)b.order;
+    p.a_resident = (int)b.a_res;
     p.planar_ld = b.npad;
     return p;
 }
@@ -144,31 +154,39 @@ int autotune(BlockPlan& b, cudaStream_t s) {
     CU(cudaEventCreate(&e1));
     const uint32_t wmax = (uint32_t)std::min<uint64_t>(256, align_up(8ull * b.B, 16));
     float best = 1e30f;
-    uint32_t bw = b.w_tile, bs = b.stages, bo = b.order;
+    uint32_t bw = b.w_tile, bs = b.stages, bo = b.order, ba = b.a_res;
     int rc = BN_OK;
     for (uint32_t w : {64u, 128u, 256u}) {
         if (w > wmax && w != 64u) continue;
-        for (uint32_t st : {3u, stages_for(w)}) {
-            for (uint32_t order : {0u, 1u}) {
-                b.w_tile = w;
-                b.stages = st;
-                b.order = order;
-                if ((rc = relayout(b)) != BN_OK) break;
-                BgParams p = g1_params(b, c);
-                p.out = reinterpret_cast<uint64_t*>(d + b.o_r);
-                p.planar_out = reinterpret_cast<uint8_t*>(d + b.o_rp);
-                float ms = 0;
-                for (int rep = 0; rep < 3; ++rep) {
-                    if (rep == 1) cudaEventRecord(e0, s);
-                    launch_bgemm(c.tmap_mp, b.tm_vp, p, b.stages, b.h->e.ctx->num_sms,
-                                 reinterpret_cast<uint32_t*>(d + b.o_err), s);
+        for (uint32_t ares : {0u, 1u}) {
+            b.w_tile = w;
+            b.a_res = ares;
+            const uint32_t smax = stages_for(g1_params(b, c));
+            if (!smax) continue;
+            for (uint32_t st : {std::min(3u, smax), smax}) {
+                for (uint32_t order : {0u, 1u}) {
+                    if (ares && order) continue;  // A-resident work order is fixed
+                    if (st == smax && smax == 3u && st != std::min(3u, smax)) continue;
+                    b.stages = st;
+                    b.order = order;
+                    if ((rc = relayout(b)) != BN_OK) break;
+                    BgParams p = g1_params(b, c);
+                    p.out = reinterpret_cast<uint64_t*>(d + b.o_r);
+                    p.planar_out = reinterpret_cast<uint8_t*>(d + b.o_rp);
+                    float ms = 0;
+                    for (int rep = 0; rep < 3; ++rep) {
+                        if (rep == 1) cudaEventRecord(e0, s);
+                        launch_bgemm(c.tmap_mp, b.tm_vp, p, b.stages, b.h->e.ctx->num_sms,
+                                     reinterpret_cast<uint32_t*>(d + b.o_err), s);
+                    }
+                    cudaEventRecord(e1, s);
+                    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+                        rc = fail(BN_ECUDA, "autotune timing failed");
+                        break;
+                    }
+                    if (ms < best) { best = ms; bw = w; bs = st; bo = order; ba = ares; }
                 }
-                cudaEventRecord(e1, s);
-                if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-                    rc = fail(BN_ECUDA, "autotune timing failed");
-                    break;
-                }
-                if (ms < best) { best = ms; bw = w; bs = st; bo = order; }
+                if (rc != BN_OK || smax <= 3u) break;
             }
             if (rc != BN_OK) break;
         }
@@ -177,6 +195,7 @@ int autotune(BlockPlan& b, cudaStream_t s) {
     b.w_tile = bw;
     b.stages = bs;
     b.order = bo;
+    b.a_res = ba;
     b.tuned_ms[0] = best / 2;  // two timed launches per candidate
     if (rc == BN_OK && b.trials) {  // K panel of the u . r GEMM
         float bestk = 1e30f;
@@ -200,7 +219,7 @@ int autotune(BlockPlan& b, cudaStream_t s) {
             float ms = 0;
             for (int rep = 0; rep < 3; ++rep) {
                 if (rep == 1) cudaEventRecord(e0, s);
-                launch_bgemm(b.tm_rp, b.tm_ub, p, stages_for(b.n_rows), b.h->e.ctx->num_sms,
+                launch_bgemm(b.tm_rp, b.tm_ub, p, stages_u(b.n_rows), b.h->e.ctx->num_sms,
                              reinterpret_cast<uint32_t*>(d + b.o_err), s);
             }
             cudaEventRecord(e1, s);
@@ -251,8 +270,16 @@ int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint3
     b->nblocks = (uint32_t)((c.rows + TC_ROWS - 1) / TC_ROWS);
     b->npanels = (uint32_t)((c.rows + TC_PANEL_ROWS - 1) / TC_PANEL_ROWS);
     b->w_tile = (uint32_t)std::min<uint64_t>(256, align_up(8ull * B, 16));
-    b->stages = stages_for(b->w_tile);
+    b->a_res = 8ull * B > b->w_tile ? 1u : 0u;  // A tiles reused across several W tiles
+    if (!c.block_ready) b->a_res = 0;
     b->k_panel4 = 4096;
+    if (!verify_only) {
+        b->stages = stages_for(g1_params(*b, c));
+        if (!b->stages) {
+            b->a_res = 0;
+            b->stages = stages_for(g1_params(*b, c));
+        }
+    }
     const int sms = f->e.ctx->num_sms;
     b->topk_ctas = (int)std::max<uint64_t>(1, std::min<uint64_t>((c.rows + 511) / 512, (uint64_t)sms * 4 / B));
     const uint32_t ks = std::max<uint32_t>(k, 1);
@@ -332,11 +359,12 @@ int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint3
     return BN_OK;
 }
 
-void block_plan_config(const BlockPlan* b, uint32_t cfg[4], float tuned_ms[2]) {
+void block_plan_config(const BlockPlan* b, uint32_t cfg[5], float tuned_ms[2]) {
     cfg[0] = b->w_tile;
     cfg[1] = b->stages;
     cfg[2] = b->order;
-    cfg[3] = b->k_panel4;
+    cfg[3] = b->a_res;
+    cfg[4] = b->k_panel4;
     if (tuned_ms) {
         tuned_ms[0] = b->tuned_ms[0];
         tuned_ms[1] = b->tuned_ms[1];
@@ -384,7 +412,7 @@ static void enqueue_verify(BlockPlan& b, const uint64_t* d_v, const uint8_t* d_s
         p.out_ld = b.B;
         p.out_pstride = (uint64_t)b.trials * b.B;
         p.order_a_fast = 1;
-        launch_bgemm(b.tm_rp, b.tm_ub, p, stages_for(b.n_rows), sms, err, s);
+        launch_bgemm(b.tm_rp, b.tm_ub, p, stages_u(b.n_rows), sms, err, s);
     }
     uint64_t* zv = reinterpret_cast<uint64_t*>(d + b.o_zv);
     launch_zv(z, d_v, b.trials, b.B, zv, s);
@@ -420,12 +448,14 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     p.out = r;
     p.planar_out = rp;
     launch_bgemm(c.tmap_mp, b.tm_vp, p, b.stages, sms, err, s);
-    // G2: f2 = -(AL g + H x)
+    // G2: f2 = -(AL g + H x)   (K = 2 n1 bytes per plane row: A tiles stay resident)
     p.k_bytes = c.k_alh;
     p.k_panel = c.k_alh;
     p.out = reinterpret_cast<uint64_t*>(d + b.o_f2);
     p.planar_out = nullptr;
-    launch_bgemm(c.tmap_alh, b.tm_gx, p, b.stages, sms, err, s);
+    p.a_resident = (p.w_tiles > 1 && c.k_alh <= BG_MAX_ASLOTS * BG_KSTEP) ? 1 : 0;
+    p.order_a_fast = p.a_resident ? 0 : (int)b.order;
+    launch_bgemm(c.tmap_alh, b.tm_gx, p, stages_for(p), sms, err, s);
     // G3: f3 = M T + S v
     BgParams q{};
     q.mode = BG_S8;
@@ -440,7 +470,7 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     q.out_ld = b.nld;
     q.corr = c.corr.at<uint64_t>();
     q.order_a_fast = (int)b.order;
-    launch_bgemm(c.tmap_ms, b.tm_tv, q, b.stages, sms, err, s);
+    launch_bgemm(c.tmap_ms, b.tm_tv, q, stages_for(q), sms, err, s);
     // Mv = r + f2 - f3 (written over f3 when asked for), fp_to_signed, top-k
     if (b.k || want_mv) {
         TopkScratch ts{reinterpret_cast<int64_t*>(d + b.o_cs), reinterpret_cast<uint32_t*>(d + b.o_ci),
