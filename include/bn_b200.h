@@ -35,6 +35,7 @@ extern "C" {
 #define BN_EBUDGET (-3)      /* payload exceeds budget    (GpuError::BudgetTooSmall) */
 #define BN_ENODEV (-4)       /* no usable CUDA device                                */
 #define BN_EUNSUPPORTED (-5) /* handle lacks the client state this call needs       */
+#define BN_EAGAIN (-6)       /* bn_server_wait: the request is not complete yet      */
 
 #define BN_TOPK_MAX 1024
 #define BN_MAX_TRIALS 64 /* Protocol 2 trials per call */
@@ -244,6 +245,58 @@ int bn_ivf_query(bn_ivf* h, uint32_t B, uint32_t nprobe, const uint32_t* probes,
                  const uint64_t* g, const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz,
                  const uint8_t* v_seeds, uint32_t trials, uint32_t k, uint32_t* ids, int64_t* scores, uint32_t* n_hits,
                  int32_t* failed_cluster, int32_t* failed_trial);
+
+/* ---------------------------------------------------------------- serving loop
+ * Continuous batching over device-resident corpora.  No counterpart in the
+ * reference, whose scorers serve one query per call with every GPU call
+ * synchronous on one stream (gpu/mod.rs:169-200); the scoring semantics per
+ * query are BnTmScorer::score (lib.rs:326-475) and BnTmIvfScorer::score
+ * (ivf.rs:746-927), so each result equals bn_flat_query / bn_ivf_query on the
+ * same inputs, alone or in any mix of requests.
+ * Requests are queued by submit; a scheduler thread keeps up to `slots`
+ * batches in flight (one stream and one workspace each).  A free slot takes
+ * up to max_batch queued requests of one corpus (IVF requests with different
+ * nprobe share a batch) once the batch is full or its oldest request has
+ * waited max_wait_us.  Admission is by device memory: a batch's workspace
+ * plus the workspaces the other slots hold must fit in mem_budget (0 = no
+ * limit beyond the context budget); a batch is cut shorter to fit, and a
+ * request that cannot fit alone fails with BN_EBUDGET. */
+typedef struct bn_server bn_server;
+#define BN_SERVER_FLAT 0
+#define BN_SERVER_IVF 1
+typedef struct bn_server_config {
+    uint32_t max_batch;   /* queries per launch, 1..=4096 */
+    uint32_t slots;       /* batches in flight, 1..=16 */
+    uint64_t mem_budget;  /* device bytes for the slots' workspaces (0: unlimited) */
+    uint32_t max_wait_us; /* batching window */
+    uint32_t trials;      /* Protocol 2 trials per query (params.verification_trials()) */
+    uint32_t k;           /* hits per query */
+} bn_server_config;
+typedef struct bn_server_stats_t {
+    uint64_t submitted, completed, batches;
+    double mean_batch;                 /* queries per launched batch */
+    double p50_us, p99_us, max_us;     /* submit -> result latency */
+    double throughput_qps;             /* completed / (last completion - first submit) */
+    uint64_t peak_workspace_bytes;
+} bn_server_stats_t;
+/* flat and/or ivf (nullable, not both), with client state, in one context. */
+int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn_server** out);
+/* Inputs as one query of bn_flat_query / bn_ivf_query (copied); v_seed = the
+ * query's Protocol 2 seed (32 bytes).  *ticket identifies the result. */
+int bn_server_submit_flat(bn_server* s, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                          const int8_t* t_sign, uint32_t t_nnz, const uint8_t* v_seed, uint64_t* ticket);
+int bn_server_submit_ivf(bn_server* s, uint32_t nprobe, const uint32_t* probes, const uint64_t* v_enc,
+                         const uint64_t* g, const uint32_t* t_idx, const int8_t* t_sign, uint32_t t_nnz,
+                         const uint8_t* v_seed, uint64_t* ticket);
+/* Waits up to timeout_ms; BN_EAGAIN when not complete by then.  On success
+ * the ticket is released: ids / scores (k entries), *n_hits, the first failing
+ * trial (and IVF list) or -1, and the request's latency. */
+int bn_server_wait(bn_server* s, uint64_t ticket, uint32_t timeout_ms, uint32_t* ids, int64_t* scores,
+                   uint32_t* n_hits, int32_t* failed_trial, int32_t* failed_cluster, double* latency_us);
+/* Counters and latency percentiles since creation or the last reset. */
+int bn_server_stats(bn_server* s, int reset, bn_server_stats_t* out);
+/* Drains queued and in-flight requests, then frees the server. */
+int bn_server_destroy(bn_server* s);
 
 /* ---------------------------------------------------------------- keygen
  * encrypt_cluster (crypto.rs:405-478) on the device with host in/out:

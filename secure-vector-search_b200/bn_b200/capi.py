@@ -16,11 +16,11 @@ N = 1024
 P = (1 << 61) - 1
 TOPK_MAX = 1024
 
-BN_OK, BN_EINVAL, BN_ECUDA, BN_EBUDGET, BN_ENODEV, BN_EUNSUPPORTED = 0, -1, -2, -3, -4, -5
+BN_OK, BN_EINVAL, BN_ECUDA, BN_EBUDGET, BN_ENODEV, BN_EUNSUPPORTED, BN_EAGAIN = 0, -1, -2, -3, -4, -5, -6
 ENGINE_TENSOR, ENGINE_CUDA_CORE = 0, 1
 BLOCK_AUTOTUNE = 1
 _NAMES = {BN_EINVAL: "EINVAL", BN_ECUDA: "ECUDA", BN_EBUDGET: "EBUDGET", BN_ENODEV: "ENODEV",
-          BN_EUNSUPPORTED: "EUNSUPPORTED"}
+          BN_EUNSUPPORTED: "EUNSUPPORTED", BN_EAGAIN: "EAGAIN"}
 
 
 class BnError(RuntimeError):
@@ -39,6 +39,17 @@ u32, u64, i32 = C.c_uint32, C.c_uint64, C.c_int32
 
 class SparseCsr(C.Structure):
     _fields_ = [("rowptr", vp), ("idx", vp), ("sign", vp)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("max_batch", u32), ("slots", u32), ("mem_budget", u64), ("max_wait_us", u32), ("trials", u32),
+                ("k", u32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", u64), ("completed", u64), ("batches", u64), ("mean_batch", C.c_double),
+                ("p50_us", C.c_double), ("p99_us", C.c_double), ("max_us", C.c_double),
+                ("throughput_qps", C.c_double), ("peak_workspace_bytes", u64)]
 
 
 _SIGS = {
@@ -82,6 +93,12 @@ _SIGS = {
     "bn_ivf_verify": (C.c_int, [vp, u32, vp, vp, vp, u32, vp, vp, vp]),
     "bn_ivf_query": (C.c_int, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
     "bn_encrypt_cluster": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, vp, vp]),
+    "bn_server_create": (C.c_int, [vp, vp, C.POINTER(ServerConfig), vp]),
+    "bn_server_submit_flat": (C.c_int, [vp, vp, vp, vp, vp, u32, vp, vp]),
+    "bn_server_submit_ivf": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, u32, vp, vp]),
+    "bn_server_wait": (C.c_int, [vp, u64, u32, vp, vp, vp, vp, vp, vp]),
+    "bn_server_stats": (C.c_int, [vp, C.c_int, C.POINTER(ServerStats)]),
+    "bn_server_destroy": (C.c_int, [vp]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)
@@ -414,6 +431,60 @@ class Ivf:
     def close(self):
         if self.h:
             lib.bn_ivf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Server:
+    """bn_server: continuous batching of flat and IVF queries over resident corpora."""
+
+    def __init__(self, flat=None, ivf=None, max_batch=64, slots=4, mem_budget=0, max_wait_us=200, trials=20, k=10):
+        self.flat, self.ivf, self.k = flat, ivf, k
+        cfg = ServerConfig(max_batch, slots, mem_budget, max_wait_us, trials, k)
+        out = vp()
+        check(lib.bn_server_create(flat.h if flat else None, ivf.h if ivf else None, C.byref(cfg), C.byref(out)))
+        self.h = out
+
+    def submit_flat(self, v_enc, g, t_idx, t_sign, v_seed) -> int:
+        v, gg = _u64(v_enc), _u64(g)
+        ti, ts = np.ascontiguousarray(t_idx, np.uint32), np.ascontiguousarray(t_sign, np.int8)
+        seed = None if v_seed is None else np.frombuffer(bytes(v_seed), np.uint8).copy()
+        t = u64(0)
+        check(lib.bn_server_submit_flat(self.h, ptr(v), ptr(gg), ptr(ti) if ti.size else None,
+                                        ptr(ts) if ts.size else None, ti.size, ptr(seed), C.byref(t)))
+        return t.value
+
+    def submit_ivf(self, probes, v_enc, g, t_idx, t_sign, v_seed) -> int:
+        pr = np.ascontiguousarray(probes, np.uint32)
+        v, gg = _u64(v_enc), _u64(g)
+        ti, ts = np.ascontiguousarray(t_idx, np.uint32), np.ascontiguousarray(t_sign, np.int8)
+        seed = None if v_seed is None else np.frombuffer(bytes(v_seed), np.uint8).copy()
+        t = u64(0)
+        check(lib.bn_server_submit_ivf(self.h, pr.size, ptr(pr) if pr.size else None, ptr(v), ptr(gg),
+                                       ptr(ti) if ti.size else None, ptr(ts) if ts.size else None, ti.size,
+                                       ptr(seed), C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60000):
+        """(ids, scores, failed_trial, failed_cluster, latency_us); raises BnError(EAGAIN) on timeout."""
+        kk = max(self.k, 1)
+        ids = np.zeros(kk, np.uint32)
+        sc = np.zeros(kk, np.int64)
+        nh, ft, fc, lat = u32(0), i32(0), i32(0), C.c_double(0)
+        check(lib.bn_server_wait(self.h, ticket, timeout_ms, ptr(ids), ptr(sc), C.byref(nh), C.byref(ft),
+                                 C.byref(fc), C.byref(lat)))
+        return ids[: nh.value].copy(), sc[: nh.value].copy(), ft.value, fc.value, lat.value
+
+    def stats(self, reset: bool = False) -> dict:
+        st = ServerStats()
+        check(lib.bn_server_stats(self.h, 1 if reset else 0, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.h:
+            lib.bn_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -40,7 +40,8 @@ int bn::api::fail(int code, const char* fmt, ...) {
 
 using namespace bn::api;
 
-namespace {
+namespace bn {
+namespace api {
 
 int corpus_tmap(Corpus& c) {
     if (!c.rows) return BN_OK;
@@ -222,71 +223,6 @@ int build_corpus_from_plain(bn_ctx* ctx, Corpus& c, const uint64_t* m_q, uint64_
 }
 
 // ------------------------------------------------------------------ pipeline
-constexpr uint32_t MAX_TRIALS = 64;  // Protocol 2 trials per call
-
-struct TcMaps {  // host-side tensor maps of the U buffer, one per pass of <= 20 trials
-    CUtensorMap u[(MAX_TRIALS + TC_MAX_TRIALS - 1) / TC_MAX_TRIALS];
-};
-inline uint32_t pass_rows(uint32_t t_cnt) { return 8 * ((t_cnt + 1) & ~1u); }
-
-struct Meta {  // device pointers (+ host tensor maps)
-    const ScanSeg* segs;
-    const uint64_t* seg_blk;
-    uint32_t nseg;
-    uint64_t total_blocks;
-    const VerifySeg* vsegs;
-    uint32_t nvseg;
-    const DecodeQuery* dq;
-    const TcBlock* tc_blocks;
-    uint32_t nblocks;
-    const TcPanel* tc_panels;
-    uint32_t npanels;
-    const uint32_t* seg_panel0;
-    const uint32_t* seg_block0;
-    const TcMaps* maps;
-};
-struct Scratch {  // device pointers
-    QLimb* limbs;
-    uint64_t* x;
-    uint64_t* r;
-    uint64_t* z_part;
-    uint64_t* ur_part;
-    uint32_t* flags;
-    uint64_t* ur;
-    uint64_t* zv;
-    TopkScratch topk;
-    uint32_t* err;  // device pipeline timeout flags
-    uint8_t* u_buf;
-    uint64_t* r_part;  // fused pass: per strip-group partial dots
-    uint64_t* zv_chunks;
-};
-struct Inputs {
-    const uint64_t* v;
-    const uint64_t* g;
-    const uint32_t* t;
-    const uint32_t* t_nnz;
-    const uint8_t* seeds;
-};
-struct Outputs {
-    uint32_t* ids;
-    int64_t* scores;
-    uint32_t* n;
-    int32_t* vfailed;  // per verify segment
-    uint64_t* mv;      // nullable
-};
-
-struct HostMeta {
-    std::vector<ScanSeg> segs;
-    std::vector<uint64_t> seg_blk;
-    std::vector<VerifySeg> vsegs;
-    std::vector<DecodeQuery> dq;
-    std::vector<uint32_t> seg_cluster;  // IVF: list id of each segment
-    std::vector<TcBlock> blocks;        // 128-row blocks of every verify segment
-    std::vector<TcPanel> panels;        // 4096-row panels of every verify segment
-    std::vector<uint32_t> seg_block0, seg_panel0;
-    uint64_t total_out = 0, max_rows = 0;
-};
-
 void finish_meta(HostMeta& hm) {
     hm.seg_blk.assign(hm.segs.size() + 1, 0);
     for (size_t i = 0; i < hm.segs.size(); ++i)
@@ -320,28 +256,11 @@ void flat_meta(uint64_t m, uint32_t B, HostMeta& hm) {
     finish_meta(hm);
 }
 
-struct Sizes {
-    uint32_t B, n1, trials, k, ctas;
-    uint64_t total_out, nseg, nvseg, nblocks, npanels;
-    FreivaldsPlan fp;  // CUDA-core engine
-    int engine;        // BN_ENGINE_*
-};
-
 int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms) {
     uint64_t by_rows = (max_rows_per_query + 255) / 256;
     uint64_t by_sms = std::max<uint64_t>(1, (uint64_t)sms * 4 / std::max<uint32_t>(B, 1));
     return (int)std::max<uint64_t>(1, std::min(by_rows, by_sms));
 }
-
-// Offsets of every device buffer of one pipeline run.
-struct RunLayout {
-    // inputs (contiguous from 0 -> one H2D)
-    uint64_t v, g, t, t_nnz, seeds, segs, seg_blk, vsegs, dq, tc_blocks, tc_panels, seg_panel0, seg_block0, in_end;
-    // outputs (contiguous -> one D2H)
-    uint64_t ids, scores, n, vfailed, ur, zv, err, out_begin, out_end;
-    // internal
-    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, r_part, zv_chunks, total;
-};
 
 RunLayout make_layout(const Sizes& z, bool want_mv) {
     Layout L;
@@ -513,12 +432,15 @@ Sizes sizes_for(const Engine& e, const HostMeta& hm, uint32_t B, uint32_t trials
                  e.ctx->engine};
 }
 
-// Host-buffer query: pack, one H2D, pipeline, one D2H, sync.
-int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
-              const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds, uint32_t trials, uint32_t k,
-              uint32_t* ids, int64_t* scores, uint32_t* n_hits, std::vector<int32_t>& vfailed, uint64_t* r_out,
-              uint64_t* mv_out) {
+// One pipeline run over host inputs, split so that a caller can keep several
+// runs in flight on different streams (the serving loop): prepare packs the
+// inputs into pinned staging, launch enqueues H2D + pipeline + D2H, finish
+// reads the outputs once the stream has drained.
+int job_prepare(Engine& e, QueryJob& j, DevMem& ws, PinnedMem& host, const uint64_t* v_enc, const uint64_t* g,
+                const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds) {
     Corpus& c = e.c;
+    const HostMeta& hm = *j.hm;
+    const uint32_t B = j.B, trials = j.trials, k = j.k;
     if (!c.client) return fail(BN_EUNSUPPORTED, "this handle has no client state (attach_client was not called)");
     if (k > BN_TOPK_MAX) return fail(BN_EINVAL, "k = %u exceeds BN_TOPK_MAX = %d", k, BN_TOPK_MAX);
     if (B > 65535) return fail(BN_EINVAL, "B = %u exceeds 65535 queries per call", B);
@@ -534,16 +456,15 @@ int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const 
     TRY(validate_residues(v_enc, (uint64_t)B * N, "v_enc"));
     TRY(validate_residues(g, (uint64_t)B * c.n1, "g"));
 
-    const Sizes z = sizes_for(e, hm, B, trials, k);
-    const RunLayout o = make_layout(z, mv_out != nullptr);
-    TRY(e.ws.reserve(e.ctx, o.total));
-    TRY(e.host.reserve(o.out_end));
-    char* d = e.ws.at<char>();
-    TcMaps maps;
-    TRY(make_tc_maps(z, reinterpret_cast<uint8_t*>(d + o.u_buf), maps));
+    j.z = sizes_for(e, hm, B, trials, k);
+    j.o = make_layout(j.z, j.want_mv);
+    const RunLayout& o = j.o;
+    TRY(ws.reserve(e.ctx, o.total));
+    TRY(host.reserve(o.out_end));
+    char* d = ws.at<char>();
+    TRY(make_tc_maps(j.z, reinterpret_cast<uint8_t*>(d + o.u_buf), j.maps));
 
-    // pack inputs
-    char* h = e.host.at<char>();
+    char* h = host.at<char>();
     memcpy(h + o.v, v_enc, (uint64_t)B * N * 8);
     memcpy(h + o.g, g, (uint64_t)B * c.n1 * 8);
     uint32_t* ht = reinterpret_cast<uint32_t*>(h + o.t);
@@ -559,37 +480,48 @@ int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const 
     if (v_seeds) memcpy(h + o.seeds, v_seeds, (uint64_t)B * 32);
     else memset(h + o.seeds, 0, (uint64_t)B * 32);
     pack_meta(h, o, hm);
+    return BN_OK;
+}
 
+int job_launch(Engine& e, QueryJob& j, DevMem& ws, PinnedMem& host, cudaStream_t s, uint64_t* r_out, uint64_t* mv_out) {
+    const HostMeta& hm = *j.hm;
+    const RunLayout& o = j.o;
+    char* d = ws.at<char>();
+    char* h = host.at<char>();
     CU(cudaSetDevice(e.ctx->device));
-    CU(cudaMemcpyAsync(d, h, o.in_end, cudaMemcpyHostToDevice, e.stream));
-    const Meta m = meta_at(d, o, hm, &maps);
+    CU(cudaMemcpyAsync(d, h, o.in_end, cudaMemcpyHostToDevice, s));
+    const Meta m = meta_at(d, o, hm, &j.maps);
     Inputs in{reinterpret_cast<uint64_t*>(d + o.v), reinterpret_cast<uint64_t*>(d + o.g),
               reinterpret_cast<uint32_t*>(d + o.t), reinterpret_cast<uint32_t*>(d + o.t_nnz),
               reinterpret_cast<uint8_t*>(d + o.seeds)};
     const Scratch sc = scratch_at(d, o);
     Outputs out{reinterpret_cast<uint32_t*>(d + o.ids), reinterpret_cast<int64_t*>(d + o.scores),
                 reinterpret_cast<uint32_t*>(d + o.n), reinterpret_cast<int32_t*>(d + o.vfailed),
-                mv_out ? reinterpret_cast<uint64_t*>(d + o.mv) : nullptr};
+                j.want_mv ? reinterpret_cast<uint64_t*>(d + o.mv) : nullptr};
     if (hm.segs.empty()) {
-        CU(cudaMemsetAsync(out.n, 0, (uint64_t)B * 4, e.stream));
-        CU(cudaMemsetAsync(sc.err, 0, 4, e.stream));
+        CU(cudaMemsetAsync(out.n, 0, (uint64_t)j.B * 4, s));
+        CU(cudaMemsetAsync(sc.err, 0, 4, s));
     } else {
-        TRY(enqueue_pipeline(e.ctx, c, z, m, in, sc, out, e.stream));
+        TRY(enqueue_pipeline(e.ctx, e.c, j.z, m, in, sc, out, s));
     }
-    CU(cudaMemcpyAsync(h + o.out_begin, d + o.out_begin, o.out_end - o.out_begin, cudaMemcpyDeviceToHost, e.stream));
-    if (r_out && hm.total_out)
-        CU(cudaMemcpyAsync(r_out, d + o.r, hm.total_out * 8, cudaMemcpyDeviceToHost, e.stream));
-    if (mv_out && hm.total_out)
-        CU(cudaMemcpyAsync(mv_out, d + o.mv, hm.total_out * 8, cudaMemcpyDeviceToHost, e.stream));
-    CU(cudaStreamSynchronize(e.stream));
-    if (const uint32_t ev = *reinterpret_cast<uint32_t*>(h + o.err))
-        return fail(BN_ECUDA, "a device pipeline wait timed out (flags 0x%x); results discarded", ev);
+    CU(cudaMemcpyAsync(h + o.out_begin, d + o.out_begin, o.out_end - o.out_begin, cudaMemcpyDeviceToHost, s));
+    if (r_out && hm.total_out) CU(cudaMemcpyAsync(r_out, d + o.r, hm.total_out * 8, cudaMemcpyDeviceToHost, s));
+    if (mv_out && hm.total_out) CU(cudaMemcpyAsync(mv_out, d + o.mv, hm.total_out * 8, cudaMemcpyDeviceToHost, s));
+    return BN_OK;
+}
 
-    const uint32_t ks = std::max<uint32_t>(k, 1);
-    const uint32_t* hid = reinterpret_cast<uint32_t*>(h + o.ids);
-    const int64_t* hsc = reinterpret_cast<int64_t*>(h + o.scores);
-    const uint32_t* hn = reinterpret_cast<uint32_t*>(h + o.n);
-    for (uint32_t b = 0; b < B; ++b) {
+int job_finish(const QueryJob& j, const PinnedMem& host, uint32_t* ids, int64_t* scores, uint32_t* n_hits,
+               std::vector<int32_t>& vfailed) {
+    const HostMeta& hm = *j.hm;
+    const RunLayout& o = j.o;
+    const char* h = host.at<char>();
+    if (const uint32_t ev = *reinterpret_cast<const uint32_t*>(h + o.err))
+        return fail(BN_ECUDA, "a device pipeline wait timed out (flags 0x%x); results discarded", ev);
+    const uint32_t k = j.k, ks = std::max<uint32_t>(k, 1);
+    const uint32_t* hid = reinterpret_cast<const uint32_t*>(h + o.ids);
+    const int64_t* hsc = reinterpret_cast<const int64_t*>(h + o.scores);
+    const uint32_t* hn = reinterpret_cast<const uint32_t*>(h + o.n);
+    for (uint32_t b = 0; b < j.B; ++b) {
         const uint32_t nh = hm.segs.empty() ? 0 : hn[b];
         if (n_hits) n_hits[b] = nh;
         if (k) {
@@ -600,6 +532,23 @@ int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const 
     vfailed.assign(hm.vsegs.size(), -1);
     if (!hm.vsegs.empty()) memcpy(vfailed.data(), h + o.vfailed, hm.vsegs.size() * 4);
     return BN_OK;
+}
+
+// Host-buffer query: pack, one H2D, pipeline, one D2H, sync.
+int run_query(Engine& e, HostMeta& hm, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+              const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds, uint32_t trials, uint32_t k,
+              uint32_t* ids, int64_t* scores, uint32_t* n_hits, std::vector<int32_t>& vfailed, uint64_t* r_out,
+              uint64_t* mv_out) {
+    QueryJob j;
+    j.hm = &hm;
+    j.B = B;
+    j.trials = trials;
+    j.k = k;
+    j.want_mv = mv_out != nullptr;
+    TRY(job_prepare(e, j, e.ws, e.host, v_enc, g, t_idx, t_sign, t_nnz, v_seeds));
+    TRY(job_launch(e, j, e.ws, e.host, e.stream, r_out, mv_out));
+    CU(cudaStreamSynchronize(e.stream));
+    return job_finish(j, e.host, ids, scores, n_hits, vfailed);
 }
 
 // Verify a claimed r for one contiguous row range (Protocol 2 only).
@@ -731,7 +680,8 @@ int run_dense_terms(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* g, 
     return BN_OK;
 }
 
-}  // namespace
+}  // namespace api
+}  // namespace bn
 
 struct bn_plan {
     bn_flat* h = nullptr;

@@ -13,6 +13,7 @@
 
 #include "bn_b200.h"
 #include "bn_kernels.cuh"
+#include "bn_tc.cuh"
 
 // ------------------------------------------------------------------ context
 struct bn_ctx {
@@ -159,6 +160,114 @@ struct Engine {
     DevMem ws;
     PinnedMem host;
 };
+
+// ---------------------------------------------------------------- one pipeline run
+constexpr uint32_t MAX_TRIALS = 64;  // Protocol 2 trials per call
+
+struct TcMaps {  // host-side tensor maps of the U buffer, one per pass of <= 20 trials
+    CUtensorMap u[(MAX_TRIALS + TC_MAX_TRIALS - 1) / TC_MAX_TRIALS];
+};
+inline uint32_t pass_rows(uint32_t t_cnt) { return 8 * ((t_cnt + 1) & ~1u); }
+
+struct Meta {  // device pointers (+ host tensor maps)
+    const ScanSeg* segs;
+    const uint64_t* seg_blk;
+    uint32_t nseg;
+    uint64_t total_blocks;
+    const VerifySeg* vsegs;
+    uint32_t nvseg;
+    const DecodeQuery* dq;
+    const TcBlock* tc_blocks;
+    uint32_t nblocks;
+    const TcPanel* tc_panels;
+    uint32_t npanels;
+    const uint32_t* seg_panel0;
+    const uint32_t* seg_block0;
+    const TcMaps* maps;
+};
+struct Scratch {  // device pointers
+    QLimb* limbs;
+    uint64_t* x;
+    uint64_t* r;
+    uint64_t* z_part;
+    uint64_t* ur_part;
+    uint32_t* flags;
+    uint64_t* ur;
+    uint64_t* zv;
+    TopkScratch topk;
+    uint32_t* err;  // device pipeline timeout flags
+    uint8_t* u_buf;
+    uint64_t* r_part;  // fused pass: per strip-group partial dots
+    uint64_t* zv_chunks;
+};
+struct Inputs {
+    const uint64_t* v;
+    const uint64_t* g;
+    const uint32_t* t;
+    const uint32_t* t_nnz;
+    const uint8_t* seeds;
+};
+struct Outputs {
+    uint32_t* ids;
+    int64_t* scores;
+    uint32_t* n;
+    int32_t* vfailed;  // per verify segment
+    uint64_t* mv;      // nullable
+};
+
+struct HostMeta {
+    std::vector<ScanSeg> segs;
+    std::vector<uint64_t> seg_blk;
+    std::vector<VerifySeg> vsegs;
+    std::vector<DecodeQuery> dq;
+    std::vector<uint32_t> seg_cluster;  // IVF: list id of each segment
+    std::vector<TcBlock> blocks;        // 128-row blocks of every verify segment
+    std::vector<TcPanel> panels;        // 4096-row panels of every verify segment
+    std::vector<uint32_t> seg_block0, seg_panel0;
+    uint64_t total_out = 0, max_rows = 0;
+};
+
+struct Sizes {
+    uint32_t B, n1, trials, k, ctas;
+    uint64_t total_out, nseg, nvseg, nblocks, npanels;
+    FreivaldsPlan fp;  // CUDA-core engine
+    int engine;        // BN_ENGINE_*
+};
+
+
+// Offsets of every device buffer of one pipeline run.
+struct RunLayout {
+    // inputs (contiguous from 0 -> one H2D)
+    uint64_t v, g, t, t_nnz, seeds, segs, seg_blk, vsegs, dq, tc_blocks, tc_panels, seg_panel0, seg_block0, in_end;
+    // outputs (contiguous -> one D2H)
+    uint64_t ids, scores, n, vfailed, ur, zv, err, out_begin, out_end;
+    // internal
+    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, r_part, zv_chunks, total;
+};
+
+// One run of the query pipeline over host inputs (bn_capi.cu): hm is the
+// segment metadata of the B queries, kept alive by the caller.
+struct QueryJob {
+    const HostMeta* hm = nullptr;
+    uint32_t B = 0, trials = 0, k = 0;
+    bool want_mv = false;
+    Sizes z{};
+    RunLayout o{};
+    TcMaps maps;
+};
+void finish_meta(HostMeta& hm);
+void flat_meta(uint64_t m, uint32_t B, HostMeta& hm);
+Sizes sizes_for(const Engine& e, const HostMeta& hm, uint32_t B, uint32_t trials, uint32_t k);
+RunLayout make_layout(const Sizes& z, bool want_mv);
+// Validates and packs the inputs into host (pinned, grown as needed) and
+// sizes ws (grown as needed, budget-accounted).
+int job_prepare(Engine& e, QueryJob& j, DevMem& ws, PinnedMem& host, const uint64_t* v_enc, const uint64_t* g,
+                const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds);
+// Enqueues H2D, the pipeline and the D2H of the outputs on s; waits for nothing.
+int job_launch(Engine& e, QueryJob& j, DevMem& ws, PinnedMem& host, cudaStream_t s, uint64_t* r_out, uint64_t* mv_out);
+// After s has drained: device flags, hits (k per query) and per-segment verdicts.
+int job_finish(const QueryJob& j, const PinnedMem& host, uint32_t* ids, int64_t* scores, uint32_t* n_hits,
+               std::vector<int32_t>& vfailed);
 
 // Block scoring (bn_block.cu).
 struct BlockPlan;
