@@ -59,6 +59,70 @@ def to_residues(x8: np.ndarray) -> np.ndarray:
     return out
 
 
+def synth_ivf(rows: int, d: int, nlist: int, seed: int):
+    """Gaussian mixture with nlist unit-norm centres and Zipf(1.1) component
+    weights; points = centre + 0.3 * N(0, I) / sqrt(d), L2-normalised,
+    int8-quantised per row.  The component of each point is its inverted
+    list (stands in for the k-means partition, which is not pinned to the
+    reference either); lists are stored in list order."""
+    rng = np.random.default_rng([seed, 0x1FF])
+    centres = rng.standard_normal((nlist, d), dtype=np.float32)
+    centres /= np.linalg.norm(centres, axis=1, keepdims=True)
+    w = 1.0 / np.arange(1, nlist + 1, dtype=np.float64) ** 1.1
+    w /= w.sum()
+    counts = rng.multinomial(rows, w)
+    sizes = np.zeros(nlist, np.int64)
+    sizes[rng.permutation(nlist)] = counts
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    m8 = np.empty((rows, d), np.int8)
+    sigma = np.float32(0.3 / np.sqrt(d))
+    c0 = 0
+    while c0 < nlist:  # lists in chunks of ~256k rows
+        c1 = c0
+        while c1 < nlist and offsets[c1] - offsets[c0] < 262144:
+            c1 += 1
+        c1 = max(c1, c0 + 1)
+        r0, r1 = int(offsets[c0]), int(offsets[c1])
+        lab = np.repeat(np.arange(c0, c1), sizes[c0:c1])
+        x = centres[lab] + sigma * rng.standard_normal((r1 - r0, d), dtype=np.float32)
+        x /= np.linalg.norm(x, axis=1, keepdims=True)
+        s = 127.0 / np.maximum(np.abs(x).max(axis=1, keepdims=True), 1e-12)
+        m8[r0:r1] = np.clip(np.rint(x * s), -127, 127).astype(np.int8)
+        c0 = c1
+    ids = rng.permutation(rows).astype(np.uint32)
+    return {"centres": centres, "weights": w, "sizes": sizes, "offsets": offsets, "m8": m8, "ids": ids,
+            "sigma": sigma, "seed": seed}
+
+
+def synth_ivf_queries(data, nq: int, seed: int):
+    """Queries drawn like the corpus points (component by weight): f32 for
+    routing, int8 for encoding."""
+    rng = np.random.default_rng([seed, 0x9E])
+    nlist, d = data["centres"].shape
+    comp = rng.choice(nlist, size=nq, p=data["sizes"] / data["sizes"].sum())
+    x = data["centres"][comp] + data["sigma"] * rng.standard_normal((nq, d), dtype=np.float32)
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    s = 127.0 / np.maximum(np.abs(x).max(axis=1, keepdims=True), 1e-12)
+    return x.astype(np.float32), np.clip(np.rint(x * s), -127, 127).astype(np.int8)
+
+
+def build_ivf(ctx, data, seed: int):
+    """BN-encrypts every list on the device (per-list h_seed, ivf.rs:258-264)."""
+    from bn_b200 import capi
+
+    rows = int(data["offsets"][-1])
+    L = capi.host_generate_subspace(bytes([seed & 0xFF, 0x1F]) * 16)
+    data["L"] = L
+    H, rp, ix, sg = capi.host_regenerate_h_s_lists(seed, data["offsets"])
+    mq = np.zeros((rows, N_DIM), np.uint64)
+    blk = 1 << 18
+    for r0 in range(0, rows, blk):
+        mq[r0 : r0 + blk] = to_residues(data["m8"][r0 : r0 + blk])
+    ivf = capi.Ivf.build_from_plain(ctx, data["offsets"], data["ids"], mq.reshape(-1), L, H, rp, ix, sg)
+    del mq, H, rp, ix, sg
+    return ivf
+
+
 class ClockSampler:
     """nvidia-smi clock / throttle sampling during the timed region."""
 

@@ -271,6 +271,9 @@ typedef struct bn_server_config {
     uint32_t max_wait_us; /* batching window */
     uint32_t trials;      /* Protocol 2 trials per query (params.verification_trials()) */
     uint32_t k;           /* hits per query */
+    uint32_t block_min;   /* flat batches of >= block_min requests run as block scoring (bn_flat_block_plan):
+                             one pass over the corpus for the batch, Protocol 2 per block with the first
+                             request's seed; 0 = every flat query verified with its own seed */
 } bn_server_config;
 typedef struct bn_server_stats_t {
     uint64_t submitted, completed, batches;
@@ -278,6 +281,7 @@ typedef struct bn_server_stats_t {
     double p50_us, p99_us, max_us;     /* submit -> result latency */
     double throughput_qps;             /* completed / (last completion - first submit) */
     uint64_t peak_workspace_bytes;
+    uint64_t block_batches;            /* flat batches that ran as block scoring */
 } bn_server_stats_t;
 /* flat and/or ivf (nullable, not both), with client state, in one context. */
 int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn_server** out);

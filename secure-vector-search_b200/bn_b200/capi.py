@@ -43,13 +43,13 @@ class SparseCsr(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("max_batch", u32), ("slots", u32), ("mem_budget", u64), ("max_wait_us", u32), ("trials", u32),
-                ("k", u32)]
+                ("k", u32), ("block_min", u32)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("submitted", u64), ("completed", u64), ("batches", u64), ("mean_batch", C.c_double),
                 ("p50_us", C.c_double), ("p99_us", C.c_double), ("max_us", C.c_double),
-                ("throughput_qps", C.c_double), ("peak_workspace_bytes", u64)]
+                ("throughput_qps", C.c_double), ("peak_workspace_bytes", u64), ("block_batches", u64)]
 
 
 _SIGS = {
@@ -440,9 +440,10 @@ class Ivf:
 class Server:
     """bn_server: continuous batching of flat and IVF queries over resident corpora."""
 
-    def __init__(self, flat=None, ivf=None, max_batch=64, slots=4, mem_budget=0, max_wait_us=200, trials=20, k=10):
+    def __init__(self, flat=None, ivf=None, max_batch=64, slots=4, mem_budget=0, max_wait_us=200, trials=20, k=10,
+                 block_min=0):
         self.flat, self.ivf, self.k = flat, ivf, k
-        cfg = ServerConfig(max_batch, slots, mem_budget, max_wait_us, trials, k)
+        cfg = ServerConfig(max_batch, slots, mem_budget, max_wait_us, trials, k, block_min)
         out = vp()
         check(lib.bn_server_create(flat.h if flat else None, ivf.h if ivf else None, C.byref(cfg), C.byref(out)))
         self.h = out

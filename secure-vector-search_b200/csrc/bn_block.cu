@@ -241,6 +241,50 @@ int autotune(BlockPlan& b, cudaStream_t s) {
 
 }  // namespace
 
+// Offsets of every buffer of a block plan's workspace; returns its size.
+uint64_t block_layout(BlockPlan& b, uint32_t n1, uint32_t k_alh, bool verify_only) {
+    const uint32_t B = b.B, k = b.k, trials = b.trials;
+    const uint32_t ks = std::max<uint32_t>(k, 1);
+    const uint32_t tt = std::max<uint32_t>(trials, 1);
+    Layout L;
+    b.o_err = L.take<uint32_t>(2);  // [0] pipeline flags, [1] operand range flags
+    b.o_bad = b.o_err + 4;
+    b.o_vseg = L.take<VerifySeg>(1);
+    b.o_blocks = L.take<TcBlock>(b.nblocks);
+    b.o_panels = L.take<TcPanel>(b.npanels);
+    const uint64_t qb = verify_only ? 0 : B;  // per-query operand buffers of the scoring GEMMs
+    b.o_vp = L.take<uint8_t>(8ull * qb * N);
+    b.o_gx = L.take<uint8_t>(8ull * qb * k_alh);
+    b.o_tv = L.take<uint8_t>(8ull * qb * 2 * N);
+    b.o_x = L.take<uint64_t>(qb * n1);
+    b.o_r = L.take<uint64_t>((uint64_t)B * b.nld);    // r = M_enc v
+    b.o_f2 = L.take<uint64_t>(qb * b.nld);             // -(AL g + H x)
+    b.o_f3 = L.take<uint64_t>(qb * b.nld);             // M T + S v   (Mv = r + f2 - f3)
+    b.o_rp = L.take<uint8_t>(8ull * B * b.npad);
+    b.o_ub = L.take<uint8_t>(trials ? (uint64_t)b.n_rows * b.npad : 0);
+    b.o_zpart = L.take<uint64_t>(trials ? (uint64_t)b.npanels * tt * N : 0);
+    b.o_z = L.take<uint64_t>((uint64_t)tt * N);
+    b.o_zv = L.take<uint64_t>((uint64_t)tt * B);
+    b.o_urpart = L.take<uint64_t>(trials ? (uint64_t)((b.npad + 4095) / 4096) * tt * B : 0);
+    b.o_ur = L.take<uint64_t>((uint64_t)tt * B);
+    b.o_fail = L.take<int32_t>(B);
+    b.o_cs = L.take<int64_t>((uint64_t)B * b.topk_ctas * ks);
+    b.o_ci = L.take<uint32_t>((uint64_t)B * b.topk_ctas * ks);
+    b.o_cn = L.take<uint32_t>((uint64_t)B * b.topk_ctas);
+    // host-buffer staging: inputs then outputs, contiguous
+    b.o_in = L.take<uint8_t>(0);
+    b.o_in_v = L.take<uint64_t>((uint64_t)B * N);
+    b.o_in_g = L.take<uint64_t>((uint64_t)B * n1);
+    b.o_in_t = L.take<uint32_t>((uint64_t)B * N);
+    b.o_in_tn = L.take<uint32_t>(B);
+    b.o_in_seed = L.take<uint8_t>(32);
+    b.o_out_ids = L.take<uint32_t>((uint64_t)B * ks);
+    b.o_out_sc = L.take<int64_t>((uint64_t)B * ks);
+    b.o_out_n = L.take<uint32_t>(B);
+    b.o_out_end = L.take<uint8_t>(0);
+    return L.off + 1024;
+}
+
 int block_prepare(bn_flat* f) {
     std::lock_guard<std::mutex> g(f->e.mu);
     return block_prepare_locked(f->e);
@@ -282,45 +326,8 @@ int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint3
     }
     const int sms = f->e.ctx->num_sms;
     b->topk_ctas = (int)std::max<uint64_t>(1, std::min<uint64_t>((c.rows + 511) / 512, (uint64_t)sms * 4 / B));
-    const uint32_t ks = std::max<uint32_t>(k, 1);
-    const uint32_t tt = std::max<uint32_t>(trials, 1);
-    Layout L;
-    b->o_err = L.take<uint32_t>(2);  // [0] pipeline flags, [1] operand range flags
-    b->o_bad = b->o_err + 4;
-    b->o_vseg = L.take<VerifySeg>(1);
-    b->o_blocks = L.take<TcBlock>(b->nblocks);
-    b->o_panels = L.take<TcPanel>(b->npanels);
-    const uint64_t qb = verify_only ? 0 : B;  // per-query operand buffers of the scoring GEMMs
-    b->o_vp = L.take<uint8_t>(8ull * qb * N);
-    b->o_gx = L.take<uint8_t>(8ull * qb * c.k_alh);
-    b->o_tv = L.take<uint8_t>(8ull * qb * 2 * N);
-    b->o_x = L.take<uint64_t>(qb * c.n1);
-    b->o_r = L.take<uint64_t>((uint64_t)B * b->nld);    // r = M_enc v
-    b->o_f2 = L.take<uint64_t>(qb * b->nld);             // -(AL g + H x)
-    b->o_f3 = L.take<uint64_t>(qb * b->nld);             // M T + S v   (Mv = r + f2 - f3)
-    b->o_rp = L.take<uint8_t>(8ull * B * b->npad);
-    b->o_ub = L.take<uint8_t>(trials ? (uint64_t)b->n_rows * b->npad : 0);
-    b->o_zpart = L.take<uint64_t>(trials ? (uint64_t)b->npanels * tt * N : 0);
-    b->o_z = L.take<uint64_t>((uint64_t)tt * N);
-    b->o_zv = L.take<uint64_t>((uint64_t)tt * B);
-    b->o_urpart = L.take<uint64_t>(trials ? (uint64_t)((b->npad + 4095) / 4096) * tt * B : 0);
-    b->o_ur = L.take<uint64_t>((uint64_t)tt * B);
-    b->o_fail = L.take<int32_t>(B);
-    b->o_cs = L.take<int64_t>((uint64_t)B * b->topk_ctas * ks);
-    b->o_ci = L.take<uint32_t>((uint64_t)B * b->topk_ctas * ks);
-    b->o_cn = L.take<uint32_t>((uint64_t)B * b->topk_ctas);
-    // host-buffer staging: inputs then outputs, contiguous
-    b->o_in = L.take<uint8_t>(0);
-    b->o_in_v = L.take<uint64_t>((uint64_t)B * N);
-    b->o_in_g = L.take<uint64_t>((uint64_t)B * c.n1);
-    b->o_in_t = L.take<uint32_t>((uint64_t)B * N);
-    b->o_in_tn = L.take<uint32_t>(B);
-    b->o_in_seed = L.take<uint8_t>(32);
-    b->o_out_ids = L.take<uint32_t>((uint64_t)B * ks);
-    b->o_out_sc = L.take<int64_t>((uint64_t)B * ks);
-    b->o_out_n = L.take<uint32_t>(B);
-    b->o_out_end = L.take<uint8_t>(0);
-    int rc = b->ws.alloc(f->e.ctx, L.off + 1024);
+    const uint64_t total = block_layout(*b, c.n1, c.k_alh, verify_only);
+    int rc = b->ws.alloc(f->e.ctx, total);
     cudaStream_t s = f->e.stream;
     if (rc == BN_OK) {
         // metadata: the whole corpus is one verification segment
@@ -337,9 +344,9 @@ int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint3
         }
         if (cudaMemsetAsync(b->ws.p, 0, b->o_vseg, s) != cudaSuccess ||
             cudaMemcpyAsync(b->ws.at<char>() + b->o_vseg, hm.data(), hm.size(), cudaMemcpyHostToDevice, s) != cudaSuccess ||
-            cudaMemsetAsync(b->ws.at<char>() + b->o_gx, 0, 8ull * qb * c.k_alh, s) != cudaSuccess ||
+            cudaMemsetAsync(b->ws.at<char>() + b->o_gx, 0, verify_only ? 0 : 8ull * B * c.k_alh, s) != cudaSuccess ||
             cudaMemsetAsync(b->ws.at<char>() + b->o_rp, 0, 8ull * B * b->npad, s) != cudaSuccess ||
-            cudaMemsetAsync(b->ws.at<char>() + b->o_vp, 0, 8ull * qb * N, s) != cudaSuccess ||
+            cudaMemsetAsync(b->ws.at<char>() + b->o_vp, 0, verify_only ? 0 : 8ull * B * N, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess)
             rc = fail(BN_ECUDA, "block plan set-up failed");
     }
@@ -357,6 +364,25 @@ int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint3
     }
     *out = b;
     return BN_OK;
+}
+
+// Workspace bytes a block plan of B queries would allocate (the corpus's
+// byte-planar copies, made once per handle, are not included).
+uint64_t block_plan_estimate(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k) {
+    const Corpus& c = f->e.c;
+    BlockPlan b;
+    b.B = B;
+    b.trials = trials;
+    b.k = k;
+    b.rows = c.rows;
+    b.nld = align_up(c.rows, 16);
+    b.npad = align_up(c.rows, 128);
+    b.t_pass = std::min<uint32_t>(std::max<uint32_t>(trials, 1), TC_MAX_TRIALS);
+    b.n_rows = 8 * ((b.t_pass + 1) & ~1u);
+    b.nblocks = (uint32_t)((c.rows + TC_ROWS - 1) / TC_ROWS);
+    b.npanels = (uint32_t)((c.rows + TC_PANEL_ROWS - 1) / TC_PANEL_ROWS);
+    b.topk_ctas = (int)std::max<uint64_t>(1, std::min<uint64_t>((c.rows + 511) / 512, (uint64_t)f->e.ctx->num_sms * 4 / B));
+    return block_layout(b, c.n1, (uint32_t)align_up(2ull * c.n1, 128), false);
 }
 
 void block_plan_config(const BlockPlan* b, uint32_t cfg[5], float tuned_ms[2]) {
@@ -489,21 +515,26 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     return BN_OK;
 }
 
-// Host-buffer block query: one H2D of the packed inputs, the block pipeline,
-// one D2H of the ranked hits.
-int block_query_host(BlockPlan& b, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
-                     const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed, uint32_t* ids, int64_t* scores,
-                     uint32_t* n_hits, int32_t* failed, uint64_t* mv_out) {
+// Host-buffer block query in two steps (so that a caller can keep several in
+// flight): launch packs the first nq <= B queries (the rest of the block is
+// padded with zero queries whose results are dropped), enqueues one H2D, the
+// block pipeline and one D2H on s; finish reads the outputs after s drained.
+int block_query_launch(BlockPlan& b, uint32_t nq, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                       const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed, cudaStream_t s, bool want_mv) {
     Corpus& c = b.h->e.c;
-    const uint32_t B = b.B, ks = std::max<uint32_t>(b.k, 1);
-    TRY(b.host.reserve(b.o_out_end - b.o_in + (uint64_t)B * 4));
+    const uint32_t B = b.B;
+    if (nq > B) return fail(BN_EINVAL, "%u queries for a block plan of %u", nq, B);
+    TRY(b.host.reserve(b.o_out_end - b.o_in + (uint64_t)B * 4 + 8));
     char* h = b.host.at<char>();
     auto at = [&](uint64_t off) { return h + (off - b.o_in); };
-    memcpy(at(b.o_in_v), v_enc, (uint64_t)B * N * 8);
-    memcpy(at(b.o_in_g), g, (uint64_t)B * c.n1 * 8);
+    memset(at(b.o_in_v), 0, (uint64_t)B * N * 8);
+    memset(at(b.o_in_g), 0, (uint64_t)B * c.n1 * 8);
+    memset(at(b.o_in_tn), 0, (uint64_t)B * 4);
+    memcpy(at(b.o_in_v), v_enc, (uint64_t)nq * N * 8);
+    memcpy(at(b.o_in_g), g, (uint64_t)nq * c.n1 * 8);
     uint32_t* ht = reinterpret_cast<uint32_t*>(at(b.o_in_t));
     uint64_t tp = 0;
-    for (uint32_t q = 0; q < B; ++q) {
+    for (uint32_t q = 0; q < nq; ++q) {
         if (t_nnz[q] > N) return fail(BN_EINVAL, "t_nnz[%u] = %u exceeds n", q, t_nnz[q]);
         for (uint32_t i = 0; i < t_nnz[q]; ++i, ++tp) {
             if (t_idx[tp] >= N || (t_sign[tp] != 1 && t_sign[tp] != -1))
@@ -511,34 +542,36 @@ int block_query_host(BlockPlan& b, const uint64_t* v_enc, const uint64_t* g, con
             ht[(uint64_t)q * N + i] = t_idx[tp] | (t_sign[tp] < 0 ? 0x80000000u : 0u);
         }
     }
-    memcpy(at(b.o_in_tn), t_nnz, (uint64_t)B * 4);
+    memcpy(at(b.o_in_tn), t_nnz, (uint64_t)nq * 4);
     if (seed) memcpy(at(b.o_in_seed), seed, 32);
     else memset(at(b.o_in_seed), 0, 32);
     char* d = b.ws.at<char>();
-    cudaStream_t s = b.h->e.stream;
     CU(cudaSetDevice(b.h->e.ctx->device));
     CU(cudaMemcpyAsync(d + b.o_in, h, b.o_out_ids - b.o_in, cudaMemcpyHostToDevice, s));
     TRY(block_enqueue(b, reinterpret_cast<uint64_t*>(d + b.o_in_v), reinterpret_cast<uint64_t*>(d + b.o_in_g),
                       reinterpret_cast<uint32_t*>(d + b.o_in_t), reinterpret_cast<uint32_t*>(d + b.o_in_tn),
                       reinterpret_cast<uint8_t*>(d + b.o_in_seed), reinterpret_cast<uint32_t*>(d + b.o_out_ids),
                       reinterpret_cast<int64_t*>(d + b.o_out_sc), reinterpret_cast<uint32_t*>(d + b.o_out_n),
-                      reinterpret_cast<int32_t*>(d + b.o_fail), s, mv_out != nullptr));
-    int32_t* hf = reinterpret_cast<int32_t*>(h + (b.o_out_end - b.o_in));
+                      reinterpret_cast<int32_t*>(d + b.o_fail), s, want_mv));
+    char* hf = h + (b.o_out_end - b.o_in);
     CU(cudaMemcpyAsync(at(b.o_out_ids), d + b.o_out_ids, b.o_out_end - b.o_out_ids, cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(hf, d + b.o_fail, (uint64_t)B * 4, cudaMemcpyDeviceToHost, s));
-    if (mv_out)
-        for (uint32_t q = 0; q < B; ++q)
-            CU(cudaMemcpyAsync(mv_out + (uint64_t)q * c.rows, d + b.o_f3 + (uint64_t)q * b.nld * 8, c.rows * 8,
-                               cudaMemcpyDeviceToHost, s));
-    uint32_t flags[2] = {0, 0};
-    CU(cudaMemcpyAsync(flags, d + b.o_err, 8, cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
+    CU(cudaMemcpyAsync(hf + (uint64_t)B * 4, d + b.o_err, 8, cudaMemcpyDeviceToHost, s));
+    return BN_OK;
+}
+
+int block_query_finish(BlockPlan& b, uint32_t nq, uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed) {
+    const uint32_t B = b.B, ks = std::max<uint32_t>(b.k, 1);
+    char* h = b.host.at<char>();
+    auto at = [&](uint64_t off) { return h + (off - b.o_in); };
+    const int32_t* hf = reinterpret_cast<const int32_t*>(h + (b.o_out_end - b.o_in));
+    const uint32_t* flags = reinterpret_cast<const uint32_t*>(hf + B);
     if (flags[0]) return fail(BN_ECUDA, "a device pipeline wait timed out or a draw hit p (flags 0x%x)", flags[0]);
     if (flags[1]) return fail(BN_EINVAL, "a T column sum leaves [-128, 127]");
-    const uint32_t* hid = reinterpret_cast<uint32_t*>(at(b.o_out_ids));
-    const int64_t* hsc = reinterpret_cast<int64_t*>(at(b.o_out_sc));
-    const uint32_t* hn = reinterpret_cast<uint32_t*>(at(b.o_out_n));
-    for (uint32_t q = 0; q < B; ++q) {
+    const uint32_t* hid = reinterpret_cast<const uint32_t*>(at(b.o_out_ids));
+    const int64_t* hsc = reinterpret_cast<const int64_t*>(at(b.o_out_sc));
+    const uint32_t* hn = reinterpret_cast<const uint32_t*>(at(b.o_out_n));
+    for (uint32_t q = 0; q < nq; ++q) {
         const uint32_t nh = b.k ? hn[q] : 0;
         if (n_hits) n_hits[q] = nh;
         for (uint32_t i = 0; i < nh; ++i) {
@@ -549,6 +582,24 @@ int block_query_host(BlockPlan& b, const uint64_t* v_enc, const uint64_t* g, con
     }
     return BN_OK;
 }
+
+// Host-buffer block query: one H2D of the packed inputs, the block pipeline,
+// one D2H of the ranked hits.
+int block_query_host(BlockPlan& b, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                     const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed, uint32_t* ids, int64_t* scores,
+                     uint32_t* n_hits, int32_t* failed, uint64_t* mv_out) {
+    Corpus& c = b.h->e.c;
+    cudaStream_t s = b.h->e.stream;
+    TRY(block_query_launch(b, b.B, v_enc, g, t_idx, t_sign, t_nnz, seed, s, mv_out != nullptr));
+    if (mv_out)
+        for (uint32_t q = 0; q < b.B; ++q)
+            CU(cudaMemcpyAsync(mv_out + (uint64_t)q * c.rows, b.ws.at<char>() + b.o_f3 + (uint64_t)q * b.nld * 8,
+                               c.rows * 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    return block_query_finish(b, b.B, ids, scores, n_hits, failed);
+}
+
+uint64_t block_plan_bytes(const BlockPlan* b) { return b->ws.bytes; }
 
 // Protocol 2 over claimed responses r (B x m, host) with the block seed.
 int block_verify_host(BlockPlan& b, const uint64_t* r, const uint64_t* v_enc, const uint8_t* seed, int32_t* failed,

@@ -309,6 +309,11 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
 int block_query_host(BlockPlan& b, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
                      const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed, uint32_t* ids, int64_t* scores,
                      uint32_t* n_hits, int32_t* failed, uint64_t* mv_out);
+int block_query_launch(BlockPlan& b, uint32_t nq, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                       const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed, cudaStream_t s, bool want_mv);
+int block_query_finish(BlockPlan& b, uint32_t nq, uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed);
+uint64_t block_plan_bytes(const BlockPlan* b);
+uint64_t block_plan_estimate(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k);
 int block_verify_host(BlockPlan& b, const uint64_t* r, const uint64_t* v_enc, const uint8_t* seed, int32_t* failed,
                       uint64_t* ur, uint64_t* zv);
 }  // namespace api

@@ -65,6 +65,13 @@ struct Slot {
     std::vector<Request> reqs;
     HostMeta hm;
     QueryJob job;
+    // block scoring of flat batches: a plan for blocks of bp_B queries
+    BlockPlan* bp = nullptr;
+    uint32_t bp_B = 0;
+    bool block_run = false;
+    ~Slot() {
+        if (bp) block_plan_free(bp);
+    }
 };
 
 }  // namespace
@@ -82,7 +89,8 @@ struct bn_server {
     bool stop = false;
     std::thread sched;
     // statistics
-    uint64_t submitted = 0, completed = 0, batches = 0, batched_queries = 0, peak_mem = 0;
+    uint64_t submitted = 0, completed = 0, batches = 0, batched_queries = 0, block_batches = 0, peak_mem = 0;
+    bool block_off = false;  // block scoring refused by the corpus: per-query path only
     std::vector<double> lat_us;
     Clock::time_point t_first{}, t_last{};
 };
@@ -120,8 +128,14 @@ void batch_meta(bn_server* s, int kind, It first, It last, HostMeta& hm) {
     finish_meta(hm);
 }
 
-// Device workspace of a batch made of the first `count` requests of q.
+uint32_t block_bucket(bn_server* s, size_t count);
+
+// Device workspace of a batch made of the first `count` requests of q (a
+// block plan's workspace when the batch runs as a block).
 uint64_t batch_bytes(bn_server* s, int kind, const std::deque<Request>& q, size_t count) {
+    if (kind == BN_SERVER_FLAT)
+        if (const uint32_t bucket = block_bucket(s, count))
+            return block_plan_estimate(s->flat, bucket, s->cfg.trials, s->cfg.k);
     HostMeta hm;
     batch_meta(s, kind, q.begin(), q.begin() + count, hm);
     const Sizes z = sizes_for(engine_of(s, kind), hm, (uint32_t)count, s->cfg.trials, s->cfg.k);
@@ -148,7 +162,10 @@ void harvest(bn_server* s, Slot& sl) {
     std::vector<int32_t> vf;
     std::vector<Result> res(B);
     int rc = cudaEventSynchronize(sl.done) == cudaSuccess ? BN_OK : fail(BN_ECUDA, "batch failed on the device");
-    if (rc == BN_OK) rc = job_finish(sl.job, sl.host, ids.data(), sc.data(), nh.data(), vf);
+    std::vector<int32_t> bf(B, -1);
+    if (rc == BN_OK)
+        rc = sl.block_run ? block_query_finish(*sl.bp, B, ids.data(), sc.data(), nh.data(), bf.data())
+                          : job_finish(sl.job, sl.host, ids.data(), sc.data(), nh.data(), vf);
     for (uint32_t b = 0; b < B; ++b) {
         Result& r = res[b];
         r.status = rc;
@@ -158,6 +175,10 @@ void harvest(bn_server* s, Slot& sl) {
         }
         r.ids.assign(ids.begin() + (uint64_t)b * k, ids.begin() + (uint64_t)b * k + nh[b]);
         r.scores.assign(sc.begin() + (uint64_t)b * k, sc.begin() + (uint64_t)b * k + nh[b]);
+        if (sl.block_run) {
+            r.failed_trial = bf[b];
+            continue;
+        }
         const DecodeQuery& dq = sl.hm.dq[b];
         for (uint32_t g = dq.seg0; g < dq.seg0 + dq.nseg; ++g)
             if (vf[g] >= 0) {
@@ -192,15 +213,41 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
         ts.insert(ts.end(), r.t_sign.begin(), r.t_sign.end());
         memcpy(&seeds[(uint64_t)b * 32], r.seed, 32);
     }
-    sl.job = QueryJob();
-    sl.job.hm = &sl.hm;
-    sl.job.B = B;
-    sl.job.trials = s->cfg.trials;
-    sl.job.k = s->cfg.k;
-    Engine& e = engine_of(s, kind);
-    int rc = job_prepare(e, sl.job, sl.ws, sl.host, v.data(), g.data(), ti.empty() ? nullptr : ti.data(),
+    int rc = BN_OK;
+    const uint32_t bucket = kind == BN_SERVER_FLAT ? block_bucket(s, B) : 0;
+    sl.block_run = false;
+    if (bucket) {
+        // block scoring: the batch's queries share one pass over the corpus;
+        // Protocol 2 runs per block with the first request's seed
+        if (!sl.bp || sl.bp_B != bucket) {
+            if (sl.bp) block_plan_free(sl.bp);
+            sl.bp = nullptr;
+            sl.bp_B = 0;
+            sl.ws.release();  // this slot's per-query workspace is not needed while it runs blocks
+            rc = block_plan_create(s->flat, bucket, s->cfg.trials, s->cfg.k, 0, &sl.bp);
+            if (rc == BN_OK) sl.bp_B = bucket;
+        }
+        if (rc == BN_OK) {
+            sl.block_run = true;
+            rc = block_query_launch(*sl.bp, B, v.data(), g.data(), ti.empty() ? nullptr : ti.data(),
+                                    ts.empty() ? nullptr : ts.data(), tn.data(), seeds.data(), sl.stream, false);
+            if (rc == BN_OK) s->block_batches += 1;
+        } else if (rc == BN_EUNSUPPORTED) {
+            s->block_off = true;  // e.g. plaintext outside int8: serve flat queries per query from now on
+            rc = BN_OK;
+        }
+    }
+    if (!sl.block_run && rc == BN_OK) {
+        sl.job = QueryJob();
+        sl.job.hm = &sl.hm;
+        sl.job.B = B;
+        sl.job.trials = s->cfg.trials;
+        sl.job.k = s->cfg.k;
+        Engine& e = engine_of(s, kind);
+        rc = job_prepare(e, sl.job, sl.ws, sl.host, v.data(), g.data(), ti.empty() ? nullptr : ti.data(),
                          ts.empty() ? nullptr : ts.data(), tn.data(), seeds.data());
-    if (rc == BN_OK) rc = job_launch(e, sl.job, sl.ws, sl.host, sl.stream, nullptr, nullptr);
+        if (rc == BN_OK) rc = job_launch(e, sl.job, sl.ws, sl.host, sl.stream, nullptr, nullptr);
+    }
     if (rc == BN_OK && cudaEventRecord(sl.done, sl.stream) != cudaSuccess) rc = fail(BN_ECUDA, "cudaEventRecord failed");
     if (rc != BN_OK) {
         std::vector<Result> res(B);
@@ -218,10 +265,20 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
     return BN_OK;
 }
 
+uint64_t slot_bytes(const Slot& sl) { return sl.ws.bytes + (sl.bp ? block_plan_bytes(sl.bp) : 0); }
+
 uint64_t held_bytes(bn_server* s) {
     uint64_t t = 0;
-    for (auto& sl : s->slots) t += sl->ws.bytes;
+    for (auto& sl : s->slots) t += slot_bytes(*sl);
     return t;
+}
+
+// Block size a flat batch of `count` requests runs as (0: per-query path).
+uint32_t block_bucket(bn_server* s, size_t count) {
+    if (!s->cfg.block_min || count < s->cfg.block_min || s->block_off) return 0;
+    uint32_t b = 8;
+    while (b < count) b <<= 1;
+    return b;
 }
 
 // One scheduling decision for a free slot: the batch to launch (empty: none now).
@@ -239,7 +296,7 @@ std::vector<Request> take_batch(bn_server* s, Slot& me, int& kind_out, bool& rej
     if (q.size() < s->cfg.max_batch && age_us < s->cfg.max_wait_us) return {};
     // memory admission: the largest prefix whose workspace fits beside the
     // other slots' workspaces
-    const uint64_t others = held_bytes(s) - me.ws.bytes;
+    const uint64_t others = held_bytes(s) - slot_bytes(me);
     const uint64_t budget = s->cfg.mem_budget;
     size_t count = std::min<size_t>(q.size(), s->cfg.max_batch);
     while (count > 0 && budget && others + batch_bytes(s, kind, q, count) > budget) count = count > 8 ? count / 2 : count - 1;
@@ -249,8 +306,13 @@ std::vector<Request> take_batch(bn_server* s, Slot& me, int& kind_out, bool& rej
         if (!any_busy) {
             // idle slots keep their workspaces: give them back, then retry once
             for (auto& sl : s->slots)
-                if (sl.get() != &me) sl->ws.release();
-            if (batch_bytes(s, kind, q, 1) + held_bytes(s) - me.ws.bytes > budget) {
+                if (sl.get() != &me) {
+                    sl->ws.release();
+                    if (sl->bp) block_plan_free(sl->bp);
+                    sl->bp = nullptr;
+                    sl->bp_B = 0;
+                }
+            if (batch_bytes(s, kind, q, 1) + held_bytes(s) - slot_bytes(me) > budget) {
                 reject_front = true;  // this request alone exceeds the budget
                 reject_kind = kind;
             } else {
@@ -369,6 +431,7 @@ int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn
     if (!cfg->slots || cfg->slots > 16) return fail(BN_EINVAL, "slots must be in 1..=16");
     if (cfg->k > BN_TOPK_MAX) return fail(BN_EINVAL, "k = %u exceeds BN_TOPK_MAX", cfg->k);
     if (cfg->trials > BN_MAX_TRIALS) return fail(BN_EINVAL, "trials = %u exceeds %d", cfg->trials, BN_MAX_TRIALS);
+    if (cfg->block_min && !flat) return fail(BN_EINVAL, "block_min needs a flat corpus");
     auto* s = new bn_server();
     s->flat = flat;
     s->ivf = ivf;
@@ -449,6 +512,7 @@ int bn_server_stats(bn_server* s, int reset, bn_server_stats_t* out) {
     out->batches = s->batches;
     out->mean_batch = s->batches ? (double)s->batched_queries / (double)s->batches : 0.0;
     out->peak_workspace_bytes = s->peak_mem;
+    out->block_batches = s->block_batches;
     std::vector<double> l = s->lat_us;
     if (!l.empty()) {
         std::sort(l.begin(), l.end());
@@ -461,7 +525,7 @@ int bn_server_stats(bn_server* s, int reset, bn_server_stats_t* out) {
     }
     if (reset) {
         s->lat_us.clear();
-        s->batches = s->batched_queries = 0;
+        s->batches = s->batched_queries = s->block_batches = 0;
         s->submitted = s->completed = 0;
     }
     return BN_OK;

@@ -163,3 +163,21 @@ def test_wait_timeout_and_bad_requests(corpora):
         srv.submit_flat(bad, enc.g, enc.t_idx, enc.t_sign, bytes(32))
     assert e.value.code == c.BN_EINVAL  # not a canonical residue
     srv.close()
+
+
+def test_flat_block_batches_match_per_query(corpora):
+    """Flat batches of >= block_min requests run as block scoring (one pass
+    over the corpus for the batch): hits identical to the per-query path,
+    honest responses accepted."""
+    c = capi()
+    flat, L, ivf, case = corpora
+    reqs = [r for r in requests(L, case, 40, 7300) if r[0] == "flat"]
+    want = [direct(flat, ivf, r) for r in reqs]
+    srv = c.Server(flat, ivf, max_batch=16, slots=2, max_wait_us=20000, trials=TRIALS, k=K, block_min=4)
+    tickets = [submit(srv, r) for r in reqs]
+    got = [srv.wait(t)[:4] for t in tickets]
+    for g, w in zip(got, want):
+        assert same(g, w)
+    st = srv.stats()
+    assert st["block_batches"] > 0 and st["completed"] == len(reqs)
+    srv.close()
