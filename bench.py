@@ -338,6 +338,11 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     plans["noverify"].close()
     if args.block_sizes:
         res["block"] = run_block(args, flat, L, seed, dev, stream, res["value"], dist)
+    if args.ivf_rows:
+        res["ivf"], ivf, data = run_ivf(args, ctx, dist)
+        if args.serve_rates:
+            res["serving"] = run_serving(args, flat, ivf, L, data, dist)
+        ivf.close()
     flat.close()
     ctx.close()
     return res
@@ -453,6 +458,125 @@ def run_block(args, flat, L, seed, dev, stream, single_qps, dist):
     return out
 
 
+def encode_pool(L, n: int, x8: np.ndarray, seed: int):
+    """Encoded queries (v_enc, g, T) and their Protocol 2 seeds."""
+    from bn_b200 import capi
+
+    encs, seeds = [], []
+    for i in range(n):
+        q_seed = capi.host_derive_h_seed(seed ^ 0x5155455259, i)
+        encs.append(capi.host_encode_query(to_residues(x8[i : i + 1])[0], L, q_seed))
+        seeds.append(capi.host_domain_separate(q_seed))
+    return encs, seeds
+
+
+def run_ivf(args, ctx, dist):
+    """BN-IVF with uneven lists (Zipf-weighted Gaussian mixture, nlist 4096):
+    batches of 64 queries, nprobe 8 / 32 / 128, every probed list of every
+    query scanned, verified (Protocol 2, per query and list), decoded and
+    ranked in one launch per stage; through the C ABI with host buffers."""
+    from bn_b200 import capi
+
+    seed, nlist, bq = 3, 4096, 64
+    t0 = time.perf_counter()
+    data = synth_ivf(args.ivf_rows, 768, nlist, seed)
+    ivf = build_ivf(ctx, data, seed)
+    setup_s = time.perf_counter() - t0
+    qx, q8 = synth_ivf_queries(data, bq, seed)
+    encs, seeds = encode_pool(data["L"], bq, q8, seed)
+    out = {"N": args.ivf_rows, "nlist": nlist, "batch": bq, "trials": args.trials, "k": 10,
+           "lists": {"max": int(data["sizes"].max()), "median": float(np.median(data["sizes"])),
+                     "min": int(data["sizes"].min())},
+           "data": "synthetic Gaussian mixture, Zipf(1.1) weights; mixture components stand in for k-means lists",
+           "setup_s": setup_s, "per_nprobe": {}}
+    vb = np.stack([e[0] for e in encs])
+    gb = np.stack([e[1] for e in encs])
+    tb = [(e[2], e[3]) for e in encs]
+    for nprobe in (8, 32, 128):
+        pr = capi.host_probe_route(data["centres"], qx, nprobe)
+        rows_q = float(np.mean([data["sizes"][p].sum() for p in pr]))
+        hits, fc, ft = ivf.query(pr, vb, gb, tb, seeds, args.trials, 10)
+        assert np.all(fc == -1), "IVF verification failed on honest responses"
+        if dist:
+            dist.barrier()
+        reps, t = 3, []
+        for _ in range(reps):
+            ta = time.perf_counter()
+            ivf.query(pr, vb, gb, tb, seeds, args.trials, 10)
+            t.append(time.perf_counter() - ta)
+        dt = statistics.median(t)
+        out["per_nprobe"][str(nprobe)] = {"qps": bq / dt, "ms_per_batch": dt * 1e3, "rows_per_query": rows_q,
+                                          "effective_gbs": bq * rows_q * N_DIM * 8 / dt / 1e9}
+    return out, ivf, data
+
+
+def run_serving(args, flat, ivf, flat_L, data, dist):
+    """Poisson arrivals, 50% flat / 50% IVF with nprobe uniform in {8, 32,
+    128}, Protocol 2 on for all, through bn_server (continuous batching,
+    memory admission); every served result compared with the per-query path
+    on the same inputs."""
+    from bn_b200 import capi
+
+    seed, pool = 4, 256
+    rng = np.random.default_rng(seed)
+    fx8 = synth_int8(pool, 768, seed + 3000)
+    fenc, fseeds = encode_pool(flat_L, pool, fx8, seed)
+    qx, q8 = synth_ivf_queries(data, pool, seed + 1)
+    ienc, iseeds = encode_pool(data["L"], pool, q8, seed + 1)
+    nps = rng.choice([8, 32, 128], size=pool)
+    probes = [capi.host_probe_route(data["centres"], qx[i], int(nps[i]))[0] for i in range(pool)]
+    # per-query references (the plain per-query path on the same GPU)
+    ref_f, ref_i = [], []
+    for i in range(pool):
+        h, f, _, _ = flat.query(fenc[i][0][None], fenc[i][1][None], [(fenc[i][2], fenc[i][3])], [fseeds[i]],
+                                args.trials, 10)
+        ref_f.append((h[0][0], h[0][1], int(f[0])))
+        h, fc, ft = ivf.query(probes[i][None], ienc[i][0][None], ienc[i][1][None], [(ienc[i][2], ienc[i][3])],
+                              [iseeds[i]], args.trials, 10)
+        ref_i.append((h[0][0], h[0][1], int(ft[0])))
+    srv = capi.Server(flat, ivf, max_batch=64, slots=4, mem_budget=24 << 30, max_wait_us=1000, trials=args.trials,
+                      k=10, block_min=8)
+    out = {"corpora": {"flat_N": flat.m, "ivf_N": int(data["offsets"][-1]), "nlist": int(len(data["sizes"]))},
+           "config": {"max_batch": 64, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 8},
+           "mix": "50% flat / 50% IVF, nprobe uniform in {8, 32, 128}", "rates": {}}
+    for rate in [float(r) for r in args.serve_rates.split(",") if r]:
+        n = int(min(max(rate * args.serve_seconds, 200), 8000))
+        kinds = rng.random(n) < 0.5
+        picks = rng.integers(0, pool, size=n)
+        gaps = rng.exponential(1.0 / rate, size=n)
+        srv.stats(reset=True)
+        tickets = []
+        t_start = time.perf_counter()
+        due = t_start
+        for j in range(n):
+            due += gaps[j]
+            while time.perf_counter() < due:
+                pass
+            i = int(picks[j])
+            if kinds[j]:
+                e = fenc[i]
+                tickets.append(srv.submit_flat(e[0], e[1], e[2], e[3], fseeds[i]))
+            else:
+                e = ienc[i]
+                tickets.append(srv.submit_ivf(probes[i], e[0], e[1], e[2], e[3], iseeds[i]))
+        offered = n / (time.perf_counter() - t_start)
+        bad = 0
+        for j, t in enumerate(tickets):
+            ids, sc, ft, fc, lat = srv.wait(t, 600000)
+            ref = ref_f[picks[j]] if kinds[j] else ref_i[picks[j]]
+            if not (np.array_equal(ids, ref[0]) and np.array_equal(sc, ref[1]) and ft == ref[2]):
+                bad += 1
+        st = srv.stats()
+        out["rates"][str(int(rate))] = {"offered_qps": offered, "requests": n, "served_qps": st["throughput_qps"],
+                                        "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
+                                        "max_ms": st["max_us"] / 1e3, "mean_batch": st["mean_batch"],
+                                        "block_batches": st["block_batches"],
+                                        "peak_workspace_gib": st["peak_workspace_bytes"] / 2**30,
+                                        "mismatches_vs_per_query": bad}
+    srv.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -464,6 +588,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--block-sizes", default="8,32,128,512",
                     help="block scoring sizes B to time after the single-query metric ('' to skip)")
+    ap.add_argument("--ivf-rows", type=int, default=2_000_000, help="IVF corpus rows (0 to skip the IVF legs)")
+    ap.add_argument("--serve-rates", default="2000,10000,50000", help="Poisson arrival rates of the serving leg")
+    ap.add_argument("--serve-seconds", type=float, default=1.5)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -464,6 +464,17 @@ struct TopkBuf {
     int have_thr;
 };
 
+// Compaction decision, uniform across the CTA: every thread reads the count
+// between two barriers, so no thread can append (next iteration) before all
+// have read it; then either all threads compact or none does (topk_compact
+// holds __syncthreads).
+__device__ __forceinline__ bool topk_full(TopkBuf& b, int limit) {
+    __syncthreads();
+    const bool full = b.cnt > limit;
+    __syncthreads();
+    return full;
+}
+
 __device__ void topk_compact(TopkBuf& b, int k) {
     __syncthreads();
     const int cnt = b.cnt;
@@ -641,8 +652,7 @@ decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ 
         const int ht = buf.have_thr;
         topk_offer(buf, valid[0], score[0], id[0], ts, ti, ht);
         topk_offer(buf, valid[1], score[1], id[1], ts, ti, ht);
-        __syncthreads();
-        if (buf.cnt > CAND_CAP - 2 * DT_THREADS) topk_compact(buf, (int)k);
+        if (topk_full(buf, CAND_CAP - 2 * DT_THREADS)) topk_compact(buf, (int)k);
     }
     topk_compact(buf, (int)k);
     const int keep = min(buf.cnt, (int)k);
@@ -677,8 +687,7 @@ topk_merge_kernel(const int64_t* __restrict__ cand_s, const uint32_t* __restrict
         const uint32_t ti = buf.thr_i;
         const int ht = buf.have_thr;
         topk_offer(buf, valid, s, id, ts, ti, ht);
-        __syncthreads();
-        if (buf.cnt > CAND_CAP - DT_THREADS) topk_compact(buf, (int)k);
+        if (topk_full(buf, CAND_CAP - DT_THREADS)) topk_compact(buf, (int)k);
     }
     topk_compact(buf, (int)k);
     const int keep = min(buf.cnt, (int)k);
@@ -742,8 +751,7 @@ topk_rows_kernel(const uint64_t* __restrict__ ra, const uint64_t* __restrict__ r
         const int ht = buf.have_thr;
         topk_offer(buf, valid[0], sc[0], id[0], ts, ti, ht);
         topk_offer(buf, valid[1], sc[1], id[1], ts, ti, ht);
-        __syncthreads();
-        if (buf.cnt > CAND_CAP - 2 * DT_THREADS) topk_compact(buf, (int)k);
+        if (topk_full(buf, CAND_CAP - 2 * DT_THREADS)) topk_compact(buf, (int)k);
     }
     topk_compact(buf, (int)k);
     const int keep = min(buf.cnt, (int)k);

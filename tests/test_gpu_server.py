@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from bnutil import cluster, query
+from bnutil import cluster, int8_matrix, query
 from ivfutil import IvfCase
 
 pytestmark = pytest.mark.gpu
@@ -181,3 +181,45 @@ def test_flat_block_batches_match_per_query(corpora):
     st = srv.stats()
     assert st["block_batches"] > 0 and st["completed"] == len(reqs)
     srv.close()
+
+
+@pytest.fixture(scope="module")
+def big_flat(ctx):
+    """100k rows: every top-k CTA compacts its candidate buffer several times."""
+    c = capi()
+    rows = 100_000
+    M = int8_matrix(rows, 768, 9100)
+    L = O.generate_subspace(bytes([9]) * 32)
+    H, rp, ix, sg = c.host_regenerate_h_s(O.derive_h_seed(91, 0), rows)
+    f = c.Flat.build_from_plain(ctx, M.reshape(-1), rows, L, H, rp, ix, sg)
+    return f, L
+
+
+def test_concurrent_block_and_per_query_batches(big_flat):
+    """Block batches and per-query batches in flight together on several
+    slots (the timing under which warps of one CTA drift apart): every result
+    equals the per-query path."""
+    c = capi()
+    flat, L = big_flat
+    pool = [query(L, 9200 + i) for i in range(64)]
+    want = []
+    for v, qs, enc in pool:
+        hits, failed, _, _ = flat.query(enc.v_enc[None], enc.g[None], [(enc.t_idx, enc.t_sign)],
+                                        [O.domain_separate(qs, b"protocol2")], TRIALS, K)
+        want.append((hits[0][0], hits[0][1]))
+    srv = c.Server(flat, None, max_batch=64, slots=4, max_wait_us=0, trials=TRIALS, k=K, block_min=8)
+    rng = np.random.default_rng(93)
+    bad = 0
+    for burst in range(12):
+        picks = rng.integers(0, len(pool), size=40)
+        ts = []
+        for i in picks:
+            v, qs, enc = pool[i]
+            ts.append(srv.submit_flat(enc.v_enc, enc.g, enc.t_idx, enc.t_sign, O.domain_separate(qs, b"protocol2")))
+        for t, i in zip(ts, picks):
+            ids, sc, ft, fc, lat = srv.wait(t)
+            bad += not (np.array_equal(ids, want[i][0]) and np.array_equal(sc, want[i][1]) and ft == -1)
+    st = srv.stats()
+    srv.close()
+    assert bad == 0
+    assert st["block_batches"] > 0 and st["batches"] > st["block_batches"]  # both paths were exercised
