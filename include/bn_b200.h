@@ -161,6 +161,14 @@ int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v_enc, uint64_t* d_r, voi
  * a bounded device-side wait timed out and the outputs must be discarded).
  * Synchronous: call after the enqueued work has completed. */
 int bn_plan_status(bn_plan* p, uint32_t* device_flags);
+/* Kernel timing for measurement: after bn_plan_profile(p, n), the next n
+ * enqueues record CUDA events on their stream right before and after the
+ * plan's dominant kernel (the one pass over m_enc: fused scan + Protocol 2 on
+ * the tensor engine, the scan otherwise); bn_plan_profile_read waits for them
+ * and returns their durations in ms (oldest first) and restarts the count.
+ * No counterpart in the reference. */
+int bn_plan_profile(bn_plan* p, uint32_t max_launches);
+int bn_plan_profile_read(bn_plan* p, float* ms, uint32_t cap, uint32_t* n);
 int bn_plan_destroy(bn_plan* p);
 
 /* ---------------------------------------------------------------- block scoring

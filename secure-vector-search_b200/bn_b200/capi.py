@@ -77,6 +77,8 @@ _SIGS = {
     "bn_plan_enqueue_scan": (C.c_int, [vp, vp, vp, vp]),
     "bn_plan_status": (C.c_int, [vp, vp]),
     "bn_plan_destroy": (C.c_int, [vp]),
+    "bn_plan_profile": (C.c_int, [vp, u32]),
+    "bn_plan_profile_read": (C.c_int, [vp, vp, u32, vp]),
     "bn_flat_block_prepare": (C.c_int, [vp]),
     "bn_flat_block_plan": (C.c_int, [vp, u32, u32, u32, u32, vp]),
     "bn_plan_block_config": (C.c_int, [vp, vp, vp]),
@@ -339,6 +341,16 @@ class Plan:
         f = u32(0)
         check(lib.bn_plan_status(self.h, C.byref(f)))
         return f.value
+
+    def profile(self, max_launches: int):
+        """Time the dominant kernel of the next max_launches enqueues (CUDA events on the launch stream)."""
+        check(lib.bn_plan_profile(self.h, max_launches))
+
+    def profile_read(self, cap: int = 65536) -> np.ndarray:
+        ms = np.zeros(max(cap, 1), np.float32)
+        n = u32(0)
+        check(lib.bn_plan_profile_read(self.h, ptr(ms), cap, C.byref(n)))
+        return ms[: n.value].copy()
 
     def close(self):
         if self.h:

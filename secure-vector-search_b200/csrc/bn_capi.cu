@@ -322,8 +322,11 @@ int make_tc_maps(const Sizes& z, const uint8_t* d_u, TcMaps& maps) {
     return BN_OK;
 }
 
+// prof0 / prof1 (nullable): events recorded on s right before and after the
+// pipeline's dominant kernel, the single pass over m_enc (fused scan +
+// Protocol 2 on the tensor engine, else the scan).
 int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m, const Inputs& in, const Scratch& sc,
-                     const Outputs& out, cudaStream_t s) {
+                     const Outputs& out, cudaStream_t s, cudaEvent_t prof0, cudaEvent_t prof1) {
     CU(cudaMemsetAsync(sc.err, 0, 4, s));
     launch_query_limbs(in.v, z.B, sc.limbs, s);
     const ChaChaKey* keys = reinterpret_cast<const ChaChaKey*>(in.seeds);
@@ -336,8 +339,10 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
             if (ps == 0) {
                 launch_tc_ugen(m.vsegs, m.tc_blocks, m.nblocks, keys, nullptr, t0, tc, nr, sc.u_buf, sc.ur_part,
                                z.trials, sc.flags, s);
+                if (prof0) CU(cudaEventRecord(prof0, s));
                 launch_tc_fused(c.tmap_m, m.maps->u[ps], m.tc_panels, m.npanels, m.vsegs, sc.limbs, tc, nr, z.trials,
                                 sc.z_part, sc.r_part, z.total_out, sc.err, ctx->num_sms, s);
+                if (prof1) CU(cudaEventRecord(prof1, s));
                 launch_tc_rreduce(m.vsegs, m.tc_blocks, m.nblocks, sc.r_part, z.total_out, tc_groups(nr), sc.u_buf, tc,
                                   nr, z.trials, sc.r, sc.ur_part, s);
             } else {
@@ -350,8 +355,10 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
         launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, in.v, m.vsegs, m.nvseg, z.trials, sc.ur,
                          sc.zv, sc.zv_chunks, out.vfailed, s);
     } else {
+        if (prof0) CU(cudaEventRecord(prof0, s));
         launch_scan(c.m_enc.at<uint64_t>(), sc.limbs, m.segs, m.seg_blk, m.nseg, m.total_blocks, sc.r, ctx->num_sms,
                     sc.err, s);
+        if (prof1) CU(cudaEventRecord(prof1, s));
         if (z.trials) {
             CU(cudaMemsetAsync(sc.flags, 0, 4, s));
             launch_freivalds(c.m_enc.at<uint64_t>(), sc.r, m.vsegs, m.nvseg, keys, z.trials, z.fp, sc.z_part, sc.ur_part,
@@ -502,7 +509,7 @@ int job_launch(Engine& e, QueryJob& j, DevMem& ws, PinnedMem& host, cudaStream_t
         CU(cudaMemsetAsync(out.n, 0, (uint64_t)j.B * 4, s));
         CU(cudaMemsetAsync(sc.err, 0, 4, s));
     } else {
-        TRY(enqueue_pipeline(e.ctx, e.c, j.z, m, in, sc, out, s));
+        TRY(enqueue_pipeline(e.ctx, e.c, j.z, m, in, sc, out, s, nullptr, nullptr));
     }
     CU(cudaMemcpyAsync(h + o.out_begin, d + o.out_begin, o.out_end - o.out_begin, cudaMemcpyDeviceToHost, s));
     if (r_out && hm.total_out) CU(cudaMemcpyAsync(r_out, d + o.r, hm.total_out * 8, cudaMemcpyDeviceToHost, s));
@@ -691,8 +698,12 @@ struct bn_plan {
     HostMeta hm;
     TcMaps maps;
     BlockPlan* block = nullptr;  // set for block plans (bn_flat_block_plan)
+    // kernel timing (bn_plan_profile): event pairs around the dominant kernel
+    std::vector<cudaEvent_t> prof;
+    uint32_t prof_n = 0;
     ~bn_plan() {
         if (block) block_plan_free(block);
+        for (cudaEvent_t e : prof) cudaEventDestroy(e);
     }
 };
 
@@ -935,7 +946,13 @@ int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v, const uint64_t* d_g, const 
     Inputs in{d_v, d_g, d_t, d_t_nnz, d_seeds};
     const Scratch sc = scratch_at(d, p->o);
     Outputs out{d_ids, d_scores, d_n, d_failed, nullptr};
-    return enqueue_pipeline(p->h->e.ctx, p->h->e.c, p->z, m, in, sc, out, s);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!p->prof.empty() && p->prof_n < p->prof.size() / 2) {
+        e0 = p->prof[2 * p->prof_n];
+        e1 = p->prof[2 * p->prof_n + 1];
+        ++p->prof_n;
+    }
+    return enqueue_pipeline(p->h->e.ctx, p->h->e.c, p->z, m, in, sc, out, s, e0, e1);
 }
 
 int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v, uint64_t* d_r, void* stream) {
@@ -951,6 +968,29 @@ int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v, uint64_t* d_r, void* s
                 (uint32_t)p->hm.segs.size(), p->hm.seg_blk.back(), d_r, p->h->e.ctx->num_sms,
                 reinterpret_cast<uint32_t*>(d + o.err), s);
     CU(cudaGetLastError());
+    return BN_OK;
+}
+
+int bn_plan_profile(bn_plan* p, uint32_t max_launches) {
+    if (!p) return fail(BN_EINVAL, "null plan");
+    if (p->block) return fail(BN_EINVAL, "block plans report their GEMM times through bn_plan_block_config");
+    if (max_launches > 65536) return fail(BN_EINVAL, "max_launches = %u exceeds 65536", max_launches);
+    for (cudaEvent_t e : p->prof) cudaEventDestroy(e);
+    p->prof.assign(2ull * max_launches, nullptr);
+    p->prof_n = 0;
+    for (auto& e : p->prof) CU(cudaEventCreate(&e));
+    return BN_OK;
+}
+
+int bn_plan_profile_read(bn_plan* p, float* ms, uint32_t cap, uint32_t* n) {
+    if (!p || !n || (cap && !ms)) return fail(BN_EINVAL, "null argument");
+    const uint32_t got = std::min(p->prof_n, cap);
+    for (uint32_t i = 0; i < got; ++i) {
+        CU(cudaEventSynchronize(p->prof[2 * i + 1]));
+        CU(cudaEventElapsedTime(&ms[i], p->prof[2 * i], p->prof[2 * i + 1]));
+    }
+    *n = got;
+    p->prof_n = 0;
     return BN_OK;
 }
 
