@@ -308,12 +308,17 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
                                       std::max<uint64_t>(z.total_out, 1))
                    : 0;
     o.zv_chunks = L.take<uint64_t>(std::max<uint64_t>(z.nvseg * z.trials * 8, 1));
+    o.wimg = (tc && z.trials) ? L.take<uint8_t>((uint64_t)z.B * WIMG_BYTES_PER_QUERY) : 0;
     o.total = L.off + 1024;
     return o;
 }
 
-int make_tc_maps(const Sizes& z, const uint8_t* d_u, TcMaps& maps) {
+int make_tc_maps(const Sizes& z, const uint8_t* d_u, const uint8_t* d_w, TcMaps& maps) {
     if (z.engine != BN_ENGINE_TENSOR || !z.trials || !z.nblocks) return BN_OK;
+    {
+        cudaError_t e = make_tmap_u8(&maps.w, d_w, 128, (uint64_t)z.B * 64 * 16, 128, WIMG_BOX_ROWS);
+        if (e != cudaSuccess) return fail(BN_ECUDA, "tensor map for the query images: %s", cudaGetErrorString(e));
+    }
     for (uint32_t t0 = 0, ps = 0; t0 < z.trials; t0 += TC_MAX_TRIALS, ++ps) {
         const uint32_t nr = pass_rows(std::min<uint32_t>(TC_MAX_TRIALS, z.trials - t0));
         cudaError_t e = make_tmap_u8(&maps.u[ps], d_u, TC_ROWS, z.nblocks * (uint64_t)nr, TC_ROWS, nr);
@@ -339,9 +344,10 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
             if (ps == 0) {
                 launch_tc_ugen(m.vsegs, m.tc_blocks, m.nblocks, keys, nullptr, t0, tc, nr, sc.u_buf, sc.ur_part,
                                z.trials, sc.flags, s);
+                launch_query_wimg(in.v, z.B, sc.wimg, s);
                 if (prof0) CU(cudaEventRecord(prof0, s));
-                launch_tc_fused(c.tmap_m, m.maps->u[ps], m.tc_panels, m.npanels, m.vsegs, sc.limbs, tc, nr, z.trials,
-                                sc.z_part, sc.r_part, z.total_out, sc.err, ctx->num_sms, s);
+                launch_tc_fused(c.tmap_m, m.maps->u[ps], m.maps->w, m.tc_panels, m.npanels, m.vsegs, tc, nr,
+                                z.trials, sc.z_part, sc.r_part, z.total_out, sc.err, ctx->num_sms, s);
                 if (prof1) CU(cudaEventRecord(prof1, s));
                 launch_tc_rreduce(m.vsegs, m.tc_blocks, m.nblocks, sc.r_part, z.total_out, tc_groups(nr), sc.u_buf, tc,
                                   nr, z.trials, sc.r, sc.ur_part, s);
@@ -398,7 +404,8 @@ Scratch scratch_at(char* d, const RunLayout& o) {
                    TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
                                reinterpret_cast<uint32_t*>(d + o.cand_n)},
                    reinterpret_cast<uint32_t*>(d + o.err), reinterpret_cast<uint8_t*>(d + o.u_buf),
-                   reinterpret_cast<uint64_t*>(d + o.r_part), reinterpret_cast<uint64_t*>(d + o.zv_chunks)};
+                   reinterpret_cast<uint64_t*>(d + o.r_part), reinterpret_cast<uint64_t*>(d + o.zv_chunks),
+                   reinterpret_cast<uint8_t*>(d + o.wimg)};
 }
 void pack_meta(char* h, const RunLayout& o, const HostMeta& hm) {
     memcpy(h + o.segs, hm.segs.data(), hm.segs.size() * sizeof(ScanSeg));
@@ -469,7 +476,7 @@ int job_prepare(Engine& e, QueryJob& j, DevMem& ws, PinnedMem& host, const uint6
     TRY(ws.reserve(e.ctx, o.total));
     TRY(host.reserve(o.out_end));
     char* d = ws.at<char>();
-    TRY(make_tc_maps(j.z, reinterpret_cast<uint8_t*>(d + o.u_buf), j.maps));
+    TRY(make_tc_maps(j.z, reinterpret_cast<uint8_t*>(d + o.u_buf), reinterpret_cast<uint8_t*>(d + o.wimg), j.maps));
 
     char* h = host.at<char>();
     memcpy(h + o.v, v_enc, (uint64_t)B * N * 8);
@@ -584,7 +591,7 @@ int run_verify(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* r, const
     char* h = e.host.at<char>();
     char* d = e.ws.at<char>();
     TcMaps maps;
-    TRY(make_tc_maps(z, reinterpret_cast<uint8_t*>(d + o.u_buf), maps));
+    TRY(make_tc_maps(z, reinterpret_cast<uint8_t*>(d + o.u_buf), reinterpret_cast<uint8_t*>(d + o.wimg), maps));
     memcpy(h + o.v, v_enc, N * 8);
     memcpy(h + o.seeds, seed, 32);
     pack_meta(h, o, hm);
@@ -918,7 +925,9 @@ int bn_flat_plan(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, bn_plan** 
     p->z = sizes_for(f->e, p->hm, B, trials, k);
     p->o = make_layout(p->z, false);
     int rc = p->ws.alloc(f->e.ctx, p->o.total);
-    if (rc == BN_OK) rc = make_tc_maps(p->z, reinterpret_cast<uint8_t*>(p->ws.at<char>() + p->o.u_buf), p->maps);
+    if (rc == BN_OK)
+        rc = make_tc_maps(p->z, reinterpret_cast<uint8_t*>(p->ws.at<char>() + p->o.u_buf),
+                          reinterpret_cast<uint8_t*>(p->ws.at<char>() + p->o.wimg), p->maps);
     if (rc == BN_OK) {
         std::vector<char> h(p->o.in_end, 0);
         pack_meta(h.data(), p->o, p->hm);

@@ -166,6 +166,7 @@ constexpr uint32_t MAX_TRIALS = 64;  // Protocol 2 trials per call
 
 struct TcMaps {  // host-side tensor maps of the U buffer, one per pass of <= 20 trials
     CUtensorMap u[(MAX_TRIALS + TC_MAX_TRIALS - 1) / TC_MAX_TRIALS];
+    CUtensorMap w;  // the queries' diagonal byte images (fused scan)
 };
 inline uint32_t pass_rows(uint32_t t_cnt) { return 8 * ((t_cnt + 1) & ~1u); }
 
@@ -199,6 +200,7 @@ struct Scratch {  // device pointers
     uint8_t* u_buf;
     uint64_t* r_part;  // fused pass: per strip-group partial dots
     uint64_t* zv_chunks;
+    uint8_t* wimg;     // fused pass: diagonal byte images of the queries
 };
 struct Inputs {
     const uint64_t* v;
@@ -242,7 +244,7 @@ struct RunLayout {
     // outputs (contiguous -> one D2H)
     uint64_t ids, scores, n, vfailed, ur, zv, err, out_begin, out_end;
     // internal
-    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, r_part, zv_chunks, total;
+    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, r_part, zv_chunks, wimg, total;
 };
 
 // One run of the query pipeline over host inputs (bn_capi.cu): hm is the

@@ -14,6 +14,8 @@
 // down (waits for its own copies and MMAs, frees TMEM) instead of hanging.
 #include <cudaTypedefs.h>
 
+#include <algorithm>
+
 #include "bn_tc.cuh"
 #include "bn_tcgen05.cuh"
 
@@ -98,8 +100,74 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
 }
 
 // ------------------------------------------------------------------ GEMM + drain
-constexpr int TC_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int TC_THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 constexpr uint32_t STRIP_BYTES = TC_ROWS * 128;  // one 128x128 M box
+constexpr int TC_EPI_WARPS = 8;                // TMEM drain warps: 2 per lane quarter
+
+// Drains one work item's accumulators into z partials.  TMEM holds, per strip
+// s < sg (columns s * n_rows ...), lanes = the strip's 128 byte columns (j, a)
+// (element j = lane / 8, byte a = lane % 8) and columns (t, b) (trial t, byte
+// b of u_t).  Warp (lane quarter q, half) reads every other 64-column chunk:
+// each lane folds its 8 trials' byte products to (lo + hi 2^32) 2^(8a) mod p,
+// then a butterfly over the 8 lanes of one element leaves lane a with trial
+// c0/8 + a's sum; 16-column remainders use a plain 3-level reduction.
+// z_out[t * N + j] receives z_t[j] for t < t_cnt.
+__device__ __forceinline__ void z_drain(uint32_t tmem, uint32_t q, uint32_t half, uint32_t lane, uint32_t sg,
+                                        uint32_t strip0, uint32_t n_rows, uint32_t t_cnt, uint64_t* __restrict__ z_out) {
+    const uint32_t a = lane & 7, xi = lane >> 3;
+    const uint32_t jl = q * 4 + xi;
+    const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+    const uint32_t wide = n_rows & ~63u;
+    const bool b2 = (a & 4) != 0, b1 = (a & 2) != 0, b0 = (a & 1) != 0;
+    for (uint32_t s = 0; s < sg; ++s) {
+        const uint32_t j = (strip0 + s) * 16 + jl;
+        const uint32_t tbase = tmem + ((q * 32) << 16) + s * n_rows;
+        for (uint32_t c0 = 64 * half; c0 < wide; c0 += 128) {
+            uint32_t v[64];
+            tmem_ld64(tbase + c0, v);
+            uint64_t part[8];
+#pragma unroll
+            for (int tt = 0; tt < 8; ++tt) {
+                uint64_t lo = 0, hi = 0;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    lo += (uint64_t)v[8 * tt + b] << (8 * b);
+                    hi += (uint64_t)v[8 * tt + 4 + b] << (8 * b);
+                }
+                part[tt] = canon(rotl61(lo, w1) + rotl61(hi, w2));
+            }
+            uint64_t k4[4], k2[2];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                k4[i] = (b2 ? part[i + 4] : part[i]) + __shfl_xor_sync(FULLMASK, b2 ? part[i] : part[i + 4], 4);
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+                k2[i] = (b1 ? k4[i + 2] : k4[i]) + __shfl_xor_sync(FULLMASK, b1 ? k4[i] : k4[i + 2], 2);
+            const uint64_t z = canon((b0 ? k2[1] : k2[0]) + __shfl_xor_sync(FULLMASK, b0 ? k2[0] : k2[1], 1));
+            const uint32_t t = c0 / 8 + a;
+            if (t < t_cnt) z_out[(uint64_t)t * N + j] = z;
+        }
+        for (uint32_t c0 = wide + 16 * half; c0 < n_rows; c0 += 32) {
+            uint32_t v[16];
+            tmem_ld16(tbase + c0, v);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t t = c0 / 8 + h;
+                uint64_t lo = 0, hi = 0;
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    lo += (uint64_t)v[8 * h + b] << (8 * b);
+                    hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
+                }
+                uint64_t zc = canon(rotl61(lo, w1) + rotl61(hi, w2));
+                zc += __shfl_xor_sync(FULLMASK, zc, 1);
+                zc += __shfl_xor_sync(FULLMASK, zc, 2);
+                zc += __shfl_xor_sync(FULLMASK, zc, 4);
+                if (a == 0 && t < t_cnt) z_out[(uint64_t)t * N + j] = canon(zc);
+            }
+        }
+    }
+}
 
 template <int S>
 __global__ void __launch_bounds__(TC_THREADS, 1)
@@ -124,7 +192,7 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
             bar_init(&empty_b[s], 1);
         }
         bar_init(&accf_b, 1);
-        bar_init(&acce_b, 4);
+        bar_init(&acce_b, TC_EPI_WARPS);
         bar_init(&done_b, 1);
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -224,47 +292,21 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
         }
     } else {
         // ---------------------------------------------------------- epilogue
-        const uint32_t q = (uint32_t)(warp & 3);          // TMEM lane quarter of this warp
-        const uint32_t lane_c = q * 32 + lane;            // byte column within the strip
-        const uint32_t jl = lane_c >> 3, a = lane_c & 7;
-        const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+        const uint32_t q = (uint32_t)(warp & 3);            // TMEM lane quarter of this warp
+        const uint32_t half = (uint32_t)(warp - 2) >> 2;    // which chunks of the item it drains
         uint64_t gc = 0;
         bool stop = false;
         for (uint32_t item = blockIdx.x; item < npanels * groups && !stop; item += gridDim.x, ++gc) {
             const uint32_t p = item / groups, g = item % groups;
-            {
-                const uint32_t sg = min((uint32_t)S, 64u - g * S);
-                const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b, (uint32_t)(gc & 1)));  // warp-uniform
-                if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
-                if (__any_sync(FULLMASK, !ok || abort_s)) { stop = true; break; }
-                tc_after();
-                for (uint32_t s = 0; s < sg; ++s) {
-                    const uint32_t j = (g * S + s) * 16 + jl;
-                    for (uint32_t c0 = 0; c0 < n_rows; c0 += 16) {
-                        uint32_t v[16];
-                        tmem_ld16(tmem + ((q * 32) << 16) + s * n_rows + c0, v);
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const uint32_t t = c0 / 8 + h;
-                            uint64_t lo = 0, hi = 0;
-#pragma unroll
-                            for (int b = 0; b < 4; ++b) {
-                                lo += (uint64_t)v[8 * h + b] << (8 * b);
-                                hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
-                            }
-                            uint64_t zc = canon(rotl61(lo, w1) + rotl61(hi, w2));  // (lo + hi 2^32) 2^(8a) mod p
-                            zc += __shfl_xor_sync(FULLMASK, zc, 1);
-                            zc += __shfl_xor_sync(FULLMASK, zc, 2);
-                            zc += __shfl_xor_sync(FULLMASK, zc, 4);
-                            if (a == 0 && t < t_cnt)
-                                z_part[((uint64_t)p * trials_total + t_base + t) * N + j] = canon(zc);
-                        }
-                    }
-                }
-                tc_before();
-                __syncwarp();
-                if (lane == 0) bar_arrive(&acce_b);
-            }
+            const uint32_t sg = min((uint32_t)S, 64u - g * S);
+            const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b, (uint32_t)(gc & 1)));  // warp-uniform
+            if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
+            if (__any_sync(FULLMASK, !ok || abort_s)) { stop = true; break; }
+            tc_after();
+            z_drain(tmem, q, half, lane, sg, g * S, n_rows, t_cnt, z_part + ((uint64_t)p * trials_total + t_base) * N);
+            tc_before();
+            __syncwarp();
+            if (lane == 0) bar_arrive(&acce_b);
         }
     }
     tc_before();
@@ -276,46 +318,59 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
 }
 
 // ------------------------------------------------------------------ fused scan + Protocol 2
-// Same pipeline as tc_freivalds_kernel, plus six scan warps that read each
-// shared-memory stage too: for the stage's 128 rows and the group's S strips
-// (16 u64 columns per strip) they form the partial dot products with the
-// query on the CUDA cores, so r = M_enc v comes out of the same single read
-// of M_enc as z = U^T M_enc.  A stage is recycled only after the MMA commit
-// and all six scan warps have released it.  r partials land per strip group
-// in r_part[group][r index]; tc_rreduce_kernel sums them.
-constexpr int FU_SCAN_WARPS = 4;
-constexpr int FU_THREADS = TC_THREADS + 32 * FU_SCAN_WARPS;  // 320
+// One pass over m_enc yields both products, all on the tensor cores.  Each
+// stage's S strips (128 rows x 128 bytes of m_enc each) feed two MMAs:
+//   z: D[c][(t,b)] += Mb^T Ub as in tc_freivalds_kernel (strip read
+//      MN-major), accumulated over the 4096-row panel and drained by the
+//      eight epilogue warps at the end of each work item;
+//   r: E[i][s] = sum_{j,a} Mb[i][8j+a] W[s][8j+a], the same strip read
+//      K-major against the query's diagonal byte image W[s][8j+a] = byte
+//      (s - a) of v_j (16 rows per strip: s = a + b < 15), so that
+//      sum_s 2^(8s) E[i][s] = sum_j M[i][j] v_j over the group's elements.
+//      E is per stage (new rows every stage): two 16-column TMEM buffers at
+//      column 480 alternate, and four drain warps turn each into r partials
+//      r_part[group][r index] while the next stage accumulates.
+// TMEM: z in columns [0, 3 n_rows) (n_rows <= 160), E in [480, 512).
+constexpr int FU_S = 3;
+constexpr int FU_DRAIN_WARPS = 4;
+constexpr int FU_THREADS = TC_THREADS + 32 * FU_DRAIN_WARPS;  // 448
+constexpr uint32_t FU_E_COL = 480;
+constexpr uint32_t W_STRIP_BYTES = 16 * 128;  // one strip's 16 diagonal rows
 
-template <int S>
 __global__ void __launch_bounds__(FU_THREADS, 1)
 tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constant__ CUtensorMap tmap_u,
-                const TcPanel* __restrict__ panels, uint32_t npanels, const VerifySeg* __restrict__ vsegs,
-                const QLimb* __restrict__ qlimbs, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
+                const __grid_constant__ CUtensorMap tmap_w, const TcPanel* __restrict__ panels, uint32_t npanels,
+                const VerifySeg* __restrict__ vsegs, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
                 uint32_t stages, uint32_t stage_bytes, uint64_t* __restrict__ z_part, uint64_t* __restrict__ r_part,
                 uint64_t r_stride, uint32_t* __restrict__ err) {
+    constexpr int S = FU_S;
     extern __shared__ uint8_t tc_dyn[];
-    __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b;
-    __shared__ QLimb qsm[64];  // the current strip group's query limbs (scan warps)
+    __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b, racc_b[2], rfree_b[2];
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
-    __shared__ volatile int scan_stop;
 
     const uint32_t base = (su32(tc_dyn) + 1023u) & ~1023u;
     uint8_t* ring = tc_dyn + (base - su32(tc_dyn));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t u_off = S * STRIP_BYTES;
     const uint32_t u_bytes = n_rows * TC_ROWS;
+    const uint32_t w_off = u_off + u_bytes;  // 1024-aligned: n_rows is a multiple of 16
+    const uint32_t w_bytes = S * W_STRIP_BYTES;
     const uint32_t groups = (64 + S - 1) / S;
     const uint32_t items = npanels * groups;
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < stages; ++s) {
             bar_init(&full_b[s], 1);
-            bar_init(&empty_b[s], 1 + FU_SCAN_WARPS);
+            bar_init(&empty_b[s], 1);
         }
         bar_init(&accf_b, 1);
-        bar_init(&acce_b, 4);
+        bar_init(&acce_b, TC_EPI_WARPS);
         bar_init(&done_b, 1);
+        for (int e = 0; e < 2; ++e) {
+            bar_init(&racc_b[e], 1);
+            bar_init(&rfree_b[e], FU_DRAIN_WARPS);
+        }
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -337,6 +392,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
             for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
                 const uint32_t p = item / groups, g = item % groups;
                 const TcPanel pn = panels[p];
+                const uint32_t query = vsegs[pn.seg].query;
                 const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
                 const uint32_t sg = min((uint32_t)S, 64u - g * S);
                 for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
@@ -349,11 +405,12 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                     }
                     if (abort_s) { stop = true; break; }
                     uint8_t* sb = ring + (uint64_t)st * stage_bytes;
-                    bar_expect_tx(&full_b[st], sg * STRIP_BYTES + u_bytes);
+                    bar_expect_tx(&full_b[st], sg * STRIP_BYTES + u_bytes + w_bytes);
                     for (uint32_t s = 0; s < sg; ++s)
                         tma_2d(sb + s * STRIP_BYTES, &tmap_m, (int)((g * S + s) * 128), (int)(pn.row0 + rb * TC_ROWS),
                                &full_b[st]);
                     tma_2d(sb + u_off, &tmap_u, 0, (int)((pn.rb0 + rb) * n_rows), &full_b[st]);
+                    tma_2d(sb + w_off, &tmap_w, 0, (int)((query * 64 + g * S) * 16), &full_b[st]);
                 }
             }
             for (uint64_t j = it > stages ? it - stages : 0; j < it; ++j)
@@ -361,7 +418,8 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
         }
     } else if (warp == 1) {
         if (lane == 0) {  // ------------------------------------------ MMA issuer
-            const uint32_t idesc = (2u << 4) | (1u << 15) | ((n_rows >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+            const uint32_t idesc_z = (2u << 4) | (1u << 15) | ((n_rows >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+            const uint32_t idesc_r = (2u << 4) | ((16u >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
             uint64_t it = 0, gc = 0;
             bool stop = false;
             for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x, ++gc) {
@@ -376,8 +434,9 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 }
                 tc_after();
                 for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
-                    const uint32_t st = (uint32_t)(it % stages);
-                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
+                    const uint32_t st = (uint32_t)(it % stages), eb = (uint32_t)(it & 1);
+                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s ||
+                        (it >= 2 && !bar_wait(&rfree_b[eb], (uint32_t)(((it >> 1) - 1) & 1)))) {
                         abort_s = 1;
                         atomicOr(err, 8u);
                         stop = true;
@@ -388,11 +447,15 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                     for (uint32_t s = 0; s < sg; ++s)
 #pragma unroll
                         for (uint32_t ks = 0; ks < TC_ROWS / 32; ++ks) {
-                            const uint64_t a = sdesc(sb + s * STRIP_BYTES + ks * 4096u, STRIP_BYTES, 1024);
-                            const uint64_t b = sdesc(sb + u_off + ks * 32u, 16, 1024);
-                            mma_i8(tmem + s * n_rows, a, b, idesc, (rb | ks) != 0);
+                            // z: strip read MN-major (M = its byte columns, K = the stage's rows)
+                            mma_i8(tmem + s * n_rows, sdesc(sb + s * STRIP_BYTES + ks * 4096u, STRIP_BYTES, 1024),
+                                   sdesc(sb + u_off + ks * 32u, 16, 1024), idesc_z, (rb | ks) != 0);
+                            // r: strip read K-major (M = the stage's rows, K = its byte columns)
+                            mma_i8(tmem + FU_E_COL + 16 * eb, sdesc(sb + s * STRIP_BYTES + ks * 32u, 16, 1024),
+                                   sdesc(sb + w_off + s * W_STRIP_BYTES + ks * 32u, 16, 1024), idesc_r, (s | ks) != 0);
                         }
-                    mma_commit(&empty_b[st]);
+                    mma_commit(&empty_b[st]);  // stage reusable once these MMAs have read it
+                    mma_commit(&racc_b[eb]);   // the stage's row products are ready for the drain warps
                 }
                 if (stop) break;
                 mma_commit(&accf_b);
@@ -400,12 +463,10 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
             mma_commit(&done_b);
             bar_wait(&done_b, 0);
         }
-    } else if (warp < 6) {
+    } else if (warp < 2 + TC_EPI_WARPS) {
         // ---------------------------------------------------------- TMEM epilogue (z)
         const uint32_t q = (uint32_t)(warp & 3);
-        const uint32_t lane_c = q * 32 + lane;
-        const uint32_t jl = lane_c >> 3, a = lane_c & 7;
-        const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+        const uint32_t half = (uint32_t)(warp - 2) >> 2;
         uint64_t gc = 0;
         for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, ++gc) {
             const uint32_t p = item / groups, g = item % groups;
@@ -414,87 +475,45 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
             if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
             if (__any_sync(FULLMASK, !ok || abort_s)) break;
             tc_after();
-            for (uint32_t s = 0; s < sg; ++s) {
-                const uint32_t j = (g * S + s) * 16 + jl;
-                for (uint32_t c0 = 0; c0 < n_rows; c0 += 16) {
-                    uint32_t v[16];
-                    tmem_ld16(tmem + ((q * 32) << 16) + s * n_rows + c0, v);
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const uint32_t t = c0 / 8 + h;
-                        uint64_t lo = 0, hi = 0;
-#pragma unroll
-                        for (int b = 0; b < 4; ++b) {
-                            lo += (uint64_t)v[8 * h + b] << (8 * b);
-                            hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
-                        }
-                        uint64_t zc = canon(rotl61(lo, w1) + rotl61(hi, w2));
-                        zc += __shfl_xor_sync(FULLMASK, zc, 1);
-                        zc += __shfl_xor_sync(FULLMASK, zc, 2);
-                        zc += __shfl_xor_sync(FULLMASK, zc, 4);
-                        if (a == 0 && t < t_cnt) z_part[((uint64_t)p * trials_total + t) * N + j] = canon(zc);
-                    }
-                }
-            }
+            z_drain(tmem, q, half, lane, sg, g * S, n_rows, t_cnt, z_part + (uint64_t)p * trials_total * N);
             tc_before();
             __syncwarp();
             if (lane == 0) bar_arrive(&acce_b);
         }
     } else {
-        // ---------------------------------------------------------- scan warps (r)
-        // Four warps, one lane per stage row: lane reads its row's S strips
-        // (16 u64 each, 128-byte swizzled) and dots them with the group's
-        // query limbs, broadcast from shared memory.  No barrier per stage:
-        // each lane writes its row's partial for this strip group directly.
-        const uint32_t sw = (uint32_t)(warp - 6);
+        // ---------------------------------------------------------- r drain warps
+        // Lane (quarter q) = stage row q*32 + lane: E[row][s] for s < 16 ->
+        // sum_s 2^(8s) E[s] mod p, grouped by 4 (weights 2^0, 2^32, 2^64 =
+        // 2^3, 2^96 = 2^35 mod p).  E < 48 * 8 * 255^2 < 2^25 per column.
+        const uint32_t q = (uint32_t)(warp & 3);
+        const uint32_t rr = q * 32 + lane;
         uint64_t it = 0;
-        for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+        bool stop = false;
+        for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
             const uint32_t p = item / groups, g = item % groups;
             const TcPanel pn = panels[p];
             const VerifySeg vs = vsegs[pn.seg];
             const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
-            const uint32_t sg = min((uint32_t)S, 64u - g * S);
             const uint64_t r0 = vs.r0 + (pn.row0 - vs.row0);  // r index of the panel's first row
-            // this group's limbs: elements (g*S + s)*16 + e, s < sg.  Barrier A
-            // also publishes the stop snapshot taken before it, so every scan
-            // warp takes the same exit decision (the next snapshot is written
-            // only after barrier B, which all warps pass after reading it).
-            if (sw == 0 && lane == 0) scan_stop = abort_s;
-            asm volatile("bar.sync 1, %0;" ::"r"(32 * FU_SCAN_WARPS) : "memory");  // A
-            if (scan_stop) break;
-            for (uint32_t e = threadIdx.x - 32 * 6; e < sg * 16; e += 32 * FU_SCAN_WARPS)
-                qsm[e] = qlimbs[(uint64_t)vs.query * N + g * S * 16 + e];
-            asm volatile("bar.sync 1, %0;" ::"r"(32 * FU_SCAN_WARPS) : "memory");  // B
             for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
-                const uint32_t st = (uint32_t)(it % stages);
-                const bool ok = __all_sync(FULLMASK, bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)));
+                const uint32_t eb = (uint32_t)(it & 1);
+                const bool ok = __all_sync(FULLMASK, bar_wait(&racc_b[eb], (uint32_t)((it >> 1) & 1)));
                 if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 32u); }
-                const uint32_t rr = sw * 32 + lane;  // stage row
-                uint64_t a0 = 0, a1 = 0, a2 = 0, e0 = 0, e1 = 0, e2 = 0;
-                if (ok) {
-                    const uint8_t* sb = ring + (uint64_t)st * stage_bytes;
-                    for (uint32_t s = 0; s < sg; ++s) {
-                        const uint8_t* row = sb + s * STRIP_BYTES + rr * 128;
-                        const QLimb* ql = qsm + s * 16;
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) {  // 16-byte chunk c holds elements 2c, 2c+1
-                            const uint4 x = *reinterpret_cast<const uint4*>(row + ((c ^ (rr & 7)) << 4));
-                            const QLimb l0 = ql[2 * c], l1 = ql[2 * c + 1];
-                            a0 = mac(mac(a0, x.x, l0.b0), x.y, l0.c0);
-                            a1 = mac(mac(a1, x.x, l0.b1), x.y, l0.c1);
-                            a2 = mac(mac(a2, x.x, l0.b2), x.y, l0.c2);
-                            e0 = mac(mac(e0, x.z, l1.b0), x.w, l1.c0);
-                            e1 = mac(mac(e1, x.z, l1.b1), x.w, l1.c1);
-                            e2 = mac(mac(e2, x.z, l1.b2), x.w, l1.c2);
-                        }
-                    }
-                }
+                if (__any_sync(FULLMASK, !ok || abort_s)) { stop = true; break; }
+                tc_after();
+                uint32_t v[16];
+                tmem_ld16(tmem + ((q * 32) << 16) + FU_E_COL + 16 * eb, v);
+                tc_before();
                 __syncwarp();
-                if (lane == 0) bar_arrive(&empty_b[st]);  // this warp is done with the stage
-                if (!ok) break;  // abort_s is set; the next barrier A turns it into a uniform exit
+                if (lane == 0) bar_arrive(&rfree_b[eb]);  // the buffer may take stage it + 2
+                uint64_t gsum[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    gsum[k] = (uint64_t)v[4 * k] + ((uint64_t)v[4 * k + 1] << 8) + ((uint64_t)v[4 * k + 2] << 16) +
+                              ((uint64_t)v[4 * k + 3] << 24);
+                const uint64_t rv = canon(gsum[0] + rotl61(gsum[1], 32) + rotl61(gsum[2], 3) + rotl61(gsum[3], 35));
                 const uint32_t lr = rb * TC_ROWS + rr;
-                // at most 64 elements per row and group: every accumulator < 2^59
-                if (lr < pn.rows) r_part[(uint64_t)g * r_stride + r0 + lr] = combine3(a0 + e0, a1 + e1, a2 + e2);
+                if (lr < pn.rows) r_part[(uint64_t)g * r_stride + r0 + lr] = rv;
             }
         }
     }
@@ -503,6 +522,25 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
     if (warp == 1) {
         tc_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+    }
+}
+
+// Diagonal byte image of each query for the fused scan MMA:
+// w[((q * 64 + strip) * 16 + s) * 128 + 8 j + a] = byte (s - a) of
+// v[q][strip * 16 + j] when 0 <= s - a <= 7, else 0.
+__global__ void query_wimg_kernel(const uint64_t* __restrict__ v, uint32_t nq, uint8_t* __restrict__ w) {
+    const uint64_t total = (uint64_t)nq * 64 * 16 * 16;  // (query, strip, s, j)
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = (uint32_t)(e & 15), s = (uint32_t)((e >> 4) & 15);
+        const uint64_t qs = e >> 8;  // q * 64 + strip
+        const uint64_t x = v[(qs >> 6) * N + (qs & 63) * 16 + j];
+        uint64_t word = 0;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int b = (int)s - a;
+            if (b >= 0 && b <= 7) word |= ((x >> (8 * b)) & 0xffull) << (8 * a);
+        }
+        *reinterpret_cast<uint64_t*>(w + (qs * 16 + s) * 128 + 8 * j) = word;
     }
 }
 
@@ -646,29 +684,29 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
     }
 }
 
-void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels, uint32_t npanels,
-                     const VerifySeg* d_vsegs, const QLimb* d_limbs, uint32_t t_cnt, uint32_t n_rows,
-                     uint32_t trials_total, uint64_t* d_z_part, uint64_t* d_r_part, uint64_t r_stride,
+void launch_query_wimg(const uint64_t* d_v, uint32_t nq, uint8_t* d_w, cudaStream_t s) {
+    if (!nq) return;
+    const uint64_t total = (uint64_t)nq * 64 * 16 * 16;
+    const unsigned grid = (unsigned)std::min<uint64_t>((total + 255) / 256, 148 * 16);
+    query_wimg_kernel<<<grid, 256, 0, s>>>(d_v, nq, d_w);
+}
+
+void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const CUtensorMap& tmap_w,
+                     const TcPanel* d_panels, uint32_t npanels, const VerifySeg* d_vsegs, uint32_t t_cnt,
+                     uint32_t n_rows, uint32_t trials_total, uint64_t* d_z_part, uint64_t* d_r_part, uint64_t r_stride,
                      uint32_t* d_err, int num_sms, cudaStream_t s) {
     if (!npanels) return;
-    const int S = n_rows <= 128 ? 4 : 3;
-    const uint32_t stage_bytes = (uint32_t)S * STRIP_BYTES + ((n_rows * TC_ROWS + 1023u) & ~1023u);
-    uint32_t stages = (216u * 1024u) / stage_bytes;
+    const uint32_t stage_bytes = (uint32_t)FU_S * STRIP_BYTES + ((n_rows * TC_ROWS + 1023u) & ~1023u) +
+                                 (uint32_t)FU_S * W_STRIP_BYTES;
+    uint32_t stages = (227u * 1024u - 2048u) / stage_bytes;
     stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
     const int smem = (int)(stages * stage_bytes + 1024);
-    const uint32_t items = npanels * ((64 + S - 1) / S);
+    const uint32_t items = npanels * ((64 + FU_S - 1) / FU_S);
     const unsigned grid = items < (uint32_t)num_sms ? items : (unsigned)num_sms;
-    if (S == 4) {
-        cudaFuncSetAttribute(tc_fused_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        tc_fused_kernel<4><<<grid, FU_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, d_vsegs, d_limbs, t_cnt,
-                                                          n_rows, trials_total, stages, stage_bytes, d_z_part, d_r_part,
-                                                          r_stride, d_err);
-    } else {
-        cudaFuncSetAttribute(tc_fused_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        tc_fused_kernel<3><<<grid, FU_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, d_vsegs, d_limbs, t_cnt,
-                                                          n_rows, trials_total, stages, stage_bytes, d_z_part, d_r_part,
-                                                          r_stride, d_err);
-    }
+    cudaFuncSetAttribute(tc_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    tc_fused_kernel<<<grid, FU_THREADS, smem, s>>>(tmap_m, tmap_u, tmap_w, d_panels, npanels, d_vsegs, t_cnt, n_rows,
+                                                   trials_total, stages, stage_bytes, d_z_part, d_r_part, r_stride,
+                                                   d_err);
 }
 
 void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const uint64_t* d_r_part,

@@ -66,15 +66,21 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
                          uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
                          uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s, int u_flat = 0);
 
-// Fused single pass over m_enc for the first <= 20 trials: z_part as above
-// plus r_part[group][r index] (S-strip group partial dots with the query,
-// r_stride = total r entries, groups = ceil(64 / S) with S = 4 when
-// n_rows <= 128 else 3), to be summed by launch_tc_rreduce.
-void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels, uint32_t npanels,
-                     const VerifySeg* d_vsegs, const QLimb* d_limbs, uint32_t t_cnt, uint32_t n_rows,
-                     uint32_t trials_total, uint64_t* d_z_part, uint64_t* d_r_part, uint64_t r_stride,
+// Fused single pass over m_enc for the first <= 20 trials, both products on
+// the tensor cores: z_part as above plus r_part[group][r index] (3-strip
+// group partial dots with the query, r_stride = total r entries, 22 groups),
+// summed by launch_tc_rreduce.  tmap_w: the queries' diagonal byte images
+// (launch_query_wimg) {128, nq * 1024}, box {128, 48}, swizzle 128B.
+void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const CUtensorMap& tmap_w,
+                     const TcPanel* d_panels, uint32_t npanels, const VerifySeg* d_vsegs, uint32_t t_cnt,
+                     uint32_t n_rows, uint32_t trials_total, uint64_t* d_z_part, uint64_t* d_r_part, uint64_t r_stride,
                      uint32_t* d_err, int num_sms, cudaStream_t s);
-inline uint32_t tc_groups(uint32_t n_rows) { return n_rows <= 128 ? 16u : 22u; }
+inline uint32_t tc_groups(uint32_t) { return 22u; }  // strip groups of the fused pass (3 strips each)
+constexpr uint32_t WIMG_BYTES_PER_QUERY = 64u * 16u * 128u;
+constexpr uint32_t WIMG_BOX_ROWS = 48;  // one strip group's diagonal rows
+// w[((q * 64 + strip) * 16 + s) * 128 + 8 j + a] = byte (s - a) of
+// v[q][strip * 16 + j] (0 <= s - a <= 7), else 0.
+void launch_query_wimg(const uint64_t* d_v, uint32_t nq, uint8_t* d_w, cudaStream_t s);
 // r = sum of the group partials, and u_t . r partials for the pass's trials
 // from the U byte image.
 void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const uint64_t* d_r_part,
