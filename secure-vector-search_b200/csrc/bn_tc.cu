@@ -330,10 +330,13 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
 //      E is per stage (new rows every stage): two 16-column TMEM buffers at
 //      column 480 alternate, and four drain warps turn each into r partials
 //      r_part[group][r index] while the next stage accumulates.
-// TMEM: z in columns [0, 3 n_rows) (n_rows <= 160), E in [480, 512).
+// The z and r MMAs are issued by two warps (1 and FU_R_WARP), so neither
+// instruction stream waits for the other; a stage is free once both have
+// committed.  TMEM: z in columns [0, 3 n_rows) (n_rows <= 160), E in [480, 512).
 constexpr int FU_S = 3;
 constexpr int FU_DRAIN_WARPS = 4;
-constexpr int FU_THREADS = TC_THREADS + 32 * FU_DRAIN_WARPS;  // 448
+constexpr int FU_R_WARP = 2 + TC_EPI_WARPS + FU_DRAIN_WARPS;           // issues the r MMAs
+constexpr int FU_THREADS = TC_THREADS + 32 * (FU_DRAIN_WARPS + 1);  // 480
 constexpr uint32_t FU_E_COL = 480;
 constexpr uint32_t W_STRIP_BYTES = 16 * 128;  // one strip's 16 diagonal rows
 
@@ -362,11 +365,11 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < stages; ++s) {
             bar_init(&full_b[s], 1);
-            bar_init(&empty_b[s], 1);
+            bar_init(&empty_b[s], 2);  // z issuer + r issuer
         }
         bar_init(&accf_b, 1);
         bar_init(&acce_b, TC_EPI_WARPS);
-        bar_init(&done_b, 1);
+        bar_init(&done_b, 2);
         for (int e = 0; e < 2; ++e) {
             bar_init(&racc_b[e], 1);
             bar_init(&rfree_b[e], FU_DRAIN_WARPS);
@@ -417,9 +420,8 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 bar_wait(&full_b[j % stages], (uint32_t)((j / stages) & 1));
         }
     } else if (warp == 1) {
-        if (lane == 0) {  // ------------------------------------------ MMA issuer
+        if (lane == 0) {  // ------------------------------------------ z MMA issuer
             const uint32_t idesc_z = (2u << 4) | (1u << 15) | ((n_rows >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
-            const uint32_t idesc_r = (2u << 4) | ((16u >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
             uint64_t it = 0, gc = 0;
             bool stop = false;
             for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x, ++gc) {
@@ -434,6 +436,39 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 }
                 tc_after();
                 for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
+                    const uint32_t st = (uint32_t)(it % stages);
+                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
+                        abort_s = 1;
+                        atomicOr(err, 8u);
+                        stop = true;
+                        break;
+                    }
+                    tc_after();
+                    const uint32_t sb = base + st * stage_bytes;
+                    for (uint32_t s = 0; s < sg; ++s)
+#pragma unroll
+                        for (uint32_t ks = 0; ks < TC_ROWS / 32; ++ks)  // strip read MN-major
+                            mma_i8(tmem + s * n_rows, sdesc(sb + s * STRIP_BYTES + ks * 4096u, STRIP_BYTES, 1024),
+                                   sdesc(sb + u_off + ks * 32u, 16, 1024), idesc_z, (rb | ks) != 0);
+                    mma_commit(&empty_b[st]);  // this issuer is done with the stage
+                }
+                if (stop) break;
+                mma_commit(&accf_b);
+            }
+            mma_commit(&done_b);
+            bar_wait(&done_b, 0);
+        }
+    } else if (warp == FU_R_WARP) {
+        if (lane == 0) {  // ------------------------------------------ r MMA issuer
+            const uint32_t idesc_r = (2u << 4) | ((16u >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+            uint64_t it = 0;
+            bool stop = false;
+            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
+                const uint32_t p = item / groups, g = item % groups;
+                const TcPanel pn = panels[p];
+                const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
+                const uint32_t sg = min((uint32_t)S, 64u - g * S);
+                for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                     const uint32_t st = (uint32_t)(it % stages), eb = (uint32_t)(it & 1);
                     if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s ||
                         (it >= 2 && !bar_wait(&rfree_b[eb], (uint32_t)(((it >> 1) - 1) & 1)))) {
@@ -446,19 +481,12 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                     const uint32_t sb = base + st * stage_bytes;
                     for (uint32_t s = 0; s < sg; ++s)
 #pragma unroll
-                        for (uint32_t ks = 0; ks < TC_ROWS / 32; ++ks) {
-                            // z: strip read MN-major (M = its byte columns, K = the stage's rows)
-                            mma_i8(tmem + s * n_rows, sdesc(sb + s * STRIP_BYTES + ks * 4096u, STRIP_BYTES, 1024),
-                                   sdesc(sb + u_off + ks * 32u, 16, 1024), idesc_z, (rb | ks) != 0);
-                            // r: strip read K-major (M = the stage's rows, K = its byte columns)
+                        for (uint32_t ks = 0; ks < TC_ROWS / 32; ++ks)  // strip read K-major
                             mma_i8(tmem + FU_E_COL + 16 * eb, sdesc(sb + s * STRIP_BYTES + ks * 32u, 16, 1024),
                                    sdesc(sb + w_off + s * W_STRIP_BYTES + ks * 32u, 16, 1024), idesc_r, (s | ks) != 0);
-                        }
-                    mma_commit(&empty_b[st]);  // stage reusable once these MMAs have read it
-                    mma_commit(&racc_b[eb]);   // the stage's row products are ready for the drain warps
+                    mma_commit(&empty_b[st]);
+                    mma_commit(&racc_b[eb]);  // the stage's row products are ready for the drain warps
                 }
-                if (stop) break;
-                mma_commit(&accf_b);
             }
             mma_commit(&done_b);
             bar_wait(&done_b, 0);
@@ -480,7 +508,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
             __syncwarp();
             if (lane == 0) bar_arrive(&acce_b);
         }
-    } else {
+    } else if (warp < FU_R_WARP) {
         // ---------------------------------------------------------- r drain warps
         // Lane (quarter q) = stage row q*32 + lane: E[row][s] for s < 16 ->
         // sum_s 2^(8s) E[s] mod p, grouped by 4 (weights 2^0, 2^32, 2^64 =
