@@ -398,7 +398,7 @@ def run_block(args, flat, L, seed, dev, stream, single_qps, dist):
         peak_tops = 2.0 * 1590.0
     best = None
     for B in sizes:
-        plan = flat.block_plan(B, trials, k, autotune=True)
+        plan = flat.block_plan(B, trials, k, autotune=args.block_autotune)
         cfg = plan.block_config()
         G = max(1, min(4, pool // B))
         reps = max(args.warmup + 1, min(10240 // B, 1280) // G)
@@ -601,6 +601,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--block-sizes", default="8,32,128,512",
                     help="block scoring sizes B to time after the single-query metric ('' to skip)")
+    ap.add_argument("--no-block-autotune", dest="block_autotune", action="store_false",
+                    help="block plans keep the default GEMM tiling (no autotuning launches)")
     ap.add_argument("--ivf-rows", type=int, default=2_000_000, help="IVF corpus rows (0 to skip the IVF legs)")
     ap.add_argument("--serve-rates", default="2000,10000,50000", help="Poisson arrival rates of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=1.5)
