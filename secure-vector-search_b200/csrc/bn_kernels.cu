@@ -512,25 +512,35 @@ __device__ __forceinline__ uint32_t find_query_seg(const ScanSeg* __restrict__ s
     return lo;
 }
 
-// Two rows per thread: every broadcast limb load serves both rows.
+// Two rows per thread: every broadcast limb load serves both rows.  The
+// column loads come in batches of 16 per row (32 independent loads in
+// flight per thread) ahead of the limb arithmetic: the kernel is bound by
+// memory latency, not by the multiply-adds.
 __device__ __forceinline__ void cm_dot2(const uint64_t* __restrict__ a_cm, uint64_t rows, uint64_t row0, uint64_t row1,
                                         bool has1, const uint4* __restrict__ vl, uint32_t n1, uint64_t& out0,
                                         uint64_t& out1) {
     uint64_t a0 = 0, a1 = 0, a2 = 0, e0 = 0, e1 = 0, e2 = 0;
     const uint64_t* p0 = a_cm + row0;
     const uint64_t* p1 = a_cm + (has1 ? row1 : row0);
-#pragma unroll 4
-    for (uint32_t k = 0; k < n1; ++k) {
-        const uint64_t x = __ldg(p0 + (uint64_t)k * rows);
-        const uint64_t y = __ldg(p1 + (uint64_t)k * rows);
-        const uint4 l0 = vl[2 * k], l1 = vl[2 * k + 1];  // {b0,b1,b2,c0}, {c1,c2,-,-}
-        const uint32_t xl = (uint32_t)x, xh = (uint32_t)(x >> 32), yl = (uint32_t)y, yh = (uint32_t)(y >> 32);
-        a0 = mac(mac(a0, xl, l0.x), xh, l0.w);
-        a1 = mac(mac(a1, xl, l0.y), xh, l1.x);
-        a2 = mac(mac(a2, xl, l0.z), xh, l1.y);
-        e0 = mac(mac(e0, yl, l0.x), yh, l0.w);
-        e1 = mac(mac(e1, yl, l0.y), yh, l1.x);
-        e2 = mac(mac(e2, yl, l0.z), yh, l1.y);
+    for (uint32_t k0 = 0; k0 < n1; k0 += 16) {  // n1 is a multiple of 16
+        uint64_t xs[16], ys[16];
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            xs[kk] = __ldg(p0 + (uint64_t)(k0 + kk) * rows);
+            ys[kk] = __ldg(p1 + (uint64_t)(k0 + kk) * rows);
+        }
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            const uint4 l0 = vl[2 * (k0 + kk)], l1 = vl[2 * (k0 + kk) + 1];  // {b0,b1,b2,c0}, {c1,c2,-,-}
+            const uint64_t x = xs[kk], y = ys[kk];
+            const uint32_t xl = (uint32_t)x, xh = (uint32_t)(x >> 32), yl = (uint32_t)y, yh = (uint32_t)(y >> 32);
+            a0 = mac(mac(a0, xl, l0.x), xh, l0.w);
+            a1 = mac(mac(a1, xl, l0.y), xh, l1.x);
+            a2 = mac(mac(a2, xl, l0.z), xh, l1.y);
+            e0 = mac(mac(e0, yl, l0.x), yh, l0.w);
+            e1 = mac(mac(e1, yl, l0.y), yh, l1.x);
+            e2 = mac(mac(e2, yl, l0.z), yh, l1.y);
+        }
     }
     out0 = combine3(a0, a1, a2);
     out1 = combine3(e0, e1, e2);
@@ -610,12 +620,17 @@ decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ 
             // M T: signed column sums, lazily folded
             uint64_t m_t = 0;
             uint32_t c = 0;
-            for (; c + 3 <= tn; c += 3) {
-                const uint32_t e0 = tl[c], e1 = tl[c + 1], e2 = tl[c + 2];
-                const uint64_t x0 = __ldg(mp_cm + (uint64_t)(e0 & 0x3ffu) * total_rows + gr);
-                const uint64_t x1 = __ldg(mp_cm + (uint64_t)(e1 & 0x3ffu) * total_rows + gr);
-                const uint64_t x2 = __ldg(mp_cm + (uint64_t)(e2 & 0x3ffu) * total_rows + gr);
-                m_t = fold(m_t) + signed_term(x0, e0 >> 31) + signed_term(x1, e1 >> 31) + signed_term(x2, e2 >> 31);
+            for (; c + 8 <= tn; c += 8) {  // 8 gathers in flight, folded two terms at a time
+                uint64_t x[8];
+                uint32_t e[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    e[q] = tl[c + q];
+                    x[q] = __ldg(mp_cm + (uint64_t)(e[q] & 0x3ffu) * total_rows + gr);
+                }
+#pragma unroll
+                for (int q = 0; q < 8; q += 2)
+                    m_t = fold(m_t) + signed_term(x[q], e[q] >> 31) + signed_term(x[q + 1], e[q + 1] >> 31);
             }
             for (; c < tn; ++c) {
                 const uint32_t e = tl[c];
@@ -627,14 +642,16 @@ decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ 
             const uint32_t sl = (uint32_t)(gr & 31), off = s_off[slice], wdt = s_w[slice];
             uint64_t s_v = 0;
             uint32_t cc = 0;
-            for (; cc + 3 <= wdt; cc += 3) {
-                const uint16_t f0 = __ldg(s_ell + off + (uint64_t)cc * 32 + sl);
-                const uint16_t f1 = __ldg(s_ell + off + (uint64_t)(cc + 1) * 32 + sl);
-                const uint16_t f2 = __ldg(s_ell + off + (uint64_t)(cc + 2) * 32 + sl);
-                const uint64_t y0 = f0 == 0xffffu ? 0 : signed_term(vs[f0 & 0x3ffu], f0 & 0x8000u);
-                const uint64_t y1 = f1 == 0xffffu ? 0 : signed_term(vs[f1 & 0x3ffu], f1 & 0x8000u);
-                const uint64_t y2 = f2 == 0xffffu ? 0 : signed_term(vs[f2 & 0x3ffu], f2 & 0x8000u);
-                s_v = fold(s_v) + y0 + y1 + y2;
+            for (; cc + 8 <= wdt; cc += 8) {  // 8 entry loads in flight
+                uint16_t f[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) f[q] = __ldg(s_ell + off + (uint64_t)(cc + q) * 32 + sl);
+#pragma unroll
+                for (int q = 0; q < 8; q += 2) {
+                    const uint64_t y0 = f[q] == 0xffffu ? 0 : signed_term(vs[f[q] & 0x3ffu], f[q] & 0x8000u);
+                    const uint64_t y1 = f[q + 1] == 0xffffu ? 0 : signed_term(vs[f[q + 1] & 0x3ffu], f[q + 1] & 0x8000u);
+                    s_v = fold(s_v) + y0 + y1;
+                }
             }
             for (; cc < wdt; ++cc) {
                 const uint16_t f = __ldg(s_ell + off + (uint64_t)cc * 32 + sl);
