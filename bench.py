@@ -203,6 +203,11 @@ def cpu_reference(d: int, trials: int, k: int, steps: int, warmup: int, n_total:
 
 
 # ------------------------------------------------------------------ GPU leg
+def progress(msg: str):
+    """Leg boundaries on stderr (stdout carries only the JSON line)."""
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
+
+
 def run_gpu(args, rank: int, world: int, local_rank: int):
     import torch
 
@@ -349,12 +354,16 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     }
     plans["full"].close()
     plans["noverify"].close()
+    progress("single-query leg done")
     if args.block_sizes:
         res["block"] = run_block(args, flat, L, seed, dev, stream, res["value"], dist)
+        progress("block leg done")
     if args.ivf_rows:
         res["ivf"], ivf, data = run_ivf(args, ctx, dist)
+        progress("IVF leg done")
         if args.serve_rates:
             res["serving"] = run_serving(args, flat, ivf, L, data, dist)
+            progress("serving leg done")
         ivf.close()
     flat.close()
     ctx.close()
@@ -518,8 +527,27 @@ def run_ivf(args, ctx, dist):
             ivf.query(pr, vb, gb, tb, seeds, args.trials, 10)
             t.append(time.perf_counter() - ta)
         dt = statistics.median(t)
-        out["per_nprobe"][str(nprobe)] = {"qps": bq / dt, "ms_per_batch": dt * 1e3, "rows_per_query": rows_q,
-                                          "effective_gbs": bq * rows_q * N_DIM * 8 / dt / 1e9}
+        uniq = np.unique(pr)
+        rows_u = float(data["sizes"][uniq].sum())
+        res = {"qps": bq / dt, "ms_per_batch": dt * 1e3, "rows_per_query": rows_q,
+               "effective_gbs": bq * rows_q * N_DIM * 8 / dt / 1e9, "distinct_lists": int(len(uniq)),
+               "distinct_rows": rows_u}
+        # block form: the batch's (query, list) pairs grouped by list, every
+        # probed list read once; Protocol 2 per block and list
+        progress(f"IVF nprobe {nprobe}: per-query path timed")
+        bseed = bytes([seed, nprobe & 0xFF]) * 16
+        bh, bfc, _ = ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
+        assert np.all(bfc == -1), "IVF block verification failed on honest responses"
+        same = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(hits, bh))
+        t = []
+        for _ in range(reps):
+            ta = time.perf_counter()
+            ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
+            t.append(time.perf_counter() - ta)
+        db = statistics.median(t)
+        res["block"] = {"qps": bq / db, "ms_per_batch": db * 1e3, "hits_equal_per_query": bool(same),
+                        "distinct_rows_gbs": rows_u * N_DIM * 8 / db / 1e9}
+        out["per_nprobe"][str(nprobe)] = res
     return out, ivf, data
 
 

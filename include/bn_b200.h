@@ -254,6 +254,31 @@ int bn_ivf_query(bn_ivf* h, uint32_t B, uint32_t nprobe, const uint32_t* probes,
                  const uint8_t* v_seeds, uint32_t trials, uint32_t k, uint32_t* ids, int64_t* scores, uint32_t* n_hits,
                  int32_t* failed_cluster, int32_t* failed_trial);
 
+/* IVF block scoring: the batch's (query, list) pairs grouped by list, so
+ * that every probed list is read once per batch (byte-planar GEMMs on the
+ * tensor cores, one group per list).  Scores and ranking as bn_ivf_query
+ * (ivf.rs:746-927: every probed list, empty ones skipped, global top-k).
+ * Protocol 2 per block and list: list c's draws are verify_response's
+ * (crypto.rs:1013-1059) on list c with block_seed as the seed (ivf.rs:791-806
+ * seeds one fresh ChaCha20Rng per list), shared by every query that probes c;
+ * failed_cluster / failed_trial as bn_ivf_query.  No counterpart in the
+ * reference, which verifies each (query, list) with the query's own seed.
+ * Needs the int8-quantised client state (as bn_flat_query_block;
+ * BN_EUNSUPPORTED otherwise); bn_ivf_block_prepare builds the byte-planar
+ * corpus copies ahead of the first call. */
+int bn_ivf_block_prepare(bn_ivf* h);
+int bn_ivf_query_block(bn_ivf* h, uint32_t B, uint32_t nprobe, const uint32_t* probes, const uint64_t* v_enc,
+                       const uint64_t* g, const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz,
+                       const uint8_t block_seed[32], uint32_t trials, uint32_t k, uint32_t* ids, int64_t* scores,
+                       uint32_t* n_hits, int32_t* failed_cluster, int32_t* failed_trial);
+/* Protocol 2 of the block form over claimed responses: r holds every
+ * (query, list) pair's m_c responses, pairs in probe order (query-major,
+ * empty lists skipped), r_len entries in all.  ur / zv (nullable, pairs x
+ * trials, [pair][t]) = u_t . r_pair and z_t^c . v_q. */
+int bn_ivf_verify_block(bn_ivf* h, uint32_t B, uint32_t nprobe, const uint32_t* probes, const uint64_t* r,
+                        uint64_t r_len, const uint64_t* v_enc, const uint8_t block_seed[32], uint32_t trials,
+                        int32_t* failed_cluster, int32_t* failed_trial, uint64_t* ur, uint64_t* zv);
+
 /* ---------------------------------------------------------------- serving loop
  * Continuous batching over device-resident corpora.  No counterpart in the
  * reference, whose scorers serve one query per call with every GPU call
@@ -279,9 +304,11 @@ typedef struct bn_server_config {
     uint32_t max_wait_us; /* batching window */
     uint32_t trials;      /* Protocol 2 trials per query (params.verification_trials()) */
     uint32_t k;           /* hits per query */
-    uint32_t block_min;   /* flat batches of >= block_min requests run as block scoring (bn_flat_block_plan):
-                             one pass over the corpus for the batch, Protocol 2 per block with the first
-                             request's seed; 0 = every flat query verified with its own seed */
+    uint32_t block_min;   /* batches of >= block_min requests run as block scoring: flat ones as
+                             bn_flat_block_plan (one pass over the corpus for the batch), IVF ones as
+                             bn_ivf_query_block (every probed list read once per batch); Protocol 2 per
+                             block (and list) with the first request's seed; 0 = every query verified
+                             with its own seed */
 } bn_server_config;
 typedef struct bn_server_stats_t {
     uint64_t submitted, completed, batches;
@@ -289,7 +316,7 @@ typedef struct bn_server_stats_t {
     double p50_us, p99_us, max_us;     /* submit -> result latency */
     double throughput_qps;             /* completed / (last completion - first submit) */
     uint64_t peak_workspace_bytes;
-    uint64_t block_batches;            /* flat batches that ran as block scoring */
+    uint64_t block_batches;            /* batches (flat or IVF) that ran as block scoring */
 } bn_server_stats_t;
 /* flat and/or ivf (nullable, not both), with client state, in one context. */
 int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn_server** out);

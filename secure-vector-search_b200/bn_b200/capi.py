@@ -94,6 +94,9 @@ _SIGS = {
     "bn_ivf_decode_dense_terms": (C.c_int, [vp, u32, vp, vp, vp, vp]),
     "bn_ivf_verify": (C.c_int, [vp, u32, vp, vp, vp, u32, vp, vp, vp]),
     "bn_ivf_query": (C.c_int, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
+    "bn_ivf_block_prepare": (C.c_int, [vp]),
+    "bn_ivf_query_block": (C.c_int, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
+    "bn_ivf_verify_block": (C.c_int, [vp, u32, u32, vp, vp, u64, vp, vp, u32, vp, vp, vp, vp]),
     "bn_encrypt_cluster": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, vp, vp]),
     "bn_server_create": (C.c_int, [vp, vp, C.POINTER(ServerConfig), vp]),
     "bn_server_submit_flat": (C.c_int, [vp, vp, vp, vp, vp, u32, vp, vp]),
@@ -439,6 +442,57 @@ class Ivf:
                                ptr(nh), ptr(fc), ptr(ft)))
         hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
         return hits, fc, ft
+
+    # ---- block scoring: the batch's (query, list) pairs grouped by list, Protocol 2 per block and list
+    def block_prepare(self):
+        check(lib.bn_ivf_block_prepare(self.h))
+
+    def query_block(self, probes, v_enc, g, t_list, block_seed, trials, k):
+        pr = np.ascontiguousarray(probes, np.uint32)
+        B, nprobe = pr.shape
+        v = _u64(v_enc).reshape(B, N)
+        gg = _u64(g).reshape(B, self.n1)
+        ti, ts, tn = _t_concat(t_list)
+        seed = None if block_seed is None else np.frombuffer(bytes(block_seed), np.uint8).copy()
+        kk = max(k, 1)
+        ids = np.zeros((B, kk), np.uint32)
+        sc = np.zeros((B, kk), np.int64)
+        nh = np.zeros(B, np.uint32)
+        fc = np.zeros(B, np.int32)
+        ft = np.zeros(B, np.int32)
+        check(lib.bn_ivf_query_block(self.h, B, nprobe, ptr(pr), ptr(v), ptr(gg), ptr(ti) if ti.size else None,
+                                     ptr(ts) if ts.size else None, ptr(tn), ptr(seed), trials, k, ptr(ids), ptr(sc),
+                                     ptr(nh), ptr(fc), ptr(ft)))
+        hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
+        return hits, fc, ft
+
+    def pairs(self, probes):
+        """(query, list, rows) of every (query, list) pair of a batch in probe order, empty lists skipped:
+        the layout of the r argument of verify_block."""
+        out = []
+        for q, row in enumerate(np.asarray(probes)):
+            for c in row:
+                m = int(self.offsets[c + 1] - self.offsets[c])
+                if m:
+                    out.append((q, int(c), m))
+        return out
+
+    def verify_block(self, probes, r, v_enc, block_seed, trials):
+        """Protocol 2 over claimed responses r (every pair's r in probe order, concatenated):
+        per query (failed_cluster, failed_trial), and per pair and trial u_t . r and z_t . v."""
+        pr = np.ascontiguousarray(probes, np.uint32)
+        B, nprobe = pr.shape
+        r = _u64(r).reshape(-1)
+        v = _u64(v_enc).reshape(B, N)
+        seed = np.frombuffer(bytes(block_seed), np.uint8).copy()
+        npairs = len(self.pairs(pr))
+        fc = np.zeros(B, np.int32)
+        ft = np.zeros(B, np.int32)
+        ur = np.zeros((max(npairs, 1), trials), np.uint64)
+        zv = np.zeros((max(npairs, 1), trials), np.uint64)
+        check(lib.bn_ivf_verify_block(self.h, B, nprobe, ptr(pr), ptr(r) if r.size else None, r.size, ptr(v),
+                                      ptr(seed), trials, ptr(fc), ptr(ft), ptr(ur), ptr(zv)))
+        return fc, ft, ur[:npairs], zv[:npairs]
 
     def close(self):
         if self.h:

@@ -28,24 +28,37 @@ using namespace tcg;
 constexpr int BG_EPI_WARPS = 8;
 constexpr int BG_THREADS = 64 + 32 * BG_EPI_WARPS;  // TMA warp, MMA warp, epilogue warps
 
+// A work item: K panel, TMA rows of the A and W tiles, and the output range.
 struct ItemIdx {
-    uint32_t kp, ta, tw;
+    uint32_t kp, tw;  // tw: W tile (A-resident mode reloads A when it wraps to 0)
+    uint32_t a_y, w_y, x0, x_lim, y0, y_lim;
 };
+__device__ __forceinline__ ItemIdx grid_item(const BgParams& p, uint32_t kp, uint32_t ta, uint32_t tw) {
+    const uint32_t x0 = p.mode == BG_S8 ? ta * BG_AROWS : ta * (BG_AROWS / 8);
+    return ItemIdx{kp, tw, ta * BG_AROWS, tw * p.w_tile, x0, p.x_count, tw * p.w_tile / 8, p.y_count};
+}
 __device__ __forceinline__ ItemIdx item_idx(const BgParams& p, uint32_t item) {
     const uint32_t per = p.a_tiles * p.w_tiles;
     const uint32_t kp = item / per, rem = item % per;
-    if (p.order_a_fast) return ItemIdx{kp, rem % p.a_tiles, rem / p.a_tiles};
-    return ItemIdx{kp, rem / p.w_tiles, rem % p.w_tiles};
+    if (p.order_a_fast) return grid_item(p, kp, rem % p.a_tiles, rem / p.a_tiles);
+    return grid_item(p, kp, rem / p.w_tiles, rem % p.w_tiles);
 }
 
 // The j-th work item of this CTA.  Streaming mode: global items blockIdx.x +
 // j * gridDim.x.  A-resident mode: this CTA owns A tiles blockIdx.x + t *
 // gridDim.x and visits every W tile of each (j = t * w_tiles + tw).
 __device__ __forceinline__ bool item_at(const BgParams& p, uint32_t items, uint32_t j, ItemIdx& ix) {
+    if (p.item_tab) {
+        const uint32_t item = blockIdx.x + j * gridDim.x;
+        if (item >= p.n_items) return false;
+        const BgItem t = p.item_tab[item];
+        ix = ItemIdx{0, 1, t.a_y, t.w_y, t.x0, t.x_lim, t.y0, t.y_lim};
+        return true;
+    }
     if (p.a_resident) {
         const uint32_t ta = blockIdx.x + (j / p.w_tiles) * gridDim.x;
         if (ta >= p.a_tiles) return false;
-        ix = ItemIdx{0, ta, j % p.w_tiles};
+        ix = grid_item(p, 0, ta, j % p.w_tiles);
         return true;
     }
     const uint32_t item = blockIdx.x + j * gridDim.x;
@@ -70,7 +83,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
     constexpr uint32_t A_BYTES = BG_AROWS * BG_KSTEP;
     const uint32_t w_bytes = p.w_tile * BG_KSTEP;
     const uint32_t kpanels = (p.k_bytes + p.k_panel - 1) / p.k_panel;
-    const uint32_t items = kpanels * p.a_tiles * p.w_tiles;
+    const uint32_t items = p.item_tab ? p.n_items : kpanels * p.a_tiles * p.w_tiles;
     const uint32_t a_slots = p.a_resident ? p.k_bytes / BG_KSTEP : 0;
     const uint32_t base = sbase + a_slots * A_BYTES;  // stage ring
     uint8_t* ring = sptr + a_slots * A_BYTES;
@@ -127,7 +140,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                             break;
                         }
                         bar_expect_tx(&afull_b[ks], A_BYTES);
-                        tma_2d(sptr + ks * A_BYTES, &tmap_a, (int)k, (int)(ix.ta * BG_AROWS), &afull_b[ks]);
+                        tma_2d(sptr + ks * A_BYTES, &tmap_a, (int)k, (int)ix.a_y, &afull_b[ks]);
                         t_last = t;
                     }
                     const uint32_t st = (uint32_t)(it % stages);
@@ -141,11 +154,11 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     uint8_t* sb = ring + (uint64_t)st * stage_bytes;
                     if (a_slots) {
                         bar_expect_tx(&full_b[st], w_bytes);
-                        tma_2d(sb, &tmap_w, (int)k, (int)(ix.tw * p.w_tile), &full_b[st]);
+                        tma_2d(sb, &tmap_w, (int)k, (int)ix.w_y, &full_b[st]);
                     } else {
                         bar_expect_tx(&full_b[st], A_BYTES + w_bytes);
-                        tma_2d(sb, &tmap_a, (int)k, (int)(ix.ta * BG_AROWS), &full_b[st]);
-                        tma_2d(sb + A_BYTES, &tmap_w, (int)k, (int)(ix.tw * p.w_tile), &full_b[st]);
+                        tma_2d(sb, &tmap_a, (int)k, (int)ix.a_y, &full_b[st]);
+                        tma_2d(sb + A_BYTES, &tmap_w, (int)k, (int)ix.w_y, &full_b[st]);
                     }
                 }
             }
@@ -218,11 +231,11 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
             if (__any_sync(FULLMASK, !ok || abort_s)) break;
             tc_after();
             const uint32_t taddr = tmem + ((q * 32u) << 16) + buf * 256u;
-            const uint32_t ybase = ix.tw * p.w_tile / 8;
+            const uint32_t ybase = ix.y0;
             const uint32_t wide = p.w_tile & ~63u;  // columns handled in 64-column chunks
             if (p.mode == BG_PLANAR) {
                 const uint32_t a = lane & 7, xi = lane >> 3;
-                const uint32_t x4 = ix.ta * (BG_AROWS / 8) + q * 4;  // first x of this warp
+                const uint32_t x4 = ix.x0 + q * 4;  // first x of this warp
                 const uint32_t x = x4 + xi;
                 const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
                 uint64_t* out = p.out + (uint64_t)ix.kp * p.out_pstride;
@@ -253,7 +266,8 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     const uint64_t f =
                         canon((b0 ? k2[1] : k2[0]) + __shfl_xor_sync(FULLMASK, b0 ? k2[0] : k2[1], 1));  // < 8p
                     const uint32_t y = ybase + c0 / 8 + a;
-                    if (y < p.y_count && x < p.x_count) out[(uint64_t)y * p.out_ld + x] = f;
+                    if (y < ix.y_lim && x < ix.x_lim)
+                        out[p.pair_base ? p.pair_base[y] + x : (uint64_t)y * p.out_ld + x] = f;
                     if (p.planar_out) {
                         // 4 x 8 byte transpose across the lanes of one y: lane
                         // (xi, a) ends with planes 4(xi&1) + 2(xi>>1) + {0, 1}
@@ -267,7 +281,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         const uint32_t keep2 = e1 ? pb : pa;
                         const uint32_t recv2 = __shfl_xor_sync(FULLMASK, e1 ? pa : pb, 16);
                         const uint32_t p0 = e1 ? recv2 : keep2, p1 = e1 ? keep2 : recv2;
-                        if (y < p.y_count && x4 < p.x_count) {
+                        if (y < ix.y_lim && x4 < ix.x_lim) {
                             const uint32_t plane = 4 * (xi & 1) + 2 * (xi >> 1);
                             uint8_t* dst = p.planar_out + ((uint64_t)y * 8 + plane) * p.planar_ld + x4;
                             *reinterpret_cast<uint32_t*>(dst) = __byte_perm(p0, p1, 0x5410);
@@ -296,17 +310,18 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         uint32_t packed = (uint32_t)((f >> (8 * a)) & 0xffu) << (8 * xi);
                         packed |= __shfl_xor_sync(FULLMASK, packed, 8);
                         packed |= __shfl_xor_sync(FULLMASK, packed, 16);
-                        if (y < p.y_count) {
-                            if (a == 0 && x < p.x_count) out[(uint64_t)y * p.out_ld + x] = f;
-                            if (p.planar_out && lane < 8 && x4 < p.x_count)
+                        if (y < ix.y_lim) {
+                            if (a == 0 && x < ix.x_lim)
+                                out[p.pair_base ? p.pair_base[y] + x : (uint64_t)y * p.out_ld + x] = f;
+                            if (p.planar_out && lane < 8 && x4 < ix.x_lim)
                                 *reinterpret_cast<uint32_t*>(p.planar_out + ((uint64_t)y * 8 + lane) * p.planar_ld +
                                                              x4) = packed;
                         }
                     }
                 }
             } else {
-                const uint32_t x = ix.ta * BG_AROWS + q * 32 + lane;
-                const bool xv = x < p.x_count;
+                const uint32_t x = ix.x0 + q * 32 + lane;
+                const bool xv = x < ix.x_lim;
                 const uint64_t corr = xv ? p.corr[x] : 0;
                 for (uint32_t c0 = 64 * half; c0 < wide; c0 += 128) {
                     uint32_t v[64];
@@ -322,7 +337,9 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         const uint64_t lr = lo < 0 ? (uint64_t)(lo + (int64_t)P) : (uint64_t)lo;
                         const uint64_t hr = hi < 0 ? (uint64_t)(hi + (int64_t)P) : (uint64_t)hi;
                         const uint32_t y = ybase + c0 / 8 + yy;
-                        if (xv && y < p.y_count) p.out[(uint64_t)y * p.out_ld + x] = add_mod(canon(lr + rotl61(hr, 32)), corr);
+                        if (xv && y < ix.y_lim)
+                            p.out[p.pair_base ? p.pair_base[y] + x : (uint64_t)y * p.out_ld + x] =
+                                add_mod(canon(lr + rotl61(hr, 32)), corr);
                     }
                 }
                 for (uint32_t c0 = wide + 16 * half; c0 < p.w_tile; c0 += 32) {
@@ -339,7 +356,9 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         const uint64_t lr = lo < 0 ? (uint64_t)(lo + (int64_t)P) : (uint64_t)lo;
                         const uint64_t hr = hi < 0 ? (uint64_t)(hi + (int64_t)P) : (uint64_t)hi;
                         const uint32_t y = ybase + c0 / 8 + h;
-                        if (xv && y < p.y_count) p.out[(uint64_t)y * p.out_ld + x] = add_mod(canon(lr + rotl61(hr, 32)), corr);
+                        if (xv && y < ix.y_lim)
+                            p.out[p.pair_base ? p.pair_base[y] + x : (uint64_t)y * p.out_ld + x] =
+                                add_mod(canon(lr + rotl61(hr, 32)), corr);
                     }
                 }
             }
@@ -531,17 +550,23 @@ uint32_t bgemm_smem_bytes(const BgParams& p, uint32_t stages) {
     return a + stages * bgemm_stage_bytes(p.w_tile, p.a_resident != 0) + 1024u;
 }
 
+uint32_t bgemm_max_stages(const BgParams& p) {
+    for (uint32_t st = BG_MAX_STAGES; st >= 2; --st)
+        if (bgemm_smem_bytes(p, st) + 1024 <= BG_MAX_SMEM) return st;
+    return 0;
+}
+
 void launch_bgemm(const CUtensorMap& tmap_a, const CUtensorMap& tmap_w, const BgParams& p, uint32_t stages, int ctas,
                   uint32_t* d_err, cudaStream_t s) {
     const uint32_t kpanels = (p.k_bytes + p.k_panel - 1) / p.k_panel;
-    const uint64_t items = (uint64_t)kpanels * p.a_tiles * p.w_tiles;
+    const uint64_t items = p.item_tab ? p.n_items : (uint64_t)kpanels * p.a_tiles * p.w_tiles;
     if (!items) return;
     const uint32_t stage_bytes = bgemm_stage_bytes(p.w_tile, p.a_resident != 0);
     // at least half the SM's shared memory: one CTA per SM, so the second
     // never waits in tcgen05.alloc for the first one's 512 TMEM columns
     const int smem = (int)std::max<uint32_t>(bgemm_smem_bytes(p, stages), 116u * 1024u);
     cudaFuncSetAttribute(bgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    const uint64_t units = p.a_resident ? p.a_tiles : items;
+    const uint64_t units = p.item_tab ? p.n_items : p.a_resident ? p.a_tiles : items;
     const unsigned grid = units < (uint64_t)ctas ? (unsigned)units : (unsigned)ctas;
     bgemm_kernel<<<grid, BG_THREADS, smem, s>>>(tmap_a, tmap_w, p, stages, stage_bytes, d_err);
 }

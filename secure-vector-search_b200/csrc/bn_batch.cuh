@@ -37,6 +37,16 @@ enum BgMode : int {
     BG_S8 = 1,
 };
 
+// One work item of a grouped GEMM (an item table): the A and W tiles' TMA row
+// coordinates, the corpus rows x in [x0, x_lim) and the output slots y in
+// [y0, y_lim) that the item's outputs may write (outputs go to
+// out[pair_base[y] + x]).  PLANAR: x0 = a_y / 8; S8: x0 = a_y.
+struct BgItem {
+    uint32_t a_y, w_y;
+    uint32_t x0, x_lim;
+    uint32_t y0, y_lim;
+};
+
 struct BgParams {
     int mode;
     uint32_t a_tiles;      // ceil(A rows / 128)
@@ -54,6 +64,11 @@ struct BgParams {
     uint64_t planar_ld;
     int order_a_fast;      // work order: 0 = W tile fastest, 1 = A tile fastest
     int a_resident;        // keep each A tile (all of K, one K panel) in shared memory across its W tiles
+    // grouped mode (nullable): work items from a table instead of the a_tiles x
+    // w_tiles grid (one K panel, no A-resident mode, no planar_out)
+    const BgItem* item_tab;
+    uint32_t n_items;
+    const uint64_t* pair_base;  // grouped outputs: out[pair_base[y] + x]
 };
 
 // tmap_a: A bytes {k_bytes, A rows}, box {128, 128}; tmap_w: W bytes
@@ -63,6 +78,8 @@ struct BgParams {
 // bgemm_smem_bytes(p, stages) <= BG_MAX_SMEM.
 void launch_bgemm(const CUtensorMap& tmap_a, const CUtensorMap& tmap_w, const BgParams& p, uint32_t stages, int ctas,
                   uint32_t* d_err, cudaStream_t s);
+// Most pipeline stages whose shared memory fits one CTA (0 when even 2 do not).
+uint32_t bgemm_max_stages(const BgParams& p);
 uint32_t bgemm_stage_bytes(uint32_t w_tile, bool a_resident);
 uint32_t bgemm_smem_bytes(const BgParams& p, uint32_t stages);
 

@@ -55,12 +55,7 @@ namespace {
 
 uint32_t kpanels_of(const BlockPlan& b) { return (uint32_t)((b.npad + b.k_panel4 - 1) / b.k_panel4); }
 
-// Most pipeline stages whose shared memory fits (0 when even 2 do not).
-uint32_t stages_for(const BgParams& p) {
-    for (uint32_t st = BG_MAX_STAGES; st >= 2; --st)
-        if (bgemm_smem_bytes(p, st) + 1024 <= BG_MAX_SMEM) return st;
-    return 0;
-}
+uint32_t stages_for(const BgParams& p) { return bgemm_max_stages(p); }
 
 // The u . r GEMM's stage count (W = the U planes, streaming A).
 uint32_t stages_u(uint32_t n_rows) {
@@ -284,6 +279,8 @@ uint64_t block_layout(BlockPlan& b, uint32_t n1, uint32_t k_alh, bool verify_onl
     b.o_out_end = L.take<uint8_t>(0);
     return L.off + 1024;
 }
+
+int block_prepare_engine(Engine& e) { return block_prepare_locked(e); }
 
 int block_prepare(bn_flat* f) {
     std::lock_guard<std::mutex> g(f->e.mu);

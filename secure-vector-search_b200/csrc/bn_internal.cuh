@@ -275,6 +275,21 @@ int job_finish(const QueryJob& j, const PinnedMem& host, uint32_t* ids, int64_t*
 struct BlockPlan;
 void block_plan_free(BlockPlan* b);
 
+// IVF block scoring (bn_ivf_block.cu): plan (host), pack (pinned staging +
+// workspace sizing), launch (H2D, pipeline, D2H on s), finish (after s drained).
+struct IvfBlockJob;
+IvfBlockJob* ivf_block_job_new();
+void ivf_block_job_free(IvfBlockJob* j);
+uint64_t ivf_block_job_bytes(const IvfBlockJob* j);
+int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* probe_off, const uint32_t* probes,
+                   uint32_t trials, uint32_t k, bool verify_only, int sms);
+int ivf_block_pack(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, const uint64_t* v_enc, const uint64_t* g,
+                   const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed);
+int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cudaStream_t s);
+int ivf_block_finish(const IvfBlockJob& j, const PinnedMem& host, uint32_t* ids, int64_t* scores, uint32_t* n_hits,
+                     int32_t* failed_cluster, int32_t* failed_trial);
+int ivf_block_prepare(bn_ivf* v);
+
 }  // namespace api
 }  // namespace bn
 
@@ -316,6 +331,10 @@ int block_query_launch(BlockPlan& b, uint32_t nq, const uint64_t* v_enc, const u
 int block_query_finish(BlockPlan& b, uint32_t nq, uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed);
 uint64_t block_plan_bytes(const BlockPlan* b);
 uint64_t block_plan_estimate(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k);
+// Byte-planar corpus copies of block scoring (once per handle; caller holds e.mu).
+int block_prepare_engine(Engine& e);
+int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms);
+int validate_residues(const uint64_t* a, uint64_t count, const char* what);
 int block_verify_host(BlockPlan& b, const uint64_t* r, const uint64_t* v_enc, const uint8_t* seed, int32_t* failed,
                       uint64_t* ur, uint64_t* zv);
 }  // namespace api

@@ -1,0 +1,721 @@
+// bn_ivf_block.cu -- IVF block scoring: a batch's (query, list) pairs grouped
+// by list, so that every probed list is read once per batch.
+//
+// The reference scores an IVF batch by looping its per-query path
+// (BnTmIvfScorer::score_batch, ivf.rs:1199-1366; on GPU handles ivf.rs:1357-1364),
+// which reads list c once for every query that probes it.  Here the pairs are
+// sorted by list and list c, probed by n_c queries of the batch, becomes one
+// group of the grouped byte-planar GEMM (bgemm item tables): its A tiles are
+// the list's rows, its W tiles the n_c queries' operand images.  Per pair (q, c):
+//   r_qc  = M_c v_q                        (G1: planes of m_enc x planes of v)
+//   f2_qc = -(AL_c g_q + H_c L^T v_q)      (G2: planes of [AL | H] x planes of -[g | x])
+//   f3_qc = M_c T_q + S_c v_q              (G3: signed bytes [M | S] x [T | bytes(v) - 128])
+//   Mv_qc = r + f2 - f3                     (decode_scores, crypto.rs:901-940)
+// in "r-space": query q's probed lists in probe order, empty lists skipped
+// (ivf.rs:787-789), then a segmented top-k per query over all its lists
+// (score desc, id asc; the global merge of ivf.rs:805-815).
+//
+// Protocol 2 per block and list: list c's draws are those of verify_response
+// (crypto.rs:1013-1059) run on list c with the block seed in place of the
+// query seed (ivf.rs:792-800 seeds a fresh ChaCha20Rng per list): u_t[i] =
+// draw t*m_c + i of ChaCha20Rng(block_seed).  They are shared by the queries
+// that probe c:
+//   z_t^c = u_t^T M_c          (tc_freivalds over the batch's distinct lists, once each)
+//   pair (q, c) passes trial t iff u_t . r_qc == z_t^c . v_q,
+// and query q is rejected at its first failing list in probe order.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "bn_batch.cuh"
+#include "bn_internal.cuh"
+#include "bn_tc.cuh"
+
+using namespace bn;
+using namespace bn::api;
+
+namespace bn {
+namespace api {
+
+namespace {
+
+// One (query, list) pair, in q-major order (query q's probes in order).
+struct IvPair {
+    uint64_t out0;     // first r-space entry
+    uint32_t q, list;  // query, list id
+    uint32_t u;        // index of the list among the batch's distinct lists
+    uint32_t ch0, nch; // its ur chunks
+    uint32_t pad;
+};
+
+// Up to IV_CHUNK_ROWS rows of one pair (u . r partial sums, ids).
+struct IvChunk {
+    uint64_t r0;    // first r-space entry
+    uint64_t row0;  // first corpus row
+    uint32_t ublk;  // first 128-row block of the list's U image
+    uint32_t rows;
+};
+constexpr uint32_t IV_CHUNK_ROWS = 4096;
+
+// ------------------------------------------------------------------ kernels
+// dst block lp (8 rows of row_bytes) = src block map[lp]
+__global__ void gather8_kernel(const uint4* __restrict__ src, uint4* __restrict__ dst, const uint32_t* __restrict__ map,
+                               uint32_t n, uint32_t row_bytes) {
+    const uint32_t per = 8 * row_bytes / 16;
+    const uint64_t total = (uint64_t)n * per;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t lp = (uint32_t)(e / per), c = (uint32_t)(e % per);
+        dst[(uint64_t)lp * per + c] = src[(uint64_t)map[lp] * per + c];
+    }
+}
+
+// idmap[r-space entry] = corpus id of its row
+__global__ void idmap_kernel(const IvChunk* __restrict__ chunks, const uint32_t* __restrict__ ids,
+                             uint32_t* __restrict__ idmap) {
+    const IvChunk c = chunks[blockIdx.x];
+    for (uint32_t i = threadIdx.x; i < c.rows; i += blockDim.x) idmap[c.r0 + i] = ids[c.row0 + i];
+}
+
+// 128-bit accumulation of a 61 x 61-bit product.
+__device__ __forceinline__ void mac128(uint64_t& lo, uint64_t& hi, uint64_t a, uint64_t b) {
+    const uint64_t pl = a * b, ph = __umul64hi(a, b);
+    lo += pl;
+    hi += ph + (lo < pl ? 1u : 0u);
+}
+
+// u_t . r per chunk, for trials [t_base, t_base + t_cnt): the U image of
+// block b (launch_tc_ugen, per-block images) holds byte a of u_t[i] at row
+// (8t + a), column i.  Warp w takes blocks w, w + 4, ...; lane l rows 4l..4l+3
+// of each: it reads one 32-bit word from each of the 8 byte rows of trial t
+// and transposes them into the four u_t values.  At most 8 blocks x 4 rows =
+// 32 products (< 2^122 each) per lane and trial are summed in 128 bits.
+__global__ void __launch_bounds__(128)
+ur_chunks_kernel(const IvChunk* __restrict__ chunks, const uint8_t* __restrict__ ub, uint32_t n_rows, uint32_t t_base,
+                 uint32_t t_cnt, uint32_t trials_total, const uint64_t* __restrict__ r, uint64_t* __restrict__ ur_part) {
+    const IvChunk c = chunks[blockIdx.x];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint64_t lo[TC_MAX_TRIALS], hi[TC_MAX_TRIALS];
+#pragma unroll
+    for (int t = 0; t < TC_MAX_TRIALS; ++t) lo[t] = hi[t] = 0;
+    const uint32_t nblk = (c.rows + TC_ROWS - 1) / TC_ROWS;
+    for (uint32_t b = warp; b < nblk; b += 4) {
+        const uint32_t i0 = b * TC_ROWS + 4 * lane;
+        uint64_t rv[4];
+#pragma unroll
+        for (int h = 0; h < 4; ++h) rv[h] = i0 + h < c.rows ? r[c.r0 + i0 + h] : 0;
+        const uint8_t* img = ub + (uint64_t)(c.ublk + b) * n_rows * TC_ROWS + 4 * lane;
+#pragma unroll
+        for (int t = 0; t < TC_MAX_TRIALS; ++t) {
+            if ((uint32_t)t < t_cnt) {
+                uint32_t w[8];
+#pragma unroll
+                for (int a = 0; a < 8; ++a) w[a] = *reinterpret_cast<const uint32_t*>(img + (uint64_t)(8 * t + a) * TC_ROWS);
+                // 8 x 4 byte transpose: byte a of u[h] = byte h of w[a]
+                const uint32_t l01 = __byte_perm(w[0], w[1], 0x5140), h01 = __byte_perm(w[0], w[1], 0x7362);
+                const uint32_t l23 = __byte_perm(w[2], w[3], 0x5140), h23 = __byte_perm(w[2], w[3], 0x7362);
+                const uint32_t l45 = __byte_perm(w[4], w[5], 0x5140), h45 = __byte_perm(w[4], w[5], 0x7362);
+                const uint32_t l67 = __byte_perm(w[6], w[7], 0x5140), h67 = __byte_perm(w[6], w[7], 0x7362);
+                uint64_t u[4];
+                u[0] = __byte_perm(l01, l23, 0x5410) | ((uint64_t)__byte_perm(l45, l67, 0x5410) << 32);
+                u[1] = __byte_perm(l01, l23, 0x7632) | ((uint64_t)__byte_perm(l45, l67, 0x7632) << 32);
+                u[2] = __byte_perm(h01, h23, 0x5410) | ((uint64_t)__byte_perm(h45, h67, 0x5410) << 32);
+                u[3] = __byte_perm(h01, h23, 0x7632) | ((uint64_t)__byte_perm(h45, h67, 0x7632) << 32);
+#pragma unroll
+                for (int h = 0; h < 4; ++h) mac128(lo[t], hi[t], u[h], rv[h]);
+            }
+        }
+    }
+    __shared__ uint64_t sh[4][TC_MAX_TRIALS];
+#pragma unroll
+    for (int t = 0; t < TC_MAX_TRIALS; ++t) {
+        if ((uint32_t)t < t_cnt) {
+            uint64_t x = reduce128(lo[t], hi[t]);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) x = add_mod(x, __shfl_xor_sync(0xffffffffu, x, off));
+            if (lane == 0) sh[warp][t] = x;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < t_cnt) {
+        const uint32_t t = threadIdx.x;
+        const uint64_t x = add_mod(add_mod(sh[0][t], sh[1][t]), add_mod(sh[2][t], sh[3][t]));
+        ur_part[(uint64_t)blockIdx.x * trials_total + t_base + t] = x;
+    }
+}
+
+// z[u][t][j] = sum of z_part[p][t][j] over list u's panels
+__global__ void zsum_lists_kernel(const uint64_t* __restrict__ z_part, const uint32_t* __restrict__ list_panel0,
+                                  uint32_t trials, uint64_t* __restrict__ z) {
+    const uint32_t u = blockIdx.x / trials, t = blockIdx.x % trials;
+    const uint32_t p0 = list_panel0[u], p1 = list_panel0[u + 1];
+    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
+        uint64_t acc = 0;
+        for (uint32_t p = p0; p < p1; ++p) acc = add_mod(acc, z_part[((uint64_t)p * trials + t) * N + j]);
+        z[((uint64_t)u * trials + t) * N + j] = acc;
+    }
+}
+
+// zv[i][t] = z_t^{list(i)} . v_{q(i)}; blocks visit the pairs list by list
+// (lm_pair) so that a list's z stays in L2 across its queries
+__global__ void __launch_bounds__(128) zv_pairs_kernel(const uint64_t* __restrict__ z, const uint64_t* __restrict__ v,
+                                                       const IvPair* __restrict__ pairs,
+                                                       const uint32_t* __restrict__ lm_pair, uint32_t trials,
+                                                       uint64_t* __restrict__ zv) {
+    const uint32_t i = lm_pair[blockIdx.x], t = blockIdx.y;
+    const IvPair pr = pairs[i];
+    const uint64_t* zr = z + ((uint64_t)pr.u * trials + t) * N;
+    const uint64_t* vr = v + (uint64_t)pr.q * N;
+    uint64_t lo = 0, hi = 0;
+    for (uint32_t j = threadIdx.x; j < N; j += 128) mac128(lo, hi, zr[j], vr[j]);  // 8 products per thread
+    uint64_t x = reduce128(lo, hi);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x = add_mod(x, __shfl_xor_sync(0xffffffffu, x, off));
+    __shared__ uint64_t sh[4];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) zv[(uint64_t)i * trials + t] = add_mod(add_mod(sh[0], sh[1]), add_mod(sh[2], sh[3]));
+}
+
+// First failing trial of each pair (-1: accepted); ur_out (nullable) [i][t].
+__global__ void pair_decide_kernel(const IvPair* __restrict__ pairs, uint32_t npairs,
+                                   const uint64_t* __restrict__ ur_part, const uint64_t* __restrict__ zv,
+                                   uint32_t trials, int32_t* __restrict__ pfail, uint64_t* __restrict__ ur_out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npairs) return;
+    const IvPair pr = pairs[i];
+    int32_t f = -1;
+    for (uint32_t t = 0; t < trials; ++t) {
+        uint64_t acc = 0;
+        for (uint32_t c = pr.ch0; c < pr.ch0 + pr.nch; ++c) acc = add_mod(acc, ur_part[(uint64_t)c * trials + t]);
+        if (ur_out) ur_out[(uint64_t)i * trials + t] = acc;
+        if (f < 0 && acc != zv[(uint64_t)i * trials + t]) {
+            f = (int32_t)t;
+            if (!ur_out) break;
+        }
+    }
+    pfail[i] = f;
+}
+
+// Query q: its first failing pair in probe order -> (list, trial), else (-1, -1).
+__global__ void query_decide_kernel(const IvPair* __restrict__ pairs, const uint32_t* __restrict__ q_pair0, uint32_t nq,
+                                    const int32_t* __restrict__ pfail, int32_t* __restrict__ fc,
+                                    int32_t* __restrict__ ft) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    int32_t c = -1, t = -1;
+    for (uint32_t i = q_pair0[q]; i < q_pair0[q + 1]; ++i)
+        if (pfail[i] >= 0) {
+            c = (int32_t)pairs[i].list;
+            t = pfail[i];
+            break;
+        }
+    fc[q] = c;
+    ft[q] = t;
+}
+
+unsigned grid_cap(uint64_t work, unsigned threads, unsigned cap) {
+    const uint64_t g = (work + threads - 1) / threads;
+    return (unsigned)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+int tmap_u8(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uint32_t box_rows, const char* what) {
+    cudaError_t e = make_tmap_u8(m, base, inner, rows, 128, box_rows);
+    if (e != cudaSuccess) return fail(BN_ECUDA, "tensor map of %s: %s", what, cudaGetErrorString(e));
+    return BN_OK;
+}
+
+}  // namespace
+
+// One IVF block run: the host plan (pairs, groups, item tables, Protocol 2
+// layout), the workspace layout and the tensor maps of the gathered operands.
+struct IvfBlockJob {
+    uint32_t B = 0, trials = 0, k = 0;
+    bool verify_only = false;
+    uint32_t P = 0, U = 0, NB = 0, NP = 0, NCH = 0, n_pl = 0, n_s8 = 0;
+    uint64_t R = 0, max_q_rows = 0;
+    uint32_t w_tile = 64, n_rows = 0, ctas = 1, st_g1 = 0, st_g2 = 0, st_g3 = 0;
+    // inputs (one H2D from the staging buffer)
+    uint64_t o_v, o_g, o_t, o_tn, o_seed, o_qoff, o_qp0, o_pairs, o_lmq, o_lmi, o_base, o_items_pl, o_items_s8, o_vsegs,
+        o_blocks, o_panels, o_lp0, o_chunks, in_end;
+    // outputs (one D2H)
+    uint64_t o_ids, o_sc, o_n, o_fc, o_ft, o_err, out_end;
+    // scratch
+    uint64_t o_vp, o_gx, o_tv, o_x, o_wv, o_wgx, o_wtv, o_r, o_f2, o_f3, o_idmap, o_ub, o_zpart, o_z, o_urpart, o_zv,
+        o_pfail, o_urout, o_cs, o_ci, o_cn, total;
+    CUtensorMap tm_wv, tm_wgx, tm_wtv, tm_u;
+    std::vector<char> meta;  // host image of [o_qoff, in_end)
+};
+
+void ivf_block_job_free(IvfBlockJob* j) { delete j; }
+IvfBlockJob* ivf_block_job_new() { return new IvfBlockJob(); }
+uint64_t ivf_block_job_bytes(const IvfBlockJob* j) { return j->total; }
+
+namespace {
+
+// W tile (MMA N) for the batch's groups: a group of n pairs spans 8n W rows;
+// each A tile is re-streamed (from L2) once per W tile of its group, so pick
+// the tile minimising sum over groups of A tiles x W tiles x (A + W rows +
+// a fixed per-item cost).
+uint32_t pick_w_tile(const std::vector<uint32_t>& n_pairs, const std::vector<uint64_t>& rows) {
+    uint32_t best_w = 64;
+    double best = 1e300;
+    for (uint32_t w : {16u, 32u, 64u, 128u, 256u}) {
+        double cost = 0;
+        for (size_t u = 0; u < n_pairs.size(); ++u)
+            cost += (double)((rows[u] + 15) / 16) * (double)((8ull * n_pairs[u] + w - 1) / w) * (128.0 + w + 64.0);
+        if (cost < best) {
+            best = cost;
+            best_w = w;
+        }
+    }
+    return best_w;
+}
+
+}  // namespace
+
+// Host plan of one batch.  probe_off[B + 1] / probes: query q probes lists
+// probes[probe_off[q] .. probe_off[q + 1]) in that order.
+int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* probe_off, const uint32_t* probes,
+                   uint32_t trials, uint32_t k, bool verify_only, int sms) {
+    const Corpus& c = v.e.c;
+    if (k > BN_TOPK_MAX) return fail(BN_EINVAL, "k = %u exceeds BN_TOPK_MAX = %d", k, BN_TOPK_MAX);
+    if (trials > BN_MAX_TRIALS) return fail(BN_EINVAL, "trials = %u exceeds %d", trials, BN_MAX_TRIALS);
+    if (B > 65535) return fail(BN_EINVAL, "B = %u exceeds 65535 queries per call", B);
+    if (c.rows * 8 >= (1ull << 31)) return fail(BN_EUNSUPPORTED, "IVF block scoring needs fewer than 2^28 corpus rows");
+    if (probe_off[B] > (1u << 24)) return fail(BN_EINVAL, "%u probes exceed 2^24 per call", probe_off[B]);
+    j.B = B;
+    j.trials = trials;
+    j.k = k;
+    j.verify_only = verify_only;
+    // pairs, q-major; empty lists skipped (ivf.rs:787-789)
+    std::vector<IvPair> pairs;
+    std::vector<uint64_t> qoff(B + 1, 0);
+    std::vector<uint32_t> qp0(B + 1, 0);
+    uint64_t R = 0;
+    for (uint32_t q = 0; q < B; ++q) {
+        qoff[q] = R;
+        qp0[q] = (uint32_t)pairs.size();
+        for (uint32_t p = probe_off[q]; p < probe_off[q + 1]; ++p) {
+            const uint32_t ci = probes[p];
+            if (ci >= v.nlist)
+                return fail(BN_EINVAL, "probe %u of query %u names list %u of %u", p - probe_off[q], q, ci, v.nlist);
+            const uint64_t m = v.offsets[ci + 1] - v.offsets[ci];
+            if (!m) continue;
+            pairs.push_back(IvPair{R, q, ci, 0, 0, 0, 0});
+            R += m;
+        }
+        j.max_q_rows = std::max(j.max_q_rows, R - qoff[q]);
+    }
+    qoff[B] = R;
+    qp0[B] = (uint32_t)pairs.size();
+    j.R = R;
+    j.P = (uint32_t)pairs.size();
+    // groups: pairs sorted by list (stable: a list's queries stay in batch order)
+    std::vector<uint32_t> order(j.P);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return pairs[a].list < pairs[b].list; });
+    std::vector<uint32_t> g_lp0, g_n, g_list;
+    std::vector<uint64_t> g_rows, g_row0;
+    for (uint32_t lp = 0; lp < j.P; ++lp) {
+        IvPair& pr = pairs[order[lp]];
+        if (g_list.empty() || g_list.back() != pr.list) {
+            g_list.push_back(pr.list);
+            g_lp0.push_back(lp);
+            g_n.push_back(0);
+            g_row0.push_back(v.offsets[pr.list]);
+            g_rows.push_back(v.offsets[pr.list + 1] - v.offsets[pr.list]);
+        }
+        pr.u = (uint32_t)g_list.size() - 1;
+        ++g_n.back();
+    }
+    j.U = (uint32_t)g_list.size();
+    std::vector<uint32_t> lmq(j.P), lmi(j.P);
+    std::vector<uint64_t> base(j.P);
+    for (uint32_t lp = 0; lp < j.P; ++lp) {
+        const IvPair& pr = pairs[order[lp]];
+        lmq[lp] = pr.q;
+        lmi[lp] = order[lp];
+        base[lp] = pr.out0 - g_row0[pr.u];  // out[base + corpus row] (mod 2^64)
+    }
+    // grouped GEMM item tables
+    std::vector<BgItem> items_pl, items_s8;
+    if (!verify_only && j.P) {
+        j.w_tile = pick_w_tile(g_n, g_rows);
+        const uint32_t wy = j.w_tile / 8;  // pairs per W tile
+        for (uint32_t u = 0; u < j.U; ++u) {
+            const uint32_t row0 = (uint32_t)g_row0[u], m = (uint32_t)g_rows[u];
+            const uint32_t lp0 = g_lp0[u], n = g_n[u];
+            for (uint32_t y = 0; y < n; y += wy)
+                for (uint32_t x = 0; x < m; x += BG_AROWS / 8)
+                    items_pl.push_back(BgItem{8 * (row0 + x), 8 * (lp0 + y), row0 + x, row0 + m, lp0 + y, lp0 + n});
+            for (uint32_t y = 0; y < n; y += wy)
+                for (uint32_t x = 0; x < m; x += BG_AROWS)
+                    items_s8.push_back(BgItem{row0 + x, 8 * (lp0 + y), row0 + x, row0 + m, lp0 + y, lp0 + n});
+        }
+        BgParams p{};
+        p.w_tile = j.w_tile;
+        j.st_g1 = j.st_g2 = j.st_g3 = bgemm_max_stages(p);
+        if (!j.st_g1) return fail(BN_EUNSUPPORTED, "no pipeline depth fits W tile %u", j.w_tile);
+    }
+    j.n_pl = (uint32_t)items_pl.size();
+    j.n_s8 = (uint32_t)items_s8.size();
+    // Protocol 2 layout: one verify segment per distinct list (128-row U
+    // blocks, 4096-row z panels), chunks of <= 4096 rows per pair
+    std::vector<VerifySeg> vsegs;
+    std::vector<TcBlock> blocks;
+    std::vector<TcPanel> panels;
+    std::vector<uint32_t> lp0v(j.U + 1, 0), block0(j.U, 0);
+    for (uint32_t u = 0; u < j.U; ++u) {
+        const uint32_t m = (uint32_t)g_rows[u];
+        vsegs.push_back(VerifySeg{g_row0[u], 0, m, 0});
+        block0[u] = (uint32_t)blocks.size();
+        lp0v[u] = (uint32_t)panels.size();
+        for (uint32_t i0 = 0; i0 < m; i0 += TC_ROWS) blocks.push_back(TcBlock{u, i0});
+        for (uint32_t p0 = 0; p0 < m; p0 += TC_PANEL_ROWS)
+            panels.push_back(TcPanel{g_row0[u] + p0, std::min<uint32_t>(TC_PANEL_ROWS, m - p0), block0[u] + p0 / TC_ROWS,
+                                     u, 0});
+    }
+    lp0v[j.U] = (uint32_t)panels.size();
+    std::vector<IvChunk> chunks;
+    for (uint32_t lp = 0; lp < j.P; ++lp) {
+        IvPair& pr = pairs[order[lp]];
+        const uint32_t m = (uint32_t)g_rows[pr.u];
+        pr.ch0 = (uint32_t)chunks.size();
+        for (uint32_t c0 = 0; c0 < m; c0 += IV_CHUNK_ROWS)
+            chunks.push_back(IvChunk{pr.out0 + c0, g_row0[pr.u] + c0, block0[pr.u] + c0 / TC_ROWS,
+                                     std::min<uint32_t>(IV_CHUNK_ROWS, m - c0)});
+        pr.nch = (uint32_t)chunks.size() - pr.ch0;
+    }
+    j.NB = (uint32_t)blocks.size();
+    j.NP = (uint32_t)panels.size();
+    j.NCH = (uint32_t)chunks.size();
+    j.n_rows = pass_rows(std::min<uint32_t>(std::max<uint32_t>(trials, 1), TC_MAX_TRIALS));
+    j.ctas = (uint32_t)pick_ctas(j.max_q_rows, std::max<uint32_t>(B, 1), sms);
+
+    // workspace layout
+    const uint32_t n1 = c.n1, ks = std::max<uint32_t>(k, 1), tt = std::max<uint32_t>(trials, 1);
+    const uint64_t qb = verify_only ? 0 : B, pb = verify_only ? 0 : j.P;
+    Layout L;
+    j.o_v = L.take<uint64_t>((uint64_t)B * N);
+    j.o_g = L.take<uint64_t>(qb * n1);
+    j.o_t = L.take<uint32_t>(qb * N);
+    j.o_tn = L.take<uint32_t>(qb);
+    j.o_seed = L.take<uint8_t>(32);
+    j.o_qoff = L.take<uint64_t>(B + 1);
+    j.o_qp0 = L.take<uint32_t>(B + 1);
+    j.o_pairs = L.take<IvPair>(j.P);
+    j.o_lmq = L.take<uint32_t>(j.P);
+    j.o_lmi = L.take<uint32_t>(j.P);
+    j.o_base = L.take<uint64_t>(j.P);
+    j.o_items_pl = L.take<BgItem>(j.n_pl);
+    j.o_items_s8 = L.take<BgItem>(j.n_s8);
+    j.o_vsegs = L.take<VerifySeg>(j.U);
+    j.o_blocks = L.take<TcBlock>(j.NB);
+    j.o_panels = L.take<TcPanel>(j.NP);
+    j.o_lp0 = L.take<uint32_t>(j.U + 1);
+    j.o_chunks = L.take<IvChunk>(j.NCH);
+    j.in_end = L.take<uint8_t>(0);
+    j.o_ids = L.take<uint32_t>((uint64_t)B * ks);
+    j.o_sc = L.take<int64_t>((uint64_t)B * ks);
+    j.o_n = L.take<uint32_t>(B);
+    j.o_fc = L.take<int32_t>(B);
+    j.o_ft = L.take<int32_t>(B);
+    j.o_err = L.take<uint32_t>(2);  // [0] pipeline flags, [1] operand range flags
+    j.out_end = L.take<uint8_t>(0);
+    j.o_vp = L.take<uint8_t>(8 * qb * N);
+    j.o_gx = L.take<uint8_t>(8 * qb * c.k_alh);
+    j.o_tv = L.take<uint8_t>(8 * qb * 2 * N);
+    j.o_x = L.take<uint64_t>(qb * n1);
+    j.o_wv = L.take<uint8_t>(8 * pb * N);
+    j.o_wgx = L.take<uint8_t>(8 * pb * c.k_alh);
+    j.o_wtv = L.take<uint8_t>(8 * pb * 2 * N);
+    const uint64_t re = R + 2;  // paired loads of the top-k may touch one entry past the end
+    j.o_r = L.take<uint64_t>(re);
+    j.o_f2 = L.take<uint64_t>(verify_only ? 0 : re);
+    j.o_f3 = L.take<uint64_t>(verify_only ? 0 : re);
+    j.o_idmap = L.take<uint32_t>(verify_only ? 0 : re);
+    j.o_ub = L.take<uint8_t>(trials ? (uint64_t)j.NB * j.n_rows * TC_ROWS : 0);
+    j.o_zpart = L.take<uint64_t>(trials ? (uint64_t)j.NP * tt * N : 0);
+    j.o_z = L.take<uint64_t>(trials ? (uint64_t)j.U * tt * N : 0);
+    j.o_urpart = L.take<uint64_t>(trials ? (uint64_t)j.NCH * tt : 0);
+    j.o_zv = L.take<uint64_t>(trials ? (uint64_t)j.P * tt : 0);
+    j.o_pfail = L.take<int32_t>(j.P);
+    j.o_urout = L.take<uint64_t>(verify_only && trials ? (uint64_t)j.P * tt : 0);
+    const uint64_t cand = (uint64_t)B * j.ctas * ks;
+    j.o_cs = L.take<int64_t>(verify_only ? 0 : cand);
+    j.o_ci = L.take<uint32_t>(verify_only ? 0 : cand);
+    j.o_cn = L.take<uint32_t>(verify_only ? 0 : (uint64_t)B * j.ctas);
+    j.total = L.off + 1024;
+
+    // host image of the metadata
+    j.meta.assign(j.in_end - j.o_qoff, 0);
+    char* h = j.meta.data() - j.o_qoff;
+    auto put = [&](uint64_t off, const void* src, uint64_t bytes) {
+        if (bytes) memcpy(h + off, src, bytes);
+    };
+    put(j.o_qoff, qoff.data(), qoff.size() * 8);
+    put(j.o_qp0, qp0.data(), qp0.size() * 4);
+    put(j.o_pairs, pairs.data(), pairs.size() * sizeof(IvPair));
+    put(j.o_lmq, lmq.data(), lmq.size() * 4);
+    put(j.o_lmi, lmi.data(), lmi.size() * 4);
+    put(j.o_base, base.data(), base.size() * 8);
+    put(j.o_items_pl, items_pl.data(), items_pl.size() * sizeof(BgItem));
+    put(j.o_items_s8, items_s8.data(), items_s8.size() * sizeof(BgItem));
+    put(j.o_vsegs, vsegs.data(), vsegs.size() * sizeof(VerifySeg));
+    put(j.o_blocks, blocks.data(), blocks.size() * sizeof(TcBlock));
+    put(j.o_panels, panels.data(), panels.size() * sizeof(TcPanel));
+    put(j.o_lp0, lp0v.data(), lp0v.size() * 4);
+    put(j.o_chunks, chunks.data(), chunks.size() * sizeof(IvChunk));
+    return BN_OK;
+}
+
+// Validates and packs the query inputs into the pinned staging buffer (grown
+// as needed) and sizes ws (grown as needed, budget-accounted); encodes the
+// tensor maps of this run's buffers.
+int ivf_block_pack(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, const uint64_t* v_enc, const uint64_t* g,
+                   const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed) {
+    const Corpus& c = e.c;
+    const uint32_t B = j.B;
+    if (!v_enc) return fail(BN_EINVAL, "null v_enc");
+    if (j.trials && !seed) return fail(BN_EINVAL, "block_seed is required when trials > 0");
+    TRY(validate_residues(v_enc, (uint64_t)B * N, "v_enc"));
+    TRY(ws.reserve(e.ctx, j.total));
+    TRY(host.reserve(j.out_end));  // inputs, then the outputs read back at the same offsets
+    char* h = host.at<char>();
+    memcpy(h + j.o_v, v_enc, (uint64_t)B * N * 8);
+    if (!j.verify_only) {
+        if (!g || !t_nnz) return fail(BN_EINVAL, "null query input");
+        TRY(validate_residues(g, (uint64_t)B * c.n1, "g"));
+        memcpy(h + j.o_g, g, (uint64_t)B * c.n1 * 8);
+        uint32_t* ht = reinterpret_cast<uint32_t*>(h + j.o_t);
+        uint64_t tp = 0;
+        for (uint32_t q = 0; q < B; ++q) {
+            if (t_nnz[q] > N) return fail(BN_EINVAL, "t_nnz[%u] = %u exceeds n", q, t_nnz[q]);
+            if (t_nnz[q] && (!t_idx || !t_sign)) return fail(BN_EINVAL, "t_idx / t_sign are null");
+            for (uint32_t i = 0; i < t_nnz[q]; ++i, ++tp) {
+                if (t_idx[tp] >= N || (t_sign[tp] != 1 && t_sign[tp] != -1))
+                    return fail(BN_EINVAL, "T entry %llu is not (col < n, sign +-1)", (unsigned long long)tp);
+                ht[(uint64_t)q * N + i] = t_idx[tp] | (t_sign[tp] < 0 ? 0x80000000u : 0u);
+            }
+        }
+        memcpy(h + j.o_tn, t_nnz, (uint64_t)B * 4);
+    }
+    if (seed) memcpy(h + j.o_seed, seed, 32);
+    else memset(h + j.o_seed, 0, 32);
+    memcpy(h + j.o_qoff, j.meta.data(), j.meta.size());
+    char* d = ws.at<char>();
+    if (!j.verify_only && j.P) {
+        TRY(tmap_u8(&j.tm_wv, d + j.o_wv, N, 8ull * j.P, j.w_tile, "gathered v planes"));
+        TRY(tmap_u8(&j.tm_wgx, d + j.o_wgx, c.k_alh, 8ull * j.P, j.w_tile, "gathered [g | x] planes"));
+        TRY(tmap_u8(&j.tm_wtv, d + j.o_wtv, 2 * N, 8ull * j.P, j.w_tile, "gathered [T | v] bytes"));
+    }
+    if (j.trials && j.NB) TRY(tmap_u8(&j.tm_u, d + j.o_ub, TC_ROWS, (uint64_t)j.NB * j.n_rows, j.n_rows, "u images"));
+    return BN_OK;
+}
+
+// Enqueues the H2D of the packed inputs, the block pipeline and the D2H of
+// the outputs on s.  r_in (verification only): the claimed responses, device
+// copy already at o_r.
+int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cudaStream_t s) {
+    const Corpus& c = e.c;
+    char* d = ws.at<char>();
+    char* h = host.at<char>();
+    const int sms = e.ctx->num_sms;
+    const uint32_t B = j.B, n1 = c.n1;
+    CU(cudaSetDevice(e.ctx->device));
+    CU(cudaMemcpyAsync(d, h, j.in_end, cudaMemcpyHostToDevice, s));
+    uint32_t* err = reinterpret_cast<uint32_t*>(d + j.o_err);
+    CU(cudaMemsetAsync(err, 0, 8, s));
+    auto U8 = [&](uint64_t o) { return reinterpret_cast<uint8_t*>(d + o); };
+    auto U64 = [&](uint64_t o) { return reinterpret_cast<uint64_t*>(d + o); };
+    auto U32 = [&](uint64_t o) { return reinterpret_cast<uint32_t*>(d + o); };
+    const uint64_t* dv = U64(j.o_v);
+    const IvPair* dpairs = reinterpret_cast<const IvPair*>(d + j.o_pairs);
+    const IvChunk* dchunks = reinterpret_cast<const IvChunk*>(d + j.o_chunks);
+    if (!j.verify_only) {
+        if (j.P) {
+            // per-query operand images, then one image per (list, query) pair, grouped by list
+            if (c.k_alh != 2 * n1) CU(cudaMemsetAsync(d + j.o_gx, 0, 8ull * B * c.k_alh, s));
+            launch_planar_rows(dv, B, N, N, 0, U8(j.o_vp), N, 0, s);
+            launch_lt_times_v(c.L.at<uint64_t>(), n1, dv, B, U64(j.o_x), s);
+            launch_planar_rows(U64(j.o_g), B, n1, n1, 1, U8(j.o_gx), c.k_alh, 0, s);
+            launch_planar_rows(U64(j.o_x), B, n1, n1, 1, U8(j.o_gx), c.k_alh, n1, s);
+            launch_w_tv(dv, U32(j.o_t), U32(j.o_tn), B, reinterpret_cast<int8_t*>(d + j.o_tv), err + 1, s);
+            const uint32_t* lmq = U32(j.o_lmq);
+            struct Img {
+                uint64_t src, dst;
+                uint32_t row_bytes;
+            };
+            const Img imgs[3] = {{j.o_vp, j.o_wv, N}, {j.o_gx, j.o_wgx, c.k_alh}, {j.o_tv, j.o_wtv, 2 * N}};
+            for (const Img& im : imgs)
+                gather8_kernel<<<grid_cap((uint64_t)j.P * im.row_bytes / 2, 256, (unsigned)sms * 8), 256, 0, s>>>(
+                    reinterpret_cast<const uint4*>(d + im.src), reinterpret_cast<uint4*>(d + im.dst), lmq, j.P,
+                    im.row_bytes);
+            idmap_kernel<<<j.NCH, 256, 0, s>>>(dchunks, c.ids.at<uint32_t>(), U32(j.o_idmap));
+            // G1 r = M_c v_q, G2 f2 = -(AL_c g_q + H_c x_q), G3 f3 = M_c T_q + S_c v_q
+            BgParams p{};
+            p.mode = BG_PLANAR;
+            p.a_tiles = p.w_tiles = 1;
+            p.w_tile = j.w_tile;
+            p.k_bytes = p.k_panel = N;
+            p.out = U64(j.o_r);
+            p.item_tab = reinterpret_cast<const BgItem*>(d + j.o_items_pl);
+            p.n_items = j.n_pl;
+            p.pair_base = U64(j.o_base);
+            launch_bgemm(c.tmap_mp, j.tm_wv, p, j.st_g1, sms, err, s);
+            p.k_bytes = p.k_panel = c.k_alh;
+            p.out = U64(j.o_f2);
+            launch_bgemm(c.tmap_alh, j.tm_wgx, p, j.st_g2, sms, err, s);
+            p.mode = BG_S8;
+            p.k_bytes = p.k_panel = 2 * N;
+            p.out = U64(j.o_f3);
+            p.corr = c.corr.at<uint64_t>();
+            p.item_tab = reinterpret_cast<const BgItem*>(d + j.o_items_s8);
+            p.n_items = j.n_s8;
+            launch_bgemm(c.tmap_ms, j.tm_wtv, p, j.st_g3, sms, err, s);
+        }
+        if (j.k && j.P) {
+            TopkScratch ts{reinterpret_cast<int64_t*>(d + j.o_cs), U32(j.o_ci), U32(j.o_cn)};
+            launch_topk_segs(U64(j.o_r), U64(j.o_f2), U64(j.o_f3), U64(j.o_qoff), B, U32(j.o_idmap), j.k, (int)j.ctas,
+                             ts, U32(j.o_ids), reinterpret_cast<int64_t*>(d + j.o_sc), U32(j.o_n), s);
+        } else {
+            CU(cudaMemsetAsync(d + j.o_n, 0, (uint64_t)B * 4, s));
+        }
+    }
+    if (j.trials && j.P) {
+        const auto* vsegs = reinterpret_cast<const VerifySeg*>(d + j.o_vsegs);
+        const auto* blocks = reinterpret_cast<const TcBlock*>(d + j.o_blocks);
+        const auto* panels = reinterpret_cast<const TcPanel*>(d + j.o_panels);
+        const auto* key = reinterpret_cast<const ChaChaKey*>(d + j.o_seed);
+        for (uint32_t t0 = 0; t0 < j.trials; t0 += TC_MAX_TRIALS) {
+            const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, j.trials - t0);
+            launch_tc_ugen(vsegs, blocks, j.NB, key, nullptr, t0, tc, j.n_rows, U8(j.o_ub), nullptr, j.trials, err, s);
+            launch_tc_freivalds(c.tmap_m, j.tm_u, panels, j.NP, t0, tc, j.n_rows, j.trials, U64(j.o_zpart), err, sms, s);
+            ur_chunks_kernel<<<j.NCH, 128, 0, s>>>(dchunks, U8(j.o_ub), j.n_rows, t0, tc, j.trials, U64(j.o_r),
+                                                  U64(j.o_urpart));
+        }
+        zsum_lists_kernel<<<j.U * j.trials, 256, 0, s>>>(U64(j.o_zpart), U32(j.o_lp0), j.trials, U64(j.o_z));
+        zv_pairs_kernel<<<dim3(j.P, j.trials), 128, 0, s>>>(U64(j.o_z), dv, dpairs, U32(j.o_lmi), j.trials, U64(j.o_zv));
+        pair_decide_kernel<<<(j.P + 127) / 128, 128, 0, s>>>(dpairs, j.P, U64(j.o_urpart), U64(j.o_zv), j.trials,
+                                                             reinterpret_cast<int32_t*>(d + j.o_pfail),
+                                                             j.verify_only ? U64(j.o_urout) : nullptr);
+        query_decide_kernel<<<(B + 127) / 128, 128, 0, s>>>(dpairs, U32(j.o_qp0), B,
+                                                            reinterpret_cast<const int32_t*>(d + j.o_pfail),
+                                                            reinterpret_cast<int32_t*>(d + j.o_fc),
+                                                            reinterpret_cast<int32_t*>(d + j.o_ft));
+    } else {
+        CU(cudaMemsetAsync(d + j.o_fc, 0xff, (uint64_t)B * 4, s));
+        CU(cudaMemsetAsync(d + j.o_ft, 0xff, (uint64_t)B * 4, s));
+    }
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(h + j.o_ids, d + j.o_ids, j.out_end - j.o_ids, cudaMemcpyDeviceToHost, s));
+    return BN_OK;
+}
+
+// After s has drained: flags, hits (k per query) and verdicts.
+int ivf_block_finish(const IvfBlockJob& j, const PinnedMem& host, uint32_t* ids, int64_t* scores, uint32_t* n_hits,
+                     int32_t* failed_cluster, int32_t* failed_trial) {
+    const char* h = host.at<char>();
+    const uint32_t* flags = reinterpret_cast<const uint32_t*>(h + j.o_err);
+    if (flags[0]) return fail(BN_ECUDA, "a device pipeline wait timed out or a draw hit p (flags 0x%x)", flags[0]);
+    if (flags[1]) return fail(BN_EINVAL, "a T column sum leaves [-128, 127]");
+    const uint32_t ks = std::max<uint32_t>(j.k, 1);
+    const uint32_t* hid = reinterpret_cast<const uint32_t*>(h + j.o_ids);
+    const int64_t* hsc = reinterpret_cast<const int64_t*>(h + j.o_sc);
+    const uint32_t* hn = reinterpret_cast<const uint32_t*>(h + j.o_n);
+    const int32_t* hfc = reinterpret_cast<const int32_t*>(h + j.o_fc);
+    const int32_t* hft = reinterpret_cast<const int32_t*>(h + j.o_ft);
+    for (uint32_t q = 0; q < j.B; ++q) {
+        const uint32_t nh = (j.k && !j.verify_only) ? hn[q] : 0;
+        if (n_hits) n_hits[q] = nh;
+        for (uint32_t i = 0; i < nh; ++i) {
+            if (ids) ids[(uint64_t)q * j.k + i] = hid[(uint64_t)q * ks + i];
+            if (scores) scores[(uint64_t)q * j.k + i] = hsc[(uint64_t)q * ks + i];
+        }
+        if (failed_cluster) failed_cluster[q] = hfc[q];
+        if (failed_trial) failed_trial[q] = hft[q];
+    }
+    return BN_OK;
+}
+
+int ivf_block_prepare(bn_ivf* v) {
+    std::lock_guard<std::mutex> g(v->e.mu);
+    return block_prepare_engine(v->e);
+}
+
+}  // namespace api
+}  // namespace bn
+
+using namespace bn::api;
+
+namespace {
+
+std::vector<uint32_t> fixed_probe_off(uint32_t B, uint32_t nprobe) {
+    std::vector<uint32_t> off(B + 1);
+    for (uint32_t q = 0; q <= B; ++q) off[q] = q * nprobe;
+    return off;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bn_ivf_block_prepare(bn_ivf* v) {
+    if (!v) return fail(BN_EINVAL, "null handle");
+    return ivf_block_prepare(v);
+}
+
+int bn_ivf_query_block(bn_ivf* v, uint32_t B, uint32_t nprobe, const uint32_t* probes, const uint64_t* v_enc,
+                       const uint64_t* g, const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz,
+                       const uint8_t* block_seed, uint32_t trials, uint32_t k, uint32_t* ids, int64_t* scores,
+                       uint32_t* n_hits, int32_t* failed_cluster, int32_t* failed_trial) {
+    if (!v) return fail(BN_EINVAL, "null handle");
+    if (B == 0) return BN_OK;
+    if (nprobe && !probes) return fail(BN_EINVAL, "null probes");
+    if ((uint64_t)B * nprobe > (1u << 24)) return fail(BN_EINVAL, "B * nprobe exceeds 2^24");
+    std::lock_guard<std::mutex> gd(v->e.mu);
+    Engine& e = v->e;
+    if (!e.c.client) return fail(BN_EUNSUPPORTED, "this handle has no client state (attach_client was not called)");
+    TRY(block_prepare_engine(e));
+    const std::vector<uint32_t> off = fixed_probe_off(B, nprobe);
+    IvfBlockJob j;
+    TRY(ivf_block_plan(*v, j, B, off.data(), probes, trials, k, false, e.ctx->num_sms));
+    TRY(ivf_block_pack(e, j, e.ws, e.host, v_enc, g, t_idx, t_sign, t_nnz, block_seed));
+    TRY(ivf_block_launch(e, j, e.ws, e.host, e.stream));
+    CU(cudaStreamSynchronize(e.stream));
+    return ivf_block_finish(j, e.host, ids, scores, n_hits, failed_cluster, failed_trial);
+}
+
+int bn_ivf_verify_block(bn_ivf* v, uint32_t B, uint32_t nprobe, const uint32_t* probes, const uint64_t* r,
+                        uint64_t r_len, const uint64_t* v_enc, const uint8_t* block_seed, uint32_t trials,
+                        int32_t* failed_cluster, int32_t* failed_trial, uint64_t* ur, uint64_t* zv) {
+    if (!v) return fail(BN_EINVAL, "null handle");
+    if (B == 0) return BN_OK;
+    if (!trials) return fail(BN_EINVAL, "trials must be at least 1");
+    if (nprobe && !probes) return fail(BN_EINVAL, "null probes");
+    if ((uint64_t)B * nprobe > (1u << 24)) return fail(BN_EINVAL, "B * nprobe exceeds 2^24");
+    std::lock_guard<std::mutex> gd(v->e.mu);
+    Engine& e = v->e;
+    const std::vector<uint32_t> off = fixed_probe_off(B, nprobe);
+    IvfBlockJob j;
+    TRY(ivf_block_plan(*v, j, B, off.data(), probes, trials, 0, true, e.ctx->num_sms));
+    if (r_len != j.R)
+        return fail(BN_EINVAL, "r holds %llu entries; the probed lists hold %llu rows", (unsigned long long)r_len,
+                    (unsigned long long)j.R);
+    if (j.R && !r) return fail(BN_EINVAL, "null r");
+    TRY(validate_residues(r, j.R, "r"));
+    TRY(ivf_block_pack(e, j, e.ws, e.host, v_enc, nullptr, nullptr, nullptr, nullptr, block_seed));
+    char* d = e.ws.at<char>();
+    cudaStream_t s = e.stream;
+    CU(cudaSetDevice(e.ctx->device));
+    if (j.R) CU(cudaMemcpyAsync(d + j.o_r, r, j.R * 8, cudaMemcpyHostToDevice, s));
+    TRY(ivf_block_launch(e, j, e.ws, e.host, s));
+    if (ur && j.P) CU(cudaMemcpyAsync(ur, d + j.o_urout, (uint64_t)j.P * trials * 8, cudaMemcpyDeviceToHost, s));
+    if (zv && j.P) CU(cudaMemcpyAsync(zv, d + j.o_zv, (uint64_t)j.P * trials * 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    return ivf_block_finish(j, e.host, nullptr, nullptr, nullptr, failed_cluster, failed_trial);
+}
+
+}  // extern "C"

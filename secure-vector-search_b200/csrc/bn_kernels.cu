@@ -722,22 +722,27 @@ topk_merge_kernel(const int64_t* __restrict__ cand_s, const uint32_t* __restrict
 // topk_merge_kernel.
 __global__ void __launch_bounds__(DT_THREADS)
 topk_rows_kernel(const uint64_t* __restrict__ ra, const uint64_t* __restrict__ rb, const uint64_t* __restrict__ rc,
-                 uint64_t ld, uint64_t rows, const uint32_t* __restrict__ ids, uint32_t k,
-                 int64_t* __restrict__ cand_s, uint32_t* __restrict__ cand_i, uint32_t* __restrict__ cand_n,
+                 uint64_t ld, uint64_t rows, const uint64_t* __restrict__ qoff, const uint32_t* __restrict__ ids,
+                 uint32_t k, int64_t* __restrict__ cand_s, uint32_t* __restrict__ cand_i, uint32_t* __restrict__ cand_n,
                  uint64_t* __restrict__ mv_out) {
     const uint32_t q = blockIdx.y;
     __shared__ TopkBuf buf;
     if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
     __syncthreads();
-    const uint64_t per = ((rows + gridDim.x - 1) / gridDim.x + 1) & ~1ull;
-    const uint64_t v_begin = min(rows, (uint64_t)blockIdx.x * per);
-    const uint64_t v_end = min(rows, v_begin + per);
-    const uint64_t base = (uint64_t)q * ld;
+    // rows of this query: [lo, hi) of row q (ld apart), or of the flat
+    // segmented array [qoff[q], qoff[q+1]) (lo rounded down to even so the
+    // paired loads stay 16-byte aligned; the extra entry is masked)
+    const uint64_t base = qoff ? 0 : (uint64_t)q * ld;
+    const uint64_t first = qoff ? qoff[q] : 0, hi = qoff ? qoff[q + 1] : rows;
+    const uint64_t lo = first & ~1ull, span = hi > lo ? hi - lo : 0;
+    const uint64_t per = ((span + gridDim.x - 1) / gridDim.x + 1) & ~1ull;
+    const uint64_t v_begin = lo + min(span, (uint64_t)blockIdx.x * per);
+    const uint64_t v_end = min(hi, v_begin + per);
     for (uint64_t tile = v_begin; tile < v_end; tile += 2 * DT_THREADS) {
         const uint64_t i0 = tile + 2 * threadIdx.x;
-        const bool valid[2] = {i0 < v_end, i0 + 1 < v_end};
+        const bool valid[2] = {i0 < v_end && i0 >= first, i0 + 1 < v_end};
         uint64_t mv[2] = {0, 0};
-        if (valid[0]) {  // v_begin, per and ld are even: the pair is 16-byte aligned and inside the row of ld
+        if (i0 < v_end) {  // v_begin, per and ld are even: the pair is 16-byte aligned and inside the row of ld
             const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(ra + base + i0);
             mv[0] = x.x;
             mv[1] = x.y;
@@ -752,7 +757,7 @@ topk_rows_kernel(const uint64_t* __restrict__ ra, const uint64_t* __restrict__ r
                 mv[1] = sub_mod(mv[1], z.y);
             }
             if (mv_out) {
-                mv_out[base + i0] = mv[0];
+                if (valid[0]) mv_out[base + i0] = mv[0];
                 if (valid[1]) mv_out[base + i0 + 1] = mv[1];
             }
         }
@@ -992,8 +997,20 @@ void launch_topk_rows(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
                       uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n, uint64_t* d_mv_out,
                       cudaStream_t s) {
     if (!nq) return;
-    topk_rows_kernel<<<dim3(ctas_per_query, nq), DT_THREADS, 0, s>>>(d_a, d_b, d_c, ld, rows, d_ids, k, scratch.cand_s,
-                                                                   scratch.cand_i, scratch.cand_n, d_mv_out);
+    topk_rows_kernel<<<dim3(ctas_per_query, nq), DT_THREADS, 0, s>>>(d_a, d_b, d_c, ld, rows, nullptr, d_ids, k,
+                                                                   scratch.cand_s, scratch.cand_i, scratch.cand_n,
+                                                                   d_mv_out);
+    topk_merge_kernel<<<nq, DT_THREADS, 0, s>>>(scratch.cand_s, scratch.cand_i, scratch.cand_n, ctas_per_query, k,
+                                                d_out_ids, d_out_scores, d_out_n);
+}
+
+void launch_topk_segs(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_c, const uint64_t* d_qoff,
+                      uint32_t nq, const uint32_t* d_ids, uint32_t k, int ctas_per_query, TopkScratch scratch,
+                      uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n, cudaStream_t s) {
+    if (!nq) return;
+    topk_rows_kernel<<<dim3(ctas_per_query, nq), DT_THREADS, 0, s>>>(d_a, d_b, d_c, 0, 0, d_qoff, d_ids, k,
+                                                                   scratch.cand_s, scratch.cand_i, scratch.cand_n,
+                                                                   nullptr);
     topk_merge_kernel<<<nq, DT_THREADS, 0, s>>>(scratch.cand_s, scratch.cand_i, scratch.cand_n, ctas_per_query, k,
                                                 d_out_ids, d_out_scores, d_out_n);
 }

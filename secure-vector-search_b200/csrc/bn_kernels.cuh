@@ -122,6 +122,12 @@ void launch_topk_rows(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
                       uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n, uint64_t* d_mv_out,
                       cudaStream_t s);
 
+// The same over a segmented array: query q's entries are [qoff[q],
+// qoff[q+1]) of a, b, c (each allocated to an even length), ids[i] per entry.
+void launch_topk_segs(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_c, const uint64_t* d_qoff,
+                      uint32_t nq, const uint32_t* d_ids, uint32_t k, int ctas_per_query, TopkScratch scratch,
+                      uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n, cudaStream_t s);
+
 // Keygen-side dense F_p GEMM: C[i][j] = sum_k A[i][k] * B[j][k]  (A: rows x K,
 // B: cols x K, both row-major), optionally C += D (same shape, row-major).
 // K must be a multiple of 16 and at most 1024.

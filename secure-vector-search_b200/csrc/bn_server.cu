@@ -69,8 +69,12 @@ struct Slot {
     BlockPlan* bp = nullptr;
     uint32_t bp_B = 0;
     bool block_run = false;
+    // block scoring of IVF batches (pairs grouped by list), in ws / host
+    IvfBlockJob* ivj = nullptr;
+    bool ivf_block_run = false;
     ~Slot() {
         if (bp) block_plan_free(bp);
+        if (ivj) ivf_block_job_free(ivj);
     }
 };
 
@@ -90,7 +94,8 @@ struct bn_server {
     std::thread sched;
     // statistics
     uint64_t submitted = 0, completed = 0, batches = 0, batched_queries = 0, block_batches = 0, peak_mem = 0;
-    bool block_off = false;  // block scoring refused by the corpus: per-query path only
+    bool block_off = false;      // block scoring refused by the flat corpus: per-query path only
+    bool ivf_block_off = false;  // the same for the IVF corpus
     std::vector<double> lat_us;
     Clock::time_point t_first{}, t_last{};
 };
@@ -130,12 +135,33 @@ void batch_meta(bn_server* s, int kind, It first, It last, HostMeta& hm) {
 
 uint32_t block_bucket(bn_server* s, size_t count);
 
+// IVF batches of at least block_min requests run as IVF block scoring.
+bool ivf_block(const bn_server* s, size_t count) {
+    return s->cfg.block_min && count >= s->cfg.block_min && !s->ivf_block_off;
+}
+
+// Host plan of an IVF block over requests [first, first + count).
+template <class It>
+int ivf_block_plan_reqs(bn_server* s, It first, size_t count, IvfBlockJob& j) {
+    std::vector<uint32_t> off(count + 1, 0), probes;
+    for (size_t b = 0; b < count; ++b) {
+        probes.insert(probes.end(), first[b].probes.begin(), first[b].probes.end());
+        off[b + 1] = (uint32_t)probes.size();
+    }
+    return ivf_block_plan(*s->ivf, j, (uint32_t)count, off.data(), probes.data(), s->cfg.trials, s->cfg.k, false,
+                          s->ivf->e.ctx->num_sms);
+}
+
 // Device workspace of a batch made of the first `count` requests of q (a
 // block plan's workspace when the batch runs as a block).
 uint64_t batch_bytes(bn_server* s, int kind, const std::deque<Request>& q, size_t count) {
     if (kind == BN_SERVER_FLAT)
         if (const uint32_t bucket = block_bucket(s, count))
             return block_plan_estimate(s->flat, bucket, s->cfg.trials, s->cfg.k);
+    if (kind == BN_SERVER_IVF && ivf_block(s, count)) {
+        std::unique_ptr<IvfBlockJob, void (*)(IvfBlockJob*)> j(ivf_block_job_new(), ivf_block_job_free);
+        if (ivf_block_plan_reqs(s, q.begin(), count, *j) == BN_OK) return ivf_block_job_bytes(j.get());
+    }
     HostMeta hm;
     batch_meta(s, kind, q.begin(), q.begin() + count, hm);
     const Sizes z = sizes_for(engine_of(s, kind), hm, (uint32_t)count, s->cfg.trials, s->cfg.k);
@@ -162,10 +188,12 @@ void harvest(bn_server* s, Slot& sl) {
     std::vector<int32_t> vf;
     std::vector<Result> res(B);
     int rc = cudaEventSynchronize(sl.done) == cudaSuccess ? BN_OK : fail(BN_ECUDA, "batch failed on the device");
-    std::vector<int32_t> bf(B, -1);
+    std::vector<int32_t> bf(B, -1), bc(B, -1);
     if (rc == BN_OK)
-        rc = sl.block_run ? block_query_finish(*sl.bp, B, ids.data(), sc.data(), nh.data(), bf.data())
-                          : job_finish(sl.job, sl.host, ids.data(), sc.data(), nh.data(), vf);
+        rc = sl.block_run       ? block_query_finish(*sl.bp, B, ids.data(), sc.data(), nh.data(), bf.data())
+             : sl.ivf_block_run ? ivf_block_finish(*sl.ivj, sl.host, ids.data(), sc.data(), nh.data(), bc.data(),
+                                                   bf.data())
+                                : job_finish(sl.job, sl.host, ids.data(), sc.data(), nh.data(), vf);
     for (uint32_t b = 0; b < B; ++b) {
         Result& r = res[b];
         r.status = rc;
@@ -175,8 +203,9 @@ void harvest(bn_server* s, Slot& sl) {
         }
         r.ids.assign(ids.begin() + (uint64_t)b * k, ids.begin() + (uint64_t)b * k + nh[b]);
         r.scores.assign(sc.begin() + (uint64_t)b * k, sc.begin() + (uint64_t)b * k + nh[b]);
-        if (sl.block_run) {
+        if (sl.block_run || sl.ivf_block_run) {
             r.failed_trial = bf[b];
+            r.failed_cluster = bc[b];
             continue;
         }
         const DecodeQuery& dq = sl.hm.dq[b];
@@ -216,6 +245,23 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
     int rc = BN_OK;
     const uint32_t bucket = kind == BN_SERVER_FLAT ? block_bucket(s, B) : 0;
     sl.block_run = false;
+    sl.ivf_block_run = false;
+    if (kind == BN_SERVER_IVF && ivf_block(s, B)) {
+        // IVF block scoring: the batch's (query, list) pairs grouped by list,
+        // every probed list read once; Protocol 2 per block and list with the
+        // first request's seed
+        if (!sl.ivj) sl.ivj = ivf_block_job_new();
+        Engine& e = s->ivf->e;
+        rc = ivf_block_plan_reqs(s, sl.reqs.begin(), B, *sl.ivj);
+        if (rc == BN_OK)
+            rc = ivf_block_pack(e, *sl.ivj, sl.ws, sl.host, v.data(), g.data(), ti.empty() ? nullptr : ti.data(),
+                                ts.empty() ? nullptr : ts.data(), tn.data(), seeds.data());
+        if (rc == BN_OK) rc = ivf_block_launch(e, *sl.ivj, sl.ws, sl.host, sl.stream);
+        if (rc == BN_OK) {
+            sl.ivf_block_run = true;
+            s->block_batches += 1;
+        }
+    }
     if (bucket) {
         // block scoring: the batch's queries share one pass over the corpus;
         // Protocol 2 runs per block with the first request's seed
@@ -237,7 +283,7 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
             rc = BN_OK;
         }
     }
-    if (!sl.block_run && rc == BN_OK) {
+    if (!sl.block_run && !sl.ivf_block_run && rc == BN_OK) {
         sl.job = QueryJob();
         sl.job.hm = &sl.hm;
         sl.job.B = B;
@@ -431,7 +477,6 @@ int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn
     if (!cfg->slots || cfg->slots > 16) return fail(BN_EINVAL, "slots must be in 1..=16");
     if (cfg->k > BN_TOPK_MAX) return fail(BN_EINVAL, "k = %u exceeds BN_TOPK_MAX", cfg->k);
     if (cfg->trials > BN_MAX_TRIALS) return fail(BN_EINVAL, "trials = %u exceeds %d", cfg->trials, BN_MAX_TRIALS);
-    if (cfg->block_min && !flat) return fail(BN_EINVAL, "block_min needs a flat corpus");
     auto* s = new bn_server();
     s->flat = flat;
     s->ivf = ivf;
@@ -453,6 +498,13 @@ int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn
             return fail(BN_ECUDA, "stream / event creation failed");
         }
         sl->ws.ctx = ctx;
+    }
+    if (cfg->block_min) {
+        // byte-planar corpus copies of block scoring, built now rather than
+        // inside the first block batch; a corpus that cannot take them
+        // (plaintext outside int8) is served per query
+        if (flat && block_prepare(flat) == BN_EUNSUPPORTED) s->block_off = true;
+        if (ivf && ivf_block_prepare(ivf) == BN_EUNSUPPORTED) s->ivf_block_off = true;
     }
     s->sched = std::thread(scheduler, s);
     *out = s;

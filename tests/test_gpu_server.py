@@ -223,3 +223,21 @@ def test_concurrent_block_and_per_query_batches(big_flat):
     srv.close()
     assert bad == 0
     assert st["block_batches"] > 0 and st["batches"] > st["block_batches"]  # both paths were exercised
+
+
+def test_ivf_block_batches_match_per_query(corpora):
+    """IVF batches of >= block_min requests (mixed nprobe) run as IVF block
+    scoring (pairs grouped by list, every probed list read once): hits
+    identical to the per-query path, honest responses accepted."""
+    c = capi()
+    flat, L, ivf, case = corpora
+    reqs = [r for r in requests(L, case, 48, 7700) if r[0] == "ivf"]
+    want = [direct(flat, ivf, r) for r in reqs]
+    srv = c.Server(flat, ivf, max_batch=16, slots=2, max_wait_us=20000, trials=TRIALS, k=K, block_min=4)
+    tickets = [submit(srv, r) for r in reqs]
+    got = [srv.wait(t)[:4] for t in tickets]
+    for g, w in zip(got, want):
+        assert np.array_equal(g[0], w[0]) and np.array_equal(g[1], w[1]) and g[2] == -1 and g[3] == -1
+    st = srv.stats()
+    assert st["block_batches"] > 0 and st["completed"] == len(reqs)
+    srv.close()
