@@ -545,8 +545,12 @@ def run_ivf(args, ctx, dist):
             ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
             t.append(time.perf_counter() - ta)
         db = statistics.median(t)
+        ivf.block_profile(True)  # one more call with stage events (not part of the timing above)
+        ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
+        stages = ivf.block_profile_read()
+        ivf.block_profile(False)
         res["block"] = {"qps": bq / db, "ms_per_batch": db * 1e3, "hits_equal_per_query": bool(same),
-                        "distinct_rows_gbs": rows_u * N_DIM * 8 / db / 1e9}
+                        "distinct_rows_gbs": rows_u * N_DIM * 8 / db / 1e9, "stages_ms": stages}
         out["per_nprobe"][str(nprobe)] = res
     return out, ivf, data
 

@@ -271,6 +271,12 @@ int bn_ivf_query_block(bn_ivf* h, uint32_t B, uint32_t nprobe, const uint32_t* p
                        const uint64_t* g, const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz,
                        const uint8_t block_seed[32], uint32_t trials, uint32_t k, uint32_t* ids, int64_t* scores,
                        uint32_t* n_hits, int32_t* failed_cluster, int32_t* failed_trial);
+/* Stage timing of later bn_ivf_query_block calls (enable = 1) and its read:
+ * ms[0] = host planning and packing, ms[1..8] = device time of the stages
+ * (H2D + operand images, G1, G2, G3, top-k, Protocol 2 passes, z . v and
+ * verdicts, D2H) of the last call; *n = 0 before the first profiled call. */
+int bn_ivf_block_profile(bn_ivf* h, int enable);
+int bn_ivf_block_profile_read(bn_ivf* h, float* ms, uint32_t cap, uint32_t* n);
 /* Protocol 2 of the block form over claimed responses: r holds every
  * (query, list) pair's m_c responses, pairs in probe order (query-major,
  * empty lists skipped), r_len entries in all.  ur / zv (nullable, pairs x

@@ -96,6 +96,8 @@ _SIGS = {
     "bn_ivf_query": (C.c_int, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
     "bn_ivf_block_prepare": (C.c_int, [vp]),
     "bn_ivf_query_block": (C.c_int, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
+    "bn_ivf_block_profile": (C.c_int, [vp, C.c_int]),
+    "bn_ivf_block_profile_read": (C.c_int, [vp, vp, u32, vp]),
     "bn_ivf_verify_block": (C.c_int, [vp, u32, u32, vp, vp, u64, vp, vp, u32, vp, vp, vp, vp]),
     "bn_encrypt_cluster": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, vp, vp]),
     "bn_server_create": (C.c_int, [vp, vp, C.POINTER(ServerConfig), vp]),
@@ -465,6 +467,19 @@ class Ivf:
                                      ptr(nh), ptr(fc), ptr(ft)))
         hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
         return hits, fc, ft
+
+    IVF_BLOCK_STAGES = ("host_plan_pack", "h2d_operand_images", "g1_r", "g2_al_h", "g3_m_t_s_v", "topk",
+                        "protocol2_passes", "zv_decide", "d2h")
+
+    def block_profile(self, enable=True):
+        check(lib.bn_ivf_block_profile(self.h, 1 if enable else 0))
+
+    def block_profile_read(self):
+        """Stage times (ms) of the last profiled query_block, by stage name."""
+        ms = np.zeros(len(self.IVF_BLOCK_STAGES), np.float32)
+        n = u32(0)
+        check(lib.bn_ivf_block_profile_read(self.h, ptr(ms), len(ms), C.byref(n)))
+        return {k: float(v) for k, v in zip(self.IVF_BLOCK_STAGES, ms[: n.value])}
 
     def pairs(self, probes):
         """(query, list, rows) of every (query, list) pair of a batch in probe order, empty lists skipped:

@@ -285,7 +285,10 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
                    uint32_t trials, uint32_t k, bool verify_only, int sms);
 int ivf_block_pack(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, const uint64_t* v_enc, const uint64_t* g,
                    const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed);
-int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cudaStream_t s);
+// ev (nullable): 9 events recorded on s at the stage boundaries (start; operand
+// images; G1; G2; G3; top-k; Protocol 2 passes; z . v and verdicts; D2H).
+int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cudaStream_t s,
+                     cudaEvent_t* ev = nullptr);
 int ivf_block_finish(const IvfBlockJob& j, const PinnedMem& host, uint32_t* ids, int64_t* scores, uint32_t* n_hits,
                      int32_t* failed_cluster, int32_t* failed_trial);
 int ivf_block_prepare(bn_ivf* v);
@@ -310,6 +313,15 @@ struct bn_ivf {
     bn::api::Engine e;
     uint32_t nlist = 0;
     std::vector<uint64_t> offsets;
+    // stage timing of the host-buffer IVF block entry point (bn_ivf_block_profile)
+    static constexpr int PROF_EVENTS = 9;
+    bool prof = false, prof_have = false;
+    cudaEvent_t prof_ev[PROF_EVENTS] = {};
+    float prof_host_ms = 0.f;
+    ~bn_ivf() {
+        for (cudaEvent_t ev : prof_ev)
+            if (ev) cudaEventDestroy(ev);
+    }
 };
 
 

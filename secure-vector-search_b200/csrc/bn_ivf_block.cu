@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <numeric>
 
@@ -145,27 +146,35 @@ ur_chunks_kernel(const IvChunk* __restrict__ chunks, const uint8_t* __restrict__
     }
 }
 
-// z[u][t][j] = sum of z_part[p][t][j] over list u's panels
-__global__ void zsum_lists_kernel(const uint64_t* __restrict__ z_part, const uint32_t* __restrict__ list_panel0,
+// A list of several z panels: z[m][t][j] = sum of its panels' z_part[p][t][j].
+struct IvZsum {
+    uint32_t p0, p1;  // panels
+    uint32_t m;       // slot in z
+};
+
+__global__ void zsum_lists_kernel(const uint64_t* __restrict__ z_part, const IvZsum* __restrict__ lists,
                                   uint32_t trials, uint64_t* __restrict__ z) {
-    const uint32_t u = blockIdx.x / trials, t = blockIdx.x % trials;
-    const uint32_t p0 = list_panel0[u], p1 = list_panel0[u + 1];
+    const IvZsum l = lists[blockIdx.x / trials];
+    const uint32_t t = blockIdx.x % trials;
     for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
         uint64_t acc = 0;
-        for (uint32_t p = p0; p < p1; ++p) acc = add_mod(acc, z_part[((uint64_t)p * trials + t) * N + j]);
-        z[((uint64_t)u * trials + t) * N + j] = acc;
+        for (uint32_t p = l.p0; p < l.p1; ++p) acc = add_mod(acc, z_part[((uint64_t)p * trials + t) * N + j]);
+        z[((uint64_t)l.m * trials + t) * N + j] = acc;
     }
 }
 
-// zv[i][t] = z_t^{list(i)} . v_{q(i)}; blocks visit the pairs list by list
-// (lm_pair) so that a list's z stays in L2 across its queries
-__global__ void __launch_bounds__(128) zv_pairs_kernel(const uint64_t* __restrict__ z, const uint64_t* __restrict__ v,
+// zv[i][t] = z_t^{list(i)} . v_{q(i)}, list u's z at zbase + zoff[u] (its
+// single panel's z_part, or its panel sum); blocks visit the pairs list by
+// list (lm_pair) so that a list's z stays in L2 across its queries
+__global__ void __launch_bounds__(128) zv_pairs_kernel(const uint64_t* __restrict__ zbase,
+                                                       const uint64_t* __restrict__ zoff,
+                                                       const uint64_t* __restrict__ v,
                                                        const IvPair* __restrict__ pairs,
                                                        const uint32_t* __restrict__ lm_pair, uint32_t trials,
                                                        uint64_t* __restrict__ zv) {
     const uint32_t i = lm_pair[blockIdx.x], t = blockIdx.y;
     const IvPair pr = pairs[i];
-    const uint64_t* zr = z + ((uint64_t)pr.u * trials + t) * N;
+    const uint64_t* zr = zbase + zoff[pr.u] + (uint64_t)t * N;
     const uint64_t* vr = v + (uint64_t)pr.q * N;
     uint64_t lo = 0, hi = 0;
     for (uint32_t j = threadIdx.x; j < N; j += 128) mac128(lo, hi, zr[j], vr[j]);  // 8 products per thread
@@ -233,12 +242,12 @@ int tmap_u8(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uin
 struct IvfBlockJob {
     uint32_t B = 0, trials = 0, k = 0;
     bool verify_only = false;
-    uint32_t P = 0, U = 0, NB = 0, NP = 0, NCH = 0, n_pl = 0, n_s8 = 0;
+    uint32_t P = 0, U = 0, NB = 0, NP = 0, NCH = 0, n_pl = 0, n_s8 = 0, NZ = 0;
     uint64_t R = 0, max_q_rows = 0;
     uint32_t w_tile = 64, n_rows = 0, ctas = 1, st_g1 = 0, st_g2 = 0, st_g3 = 0;
     // inputs (one H2D from the staging buffer)
     uint64_t o_v, o_g, o_t, o_tn, o_seed, o_qoff, o_qp0, o_pairs, o_lmq, o_lmi, o_base, o_items_pl, o_items_s8, o_vsegs,
-        o_blocks, o_panels, o_lp0, o_chunks, in_end;
+        o_blocks, o_panels, o_zoff, o_zsum, o_chunks, in_end;
     // outputs (one D2H)
     uint64_t o_ids, o_sc, o_n, o_fc, o_ft, o_err, out_end;
     // scratch
@@ -367,6 +376,8 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     std::vector<TcBlock> blocks;
     std::vector<TcPanel> panels;
     std::vector<uint32_t> lp0v(j.U + 1, 0), block0(j.U, 0);
+    std::vector<uint64_t> zoff(j.U, 0);  // element offsets from z_part: a single panel's, or z's slot
+    std::vector<IvZsum> zsum;
     for (uint32_t u = 0; u < j.U; ++u) {
         const uint32_t m = (uint32_t)g_rows[u];
         vsegs.push_back(VerifySeg{g_row0[u], 0, m, 0});
@@ -378,6 +389,17 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
                                      u, 0});
     }
     lp0v[j.U] = (uint32_t)panels.size();
+    const uint64_t tt0 = std::max<uint32_t>(trials, 1);
+    const uint64_t z_from_zpart = (uint64_t)panels.size() * tt0 * N;  // z follows z_part in the workspace
+    for (uint32_t u = 0; u < j.U; ++u) {
+        if (lp0v[u + 1] - lp0v[u] == 1) {
+            zoff[u] = (uint64_t)lp0v[u] * tt0 * N;
+        } else {
+            zoff[u] = z_from_zpart + (uint64_t)zsum.size() * tt0 * N;
+            zsum.push_back(IvZsum{lp0v[u], lp0v[u + 1], (uint32_t)zsum.size()});
+        }
+    }
+    j.NZ = (uint32_t)zsum.size();
     std::vector<IvChunk> chunks;
     for (uint32_t lp = 0; lp < j.P; ++lp) {
         IvPair& pr = pairs[order[lp]];
@@ -414,7 +436,8 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.o_vsegs = L.take<VerifySeg>(j.U);
     j.o_blocks = L.take<TcBlock>(j.NB);
     j.o_panels = L.take<TcPanel>(j.NP);
-    j.o_lp0 = L.take<uint32_t>(j.U + 1);
+    j.o_zoff = L.take<uint64_t>(j.U);
+    j.o_zsum = L.take<IvZsum>(j.NZ);
     j.o_chunks = L.take<IvChunk>(j.NCH);
     j.in_end = L.take<uint8_t>(0);
     j.o_ids = L.take<uint32_t>((uint64_t)B * ks);
@@ -437,8 +460,9 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.o_f3 = L.take<uint64_t>(verify_only ? 0 : re);
     j.o_idmap = L.take<uint32_t>(verify_only ? 0 : re);
     j.o_ub = L.take<uint8_t>(trials ? (uint64_t)j.NB * j.n_rows * TC_ROWS : 0);
-    j.o_zpart = L.take<uint64_t>(trials ? (uint64_t)j.NP * tt * N : 0);
-    j.o_z = L.take<uint64_t>(trials ? (uint64_t)j.U * tt * N : 0);
+    // z directly after z_part (zoff counts from z_part in elements)
+    j.o_zpart = L.take<uint64_t>(trials ? (uint64_t)j.NP * tt * N + (uint64_t)j.NZ * tt * N : 0);
+    j.o_z = j.o_zpart + (uint64_t)j.NP * tt * N * 8;
     j.o_urpart = L.take<uint64_t>(trials ? (uint64_t)j.NCH * tt : 0);
     j.o_zv = L.take<uint64_t>(trials ? (uint64_t)j.P * tt : 0);
     j.o_pfail = L.take<int32_t>(j.P);
@@ -466,7 +490,8 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     put(j.o_vsegs, vsegs.data(), vsegs.size() * sizeof(VerifySeg));
     put(j.o_blocks, blocks.data(), blocks.size() * sizeof(TcBlock));
     put(j.o_panels, panels.data(), panels.size() * sizeof(TcPanel));
-    put(j.o_lp0, lp0v.data(), lp0v.size() * 4);
+    put(j.o_zoff, zoff.data(), zoff.size() * 8);
+    put(j.o_zsum, zsum.data(), zsum.size() * sizeof(IvZsum));
     put(j.o_chunks, chunks.data(), chunks.size() * sizeof(IvChunk));
     return BN_OK;
 }
@@ -518,13 +543,20 @@ int ivf_block_pack(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, const
 // Enqueues the H2D of the packed inputs, the block pipeline and the D2H of
 // the outputs on s.  r_in (verification only): the claimed responses, device
 // copy already at o_r.
-int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cudaStream_t s) {
+int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cudaStream_t s, cudaEvent_t* ev) {
     const Corpus& c = e.c;
     char* d = ws.at<char>();
     char* h = host.at<char>();
     const int sms = e.ctx->num_sms;
     const uint32_t B = j.B, n1 = c.n1;
+    int last = -1;  // skipped stages are recorded with the next one (0 ms)
+    auto mark = [&](int i) {
+        if (ev)
+            for (int x = last + 1; x <= i; ++x) cudaEventRecord(ev[x], s);
+        last = i;
+    };
     CU(cudaSetDevice(e.ctx->device));
+    mark(0);
     CU(cudaMemcpyAsync(d, h, j.in_end, cudaMemcpyHostToDevice, s));
     uint32_t* err = reinterpret_cast<uint32_t*>(d + j.o_err);
     CU(cudaMemsetAsync(err, 0, 8, s));
@@ -554,6 +586,7 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
                     reinterpret_cast<const uint4*>(d + im.src), reinterpret_cast<uint4*>(d + im.dst), lmq, j.P,
                     im.row_bytes);
             idmap_kernel<<<j.NCH, 256, 0, s>>>(dchunks, c.ids.at<uint32_t>(), U32(j.o_idmap));
+            mark(1);
             // G1 r = M_c v_q, G2 f2 = -(AL_c g_q + H_c x_q), G3 f3 = M_c T_q + S_c v_q
             BgParams p{};
             p.mode = BG_PLANAR;
@@ -565,9 +598,11 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             p.n_items = j.n_pl;
             p.pair_base = U64(j.o_base);
             launch_bgemm(c.tmap_mp, j.tm_wv, p, j.st_g1, sms, err, s);
+            mark(2);
             p.k_bytes = p.k_panel = c.k_alh;
             p.out = U64(j.o_f2);
             launch_bgemm(c.tmap_alh, j.tm_wgx, p, j.st_g2, sms, err, s);
+            mark(3);
             p.mode = BG_S8;
             p.k_bytes = p.k_panel = 2 * N;
             p.out = U64(j.o_f3);
@@ -575,6 +610,7 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             p.item_tab = reinterpret_cast<const BgItem*>(d + j.o_items_s8);
             p.n_items = j.n_s8;
             launch_bgemm(c.tmap_ms, j.tm_wtv, p, j.st_g3, sms, err, s);
+            mark(4);
         }
         if (j.k && j.P) {
             TopkScratch ts{reinterpret_cast<int64_t*>(d + j.o_cs), U32(j.o_ci), U32(j.o_cn)};
@@ -583,6 +619,7 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
         } else {
             CU(cudaMemsetAsync(d + j.o_n, 0, (uint64_t)B * 4, s));
         }
+        mark(5);
     }
     if (j.trials && j.P) {
         const auto* vsegs = reinterpret_cast<const VerifySeg*>(d + j.o_vsegs);
@@ -596,8 +633,13 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             ur_chunks_kernel<<<j.NCH, 128, 0, s>>>(dchunks, U8(j.o_ub), j.n_rows, t0, tc, j.trials, U64(j.o_r),
                                                   U64(j.o_urpart));
         }
-        zsum_lists_kernel<<<j.U * j.trials, 256, 0, s>>>(U64(j.o_zpart), U32(j.o_lp0), j.trials, U64(j.o_z));
-        zv_pairs_kernel<<<dim3(j.P, j.trials), 128, 0, s>>>(U64(j.o_z), dv, dpairs, U32(j.o_lmi), j.trials, U64(j.o_zv));
+        mark(6);
+        if (j.NZ)
+            zsum_lists_kernel<<<j.NZ * j.trials, 256, 0, s>>>(U64(j.o_zpart),
+                                                              reinterpret_cast<const IvZsum*>(d + j.o_zsum), j.trials,
+                                                              U64(j.o_z));
+        zv_pairs_kernel<<<dim3(j.P, j.trials), 128, 0, s>>>(U64(j.o_zpart), U64(j.o_zoff), dv, dpairs, U32(j.o_lmi),
+                                                           j.trials, U64(j.o_zv));
         pair_decide_kernel<<<(j.P + 127) / 128, 128, 0, s>>>(dpairs, j.P, U64(j.o_urpart), U64(j.o_zv), j.trials,
                                                              reinterpret_cast<int32_t*>(d + j.o_pfail),
                                                              j.verify_only ? U64(j.o_urout) : nullptr);
@@ -609,8 +651,10 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
         CU(cudaMemsetAsync(d + j.o_fc, 0xff, (uint64_t)B * 4, s));
         CU(cudaMemsetAsync(d + j.o_ft, 0xff, (uint64_t)B * 4, s));
     }
+    mark(7);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(h + j.o_ids, d + j.o_ids, j.out_end - j.o_ids, cudaMemcpyDeviceToHost, s));
+    mark(8);
     return BN_OK;
 }
 
@@ -679,13 +723,49 @@ int bn_ivf_query_block(bn_ivf* v, uint32_t B, uint32_t nprobe, const uint32_t* p
     Engine& e = v->e;
     if (!e.c.client) return fail(BN_EUNSUPPORTED, "this handle has no client state (attach_client was not called)");
     TRY(block_prepare_engine(e));
+    const auto t0 = std::chrono::steady_clock::now();
     const std::vector<uint32_t> off = fixed_probe_off(B, nprobe);
     IvfBlockJob j;
     TRY(ivf_block_plan(*v, j, B, off.data(), probes, trials, k, false, e.ctx->num_sms));
     TRY(ivf_block_pack(e, j, e.ws, e.host, v_enc, g, t_idx, t_sign, t_nnz, block_seed));
-    TRY(ivf_block_launch(e, j, e.ws, e.host, e.stream));
+    v->prof_host_ms = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    v->prof_have = false;
+    TRY(ivf_block_launch(e, j, e.ws, e.host, e.stream, v->prof ? v->prof_ev : nullptr));
     CU(cudaStreamSynchronize(e.stream));
+    v->prof_have = v->prof;
     return ivf_block_finish(j, e.host, ids, scores, n_hits, failed_cluster, failed_trial);
+}
+
+int bn_ivf_block_profile(bn_ivf* v, int enable) {
+    if (!v) return fail(BN_EINVAL, "null handle");
+    std::lock_guard<std::mutex> gd(v->e.mu);
+    CU(cudaSetDevice(v->e.ctx->device));
+    if (enable)
+        for (cudaEvent_t& ev : v->prof_ev)
+            if (!ev) CU(cudaEventCreate(&ev));
+    v->prof = enable != 0;
+    v->prof_have = false;
+    return BN_OK;
+}
+
+int bn_ivf_block_profile_read(bn_ivf* v, float* ms, uint32_t cap, uint32_t* n) {
+    if (!v || !n) return fail(BN_EINVAL, "null argument");
+    std::lock_guard<std::mutex> gd(v->e.mu);
+    *n = 0;
+    if (!v->prof_have) return BN_OK;
+    const uint32_t total = bn_ivf::PROF_EVENTS;  // host plan + pack, then the 8 device stages
+    for (uint32_t i = 0; i < total && i < cap; ++i) {
+        if (i == 0) {
+            ms[0] = v->prof_host_ms;
+        } else {
+            float x = 0.f;
+            if (cudaEventElapsedTime(&x, v->prof_ev[i - 1], v->prof_ev[i]) != cudaSuccess) x = -1.f;
+            ms[i] = x;
+        }
+        *n = i + 1;
+    }
+    cudaGetLastError();  // an unrecorded stage (skipped work) reports -1, not a sticky error
+    return BN_OK;
 }
 
 int bn_ivf_verify_block(bn_ivf* v, uint32_t B, uint32_t nprobe, const uint32_t* probes, const uint64_t* r,
