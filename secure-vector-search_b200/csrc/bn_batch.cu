@@ -483,17 +483,25 @@ __global__ void w_tv_kernel(const uint64_t* __restrict__ v, uint32_t nq, int8_t*
     }
 }
 
-__global__ void w_t_kernel(const uint32_t* __restrict__ t_ent, const uint32_t* __restrict__ t_nnz, uint32_t nq,
-                           int8_t* __restrict__ dst, uint32_t* __restrict__ bad) {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nq) return;
-    int8_t* row = dst + (uint64_t)q * 8 * (2 * N);  // row (q, b = 0)
+// T part of row (q, b = 0): column sums of query q's +-1 entries, one CTA per
+// query (shared-memory counters, so repeated columns add up).
+__global__ void __launch_bounds__(256) w_t_kernel(const uint32_t* __restrict__ t_ent, const uint32_t* __restrict__ t_nnz,
+                                                  int8_t* __restrict__ dst, uint32_t* __restrict__ bad) {
+    const uint32_t q = blockIdx.x;
+    __shared__ int acc[N];
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) acc[i] = 0;
+    __syncthreads();
     const uint32_t tn = min(t_nnz[q], (uint32_t)N);
-    for (uint32_t c = 0; c < tn; ++c) {
+    for (uint32_t c = threadIdx.x; c < tn; c += blockDim.x) {
         const uint32_t e = t_ent[(uint64_t)q * N + c];
-        const int nv = (int)row[e & 0x3ffu] + ((e >> 31) ? -1 : 1);
-        if (nv < -128 || nv > 127) atomicOr(bad, 2u);
-        row[e & 0x3ffu] = (int8_t)nv;
+        atomicAdd(&acc[e & 0x3ffu], (e >> 31) ? -1 : 1);
+    }
+    __syncthreads();
+    int8_t* row = dst + (uint64_t)q * 8 * (2 * N);  // row (q, b = 0)
+    for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) {
+        const int v = acc[i];
+        if (v < -128 || v > 127) atomicOr(bad, 2u);
+        row[i] = (int8_t)v;
     }
 }
 
@@ -595,7 +603,7 @@ void launch_w_tv(const uint64_t* d_v, const uint32_t* d_t, const uint32_t* d_t_n
                  uint32_t* d_bad, cudaStream_t s) {
     if (!nq) return;
     w_tv_kernel<<<grid_for((uint64_t)nq * 8 * (N / 16), 256, 148 * 8), 256, 0, s>>>(d_v, nq, d_dst);
-    w_t_kernel<<<(nq + 127) / 128, 128, 0, s>>>(d_t, d_t_nnz, nq, d_dst, d_bad);
+    w_t_kernel<<<nq, 256, 0, s>>>(d_t, d_t_nnz, d_dst, d_bad);
 }
 
 void launch_zsum(const uint64_t* d_z_part, uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t trials_total,

@@ -60,6 +60,19 @@ struct IvChunk {
 };
 constexpr uint32_t IV_CHUNK_ROWS = 4096;
 
+// One distinct list of a batch: a group of the grouped GEMMs.
+struct IvGroup {
+    uint32_t row0, m;       // corpus rows of the list
+    uint32_t lp0, n;        // its pairs, list-major
+    uint32_t it_pl, it_s8;  // first item of the PLANAR (16-row A tiles) and S8 (128-row A tiles) tables
+};
+
+// A list of several z panels: z[m][t][j] = sum of its panels' z_part[p][t][j].
+struct IvZsum {
+    uint32_t p0, p1;  // panels
+    uint32_t m;       // slot in z
+};
+
 // ------------------------------------------------------------------ kernels
 // dst block lp (8 rows of row_bytes) = src block map[lp]
 __global__ void gather8_kernel(const uint4* __restrict__ src, uint4* __restrict__ dst, const uint32_t* __restrict__ map,
@@ -70,6 +83,31 @@ __global__ void gather8_kernel(const uint4* __restrict__ src, uint4* __restrict_
         const uint32_t lp = (uint32_t)(e / per), c = (uint32_t)(e % per);
         dst[(uint64_t)lp * per + c] = src[(uint64_t)map[lp] * per + c];
     }
+}
+
+// The grouped GEMMs' item tables: group u owns PLANAR items [it_pl(u),
+// it_pl(u + 1)), W tiles outer x 16-row A tiles inner, and S8 items likewise
+// with 128-row A tiles (every group has at least one item of each).
+__global__ void expand_items_kernel(const IvGroup* __restrict__ groups, uint32_t U, uint32_t n_pl, uint32_t n_s8,
+                                    uint32_t wy, BgItem* __restrict__ items_pl, BgItem* __restrict__ items_s8) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n_pl + n_s8) return;
+    const bool s8 = e >= n_pl;
+    const uint32_t it = s8 ? e - n_pl : e;
+    uint32_t lo = 0, hi = U;  // first(lo) <= it < first(hi), first(U) = table size
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((s8 ? groups[mid].it_s8 : groups[mid].it_pl) <= it) lo = mid;
+        else hi = mid;
+    }
+    const IvGroup g = groups[lo];
+    const uint32_t rows_per = s8 ? (uint32_t)BG_AROWS : (uint32_t)BG_AROWS / 8;
+    const uint32_t xt = (g.m + rows_per - 1) / rows_per;
+    const uint32_t local = it - (s8 ? g.it_s8 : g.it_pl);
+    const uint32_t x0 = g.row0 + (local % xt) * rows_per, y0 = g.lp0 + (local / xt) * wy;
+    const BgItem item{s8 ? x0 : 8 * x0, 8 * y0, x0, g.row0 + g.m, y0, g.lp0 + g.n};
+    if (s8) items_s8[it] = item;
+    else items_pl[it] = item;
 }
 
 // idmap[r-space entry] = corpus id of its row
@@ -145,12 +183,6 @@ ur_chunks_kernel(const IvChunk* __restrict__ chunks, const uint8_t* __restrict__
         ur_part[(uint64_t)blockIdx.x * trials_total + t_base + t] = x;
     }
 }
-
-// A list of several z panels: z[m][t][j] = sum of its panels' z_part[p][t][j].
-struct IvZsum {
-    uint32_t p0, p1;  // panels
-    uint32_t m;       // slot in z
-};
 
 __global__ void zsum_lists_kernel(const uint64_t* __restrict__ z_part, const IvZsum* __restrict__ lists,
                                   uint32_t trials, uint64_t* __restrict__ z) {
@@ -237,24 +269,31 @@ int tmap_u8(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uin
 
 }  // namespace
 
-// One IVF block run: the host plan (pairs, groups, item tables, Protocol 2
-// layout), the workspace layout and the tensor maps of the gathered operands.
+// One IVF block run: the host plan (pairs, groups, Protocol 2 layout), the
+// workspace layout and the tensor maps of the gathered operands.
 struct IvfBlockJob {
     uint32_t B = 0, trials = 0, k = 0;
     bool verify_only = false;
     uint32_t P = 0, U = 0, NB = 0, NP = 0, NCH = 0, n_pl = 0, n_s8 = 0, NZ = 0;
+    uint32_t NP_big = 0;  // panels [0, NP_big) belong to lists longer than TC_SMALL_PANEL_ROWS
     uint64_t R = 0, max_q_rows = 0;
     uint32_t w_tile = 64, n_rows = 0, ctas = 1, st_g1 = 0, st_g2 = 0, st_g3 = 0;
+    // host plan
+    std::vector<IvPair> pairs;          // q-major
+    std::vector<uint32_t> order;        // list-major position -> q-major pair
+    std::vector<IvGroup> groups;        // distinct lists, by list id
+    std::vector<uint32_t> block0, panel0;  // per group: first U block, first z panel
+    std::vector<uint64_t> qoff;         // per query: first r-space entry (B + 1)
+    std::vector<uint32_t> qp0;          // per query: first pair (B + 1)
     // inputs (one H2D from the staging buffer)
-    uint64_t o_v, o_g, o_t, o_tn, o_seed, o_qoff, o_qp0, o_pairs, o_lmq, o_lmi, o_base, o_items_pl, o_items_s8, o_vsegs,
-        o_blocks, o_panels, o_zoff, o_zsum, o_chunks, in_end;
+    uint64_t o_v, o_g, o_t, o_tn, o_seed, o_qoff, o_qp0, o_pairs, o_lmq, o_lmi, o_base, o_groups, o_vsegs, o_blocks,
+        o_panels, o_zoff, o_zsum, o_chunks, in_end;
     // outputs (one D2H)
     uint64_t o_ids, o_sc, o_n, o_fc, o_ft, o_err, out_end;
     // scratch
-    uint64_t o_vp, o_gx, o_tv, o_x, o_wv, o_wgx, o_wtv, o_r, o_f2, o_f3, o_idmap, o_ub, o_zpart, o_z, o_urpart, o_zv,
-        o_pfail, o_urout, o_cs, o_ci, o_cn, total;
+    uint64_t o_items_pl, o_items_s8, o_vp, o_gx, o_tv, o_x, o_wv, o_wgx, o_wtv, o_r, o_f2, o_f3, o_idmap, o_ub, o_zpart,
+        o_z, o_urpart, o_zv, o_pfail, o_urout, o_cs, o_ci, o_cn, total;
     CUtensorMap tm_wv, tm_wgx, tm_wtv, tm_u;
-    std::vector<char> meta;  // host image of [o_qoff, in_end)
 };
 
 void ivf_block_job_free(IvfBlockJob* j) { delete j; }
@@ -267,13 +306,13 @@ namespace {
 // each A tile is re-streamed (from L2) once per W tile of its group, so pick
 // the tile minimising sum over groups of A tiles x W tiles x (A + W rows +
 // a fixed per-item cost).
-uint32_t pick_w_tile(const std::vector<uint32_t>& n_pairs, const std::vector<uint64_t>& rows) {
+uint32_t pick_w_tile(const std::vector<IvGroup>& groups) {
     uint32_t best_w = 64;
     double best = 1e300;
     for (uint32_t w : {16u, 32u, 64u, 128u, 256u}) {
         double cost = 0;
-        for (size_t u = 0; u < n_pairs.size(); ++u)
-            cost += (double)((rows[u] + 15) / 16) * (double)((8ull * n_pairs[u] + w - 1) / w) * (128.0 + w + 64.0);
+        for (const IvGroup& g : groups)
+            cost += (double)((g.m + 15) / 16) * (double)((8ull * g.n + w - 1) / w) * (128.0 + w + 64.0);
         if (cost < best) {
             best = cost;
             best_w = w;
@@ -285,7 +324,9 @@ uint32_t pick_w_tile(const std::vector<uint32_t>& n_pairs, const std::vector<uin
 }  // namespace
 
 // Host plan of one batch.  probe_off[B + 1] / probes: query q probes lists
-// probes[probe_off[q] .. probe_off[q + 1]) in that order.
+// probes[probe_off[q] .. probe_off[q + 1]) in that order.  O(pairs log pairs
+// + distinct lists); the per-block / per-panel / per-chunk tables are written
+// by ivf_block_pack and the GEMM item tables on the device.
 int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* probe_off, const uint32_t* probes,
                    uint32_t trials, uint32_t k, bool verify_only, int sms) {
     const Corpus& c = v.e.c;
@@ -299,120 +340,90 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.k = k;
     j.verify_only = verify_only;
     // pairs, q-major; empty lists skipped (ivf.rs:787-789)
-    std::vector<IvPair> pairs;
-    std::vector<uint64_t> qoff(B + 1, 0);
-    std::vector<uint32_t> qp0(B + 1, 0);
+    j.pairs.clear();
+    j.pairs.reserve(probe_off[B]);
+    j.qoff.assign(B + 1, 0);
+    j.qp0.assign(B + 1, 0);
+    j.max_q_rows = 0;
     uint64_t R = 0;
     for (uint32_t q = 0; q < B; ++q) {
-        qoff[q] = R;
-        qp0[q] = (uint32_t)pairs.size();
+        j.qoff[q] = R;
+        j.qp0[q] = (uint32_t)j.pairs.size();
         for (uint32_t p = probe_off[q]; p < probe_off[q + 1]; ++p) {
             const uint32_t ci = probes[p];
             if (ci >= v.nlist)
                 return fail(BN_EINVAL, "probe %u of query %u names list %u of %u", p - probe_off[q], q, ci, v.nlist);
             const uint64_t m = v.offsets[ci + 1] - v.offsets[ci];
             if (!m) continue;
-            pairs.push_back(IvPair{R, q, ci, 0, 0, 0, 0});
+            j.pairs.push_back(IvPair{R, q, ci, 0, 0, 0, 0});
             R += m;
         }
-        j.max_q_rows = std::max(j.max_q_rows, R - qoff[q]);
+        j.max_q_rows = std::max(j.max_q_rows, R - j.qoff[q]);
     }
-    qoff[B] = R;
-    qp0[B] = (uint32_t)pairs.size();
+    j.qoff[B] = R;
+    j.qp0[B] = (uint32_t)j.pairs.size();
     j.R = R;
-    j.P = (uint32_t)pairs.size();
-    // groups: pairs sorted by list (stable: a list's queries stay in batch order)
-    std::vector<uint32_t> order(j.P);
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return pairs[a].list < pairs[b].list; });
-    std::vector<uint32_t> g_lp0, g_n, g_list;
-    std::vector<uint64_t> g_rows, g_row0;
+    j.P = (uint32_t)j.pairs.size();
+    // groups: pairs sorted by (list, pair), so a list's queries stay in batch order
+    std::vector<uint64_t> keys(j.P);
+    for (uint32_t i = 0; i < j.P; ++i) keys[i] = ((uint64_t)j.pairs[i].list << 32) | i;
+    std::sort(keys.begin(), keys.end());
+    j.order.resize(j.P);
+    j.groups.clear();
+    j.block0.clear();
+    j.panel0.clear();
+    uint32_t nb = 0, np = 0, nch = 0;
     for (uint32_t lp = 0; lp < j.P; ++lp) {
-        IvPair& pr = pairs[order[lp]];
-        if (g_list.empty() || g_list.back() != pr.list) {
-            g_list.push_back(pr.list);
-            g_lp0.push_back(lp);
-            g_n.push_back(0);
-            g_row0.push_back(v.offsets[pr.list]);
-            g_rows.push_back(v.offsets[pr.list + 1] - v.offsets[pr.list]);
+        const uint32_t i = (uint32_t)keys[lp];
+        j.order[lp] = i;
+        IvPair& pr = j.pairs[i];
+        if (lp == 0 || j.pairs[j.order[lp - 1]].list != pr.list) {
+            const uint32_t m = (uint32_t)(v.offsets[pr.list + 1] - v.offsets[pr.list]);
+            j.groups.push_back(IvGroup{(uint32_t)v.offsets[pr.list], m, lp, 0, 0, 0});
+            j.block0.push_back(nb);
+            nb += (m + TC_ROWS - 1) / TC_ROWS;
         }
-        pr.u = (uint32_t)g_list.size() - 1;
-        ++g_n.back();
+        IvGroup& g = j.groups.back();
+        pr.u = (uint32_t)j.groups.size() - 1;
+        pr.ch0 = nch;
+        pr.nch = (g.m + IV_CHUNK_ROWS - 1) / IV_CHUNK_ROWS;
+        nch += pr.nch;
+        ++g.n;
     }
-    j.U = (uint32_t)g_list.size();
-    std::vector<uint32_t> lmq(j.P), lmi(j.P);
-    std::vector<uint64_t> base(j.P);
-    for (uint32_t lp = 0; lp < j.P; ++lp) {
-        const IvPair& pr = pairs[order[lp]];
-        lmq[lp] = pr.q;
-        lmi[lp] = order[lp];
-        base[lp] = pr.out0 - g_row0[pr.u];  // out[base + corpus row] (mod 2^64)
-    }
-    // grouped GEMM item tables
-    std::vector<BgItem> items_pl, items_s8;
+    j.U = (uint32_t)j.groups.size();
+    // z panels: the long lists' first (tc_freivalds_kernel), then the short
+    // lists' single panels (tc_freivalds_small_kernel)
+    j.panel0.assign(j.U, 0);
+    for (uint32_t u = 0; u < j.U; ++u)
+        if (j.groups[u].m > TC_SMALL_PANEL_ROWS) {
+            j.panel0[u] = np;
+            np += (j.groups[u].m + TC_PANEL_ROWS - 1) / TC_PANEL_ROWS;
+        }
+    j.NP_big = np;
+    for (uint32_t u = 0; u < j.U; ++u)
+        if (j.groups[u].m <= TC_SMALL_PANEL_ROWS) j.panel0[u] = np++;
+    j.NB = nb;
+    j.NP = np;
+    j.NCH = nch;
+    j.NZ = 0;
+    for (uint32_t u = 0; u < j.U; ++u) j.NZ += (j.groups[u].m > TC_PANEL_ROWS) ? 1u : 0u;
+    // grouped GEMM item counts (the tables themselves are expanded on the device)
+    j.n_pl = j.n_s8 = 0;
     if (!verify_only && j.P) {
-        j.w_tile = pick_w_tile(g_n, g_rows);
+        j.w_tile = pick_w_tile(j.groups);
         const uint32_t wy = j.w_tile / 8;  // pairs per W tile
-        for (uint32_t u = 0; u < j.U; ++u) {
-            const uint32_t row0 = (uint32_t)g_row0[u], m = (uint32_t)g_rows[u];
-            const uint32_t lp0 = g_lp0[u], n = g_n[u];
-            for (uint32_t y = 0; y < n; y += wy)
-                for (uint32_t x = 0; x < m; x += BG_AROWS / 8)
-                    items_pl.push_back(BgItem{8 * (row0 + x), 8 * (lp0 + y), row0 + x, row0 + m, lp0 + y, lp0 + n});
-            for (uint32_t y = 0; y < n; y += wy)
-                for (uint32_t x = 0; x < m; x += BG_AROWS)
-                    items_s8.push_back(BgItem{row0 + x, 8 * (lp0 + y), row0 + x, row0 + m, lp0 + y, lp0 + n});
+        for (IvGroup& g : j.groups) {
+            const uint32_t yt = (g.n + wy - 1) / wy;
+            g.it_pl = j.n_pl;
+            g.it_s8 = j.n_s8;
+            j.n_pl += yt * ((g.m + BG_AROWS / 8 - 1) / (BG_AROWS / 8));
+            j.n_s8 += yt * ((g.m + BG_AROWS - 1) / BG_AROWS);
         }
         BgParams p{};
         p.w_tile = j.w_tile;
         j.st_g1 = j.st_g2 = j.st_g3 = bgemm_max_stages(p);
         if (!j.st_g1) return fail(BN_EUNSUPPORTED, "no pipeline depth fits W tile %u", j.w_tile);
     }
-    j.n_pl = (uint32_t)items_pl.size();
-    j.n_s8 = (uint32_t)items_s8.size();
-    // Protocol 2 layout: one verify segment per distinct list (128-row U
-    // blocks, 4096-row z panels), chunks of <= 4096 rows per pair
-    std::vector<VerifySeg> vsegs;
-    std::vector<TcBlock> blocks;
-    std::vector<TcPanel> panels;
-    std::vector<uint32_t> lp0v(j.U + 1, 0), block0(j.U, 0);
-    std::vector<uint64_t> zoff(j.U, 0);  // element offsets from z_part: a single panel's, or z's slot
-    std::vector<IvZsum> zsum;
-    for (uint32_t u = 0; u < j.U; ++u) {
-        const uint32_t m = (uint32_t)g_rows[u];
-        vsegs.push_back(VerifySeg{g_row0[u], 0, m, 0});
-        block0[u] = (uint32_t)blocks.size();
-        lp0v[u] = (uint32_t)panels.size();
-        for (uint32_t i0 = 0; i0 < m; i0 += TC_ROWS) blocks.push_back(TcBlock{u, i0});
-        for (uint32_t p0 = 0; p0 < m; p0 += TC_PANEL_ROWS)
-            panels.push_back(TcPanel{g_row0[u] + p0, std::min<uint32_t>(TC_PANEL_ROWS, m - p0), block0[u] + p0 / TC_ROWS,
-                                     u, 0});
-    }
-    lp0v[j.U] = (uint32_t)panels.size();
-    const uint64_t tt0 = std::max<uint32_t>(trials, 1);
-    const uint64_t z_from_zpart = (uint64_t)panels.size() * tt0 * N;  // z follows z_part in the workspace
-    for (uint32_t u = 0; u < j.U; ++u) {
-        if (lp0v[u + 1] - lp0v[u] == 1) {
-            zoff[u] = (uint64_t)lp0v[u] * tt0 * N;
-        } else {
-            zoff[u] = z_from_zpart + (uint64_t)zsum.size() * tt0 * N;
-            zsum.push_back(IvZsum{lp0v[u], lp0v[u + 1], (uint32_t)zsum.size()});
-        }
-    }
-    j.NZ = (uint32_t)zsum.size();
-    std::vector<IvChunk> chunks;
-    for (uint32_t lp = 0; lp < j.P; ++lp) {
-        IvPair& pr = pairs[order[lp]];
-        const uint32_t m = (uint32_t)g_rows[pr.u];
-        pr.ch0 = (uint32_t)chunks.size();
-        for (uint32_t c0 = 0; c0 < m; c0 += IV_CHUNK_ROWS)
-            chunks.push_back(IvChunk{pr.out0 + c0, g_row0[pr.u] + c0, block0[pr.u] + c0 / TC_ROWS,
-                                     std::min<uint32_t>(IV_CHUNK_ROWS, m - c0)});
-        pr.nch = (uint32_t)chunks.size() - pr.ch0;
-    }
-    j.NB = (uint32_t)blocks.size();
-    j.NP = (uint32_t)panels.size();
-    j.NCH = (uint32_t)chunks.size();
     j.n_rows = pass_rows(std::min<uint32_t>(std::max<uint32_t>(trials, 1), TC_MAX_TRIALS));
     j.ctas = (uint32_t)pick_ctas(j.max_q_rows, std::max<uint32_t>(B, 1), sms);
 
@@ -431,8 +442,7 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.o_lmq = L.take<uint32_t>(j.P);
     j.o_lmi = L.take<uint32_t>(j.P);
     j.o_base = L.take<uint64_t>(j.P);
-    j.o_items_pl = L.take<BgItem>(j.n_pl);
-    j.o_items_s8 = L.take<BgItem>(j.n_s8);
+    j.o_groups = L.take<IvGroup>(j.U);
     j.o_vsegs = L.take<VerifySeg>(j.U);
     j.o_blocks = L.take<TcBlock>(j.NB);
     j.o_panels = L.take<TcPanel>(j.NP);
@@ -447,6 +457,8 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.o_ft = L.take<int32_t>(B);
     j.o_err = L.take<uint32_t>(2);  // [0] pipeline flags, [1] operand range flags
     j.out_end = L.take<uint8_t>(0);
+    j.o_items_pl = L.take<BgItem>(j.n_pl);
+    j.o_items_s8 = L.take<BgItem>(j.n_s8);
     j.o_vp = L.take<uint8_t>(8 * qb * N);
     j.o_gx = L.take<uint8_t>(8 * qb * c.k_alh);
     j.o_tv = L.take<uint8_t>(8 * qb * 2 * N);
@@ -472,33 +484,12 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.o_ci = L.take<uint32_t>(verify_only ? 0 : cand);
     j.o_cn = L.take<uint32_t>(verify_only ? 0 : (uint64_t)B * j.ctas);
     j.total = L.off + 1024;
-
-    // host image of the metadata
-    j.meta.assign(j.in_end - j.o_qoff, 0);
-    char* h = j.meta.data() - j.o_qoff;
-    auto put = [&](uint64_t off, const void* src, uint64_t bytes) {
-        if (bytes) memcpy(h + off, src, bytes);
-    };
-    put(j.o_qoff, qoff.data(), qoff.size() * 8);
-    put(j.o_qp0, qp0.data(), qp0.size() * 4);
-    put(j.o_pairs, pairs.data(), pairs.size() * sizeof(IvPair));
-    put(j.o_lmq, lmq.data(), lmq.size() * 4);
-    put(j.o_lmi, lmi.data(), lmi.size() * 4);
-    put(j.o_base, base.data(), base.size() * 8);
-    put(j.o_items_pl, items_pl.data(), items_pl.size() * sizeof(BgItem));
-    put(j.o_items_s8, items_s8.data(), items_s8.size() * sizeof(BgItem));
-    put(j.o_vsegs, vsegs.data(), vsegs.size() * sizeof(VerifySeg));
-    put(j.o_blocks, blocks.data(), blocks.size() * sizeof(TcBlock));
-    put(j.o_panels, panels.data(), panels.size() * sizeof(TcPanel));
-    put(j.o_zoff, zoff.data(), zoff.size() * 8);
-    put(j.o_zsum, zsum.data(), zsum.size() * sizeof(IvZsum));
-    put(j.o_chunks, chunks.data(), chunks.size() * sizeof(IvChunk));
     return BN_OK;
 }
 
-// Validates and packs the query inputs into the pinned staging buffer (grown
-// as needed) and sizes ws (grown as needed, budget-accounted); encodes the
-// tensor maps of this run's buffers.
+// Validates and packs the query inputs and the plan's tables into the pinned
+// staging buffer (grown as needed) and sizes ws (grown as needed,
+// budget-accounted); encodes the tensor maps of this run's buffers.
 int ivf_block_pack(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, const uint64_t* v_enc, const uint64_t* g,
                    const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* seed) {
     const Corpus& c = e.c;
@@ -529,7 +520,52 @@ int ivf_block_pack(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, const
     }
     if (seed) memcpy(h + j.o_seed, seed, 32);
     else memset(h + j.o_seed, 0, 32);
-    memcpy(h + j.o_qoff, j.meta.data(), j.meta.size());
+    // plan tables, written in place
+    memcpy(h + j.o_qoff, j.qoff.data(), j.qoff.size() * 8);
+    memcpy(h + j.o_qp0, j.qp0.data(), j.qp0.size() * 4);
+    if (j.P) memcpy(h + j.o_pairs, j.pairs.data(), (uint64_t)j.P * sizeof(IvPair));
+    if (j.U) memcpy(h + j.o_groups, j.groups.data(), (uint64_t)j.U * sizeof(IvGroup));
+    uint32_t* lmq = reinterpret_cast<uint32_t*>(h + j.o_lmq);
+    uint32_t* lmi = reinterpret_cast<uint32_t*>(h + j.o_lmi);
+    uint64_t* base = reinterpret_cast<uint64_t*>(h + j.o_base);
+    IvChunk* ch = reinterpret_cast<IvChunk*>(h + j.o_chunks);
+    for (uint32_t lp = 0, nc = 0; lp < j.P; ++lp) {
+        const uint32_t i = j.order[lp];
+        const IvPair& pr = j.pairs[i];
+        const IvGroup& gr = j.groups[pr.u];
+        lmq[lp] = pr.q;
+        lmi[lp] = i;
+        base[lp] = pr.out0 - gr.row0;  // out[base + corpus row] (mod 2^64)
+        for (uint32_t c0 = 0; c0 < gr.m; c0 += IV_CHUNK_ROWS)
+            ch[nc++] = IvChunk{pr.out0 + c0, (uint64_t)gr.row0 + c0, j.block0[pr.u] + c0 / TC_ROWS,
+                               std::min<uint32_t>(IV_CHUNK_ROWS, gr.m - c0)};
+    }
+    // Protocol 2 layout: one verify segment per distinct list (128-row U
+    // blocks, 4096-row z panels); z of a single-panel list is its z_part,
+    // several panels are summed into a z slot (after z_part)
+    VerifySeg* vs = reinterpret_cast<VerifySeg*>(h + j.o_vsegs);
+    TcBlock* bl = reinterpret_cast<TcBlock*>(h + j.o_blocks);
+    TcPanel* pn = reinterpret_cast<TcPanel*>(h + j.o_panels);
+    uint64_t* zoff = reinterpret_cast<uint64_t*>(h + j.o_zoff);
+    IvZsum* zs = reinterpret_cast<IvZsum*>(h + j.o_zsum);
+    const uint64_t tt = std::max<uint32_t>(j.trials, 1);
+    for (uint32_t u = 0, nb = 0, nz = 0; u < j.U; ++u) {
+        const IvGroup& gr = j.groups[u];
+        vs[u] = VerifySeg{gr.row0, 0, gr.m, 0};
+        for (uint32_t i0 = 0; i0 < gr.m; i0 += TC_ROWS) bl[nb++] = TcBlock{u, i0};
+        const uint32_t p0 = j.panel0[u];
+        uint32_t np = p0;
+        for (uint32_t r0 = 0; r0 < gr.m; r0 += TC_PANEL_ROWS)
+            pn[np++] = TcPanel{(uint64_t)gr.row0 + r0, std::min<uint32_t>(TC_PANEL_ROWS, gr.m - r0),
+                               j.block0[u] + r0 / TC_ROWS, u, 0};
+        if (np - p0 == 1) {
+            zoff[u] = (uint64_t)p0 * tt * N;
+        } else {
+            zoff[u] = ((uint64_t)j.NP + nz) * tt * N;
+            zs[nz] = IvZsum{p0, np, nz};
+            ++nz;
+        }
+    }
     char* d = ws.at<char>();
     if (!j.verify_only && j.P) {
         TRY(tmap_u8(&j.tm_wv, d + j.o_wv, N, 8ull * j.P, j.w_tile, "gathered v planes"));
@@ -586,6 +622,9 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
                     reinterpret_cast<const uint4*>(d + im.src), reinterpret_cast<uint4*>(d + im.dst), lmq, j.P,
                     im.row_bytes);
             idmap_kernel<<<j.NCH, 256, 0, s>>>(dchunks, c.ids.at<uint32_t>(), U32(j.o_idmap));
+            expand_items_kernel<<<(j.n_pl + j.n_s8 + 255) / 256, 256, 0, s>>>(
+                reinterpret_cast<const IvGroup*>(d + j.o_groups), j.U, j.n_pl, j.n_s8, j.w_tile / 8,
+                reinterpret_cast<BgItem*>(d + j.o_items_pl), reinterpret_cast<BgItem*>(d + j.o_items_s8));
             mark(1);
             // G1 r = M_c v_q, G2 f2 = -(AL_c g_q + H_c x_q), G3 f3 = M_c T_q + S_c v_q
             BgParams p{};
@@ -629,7 +668,10 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
         for (uint32_t t0 = 0; t0 < j.trials; t0 += TC_MAX_TRIALS) {
             const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, j.trials - t0);
             launch_tc_ugen(vsegs, blocks, j.NB, key, nullptr, t0, tc, j.n_rows, U8(j.o_ub), nullptr, j.trials, err, s);
-            launch_tc_freivalds(c.tmap_m, j.tm_u, panels, j.NP, t0, tc, j.n_rows, j.trials, U64(j.o_zpart), err, sms, s);
+            launch_tc_freivalds(c.tmap_m, j.tm_u, panels, j.NP_big, t0, tc, j.n_rows, j.trials, U64(j.o_zpart), err,
+                                sms, s);
+            launch_tc_freivalds_small(c.tmap_m, j.tm_u, panels, j.NP_big, j.NP - j.NP_big, t0, tc, j.n_rows, j.trials,
+                                      U64(j.o_zpart), err, sms, s);
             ur_chunks_kernel<<<j.NCH, 128, 0, s>>>(dchunks, U8(j.o_ub), j.n_rows, t0, tc, j.trials, U64(j.o_r),
                                                   U64(j.o_urpart));
         }

@@ -112,60 +112,78 @@ constexpr int TC_EPI_WARPS = 8;                // TMEM drain warps: 2 per lane q
 // then a butterfly over the 8 lanes of one element leaves lane a with trial
 // c0/8 + a's sum; 16-column remainders use a plain 3-level reduction.
 // z_out[t * N + j] receives z_t[j] for t < t_cnt.
+// One 64-column chunk (8 trials) of a strip: lane (xi, a) folds its 8
+// trials' byte products to (lo + hi 2^32) 2^(8a) mod p, a butterfly over the
+// 8 lanes of one element leaves lane a with trial c0/8 + a's sum.
+__device__ __forceinline__ void z_drain64(uint32_t taddr, uint32_t lane, uint32_t j, uint32_t c0, uint32_t t_cnt,
+                                          uint64_t* __restrict__ z_out) {
+    const uint32_t a = lane & 7;
+    const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+    const bool b2 = (a & 4) != 0, b1 = (a & 2) != 0, b0 = (a & 1) != 0;
+    uint32_t v[64];
+    tmem_ld64(taddr, v);
+    uint64_t part[8];
+#pragma unroll
+    for (int tt = 0; tt < 8; ++tt) {
+        uint64_t lo = 0, hi = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            lo += (uint64_t)v[8 * tt + b] << (8 * b);
+            hi += (uint64_t)v[8 * tt + 4 + b] << (8 * b);
+        }
+        part[tt] = canon(rotl61(lo, w1) + rotl61(hi, w2));
+    }
+    uint64_t k4[4], k2[2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        k4[i] = (b2 ? part[i + 4] : part[i]) + __shfl_xor_sync(FULLMASK, b2 ? part[i] : part[i + 4], 4);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+        k2[i] = (b1 ? k4[i + 2] : k4[i]) + __shfl_xor_sync(FULLMASK, b1 ? k4[i] : k4[i + 2], 2);
+    const uint64_t z = canon((b0 ? k2[1] : k2[0]) + __shfl_xor_sync(FULLMASK, b0 ? k2[0] : k2[1], 1));
+    const uint32_t t = c0 / 8 + a;
+    if (t < t_cnt) z_out[(uint64_t)t * N + j] = z;
+}
+
+// One 16-column chunk (2 trials) of a strip: plain 3-level reduction.
+__device__ __forceinline__ void z_drain16(uint32_t taddr, uint32_t lane, uint32_t j, uint32_t c0, uint32_t t_cnt,
+                                          uint64_t* __restrict__ z_out) {
+    const uint32_t a = lane & 7;
+    const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+    uint32_t v[16];
+    tmem_ld16(taddr, v);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t t = c0 / 8 + h;
+        uint64_t lo = 0, hi = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            lo += (uint64_t)v[8 * h + b] << (8 * b);
+            hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
+        }
+        uint64_t zc = canon(rotl61(lo, w1) + rotl61(hi, w2));
+        zc += __shfl_xor_sync(FULLMASK, zc, 1);
+        zc += __shfl_xor_sync(FULLMASK, zc, 2);
+        zc += __shfl_xor_sync(FULLMASK, zc, 4);
+        if (a == 0 && t < t_cnt) z_out[(uint64_t)t * N + j] = canon(zc);
+    }
+}
+
+// Drains one work item's accumulators into z partials.  TMEM holds, per strip
+// s < sg (columns s * n_rows ...), lanes = the strip's 128 byte columns (j, a)
+// (element j = lane / 8, byte a = lane % 8) and columns (t, b) (trial t, byte
+// b of u_t).  Warp (lane quarter q, half) reads every other 64-column chunk,
+// then every other 16-column remainder chunk.
+// z_out[t * N + j] receives z_t[j] for t < t_cnt.
 __device__ __forceinline__ void z_drain(uint32_t tmem, uint32_t q, uint32_t half, uint32_t lane, uint32_t sg,
                                         uint32_t strip0, uint32_t n_rows, uint32_t t_cnt, uint64_t* __restrict__ z_out) {
-    const uint32_t a = lane & 7, xi = lane >> 3;
-    const uint32_t jl = q * 4 + xi;
-    const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+    const uint32_t jl = q * 4 + (lane >> 3);
     const uint32_t wide = n_rows & ~63u;
-    const bool b2 = (a & 4) != 0, b1 = (a & 2) != 0, b0 = (a & 1) != 0;
     for (uint32_t s = 0; s < sg; ++s) {
         const uint32_t j = (strip0 + s) * 16 + jl;
         const uint32_t tbase = tmem + ((q * 32) << 16) + s * n_rows;
-        for (uint32_t c0 = 64 * half; c0 < wide; c0 += 128) {
-            uint32_t v[64];
-            tmem_ld64(tbase + c0, v);
-            uint64_t part[8];
-#pragma unroll
-            for (int tt = 0; tt < 8; ++tt) {
-                uint64_t lo = 0, hi = 0;
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    lo += (uint64_t)v[8 * tt + b] << (8 * b);
-                    hi += (uint64_t)v[8 * tt + 4 + b] << (8 * b);
-                }
-                part[tt] = canon(rotl61(lo, w1) + rotl61(hi, w2));
-            }
-            uint64_t k4[4], k2[2];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                k4[i] = (b2 ? part[i + 4] : part[i]) + __shfl_xor_sync(FULLMASK, b2 ? part[i] : part[i + 4], 4);
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-                k2[i] = (b1 ? k4[i + 2] : k4[i]) + __shfl_xor_sync(FULLMASK, b1 ? k4[i] : k4[i + 2], 2);
-            const uint64_t z = canon((b0 ? k2[1] : k2[0]) + __shfl_xor_sync(FULLMASK, b0 ? k2[0] : k2[1], 1));
-            const uint32_t t = c0 / 8 + a;
-            if (t < t_cnt) z_out[(uint64_t)t * N + j] = z;
-        }
-        for (uint32_t c0 = wide + 16 * half; c0 < n_rows; c0 += 32) {
-            uint32_t v[16];
-            tmem_ld16(tbase + c0, v);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const uint32_t t = c0 / 8 + h;
-                uint64_t lo = 0, hi = 0;
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    lo += (uint64_t)v[8 * h + b] << (8 * b);
-                    hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
-                }
-                uint64_t zc = canon(rotl61(lo, w1) + rotl61(hi, w2));
-                zc += __shfl_xor_sync(FULLMASK, zc, 1);
-                zc += __shfl_xor_sync(FULLMASK, zc, 2);
-                zc += __shfl_xor_sync(FULLMASK, zc, 4);
-                if (a == 0 && t < t_cnt) z_out[(uint64_t)t * N + j] = canon(zc);
-            }
-        }
+        for (uint32_t c0 = 64 * half; c0 < wide; c0 += 128) z_drain64(tbase + c0, lane, j, c0, t_cnt, z_out);
+        for (uint32_t c0 = wide + 16 * half; c0 < n_rows; c0 += 32) z_drain16(tbase + c0, lane, j, c0, t_cnt, z_out);
     }
 }
 
@@ -307,6 +325,200 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
             tc_before();
             __syncwarp();
             if (lane == 0) bar_arrive(&acce_b);
+        }
+    }
+    tc_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------ small panels
+// tc_freivalds_kernel for panels of at most TC_SMALL_RB row blocks (the short
+// inverted lists of an IVF batch, most of them a single 128-row block).  A
+// CTA takes whole panels: the panel's U tiles are loaded once into one of two
+// shared-memory regions (the next panel's load overlaps this one's MMAs) and
+// stay there while the panel's 64 strips of m_enc stream through the stage
+// ring, one strip per item, into three rotating TMEM accumulators (3 x n_rows
+// <= 480 columns): the drain of a strip overlaps the MMAs of the next two.
+// Roles: warp 0 TMA, warp 1 MMA issuer, warps 2-17 drain (4 per lane
+// quarter; a strip's 64- and 16-column chunks are dealt out among them).
+// Every mbarrier wait is bounded; on timeout the CTA sets *err and winds down.
+constexpr uint32_t TC_SMALL_RB = TC_SMALL_PANEL_ROWS / TC_ROWS;
+constexpr uint32_t SM_STAGES = 6;
+constexpr int SM_EPI_WARPS = 16;
+constexpr int SM_THREADS = 64 + 32 * SM_EPI_WARPS;
+
+__global__ void __launch_bounds__(SM_THREADS, 1)
+tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constant__ CUtensorMap tmap_u,
+                          const TcPanel* __restrict__ panels, uint32_t p_first, uint32_t npanels,
+                          uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
+                          uint64_t* __restrict__ z_part, uint32_t* __restrict__ err) {
+    extern __shared__ uint8_t tc_dyn[];
+    __shared__ uint64_t full_b[SM_STAGES], empty_b[SM_STAGES], accf_b[3], acce_b[3], ufull_b[2], ufree_b[2], done_b;
+    __shared__ uint32_t tmem_base_s;
+    __shared__ volatile int abort_s;
+
+    // 1024-byte aligned: [U region 0][U region 1][stage ring]
+    const uint32_t base = (su32(tc_dyn) + 1023u) & ~1023u;
+    uint8_t* sm = tc_dyn + (base - su32(tc_dyn));
+    const uint32_t u_tile = n_rows * TC_ROWS;  // one row block's U tile (a multiple of 2048 bytes)
+    const uint32_t u_region = TC_SMALL_RB * u_tile;
+    const uint32_t ring_off = 2 * u_region;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < SM_STAGES; ++s) {
+            bar_init(&full_b[s], 1);
+            bar_init(&empty_b[s], 1);
+        }
+        for (int b = 0; b < 3; ++b) {
+            bar_init(&accf_b[b], 1);
+            bar_init(&acce_b[b], SM_EPI_WARPS);
+        }
+        for (int b = 0; b < 2; ++b) {
+            bar_init(&ufull_b[b], 1);
+            bar_init(&ufree_b[b], 1);
+        }
+        bar_init(&done_b, 1);
+        abort_s = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_base_s)),
+                     "r"(512u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tmem = tmem_base_s;
+
+    if (warp == 0) {
+        // ---------------------------------------------------------- TMA producer
+        if (lane == 0) {
+            uint64_t it = 0;
+            uint32_t pc = 0;
+            bool stop = false;
+            for (uint32_t w = blockIdx.x; w < npanels && !stop; w += gridDim.x, ++pc) {
+                const TcPanel pn = panels[p_first + w];
+                const uint32_t nrb = min((pn.rows + TC_ROWS - 1) / TC_ROWS, TC_SMALL_RB);
+                const uint32_t ub = pc & 1;
+                // U region ub is free once the MMAs of panel pc - 2 have read it
+                if (pc >= 2 && !bar_wait(&ufree_b[ub], ((pc >> 1) - 1) & 1)) {
+                    abort_s = 1;
+                    atomicOr(err, 4u);
+                    break;
+                }
+                if (abort_s) break;
+                bar_expect_tx(&ufull_b[ub], nrb * u_tile);
+                for (uint32_t rb = 0; rb < nrb; ++rb)
+                    tma_2d(sm + ub * u_region + rb * u_tile, &tmap_u, 0, (int)((pn.rb0 + rb) * n_rows), &ufull_b[ub]);
+                for (uint32_t s = 0; s < 64 && !stop; ++s)
+                    for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
+                        const uint32_t st = (uint32_t)(it % SM_STAGES);
+                        if (it >= SM_STAGES && !bar_wait(&empty_b[st], (uint32_t)(((it / SM_STAGES) - 1) & 1))) {
+                            abort_s = 1;
+                            atomicOr(err, 4u);
+                            stop = true;
+                            break;
+                        }
+                        if (abort_s) { stop = true; break; }
+                        bar_expect_tx(&full_b[st], STRIP_BYTES);
+                        tma_2d(sm + ring_off + st * STRIP_BYTES, &tmap_m, (int)(s * 128), (int)(pn.row0 + rb * TC_ROWS),
+                               &full_b[st]);
+                    }
+            }
+            // no copy may still be landing in shared memory when the CTA exits:
+            // the last ring stages and the U loads of the last two panels
+            for (uint64_t j = it > SM_STAGES ? it - SM_STAGES : 0; j < it; ++j)
+                bar_wait(&full_b[j % SM_STAGES], (uint32_t)((j / SM_STAGES) & 1));
+            for (uint32_t x = pc > 2 ? pc - 2 : 0; x < pc; ++x) bar_wait(&ufull_b[x & 1], (x >> 1) & 1);
+        }
+    } else if (warp == 1) {
+        // ---------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            const uint32_t idesc = (2u << 4) | (1u << 15) | ((n_rows >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+            uint64_t it = 0, sc = 0;
+            uint32_t pc = 0;
+            bool stop = false;
+            for (uint32_t w = blockIdx.x; w < npanels && !stop; w += gridDim.x, ++pc) {
+                const TcPanel pn = panels[p_first + w];
+                const uint32_t nrb = min((pn.rows + TC_ROWS - 1) / TC_ROWS, TC_SMALL_RB);
+                const uint32_t ub = pc & 1;
+                if (!bar_wait(&ufull_b[ub], (pc >> 1) & 1) || abort_s) {
+                    abort_s = 1;
+                    atomicOr(err, 8u);
+                    break;
+                }
+                tc_after();
+                for (uint32_t s = 0; s < 64 && !stop; ++s, ++sc) {
+                    const uint32_t b = (uint32_t)(sc % 3), use = (uint32_t)(sc / 3);
+                    if (use > 0 && !bar_wait(&acce_b[b], (use - 1) & 1)) {
+                        abort_s = 1;
+                        atomicOr(err, 8u);
+                        stop = true;
+                        break;
+                    }
+                    tc_after();
+                    const uint32_t d = tmem + b * n_rows;
+                    for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
+                        const uint32_t st = (uint32_t)(it % SM_STAGES);
+                        if (!bar_wait(&full_b[st], (uint32_t)((it / SM_STAGES) & 1)) || abort_s) {
+                            abort_s = 1;
+                            atomicOr(err, 8u);
+                            stop = true;
+                            break;
+                        }
+                        tc_after();
+                        const uint32_t sa = base + ring_off + st * STRIP_BYTES;
+                        const uint32_t su = base + ub * u_region + rb * u_tile;
+#pragma unroll
+                        for (uint32_t ks = 0; ks < TC_ROWS / 32; ++ks)
+                            mma_i8(d, sdesc(sa + ks * 4096u, STRIP_BYTES, 1024), sdesc(su + ks * 32u, 16, 1024), idesc,
+                                   (rb | ks) != 0);
+                        mma_commit(&empty_b[st]);  // stage reusable once these MMAs have read it
+                    }
+                    if (stop) break;
+                    mma_commit(&accf_b[b]);  // this strip's accumulator is complete
+                }
+                if (stop) break;
+                mma_commit(&ufree_b[ub]);  // U region reusable once this panel's MMAs are done
+            }
+            mma_commit(&done_b);
+            bar_wait(&done_b, 0);  // every issued MMA has finished before TMEM is freed
+        }
+    } else {
+        // ---------------------------------------------------------- drain
+        const uint32_t q = (uint32_t)(warp & 3);             // TMEM lane quarter of this warp
+        const uint32_t part = (uint32_t)(warp - 2) >> 2;      // 0..3: its share of each strip's chunks
+        const uint32_t jl = q * 4 + (lane >> 3);
+        const uint32_t wide = n_rows & ~63u, nwide = wide / 64;
+        const uint32_t tasks = nwide + (n_rows - wide) / 16;
+        uint64_t sc = 0;
+        bool stop = false;
+        for (uint32_t w = blockIdx.x; w < npanels && !stop; w += gridDim.x) {
+            const uint32_t p = p_first + w;
+            uint64_t* z_out = z_part + ((uint64_t)p * trials_total + t_base) * N;
+            for (uint32_t s = 0; s < 64; ++s, ++sc) {
+                const uint32_t b = (uint32_t)(sc % 3), use = (uint32_t)(sc / 3);
+                const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b[b], use & 1));  // warp-uniform
+                if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
+                if (__any_sync(FULLMASK, !ok || abort_s)) { stop = true; break; }
+                tc_after();
+                const uint32_t tbase = tmem + ((q * 32) << 16) + b * n_rows;
+                const uint32_t j = s * 16 + jl;
+                for (uint32_t k = part; k < tasks; k += 4) {
+                    if (k < nwide) z_drain64(tbase + 64 * k, lane, j, 64 * k, t_cnt, z_out);
+                    else z_drain16(tbase + wide + 16 * (k - nwide), lane, j, wide + 16 * (k - nwide), t_cnt, z_out);
+                }
+                tc_before();
+                __syncwarp();
+                if (lane == 0) bar_arrive(&acce_b[b]);
+            }
         }
     }
     tc_before();
@@ -710,6 +922,18 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
         tc_freivalds_kernel<3><<<grid, TC_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, t_base, t_cnt, n_rows,
                                                               trials_total, stages, stage_bytes, d_z_part, d_err, u_flat);
     }
+}
+
+void launch_tc_freivalds_small(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
+                               uint32_t p_first, uint32_t npanels, uint32_t t_base, uint32_t t_cnt,
+                               uint32_t n_rows, uint32_t trials_total, uint64_t* d_z_part, uint32_t* d_err,
+                               int num_sms, cudaStream_t s) {
+    if (!npanels) return;
+    const int smem = (int)(2 * TC_SMALL_RB * n_rows * TC_ROWS + SM_STAGES * STRIP_BYTES + 1024);
+    cudaFuncSetAttribute(tc_freivalds_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const unsigned grid = npanels < (uint32_t)num_sms ? npanels : (unsigned)num_sms;
+    tc_freivalds_small_kernel<<<grid, SM_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, p_first, npanels, t_base, t_cnt,
+                                                             n_rows, trials_total, d_z_part, d_err);
 }
 
 void launch_query_wimg(const uint64_t* d_v, uint32_t nq, uint8_t* d_w, cudaStream_t s) {

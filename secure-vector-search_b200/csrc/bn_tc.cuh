@@ -66,6 +66,16 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
                          uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
                          uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s, int u_flat = 0);
 
+// The same for panels [p_first, p_first + npanels) of at most
+// TC_SMALL_PANEL_ROWS rows (short IVF lists): whole panels per CTA, the
+// panel's U tiles resident in shared memory, one strip per work item into
+// three rotating accumulators (n_rows <= 160) so drains overlap the MMAs.
+constexpr uint32_t TC_SMALL_PANEL_ROWS = 3 * 128;
+void launch_tc_freivalds_small(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
+                               uint32_t p_first, uint32_t npanels, uint32_t t_base, uint32_t t_cnt,
+                               uint32_t n_rows, uint32_t trials_total, uint64_t* d_z_part, uint32_t* d_err,
+                               int num_sms, cudaStream_t s);
+
 // Fused single pass over m_enc for the first <= 20 trials, both products on
 // the tensor cores: z_part as above plus r_part[group][r index] (3-strip
 // group partial dots with the query, r_stride = total r entries, 22 groups),
