@@ -67,6 +67,25 @@ __device__ __forceinline__ bool item_at(const BgParams& p, uint32_t items, uint3
     return true;
 }
 
+// This CTA's items in order, the next item's entry fetched one item ahead (in
+// grouped mode an item-table load, whose latency then overlaps the current item).
+struct ItemCursor {
+    const BgParams& p;
+    uint32_t items, j = 0;
+    ItemIdx cur, nxt;
+    bool have_cur, have_nxt;
+    __device__ __forceinline__ ItemCursor(const BgParams& p_, uint32_t items_) : p(p_), items(items_) {
+        have_cur = item_at(p, items, 0, cur);
+        have_nxt = have_cur && item_at(p, items, 1, nxt);
+    }
+    __device__ __forceinline__ void advance() {
+        ++j;
+        cur = nxt;
+        have_cur = have_nxt;
+        if (have_cur) have_nxt = item_at(p, items, j + 1, nxt);
+    }
+};
+
 __global__ void __launch_bounds__(BG_THREADS, 1)
 bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CUtensorMap tmap_w,
              const BgParams p, uint32_t stages, uint32_t stage_bytes, uint32_t* __restrict__ err) {
@@ -125,8 +144,9 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
             uint64_t it = 0;
             uint32_t t_last = 0xffffffffu;
             bool stop = false;
-            ItemIdx ix;
-            for (uint32_t j = 0; !stop && item_at(p, items, j, ix); ++j) {
+            for (ItemCursor cs(p, items); !stop && cs.have_cur; cs.advance()) {
+                const ItemIdx& ix = cs.cur;
+                const uint32_t j = cs.j;
                 const uint32_t t = a_slots ? j / p.w_tiles : 0;
                 const bool load_a = a_slots && ix.tw == 0;
                 const uint32_t k0 = ix.kp * p.k_panel, k1 = min(p.k_bytes, k0 + p.k_panel);
@@ -173,10 +193,12 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
             const uint32_t sgn = p.mode == BG_S8 ? 1u : 0u;
             const uint32_t idesc = (2u << 4) | (sgn << 7) | (sgn << 10) | ((p.w_tile >> 3) << 17) |
                                    ((uint32_t)(BG_AROWS >> 4) << 24);
-            uint64_t it = 0, n = 0;
+            uint64_t it = 0;
             bool stop = false;
-            ItemIdx ix;
-            for (uint32_t j = 0; !stop && item_at(p, items, j, ix); ++j, ++n) {
+            for (ItemCursor cs(p, items); !stop && cs.have_cur; cs.advance()) {
+                const ItemIdx& ix = cs.cur;
+                const uint32_t j = cs.j;
+                const uint64_t n = j;
                 const uint32_t t = a_slots ? j / p.w_tiles : 0;
                 const bool last_of_a = a_slots && ix.tw == p.w_tiles - 1;
                 const uint32_t buf = (uint32_t)(n & 1), use = (uint32_t)(n >> 1);
@@ -222,24 +244,40 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
         // 64-column chunk (half = (w - 2) / 4) of each item.
         const uint32_t q = (uint32_t)(warp & 3);
         const uint32_t half = (uint32_t)(warp - 2) >> 2;
-        uint64_t n = 0;
-        ItemIdx ix;
-        for (uint32_t j = 0; item_at(p, items, j, ix); ++j, ++n) {
+        const uint32_t wide = p.w_tile & ~63u;  // columns handled in 64-column chunks
+        for (ItemCursor cs(p, items); cs.have_cur; cs.advance()) {
+            const ItemIdx& ix = cs.cur;
+            const uint64_t n = cs.j;
             const uint32_t buf = (uint32_t)(n & 1), use = (uint32_t)(n >> 1);
+            // output bases of the y this lane stores, loaded before the wait:
+            // PLANAR lane (xi, a) stores y = chunk + a (wide chunks) and
+            // chunk + {0, 1} (16-column chunks); S8 lanes share every y, so
+            // lane l holds chunk + (l & 7) and the stores shuffle it out
+            const uint32_t ybase = ix.y0;
+            auto obase = [&](uint32_t y) -> uint64_t {
+                return y < ix.y_lim ? (p.pair_base ? p.pair_base[y] : (uint64_t)y * p.out_ld) : 0;
+            };
+            const uint32_t ysel = lane & 7;  // PLANAR: a; S8: the y this lane holds for the shuffles
+            uint64_t ob_w[2], ob_r[2][2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const uint32_t cw = 64 * half + 128 * k, cr = wide + 16 * half + 32 * k;
+                ob_w[k] = cw < wide ? obase(ybase + cw / 8 + ysel) : 0;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) ob_r[k][h] = cr < p.w_tile ? obase(ybase + cr / 8 + h) : 0;
+            }
             const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b[buf], use & 1));  // warp-uniform
             if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
             if (__any_sync(FULLMASK, !ok || abort_s)) break;
             tc_after();
             const uint32_t taddr = tmem + ((q * 32u) << 16) + buf * 256u;
-            const uint32_t ybase = ix.y0;
-            const uint32_t wide = p.w_tile & ~63u;  // columns handled in 64-column chunks
             if (p.mode == BG_PLANAR) {
                 const uint32_t a = lane & 7, xi = lane >> 3;
                 const uint32_t x4 = ix.x0 + q * 4;  // first x of this warp
                 const uint32_t x = x4 + xi;
                 const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
                 uint64_t* out = p.out + (uint64_t)ix.kp * p.out_pstride;
-                for (uint32_t c0 = 64 * half; c0 < wide; c0 += 128) {
+                for (uint32_t c0 = 64 * half, k = 0; c0 < wide; c0 += 128, ++k) {
                     uint32_t v[64];
                     tmem_ld64(taddr + c0, v);
                     uint64_t part[8];  // (lo + hi 2^32) 2^(8a) mod p for the chunk's 8 y
@@ -266,8 +304,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     const uint64_t f =
                         canon((b0 ? k2[1] : k2[0]) + __shfl_xor_sync(FULLMASK, b0 ? k2[0] : k2[1], 1));  // < 8p
                     const uint32_t y = ybase + c0 / 8 + a;
-                    if (y < ix.y_lim && x < ix.x_lim)
-                        out[p.pair_base ? p.pair_base[y] + x : (uint64_t)y * p.out_ld + x] = f;
+                    if (y < ix.y_lim && x < ix.x_lim) out[(k ? ob_w[1] : ob_w[0]) + x] = f;
                     if (p.planar_out) {
                         // 4 x 8 byte transpose across the lanes of one y: lane
                         // (xi, a) ends with planes 4(xi&1) + 2(xi>>1) + {0, 1}
@@ -290,12 +327,13 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     }
                 }
                 // remaining columns (w_tile not a multiple of 64): 16 at a time
-                for (uint32_t c0 = wide + 16 * half; c0 < p.w_tile; c0 += 32) {
+                for (uint32_t c0 = wide + 16 * half, k = 0; c0 < p.w_tile; c0 += 32, ++k) {
                     uint32_t v[16];
                     tmem_ld16(taddr + c0, v);
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         const uint32_t y = ybase + c0 / 8 + h;
+                        const uint64_t ob = k ? ob_r[1][h] : ob_r[0][h];
                         uint64_t lo = 0, hi = 0;
 #pragma unroll
                         for (int b = 0; b < 4; ++b) {
@@ -311,8 +349,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         packed |= __shfl_xor_sync(FULLMASK, packed, 8);
                         packed |= __shfl_xor_sync(FULLMASK, packed, 16);
                         if (y < ix.y_lim) {
-                            if (a == 0 && x < ix.x_lim)
-                                out[p.pair_base ? p.pair_base[y] + x : (uint64_t)y * p.out_ld + x] = f;
+                            if (a == 0 && x < ix.x_lim) out[ob + x] = f;
                             if (p.planar_out && lane < 8 && x4 < ix.x_lim)
                                 *reinterpret_cast<uint32_t*>(p.planar_out + ((uint64_t)y * 8 + lane) * p.planar_ld +
                                                              x4) = packed;
@@ -323,11 +360,13 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 const uint32_t x = ix.x0 + q * 32 + lane;
                 const bool xv = x < ix.x_lim;
                 const uint64_t corr = xv ? p.corr[x] : 0;
-                for (uint32_t c0 = 64 * half; c0 < wide; c0 += 128) {
+                for (uint32_t c0 = 64 * half, k = 0; c0 < wide; c0 += 128, ++k) {
                     uint32_t v[64];
                     tmem_ld64(taddr + c0, v);
+                    const uint64_t obk = k ? ob_w[1] : ob_w[0];
 #pragma unroll
                     for (int yy = 0; yy < 8; ++yy) {
+                        const uint64_t ob = __shfl_sync(FULLMASK, obk, yy);
                         int64_t lo = 0, hi = 0;
 #pragma unroll
                         for (int b = 0; b < 4; ++b) {
@@ -337,16 +376,15 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         const uint64_t lr = lo < 0 ? (uint64_t)(lo + (int64_t)P) : (uint64_t)lo;
                         const uint64_t hr = hi < 0 ? (uint64_t)(hi + (int64_t)P) : (uint64_t)hi;
                         const uint32_t y = ybase + c0 / 8 + yy;
-                        if (xv && y < ix.y_lim)
-                            p.out[p.pair_base ? p.pair_base[y] + x : (uint64_t)y * p.out_ld + x] =
-                                add_mod(canon(lr + rotl61(hr, 32)), corr);
+                        if (xv && y < ix.y_lim) p.out[ob + x] = add_mod(canon(lr + rotl61(hr, 32)), corr);
                     }
                 }
-                for (uint32_t c0 = wide + 16 * half; c0 < p.w_tile; c0 += 32) {
+                for (uint32_t c0 = wide + 16 * half, k = 0; c0 < p.w_tile; c0 += 32, ++k) {
                     uint32_t v[16];
                     tmem_ld16(taddr + c0, v);
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
+                        const uint64_t ob = k ? ob_r[1][h] : ob_r[0][h];
                         int64_t lo = 0, hi = 0;
 #pragma unroll
                         for (int b = 0; b < 4; ++b) {
@@ -356,9 +394,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         const uint64_t lr = lo < 0 ? (uint64_t)(lo + (int64_t)P) : (uint64_t)lo;
                         const uint64_t hr = hi < 0 ? (uint64_t)(hi + (int64_t)P) : (uint64_t)hi;
                         const uint32_t y = ybase + c0 / 8 + h;
-                        if (xv && y < ix.y_lim)
-                            p.out[p.pair_base ? p.pair_base[y] + x : (uint64_t)y * p.out_ld + x] =
-                                add_mod(canon(lr + rotl61(hr, 32)), corr);
+                        if (xv && y < ix.y_lim) p.out[ob + x] = add_mod(canon(lr + rotl61(hr, 32)), corr);
                     }
                 }
             }
