@@ -580,9 +580,9 @@ def run_serving(args, flat, ivf, flat_L, data, dist):
                               [iseeds[i]], args.trials, 10)
         ref_i.append((h[0][0], h[0][1], int(ft[0])))
     srv = capi.Server(flat, ivf, max_batch=64, slots=4, mem_budget=24 << 30, max_wait_us=1000, trials=args.trials,
-                      k=10, block_min=8)
+                      k=10, block_min=2)
     out = {"corpora": {"flat_N": flat.m, "ivf_N": int(data["offsets"][-1]), "nlist": int(len(data["sizes"]))},
-           "config": {"max_batch": 64, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 8},
+           "config": {"max_batch": 64, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 2},
            "mix": "50% flat / 50% IVF, nprobe uniform in {8, 32, 128}", "rates": {}}
     for rate in [float(r) for r in args.serve_rates.split(",") if r]:
         n = int(min(max(rate * args.serve_seconds, 200), 8000))

@@ -35,7 +35,7 @@ struct ItemIdx {
 };
 __device__ __forceinline__ ItemIdx grid_item(const BgParams& p, uint32_t kp, uint32_t ta, uint32_t tw) {
     const uint32_t x0 = p.mode == BG_S8 ? ta * BG_AROWS : ta * (BG_AROWS / 8);
-    return ItemIdx{kp, tw, ta * BG_AROWS, tw * p.w_tile, x0, p.x_count, tw * p.w_tile / 8, p.y_count};
+    return ItemIdx{kp, tw, p.a_blocked ? ta : ta * BG_AROWS, tw * p.w_tile, x0, p.x_count, tw * p.w_tile / 8, p.y_count};
 }
 __device__ __forceinline__ ItemIdx item_idx(const BgParams& p, uint32_t item) {
     const uint32_t per = p.a_tiles * p.w_tiles;
@@ -106,6 +106,13 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
     const uint32_t a_slots = p.a_resident ? p.k_bytes / BG_KSTEP : 0;
     const uint32_t base = sbase + a_slots * A_BYTES;  // stage ring
     uint8_t* ring = sptr + a_slots * A_BYTES;
+    // TMA coordinates of A's K step at byte k: row-major (x = k, y = row), or
+    // K-blocked (x = 0, y = (tile * K steps + k / 128) * 128)
+    const uint32_t a_ksteps = p.k_bytes / BG_KSTEP;
+    auto a_x = [&](uint32_t k) -> int { return p.a_blocked ? 0 : (int)k; };
+    auto a_row = [&](const ItemIdx& ix, uint32_t k) -> int {
+        return p.a_blocked ? (int)((ix.a_y * a_ksteps + k / BG_KSTEP) * BG_AROWS) : (int)ix.a_y;
+    };
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < stages; ++s) {
@@ -160,7 +167,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                             break;
                         }
                         bar_expect_tx(&afull_b[ks], A_BYTES);
-                        tma_2d(sptr + ks * A_BYTES, &tmap_a, (int)k, (int)ix.a_y, &afull_b[ks]);
+                        tma_2d(sptr + ks * A_BYTES, &tmap_a, a_x(k), a_row(ix, k), &afull_b[ks]);
                         t_last = t;
                     }
                     const uint32_t st = (uint32_t)(it % stages);
@@ -177,7 +184,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                         tma_2d(sb, &tmap_w, (int)k, (int)ix.w_y, &full_b[st]);
                     } else {
                         bar_expect_tx(&full_b[st], A_BYTES + w_bytes);
-                        tma_2d(sb, &tmap_a, (int)k, (int)ix.a_y, &full_b[st]);
+                        tma_2d(sb, &tmap_a, a_x(k), a_row(ix, k), &full_b[st]);
                         tma_2d(sb + A_BYTES, &tmap_w, (int)k, (int)ix.w_y, &full_b[st]);
                     }
                 }
@@ -275,7 +282,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 const uint32_t a = lane & 7, xi = lane >> 3;
                 const uint32_t x4 = ix.x0 + q * 4;  // first x of this warp
                 const uint32_t x = x4 + xi;
-                const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+                const uint32_t w1 = 8 * a;
                 uint64_t* out = p.out + (uint64_t)ix.kp * p.out_pstride;
                 for (uint32_t c0 = 64 * half, k = 0; c0 < wide; c0 += 128, ++k) {
                     uint32_t v[64];
@@ -289,7 +296,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                             lo += (uint64_t)v[8 * yy + b] << (8 * b);
                             hi += (uint64_t)v[8 * yy + 4 + b] << (8 * b);
                         }
-                        part[yy] = canon(rotl61(lo, w1) + rotl61(hi, w2));
+                        part[yy] = fold(rotl61(lo + rotl61(hi, 32), w1));  // < 2^61 + 8: 8 sum below 2^64
                     }
                     // butterfly over the 8 lanes of one x: each level halves the
                     // y values a lane carries; lane a ends with y = a
@@ -340,7 +347,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                             lo += (uint64_t)v[8 * h + b] << (8 * b);
                             hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
                         }
-                        uint64_t f = canon(rotl61(lo, w1) + rotl61(hi, w2));
+                        uint64_t f = fold(rotl61(lo + rotl61(hi, 32), w1));
                         f += __shfl_xor_sync(FULLMASK, f, 1);
                         f += __shfl_xor_sync(FULLMASK, f, 2);
                         f += __shfl_xor_sync(FULLMASK, f, 4);
@@ -412,8 +419,18 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
 }
 
 // ------------------------------------------------------------------ layouts and operands
+// Byte offset of byte column c of row pr in a K-blocked operand: tiles of 128
+// rows, each stored as its ks K-steps of 128 rows x 128 bytes, so that every
+// (tile, K-step) TMA box is one contiguous 16 KB run.
+__device__ __forceinline__ uint64_t blk_off(uint64_t pr, uint32_t c, uint32_t ks) {
+    return ((((pr >> 7) * ks + (c >> 7)) << 7) + (pr & 127)) * 128 + (c & 127);
+}
+
+// Byte planes of rows of src: row i's byte a lands in row (prow[i] or i) * 8 + a,
+// row-major with dst_ld (ks = 0) or K-blocked with ks K-steps per tile.
 __global__ void planar_rows_kernel(const uint64_t* __restrict__ src, uint64_t rows, uint32_t k, uint64_t src_ld,
-                                   int negate, uint8_t* __restrict__ dst, uint64_t dst_ld, uint32_t col0) {
+                                   int negate, uint8_t* __restrict__ dst, uint64_t dst_ld, uint32_t col0,
+                                   const uint32_t* __restrict__ prow, uint32_t ks) {
     const uint32_t chunks = k / 16;
     const uint64_t total = rows * chunks;
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
@@ -426,18 +443,21 @@ __global__ void planar_rows_kernel(const uint64_t* __restrict__ src, uint64_t ro
             const uint64_t y = s[t];
             x[t] = negate ? (y == 0 ? 0 : P - y) : y;
         }
+        const uint64_t pi = prow ? prow[i] : i;
 #pragma unroll
         for (int a = 0; a < 8; ++a) {
             uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
             for (int t = 0; t < 16; ++t) w[t >> 2] |= (uint32_t)((x[t] >> (8 * a)) & 0xffu) << (8 * (t & 3));
-            *reinterpret_cast<uint4*>(dst + (i * 8 + a) * dst_ld + col0 + jc * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+            uint8_t* d = ks ? dst + blk_off(pi * 8 + a, col0 + jc * 16, ks) : dst + (pi * 8 + a) * dst_ld + col0 + jc * 16;
+            *reinterpret_cast<uint4*>(d) = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
 }
 
 __global__ void planar_cm_kernel(const uint64_t* __restrict__ src_cm, uint64_t rows, uint32_t k,
-                                 uint8_t* __restrict__ dst, uint64_t dst_ld, uint32_t col0) {
+                                 uint8_t* __restrict__ dst, uint64_t dst_ld, uint32_t col0,
+                                 const uint32_t* __restrict__ prow, uint32_t ks) {
     const uint32_t chunks = k / 16;
     const uint64_t total = rows * chunks;
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
@@ -446,18 +466,22 @@ __global__ void planar_cm_kernel(const uint64_t* __restrict__ src_cm, uint64_t r
         uint64_t x[16];
 #pragma unroll
         for (int t = 0; t < 16; ++t) x[t] = src_cm[(uint64_t)(jc * 16 + t) * rows + i];
+        const uint64_t pi = prow ? prow[i] : i;
 #pragma unroll
         for (int a = 0; a < 8; ++a) {
             uint32_t w[4] = {0, 0, 0, 0};
 #pragma unroll
             for (int t = 0; t < 16; ++t) w[t >> 2] |= (uint32_t)((x[t] >> (8 * a)) & 0xffu) << (8 * (t & 3));
-            *reinterpret_cast<uint4*>(dst + (i * 8 + a) * dst_ld + col0 + jc * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+            uint8_t* d = ks ? dst + blk_off(pi * 8 + a, col0 + jc * 16, ks) : dst + (pi * 8 + a) * dst_ld + col0 + jc * 16;
+            *reinterpret_cast<uint4*>(d) = make_uint4(w[0], w[1], w[2], w[3]);
         }
     }
 }
 
+// [M | S] rows as signed bytes, K-blocked (16 K-steps of 128 bytes per
+// 128-row tile), corpus row i at row prow[i] (or i).
 __global__ void ms8_m_kernel(const uint64_t* __restrict__ mp_cm, uint64_t rows, int8_t* __restrict__ dst,
-                             uint32_t* __restrict__ bad) {
+                             uint32_t* __restrict__ bad, const uint32_t* __restrict__ prow) {
     const uint32_t chunks = N / 16;
     const uint64_t total = rows * chunks;
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t)gridDim.x * blockDim.x) {
@@ -472,17 +496,20 @@ __global__ void ms8_m_kernel(const uint64_t* __restrict__ mp_cm, uint64_t rows, 
             w[t >> 2] |= (uint32_t)((uint8_t)(int8_t)sv) << (8 * (t & 3));
         }
         if (out_of_range) atomicOr(bad, 1u);
-        *reinterpret_cast<uint4*>(dst + i * (2 * N) + jc * 16) = make_uint4(w[0], w[1], w[2], w[3]);
+        *reinterpret_cast<uint4*>(dst + blk_off(prow ? prow[i] : i, jc * 16, 2 * N / 128)) =
+            make_uint4(w[0], w[1], w[2], w[3]);
     }
 }
 
 __global__ void ms8_s_kernel(const uint16_t* __restrict__ s_ell, const uint32_t* __restrict__ s_off,
                              const uint16_t* __restrict__ s_w, uint64_t rows, int8_t* __restrict__ dst,
-                             uint64_t* __restrict__ corr, uint32_t* __restrict__ bad) {
+                             uint64_t* __restrict__ corr, uint32_t* __restrict__ bad, const uint32_t* __restrict__ prow) {
     const uint64_t c_mod = canon(0x0101010101010101ull);  // sum_b 2^(8b)
+    constexpr uint32_t KS = 2 * N / 128;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x) {
-        int8_t* row = dst + i * (2 * N) + N;
-        for (uint32_t c = 0; c < N / 16; ++c) reinterpret_cast<uint4*>(row)[c] = make_uint4(0, 0, 0, 0);
+        const uint64_t pi = prow ? prow[i] : i;
+        for (uint32_t c = 0; c < N / 16; ++c)
+            *reinterpret_cast<uint4*>(dst + blk_off(pi, N + 16 * c, KS)) = make_uint4(0, 0, 0, 0);
         const uint64_t slice = i >> 5;
         const uint32_t sl = (uint32_t)(i & 31), off = s_off[slice], wdt = s_w[slice];
         int rs = 0;
@@ -490,9 +517,10 @@ __global__ void ms8_s_kernel(const uint16_t* __restrict__ s_ell, const uint32_t*
             const uint16_t f = s_ell[off + (uint64_t)cc * 32 + sl];
             if (f == 0xffffu) continue;
             const int sgn = (f & 0x8000u) ? -1 : 1;
-            const int nv = (int)row[f & 0x3ffu] + sgn;
+            int8_t* e = dst + blk_off(pi, N + (f & 0x3ffu), KS);
+            const int nv = (int)*e + sgn;
             if (nv < -128 || nv > 127) atomicOr(bad, 1u);
-            row[f & 0x3ffu] = (int8_t)nv;
+            *e = (int8_t)nv;
             rs += sgn;
         }
         const uint64_t m = mul_mod((uint64_t)(128 * (rs < 0 ? -rs : rs)), c_mod);
@@ -616,23 +644,26 @@ void launch_bgemm(const CUtensorMap& tmap_a, const CUtensorMap& tmap_w, const Bg
 }
 
 void launch_planar_rows(const uint64_t* d_src, uint64_t rows, uint32_t k, uint64_t src_ld, int negate, uint8_t* d_dst,
-                        uint64_t dst_ld, uint32_t col0, cudaStream_t s) {
+                        uint64_t dst_ld, uint32_t col0, cudaStream_t s, const uint32_t* d_prow, uint32_t ks) {
     if (!rows) return;
     planar_rows_kernel<<<grid_for(rows * (k / 16), 256, 148 * 16), 256, 0, s>>>(d_src, rows, k, src_ld, negate, d_dst,
-                                                                              dst_ld, col0);
+                                                                              dst_ld, col0, d_prow, ks);
 }
 
 void launch_planar_cm(const uint64_t* d_src_cm, uint64_t rows, uint32_t k, uint8_t* d_dst, uint64_t dst_ld,
-                      uint32_t col0, cudaStream_t s) {
+                      uint32_t col0, cudaStream_t s, const uint32_t* d_prow, uint32_t ks) {
     if (!rows) return;
-    planar_cm_kernel<<<grid_for(rows * (k / 16), 256, 148 * 16), 256, 0, s>>>(d_src_cm, rows, k, d_dst, dst_ld, col0);
+    planar_cm_kernel<<<grid_for(rows * (k / 16), 256, 148 * 16), 256, 0, s>>>(d_src_cm, rows, k, d_dst, dst_ld, col0,
+                                                                            d_prow, ks);
 }
 
 void launch_ms8(const uint64_t* d_mp_cm, const uint16_t* d_s_ell, const uint32_t* d_s_off, const uint16_t* d_s_w,
-                uint64_t rows, int8_t* d_dst, uint64_t* d_corr, uint32_t* d_bad, cudaStream_t s) {
+                uint64_t rows, int8_t* d_dst, uint64_t* d_corr, uint32_t* d_bad, cudaStream_t s,
+                const uint32_t* d_prow) {
     if (!rows) return;
-    ms8_m_kernel<<<grid_for(rows * (N / 16), 256, 148 * 16), 256, 0, s>>>(d_mp_cm, rows, d_dst, d_bad);
-    ms8_s_kernel<<<grid_for(rows, 128, 148 * 16), 128, 0, s>>>(d_s_ell, d_s_off, d_s_w, rows, d_dst, d_corr, d_bad);
+    ms8_m_kernel<<<grid_for(rows * (N / 16), 256, 148 * 16), 256, 0, s>>>(d_mp_cm, rows, d_dst, d_bad, d_prow);
+    ms8_s_kernel<<<grid_for(rows, 128, 148 * 16), 128, 0, s>>>(d_s_ell, d_s_off, d_s_w, rows, d_dst, d_corr, d_bad,
+                                                               d_prow);
 }
 
 void launch_w_tv(const uint64_t* d_v, const uint32_t* d_t, const uint32_t* d_t_nnz, uint32_t nq, int8_t* d_dst,

@@ -37,10 +37,10 @@ enum BgMode : int {
     BG_S8 = 1,
 };
 
-// One work item of a grouped GEMM (an item table): the A and W tiles' TMA row
-// coordinates, the corpus rows x in [x0, x_lim) and the output slots y in
-// [y0, y_lim) that the item's outputs may write (outputs go to
-// out[pair_base[y] + x]).  PLANAR: x0 = a_y / 8; S8: x0 = a_y.
+// One work item of a grouped GEMM (an item table): the A tile (its TMA row,
+// or its tile index when A is K-blocked) and the W tile's TMA row, the corpus
+// rows x in [x0, x_lim) and the output slots y in [y0, y_lim) that the item's
+// outputs may write (outputs go to out[pair_base[y] + x]).
 struct BgItem {
     uint32_t a_y, w_y;
     uint32_t x0, x_lim;
@@ -64,6 +64,7 @@ struct BgParams {
     uint64_t planar_ld;
     int order_a_fast;      // work order: 0 = W tile fastest, 1 = A tile fastest
     int a_resident;        // keep each A tile (all of K, one K panel) in shared memory across its W tiles
+    int a_blocked;         // A is K-blocked (launch_planar_rows with ks = k_bytes / 128): a_y = tile index
     // grouped mode (nullable): work items from a table instead of the a_tiles x
     // w_tiles grid (one K panel, no A-resident mode, no planar_out)
     const BgItem* item_tab;
@@ -83,18 +84,25 @@ uint32_t bgemm_max_stages(const BgParams& p);
 uint32_t bgemm_stage_bytes(uint32_t w_tile, bool a_resident);
 uint32_t bgemm_smem_bytes(const BgParams& p, uint32_t stages);
 
-// Byte planes of a row-major u64 matrix: dst[(i*8 + a) * dst_ld + col0 + j] =
-// byte a of (negate ? p - src : src)[i * src_ld + j], j < k (k % 16 == 0).
+// Byte planes of a row-major u64 matrix: byte a of (negate ? p - src :
+// src)[i * src_ld + j], j < k (k % 16 == 0), goes to plane row r = pi * 8 + a
+// (pi = d_prow[i], or i when d_prow is null), column col0 + j: row-major at
+// dst[r * dst_ld + col0 + j] (ks = 0), or K-blocked (ks > 0: tiles of 128
+// plane rows stored as ks runs of 128 rows x 128 bytes, the layout of the
+// corpus-side A operands, whose every (tile, K-step) TMA box is contiguous).
 void launch_planar_rows(const uint64_t* d_src, uint64_t rows, uint32_t k, uint64_t src_ld, int negate, uint8_t* d_dst,
-                        uint64_t dst_ld, uint32_t col0, cudaStream_t s);
+                        uint64_t dst_ld, uint32_t col0, cudaStream_t s, const uint32_t* d_prow = nullptr,
+                        uint32_t ks = 0);
 // Same from a column-major source: element (i, j) at src_cm[j * rows + i].
 void launch_planar_cm(const uint64_t* d_src_cm, uint64_t rows, uint32_t k, uint8_t* d_dst, uint64_t dst_ld,
-                      uint32_t col0, cudaStream_t s);
-// [M | S] as signed bytes, row-major [rows][2n]: M from mp_cm (residues of
+                      uint32_t col0, cudaStream_t s, const uint32_t* d_prow = nullptr, uint32_t ks = 0);
+// [M | S] as signed bytes, 2n per row, K-blocked (16 K-steps per 128-row
+// tile), corpus row i at row d_prow[i] (or i): M from mp_cm (residues of
 // values in [-128, 127], else *bad |= 1), S from the sliced ELL; corr[i] =
 // 128 * rowsum(S_i) * (2^64 - 1) / 255 mod p.
 void launch_ms8(const uint64_t* d_mp_cm, const uint16_t* d_s_ell, const uint32_t* d_s_off, const uint16_t* d_s_w,
-                uint64_t rows, int8_t* d_dst, uint64_t* d_corr, uint32_t* d_bad, cudaStream_t s);
+                uint64_t rows, int8_t* d_dst, uint64_t* d_corr, uint32_t* d_bad, cudaStream_t s,
+                const uint32_t* d_prow = nullptr);
 // W operand of the signed decode GEMM for nq queries: rows (q, b) of 2n
 // bytes: [T_q if b == 0 else 0 | byte b of v_q - 128].  T entries as in
 // DecodeQuery (col | 0x80000000 for -1); *bad |= 2 when a column sum leaves

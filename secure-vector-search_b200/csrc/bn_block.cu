@@ -70,8 +70,9 @@ int tmap(CUtensorMap* m, const void* base, uint64_t inner, uint64_t rows, uint32
     return BN_OK;
 }
 
-// Byte-planar operands of the corpus (once per handle).
-int block_prepare_locked(Engine& e) {
+// Byte-planar operands of the corpus (once per handle), K-blocked, each list
+// (the whole corpus when offsets is null) starting on a tile boundary.
+int block_prepare_locked(Engine& e, const std::vector<uint64_t>* offsets) {
     Corpus& c = e.c;
     if (c.block_ready) return BN_OK;
     if (!c.client) return fail(BN_EUNSUPPORTED, "block scoring needs the client state (attach_client was not called)");
@@ -80,20 +81,61 @@ int block_prepare_locked(Engine& e) {
     CU(cudaSetDevice(e.ctx->device));
     const uint64_t rows = c.rows;
     c.k_alh = (uint32_t)align_up(2ull * c.n1, 128);
-    TRY(c.mp8.alloc(e.ctx, rows * 8 * N));
-    TRY(c.alh8.alloc(e.ctx, rows * 8 * c.k_alh));
-    TRY(c.ms8.alloc(e.ctx, rows * 2 * N));
+    // padded rows: list l's rows at list_p16[l] + i (16-row tiles of the
+    // planes) and list_p128[l] + i (128-row tiles of [M | S])
+    const std::vector<uint64_t> whole{0, rows};
+    const std::vector<uint64_t>& off = offsets ? *offsets : whole;
+    const size_t nl = off.size() - 1;
+    c.list_p16.assign(nl, 0);
+    c.list_p128.assign(nl, 0);
+    std::vector<uint32_t> prow16, prow128;
+    if (nl > 1) {
+        prow16.resize(rows);
+        prow128.resize(rows);
+    }
+    uint64_t p16 = 0, p128 = 0;
+    for (size_t l = 0; l < nl; ++l) {
+        const uint64_t r0 = off[l], m = off[l + 1] - r0;
+        c.list_p16[l] = p16;
+        c.list_p128[l] = p128;
+        if (nl > 1)
+            for (uint64_t i = 0; i < m; ++i) {
+                prow16[r0 + i] = (uint32_t)(p16 + i);
+                prow128[r0 + i] = (uint32_t)(p128 + i);
+            }
+        p16 += align_up(m, 16);
+        p128 += align_up(m, 128);
+    }
+    if (p128 >= (1ull << 31) / 16) return fail(BN_EUNSUPPORTED, "corpus too large for block scoring");
+    c.rows16 = p16;
+    c.rows128 = p128;
+    TRY(c.mp8.alloc(e.ctx, c.rows16 * 8 * N));
+    TRY(c.alh8.alloc(e.ctx, c.rows16 * 8 * c.k_alh));
+    TRY(c.ms8.alloc(e.ctx, c.rows128 * 2 * N));
     TRY(c.corr.alloc(e.ctx, rows * 8));
-    DevMem bad;
+    DevMem bad, d_p16, d_p128;
     TRY(bad.alloc(e.ctx, 4));
     cudaStream_t s = e.stream;
+    const uint32_t* pr16 = nullptr;
+    const uint32_t* pr128 = nullptr;
+    if (nl > 1) {
+        TRY(d_p16.alloc(e.ctx, rows * 4));
+        TRY(d_p128.alloc(e.ctx, rows * 4));
+        CU(cudaMemcpyAsync(d_p16.p, prow16.data(), rows * 4, cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(d_p128.p, prow128.data(), rows * 4, cudaMemcpyHostToDevice, s));
+        pr16 = d_p16.at<uint32_t>();
+        pr128 = d_p128.at<uint32_t>();
+    }
     CU(cudaMemsetAsync(bad.p, 0, 4, s));
-    if (c.k_alh != 2 * c.n1) CU(cudaMemsetAsync(c.alh8.p, 0, c.alh8.bytes, s));
-    launch_planar_rows(c.m_enc.at<uint64_t>(), rows, N, N, 0, c.mp8.at<uint8_t>(), N, 0, s);
-    launch_planar_cm(c.al_cm.at<uint64_t>(), rows, c.n1, c.alh8.at<uint8_t>(), c.k_alh, 0, s);
-    launch_planar_cm(c.h_cm.at<uint64_t>(), rows, c.n1, c.alh8.at<uint8_t>(), c.k_alh, c.n1, s);
+    // pad rows (and pad columns of [AL | H]) stay zero
+    CU(cudaMemsetAsync(c.mp8.p, 0, c.mp8.bytes, s));
+    CU(cudaMemsetAsync(c.alh8.p, 0, c.alh8.bytes, s));
+    CU(cudaMemsetAsync(c.ms8.p, 0, c.ms8.bytes, s));
+    launch_planar_rows(c.m_enc.at<uint64_t>(), rows, N, N, 0, c.mp8.at<uint8_t>(), 0, 0, s, pr16, N / BG_KSTEP);
+    launch_planar_cm(c.al_cm.at<uint64_t>(), rows, c.n1, c.alh8.at<uint8_t>(), 0, 0, s, pr16, c.k_alh / BG_KSTEP);
+    launch_planar_cm(c.h_cm.at<uint64_t>(), rows, c.n1, c.alh8.at<uint8_t>(), 0, c.n1, s, pr16, c.k_alh / BG_KSTEP);
     launch_ms8(c.mp_cm.at<uint64_t>(), c.s_ell.at<uint16_t>(), c.s_off.at<uint32_t>(), c.s_w.at<uint16_t>(), rows,
-               c.ms8.at<int8_t>(), c.corr.at<uint64_t>(), bad.at<uint32_t>(), s);
+               c.ms8.at<int8_t>(), c.corr.at<uint64_t>(), bad.at<uint32_t>(), s, pr128);
     CU(cudaGetLastError());
     uint32_t hb = 0;
     CU(cudaMemcpyAsync(&hb, bad.p, 4, cudaMemcpyDeviceToHost, s));
@@ -106,9 +148,10 @@ int block_prepare_locked(Engine& e) {
         return fail(BN_EUNSUPPORTED,
                     "block scoring needs m_plain entries and S row entries in [-128, 127] (int8-quantised corpus)");
     }
-    TRY(tmap(&c.tmap_mp, c.mp8.p, N, rows * 8, 128, "m_enc planes"));
-    TRY(tmap(&c.tmap_alh, c.alh8.p, c.k_alh, rows * 8, 128, "[AL | H] planes"));
-    TRY(tmap(&c.tmap_ms, c.ms8.p, 2 * N, rows, 128, "[M | S] bytes"));
+    // K-blocked: rows of 128 bytes, one (tile, K step) box = 128 consecutive rows
+    TRY(tmap(&c.tmap_mp, c.mp8.p, BG_KSTEP, c.mp8.bytes / BG_KSTEP, 128, "m_enc planes"));
+    TRY(tmap(&c.tmap_alh, c.alh8.p, BG_KSTEP, c.alh8.bytes / BG_KSTEP, 128, "[AL | H] planes"));
+    TRY(tmap(&c.tmap_ms, c.ms8.p, BG_KSTEP, c.ms8.bytes / BG_KSTEP, 128, "[M | S] bytes"));
     c.block_ready = true;
     return BN_OK;
 }
@@ -126,6 +169,7 @@ BgParams g1_params(const BlockPlan& b, const Corpus& c) {
     p.out_ld = b.nld;
     p.order_a_fast = (int)b.order;
     p.a_resident = (int)b.a_res;
+    p.a_blocked = 1;
     p.planar_ld = b.npad;
     return p;
 }
@@ -280,11 +324,11 @@ uint64_t block_layout(BlockPlan& b, uint32_t n1, uint32_t k_alh, bool verify_onl
     return L.off + 1024;
 }
 
-int block_prepare_engine(Engine& e) { return block_prepare_locked(e); }
+int block_prepare_engine(Engine& e, const std::vector<uint64_t>* offsets) { return block_prepare_locked(e, offsets); }
 
 int block_prepare(bn_flat* f) {
     std::lock_guard<std::mutex> g(f->e.mu);
-    return block_prepare_locked(f->e);
+    return block_prepare_locked(f->e, nullptr);
 }
 
 int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint32_t flags, BlockPlan** out) {
@@ -295,7 +339,7 @@ int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint3
     if (!f->m) return fail(BN_EINVAL, "empty corpus");
     const bool verify_only = (flags & BLOCK_VERIFY_ONLY) != 0;  // Protocol 2 over claimed r: no planar corpus needed
     std::lock_guard<std::mutex> g(f->e.mu);
-    if (!verify_only) TRY(block_prepare_locked(f->e));
+    if (!verify_only) TRY(block_prepare_locked(f->e, nullptr));
     Corpus& c = f->e.c;
     auto* b = new BlockPlan();
     b->h = f;
@@ -493,6 +537,7 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     q.out_ld = b.nld;
     q.corr = c.corr.at<uint64_t>();
     q.order_a_fast = (int)b.order;
+    q.a_blocked = 1;
     launch_bgemm(c.tmap_ms, b.tm_tv, q, stages_for(q), sms, err, s);
     // Mv = r + f2 - f3 (written over f3 when asked for), fp_to_signed, top-k
     if (b.k || want_mv) {

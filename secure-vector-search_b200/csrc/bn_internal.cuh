@@ -138,11 +138,16 @@ struct Corpus {
     CUtensorMap tmap_m;  // m_enc as bytes {8192, rows}, 128x128 boxes, 128-byte swizzle
 
     // Byte-planar operands of block scoring (built on first use, see
-    // bn_block.cu): m_enc planes [rows*8][1024], [AL | H] planes
-    // [rows*8][k_alh], [M | S] as signed bytes [rows][2048], corr[rows].
+    // bn_block.cu), K-blocked for the GEMMs' A operand: m_enc planes
+    // (rows16 * 8 plane rows x 1024 bytes), [AL | H] planes (rows16 * 8 x
+    // k_alh), [M | S] as signed bytes (rows128 x 2048), corr[rows].  Each
+    // list starts on a tile boundary: list c's rows sit at padded rows
+    // list_p16[c] (16-row plane tiles) and list_p128[c] (128-row tiles).
     bool block_ready = false;
     DevMem mp8, alh8, ms8, corr;
     uint32_t k_alh = 0;
+    uint64_t rows16 = 0, rows128 = 0;
+    std::vector<uint64_t> list_p16, list_p128;
     CUtensorMap tmap_mp, tmap_alh, tmap_ms;
 
     uint64_t bytes() const {
@@ -343,8 +348,9 @@ int block_query_launch(BlockPlan& b, uint32_t nq, const uint64_t* v_enc, const u
 int block_query_finish(BlockPlan& b, uint32_t nq, uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed);
 uint64_t block_plan_bytes(const BlockPlan* b);
 uint64_t block_plan_estimate(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k);
-// Byte-planar corpus copies of block scoring (once per handle; caller holds e.mu).
-int block_prepare_engine(Engine& e);
+// Byte-planar corpus copies of block scoring (once per handle; caller holds
+// e.mu); offsets (nullable): the IVF list boundaries.
+int block_prepare_engine(Engine& e, const std::vector<uint64_t>* offsets);
 int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms);
 int validate_residues(const uint64_t* a, uint64_t count, const char* what);
 int block_verify_host(BlockPlan& b, const uint64_t* r, const uint64_t* v_enc, const uint8_t* seed, int32_t* failed,

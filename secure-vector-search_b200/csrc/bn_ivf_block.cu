@@ -65,6 +65,7 @@ struct IvGroup {
     uint32_t row0, m;       // corpus rows of the list
     uint32_t lp0, n;        // its pairs, list-major
     uint32_t it_pl, it_s8;  // first item of the PLANAR (16-row A tiles) and S8 (128-row A tiles) tables
+    uint32_t t16, t128;     // the list's first tile in the K-blocked planes / [M | S] bytes
 };
 
 // A list of several z panels: z[m][t][j] = sum of its panels' z_part[p][t][j].
@@ -104,8 +105,8 @@ __global__ void expand_items_kernel(const IvGroup* __restrict__ groups, uint32_t
     const uint32_t rows_per = s8 ? (uint32_t)BG_AROWS : (uint32_t)BG_AROWS / 8;
     const uint32_t xt = (g.m + rows_per - 1) / rows_per;
     const uint32_t local = it - (s8 ? g.it_s8 : g.it_pl);
-    const uint32_t x0 = g.row0 + (local % xt) * rows_per, y0 = g.lp0 + (local / xt) * wy;
-    const BgItem item{s8 ? x0 : 8 * x0, 8 * y0, x0, g.row0 + g.m, y0, g.lp0 + g.n};
+    const uint32_t xi = local % xt, x0 = g.row0 + xi * rows_per, y0 = g.lp0 + (local / xt) * wy;
+    const BgItem item{(s8 ? g.t128 : g.t16) + xi, 8 * y0, x0, g.row0 + g.m, y0, g.lp0 + g.n};
     if (s8) items_s8[it] = item;
     else items_pl[it] = item;
 }
@@ -379,7 +380,10 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
         IvPair& pr = j.pairs[i];
         if (lp == 0 || j.pairs[j.order[lp - 1]].list != pr.list) {
             const uint32_t m = (uint32_t)(v.offsets[pr.list + 1] - v.offsets[pr.list]);
-            j.groups.push_back(IvGroup{(uint32_t)v.offsets[pr.list], m, lp, 0, 0, 0});
+            const bool tiles = !c.list_p16.empty();  // K-blocked copies exist (not needed to verify only)
+            j.groups.push_back(IvGroup{(uint32_t)v.offsets[pr.list], m, lp, 0, 0, 0,
+                                       tiles ? (uint32_t)(c.list_p16[pr.list] / 16) : 0u,
+                                       tiles ? (uint32_t)(c.list_p128[pr.list] / 128) : 0u});
             j.block0.push_back(nb);
             nb += (m + TC_ROWS - 1) / TC_ROWS;
         }
@@ -410,6 +414,7 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     // grouped GEMM item counts (the tables themselves are expanded on the device)
     j.n_pl = j.n_s8 = 0;
     if (!verify_only && j.P) {
+        if (c.list_p16.size() != v.nlist) return fail(BN_EINVAL, "block scoring copies are not prepared");
         j.w_tile = pick_w_tile(j.groups);
         const uint32_t wy = j.w_tile / 8;  // pairs per W tile
         for (IvGroup& g : j.groups) {
@@ -636,6 +641,7 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             p.item_tab = reinterpret_cast<const BgItem*>(d + j.o_items_pl);
             p.n_items = j.n_pl;
             p.pair_base = U64(j.o_base);
+            p.a_blocked = 1;
             launch_bgemm(c.tmap_mp, j.tm_wv, p, j.st_g1, sms, err, s);
             mark(2);
             p.k_bytes = p.k_panel = c.k_alh;
@@ -728,7 +734,7 @@ int ivf_block_finish(const IvfBlockJob& j, const PinnedMem& host, uint32_t* ids,
 
 int ivf_block_prepare(bn_ivf* v) {
     std::lock_guard<std::mutex> g(v->e.mu);
-    return block_prepare_engine(v->e);
+    return block_prepare_engine(v->e, &v->offsets);
 }
 
 }  // namespace api
@@ -764,7 +770,7 @@ int bn_ivf_query_block(bn_ivf* v, uint32_t B, uint32_t nprobe, const uint32_t* p
     std::lock_guard<std::mutex> gd(v->e.mu);
     Engine& e = v->e;
     if (!e.c.client) return fail(BN_EUNSUPPORTED, "this handle has no client state (attach_client was not called)");
-    TRY(block_prepare_engine(e));
+    TRY(block_prepare_engine(e, &v->offsets));
     const auto t0 = std::chrono::steady_clock::now();
     const std::vector<uint32_t> off = fixed_probe_off(B, nprobe);
     IvfBlockJob j;

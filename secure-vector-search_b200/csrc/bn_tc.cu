@@ -100,6 +100,7 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
 }
 
 // ------------------------------------------------------------------ GEMM + drain
+
 constexpr int TC_THREADS = 320;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 constexpr uint32_t STRIP_BYTES = TC_ROWS * 128;  // one 128x128 M box
 constexpr int TC_EPI_WARPS = 8;                // TMEM drain warps: 2 per lane quarter
@@ -112,13 +113,48 @@ constexpr int TC_EPI_WARPS = 8;                // TMEM drain warps: 2 per lane q
 // then a butterfly over the 8 lanes of one element leaves lane a with trial
 // c0/8 + a's sum; 16-column remainders use a plain 3-level reduction.
 // z_out[t * N + j] receives z_t[j] for t < t_cnt.
+// (lo + hi 2^32) 2^w mod p, folded below 2^61 + 8 (so 8 of them sum below
+// 2^64): lo, hi < 2^56 (byte sums of s32 accumulators), 0 <= w < 61.
+__device__ __forceinline__ uint64_t fold_part(uint64_t lo, uint64_t hi, uint32_t w) {
+    return fold(rotl61(lo + rotl61(hi, 32), w));
+}
+
+// One 32-column chunk (4 trials) of a strip: two butterfly levels leave
+// lanes a and a ^ 1 with trial c0/8 + 2 (a >> 2 & 1) + (a >> 1 & 1).
+__device__ __forceinline__ void z_drain32(uint32_t taddr, uint32_t lane, uint32_t j, uint32_t c0, uint32_t t_cnt,
+                                          uint64_t* __restrict__ z_out) {
+    const uint32_t a = lane & 7;
+    const bool b2 = (a & 4) != 0, b1 = (a & 2) != 0;
+    uint32_t v[32];
+    tmem_ld32(taddr, v);
+    uint64_t part[4];
+#pragma unroll
+    for (int tt = 0; tt < 4; ++tt) {
+        uint64_t lo = 0, hi = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            lo += (uint64_t)v[8 * tt + b] << (8 * b);
+            hi += (uint64_t)v[8 * tt + 4 + b] << (8 * b);
+        }
+        part[tt] = fold_part(lo, hi, 8 * a);
+    }
+    uint64_t k2[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+        k2[i] = (b2 ? part[i + 2] : part[i]) + __shfl_xor_sync(FULLMASK, b2 ? part[i] : part[i + 2], 4);
+    uint64_t k1 = (b1 ? k2[1] : k2[0]) + __shfl_xor_sync(FULLMASK, b1 ? k2[0] : k2[1], 2);
+    k1 += __shfl_xor_sync(FULLMASK, k1, 1);
+    const uint32_t t = c0 / 8 + (b2 ? 2u : 0u) + (b1 ? 1u : 0u);
+    if ((a & 1) == 0 && t < t_cnt) z_out[(uint64_t)t * N + j] = canon(k1);
+}
+
 // One 64-column chunk (8 trials) of a strip: lane (xi, a) folds its 8
 // trials' byte products to (lo + hi 2^32) 2^(8a) mod p, a butterfly over the
 // 8 lanes of one element leaves lane a with trial c0/8 + a's sum.
 __device__ __forceinline__ void z_drain64(uint32_t taddr, uint32_t lane, uint32_t j, uint32_t c0, uint32_t t_cnt,
                                           uint64_t* __restrict__ z_out) {
     const uint32_t a = lane & 7;
-    const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+    const uint32_t w1 = 8 * a;
     const bool b2 = (a & 4) != 0, b1 = (a & 2) != 0, b0 = (a & 1) != 0;
     uint32_t v[64];
     tmem_ld64(taddr, v);
@@ -131,7 +167,7 @@ __device__ __forceinline__ void z_drain64(uint32_t taddr, uint32_t lane, uint32_
             lo += (uint64_t)v[8 * tt + b] << (8 * b);
             hi += (uint64_t)v[8 * tt + 4 + b] << (8 * b);
         }
-        part[tt] = canon(rotl61(lo, w1) + rotl61(hi, w2));
+        part[tt] = fold_part(lo, hi, w1);
     }
     uint64_t k4[4], k2[2];
 #pragma unroll
@@ -149,7 +185,7 @@ __device__ __forceinline__ void z_drain64(uint32_t taddr, uint32_t lane, uint32_
 __device__ __forceinline__ void z_drain16(uint32_t taddr, uint32_t lane, uint32_t j, uint32_t c0, uint32_t t_cnt,
                                           uint64_t* __restrict__ z_out) {
     const uint32_t a = lane & 7;
-    const uint32_t w1 = 8 * a, w2 = (8 * a + 32) % 61;
+    const uint32_t w1 = 8 * a;
     uint32_t v[16];
     tmem_ld16(taddr, v);
 #pragma unroll
@@ -161,7 +197,7 @@ __device__ __forceinline__ void z_drain16(uint32_t taddr, uint32_t lane, uint32_
             lo += (uint64_t)v[8 * h + b] << (8 * b);
             hi += (uint64_t)v[8 * h + 4 + b] << (8 * b);
         }
-        uint64_t zc = canon(rotl61(lo, w1) + rotl61(hi, w2));
+        uint64_t zc = fold_part(lo, hi, w1);
         zc += __shfl_xor_sync(FULLMASK, zc, 1);
         zc += __shfl_xor_sync(FULLMASK, zc, 2);
         zc += __shfl_xor_sync(FULLMASK, zc, 4);
@@ -252,7 +288,7 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
                         for (uint32_t s = 0; s < sg; ++s)
                             tma_2d(sb + s * STRIP_BYTES, &tmap_m, (int)((g * S + s) * 128), (int)(pn.row0 + rb * TC_ROWS),
                                    &full_b[st]);
-                        if (u_flat)
+                            if (u_flat)
                             tma_2d(sb + u_off, &tmap_u, (int)((pn.rb0 + rb) * TC_ROWS), 0, &full_b[st]);
                         else
                             tma_2d(sb + u_off, &tmap_u, 0, (int)((pn.rb0 + rb) * n_rows), &full_b[st]);
@@ -343,12 +379,14 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
 // stay there while the panel's 64 strips of m_enc stream through the stage
 // ring, one strip per item, into three rotating TMEM accumulators (3 x n_rows
 // <= 480 columns): the drain of a strip overlaps the MMAs of the next two.
-// Roles: warp 0 TMA, warp 1 MMA issuer, warps 2-17 drain (4 per lane
-// quarter; a strip's 64- and 16-column chunks are dealt out among them).
+// Roles: warp 0 TMA, warp 1 MMA issuer, warps 2-21 drain (5 per lane
+// quarter; a strip's 32-column chunks, and a last 16-column one when n_rows
+// is not a multiple of 32, are dealt out among them: one each at 20 trials).
 // Every mbarrier wait is bounded; on timeout the CTA sets *err and winds down.
 constexpr uint32_t TC_SMALL_RB = TC_SMALL_PANEL_ROWS / TC_ROWS;
 constexpr uint32_t SM_STAGES = 6;
-constexpr int SM_EPI_WARPS = 16;
+constexpr int SM_EPI_WARPS = 20;
+constexpr uint32_t SM_DRAIN_PARTS = SM_EPI_WARPS / 4;
 constexpr int SM_THREADS = 64 + 32 * SM_EPI_WARPS;
 
 __global__ void __launch_bounds__(SM_THREADS, 1)
@@ -494,10 +532,9 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
     } else {
         // ---------------------------------------------------------- drain
         const uint32_t q = (uint32_t)(warp & 3);             // TMEM lane quarter of this warp
-        const uint32_t part = (uint32_t)(warp - 2) >> 2;      // 0..3: its share of each strip's chunks
+        const uint32_t part = (uint32_t)(warp - 2) >> 2;      // its share of each strip's chunks
         const uint32_t jl = q * 4 + (lane >> 3);
-        const uint32_t wide = n_rows & ~63u, nwide = wide / 64;
-        const uint32_t tasks = nwide + (n_rows - wide) / 16;
+        const uint32_t tasks = (n_rows + 31) / 32;            // 32-column chunks (the last may be 16)
         uint64_t sc = 0;
         bool stop = false;
         for (uint32_t w = blockIdx.x; w < npanels && !stop; w += gridDim.x) {
@@ -511,9 +548,9 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
                 tc_after();
                 const uint32_t tbase = tmem + ((q * 32) << 16) + b * n_rows;
                 const uint32_t j = s * 16 + jl;
-                for (uint32_t k = part; k < tasks; k += 4) {
-                    if (k < nwide) z_drain64(tbase + 64 * k, lane, j, 64 * k, t_cnt, z_out);
-                    else z_drain16(tbase + wide + 16 * (k - nwide), lane, j, wide + 16 * (k - nwide), t_cnt, z_out);
+                for (uint32_t k = part; k < tasks; k += SM_DRAIN_PARTS) {
+                    if (32 * k + 32 <= n_rows) z_drain32(tbase + 32 * k, lane, j, 32 * k, t_cnt, z_out);
+                    else z_drain16(tbase + 32 * k, lane, j, 32 * k, t_cnt, z_out);
                 }
                 tc_before();
                 __syncwarp();
