@@ -548,9 +548,22 @@ def run_ivf(args, ctx, dist):
         ivf.block_profile(True)  # one more call with stage events (not part of the timing above)
         ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
         stages = ivf.block_profile_read()
+        # GEMM tilings (W rows per tile, pipeline stages; 0 = automatic): G1 time of each
+        sweep = {}
+        for w_tile, st in ((32, 0), (64, 0), (128, 0), (256, 0), (64, 6)):
+            ivf.block_tune(w_tile, st)
+            ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
+            g1 = []
+            for _ in range(3):
+                ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
+                g1.append(ivf.block_profile_read())
+            sweep[f"w{w_tile}_s{st}"] = {k: round(statistics.median(x[k] for x in g1), 3)
+                                         for k in ("g1_r", "g2_al_h", "g3_m_t_s_v")}
+        ivf.block_tune(0, 0)
         ivf.block_profile(False)
         res["block"] = {"qps": bq / db, "ms_per_batch": db * 1e3, "hits_equal_per_query": bool(same),
-                        "distinct_rows_gbs": rows_u * N_DIM * 8 / db / 1e9, "stages_ms": stages}
+                        "distinct_rows_gbs": rows_u * N_DIM * 8 / db / 1e9, "stages_ms": stages,
+                        "tiling_sweep_ms": sweep}
         out["per_nprobe"][str(nprobe)] = res
     return out, ivf, data
 

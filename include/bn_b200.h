@@ -271,6 +271,10 @@ int bn_ivf_query_block(bn_ivf* h, uint32_t B, uint32_t nprobe, const uint32_t* p
                        const uint64_t* g, const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz,
                        const uint8_t block_seed[32], uint32_t trials, uint32_t k, uint32_t* ids, int64_t* scores,
                        uint32_t* n_hits, int32_t* failed_cluster, int32_t* failed_trial);
+/* GEMM tiling of later block calls (and of a server's IVF block batches):
+ * W rows per tile (a multiple of 16 up to 256; the MMA N) and pipeline stages
+ * (2..=12, capped by shared memory); 0 = chosen per batch from its groups. */
+int bn_ivf_block_tune(bn_ivf* h, uint32_t w_tile, uint32_t stages);
 /* Stage timing of later bn_ivf_query_block calls (enable = 1) and its read:
  * ms[0] = host planning and packing, ms[1..8] = device time of the stages
  * (H2D + operand images, G1, G2, G3, top-k, Protocol 2 passes, z . v and

@@ -96,6 +96,7 @@ _SIGS = {
     "bn_ivf_query": (C.c_int, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
     "bn_ivf_block_prepare": (C.c_int, [vp]),
     "bn_ivf_query_block": (C.c_int, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
+    "bn_ivf_block_tune": (C.c_int, [vp, u32, u32]),
     "bn_ivf_block_profile": (C.c_int, [vp, C.c_int]),
     "bn_ivf_block_profile_read": (C.c_int, [vp, vp, u32, vp]),
     "bn_ivf_verify_block": (C.c_int, [vp, u32, u32, vp, vp, u64, vp, vp, u32, vp, vp, vp, vp]),
@@ -470,6 +471,10 @@ class Ivf:
 
     IVF_BLOCK_STAGES = ("host_plan_pack", "h2d_operand_images", "g1_r", "g2_al_h", "g3_m_t_s_v", "topk",
                         "protocol2_passes", "zv_decide", "d2h")
+
+    def block_tune(self, w_tile=0, stages=0):
+        """GEMM tiling of later block calls: W rows per tile, pipeline stages (0 = automatic)."""
+        check(lib.bn_ivf_block_tune(self.h, w_tile, stages))
 
     def block_profile(self, enable=True):
         check(lib.bn_ivf_block_profile(self.h, 1 if enable else 0))

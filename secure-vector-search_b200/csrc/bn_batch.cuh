@@ -22,7 +22,7 @@ namespace bn {
 
 constexpr int BG_AROWS = 128;              // A rows per work item (TMEM lanes)
 constexpr int BG_KSTEP = 128;              // K bytes per pipeline stage (one 128-byte swizzle atom)
-constexpr int BG_MAX_STAGES = 6;
+constexpr int BG_MAX_STAGES = 12;
 constexpr int BG_MAX_ASLOTS = 8;           // A-resident mode: K <= 8 * 128 bytes
 constexpr uint32_t BG_MAX_SMEM = 232448;   // dynamic shared memory per CTA on sm_100
 constexpr uint32_t BG_MAX_KPANEL = 16384;  // K bytes summed in s32 before a drain: 16384 * 255^2 < 2^31

@@ -318,6 +318,8 @@ struct bn_ivf {
     bn::api::Engine e;
     uint32_t nlist = 0;
     std::vector<uint64_t> offsets;
+    // block GEMM tiling chosen by the caller (bn_ivf_block_tune; 0 = automatic)
+    uint32_t blk_w = 0, blk_stages = 0;
     // stage timing of the host-buffer IVF block entry point (bn_ivf_block_profile)
     static constexpr int PROF_EVENTS = 9;
     bool prof = false, prof_have = false;

@@ -415,7 +415,7 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.n_pl = j.n_s8 = 0;
     if (!verify_only && j.P) {
         if (c.list_p16.size() != v.nlist) return fail(BN_EINVAL, "block scoring copies are not prepared");
-        j.w_tile = pick_w_tile(j.groups);
+        j.w_tile = v.blk_w ? v.blk_w : pick_w_tile(j.groups);
         const uint32_t wy = j.w_tile / 8;  // pairs per W tile
         for (IvGroup& g : j.groups) {
             const uint32_t yt = (g.n + wy - 1) / wy;
@@ -428,6 +428,7 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
         p.w_tile = j.w_tile;
         j.st_g1 = j.st_g2 = j.st_g3 = bgemm_max_stages(p);
         if (!j.st_g1) return fail(BN_EUNSUPPORTED, "no pipeline depth fits W tile %u", j.w_tile);
+        if (v.blk_stages) j.st_g1 = j.st_g2 = j.st_g3 = std::min(j.st_g1, v.blk_stages);
     }
     j.n_rows = pass_rows(std::min<uint32_t>(std::max<uint32_t>(trials, 1), TC_MAX_TRIALS));
     j.ctas = (uint32_t)pick_ctas(j.max_q_rows, std::max<uint32_t>(B, 1), sms);
@@ -782,6 +783,16 @@ int bn_ivf_query_block(bn_ivf* v, uint32_t B, uint32_t nprobe, const uint32_t* p
     CU(cudaStreamSynchronize(e.stream));
     v->prof_have = v->prof;
     return ivf_block_finish(j, e.host, ids, scores, n_hits, failed_cluster, failed_trial);
+}
+
+int bn_ivf_block_tune(bn_ivf* v, uint32_t w_tile, uint32_t stages) {
+    if (!v) return fail(BN_EINVAL, "null handle");
+    if (w_tile && (w_tile % 16 || w_tile > 256)) return fail(BN_EINVAL, "w_tile = %u is not 0 or a multiple of 16 up to 256", w_tile);
+    if (stages && (stages < 2 || stages > BG_MAX_STAGES)) return fail(BN_EINVAL, "stages = %u outside 2..=%d", stages, BG_MAX_STAGES);
+    std::lock_guard<std::mutex> gd(v->e.mu);
+    v->blk_w = w_tile;
+    v->blk_stages = stages;
+    return BN_OK;
 }
 
 int bn_ivf_block_profile(bn_ivf* v, int enable) {
