@@ -51,14 +51,25 @@ struct IvPair {
     uint32_t pad;
 };
 
-// Up to IV_CHUNK_ROWS rows of one pair (u . r partial sums, ids).
+// Up to IV_CHUNK_ROWS rows of one pair (ids; u . r partial sums per chunk).
 struct IvChunk {
     uint64_t r0;    // first r-space entry
     uint64_t row0;  // first corpus row
     uint32_t ublk;  // first 128-row block of the list's U image
     uint32_t rows;
 };
-constexpr uint32_t IV_CHUNK_ROWS = 4096;
+constexpr uint32_t IV_CHUNK_ROWS = 2048;
+
+// u . r work of one CTA: chunk c of a list (its U blocks from ublk0 on) for
+// up to UR_SLAB of the list's pairs (list-major positions lp0 ...).
+struct IvUrTask {
+    uint32_t ublk0, rows;
+    uint32_t lp0, npairs;
+    uint32_t c;
+};
+constexpr uint32_t UR_SLAB = 8;
+constexpr uint32_t UR_WARPS = 8;
+constexpr uint32_t UR_PER_WARP = (UR_SLAB * TC_MAX_TRIALS + UR_WARPS - 1) / UR_WARPS;
 
 // One distinct list of a batch: a group of the grouped GEMMs.
 struct IvGroup {
@@ -125,33 +136,53 @@ __device__ __forceinline__ void mac128(uint64_t& lo, uint64_t& hi, uint64_t a, u
     hi += ph + (lo < pl ? 1u : 0u);
 }
 
-// u_t . r per chunk, for trials [t_base, t_base + t_cnt): the U image of
-// block b (launch_tc_ugen, per-block images) holds byte a of u_t[i] at row
-// (8t + a), column i.  Warp w takes blocks w, w + 4, ...; lane l rows 4l..4l+3
-// of each: it reads one 32-bit word from each of the 8 byte rows of trial t
-// and transposes them into the four u_t values.  At most 8 blocks x 4 rows =
-// 32 products (< 2^122 each) per lane and trial are summed in 128 bits.
-__global__ void __launch_bounds__(128)
-ur_chunks_kernel(const IvChunk* __restrict__ chunks, const uint8_t* __restrict__ ub, uint32_t n_rows, uint32_t t_base,
-                 uint32_t t_cnt, uint32_t trials_total, const uint64_t* __restrict__ r, uint64_t* __restrict__ ur_part) {
-    const IvChunk c = chunks[blockIdx.x];
+// u_t . r for the pairs of one list chunk, trials [t_base, t_base + t_cnt):
+// the chunk's U blocks (launch_tc_ugen, per-block images: byte a of u_t[i] at
+// row 8t + a, column i) are read once each into shared memory and serve every
+// pair of the slab.  Warp w owns the (pair, trial) combos w, w + 8, ... for
+// the whole chunk; lane l takes rows 4l .. 4l + 3 of each block, reads one
+// 32-bit word from each of the 8 byte rows of trial t and transposes them
+// into the four u_t values.  16 blocks x 4 rows = 64 products (< 2^122 each)
+// per lane and combo are summed in 128 bits.
+__global__ void __launch_bounds__(UR_WARPS * 32)
+ur_lists_kernel(const IvUrTask* __restrict__ tasks, const IvPair* __restrict__ pairs, const uint32_t* __restrict__ lmi,
+                const uint8_t* __restrict__ ub, uint32_t n_rows, uint32_t t_base, uint32_t t_cnt,
+                uint32_t trials_total, const uint64_t* __restrict__ r, uint64_t* __restrict__ ur_part) {
+    extern __shared__ uint4 u_img[];  // one U block: 8 t_cnt rows x 128 bytes
+    __shared__ uint64_t rbase_s[UR_SLAB];
+    __shared__ uint32_t out_s[UR_SLAB];
+    const IvUrTask tk = tasks[blockIdx.x];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint64_t lo[TC_MAX_TRIALS], hi[TC_MAX_TRIALS];
+    if (threadIdx.x < tk.npairs) {
+        const IvPair pr = pairs[lmi[tk.lp0 + threadIdx.x]];
+        rbase_s[threadIdx.x] = pr.out0 + (uint64_t)tk.c * IV_CHUNK_ROWS;
+        out_s[threadIdx.x] = pr.ch0 + tk.c;
+    }
+    const uint32_t combos = tk.npairs * t_cnt;
+    uint64_t lo[UR_PER_WARP], hi[UR_PER_WARP];
 #pragma unroll
-    for (int t = 0; t < TC_MAX_TRIALS; ++t) lo[t] = hi[t] = 0;
-    const uint32_t nblk = (c.rows + TC_ROWS - 1) / TC_ROWS;
-    for (uint32_t b = warp; b < nblk; b += 4) {
+    for (uint32_t ii = 0; ii < UR_PER_WARP; ++ii) lo[ii] = hi[ii] = 0;
+    const uint32_t nblk = (tk.rows + TC_ROWS - 1) / TC_ROWS;
+    const uint32_t img_words = 8 * t_cnt * TC_ROWS / 16;
+    const uint8_t* img = reinterpret_cast<const uint8_t*>(u_img) + 4 * lane;
+    for (uint32_t b = 0; b < nblk; ++b) {
+        __syncthreads();  // the previous block's image is no longer read (and rbase_s is set)
+        const uint4* src = reinterpret_cast<const uint4*>(ub + (uint64_t)(tk.ublk0 + b) * n_rows * TC_ROWS);
+        for (uint32_t x = threadIdx.x; x < img_words; x += blockDim.x) u_img[x] = src[x];
+        __syncthreads();
         const uint32_t i0 = b * TC_ROWS + 4 * lane;
-        uint64_t rv[4];
 #pragma unroll
-        for (int h = 0; h < 4; ++h) rv[h] = i0 + h < c.rows ? r[c.r0 + i0 + h] : 0;
-        const uint8_t* img = ub + (uint64_t)(c.ublk + b) * n_rows * TC_ROWS + 4 * lane;
+        for (uint32_t ii = 0; ii < UR_PER_WARP; ++ii) {
+            const uint32_t k = warp + UR_WARPS * ii;
+            if (k < combos) {
+                const uint32_t pk = k / t_cnt, t = k % t_cnt;
+                const uint64_t rb = rbase_s[pk];
+                uint64_t rv[4];
 #pragma unroll
-        for (int t = 0; t < TC_MAX_TRIALS; ++t) {
-            if ((uint32_t)t < t_cnt) {
+                for (int h = 0; h < 4; ++h) rv[h] = i0 + h < tk.rows ? r[rb + i0 + h] : 0;
                 uint32_t w[8];
 #pragma unroll
-                for (int a = 0; a < 8; ++a) w[a] = *reinterpret_cast<const uint32_t*>(img + (uint64_t)(8 * t + a) * TC_ROWS);
+                for (int a = 0; a < 8; ++a) w[a] = *reinterpret_cast<const uint32_t*>(img + (8 * t + a) * TC_ROWS);
                 // 8 x 4 byte transpose: byte a of u[h] = byte h of w[a]
                 const uint32_t l01 = __byte_perm(w[0], w[1], 0x5140), h01 = __byte_perm(w[0], w[1], 0x7362);
                 const uint32_t l23 = __byte_perm(w[2], w[3], 0x5140), h23 = __byte_perm(w[2], w[3], 0x7362);
@@ -163,25 +194,19 @@ ur_chunks_kernel(const IvChunk* __restrict__ chunks, const uint8_t* __restrict__
                 u[2] = __byte_perm(h01, h23, 0x5410) | ((uint64_t)__byte_perm(h45, h67, 0x5410) << 32);
                 u[3] = __byte_perm(h01, h23, 0x7632) | ((uint64_t)__byte_perm(h45, h67, 0x7632) << 32);
 #pragma unroll
-                for (int h = 0; h < 4; ++h) mac128(lo[t], hi[t], u[h], rv[h]);
+                for (int h = 0; h < 4; ++h) mac128(lo[ii], hi[ii], u[h], rv[h]);
             }
         }
     }
-    __shared__ uint64_t sh[4][TC_MAX_TRIALS];
 #pragma unroll
-    for (int t = 0; t < TC_MAX_TRIALS; ++t) {
-        if ((uint32_t)t < t_cnt) {
-            uint64_t x = reduce128(lo[t], hi[t]);
+    for (uint32_t ii = 0; ii < UR_PER_WARP; ++ii) {
+        const uint32_t k = warp + UR_WARPS * ii;
+        if (k < combos) {  // warp-uniform
+            uint64_t x = reduce128(lo[ii], hi[ii]);
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) x = add_mod(x, __shfl_xor_sync(0xffffffffu, x, off));
-            if (lane == 0) sh[warp][t] = x;
+            if (lane == 0) ur_part[(uint64_t)out_s[k / t_cnt] * trials_total + t_base + k % t_cnt] = x;
         }
-    }
-    __syncthreads();
-    if (threadIdx.x < t_cnt) {
-        const uint32_t t = threadIdx.x;
-        const uint64_t x = add_mod(add_mod(sh[0][t], sh[1][t]), add_mod(sh[2][t], sh[3][t]));
-        ur_part[(uint64_t)blockIdx.x * trials_total + t_base + t] = x;
     }
 }
 
@@ -277,6 +302,7 @@ struct IvfBlockJob {
     bool verify_only = false;
     uint32_t P = 0, U = 0, NB = 0, NP = 0, NCH = 0, n_pl = 0, n_s8 = 0, NZ = 0;
     uint32_t NP_big = 0;  // panels [0, NP_big) belong to lists longer than TC_SMALL_PANEL_ROWS
+    uint32_t NUR = 0;     // u . r tasks (list chunk x pair slab)
     uint64_t R = 0, max_q_rows = 0;
     uint32_t w_tile = 64, n_rows = 0, ctas = 1, st_g1 = 0, st_g2 = 0, st_g3 = 0;
     // host plan
@@ -288,7 +314,7 @@ struct IvfBlockJob {
     std::vector<uint32_t> qp0;          // per query: first pair (B + 1)
     // inputs (one H2D from the staging buffer)
     uint64_t o_v, o_g, o_t, o_tn, o_seed, o_qoff, o_qp0, o_pairs, o_lmq, o_lmi, o_base, o_groups, o_vsegs, o_blocks,
-        o_panels, o_zoff, o_zsum, o_chunks, in_end;
+        o_panels, o_zoff, o_zsum, o_chunks, o_urtasks, in_end;
     // outputs (one D2H)
     uint64_t o_ids, o_sc, o_n, o_fc, o_ft, o_err, out_end;
     // scratch
@@ -410,7 +436,11 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.NP = np;
     j.NCH = nch;
     j.NZ = 0;
-    for (uint32_t u = 0; u < j.U; ++u) j.NZ += (j.groups[u].m > TC_PANEL_ROWS) ? 1u : 0u;
+    j.NUR = 0;
+    for (uint32_t u = 0; u < j.U; ++u) {
+        j.NZ += (j.groups[u].m > TC_PANEL_ROWS) ? 1u : 0u;
+        j.NUR += ((j.groups[u].m + IV_CHUNK_ROWS - 1) / IV_CHUNK_ROWS) * ((j.groups[u].n + UR_SLAB - 1) / UR_SLAB);
+    }
     // grouped GEMM item counts (the tables themselves are expanded on the device)
     j.n_pl = j.n_s8 = 0;
     if (!verify_only && j.P) {
@@ -455,6 +485,7 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.o_zoff = L.take<uint64_t>(j.U);
     j.o_zsum = L.take<IvZsum>(j.NZ);
     j.o_chunks = L.take<IvChunk>(j.NCH);
+    j.o_urtasks = L.take<IvUrTask>(j.NUR);
     j.in_end = L.take<uint8_t>(0);
     j.o_ids = L.take<uint32_t>((uint64_t)B * ks);
     j.o_sc = L.take<int64_t>((uint64_t)B * ks);
@@ -549,6 +580,15 @@ int ivf_block_pack(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, const
     // Protocol 2 layout: one verify segment per distinct list (128-row U
     // blocks, 4096-row z panels); z of a single-panel list is its z_part,
     // several panels are summed into a z slot (after z_part)
+    IvUrTask* ut = reinterpret_cast<IvUrTask*>(h + j.o_urtasks);
+    for (uint32_t u = 0, nt = 0; u < j.U; ++u) {
+        const IvGroup& gr = j.groups[u];
+        for (uint32_t c = 0; c * IV_CHUNK_ROWS < gr.m; ++c)
+            for (uint32_t p0 = 0; p0 < gr.n; p0 += UR_SLAB)
+                ut[nt++] = IvUrTask{j.block0[u] + c * (IV_CHUNK_ROWS / TC_ROWS),
+                                    std::min<uint32_t>(IV_CHUNK_ROWS, gr.m - c * IV_CHUNK_ROWS), gr.lp0 + p0,
+                                    std::min<uint32_t>(UR_SLAB, gr.n - p0), c};
+    }
     VerifySeg* vs = reinterpret_cast<VerifySeg*>(h + j.o_vsegs);
     TcBlock* bl = reinterpret_cast<TcBlock*>(h + j.o_blocks);
     TcPanel* pn = reinterpret_cast<TcPanel*>(h + j.o_panels);
@@ -679,8 +719,9 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
                                 sms, s);
             launch_tc_freivalds_small(c.tmap_m, j.tm_u, panels, j.NP_big, j.NP - j.NP_big, t0, tc, j.n_rows, j.trials,
                                       U64(j.o_zpart), err, sms, s);
-            ur_chunks_kernel<<<j.NCH, 128, 0, s>>>(dchunks, U8(j.o_ub), j.n_rows, t0, tc, j.trials, U64(j.o_r),
-                                                  U64(j.o_urpart));
+            ur_lists_kernel<<<j.NUR, UR_WARPS * 32, 8 * tc * TC_ROWS, s>>>(
+                reinterpret_cast<const IvUrTask*>(d + j.o_urtasks), dpairs, U32(j.o_lmi), U8(j.o_ub), j.n_rows, t0, tc,
+                j.trials, U64(j.o_r), U64(j.o_urpart));
         }
         mark(6);
         if (j.NZ)

@@ -265,11 +265,14 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
     if (bucket) {
         // block scoring: the batch's queries share one pass over the corpus;
         // Protocol 2 runs per block with the first request's seed
-        if (!sl.bp || sl.bp_B != bucket) {
+        // a slot keeps its largest plan so far (smaller batches pad it with
+        // zero queries) and its workspace for per-query / IVF batches:
+        // creating plans or freeing device memory mid-stream synchronises the
+        // device and stalls every slot
+        if (!sl.bp || sl.bp_B < bucket) {
             if (sl.bp) block_plan_free(sl.bp);
             sl.bp = nullptr;
             sl.bp_B = 0;
-            sl.ws.release();  // this slot's per-query workspace is not needed while it runs blocks
             rc = block_plan_create(s->flat, bucket, s->cfg.trials, s->cfg.k, 0, &sl.bp);
             if (rc == BN_OK) sl.bp_B = bucket;
         }
@@ -341,24 +344,32 @@ std::vector<Request> take_batch(bn_server* s, Slot& me, int& kind_out, bool& rej
     const double age_us = std::chrono::duration<double, std::micro>(Clock::now() - q.front().t_submit).count();
     if (q.size() < s->cfg.max_batch && age_us < s->cfg.max_wait_us) return {};
     // memory admission: the largest prefix whose workspace fits beside the
-    // other slots' workspaces
+    // other slots' memory and what this slot keeps besides the batch's own
+    // (its block plan while it runs a per-query or IVF batch, its workspace
+    // while it runs a flat block; a kept plan at least the batch's bucket is
+    // reused, so it is the batch's own)
     const uint64_t others = held_bytes(s) - slot_bytes(me);
     const uint64_t budget = s->cfg.mem_budget;
+    auto need = [&](size_t cnt) -> uint64_t {
+        const uint32_t bucket = kind == BN_SERVER_FLAT ? block_bucket(s, cnt) : 0;
+        if (bucket && me.bp && me.bp_B >= bucket) return me.ws.bytes + block_plan_bytes(me.bp);
+        const uint64_t own = batch_bytes(s, kind, q, cnt);
+        return own + (bucket ? me.ws.bytes : (me.bp ? block_plan_bytes(me.bp) : 0));
+    };
     size_t count = std::min<size_t>(q.size(), s->cfg.max_batch);
-    while (count > 0 && budget && others + batch_bytes(s, kind, q, count) > budget) count = count > 8 ? count / 2 : count - 1;
+    while (count > 0 && budget && others + need(count) > budget) count = count > 8 ? count / 2 : count - 1;
     if (count == 0) {
         bool any_busy = false;
         for (auto& sl : s->slots) any_busy |= sl->busy;
         if (!any_busy) {
-            // idle slots keep their workspaces: give them back, then retry once
-            for (auto& sl : s->slots)
-                if (sl.get() != &me) {
-                    sl->ws.release();
-                    if (sl->bp) block_plan_free(sl->bp);
-                    sl->bp = nullptr;
-                    sl->bp_B = 0;
-                }
-            if (batch_bytes(s, kind, q, 1) + held_bytes(s) - slot_bytes(me) > budget) {
+            // idle slots keep their memory: give it back (this slot's too), then retry once
+            for (auto& sl : s->slots) {
+                sl->ws.release();
+                if (sl->bp) block_plan_free(sl->bp);
+                sl->bp = nullptr;
+                sl->bp_B = 0;
+            }
+            if (batch_bytes(s, kind, q, 1) + held_bytes(s) > budget) {
                 reject_front = true;  // this request alone exceeds the budget
                 reject_kind = kind;
             } else {
