@@ -208,6 +208,23 @@ def progress(msg: str):
     print(f"[bench] {msg}", file=sys.stderr, flush=True)
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The slowest rank's value of x (a time): every rank calls it at the same
+    point; on one process (dist None) it is x itself."""
+    if not dist:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, world: int, slowest_s: float) -> float:
+    """Units all ranks processed (each rank the same count) per second of the slowest rank."""
+    return world * units_per_rank / slowest_s
+
+
 def run_gpu(args, rank: int, world: int, local_rank: int):
     import torch
 
@@ -278,12 +295,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         ev1.record(stream)
         ev1.synchronize()
         torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1)
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
 
     # the dominant kernel (the one pass over M_enc: fused scan + Protocol 2) is
     # timed inside every timed step with CUDA events on its launch stream
@@ -305,11 +317,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     for i in range(args.steps):
         j = args.warmup + i
         flat.query(encs[j][0][None], encs[j][1][None], [(encs[j][2], encs[j][3])], [seeds[j]], trials, k)
-    e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
 
     per_step_full = full_ms / args.steps / 1e3
     scan_s = scan_ms / args.steps / 1e3
@@ -324,7 +332,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     d2h = k * 12 + 8
     res = {
         "metric": METRIC,
-        "value": world * args.steps / (full_ms / 1e3),
+        "value": whole_job_rate(args.steps, world, full_ms / 1e3),
         "unit": "queries/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -346,7 +354,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                      "algorithmic_bytes_per_launch": bytes_scan, "launches_timed": int(len(fused_ms)),
                      "scan_only_kernel_step": {"achieved": bytes_scan / scan_s / 1e9,
                                                "frac": bytes_scan / scan_s / 1e9 / peak}},
-        "e2e": {"value": world * args.steps / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": whole_job_rate(args.steps, world, e2e_s), "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": 9 * args.steps,  # limbs, ugen, fused, rreduce, finish, decide, L^T v, decode, merge
         "clocks": clk.summary(),
@@ -437,17 +445,13 @@ def run_block(args, flat, L, seed, dev, stream, single_qps, dist):
             graph.replay()
         ev1.record()
         ev1.synchronize()
-        ms = ev0.elapsed_time(ev1)
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
         del graph
         status = plan.status()
         fl = d_f[: G * B].cpu().numpy()
         assert status == 0 and np.all(fl == -1), "block verification failed on honest responses"
         nq = reps * G * B
-        qps = (dist.get_world_size() if dist else 1) * nq / (ms / 1e3)
+        qps = whole_job_rate(nq, dist.get_world_size() if dist else 1, ms / 1e3)
         macs = flat.m * 8 * 8 * B * N_DIM  # byte-planar r = M_enc v GEMM
         gemm_tops = 2 * macs / (cfg["tuned_scan_ms"] / 1e3) / 1e12 if cfg["tuned_scan_ms"] else None
         out["per_B"][str(B)] = {"qps": qps, "ms_per_block": ms / (reps * G), "queries_timed": nq, "graph_blocks": G,
