@@ -246,23 +246,27 @@ __global__ void __launch_bounds__(128) zv_pairs_kernel(const uint64_t* __restric
 }
 
 // First failing trial of each pair (-1: accepted); ur_out (nullable) [i][t].
+// One warp per pair: lanes sum its chunks' partials, trial by trial.
 __global__ void pair_decide_kernel(const IvPair* __restrict__ pairs, uint32_t npairs,
                                    const uint64_t* __restrict__ ur_part, const uint64_t* __restrict__ zv,
                                    uint32_t trials, int32_t* __restrict__ pfail, uint64_t* __restrict__ ur_out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= npairs) return;
+    const uint32_t i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= npairs) return;  // warp-uniform
     const IvPair pr = pairs[i];
     int32_t f = -1;
     for (uint32_t t = 0; t < trials; ++t) {
         uint64_t acc = 0;
-        for (uint32_t c = pr.ch0; c < pr.ch0 + pr.nch; ++c) acc = add_mod(acc, ur_part[(uint64_t)c * trials + t]);
-        if (ur_out) ur_out[(uint64_t)i * trials + t] = acc;
+        for (uint32_t c = pr.ch0 + lane; c < pr.ch0 + pr.nch; c += 32)
+            acc = add_mod(acc, ur_part[(uint64_t)c * trials + t]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc = add_mod(acc, __shfl_xor_sync(0xffffffffu, acc, off));
+        if (ur_out && lane == 0) ur_out[(uint64_t)i * trials + t] = acc;
         if (f < 0 && acc != zv[(uint64_t)i * trials + t]) {
             f = (int32_t)t;
             if (!ur_out) break;
         }
     }
-    pfail[i] = f;
+    if (lane == 0) pfail[i] = f;
 }
 
 // Query q: its first failing pair in probe order -> (list, trial), else (-1, -1).
@@ -730,7 +734,7 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
                                                               U64(j.o_z));
         zv_pairs_kernel<<<dim3(j.P, j.trials), 128, 0, s>>>(U64(j.o_zpart), U64(j.o_zoff), dv, dpairs, U32(j.o_lmi),
                                                            j.trials, U64(j.o_zv));
-        pair_decide_kernel<<<(j.P + 127) / 128, 128, 0, s>>>(dpairs, j.P, U64(j.o_urpart), U64(j.o_zv), j.trials,
+        pair_decide_kernel<<<(j.P + 3) / 4, 128, 0, s>>>(dpairs, j.P, U64(j.o_urpart), U64(j.o_zv), j.trials,
                                                              reinterpret_cast<int32_t*>(d + j.o_pfail),
                                                              j.verify_only ? U64(j.o_urout) : nullptr);
         query_decide_kernel<<<(B + 127) / 128, 128, 0, s>>>(dpairs, U32(j.o_qp0), B,
