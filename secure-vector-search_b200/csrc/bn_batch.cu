@@ -88,7 +88,8 @@ struct ItemCursor {
 
 __global__ void __launch_bounds__(BG_THREADS, 1)
 bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__ CUtensorMap tmap_w,
-             const BgParams p, uint32_t stages, uint32_t stage_bytes, uint32_t* __restrict__ err) {
+             const __grid_constant__ CUtensorMap tmap_a2, const __grid_constant__ CUtensorMap tmap_w2, const BgParams p,
+             uint32_t stages, uint32_t stage_bytes, uint32_t* __restrict__ err) {
     extern __shared__ uint8_t bg_dyn[];
     __shared__ uint64_t full_b[BG_MAX_STAGES], empty_b[BG_MAX_STAGES], accf_b[2], acce_b[2], done_b;
     __shared__ uint64_t afull_b[BG_MAX_ASLOTS], aempty_b[BG_MAX_ASLOTS];  // A-resident slots
@@ -101,6 +102,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr uint32_t A_BYTES = BG_AROWS * BG_KSTEP;
     const uint32_t w_bytes = p.w_tile * BG_KSTEP;
+    const uint32_t ksub = p.ksteps2 ? 2u : 1u, kstage = ksub * BG_KSTEP;  // K steps / bytes per stage
     const uint32_t kpanels = (p.k_bytes + p.k_panel - 1) / p.k_panel;
     const uint32_t items = p.item_tab ? p.n_items : kpanels * p.a_tiles * p.w_tiles;
     const uint32_t a_slots = p.a_resident ? p.k_bytes / BG_KSTEP : 0;
@@ -157,7 +159,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 const uint32_t t = a_slots ? j / p.w_tiles : 0;
                 const bool load_a = a_slots && ix.tw == 0;
                 const uint32_t k0 = ix.kp * p.k_panel, k1 = min(p.k_bytes, k0 + p.k_panel);
-                for (uint32_t k = k0; k < k1; k += BG_KSTEP, ++it) {
+                for (uint32_t k = k0; k < k1; k += kstage, ++it) {
                     const uint32_t ks = (k - k0) / BG_KSTEP;
                     if (load_a) {
                         if (t > 0 && !bar_wait(&aempty_b[ks], (t - 1) & 1)) {
@@ -182,6 +184,10 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     if (a_slots) {
                         bar_expect_tx(&full_b[st], w_bytes);
                         tma_2d(sb, &tmap_w, (int)k, (int)ix.w_y, &full_b[st]);
+                    } else if (ksub == 2) {  // [A step k | A step k+1 | W step k | W step k+1]
+                        bar_expect_tx(&full_b[st], 2 * (A_BYTES + w_bytes));
+                        tma_2d(sb, &tmap_a2, 0, a_row(ix, k), &full_b[st]);
+                        tma_3d(sb + 2 * A_BYTES, &tmap_w2, 0, (int)ix.w_y, (int)(k / BG_KSTEP), &full_b[st]);
                     } else {
                         bar_expect_tx(&full_b[st], A_BYTES + w_bytes);
                         tma_2d(sb, &tmap_a, a_x(k), a_row(ix, k), &full_b[st]);
@@ -218,7 +224,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 const uint32_t d = tmem + buf * 256u;
                 const uint32_t k0 = ix.kp * p.k_panel, k1 = min(p.k_bytes, k0 + p.k_panel);
                 bool first = true;
-                for (uint32_t k = k0; k < k1; k += BG_KSTEP, ++it) {
+                for (uint32_t k = k0; k < k1; k += kstage, ++it) {
                     const uint32_t st = (uint32_t)(it % stages);
                     const uint32_t ks = (k - k0) / BG_KSTEP;
                     if ((a_slots && !bar_wait(&afull_b[ks], t & 1)) || !bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) ||
@@ -230,11 +236,13 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     }
                     tc_after();
                     const uint32_t sa = a_slots ? sbase + ks * A_BYTES : base + st * stage_bytes;
-                    const uint32_t sw = a_slots ? base + st * stage_bytes : sa + A_BYTES;
+                    const uint32_t sw = a_slots ? base + st * stage_bytes : sa + ksub * A_BYTES;
+                    for (uint32_t sub = 0; sub < ksub; ++sub)
 #pragma unroll
-                    for (uint32_t kk = 0; kk < BG_KSTEP / 32; ++kk)
-                        mma_i8(d, sdesc(sa + kk * 32u, 16, 1024), sdesc(sw + kk * 32u, 16, 1024), idesc,
-                               (first && kk == 0) ? 0u : 1u);
+                        for (uint32_t kk = 0; kk < BG_KSTEP / 32; ++kk)
+                            mma_i8(d, sdesc(sa + sub * A_BYTES + kk * 32u, 16, 1024),
+                                   sdesc(sw + sub * w_bytes + kk * 32u, 16, 1024), idesc,
+                                   (first && sub == 0 && kk == 0) ? 0u : 1u);
                     first = false;
                     mma_commit(&empty_b[st]);                // stage reusable once these MMAs have read it
                     if (last_of_a) mma_commit(&aempty_b[ks]);  // A slot reusable for the next A tile
@@ -613,13 +621,13 @@ unsigned grid_for(uint64_t work, unsigned threads, unsigned cap) {
 
 }  // namespace
 
-uint32_t bgemm_stage_bytes(uint32_t w_tile, bool a_resident) {
-    return (a_resident ? 0u : (uint32_t)(BG_AROWS * BG_KSTEP)) + ((w_tile * BG_KSTEP + 1023u) & ~1023u);
+uint32_t bgemm_stage_bytes(uint32_t w_tile, bool a_resident, uint32_t ksub) {
+    return ksub * ((a_resident ? 0u : (uint32_t)(BG_AROWS * BG_KSTEP)) + ((w_tile * BG_KSTEP + 1023u) & ~1023u));
 }
 
 uint32_t bgemm_smem_bytes(const BgParams& p, uint32_t stages) {
     const uint32_t a = p.a_resident ? (p.k_bytes / BG_KSTEP) * BG_AROWS * BG_KSTEP : 0u;
-    return a + stages * bgemm_stage_bytes(p.w_tile, p.a_resident != 0) + 1024u;
+    return a + stages * bgemm_stage_bytes(p.w_tile, p.a_resident != 0, p.ksteps2 ? 2u : 1u) + 1024u;
 }
 
 uint32_t bgemm_max_stages(const BgParams& p) {
@@ -629,18 +637,25 @@ uint32_t bgemm_max_stages(const BgParams& p) {
 }
 
 void launch_bgemm(const CUtensorMap& tmap_a, const CUtensorMap& tmap_w, const BgParams& p, uint32_t stages, int ctas,
-                  uint32_t* d_err, cudaStream_t s) {
+                  uint32_t* d_err, cudaStream_t s, const CUtensorMap* tmap_a2, const CUtensorMap* tmap_w2) {
+    if (p.ksteps2 && (p.k_panel % (2 * BG_KSTEP) || p.a_resident || !p.a_blocked || !tmap_a2 || !tmap_w2)) {
+        BgParams q = p;  // two K steps per stage do not apply: one per stage
+        q.ksteps2 = 0;
+        launch_bgemm(tmap_a, tmap_w, q, stages, ctas, d_err, s);
+        return;
+    }
     const uint32_t kpanels = (p.k_bytes + p.k_panel - 1) / p.k_panel;
     const uint64_t items = p.item_tab ? p.n_items : (uint64_t)kpanels * p.a_tiles * p.w_tiles;
     if (!items) return;
-    const uint32_t stage_bytes = bgemm_stage_bytes(p.w_tile, p.a_resident != 0);
+    const uint32_t stage_bytes = bgemm_stage_bytes(p.w_tile, p.a_resident != 0, p.ksteps2 ? 2u : 1u);
     // at least half the SM's shared memory: one CTA per SM, so the second
     // never waits in tcgen05.alloc for the first one's 512 TMEM columns
     const int smem = (int)std::max<uint32_t>(bgemm_smem_bytes(p, stages), 116u * 1024u);
     cudaFuncSetAttribute(bgemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const uint64_t units = p.item_tab ? p.n_items : p.a_resident ? p.a_tiles : items;
     const unsigned grid = units < (uint64_t)ctas ? (unsigned)units : (unsigned)ctas;
-    bgemm_kernel<<<grid, BG_THREADS, smem, s>>>(tmap_a, tmap_w, p, stages, stage_bytes, d_err);
+    bgemm_kernel<<<grid, BG_THREADS, smem, s>>>(tmap_a, tmap_w, tmap_a2 ? *tmap_a2 : tmap_a, tmap_w2 ? *tmap_w2 : tmap_w,
+                                                p, stages, stage_bytes, d_err);
 }
 
 void launch_planar_rows(const uint64_t* d_src, uint64_t rows, uint32_t k, uint64_t src_ld, int negate, uint8_t* d_dst,

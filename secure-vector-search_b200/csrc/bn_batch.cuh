@@ -65,6 +65,8 @@ struct BgParams {
     int order_a_fast;      // work order: 0 = W tile fastest, 1 = A tile fastest
     int a_resident;        // keep each A tile (all of K, one K panel) in shared memory across its W tiles
     int a_blocked;         // A is K-blocked (launch_planar_rows with ks = k_bytes / 128): a_y = tile index
+    int ksteps2;           // two K steps (256 bytes) per pipeline stage: needs a_blocked, no A-resident
+                           // mode, k_panel a multiple of 256, and the tmap_a2 / tmap_w2 maps
     // grouped mode (nullable): work items from a table instead of the a_tiles x
     // w_tiles grid (one K panel, no A-resident mode, no planar_out)
     const BgItem* item_tab;
@@ -77,11 +79,14 @@ struct BgParams {
 // [2, BG_MAX_STAGES].  *err: bit 2/3/4 set when a bounded wait timed out.
 // A-resident mode needs k_panel == k_bytes <= BG_MAX_ASLOTS * 128 and
 // bgemm_smem_bytes(p, stages) <= BG_MAX_SMEM.
+// With p.ksteps2: tmap_a2 = the K-blocked A with 256-row boxes (two K steps
+// of a tile), tmap_w2 = make_tmap_u8_ksteps2 of the W bytes.
 void launch_bgemm(const CUtensorMap& tmap_a, const CUtensorMap& tmap_w, const BgParams& p, uint32_t stages, int ctas,
-                  uint32_t* d_err, cudaStream_t s);
+                  uint32_t* d_err, cudaStream_t s, const CUtensorMap* tmap_a2 = nullptr,
+                  const CUtensorMap* tmap_w2 = nullptr);
 // Most pipeline stages whose shared memory fits one CTA (0 when even 2 do not).
 uint32_t bgemm_max_stages(const BgParams& p);
-uint32_t bgemm_stage_bytes(uint32_t w_tile, bool a_resident);
+uint32_t bgemm_stage_bytes(uint32_t w_tile, bool a_resident, uint32_t ksub = 1);
 uint32_t bgemm_smem_bytes(const BgParams& p, uint32_t stages);
 
 // Byte planes of a row-major u64 matrix: byte a of (negate ? p - src :

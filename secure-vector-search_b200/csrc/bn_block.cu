@@ -152,6 +152,9 @@ int block_prepare_locked(Engine& e, const std::vector<uint64_t>* offsets) {
     TRY(tmap(&c.tmap_mp, c.mp8.p, BG_KSTEP, c.mp8.bytes / BG_KSTEP, 128, "m_enc planes"));
     TRY(tmap(&c.tmap_alh, c.alh8.p, BG_KSTEP, c.alh8.bytes / BG_KSTEP, 128, "[AL | H] planes"));
     TRY(tmap(&c.tmap_ms, c.ms8.p, BG_KSTEP, c.ms8.bytes / BG_KSTEP, 128, "[M | S] bytes"));
+    TRY(tmap(&c.tmap_mp2, c.mp8.p, BG_KSTEP, c.mp8.bytes / BG_KSTEP, 256, "m_enc planes"));
+    TRY(tmap(&c.tmap_alh2, c.alh8.p, BG_KSTEP, c.alh8.bytes / BG_KSTEP, 256, "[AL | H] planes"));
+    TRY(tmap(&c.tmap_ms2, c.ms8.p, BG_KSTEP, c.ms8.bytes / BG_KSTEP, 256, "[M | S] bytes"));
     c.block_ready = true;
     return BN_OK;
 }

@@ -149,6 +149,7 @@ struct Corpus {
     uint64_t rows16 = 0, rows128 = 0;
     std::vector<uint64_t> list_p16, list_p128;
     CUtensorMap tmap_mp, tmap_alh, tmap_ms;
+    CUtensorMap tmap_mp2, tmap_alh2, tmap_ms2;  // the same with 256-row boxes (two K steps of a tile)
 
     uint64_t bytes() const {
         return m_enc.bytes + al_cm.bytes + h_cm.bytes + L.bytes + mp_cm.bytes + s_ell.bytes + s_off.bytes + s_w.bytes +

@@ -325,6 +325,7 @@ struct IvfBlockJob {
     uint64_t o_items_pl, o_items_s8, o_vp, o_gx, o_tv, o_x, o_wv, o_wgx, o_wtv, o_r, o_f2, o_f3, o_idmap, o_ub, o_zpart,
         o_z, o_urpart, o_zv, o_pfail, o_urout, o_cs, o_ci, o_cn, total;
     CUtensorMap tm_wv, tm_wgx, tm_wtv, tm_u;
+    CUtensorMap tm_wv2, tm_wgx2, tm_wtv2;  // 3-D views: two K steps per box
 };
 
 void ivf_block_job_free(IvfBlockJob* j) { delete j; }
@@ -460,6 +461,7 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
         }
         BgParams p{};
         p.w_tile = j.w_tile;
+        p.ksteps2 = 1;
         j.st_g1 = j.st_g2 = j.st_g3 = bgemm_max_stages(p);
         if (!j.st_g1) return fail(BN_EUNSUPPORTED, "no pipeline depth fits W tile %u", j.w_tile);
         if (v.blk_stages) j.st_g1 = j.st_g2 = j.st_g3 = std::min(j.st_g1, v.blk_stages);
@@ -621,6 +623,14 @@ int ivf_block_pack(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, const
         TRY(tmap_u8(&j.tm_wv, d + j.o_wv, N, 8ull * j.P, j.w_tile, "gathered v planes"));
         TRY(tmap_u8(&j.tm_wgx, d + j.o_wgx, c.k_alh, 8ull * j.P, j.w_tile, "gathered [g | x] planes"));
         TRY(tmap_u8(&j.tm_wtv, d + j.o_wtv, 2 * N, 8ull * j.P, j.w_tile, "gathered [T | v] bytes"));
+        const struct {
+            CUtensorMap* m;
+            uint64_t off, row_bytes;
+        } w2[3] = {{&j.tm_wv2, j.o_wv, N}, {&j.tm_wgx2, j.o_wgx, c.k_alh}, {&j.tm_wtv2, j.o_wtv, 2 * N}};
+        for (const auto& x : w2) {
+            const cudaError_t e = make_tmap_u8_ksteps2(x.m, d + x.off, x.row_bytes, 8ull * j.P, j.w_tile);
+            if (e != cudaSuccess) return fail(BN_ECUDA, "tensor map of the W operands: %s", cudaGetErrorString(e));
+        }
     }
     if (j.trials && j.NB) TRY(tmap_u8(&j.tm_u, d + j.o_ub, TC_ROWS, (uint64_t)j.NB * j.n_rows, j.n_rows, "u images"));
     return BN_OK;
@@ -687,11 +697,12 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             p.n_items = j.n_pl;
             p.pair_base = U64(j.o_base);
             p.a_blocked = 1;
-            launch_bgemm(c.tmap_mp, j.tm_wv, p, j.st_g1, sms, err, s);
+            p.ksteps2 = 1;  // two K steps per stage: half the producer / MMA handoffs per item
+            launch_bgemm(c.tmap_mp, j.tm_wv, p, j.st_g1, sms, err, s, &c.tmap_mp2, &j.tm_wv2);
             mark(2);
             p.k_bytes = p.k_panel = c.k_alh;
             p.out = U64(j.o_f2);
-            launch_bgemm(c.tmap_alh, j.tm_wgx, p, j.st_g2, sms, err, s);
+            launch_bgemm(c.tmap_alh, j.tm_wgx, p, j.st_g2, sms, err, s, &c.tmap_alh2, &j.tm_wgx2);
             mark(3);
             p.mode = BG_S8;
             p.k_bytes = p.k_panel = 2 * N;
@@ -699,7 +710,7 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             p.corr = c.corr.at<uint64_t>();
             p.item_tab = reinterpret_cast<const BgItem*>(d + j.o_items_s8);
             p.n_items = j.n_s8;
-            launch_bgemm(c.tmap_ms, j.tm_wtv, p, j.st_g3, sms, err, s);
+            launch_bgemm(c.tmap_ms, j.tm_wtv, p, j.st_g3, sms, err, s, &c.tmap_ms2, &j.tm_wtv2);
             mark(4);
         }
         if (j.k && j.P) {

@@ -43,6 +43,11 @@ struct TcBlock {
 // Returns cudaSuccess or the failure.
 cudaError_t make_tmap_u8(CUtensorMap* map, const void* base, uint64_t inner_bytes, uint64_t rows, uint32_t box_inner,
                          uint32_t box_rows);
+// 3-D view {128 bytes, rows, row_bytes / 128 K steps} of a row-major byte
+// matrix whose box {128, box_rows, 2} lands as two consecutive K steps'
+// [box_rows x 128] tiles (128-byte swizzle); coordinates (0, row, k / 128).
+cudaError_t make_tmap_u8_ksteps2(CUtensorMap* map, const void* base, uint64_t row_bytes, uint64_t rows,
+                                 uint32_t box_rows);
 
 // u generation: for each row block, U tile bytes [(t,b)][128 rows] (K-major
 // B operand image, un-swizzled; TMA applies the swizzle) for trials

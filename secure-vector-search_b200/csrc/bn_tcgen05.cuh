@@ -45,6 +45,13 @@ static __device__ __forceinline__ void tma_2d(void* dst, const CUtensorMap* map,
         "l"(map), "r"(x), "r"(y), "r"(su32(b))
         : "memory");
 }
+static __device__ __forceinline__ void tma_3d(void* dst, const CUtensorMap* map, int x, int y, int z, uint64_t* b) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(
+            su32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(su32(b))
+        : "memory");
+}
 static __device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 static __device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
