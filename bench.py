@@ -455,7 +455,8 @@ def run_block(args, flat, L, seed, dev, stream, single_qps, dist):
         macs = flat.m * 8 * 8 * B * N_DIM  # byte-planar r = M_enc v GEMM
         gemm_tops = 2 * macs / (cfg["tuned_scan_ms"] / 1e3) / 1e12 if cfg["tuned_scan_ms"] else None
         out["per_B"][str(B)] = {"qps": qps, "ms_per_block": ms / (reps * G), "queries_timed": nq, "graph_blocks": G,
-                                "tiling": {kk: cfg[kk] for kk in ("w_tile", "stages", "order", "a_resident", "k_panel")},
+                                "tiling": {kk: cfg[kk] for kk in ("w_tile", "stages", "order", "a_resident", "k_panel",
+                                                                  "two_ksteps_per_stage")},
                                 "scan_gemm_ms": cfg["tuned_scan_ms"], "scan_gemm_tops": gemm_tops}
         if best is None or qps > best[1]:
             best = (B, qps, gemm_tops)

@@ -193,10 +193,11 @@ int bn_flat_block_prepare(bn_flat* h);
 int bn_flat_block_plan(bn_flat* h, uint32_t B, uint32_t trials, uint32_t k, uint32_t flags, bn_plan** out);
 /* Chosen configuration: {W rows per tile (queries x 8), pipeline stages,
  * work order (0 = W tile fastest), A tiles resident in shared memory (0/1),
- * K panel of the u . r GEMM}; tuned_ms
+ * K panel of the u . r GEMM, K steps of 128 bytes per pipeline stage - 1};
+ * tuned_ms
  * (nullable) = the autotuner's measured launch times of the r = M_enc v GEMM
  * and of the u . r GEMM with that configuration (0 when not autotuned). */
-int bn_plan_block_config(const bn_plan* p, uint32_t config[5], float tuned_ms[2]);
+int bn_plan_block_config(const bn_plan* p, uint32_t config[6], float tuned_ms[2]);
 /* Device buffers as bn_plan_enqueue, with one 32-byte d_block_seed.
  * bn_plan_status reports bit 8 when a T column sum left [-128, 127]. */
 int bn_plan_enqueue_block(bn_plan* p, const uint64_t* d_v_enc, const uint64_t* d_g, const uint32_t* d_t,

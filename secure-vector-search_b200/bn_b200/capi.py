@@ -333,11 +333,11 @@ class Plan:
         check(fn(self.h, d_v, d_g, d_t, d_t_nnz, d_seeds, d_ids, d_scores, d_n, d_failed, stream))
 
     def block_config(self):
-        cfg = np.zeros(5, np.uint32)
+        cfg = np.zeros(6, np.uint32)
         ms = np.zeros(2, np.float32)
         check(lib.bn_plan_block_config(self.h, ptr(cfg), ptr(ms)))
         return {"w_tile": int(cfg[0]), "stages": int(cfg[1]), "order": int(cfg[2]), "a_resident": int(cfg[3]),
-                "k_panel": int(cfg[4]),
+                "k_panel": int(cfg[4]), "two_ksteps_per_stage": int(cfg[5]),
                 "tuned_scan_ms": float(ms[0]), "tuned_ur_ms": float(ms[1])}
 
     def enqueue_scan(self, d_v, d_r, stream: int):

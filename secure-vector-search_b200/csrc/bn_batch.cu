@@ -162,14 +162,18 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 for (uint32_t k = k0; k < k1; k += kstage, ++it) {
                     const uint32_t ks = (k - k0) / BG_KSTEP;
                     if (load_a) {
-                        if (t > 0 && !bar_wait(&aempty_b[ks], (t - 1) & 1)) {
-                            abort_s = 1;
-                            atomicOr(err, 4u);
-                            stop = true;
-                            break;
+                        for (uint32_t sub = 0; sub < ksub && !stop; ++sub) {
+                            if (t > 0 && !bar_wait(&aempty_b[ks + sub], (t - 1) & 1)) {
+                                abort_s = 1;
+                                atomicOr(err, 4u);
+                                stop = true;
+                                break;
+                            }
+                            const uint32_t kq = k + sub * BG_KSTEP;
+                            bar_expect_tx(&afull_b[ks + sub], A_BYTES);
+                            tma_2d(sptr + (ks + sub) * A_BYTES, &tmap_a, a_x(kq), a_row(ix, kq), &afull_b[ks + sub]);
                         }
-                        bar_expect_tx(&afull_b[ks], A_BYTES);
-                        tma_2d(sptr + ks * A_BYTES, &tmap_a, a_x(k), a_row(ix, k), &afull_b[ks]);
+                        if (stop) break;
                         t_last = t;
                     }
                     const uint32_t st = (uint32_t)(it % stages);
@@ -181,7 +185,10 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     }
                     if (abort_s) { stop = true; break; }
                     uint8_t* sb = ring + (uint64_t)st * stage_bytes;
-                    if (a_slots) {
+                    if (a_slots && ksub == 2) {  // [W step k | W step k+1]
+                        bar_expect_tx(&full_b[st], 2 * w_bytes);
+                        tma_3d(sb, &tmap_w2, 0, (int)ix.w_y, (int)(k / BG_KSTEP), &full_b[st]);
+                    } else if (a_slots) {
                         bar_expect_tx(&full_b[st], w_bytes);
                         tma_2d(sb, &tmap_w, (int)k, (int)ix.w_y, &full_b[st]);
                     } else if (ksub == 2) {  // [A step k | A step k+1 | W step k | W step k+1]
@@ -227,8 +234,9 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 for (uint32_t k = k0; k < k1; k += kstage, ++it) {
                     const uint32_t st = (uint32_t)(it % stages);
                     const uint32_t ks = (k - k0) / BG_KSTEP;
-                    if ((a_slots && !bar_wait(&afull_b[ks], t & 1)) || !bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) ||
-                        abort_s) {
+                    bool a_ok = true;
+                    for (uint32_t sub = 0; a_slots && sub < ksub; ++sub) a_ok = a_ok && bar_wait(&afull_b[ks + sub], t & 1);
+                    if (!a_ok || !bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
                         abort_s = 1;
                         atomicOr(err, 8u);
                         stop = true;
@@ -245,7 +253,9 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                                    (first && sub == 0 && kk == 0) ? 0u : 1u);
                     first = false;
                     mma_commit(&empty_b[st]);                // stage reusable once these MMAs have read it
-                    if (last_of_a) mma_commit(&aempty_b[ks]);  // A slot reusable for the next A tile
+                    if (last_of_a)
+                        for (uint32_t sub = 0; sub < ksub; ++sub)
+                            mma_commit(&aempty_b[ks + sub]);  // A slots reusable for the next A tile
                 }
                 if (stop) break;
                 mma_commit(&accf_b[buf]);  // accumulator complete for this item
@@ -638,7 +648,7 @@ uint32_t bgemm_max_stages(const BgParams& p) {
 
 void launch_bgemm(const CUtensorMap& tmap_a, const CUtensorMap& tmap_w, const BgParams& p, uint32_t stages, int ctas,
                   uint32_t* d_err, cudaStream_t s, const CUtensorMap* tmap_a2, const CUtensorMap* tmap_w2) {
-    if (p.ksteps2 && (p.k_panel % (2 * BG_KSTEP) || p.a_resident || !p.a_blocked || !tmap_a2 || !tmap_w2)) {
+    if (p.ksteps2 && (p.k_panel % (2 * BG_KSTEP) || !tmap_w2 || (!p.a_resident && (!p.a_blocked || !tmap_a2)))) {
         BgParams q = p;  // two K steps per stage do not apply: one per stage
         q.ksteps2 = 0;
         launch_bgemm(tmap_a, tmap_w, q, stages, ctas, d_err, s);

@@ -65,8 +65,8 @@ struct BgParams {
     int order_a_fast;      // work order: 0 = W tile fastest, 1 = A tile fastest
     int a_resident;        // keep each A tile (all of K, one K panel) in shared memory across its W tiles
     int a_blocked;         // A is K-blocked (launch_planar_rows with ks = k_bytes / 128): a_y = tile index
-    int ksteps2;           // two K steps (256 bytes) per pipeline stage: needs a_blocked, no A-resident
-                           // mode, k_panel a multiple of 256, and the tmap_a2 / tmap_w2 maps
+    int ksteps2;           // two K steps (256 bytes) per pipeline stage: needs k_panel a multiple of
+                           // 256, tmap_w2, and (streaming A) a_blocked with tmap_a2
     // grouped mode (nullable): work items from a table instead of the a_tiles x
     // w_tiles grid (one K panel, no A-resident mode, no planar_out)
     const BgItem* item_tab;

@@ -38,6 +38,7 @@ struct BlockPlan {
     uint32_t nblocks = 0, npanels = 0;  // U row blocks, z panels (4096 rows)
     // tuned GEMM configuration
     uint32_t w_tile = 256, stages = 4, order = 0, a_res = 0, k_panel4 = 16384;
+    uint32_t ks2 = 1;  // two K steps per pipeline stage in G1-G3
     float tuned_ms[2] = {0.f, 0.f};  // autotuner's best G1 and G4 launch times
     int topk_ctas = 1;
     // workspace
@@ -46,6 +47,7 @@ struct BlockPlan {
         o_urpart, o_ur, o_fail, o_cs, o_ci, o_cn, o_in, o_in_v, o_in_g, o_in_t, o_in_tn, o_in_seed, o_out_ids,
         o_out_sc, o_out_n, o_out_end;
     CUtensorMap tm_vp, tm_gx, tm_tv, tm_rp, tm_ub;
+    CUtensorMap tm_vp2, tm_gx2, tm_tv2;  // 3-D views of the W operands: two K steps per box
     PinnedMem host;  // staging for the host-buffer entry points
 };
 
@@ -173,6 +175,7 @@ BgParams g1_params(const BlockPlan& b, const Corpus& c) {
     p.order_a_fast = (int)b.order;
     p.a_resident = (int)b.a_res;
     p.a_blocked = 1;
+    p.ksteps2 = (int)b.ks2;  // two K steps per stage: half the producer / MMA handoffs per item
     p.planar_ld = b.npad;
     return p;
 }
@@ -183,6 +186,14 @@ int relayout(BlockPlan& b) {
     TRY(tmap(&b.tm_vp, d + b.o_vp, N, 8ull * b.B, b.w_tile, "v planes"));
     TRY(tmap(&b.tm_gx, d + b.o_gx, b.h->e.c.k_alh, 8ull * b.B, b.w_tile, "[g | x] planes"));
     TRY(tmap(&b.tm_tv, d + b.o_tv, 2 * N, 8ull * b.B, b.w_tile, "[T | v] bytes"));
+    const struct {
+        CUtensorMap* m;
+        uint64_t off, row_bytes;
+    } w2[3] = {{&b.tm_vp2, b.o_vp, N}, {&b.tm_gx2, b.o_gx, b.h->e.c.k_alh}, {&b.tm_tv2, b.o_tv, 2 * N}};
+    for (const auto& x : w2) {
+        const cudaError_t e = make_tmap_u8_ksteps2(x.m, d + x.off, x.row_bytes, 8ull * b.B, b.w_tile);
+        if (e != cudaSuccess) return fail(BN_ECUDA, "tensor map of the W operands: %s", cudaGetErrorString(e));
+    }
     return BN_OK;
 }
 
@@ -196,13 +207,15 @@ int autotune(BlockPlan& b, cudaStream_t s) {
     CU(cudaEventCreate(&e1));
     const uint32_t wmax = (uint32_t)std::min<uint64_t>(256, align_up(8ull * b.B, 16));
     float best = 1e30f;
-    uint32_t bw = b.w_tile, bs = b.stages, bo = b.order, ba = b.a_res;
+    uint32_t bw = b.w_tile, bs = b.stages, bo = b.order, ba = b.a_res, bk = b.ks2;
     int rc = BN_OK;
     for (uint32_t w : {64u, 128u, 256u}) {
         if (w > wmax && w != 64u) continue;
-        for (uint32_t ares : {0u, 1u}) {
+        for (uint32_t combo = 0; combo < 4 && rc == BN_OK; ++combo) {  // (A resident, two K steps per stage)
+            const uint32_t ares = combo >> 1;
             b.w_tile = w;
             b.a_res = ares;
+            b.ks2 = combo & 1;
             const uint32_t smax = stages_for(g1_params(b, c));
             if (!smax) continue;
             for (uint32_t st : {std::min(3u, smax), smax}) {
@@ -219,14 +232,14 @@ int autotune(BlockPlan& b, cudaStream_t s) {
                     for (int rep = 0; rep < 3; ++rep) {
                         if (rep == 1) cudaEventRecord(e0, s);
                         launch_bgemm(c.tmap_mp, b.tm_vp, p, b.stages, b.h->e.ctx->num_sms,
-                                     reinterpret_cast<uint32_t*>(d + b.o_err), s);
+                                     reinterpret_cast<uint32_t*>(d + b.o_err), s, &c.tmap_mp2, &b.tm_vp2);
                     }
                     cudaEventRecord(e1, s);
                     if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
                         rc = fail(BN_ECUDA, "autotune timing failed");
                         break;
                     }
-                    if (ms < best) { best = ms; bw = w; bs = st; bo = order; ba = ares; }
+                    if (ms < best) { best = ms; bw = w; bs = st; bo = order; ba = ares; bk = b.ks2; }
                 }
                 if (rc != BN_OK || smax <= 3u) break;
             }
@@ -238,6 +251,7 @@ int autotune(BlockPlan& b, cudaStream_t s) {
     b.stages = bs;
     b.order = bo;
     b.a_res = ba;
+    b.ks2 = bk;
     b.tuned_ms[0] = best / 2;  // two timed launches per candidate
     if (rc == BN_OK && b.trials) {  // K panel of the u . r GEMM
         float bestk = 1e30f;
@@ -362,10 +376,19 @@ int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint3
     if (!c.block_ready) b->a_res = 0;
     b->k_panel4 = 4096;
     if (!verify_only) {
-        b->stages = stages_for(g1_params(*b, c));
-        if (!b->stages) {
-            b->a_res = 0;
-            b->stages = stages_for(g1_params(*b, c));
+        // the first configuration with a pipeline of at least 3 stages, else of 2:
+        // (A resident if useful, two K steps per stage) before (.., one K step)
+        // before streaming A
+        const uint32_t pref_ares = b->a_res;
+        bool found = false;
+        for (uint32_t min_st : {3u, 2u}) {
+            for (uint32_t combo = 0; combo < 4 && !found; ++combo) {
+                b->a_res = combo < 2 ? pref_ares : 0u;
+                b->ks2 = (combo & 1) ? 0u : 1u;
+                b->stages = stages_for(g1_params(*b, c));
+                found = b->stages >= min_st;
+            }
+            if (found) break;
         }
     }
     const int sms = f->e.ctx->num_sms;
@@ -429,12 +452,13 @@ uint64_t block_plan_estimate(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k
     return block_layout(b, c.n1, (uint32_t)align_up(2ull * c.n1, 128), false);
 }
 
-void block_plan_config(const BlockPlan* b, uint32_t cfg[5], float tuned_ms[2]) {
+void block_plan_config(const BlockPlan* b, uint32_t cfg[6], float tuned_ms[2]) {
     cfg[0] = b->w_tile;
     cfg[1] = b->stages;
     cfg[2] = b->order;
     cfg[3] = b->a_res;
     cfg[4] = b->k_panel4;
+    cfg[5] = b->ks2;
     if (tuned_ms) {
         tuned_ms[0] = b->tuned_ms[0];
         tuned_ms[1] = b->tuned_ms[1];
@@ -517,7 +541,7 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     BgParams p = g1_params(b, c);
     p.out = r;
     p.planar_out = rp;
-    launch_bgemm(c.tmap_mp, b.tm_vp, p, b.stages, sms, err, s);
+    launch_bgemm(c.tmap_mp, b.tm_vp, p, b.stages, sms, err, s, &c.tmap_mp2, &b.tm_vp2);
     // G2: f2 = -(AL g + H x)   (K = 2 n1 bytes per plane row: A tiles stay resident)
     p.k_bytes = c.k_alh;
     p.k_panel = c.k_alh;
@@ -525,7 +549,7 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     p.planar_out = nullptr;
     p.a_resident = (p.w_tiles > 1 && c.k_alh <= BG_MAX_ASLOTS * BG_KSTEP) ? 1 : 0;
     p.order_a_fast = p.a_resident ? 0 : (int)b.order;
-    launch_bgemm(c.tmap_alh, b.tm_gx, p, stages_for(p), sms, err, s);
+    launch_bgemm(c.tmap_alh, b.tm_gx, p, stages_for(p), sms, err, s, &c.tmap_alh2, &b.tm_gx2);
     // G3: f3 = M T + S v
     BgParams q{};
     q.mode = BG_S8;
@@ -541,7 +565,8 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     q.corr = c.corr.at<uint64_t>();
     q.order_a_fast = (int)b.order;
     q.a_blocked = 1;
-    launch_bgemm(c.tmap_ms, b.tm_tv, q, stages_for(q), sms, err, s);
+    q.ksteps2 = (int)b.ks2;
+    launch_bgemm(c.tmap_ms, b.tm_tv, q, stages_for(q), sms, err, s, &c.tmap_ms2, &b.tm_tv2);
     // Mv = r + f2 - f3 (written over f3 when asked for), fp_to_signed, top-k
     if (b.k || want_mv) {
         TopkScratch ts{reinterpret_cast<int64_t*>(d + b.o_cs), reinterpret_cast<uint32_t*>(d + b.o_ci),

@@ -1029,7 +1029,7 @@ int bn_flat_block_plan(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint
     return BN_OK;
 }
 
-int bn_plan_block_config(const bn_plan* p, uint32_t config[5], float tuned_ms[2]) {
+int bn_plan_block_config(const bn_plan* p, uint32_t config[6], float tuned_ms[2]) {
     if (!p || !config) return fail(BN_EINVAL, "null argument");
     if (!p->block) return fail(BN_EINVAL, "not a block plan");
     block_plan_config(p->block, config, tuned_ms);

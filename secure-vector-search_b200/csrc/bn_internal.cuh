@@ -338,7 +338,7 @@ namespace api {
 int block_prepare(bn_flat* f);
 constexpr uint32_t BLOCK_VERIFY_ONLY = 1u << 31;  // internal block_plan_create flag
 int block_plan_create(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, uint32_t flags, BlockPlan** out);
-void block_plan_config(const BlockPlan* b, uint32_t cfg[5], float tuned_ms[2]);
+void block_plan_config(const BlockPlan* b, uint32_t cfg[6], float tuned_ms[2]);
 int block_plan_status(BlockPlan* b, uint32_t* flags);
 int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const uint32_t* d_t, const uint32_t* d_tn,
                   const uint8_t* d_seed, uint32_t* d_ids, int64_t* d_scores, uint32_t* d_n, int32_t* d_failed,

@@ -147,7 +147,7 @@ def test_block_plan_autotune_and_graph_capture(ctx):
     d_f = torch.zeros(B, dtype=torch.int32, device=dev)
     plan = f.block_plan(B, trials, k, autotune=True)
     cfg = plan.block_config()
-    assert cfg["w_tile"] in (64, 128, 256) and 2 <= cfg["stages"] <= 6 and cfg["k_panel"] in (4096, 8192, 16384)
+    assert cfg["w_tile"] in (64, 128, 256) and 2 <= cfg["stages"] <= 12 and cfg["two_ksteps_per_stage"] in (0, 1) and cfg["k_panel"] in (4096, 8192, 16384)
     stream = torch.cuda.Stream()
     args = [x.data_ptr() for x in (d_v, d_g, d_t, d_tn, d_s, d_ids, d_sc, d_n, d_f)]
 
