@@ -356,7 +356,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                                                "frac": bytes_scan / scan_s / 1e9 / peak}},
         "e2e": {"value": whole_job_rate(args.steps, world, e2e_s), "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
-        "gpu_launches": 9 * args.steps,  # limbs, ugen, fused, rreduce, finish, decide, L^T v, decode, merge
+        "gpu_launches": 9 * args.steps,  # limbs, ugen, query image, fused, rreduce, finish, decide, L^T v, decode + top-k
         "clocks": clk.summary(),
         "setup_s": setup_s,
     }
@@ -407,12 +407,13 @@ def run_block(args, flat, L, seed, dev, stream, single_qps, dist):
     d_f = torch.full((pool,), 7, dtype=torch.int32, device=dev)
     flat.block_prepare()
     out = {"trials": trials, "k": k, "freivalds": "one seed per block, every query checked", "per_B": {}}
-    peak_tops = None
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
             peak_tops = 2.0 * float(json.load(f)["bf16_tflops"])  # dense int8 rate = 2x dense bf16 on sm_100
+        peak_src = "2 x measured dense bf16 (int8 tensor rate on sm_100)"
     except (OSError, KeyError, ValueError):
         peak_tops = 2.0 * 1590.0
+        peak_src = "2 x fallback dense bf16 1590 TFLOP/s (int8 tensor rate on sm_100)"
     best = None
     for B in sizes:
         plan = flat.block_plan(B, trials, k, autotune=args.block_autotune)
@@ -465,7 +466,7 @@ def run_block(args, flat, L, seed, dev, stream, single_qps, dist):
     if best[2]:
         out["roofline"] = {"kernel": f"bgemm r = M_enc v (B={best[0]})", "bound": "tensor", "achieved": best[2],
                            "peak": peak_tops, "unit": "TOP/s int8", "frac": best[2] / peak_tops,
-                           "peak_source": "2 x measured dense bf16 (int8 tensor rate on sm_100)"}
+                           "peak_source": peak_src}
     # e2e through the C ABI with host buffers (pack + H2D + block pipeline + D2H of hits)
     B = 32 if 32 in sizes else sizes[0]
     vb = np.stack([e[0] for e in encs[:B]])

@@ -134,6 +134,30 @@ int validate_residues(const uint64_t* a, uint64_t count, const char* what) {
     return BN_OK;
 }
 
+// The decode's 32-row-blocked copies of [AL | H] and (for int8-valued
+// plaintext) M, built once the client state is on the device.
+int build_decode_layout(bn_ctx* ctx, Corpus& c, cudaStream_t s) {
+    const uint64_t rows32 = (c.rows + 31) / 32 * 32;
+    TRY(c.alh_b.alloc(ctx, rows32 * 2 * c.n1 * 8));
+    TRY(c.m8_b.alloc(ctx, rows32 * N));
+    DevMem bad;
+    TRY(bad.alloc(ctx, 4));
+    launch_decode_layout(c.al_cm.at<uint64_t>(), c.h_cm.at<uint64_t>(), c.mp_cm.at<uint64_t>(), c.rows, c.n1,
+                         c.alh_b.at<uint64_t>(), c.m8_b.at<int8_t>(), bad.at<uint32_t>(), s);
+    CU(cudaGetLastError());
+    uint32_t hb = 0;
+    CU(cudaMemcpyAsync(&hb, bad.p, 4, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (hb) c.m8_b.release();  // M T from the residues
+    return BN_OK;
+}
+
+DecodeCorpus decode_corpus(const Corpus& c) {
+    return DecodeCorpus{c.alh_b.at<uint64_t>(), c.m8_b.p ? c.m8_b.at<int8_t>() : nullptr, c.mp_cm.at<uint64_t>(),
+                        c.s_ell.at<uint16_t>(), c.s_off.at<uint32_t>(), c.s_w.at<uint16_t>(),
+                        c.ids.p ? c.ids.at<uint32_t>() : nullptr, c.rows, c.n1};
+}
+
 int attach_client(bn_ctx* ctx, Corpus& c, const uint64_t* L, const uint64_t* m_plain, bn_sparse_csr S, cudaStream_t s) {
     if (!L || !m_plain || (c.rows && (!S.rowptr || (S.rowptr[c.rows] && (!S.idx || !S.sign)))))
         return fail(BN_EINVAL, "attach_client: l_subspace, m_plain and s_mat are required");
@@ -143,6 +167,7 @@ int attach_client(bn_ctx* ctx, Corpus& c, const uint64_t* L, const uint64_t* m_p
     TRY(upload_colmajor(ctx, m_plain, c.rows, N, c.mp_cm, s));
     TRY(upload_sparse_ell(ctx, S, c.rows, c, s));
     CU(cudaStreamSynchronize(s));
+    TRY(build_decode_layout(ctx, c, s));
     c.client = true;
     return BN_OK;
 }
@@ -218,6 +243,7 @@ int build_corpus_from_plain(bn_ctx* ctx, Corpus& c, const uint64_t* m_q, uint64_
     CU(cudaMemcpyAsync(c.L.p, L, (uint64_t)N * n1 * 8, cudaMemcpyHostToDevice, s));
     TRY(upload_sparse_ell(ctx, S, rows, c, s));
     CU(cudaStreamSynchronize(s));
+    TRY(build_decode_layout(ctx, c, s));
     c.client = true;
     return BN_OK;
 }
@@ -298,10 +324,11 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
     o.z_part = L.take<uint64_t>(std::max<uint64_t>(zp, 1));
     o.ur_part = L.take<uint64_t>(std::max<uint64_t>(up, 1));
     o.flags = L.take<uint32_t>(1);
-    const uint64_t cand = (uint64_t)z.B * z.ctas * std::max<uint32_t>(z.k, 1);
+    const uint64_t cand = (uint64_t)z.ctas * std::max<uint32_t>(z.k, 1);  // z.ctas: decode CTAs of all queries
     o.cand_s = L.take<int64_t>(cand);
     o.cand_i = L.take<uint32_t>(cand);
-    o.cand_n = L.take<uint32_t>((uint64_t)z.B * z.ctas);
+    o.cand_n = L.take<uint32_t>(z.ctas);
+    o.cand_done = L.take<uint32_t>(z.B);
     o.u_buf = (tc && z.trials) ? L.take<uint8_t>(std::max<uint64_t>(z.nblocks, 1) * pass_rows(TC_MAX_TRIALS) * TC_ROWS) : 0;
     o.r_part = (tc && z.trials)
                    ? L.take<uint64_t>((uint64_t)tc_groups(pass_rows(std::min<uint32_t>(TC_MAX_TRIALS, z.trials))) *
@@ -377,10 +404,8 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
     }
     if (z.k) {
         launch_lt_times_v(c.L.at<uint64_t>(), c.n1, in.v, z.B, sc.x, s);
-        launch_decode_topk(sc.r, c.al_cm.at<uint64_t>(), c.h_cm.at<uint64_t>(), c.mp_cm.at<uint64_t>(),
-                           c.s_ell.at<uint16_t>(), c.s_off.at<uint32_t>(), c.s_w.at<uint16_t>(),
-                           c.ids.p ? c.ids.at<uint32_t>() : nullptr, c.rows, c.n1, m.segs, m.dq, z.B, in.v, in.g, sc.x,
-                           in.t, in.t_nnz, z.k, (int)z.ctas, sc.topk, out.mv, out.ids, out.scores, out.n, s);
+        launch_decode_topk(sc.r, decode_corpus(c), m.segs, m.dq, z.B, in.v, in.g, sc.x, in.t, in.t_nnz, z.k,
+                           z.ctas, sc.topk, out.mv, out.ids, out.scores, out.n, s);
     } else {
         CU(cudaMemsetAsync(out.n, 0, (uint64_t)z.B * 4, s));
     }
@@ -402,7 +427,7 @@ Scratch scratch_at(char* d, const RunLayout& o) {
                    reinterpret_cast<uint64_t*>(d + o.ur_part), reinterpret_cast<uint32_t*>(d + o.flags),
                    reinterpret_cast<uint64_t*>(d + o.ur), reinterpret_cast<uint64_t*>(d + o.zv),
                    TopkScratch{reinterpret_cast<int64_t*>(d + o.cand_s), reinterpret_cast<uint32_t*>(d + o.cand_i),
-                               reinterpret_cast<uint32_t*>(d + o.cand_n)},
+                               reinterpret_cast<uint32_t*>(d + o.cand_n), reinterpret_cast<uint32_t*>(d + o.cand_done)},
                    reinterpret_cast<uint32_t*>(d + o.err), reinterpret_cast<uint8_t*>(d + o.u_buf),
                    reinterpret_cast<uint64_t*>(d + o.r_part), reinterpret_cast<uint64_t*>(d + o.zv_chunks),
                    reinterpret_cast<uint8_t*>(d + o.wimg)};
@@ -432,14 +457,31 @@ void engine_free(Engine& e) {
     }
 }
 
-Sizes sizes_for(const Engine& e, const HostMeta& hm, uint32_t B, uint32_t trials, uint32_t k) {
-    uint64_t max_q_rows = 0;
-    for (auto& d : hm.dq) {
-        uint64_t rsum = 0;
-        for (uint32_t s = d.seg0; s < d.seg0 + d.nseg; ++s) rsum += hm.segs[s].rows;
-        max_q_rows = std::max(max_q_rows, rsum);
+// Decode CTAs of a run: about four per SM in total (one wave of the decode
+// kernel), shared among the queries in proportion to their rows, at least
+// one per query and at most one per 256-row tile.  Returns the total.
+uint32_t assign_decode_ctas(HostMeta& hm, int sms) {
+    std::vector<uint64_t> rows(hm.dq.size(), 0);
+    uint64_t total = 0;
+    for (size_t q = 0; q < hm.dq.size(); ++q) {
+        const DecodeQuery& d = hm.dq[q];
+        for (uint32_t s = d.seg0; s < d.seg0 + d.nseg; ++s) rows[q] += hm.segs[s].rows;
+        total += rows[q];
     }
-    return Sizes{B, e.c.n1, trials, k, (uint32_t)pick_ctas(max_q_rows, B, e.ctx->num_sms), hm.total_out,
+    const uint64_t target = (uint64_t)sms * 4;
+    uint32_t next = 0;
+    for (size_t q = 0; q < hm.dq.size(); ++q) {
+        uint64_t c = total ? (target * rows[q] + total - 1) / total : 1;
+        c = std::max<uint64_t>(1, std::min(c, (rows[q] + 255) / 256));
+        hm.dq[q].cta0 = next;
+        hm.dq[q].ctas = (uint32_t)c;
+        next += (uint32_t)c;
+    }
+    return next;
+}
+
+Sizes sizes_for(const Engine& e, HostMeta& hm, uint32_t B, uint32_t trials, uint32_t k) {
+    return Sizes{B, e.c.n1, trials, k, assign_decode_ctas(hm, e.ctx->num_sms), hm.total_out,
                  hm.segs.size(), hm.vsegs.size(), hm.blocks.size(), hm.panels.size(),
                  plan_freivalds(std::max<uint64_t>(hm.max_rows, 1), (uint32_t)std::max<size_t>(hm.vsegs.size(), 1),
                                 e.ctx->num_sms),
@@ -453,7 +495,7 @@ Sizes sizes_for(const Engine& e, const HostMeta& hm, uint32_t B, uint32_t trials
 int job_prepare(Engine& e, QueryJob& j, DevMem& ws, PinnedMem& host, const uint64_t* v_enc, const uint64_t* g,
                 const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds) {
     Corpus& c = e.c;
-    const HostMeta& hm = *j.hm;
+    HostMeta& hm = *j.hm;
     const uint32_t B = j.B, trials = j.trials, k = j.k;
     if (!c.client) return fail(BN_EUNSUPPORTED, "this handle has no client state (attach_client was not called)");
     if (k > BN_TOPK_MAX) return fail(BN_EINVAL, "k = %u exceeds BN_TOPK_MAX = %d", k, BN_TOPK_MAX);

@@ -135,6 +135,7 @@ struct Corpus {
     DevMem m_enc, al_cm, h_cm;
     bool client = false;
     DevMem L, mp_cm, s_ell, s_off, s_w, ids;
+    DevMem alh_b, m8_b;  // decode copies in 32-row blocks (bn_kernels.cuh); m8_b only for int8-valued M
     CUtensorMap tmap_m;  // m_enc as bytes {8192, rows}, 128x128 boxes, 128-byte swizzle
 
     // Byte-planar operands of block scoring (built on first use, see
@@ -153,7 +154,7 @@ struct Corpus {
 
     uint64_t bytes() const {
         return m_enc.bytes + al_cm.bytes + h_cm.bytes + L.bytes + mp_cm.bytes + s_ell.bytes + s_off.bytes + s_w.bytes +
-               ids.bytes + mp8.bytes + alh8.bytes + ms8.bytes + corr.bytes;
+               ids.bytes + alh_b.bytes + m8_b.bytes + mp8.bytes + alh8.bytes + ms8.bytes + corr.bytes;
     }
 };
 
@@ -236,7 +237,7 @@ struct HostMeta {
 };
 
 struct Sizes {
-    uint32_t B, n1, trials, k, ctas;
+    uint32_t B, n1, trials, k, ctas;  // ctas: decode CTAs of all queries together
     uint64_t total_out, nseg, nvseg, nblocks, npanels;
     FreivaldsPlan fp;  // CUDA-core engine
     int engine;        // BN_ENGINE_*
@@ -250,13 +251,14 @@ struct RunLayout {
     // outputs (contiguous -> one D2H)
     uint64_t ids, scores, n, vfailed, ur, zv, err, out_begin, out_end;
     // internal
-    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, u_buf, r_part, zv_chunks, wimg, total;
+    uint64_t limbs, x, r, mv, z_part, ur_part, flags, cand_s, cand_i, cand_n, cand_done, u_buf, r_part, zv_chunks, wimg,
+        total;
 };
 
 // One run of the query pipeline over host inputs (bn_capi.cu): hm is the
 // segment metadata of the B queries, kept alive by the caller.
 struct QueryJob {
-    const HostMeta* hm = nullptr;
+    HostMeta* hm = nullptr;  // job_prepare assigns the decode CTAs into it
     uint32_t B = 0, trials = 0, k = 0;
     bool want_mv = false;
     Sizes z{};
@@ -265,7 +267,7 @@ struct QueryJob {
 };
 void finish_meta(HostMeta& hm);
 void flat_meta(uint64_t m, uint32_t B, HostMeta& hm);
-Sizes sizes_for(const Engine& e, const HostMeta& hm, uint32_t B, uint32_t trials, uint32_t k);
+Sizes sizes_for(const Engine& e, HostMeta& hm, uint32_t B, uint32_t trials, uint32_t k);
 RunLayout make_layout(const Sizes& z, bool want_mv);
 // Validates and packs the inputs into host (pinned, grown as needed) and
 // sizes ws (grown as needed, budget-accounted).

@@ -378,17 +378,41 @@ freivalds_finish_kernel(const uint64_t* __restrict__ z_part, const uint64_t* __r
 }
 
 // ------------------------------------------------------------------ L^T v
+// One CTA of 1024 threads per query: column k = tid % n1, rows j = slice,
+// slice + slices, ... with v_j's limbs in shared memory, so each term is six
+// multiply-adds into three accumulators and the column loads are
+// independent (batches of 16 in flight).  Each thread sums at most 512
+// terms below 2^53.2 (hi < 2^29), so the accumulators stay below 2^64.
 __global__ void __launch_bounds__(1024)
 lt_times_v_kernel(const uint64_t* __restrict__ L, uint32_t n1, const uint64_t* __restrict__ v, uint64_t* __restrict__ x) {
-    // 1024 threads: column k = tid % n1, j-slice tid / n1; slices combined in shared memory
     const uint32_t q = blockIdx.x;
     const uint32_t k = threadIdx.x % n1, slices = blockDim.x / n1, sl = threadIdx.x / n1;
+    __shared__ uint4 vl[2 * N];
     __shared__ uint64_t part[1024];
-    uint64_t acc = 0;
-    if (sl < slices)
-        for (uint32_t j = sl; j < N; j += slices)
-            acc = add_mod(acc, mul_mod(L[(uint64_t)j * n1 + k], v[(uint64_t)q * N + j]));
-    part[threadIdx.x] = acc;
+    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
+        const uint64_t w = v[(uint64_t)q * N + j];
+        const Limbs3 b = limbs(w), c = limbs_hi(w);
+        vl[2 * j] = make_uint4(b.b0, b.b1, b.b2, c.b0);
+        vl[2 * j + 1] = make_uint4(c.b1, c.b2, 0u, 0u);
+    }
+    __syncthreads();
+    uint64_t a0 = 0, a1 = 0, a2 = 0;
+    const uint32_t terms = N / slices;  // multiple of 16: slices <= 16
+    for (uint32_t i0 = 0; i0 < terms; i0 += 16) {
+        uint64_t xs[16];
+#pragma unroll
+        for (int ii = 0; ii < 16; ++ii) xs[ii] = __ldg(L + (uint64_t)(sl + (i0 + ii) * slices) * n1 + k);
+#pragma unroll
+        for (int ii = 0; ii < 16; ++ii) {
+            const uint32_t j = sl + (i0 + ii) * slices;
+            const uint4 l0 = vl[2 * j], l1 = vl[2 * j + 1];
+            const uint32_t xl = (uint32_t)xs[ii], xh = (uint32_t)(xs[ii] >> 32);
+            a0 = mac(mac(a0, xl, l0.x), xh, l0.w);
+            a1 = mac(mac(a1, xl, l0.y), xh, l1.x);
+            a2 = mac(mac(a2, xl, l0.z), xh, l1.y);
+        }
+    }
+    part[threadIdx.x] = combine3(a0, a1, a2);
     __syncthreads();
     if (threadIdx.x < n1) {
         uint64_t s = 0;
@@ -426,6 +450,33 @@ __global__ void dense_terms_kernel(const uint64_t* __restrict__ al_cm, const uin
     __syncthreads();
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x)
         out[i] = add_mod(cm_dot(al_cm, rows, i, gl, n1), cm_dot(h_cm, rows, i, xl, n1));
+}
+
+// Decode copies of the client state in 32-row blocks (layouts in
+// bn_kernels.cuh); reads and writes are both coalesced along the rows.
+__global__ void decode_layout_kernel(const uint64_t* __restrict__ al_cm, const uint64_t* __restrict__ h_cm,
+                                     const uint64_t* __restrict__ mp_cm, uint64_t rows, uint32_t n1,
+                                     uint64_t* __restrict__ alh_b, int8_t* __restrict__ m8_b, uint32_t* __restrict__ bad) {
+    const uint64_t rows32 = (rows + 31) / 32 * 32;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const uint64_t n_alh = rows32 * 2 * n1;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_alh; e += stride) {
+        const uint64_t col = (e >> 5) % (2 * n1), gr = ((e >> 5) / (2 * n1)) * 32 + (e & 31);
+        uint64_t x = 0;
+        if (gr < rows) x = col < n1 ? al_cm[col * rows + gr] : h_cm[(col - n1) * rows + gr];
+        alh_b[e] = x;
+    }
+    if (!m8_b) return;
+    bool out_of_range = false;
+    const uint64_t n_m = rows32 * N;
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_m; e += stride) {
+        const uint64_t col = (e >> 5) & (N - 1), gr = (e >> 15) * 32 + (e & 31);
+        int64_t v = 0;
+        if (gr < rows) v = to_signed(mp_cm[col * rows + gr]);
+        out_of_range |= v < -128 || v > 127;
+        m8_b[e] = (int8_t)v;
+    }
+    if (out_of_range) atomicOr(bad, 1u);
 }
 
 constexpr int DT_THREADS = 256;
@@ -512,173 +563,240 @@ __device__ __forceinline__ uint32_t find_query_seg(const ScanSeg* __restrict__ s
     return lo;
 }
 
-// Two rows per thread: every broadcast limb load serves both rows.  The
-// column loads come in batches of 16 per row (32 independent loads in
-// flight per thread) ahead of the limb arithmetic: the kernel is bound by
-// memory latency, not by the multiply-adds.
-__device__ __forceinline__ void cm_dot2(const uint64_t* __restrict__ a_cm, uint64_t rows, uint64_t row0, uint64_t row1,
-                                        bool has1, const uint4* __restrict__ vl, uint32_t n1, uint64_t& out0,
-                                        uint64_t& out1) {
-    uint64_t a0 = 0, a1 = 0, a2 = 0, e0 = 0, e1 = 0, e2 = 0;
-    const uint64_t* p0 = a_cm + row0;
-    const uint64_t* p1 = a_cm + (has1 ? row1 : row0);
-    for (uint32_t k0 = 0; k0 < n1; k0 += 16) {  // n1 is a multiple of 16
-        uint64_t xs[16], ys[16];
-#pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            xs[kk] = __ldg(p0 + (uint64_t)(k0 + kk) * rows);
-            ys[kk] = __ldg(p1 + (uint64_t)(k0 + kk) * rows);
-        }
-#pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
-            const uint4 l0 = vl[2 * (k0 + kk)], l1 = vl[2 * (k0 + kk) + 1];  // {b0,b1,b2,c0}, {c1,c2,-,-}
-            const uint64_t x = xs[kk], y = ys[kk];
-            const uint32_t xl = (uint32_t)x, xh = (uint32_t)(x >> 32), yl = (uint32_t)y, yh = (uint32_t)(y >> 32);
-            a0 = mac(mac(a0, xl, l0.x), xh, l0.w);
-            a1 = mac(mac(a1, xl, l0.y), xh, l1.x);
-            a2 = mac(mac(a2, xl, l0.z), xh, l1.y);
-            e0 = mac(mac(e0, yl, l0.x), yh, l0.w);
-            e1 = mac(mac(e1, yl, l0.y), yh, l1.x);
-            e2 = mac(mac(e2, yl, l0.z), yh, l1.y);
-        }
-    }
-    out0 = combine3(a0, a1, a2);
-    out1 = combine3(e0, e1, e2);
-}
-
 // Sum of +-x (sign in bit 31 of the entry) over a gathered column list,
 // folded lazily: every term is < 2^61, three terms fit below 2^63.
 __device__ __forceinline__ uint64_t signed_term(uint64_t x, bool neg) { return neg ? P - x : x; }
 
+// AL_i . g + H_i . x for corpus row gr from the 32-row-blocked alh_b: the
+// 2 n1 columns of the row's block are contiguous, so a warp's batch of 16
+// column loads is one 4 KB run.  lim[2k], lim[2k+1] hold the limbs of g_k
+// (k < n1) and of x_(k-n1) (k >= n1).  Every column adds lo*b + hi*c <
+// 2^53 + 2^50 (hi < 2^29: residues are < 2^61) to an accumulator, so the
+// 2 n1 <= 1024 columns stay below 2^64 with no fold.
+__device__ __forceinline__ uint64_t dense_terms_row(const uint64_t* __restrict__ alh_b, uint32_t n1, uint64_t gr,
+                                                    const uint4* __restrict__ lim) {
+    const uint64_t* p = alh_b + (gr >> 5) * (2ull * n1) * 32 + (gr & 31);
+    uint64_t a0 = 0, a1 = 0, a2 = 0;
+    for (uint32_t k0 = 0; k0 < 2 * n1; k0 += 16) {  // 2 n1 is a multiple of 16
+        uint64_t xs[16];
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) xs[kk] = __ldg(p + (uint64_t)(k0 + kk) * 32);
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            const uint4 l0 = lim[2 * (k0 + kk)], l1 = lim[2 * (k0 + kk) + 1];  // {b0,b1,b2,c0}, {c1,c2,-,-}
+            const uint32_t xl = (uint32_t)xs[kk], xh = (uint32_t)(xs[kk] >> 32);
+            a0 = mac(mac(a0, xl, l0.x), xh, l0.w);
+            a1 = mac(mac(a1, xl, l0.y), xh, l1.x);
+            a2 = mac(mac(a2, xl, l0.z), xh, l1.y);
+        }
+    }
+    return combine3(a0, a1, a2);
+}
+
+// M_i . T: signed column sums over the query's T entries (col | 0x80000000
+// for -1).  From the int8 blocks the sum is an exact integer, |sum| <=
+// 1024 * 128; else from the column-major residues, lazily folded.
+__device__ __forceinline__ uint64_t m_times_t_row(const DecodeCorpus& dc, uint64_t gr, const uint32_t* __restrict__ tl,
+                                                  uint32_t tn) {
+    if (dc.m8_b) {
+        const int8_t* p = dc.m8_b + (gr >> 5) * ((uint64_t)N * 32) + (gr & 31);
+        int32_t acc = 0;
+        uint32_t c = 0;
+        for (; c + 16 <= tn; c += 16) {
+            int32_t x[16];
+            uint32_t e[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                e[q] = tl[c + q];
+                x[q] = __ldg(p + (e[q] & 0x3ffu) * 32);
+            }
+#pragma unroll
+            for (int q = 0; q < 16; ++q) acc += (e[q] >> 31) ? -x[q] : x[q];
+        }
+        for (; c < tn; ++c) {
+            const uint32_t e = tl[c];
+            const int32_t x = __ldg(p + (e & 0x3ffu) * 32);
+            acc += (e >> 31) ? -x : x;
+        }
+        return acc >= 0 ? (uint64_t)acc : P - (uint64_t)(-(int64_t)acc);
+    }
+    uint64_t m_t = 0;
+    uint32_t c = 0;
+    for (; c + 8 <= tn; c += 8) {  // 8 gathers in flight, folded two terms at a time
+        uint64_t x[8];
+        uint32_t e[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            e[q] = tl[c + q];
+            x[q] = __ldg(dc.mp_cm + (uint64_t)(e[q] & 0x3ffu) * dc.rows + gr);
+        }
+#pragma unroll
+        for (int q = 0; q < 8; q += 2)
+            m_t = fold(m_t) + signed_term(x[q], e[q] >> 31) + signed_term(x[q + 1], e[q + 1] >> 31);
+    }
+    for (; c < tn; ++c) {
+        const uint32_t e = tl[c];
+        m_t = fold(m_t) + signed_term(__ldg(dc.mp_cm + (uint64_t)(e & 0x3ffu) * dc.rows + gr), e >> 31);
+    }
+    return canon(m_t);
+}
+
+// S_i . v_enc over the row's sliced-ELL entries (v_enc in shared memory).
+__device__ __forceinline__ uint64_t s_times_v_row(const DecodeCorpus& dc, uint64_t gr, const uint64_t* __restrict__ vs) {
+    const uint64_t slice = gr >> 5;
+    const uint32_t sl = (uint32_t)(gr & 31), off = dc.s_off[slice], wdt = dc.s_w[slice];
+    uint64_t s_v = 0;
+    uint32_t cc = 0;
+    for (; cc + 8 <= wdt; cc += 8) {  // 8 entry loads in flight
+        uint16_t f[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) f[q] = __ldg(dc.s_ell + off + (uint64_t)(cc + q) * 32 + sl);
+#pragma unroll
+        for (int q = 0; q < 8; q += 2) {
+            const uint64_t y0 = f[q] == 0xffffu ? 0 : signed_term(vs[f[q] & 0x3ffu], f[q] & 0x8000u);
+            const uint64_t y1 = f[q + 1] == 0xffffu ? 0 : signed_term(vs[f[q + 1] & 0x3ffu], f[q + 1] & 0x8000u);
+            s_v = fold(s_v) + y0 + y1;
+        }
+    }
+    for (; cc < wdt; ++cc) {
+        const uint16_t f = __ldg(dc.s_ell + off + (uint64_t)cc * 32 + sl);
+        s_v = fold(s_v) + (f == 0xffffu ? 0 : signed_term(vs[f & 0x3ffu], f & 0x8000u));
+    }
+    return canon(s_v);
+}
+
+// One row per thread; the CTAs of a query take 256-row tiles of its r-space
+// range in turn, so every CTA of the query gets the same number of tiles
+// give or take one (the host gives each query CTAs in proportion to its
+// rows).  Mv = r - (AL g + H x) - M T - S v, ranked by
+// fp_to_signed into the CTA's candidate buffer; the CTA's best k go to the
+// scratch lists, and the last CTA of the query to finish (a ticket taken
+// after a device-scope fence, no waiting) merges them.
 __global__ void __launch_bounds__(DT_THREADS)
-decode_topk_kernel(const uint64_t* __restrict__ r, const uint64_t* __restrict__ al_cm, const uint64_t* __restrict__ h_cm,
-                   const uint64_t* __restrict__ mp_cm, const uint16_t* __restrict__ s_ell,
-                   const uint32_t* __restrict__ s_off, const uint16_t* __restrict__ s_w,
-                   const uint32_t* __restrict__ ids, uint64_t total_rows, uint32_t n1, const ScanSeg* __restrict__ segs,
+decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSeg* __restrict__ segs,
                    const DecodeQuery* __restrict__ queries, const uint64_t* __restrict__ vv,
                    const uint64_t* __restrict__ gg, const uint64_t* __restrict__ xx,
-                   const uint32_t* __restrict__ t_ent, const uint32_t* __restrict__ t_nnz, uint32_t k,
-                   int64_t* __restrict__ cand_s, uint32_t* __restrict__ cand_i, uint32_t* __restrict__ cand_n,
-                   uint64_t* __restrict__ mv_out) {
-    const uint32_t q = blockIdx.y;
-    const DecodeQuery dq = queries[q];
-    if (dq.nseg == 0) {  // every probed list of this query was empty
-        if (threadIdx.x == 0) cand_n[(uint64_t)q * gridDim.x + blockIdx.x] = 0;
-        return;
+                   const uint32_t* __restrict__ t_ent, const uint32_t* __restrict__ t_nnz, uint32_t k, TopkScratch ts,
+                   uint64_t* __restrict__ mv_out, uint32_t* __restrict__ out_ids, int64_t* __restrict__ out_scores,
+                   uint32_t* __restrict__ out_n, uint32_t nq) {
+    uint32_t lo = 0, hi = nq;  // the query owning this CTA: last one with cta0 <= blockIdx.x
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (queries[mid].cta0 <= blockIdx.x) lo = mid; else hi = mid;
     }
-    extern __shared__ uint4 dyn_limbs[];
-    uint4* gl = dyn_limbs;           // 2 x uint4 per k
-    uint4* xl = dyn_limbs + 2 * n1;
+    const uint32_t q = lo;
+    const DecodeQuery dq = queries[q];
+    const uint32_t cta = blockIdx.x - dq.cta0;
+    const uint32_t n1 = dc.n1;
+    extern __shared__ uint4 dyn_limbs[];  // 2 x uint4 per column: g's n1 columns, then x's
     __shared__ uint64_t vs[N];
     __shared__ uint32_t tl[N];
     __shared__ TopkBuf buf;
+    __shared__ int last_s;
     const uint32_t tn = min(t_nnz[q], (uint32_t)N);
-    for (uint32_t kk = threadIdx.x; kk < n1; kk += blockDim.x) {
-        const uint64_t gv = gg[(uint64_t)q * n1 + kk], xv = xx[(uint64_t)q * n1 + kk];
-        Limbs3 b = limbs(gv), c = limbs_hi(gv);
-        gl[2 * kk] = make_uint4(b.b0, b.b1, b.b2, c.b0);
-        gl[2 * kk + 1] = make_uint4(c.b1, c.b2, 0u, 0u);
-        b = limbs(xv); c = limbs_hi(xv);
-        xl[2 * kk] = make_uint4(b.b0, b.b1, b.b2, c.b0);
-        xl[2 * kk + 1] = make_uint4(c.b1, c.b2, 0u, 0u);
+    for (uint32_t kk = threadIdx.x; kk < 2 * n1; kk += blockDim.x) {
+        const uint64_t w = kk < n1 ? gg[(uint64_t)q * n1 + kk] : xx[(uint64_t)q * n1 + (kk - n1)];
+        const Limbs3 b = limbs(w), c = limbs_hi(w);
+        dyn_limbs[2 * kk] = make_uint4(b.b0, b.b1, b.b2, c.b0);
+        dyn_limbs[2 * kk + 1] = make_uint4(c.b1, c.b2, 0u, 0u);
     }
     for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) vs[j] = vv[(uint64_t)q * N + j];
     for (uint32_t c = threadIdx.x; c < tn; c += blockDim.x) tl[c] = t_ent[(uint64_t)q * N + c];
     if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
     __syncthreads();
 
-    const uint64_t rbase = segs[dq.seg0].out0;
-    const ScanSeg last = segs[dq.seg0 + dq.nseg - 1];
-    const uint64_t qrows = last.out0 + last.rows - rbase;
-    const uint64_t per = (qrows + gridDim.x - 1) / gridDim.x;
-    const uint64_t v_begin = (uint64_t)blockIdx.x * per;
-    const uint64_t v_end = min(qrows, v_begin + per);
+    uint64_t rbase = 0, qrows = 0;
+    if (dq.nseg) {  // nseg == 0: every probed list of this query was empty
+        rbase = segs[dq.seg0].out0;
+        const ScanSeg last = segs[dq.seg0 + dq.nseg - 1];
+        qrows = last.out0 + last.rows - rbase;
+    }
     const bool one_seg = dq.nseg == 1;
-
-    for (uint64_t tile = v_begin; tile < v_end; tile += 2 * DT_THREADS) {
-        uint64_t vrow[2], grow[2], ridx[2];
-        bool valid[2];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            vrow[h] = tile + threadIdx.x + (uint64_t)h * DT_THREADS;
-            valid[h] = vrow[h] < v_end;
-            ridx[h] = rbase + (valid[h] ? vrow[h] : v_begin);
-            const ScanSeg sg = segs[one_seg ? dq.seg0 : find_query_seg(segs, dq.seg0, dq.nseg, ridx[h])];
-            grow[h] = sg.row0 + (ridx[h] - sg.out0);
+    const uint64_t tiles = (qrows + DT_THREADS - 1) / DT_THREADS;
+    for (uint64_t tile = cta; tile < tiles; tile += dq.ctas) {
+        const uint64_t v = tile * DT_THREADS + threadIdx.x;
+        const bool valid = v < qrows;
+        int64_t score = 0;
+        uint32_t id = 0;
+        if (valid) {
+            const uint64_t ridx = rbase + v;
+            const ScanSeg sg = segs[one_seg ? dq.seg0 : find_query_seg(segs, dq.seg0, dq.nseg, ridx)];
+            const uint64_t gr = sg.row0 + (ridx - sg.out0);
+            const uint64_t dense = dense_terms_row(dc.alh_b, n1, gr, dyn_limbs);
+            const uint64_t m_t = m_times_t_row(dc, gr, tl, tn);
+            const uint64_t s_v = s_times_v_row(dc, gr, vs);
+            const uint64_t mv = sub_mod(sub_mod(r[ridx], add_mod(dense, m_t)), s_v);
+            if (mv_out) mv_out[ridx] = mv;
+            score = to_signed(mv);
+            id = dc.ids ? dc.ids[gr] : (uint32_t)gr;
         }
-        uint64_t al_g0 = 0, al_g1 = 0, h_x0 = 0, h_x1 = 0;
-        if (valid[0]) {
-            cm_dot2(al_cm, total_rows, grow[0], grow[1], valid[1], gl, n1, al_g0, al_g1);
-            cm_dot2(h_cm, total_rows, grow[0], grow[1], valid[1], xl, n1, h_x0, h_x1);
-        }
-        int64_t score[2] = {0, 0};
-        uint32_t id[2] = {0, 0};
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            if (!valid[h]) continue;
-            const uint64_t gr = grow[h];
-            // M T: signed column sums, lazily folded
-            uint64_t m_t = 0;
-            uint32_t c = 0;
-            for (; c + 8 <= tn; c += 8) {  // 8 gathers in flight, folded two terms at a time
-                uint64_t x[8];
-                uint32_t e[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) {
-                    e[q] = tl[c + q];
-                    x[q] = __ldg(mp_cm + (uint64_t)(e[q] & 0x3ffu) * total_rows + gr);
-                }
-#pragma unroll
-                for (int q = 0; q < 8; q += 2)
-                    m_t = fold(m_t) + signed_term(x[q], e[q] >> 31) + signed_term(x[q + 1], e[q + 1] >> 31);
-            }
-            for (; c < tn; ++c) {
-                const uint32_t e = tl[c];
-                m_t = fold(m_t) + signed_term(__ldg(mp_cm + (uint64_t)(e & 0x3ffu) * total_rows + gr), e >> 31);
-            }
-            m_t = canon(m_t);
-            // S v_enc over this row's sliced-ELL entries
-            const uint64_t slice = gr >> 5;
-            const uint32_t sl = (uint32_t)(gr & 31), off = s_off[slice], wdt = s_w[slice];
-            uint64_t s_v = 0;
-            uint32_t cc = 0;
-            for (; cc + 8 <= wdt; cc += 8) {  // 8 entry loads in flight
-                uint16_t f[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) f[q] = __ldg(s_ell + off + (uint64_t)(cc + q) * 32 + sl);
-#pragma unroll
-                for (int q = 0; q < 8; q += 2) {
-                    const uint64_t y0 = f[q] == 0xffffu ? 0 : signed_term(vs[f[q] & 0x3ffu], f[q] & 0x8000u);
-                    const uint64_t y1 = f[q + 1] == 0xffffu ? 0 : signed_term(vs[f[q + 1] & 0x3ffu], f[q + 1] & 0x8000u);
-                    s_v = fold(s_v) + y0 + y1;
-                }
-            }
-            for (; cc < wdt; ++cc) {
-                const uint16_t f = __ldg(s_ell + off + (uint64_t)cc * 32 + sl);
-                s_v = fold(s_v) + (f == 0xffffu ? 0 : signed_term(vs[f & 0x3ffu], f & 0x8000u));
-            }
-            s_v = canon(s_v);
-            const uint64_t alg = h ? al_g1 : al_g0, hx = h ? h_x1 : h_x0;
-            const uint64_t mv = sub_mod(sub_mod(r[ridx[h]], add_mod(alg, m_t)), add_mod(hx, s_v));
-            if (mv_out) mv_out[ridx[h]] = mv;
-            score[h] = to_signed(mv);
-            id[h] = ids ? ids[gr] : (uint32_t)gr;
-        }
-        const int64_t ts = buf.thr_s;
-        const uint32_t ti = buf.thr_i;
+        const int64_t th_s = buf.thr_s;
+        const uint32_t th_i = buf.thr_i;
         const int ht = buf.have_thr;
-        topk_offer(buf, valid[0], score[0], id[0], ts, ti, ht);
-        topk_offer(buf, valid[1], score[1], id[1], ts, ti, ht);
-        if (topk_full(buf, CAND_CAP - 2 * DT_THREADS)) topk_compact(buf, (int)k);
+        topk_offer(buf, valid, score, id, th_s, th_i, ht);
+        if (topk_full(buf, CAND_CAP - DT_THREADS)) topk_compact(buf, (int)k);
     }
     topk_compact(buf, (int)k);
     const int keep = min(buf.cnt, (int)k);
-    const uint64_t slot = (uint64_t)q * gridDim.x + blockIdx.x;
+    const uint32_t ctas = dq.ctas;
+    const uint64_t slot = blockIdx.x;
     for (int i = threadIdx.x; i < keep; i += blockDim.x) {
-        cand_s[slot * k + i] = buf.s[i];
-        cand_i[slot * k + i] = buf.id[i];
+        ts.cand_s[slot * k + i] = buf.s[i];
+        ts.cand_i[slot * k + i] = buf.id[i];
     }
-    if (threadIdx.x == 0) cand_n[slot] = (uint32_t)keep;
+    if (threadIdx.x == 0) ts.cand_n[slot] = (uint32_t)keep;
+    __threadfence();  // this CTA's lists are visible device-wide before its ticket
+    __syncthreads();
+    if (threadIdx.x == 0) last_s = atomicAdd(&ts.done[q], 1u) == ctas - 1;
+    __syncthreads();
+    if (!last_s) return;
+
+    // ---------------------------------------------------------- merge (last CTA of the query)
+    __threadfence();
+    if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
+    __syncthreads();
+    // Four tiles of entries per round: their loads (written by other CTAs
+    // during this launch, so read through L2) are all in flight before the
+    // offers; entries past a list's count are loaded and ignored.
+    const uint64_t total = (uint64_t)ctas * k;
+    for (uint64_t t0 = 0; t0 < total; t0 += 4 * DT_THREADS) {
+        bool valid[4];
+        int64_t sc[4];
+        uint32_t id[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t e = t0 + u * DT_THREADS + threadIdx.x;
+            valid[u] = false;
+            sc[u] = 0;
+            id[u] = 0;
+            if (e < total) {
+                const uint64_t sl = (uint64_t)dq.cta0 + e / k;
+                const uint32_t i = (uint32_t)(e % k);
+                const uint32_t n = __ldcg(ts.cand_n + sl);
+                sc[u] = __ldcg(ts.cand_s + sl * k + i);
+                id[u] = __ldcg(ts.cand_i + sl * k + i);
+                valid[u] = i < n;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int64_t th_s = buf.thr_s;
+            const uint32_t th_i = buf.thr_i;
+            const int ht = buf.have_thr;
+            topk_offer(buf, valid[u], sc[u], id[u], th_s, th_i, ht);
+            if (topk_full(buf, CAND_CAP - DT_THREADS)) topk_compact(buf, (int)k);
+        }
+    }
+    topk_compact(buf, (int)k);
+    const int out_keep = min(buf.cnt, (int)k);
+    for (int i = threadIdx.x; i < out_keep; i += blockDim.x) {
+        out_ids[(uint64_t)q * k + i] = buf.id[i];
+        out_scores[(uint64_t)q * k + i] = buf.s[i];
+    }
+    if (threadIdx.x == 0) {
+        out_n[q] = (uint32_t)out_keep;
+        ts.done[q] = 0;
+    }
 }
 
 __global__ void __launch_bounds__(DT_THREADS)
@@ -972,24 +1090,28 @@ void launch_dense_terms(const uint64_t* d_al_cm, const uint64_t* d_h_cm, uint64_
     dense_terms_kernel<<<grid_for(rows, 256, 148 * 8), 256, 0, s>>>(d_al_cm, d_h_cm, rows, n1, d_g, d_x, d_out);
 }
 
-void launch_decode_topk(const uint64_t* d_r, const uint64_t* d_al_cm, const uint64_t* d_h_cm, const uint64_t* d_mp_cm,
-                        const uint16_t* d_s_ell, const uint32_t* d_s_off, const uint16_t* d_s_w, const uint32_t* d_ids,
-                        uint64_t total_rows, uint32_t n1, const ScanSeg* d_segs, const DecodeQuery* d_q, uint32_t nq,
-                        const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
-                        const uint32_t* d_t_nnz, uint32_t k, int ctas_per_query, TopkScratch scratch,
+void launch_decode_layout(const uint64_t* d_al_cm, const uint64_t* d_h_cm, const uint64_t* d_mp_cm, uint64_t rows,
+                          uint32_t n1, uint64_t* d_alh_b, int8_t* d_m8_b, uint32_t* d_bad, cudaStream_t s) {
+    cudaMemsetAsync(d_bad, 0, 4, s);
+    if (!rows) return;
+    decode_layout_kernel<<<148 * 16, 256, 0, s>>>(d_al_cm, d_h_cm, d_mp_cm, rows, n1, d_alh_b, d_m8_b, d_bad);
+}
+
+void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanSeg* d_segs, const DecodeQuery* d_q,
+                        uint32_t nq, const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
+                        const uint32_t* d_t_nnz, uint32_t k, uint32_t total_ctas, TopkScratch scratch,
                         uint64_t* d_mv_out, uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n,
                         cudaStream_t s) {
+    if (!nq) return;
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(decode_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 32 * 512);
+        cudaFuncSetAttribute(decode_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 2 * 512 * 16);
         attr_set = true;
     }
-    dim3 grid(ctas_per_query, nq);
-    decode_topk_kernel<<<grid, DT_THREADS, 2 * 32 * n1, s>>>(d_r, d_al_cm, d_h_cm, d_mp_cm, d_s_ell, d_s_off, d_s_w, d_ids,
-                                                   total_rows, n1, d_segs, d_q, d_v, d_g, d_x, d_t, d_t_nnz, k,
-                                                   scratch.cand_s, scratch.cand_i, scratch.cand_n, d_mv_out);
-    topk_merge_kernel<<<nq, DT_THREADS, 0, s>>>(scratch.cand_s, scratch.cand_i, scratch.cand_n, ctas_per_query, k,
-                                                d_out_ids, d_out_scores, d_out_n);
+    cudaMemsetAsync(scratch.done, 0, (uint64_t)nq * 4, s);
+    decode_topk_kernel<<<total_ctas, DT_THREADS, 2 * 2 * dc.n1 * 16, s>>>(d_r, dc, d_segs, d_q, d_v, d_g, d_x, d_t,
+                                                                         d_t_nnz, k, scratch, d_mv_out, d_out_ids,
+                                                                         d_out_scores, d_out_n, nq);
 }
 
 void launch_topk_rows(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_c, uint64_t ld, uint64_t rows,

@@ -10,8 +10,15 @@
 //           0xFFFF = padding; s_off[slice] = u32 offset of the slice's data,
 //           s_w[slice] = width
 //   ids     u32 [rows]         global vector id of each row (IVF), or null
-// Column-major client arrays make the decode's thread-per-row reads
-// coalesced; the row-major m_enc makes the scan's warp-per-row reads
+// Decode copies of the client state, in blocks of 32 rows (rows32 = rows
+// rounded up to 32; entries past the last row are 0):
+//   alh_b   u64 [rows32/32][2*n1][32]  AL columns then H columns
+//   m8_b    s8  [rows32/32][1024][32]  plaintext M when every entry is
+//           int8-valued (quantised corpora), else absent
+// A warp that decodes 32 consecutive rows reads one 256-byte (u64) or
+// 32-byte (s8) run per column, and a block's columns are contiguous.
+// Column-major client arrays make the thread-per-row reads of the other
+// kernels coalesced; the row-major m_enc makes the scan's warp-per-row reads
 // coalesced.
 #pragma once
 #include <cuda_runtime.h>
@@ -90,6 +97,8 @@ void launch_dense_terms(const uint64_t* d_al_cm, const uint64_t* d_h_cm, uint64_
 struct DecodeQuery {
     uint32_t seg0;     // first segment of this query in the segment array
     uint32_t nseg;
+    uint32_t cta0;     // the query's decode CTAs: [cta0, cta0 + ctas) of the launch
+    uint32_t ctas;
 };
 
 // Top-k candidate lists.
@@ -97,20 +106,41 @@ constexpr int TOPK_MAX = 1024;
 constexpr int DECODE_CTAS_PER_QUERY_MAX = 148;
 
 struct TopkScratch {
-    int64_t* cand_s;    // [nq][ctas][k]
+    int64_t* cand_s;    // [CTAs][k]
     uint32_t* cand_i;
-    uint32_t* cand_n;   // [nq][ctas]
+    uint32_t* cand_n;   // [CTAs]
+    uint32_t* done;     // [nq] CTAs finished (decode_topk only; zeroed by its launcher)
 };
 
-// Decode + fp_to_signed + per-CTA top-k for every query, then a merge into
+// The corpus arrays the decode reads (layouts above).
+struct DecodeCorpus {
+    const uint64_t* alh_b;
+    const int8_t* m8_b;     // null: M T from mp_cm
+    const uint64_t* mp_cm;
+    const uint16_t* s_ell;
+    const uint32_t* s_off;
+    const uint16_t* s_w;
+    const uint32_t* ids;    // null: ids are row numbers
+    uint64_t rows;
+    uint32_t n1;
+};
+
+// Builds alh_b from al_cm / h_cm and m8_b from mp_cm (m8_b nullable, e.g.
+// without client state); *d_bad (zeroed here) gets bit 0 if an entry of
+// mp_cm is not int8-valued, in which case m8_b must not be used.
+void launch_decode_layout(const uint64_t* d_al_cm, const uint64_t* d_h_cm, const uint64_t* d_mp_cm, uint64_t rows,
+                          uint32_t n1, uint64_t* d_alh_b, int8_t* d_m8_b, uint32_t* d_bad, cudaStream_t s);
+
+// Decode + fp_to_signed + top-k for every query: each CTA ranks its rows,
+// and the last CTA of a query to finish merges the CTAs' lists into
 // out_ids/out_scores [nq][k] (score desc, id asc) and out_n [nq].
 // r is indexed like the scan output (segment out0).  mv_out (nullable)
-// receives the decoded residues at the same offsets.
-void launch_decode_topk(const uint64_t* d_r, const uint64_t* d_al_cm, const uint64_t* d_h_cm, const uint64_t* d_mp_cm,
-                        const uint16_t* d_s_ell, const uint32_t* d_s_off, const uint16_t* d_s_w, const uint32_t* d_ids,
-                        uint64_t total_rows, uint32_t n1, const ScanSeg* d_segs, const DecodeQuery* d_q, uint32_t nq,
-                        const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
-                        const uint32_t* d_t_nnz, uint32_t k, int ctas_per_query, TopkScratch scratch,
+// receives the decoded residues at the same offsets.  The launch has
+// total_ctas CTAs, query q owning d_q[q].cta0 .. + d_q[q].ctas (every query
+// at least one; cta0 ascending); the scratch lists are indexed by CTA.
+void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanSeg* d_segs, const DecodeQuery* d_q,
+                        uint32_t nq, const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
+                        const uint32_t* d_t_nnz, uint32_t k, uint32_t total_ctas, TopkScratch scratch,
                         uint64_t* d_mv_out, uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n,
                         cudaStream_t s);
 

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from bnutil import N, P, cluster, query, uniform_fp
+from bnutil import N, P, cluster, int8_matrix, query, uniform_fp
 
 pytestmark = pytest.mark.gpu
 
@@ -162,6 +162,45 @@ def test_query_matches_oracle(ctx, engine, m, trials, k):
         assert failed[b] == fo == -1
         assert np.array_equal(hits[b][0], ids) and np.array_equal(hits[b][1], sc)
         assert len(hits[b][0]) == min(k, m)
+
+
+@pytest.mark.parametrize("mode", ["int8", "uniform", "row_of_128", "row_of_minus_129"])
+def test_query_plaintext_ranges_match_oracle(ctx, mode):
+    """The decode sums M T from an int8 copy of the plaintext when every entry
+    is int8-valued, and from the u64 residues otherwise (uniform residues, or
+    one row just outside [-128, 127]); both are bit-exact."""
+    m = 1500
+    if mode == "uniform":
+        M, L, cl = cluster(m, 61, uniform=True)
+    else:
+        M = int8_matrix(m, 768, 62)
+        if mode != "int8":
+            M[777, :768] = 128 if mode == "row_of_128" else P - 129
+        L = O.generate_subspace(bytes([1]) * 32)
+        cl = O.encrypt_cluster(M.reshape(-1), m, L, O.derive_h_seed(7, 0))
+    f = flat_from_cluster(ctx, M, L, cl)
+    v, q_seed, _ = query(L, 63)
+    fo, ids, sc, ro, mvo, enc = _oracle_query(M, L, cl, v, q_seed, 2, 20)
+    hits, failed, r, mv = f.query(enc.v_enc[None], enc.g[None], [(enc.t_idx, enc.t_sign)],
+                                  [O.domain_separate(q_seed, b"protocol2")], 2, 20, want_r=True, want_mv=True)
+    assert np.array_equal(r[0], ro) and np.array_equal(mv[0], mvo)
+    assert np.array_equal(hits[0][0], ids) and np.array_equal(hits[0][1], sc)
+    assert failed[0] == fo == -1
+
+
+def test_decode_int8_copy_is_kept_only_for_int8_plaintext(ctx):
+    """Device bytes of the client state: the int8 copy of M (1024 bytes per
+    row, rows rounded up to 32) exists only for int8-valued plaintext."""
+    m = 1000
+    M = int8_matrix(m, 768, 64)
+    L = O.generate_subspace(bytes([1]) * 32)
+    cl = O.encrypt_cluster(M.reshape(-1), m, L, O.derive_h_seed(7, 0))
+    a = flat_from_cluster(ctx, M, L, cl).info()[1]
+    M2 = M.copy()
+    M2[3, 0] = 128
+    cl2 = O.encrypt_cluster(M2.reshape(-1), m, L, O.derive_h_seed(7, 0))
+    b = flat_from_cluster(ctx, M2, L, cl2).info()[1]
+    assert a - b == (m + 31) // 32 * 32 * N
 
 
 def test_device_encrypted_handle_matches_host_encrypted(ctx):
