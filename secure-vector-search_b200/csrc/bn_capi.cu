@@ -251,8 +251,12 @@ int build_corpus_from_plain(bn_ctx* ctx, Corpus& c, const uint64_t* m_q, uint64_
 // ------------------------------------------------------------------ pipeline
 void finish_meta(HostMeta& hm) {
     hm.seg_blk.assign(hm.segs.size() + 1, 0);
-    for (size_t i = 0; i < hm.segs.size(); ++i)
-        hm.seg_blk[i + 1] = hm.seg_blk[i] + (hm.segs[i].rows + SCAN_ROWS - 1) / SCAN_ROWS;
+    hm.seg_unit.assign(hm.segs.size() + 1, 0);
+    for (size_t i = 0; i < hm.segs.size(); ++i) {
+        const ScanSeg& sg = hm.segs[i];
+        hm.seg_blk[i + 1] = hm.seg_blk[i] + (sg.rows + SCAN_ROWS - 1) / SCAN_ROWS;
+        hm.seg_unit[i + 1] = hm.seg_unit[i] + (sg.rows ? ((sg.row0 + sg.rows - 1) >> 5) - (sg.row0 >> 5) + 1 : 0);
+    }
     hm.blocks.clear();
     hm.panels.clear();
     hm.seg_block0.assign(hm.vsegs.size() + 1, 0);
@@ -298,6 +302,7 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
     o.seeds = L.take<uint8_t>((uint64_t)z.B * 32);
     o.segs = L.take<ScanSeg>(z.nseg);
     o.seg_blk = L.take<uint64_t>(z.nseg + 1);
+    o.seg_unit = L.take<uint64_t>(z.nseg + 1);
     o.vsegs = L.take<VerifySeg>(z.nvseg);
     o.dq = L.take<DecodeQuery>(z.B);
     o.tc_blocks = L.take<TcBlock>(z.nblocks);
@@ -404,7 +409,7 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
     }
     if (z.k) {
         launch_lt_times_v(c.L.at<uint64_t>(), c.n1, in.v, z.B, sc.x, s);
-        launch_decode_topk(sc.r, decode_corpus(c), m.segs, m.dq, z.B, in.v, in.g, sc.x, in.t, in.t_nnz, z.k,
+        launch_decode_topk(sc.r, decode_corpus(c), m.segs, m.seg_unit, m.dq, z.B, in.v, in.g, sc.x, in.t, in.t_nnz, z.k,
                            z.ctas, sc.topk, out.mv, out.ids, out.scores, out.n, s);
     } else {
         CU(cudaMemsetAsync(out.n, 0, (uint64_t)z.B * 4, s));
@@ -415,7 +420,7 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
 
 Meta meta_at(char* d, const RunLayout& o, const HostMeta& hm, const TcMaps* maps) {
     return Meta{reinterpret_cast<ScanSeg*>(d + o.segs), reinterpret_cast<uint64_t*>(d + o.seg_blk),
-                (uint32_t)hm.segs.size(), hm.seg_blk.empty() ? 0 : hm.seg_blk.back(),
+                reinterpret_cast<uint64_t*>(d + o.seg_unit), (uint32_t)hm.segs.size(), hm.seg_blk.empty() ? 0 : hm.seg_blk.back(),
                 reinterpret_cast<VerifySeg*>(d + o.vsegs), (uint32_t)hm.vsegs.size(),
                 reinterpret_cast<DecodeQuery*>(d + o.dq), reinterpret_cast<TcBlock*>(d + o.tc_blocks),
                 (uint32_t)hm.blocks.size(), reinterpret_cast<TcPanel*>(d + o.tc_panels), (uint32_t)hm.panels.size(),
@@ -435,6 +440,7 @@ Scratch scratch_at(char* d, const RunLayout& o) {
 void pack_meta(char* h, const RunLayout& o, const HostMeta& hm) {
     memcpy(h + o.segs, hm.segs.data(), hm.segs.size() * sizeof(ScanSeg));
     memcpy(h + o.seg_blk, hm.seg_blk.data(), hm.seg_blk.size() * 8);
+    memcpy(h + o.seg_unit, hm.seg_unit.data(), hm.seg_unit.size() * 8);
     memcpy(h + o.vsegs, hm.vsegs.data(), hm.vsegs.size() * sizeof(VerifySeg));
     memcpy(h + o.dq, hm.dq.data(), hm.dq.size() * sizeof(DecodeQuery));
     memcpy(h + o.tc_blocks, hm.blocks.data(), hm.blocks.size() * sizeof(TcBlock));
@@ -458,21 +464,22 @@ void engine_free(Engine& e) {
 }
 
 // Decode CTAs of a run: about four per SM in total (one wave of the decode
-// kernel), shared among the queries in proportion to their rows, at least
-// one per query and at most one per 256-row tile.  Returns the total.
+// kernel), shared among the queries in proportion to their units (32-row
+// blocks), at least one per query and at most one per tile of 8 units.
+// Returns the total.
 uint32_t assign_decode_ctas(HostMeta& hm, int sms) {
-    std::vector<uint64_t> rows(hm.dq.size(), 0);
+    std::vector<uint64_t> units(hm.dq.size(), 0);
     uint64_t total = 0;
     for (size_t q = 0; q < hm.dq.size(); ++q) {
         const DecodeQuery& d = hm.dq[q];
-        for (uint32_t s = d.seg0; s < d.seg0 + d.nseg; ++s) rows[q] += hm.segs[s].rows;
-        total += rows[q];
+        if (d.nseg) units[q] = hm.seg_unit[d.seg0 + d.nseg] - hm.seg_unit[d.seg0];
+        total += units[q];
     }
     const uint64_t target = (uint64_t)sms * 4;
     uint32_t next = 0;
     for (size_t q = 0; q < hm.dq.size(); ++q) {
-        uint64_t c = total ? (target * rows[q] + total - 1) / total : 1;
-        c = std::max<uint64_t>(1, std::min(c, (rows[q] + 255) / 256));
+        uint64_t c = total ? (target * units[q] + total - 1) / total : 1;
+        c = std::max<uint64_t>(1, std::min(c, (units[q] + 7) / 8));
         hm.dq[q].cta0 = next;
         hm.dq[q].ctas = (uint32_t)c;
         next += (uint32_t)c;

@@ -180,6 +180,7 @@ inline uint32_t pass_rows(uint32_t t_cnt) { return 8 * ((t_cnt + 1) & ~1u); }
 struct Meta {  // device pointers (+ host tensor maps)
     const ScanSeg* segs;
     const uint64_t* seg_blk;
+    const uint64_t* seg_unit;  // decode units (32-row corpus blocks) per segment, prefix sums
     uint32_t nseg;
     uint64_t total_blocks;
     const VerifySeg* vsegs;
@@ -227,6 +228,7 @@ struct Outputs {
 struct HostMeta {
     std::vector<ScanSeg> segs;
     std::vector<uint64_t> seg_blk;
+    std::vector<uint64_t> seg_unit;     // prefix sums of the 32-row corpus blocks each segment touches
     std::vector<VerifySeg> vsegs;
     std::vector<DecodeQuery> dq;
     std::vector<uint32_t> seg_cluster;  // IVF: list id of each segment
@@ -247,7 +249,8 @@ struct Sizes {
 // Offsets of every device buffer of one pipeline run.
 struct RunLayout {
     // inputs (contiguous from 0 -> one H2D)
-    uint64_t v, g, t, t_nnz, seeds, segs, seg_blk, vsegs, dq, tc_blocks, tc_panels, seg_panel0, seg_block0, in_end;
+    uint64_t v, g, t, t_nnz, seeds, segs, seg_blk, seg_unit, vsegs, dq, tc_blocks, tc_panels, seg_panel0, seg_block0,
+        in_end;
     // outputs (contiguous -> one D2H)
     uint64_t ids, scores, n, vfailed, ur, zv, err, out_begin, out_end;
     // internal

@@ -553,16 +553,6 @@ __device__ __forceinline__ void topk_offer(TopkBuf& b, bool valid, int64_t s, ui
     }
 }
 
-__device__ __forceinline__ uint32_t find_query_seg(const ScanSeg* __restrict__ segs, uint32_t seg0, uint32_t nseg,
-                                                   uint64_t r_idx) {
-    uint32_t lo = seg0, hi = seg0 + nseg;  // last s with segs[s].out0 <= r_idx
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (segs[mid].out0 <= r_idx) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
 // Sum of +-x (sign in bit 31 of the entry) over a gathered column list,
 // folded lazily: every term is < 2^61, three terms fit below 2^63.
 __device__ __forceinline__ uint64_t signed_term(uint64_t x, bool neg) { return neg ? P - x : x; }
@@ -593,33 +583,90 @@ __device__ __forceinline__ uint64_t dense_terms_row(const uint64_t* __restrict__
     return combine3(a0, a1, a2);
 }
 
-// M_i . T: signed column sums over the query's T entries (col | 0x80000000
-// for -1).  From the int8 blocks the sum is an exact integer, |sum| <=
-// 1024 * 128; else from the column-major residues, lazily folded.
-__device__ __forceinline__ uint64_t m_times_t_row(const DecodeCorpus& dc, uint64_t gr, const uint32_t* __restrict__ tl,
-                                                  uint32_t tn) {
-    if (dc.m8_b) {
-        const int8_t* p = dc.m8_b + (gr >> 5) * ((uint64_t)N * 32) + (gr & 31);
-        int32_t acc = 0;
-        uint32_t c = 0;
-        for (; c + 16 <= tn; c += 16) {
-            int32_t x[16];
-            uint32_t e[16];
+// Two sign-extended int16 halves from bytes 0, 1 (sel 0x9180) or 2, 3
+// (sel 0xB3A2) of x: prmt's selector msb replicates the byte's sign.
+__device__ __forceinline__ uint32_t sext_pair(uint32_t x, uint32_t sel) {
+    uint32_t d;
+    asm("prmt.b32 %0, %1, 0, %2;" : "=r"(d) : "r"(x), "r"(sel));
+    return d;
+}
+
+// M . T for the warp's 32-row block (lane l = row 32 blk + l): the T
+// columns go 32 at a time, one per lane; a lane loads its column's 32 row
+// bytes (one 32-byte run of the int8 block), widens them to 16 signed int16
+// pairs with the entry's sign, and a reduce-scatter over the lanes (lane
+// bit 4 keeps rows 0-15 or 16-31, then bits 3..0) leaves lane l the sum of
+// row l over those 32 columns (|sum| <= 32 * 128, exact in int16).  Four
+// groups of loads are in flight at a time.  Returns the exact integer.
+__device__ __forceinline__ int32_t m_times_t_warp(const int8_t* __restrict__ m8_b, uint64_t blk,
+                                                  const uint32_t* __restrict__ tl, uint32_t tn, uint32_t lane) {
+    const uint4* base = reinterpret_cast<const uint4*>(m8_b + blk * ((uint64_t)N * 32));
+    int32_t acc = 0;
+    for (uint32_t g0 = 0; g0 < tn; g0 += 4 * 32) {
+        uint4 lo[4], hi[4];
+        uint32_t neg[4];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) {
-                e[q] = tl[c + q];
-                x[q] = __ldg(p + (e[q] & 0x3ffu) * 32);
+        for (int u = 0; u < 4; ++u) {
+            const uint32_t c = g0 + u * 32 + lane;
+            lo[u] = hi[u] = make_uint4(0u, 0u, 0u, 0u);
+            neg[u] = 0;
+            if (c < tn) {
+                const uint32_t e = tl[c];
+                lo[u] = __ldg(base + (e & 0x3ffu) * 2);
+                hi[u] = __ldg(base + (e & 0x3ffu) * 2 + 1);
+                neg[u] = e >> 31;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (g0 + u * 32 >= tn) break;  // warp-uniform
+            const uint32_t wds[8] = {lo[u].x, lo[u].y, lo[u].z, lo[u].w, hi[u].x, hi[u].y, hi[u].z, hi[u].w};
+            uint32_t v[16];  // v[w]: rows 2w (low half), 2w + 1 (high half)
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                v[2 * i] = sext_pair(wds[i], 0x9180u);
+                v[2 * i + 1] = sext_pair(wds[i], 0xB3A2u);
+            }
+            if (neg[u]) {
+#pragma unroll
+                for (int w = 0; w < 16; ++w) v[w] = __vsub2(0u, v[w]);
+            }
+            // reduce-scatter: after the step over lane bit b the lane keeps
+            // the half of its words that its bit b selects
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+                const bool up = lane & 16;
+                const uint32_t send = up ? v[w] : v[w + 8], keep = up ? v[w + 8] : v[w];
+                v[w] = __vadd2(keep, __shfl_xor_sync(FULL, send, 16));
             }
 #pragma unroll
-            for (int q = 0; q < 16; ++q) acc += (e[q] >> 31) ? -x[q] : x[q];
+            for (int w = 0; w < 4; ++w) {
+                const bool up = lane & 8;
+                const uint32_t send = up ? v[w] : v[w + 4], keep = up ? v[w + 4] : v[w];
+                v[w] = __vadd2(keep, __shfl_xor_sync(FULL, send, 8));
+            }
+#pragma unroll
+            for (int w = 0; w < 2; ++w) {
+                const bool up = lane & 4;
+                const uint32_t send = up ? v[w] : v[w + 2], keep = up ? v[w + 2] : v[w];
+                v[w] = __vadd2(keep, __shfl_xor_sync(FULL, send, 4));
+            }
+            {
+                const bool up = lane & 2;
+                const uint32_t send = up ? v[0] : v[1], keep = up ? v[1] : v[0];
+                v[0] = __vadd2(keep, __shfl_xor_sync(FULL, send, 2));
+            }
+            const uint32_t pair = __vadd2(v[0], __shfl_xor_sync(FULL, v[0], 1));
+            acc += (lane & 1) ? (int32_t)(int16_t)(pair >> 16) : (int32_t)(int16_t)(pair & 0xffffu);
         }
-        for (; c < tn; ++c) {
-            const uint32_t e = tl[c];
-            const int32_t x = __ldg(p + (e & 0x3ffu) * 32);
-            acc += (e >> 31) ? -x : x;
-        }
-        return acc >= 0 ? (uint64_t)acc : P - (uint64_t)(-(int64_t)acc);
     }
+    return acc;
+}
+
+// M_i . T from the column-major residues (plaintext not int8-valued): one
+// row per lane, gathers lazily folded.
+__device__ __forceinline__ uint64_t m_times_t_cm(const uint64_t* __restrict__ mp_cm, uint64_t rows, uint64_t gr,
+                                                 const uint32_t* __restrict__ tl, uint32_t tn) {
     uint64_t m_t = 0;
     uint32_t c = 0;
     for (; c + 8 <= tn; c += 8) {  // 8 gathers in flight, folded two terms at a time
@@ -628,7 +675,7 @@ __device__ __forceinline__ uint64_t m_times_t_row(const DecodeCorpus& dc, uint64
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             e[q] = tl[c + q];
-            x[q] = __ldg(dc.mp_cm + (uint64_t)(e[q] & 0x3ffu) * dc.rows + gr);
+            x[q] = __ldg(mp_cm + (uint64_t)(e[q] & 0x3ffu) * rows + gr);
         }
 #pragma unroll
         for (int q = 0; q < 8; q += 2)
@@ -636,46 +683,81 @@ __device__ __forceinline__ uint64_t m_times_t_row(const DecodeCorpus& dc, uint64
     }
     for (; c < tn; ++c) {
         const uint32_t e = tl[c];
-        m_t = fold(m_t) + signed_term(__ldg(dc.mp_cm + (uint64_t)(e & 0x3ffu) * dc.rows + gr), e >> 31);
+        m_t = fold(m_t) + signed_term(__ldg(mp_cm + (uint64_t)(e & 0x3ffu) * rows + gr), e >> 31);
     }
     return canon(m_t);
 }
 
-// S_i . v_enc over the row's sliced-ELL entries (v_enc in shared memory).
-__device__ __forceinline__ uint64_t s_times_v_row(const DecodeCorpus& dc, uint64_t gr, const uint64_t* __restrict__ vs) {
-    const uint64_t slice = gr >> 5;
-    const uint32_t sl = (uint32_t)(gr & 31), off = dc.s_off[slice], wdt = dc.s_w[slice];
-    uint64_t s_v = 0;
-    uint32_t cc = 0;
-    for (; cc + 8 <= wdt; cc += 8) {  // 8 entry loads in flight
-        uint16_t f[8];
+// S . v_enc for the warp's 32-row block, which is exactly one sliced-ELL
+// slice ([width][32 rows] u16).  The slice is read as 16-byte chunks, chunk
+// j = lane + 32 i holding entries of column slot j / 4 for rows 8 (j % 4) ..
+// + 7, so a lane always sees the same 8 rows (8 (lane % 4) + 0..7) and
+// keeps 8 partial sums; a reduce-scatter over lane bits 4, 3, 2 then leaves
+// one row's sum per lane, and a shuffle hands row l to lane l.
+__device__ __forceinline__ uint64_t s_times_v_warp(const DecodeCorpus& dc, uint64_t blk, const uint64_t* __restrict__ vs,
+                                                   uint32_t lane) {
+    const uint32_t off = dc.s_off[blk], wdt = dc.s_w[blk];
+    const uint4* base = reinterpret_cast<const uint4*>(dc.s_ell + off);  // slice data is 64 * wdt bytes
+    const uint32_t chunks = wdt * 4;
+    uint64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t j0 = 0; j0 < chunks; j0 += 8 * 32) {
+        uint4 ch[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) f[q] = __ldg(dc.s_ell + off + (uint64_t)(cc + q) * 32 + sl);
+        for (int u = 0; u < 8; ++u) {
+            const uint32_t j = j0 + u * 32 + lane;
+            ch[u] = j < chunks ? __ldg(base + j) : make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
+        }
 #pragma unroll
-        for (int q = 0; q < 8; q += 2) {
-            const uint64_t y0 = f[q] == 0xffffu ? 0 : signed_term(vs[f[q] & 0x3ffu], f[q] & 0x8000u);
-            const uint64_t y1 = f[q + 1] == 0xffffu ? 0 : signed_term(vs[f[q + 1] & 0x3ffu], f[q + 1] & 0x8000u);
-            s_v = fold(s_v) + y0 + y1;
+        for (int u = 0; u < 8; ++u) {
+            const uint32_t w[4] = {ch[u].x, ch[u].y, ch[u].z, ch[u].w};
+#pragma unroll
+            for (int h = 0; h < 8; ++h) {
+                const uint32_t f = (w[h >> 1] >> (16 * (h & 1))) & 0xffffu;
+                const uint64_t y = f == 0xffffu ? 0 : signed_term(vs[f & 0x3ffu], f & 0x8000u);
+                acc[h] = fold(acc[h]) + y;
+            }
         }
     }
-    for (; cc < wdt; ++cc) {
-        const uint16_t f = __ldg(dc.s_ell + off + (uint64_t)cc * 32 + sl);
-        s_v = fold(s_v) + (f == 0xffffu ? 0 : signed_term(vs[f & 0x3ffu], f & 0x8000u));
+    // each step adds two values below 2^61 + 8 and folds the sum
+#pragma unroll
+    for (int h = 0; h < 8; ++h) acc[h] = fold(acc[h]);
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {  // lane bit 4: keep rows h + 4 * bit
+        const bool up = lane & 16;
+        const uint64_t send = up ? acc[h] : acc[h + 4], keep = up ? acc[h + 4] : acc[h];
+        acc[h] = fold(keep + __shfl_xor_sync(FULL, send, 16));
     }
-    return canon(s_v);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {  // lane bit 3
+        const bool up = lane & 8;
+        const uint64_t send = up ? acc[h] : acc[h + 2], keep = up ? acc[h + 2] : acc[h];
+        acc[h] = fold(keep + __shfl_xor_sync(FULL, send, 8));
+    }
+    {  // lane bit 2
+        const bool up = lane & 4;
+        const uint64_t send = up ? acc[0] : acc[1], keep = up ? acc[1] : acc[0];
+        acc[0] = fold(keep + __shfl_xor_sync(FULL, send, 4));
+    }
+    // lane l now holds row 8 (l & 3) + 4 b4 + 2 b3 + b2 (b = bits of l); lane
+    // r fetches its row from the lane that holds it
+    const uint32_t src = (lane >> 3) | ((lane & 1) << 2) | (((lane >> 1) & 1) << 3) | (((lane >> 2) & 1) << 4);
+    return canon(__shfl_sync(FULL, acc[0], src));
 }
 
-// One row per thread; the CTAs of a query take 256-row tiles of its r-space
-// range in turn, so every CTA of the query gets the same number of tiles
-// give or take one (the host gives each query CTAs in proportion to its
-// rows).  Mv = r - (AL g + H x) - M T - S v, ranked by
+// A warp decodes one unit: a segment's rows inside one aligned 32-row block
+// of the corpus (lane l = row 32 blk + l; lanes outside the segment idle in
+// the row work but join the block-wide M T and S v).  A CTA takes tiles of
+// 8 units of its query in turn (the host gives each query CTAs in
+// proportion to its units).  Mv = r - (AL g + H x) - M T - S v, ranked by
 // fp_to_signed into the CTA's candidate buffer; the CTA's best k go to the
 // scratch lists, and the last CTA of the query to finish (a ticket taken
 // after a device-scope fence, no waiting) merges them.
-__global__ void __launch_bounds__(DT_THREADS)
+constexpr uint32_t DT_WARPS = DT_THREADS / 32;
+
+__global__ void __launch_bounds__(DT_THREADS, 4)
 decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSeg* __restrict__ segs,
-                   const DecodeQuery* __restrict__ queries, const uint64_t* __restrict__ vv,
-                   const uint64_t* __restrict__ gg, const uint64_t* __restrict__ xx,
+                   const uint64_t* __restrict__ seg_unit, const DecodeQuery* __restrict__ queries,
+                   const uint64_t* __restrict__ vv, const uint64_t* __restrict__ gg, const uint64_t* __restrict__ xx,
                    const uint32_t* __restrict__ t_ent, const uint32_t* __restrict__ t_nnz, uint32_t k, TopkScratch ts,
                    uint64_t* __restrict__ mv_out, uint32_t* __restrict__ out_ids, int64_t* __restrict__ out_scores,
                    uint32_t* __restrict__ out_n, uint32_t nq) {
@@ -688,6 +770,7 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
     const DecodeQuery dq = queries[q];
     const uint32_t cta = blockIdx.x - dq.cta0;
     const uint32_t n1 = dc.n1;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     extern __shared__ uint4 dyn_limbs[];  // 2 x uint4 per column: g's n1 columns, then x's
     __shared__ uint64_t vs[N];
     __shared__ uint32_t tl[N];
@@ -705,30 +788,47 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
     if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
     __syncthreads();
 
-    uint64_t rbase = 0, qrows = 0;
-    if (dq.nseg) {  // nseg == 0: every probed list of this query was empty
-        rbase = segs[dq.seg0].out0;
-        const ScanSeg last = segs[dq.seg0 + dq.nseg - 1];
-        qrows = last.out0 + last.rows - rbase;
+    uint64_t u_begin = 0, u_count = 0;  // nseg == 0: every probed list of this query was empty
+    if (dq.nseg) {
+        u_begin = seg_unit[dq.seg0];
+        u_count = seg_unit[dq.seg0 + dq.nseg] - u_begin;
     }
-    const bool one_seg = dq.nseg == 1;
-    const uint64_t tiles = (qrows + DT_THREADS - 1) / DT_THREADS;
+    const uint64_t tiles = (u_count + DT_WARPS - 1) / DT_WARPS;
     for (uint64_t tile = cta; tile < tiles; tile += dq.ctas) {
-        const uint64_t v = tile * DT_THREADS + threadIdx.x;
-        const bool valid = v < qrows;
+        const uint64_t u = tile * DT_WARPS + warp;
+        bool valid = false;
         int64_t score = 0;
         uint32_t id = 0;
-        if (valid) {
-            const uint64_t ridx = rbase + v;
-            const ScanSeg sg = segs[one_seg ? dq.seg0 : find_query_seg(segs, dq.seg0, dq.nseg, ridx)];
-            const uint64_t gr = sg.row0 + (ridx - sg.out0);
-            const uint64_t dense = dense_terms_row(dc.alh_b, n1, gr, dyn_limbs);
-            const uint64_t m_t = m_times_t_row(dc, gr, tl, tn);
-            const uint64_t s_v = s_times_v_row(dc, gr, vs);
-            const uint64_t mv = sub_mod(sub_mod(r[ridx], add_mod(dense, m_t)), s_v);
-            if (mv_out) mv_out[ridx] = mv;
-            score = to_signed(mv);
-            id = dc.ids ? dc.ids[gr] : (uint32_t)gr;
+        if (u < u_count) {  // warp-uniform
+            const uint64_t gu = u_begin + u;
+            uint32_t sa = dq.seg0, sb = dq.seg0 + dq.nseg;  // last segment with seg_unit <= gu
+            while (sb - sa > 1) {
+                const uint32_t mid = (sa + sb) >> 1;
+                if (seg_unit[mid] <= gu) sa = mid; else sb = mid;
+            }
+            const ScanSeg sg = segs[sa];
+            const uint64_t blk = (sg.row0 >> 5) + (gu - seg_unit[sa]);
+            const uint64_t gr = blk * 32 + lane;
+            valid = gr >= sg.row0 && gr < sg.row0 + sg.rows;
+            const uint64_t ridx = sg.out0 + (gr - sg.row0);
+            uint64_t rv = 0;
+            if (valid) {
+                rv = r[ridx];
+                id = dc.ids ? dc.ids[gr] : (uint32_t)gr;
+            }
+            uint64_t m_t = 0;
+            if (dc.m8_b) {
+                const int32_t mt = m_times_t_warp(dc.m8_b, blk, tl, tn, lane);
+                m_t = mt >= 0 ? (uint64_t)mt : P - (uint64_t)(-(int64_t)mt);
+            }
+            const uint64_t s_v = s_times_v_warp(dc, blk, vs, lane);
+            if (valid) {
+                if (!dc.m8_b) m_t = m_times_t_cm(dc.mp_cm, dc.rows, gr, tl, tn);
+                const uint64_t dense = dense_terms_row(dc.alh_b, n1, gr, dyn_limbs);
+                const uint64_t mv = sub_mod(sub_mod(rv, add_mod(dense, m_t)), s_v);
+                if (mv_out) mv_out[ridx] = mv;
+                score = to_signed(mv);
+            }
         }
         const int64_t th_s = buf.thr_s;
         const uint32_t th_i = buf.thr_i;
@@ -1097,8 +1197,8 @@ void launch_decode_layout(const uint64_t* d_al_cm, const uint64_t* d_h_cm, const
     decode_layout_kernel<<<148 * 16, 256, 0, s>>>(d_al_cm, d_h_cm, d_mp_cm, rows, n1, d_alh_b, d_m8_b, d_bad);
 }
 
-void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanSeg* d_segs, const DecodeQuery* d_q,
-                        uint32_t nq, const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
+void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanSeg* d_segs, const uint64_t* d_seg_unit,
+                        const DecodeQuery* d_q, uint32_t nq, const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
                         const uint32_t* d_t_nnz, uint32_t k, uint32_t total_ctas, TopkScratch scratch,
                         uint64_t* d_mv_out, uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n,
                         cudaStream_t s) {
@@ -1109,9 +1209,9 @@ void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanS
         attr_set = true;
     }
     cudaMemsetAsync(scratch.done, 0, (uint64_t)nq * 4, s);
-    decode_topk_kernel<<<total_ctas, DT_THREADS, 2 * 2 * dc.n1 * 16, s>>>(d_r, dc, d_segs, d_q, d_v, d_g, d_x, d_t,
-                                                                         d_t_nnz, k, scratch, d_mv_out, d_out_ids,
-                                                                         d_out_scores, d_out_n, nq);
+    decode_topk_kernel<<<total_ctas, DT_THREADS, 2 * 2 * dc.n1 * 16, s>>>(d_r, dc, d_segs, d_seg_unit, d_q, d_v, d_g,
+                                                                         d_x, d_t, d_t_nnz, k, scratch, d_mv_out,
+                                                                         d_out_ids, d_out_scores, d_out_n, nq);
 }
 
 void launch_topk_rows(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_c, uint64_t ld, uint64_t rows,

@@ -135,11 +135,13 @@ void launch_decode_layout(const uint64_t* d_al_cm, const uint64_t* d_h_cm, const
 // and the last CTA of a query to finish merges the CTAs' lists into
 // out_ids/out_scores [nq][k] (score desc, id asc) and out_n [nq].
 // r is indexed like the scan output (segment out0).  mv_out (nullable)
-// receives the decoded residues at the same offsets.  The launch has
-// total_ctas CTAs, query q owning d_q[q].cta0 .. + d_q[q].ctas (every query
-// at least one; cta0 ascending); the scratch lists are indexed by CTA.
-void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanSeg* d_segs, const DecodeQuery* d_q,
-                        uint32_t nq, const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
+// receives the decoded residues at the same offsets.  The work units are
+// the aligned 32-row corpus blocks each segment touches: segment s owns
+// units [d_seg_unit[s], d_seg_unit[s + 1]) (nseg + 1 entries).  The launch
+// has total_ctas CTAs, query q owning d_q[q].cta0 .. + d_q[q].ctas (every
+// query at least one; cta0 ascending); the scratch lists are indexed by CTA.
+void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanSeg* d_segs, const uint64_t* d_seg_unit,
+                        const DecodeQuery* d_q, uint32_t nq, const uint64_t* d_v, const uint64_t* d_g, const uint64_t* d_x, const uint32_t* d_t,
                         const uint32_t* d_t_nnz, uint32_t k, uint32_t total_ctas, TopkScratch scratch,
                         uint64_t* d_mv_out, uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n,
                         cudaStream_t s);
