@@ -602,7 +602,20 @@ def run_serving(args, flat, ivf, flat_L, data, dist):
                       k=10, block_min=2)
     out = {"corpora": {"flat_N": flat.m, "ivf_N": int(data["offsets"][-1]), "nlist": int(len(data["sizes"]))},
            "config": {"max_batch": 64, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 2},
-           "mix": "50% flat / 50% IVF, nprobe uniform in {8, 32, 128}", "rates": {}}
+           "mix": "50% flat / 50% IVF, nprobe uniform in {8, 32, 128}",
+           "warmup": "512 requests submitted at once before the timed rates (slots create their plans and "
+                     "workspaces), not counted", "rates": {}}
+    # warm-up: the slots grow their block plans and workspaces to the largest
+    # batches once, as a service does at start-up
+    warm = []
+    for j in range(512):
+        i = j % pool
+        if j & 1:
+            warm.append(srv.submit_flat(fenc[i][0], fenc[i][1], fenc[i][2], fenc[i][3], fseeds[i]))
+        else:
+            warm.append(srv.submit_ivf(probes[i], ienc[i][0], ienc[i][1], ienc[i][2], ienc[i][3], iseeds[i]))
+    for t in warm:
+        srv.wait(t, 600000)
     for rate in [float(r) for r in args.serve_rates.split(",") if r]:
         n = int(min(max(rate * args.serve_seconds, 200), 8000))
         kinds = rng.random(n) < 0.5

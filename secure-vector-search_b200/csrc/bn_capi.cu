@@ -463,10 +463,10 @@ void engine_free(Engine& e) {
     }
 }
 
-// Decode CTAs of a run: about four per SM in total (one wave of the decode
-// kernel), shared among the queries in proportion to their units (32-row
-// blocks), at least one per query and at most one per tile of 8 units.
-// Returns the total.
+// Decode CTAs of a run: DECODE_CTAS_PER_SM per SM in total (one wave of
+// the decode kernel), shared among the queries in proportion to their
+// units (32-row blocks), at least one per query and at most one per tile
+// of 8 units.  Returns the total.
 uint32_t assign_decode_ctas(HostMeta& hm, int sms) {
     std::vector<uint64_t> units(hm.dq.size(), 0);
     uint64_t total = 0;
@@ -475,7 +475,7 @@ uint32_t assign_decode_ctas(HostMeta& hm, int sms) {
         if (d.nseg) units[q] = hm.seg_unit[d.seg0 + d.nseg] - hm.seg_unit[d.seg0];
         total += units[q];
     }
-    const uint64_t target = (uint64_t)sms * 4;
+    const uint64_t target = (uint64_t)sms * DECODE_CTAS_PER_SM;
     uint32_t next = 0;
     for (size_t q = 0; q < hm.dq.size(); ++q) {
         uint64_t c = total ? (target * units[q] + total - 1) / total : 1;

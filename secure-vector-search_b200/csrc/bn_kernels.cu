@@ -558,8 +558,8 @@ __device__ __forceinline__ void topk_offer(TopkBuf& b, bool valid, int64_t s, ui
 __device__ __forceinline__ uint64_t signed_term(uint64_t x, bool neg) { return neg ? P - x : x; }
 
 // AL_i . g + H_i . x for corpus row gr from the 32-row-blocked alh_b: the
-// 2 n1 columns of the row's block are contiguous, so a warp's batch of 16
-// column loads is one 4 KB run.  lim[2k], lim[2k+1] hold the limbs of g_k
+// 2 n1 columns of the row's block are contiguous, so a warp's batch of 32
+// column loads is one 8 KB run.  lim[2k], lim[2k+1] hold the limbs of g_k
 // (k < n1) and of x_(k-n1) (k >= n1).  Every column adds lo*b + hi*c <
 // 2^53 + 2^50 (hi < 2^29: residues are < 2^61) to an accumulator, so the
 // 2 n1 <= 1024 columns stay below 2^64 with no fold.
@@ -567,12 +567,12 @@ __device__ __forceinline__ uint64_t dense_terms_row(const uint64_t* __restrict__
                                                     const uint4* __restrict__ lim) {
     const uint64_t* p = alh_b + (gr >> 5) * (2ull * n1) * 32 + (gr & 31);
     uint64_t a0 = 0, a1 = 0, a2 = 0;
-    for (uint32_t k0 = 0; k0 < 2 * n1; k0 += 16) {  // 2 n1 is a multiple of 16
-        uint64_t xs[16];
+    for (uint32_t k0 = 0; k0 < 2 * n1; k0 += 32) {  // 2 n1 is a multiple of 32 (n1 >= 64)
+        uint64_t xs[32];
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) xs[kk] = __ldg(p + (uint64_t)(k0 + kk) * 32);
+        for (int kk = 0; kk < 32; ++kk) xs[kk] = __ldg(p + (uint64_t)(k0 + kk) * 32);
 #pragma unroll
-        for (int kk = 0; kk < 16; ++kk) {
+        for (int kk = 0; kk < 32; ++kk) {
             const uint4 l0 = lim[2 * (k0 + kk)], l1 = lim[2 * (k0 + kk) + 1];  // {b0,b1,b2,c0}, {c1,c2,-,-}
             const uint32_t xl = (uint32_t)xs[kk], xh = (uint32_t)(xs[kk] >> 32);
             a0 = mac(mac(a0, xl, l0.x), xh, l0.w);
@@ -754,7 +754,7 @@ __device__ __forceinline__ uint64_t s_times_v_warp(const DecodeCorpus& dc, uint6
 // after a device-scope fence, no waiting) merges them.
 constexpr uint32_t DT_WARPS = DT_THREADS / 32;
 
-__global__ void __launch_bounds__(DT_THREADS, 4)
+__global__ void __launch_bounds__(DT_THREADS, DECODE_CTAS_PER_SM)
 decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSeg* __restrict__ segs,
                    const uint64_t* __restrict__ seg_unit, const DecodeQuery* __restrict__ queries,
                    const uint64_t* __restrict__ vv, const uint64_t* __restrict__ gg, const uint64_t* __restrict__ xx,

@@ -101,6 +101,10 @@ struct DecodeQuery {
     uint32_t ctas;
 };
 
+// Resident decode_topk CTAs per SM (its register bound); the host sizes
+// the decode grid to one wave of them.
+constexpr int DECODE_CTAS_PER_SM = 3;
+
 // Top-k candidate lists.
 constexpr int TOPK_MAX = 1024;
 constexpr int DECODE_CTAS_PER_QUERY_MAX = 148;

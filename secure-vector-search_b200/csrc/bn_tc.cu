@@ -822,40 +822,57 @@ __global__ void query_wimg_kernel(const uint64_t* __restrict__ v, uint32_t nq, u
 }
 
 // r[i] = sum over strip groups of r_part, then u_t . r for this pass's draws
-// rebuilt from their byte image (one CTA per 128-row block).
+// rebuilt from their byte image (one CTA per 128-row block).  For the dot
+// products warp w takes trials w, w + 4, ... (at most 5) and lane l rows
+// 4l .. 4l + 3, whose bytes of draw plane (t, b) are one 32-bit word of the
+// image: all of a warp's words are loaded before the arithmetic.
 __global__ void __launch_bounds__(TC_ROWS)
 tc_rreduce_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ blocks,
                   const uint64_t* __restrict__ r_part, uint64_t r_stride, uint32_t groups,
                   const uint8_t* __restrict__ u_img, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
                   uint64_t* __restrict__ r, uint64_t* __restrict__ ur_part) {
+    constexpr int TPW = TC_MAX_TRIALS / (TC_ROWS / 32);  // trials per warp
     const uint32_t blk = blockIdx.x;
     const TcBlock tb = blocks[blk];
     const VerifySeg vs = vsegs[tb.seg];
     const uint32_t i = threadIdx.x;
     const bool valid = tb.i0 + i < vs.rows;
     const uint64_t ri = vs.r0 + tb.i0 + i;
+    __shared__ uint64_t rs[TC_ROWS];
     uint64_t rv = 0;
     if (valid) {
+#pragma unroll 8
         for (uint32_t g = 0; g < groups; ++g) rv = add_mod(rv, r_part[(uint64_t)g * r_stride + ri]);
         r[ri] = rv;
     }
-    __shared__ uint64_t sh[TC_MAX_TRIALS][TC_ROWS / 32];
-    const uint8_t* img = u_img + (uint64_t)blk * n_rows * TC_ROWS;
+    rs[i] = rv;  // 0 past the segment's last row
     const int warp = i >> 5, lane = i & 31;
-    for (uint32_t t = 0; t < t_cnt; ++t) {
-        uint64_t u = 0;
+    const uint8_t* img = u_img + (uint64_t)blk * n_rows * TC_ROWS + 4 * lane;
+    uint32_t w[TPW][8];
 #pragma unroll
-        for (int b = 0; b < 8; ++b) u |= (uint64_t)img[(uint64_t)(8 * t + b) * TC_ROWS + i] << (8 * b);
-        uint64_t part = valid ? mul_mod(u, rv) : 0;
+    for (int j = 0; j < TPW; ++j) {
+        const uint32_t t = warp + 4 * j;
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) part = add_mod(part, __shfl_xor_sync(FULLMASK, part, off));
-        if (lane == 0) sh[t][warp] = part;
+        for (int b = 0; b < 8; ++b)
+            w[j][b] = t < t_cnt ? *reinterpret_cast<const uint32_t*>(img + (uint64_t)(8 * t + b) * TC_ROWS) : 0u;
     }
     __syncthreads();
-    if (i < t_cnt) {
-        uint64_t tot = 0;
-        for (int w = 0; w < TC_ROWS / 32; ++w) tot = add_mod(tot, sh[i][w]);
-        ur_part[(uint64_t)blk * trials_total + i] = tot;
+    const uint64_t rr[4] = {rs[4 * lane], rs[4 * lane + 1], rs[4 * lane + 2], rs[4 * lane + 3]};
+#pragma unroll
+    for (int j = 0; j < TPW; ++j) {
+        const uint32_t t = warp + 4 * j;
+        if (t >= t_cnt) break;  // warp-uniform
+        uint64_t part = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint64_t u = 0;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) u |= (uint64_t)((w[j][b] >> (8 * q)) & 0xffu) << (8 * b);
+            part = add_mod(part, mul_mod(u, rr[q]));
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) part = add_mod(part, __shfl_xor_sync(FULLMASK, part, off));
+        if (lane == 0) ur_part[(uint64_t)blk * trials_total + t] = part;
     }
 }
 
