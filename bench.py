@@ -36,7 +36,7 @@ P = (1 << 61) - 1
 # DRAM bytes (read + write) per corpus row of one tc_fused_kernel launch, from
 # the ncu capture in profiles/tc_fused_flat131k.md (131072 rows; the traffic
 # grows in proportion to the rows, so it is scaled to the bench's N).
-FUSED_DRAM_BYTES_PER_ROW = 8923
+FUSED_DRAM_BYTES_PER_ROW = 8628
 METRIC = "BN F_p scan queries/s (flat N=1M, d=768, Freivalds k=20 fused, decode + top-10)"
 
 
