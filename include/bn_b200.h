@@ -88,7 +88,11 @@ int bn_flat_build(bn_ctx* ctx, const uint64_t* m_enc, const uint64_t* a_l, const
                   uint32_t n, uint32_t n1, bn_flat** out);
 /* Client-side state for on-device decode: L (n x n1 row-major), the
  * plaintext M (m x n row-major) and S (crypto.rs:353-392 EncryptedCluster
- * fields l_subspace/m_plain/s_mat).  Needed by bn_flat_query. */
+ * fields l_subspace/m_plain/s_mat).  Needed by bn_flat_query.  Besides the
+ * uploaded arrays the decode keeps copies in 32-row blocks: 16 * n1 bytes
+ * per row of [AL | H], plus 1024 bytes per row of M when every entry of M
+ * is int8-valued (rows rounded up to a multiple of 32; counted in
+ * bn_flat_info's device_bytes and against the context budget). */
 int bn_flat_attach_client(bn_flat* h, const uint64_t* l_subspace, const uint64_t* m_plain, bn_sparse_csr s_mat);
 /* Encrypt on the device and build in one step (crypto.rs:405-478 +
  * gpu/mod.rs:300-332): M_enc = M + H L^T + S and AL = M L are computed
@@ -224,6 +228,8 @@ int bn_flat_verify_block(bn_flat* h, uint32_t B, const uint64_t* r, const uint64
  * (ivf-index IvfIndex::clusters membership). */
 int bn_ivf_build(bn_ctx* ctx, uint32_t nlist, const uint64_t* list_offsets, const uint32_t* ids, const uint64_t* m_enc,
                  const uint64_t* a_l, const uint64_t* h, uint32_t n, uint32_t n1, bn_ivf** out);
+/* As bn_flat_attach_client, for the concatenated lists (the same decode
+ * copies per row). */
 int bn_ivf_attach_client(bn_ivf* h, const uint64_t* l_subspace, const uint64_t* m_plain, bn_sparse_csr s_mat);
 /* Device encryption of every list (crypto.rs:405-478 per cluster,
  * ivf.rs:627-653) followed by bn_ivf_build + bn_ivf_attach_client.  h and
