@@ -57,6 +57,45 @@ uint32_t bn_host_encode_query(const uint64_t* v_q, const uint64_t* L, uint32_t n
 void bn_host_probe_route(const float* centroids, uint32_t nlist, uint32_t d, const float* queries, uint64_t count,
                          uint32_t nprobe, uint32_t* out);
 
+/* ---------------------------------------------------------------- reference IVF cache files
+ * Reader of the `.bntm-ivf-cache-<16 hex>.bin` files the reference's
+ * BnTmIvfScorer writes (scorer-bntm/src/ivf.rs:440-560; its loader
+ * load_bntm_ivf_cache, ivf.rs:1755-1901): the k-means index, and per list
+ * the encrypted m_enc, a_l, the plaintext m_plain and H, plus L.  S is
+ * not stored; regenerate it per list from the list's h_seed with
+ * bn_host_regenerate_h_s, as the reference does.
+ *
+ * bn_host_cache_fingerprint: the header hash of scorer-core/src/cache.rs
+ * (FNV-1a 64 over the parts, each prefixed by its u64 LE length); the
+ * reference's parts for this cache are ivf.rs:321-331 ("bntm-ivf2",
+ * n_centroids, train_seed, max_iter, number of vectors, upload_seed,
+ * key_seed, n1, quantisation_q; integers as u64 LE, key_seed 32 bytes),
+ * and the file name is ".bntm-ivf-cache-" + 16 lower-case hex digits of it
+ * + ".bin". */
+uint64_t bn_host_cache_fingerprint(const uint8_t* const* parts, const uint64_t* lens, uint32_t nparts);
+
+typedef struct bn_ivf_cache bn_ivf_cache;
+/* Maps and indexes the file.  fingerprint: the expected header hash, or 0
+ * to accept any (the magic and version are always checked).  n, n1: the BN
+ * dimensions the index was built with.  Returns BN_OK, or BN_EINVAL with
+ * bn_last_error() naming the first inconsistency (the reference treats the
+ * same conditions as a cache miss or as invalid data): bad magic, version
+ * or fingerprint, a truncated region, or list sizes that differ between
+ * the index and the encrypted part. */
+int bn_host_ivf_cache_open(const char* path, uint64_t fingerprint, uint32_t n, uint32_t n1, bn_ivf_cache** out);
+void bn_host_ivf_cache_close(bn_ivf_cache* c);
+/* Lists, dimension of the index's f32 vectors, total rows. */
+void bn_host_ivf_cache_info(const bn_ivf_cache* c, uint32_t* nlist, uint32_t* dim, uint64_t* rows);
+/* list_offsets (nlist + 1), ids (rows, the vector ids in list order),
+ * centroids (nlist x dim f32) and h_seeds (nlist x 32 bytes); each
+ * nullable. */
+void bn_host_ivf_cache_lists(const bn_ivf_cache* c, uint64_t* list_offsets, uint32_t* ids, float* centroids,
+                             uint8_t* h_seeds);
+/* The lists' arrays concatenated in list order, each nullable: m_enc and
+ * m_plain rows x n, a_l and h rows x n1 (row-major), l_subspace n x n1. */
+void bn_host_ivf_cache_arrays(const bn_ivf_cache* c, uint64_t* m_enc, uint64_t* a_l, uint64_t* m_plain, uint64_t* h,
+                              uint64_t* l_subspace);
+
 #ifdef __cplusplus
 }
 #endif

@@ -599,6 +599,12 @@ _HOST_SIGS = {
     "bn_host_quantise": (None, [vp, u64, u32, u32, u64, vp]),
     "bn_host_encode_query": (u32, [vp, vp, u32, u32, vp, vp, vp, vp, vp]),
     "bn_host_probe_route": (None, [vp, u32, u32, vp, u64, u32, vp]),
+    "bn_host_cache_fingerprint": (u64, [vp, vp, u32]),
+    "bn_host_ivf_cache_open": (C.c_int, [C.c_char_p, u64, u32, u32, C.POINTER(vp)]),
+    "bn_host_ivf_cache_close": (None, [vp]),
+    "bn_host_ivf_cache_info": (None, [vp, vp, vp, vp]),
+    "bn_host_ivf_cache_lists": (None, [vp, vp, vp, vp, vp]),
+    "bn_host_ivf_cache_arrays": (None, [vp, vp, vp, vp, vp, vp]),
 }
 for _name, (_res, _args) in _HOST_SIGS.items():
     _f = getattr(lib, _name)
@@ -687,3 +693,99 @@ def host_probe_route(centroids, queries, nprobe: int) -> np.ndarray:
     out = np.zeros((q.shape[0], np_), np.uint32)
     lib.bn_host_probe_route(ptr(c), c.shape[0], c.shape[1], ptr(q), q.shape[0], nprobe, ptr(out))
     return out
+
+
+# ---------------------------------------------------------------- reference IVF cache files
+def cache_fingerprint(parts) -> int:
+    """scorer-core/src/cache.rs fingerprint64 of byte strings `parts`."""
+    bufs = [np.frombuffer(bytes(pt), np.uint8).copy() if len(pt) else np.zeros(1, np.uint8) for pt in parts]
+    ptrs = (vp * max(len(bufs), 1))(*[b.ctypes.data for b in bufs])
+    lens = np.array([len(pt) for pt in parts] or [0], np.uint64)
+    return int(lib.bn_host_cache_fingerprint(ptrs, ptr(lens), len(parts)))
+
+
+def bntm_ivf_cache_parts(n_centroids: int, train_seed: int, max_iter: int, n_vectors: int, upload_seed: int,
+                         key_seed: bytes, n1: int, quantisation_q: int) -> list:
+    """The reference's fingerprint parts of a BN-IVF cache (scorer-bntm/src/ivf.rs:321-331)."""
+    le = lambda x: int(x).to_bytes(8, "little")
+    return [b"bntm-ivf2", le(n_centroids), le(train_seed), le(max_iter), le(n_vectors), le(upload_seed),
+            bytes(key_seed), le(n1), le(quantisation_q)]
+
+
+def bntm_ivf_cache_name(*args, **kw) -> tuple:
+    """(fingerprint, file name) of the reference's cache for these parameters (ivf.rs:332-337)."""
+    fp = cache_fingerprint(bntm_ivf_cache_parts(*args, **kw))
+    return fp, f".bntm-ivf-cache-{fp:016x}.bin"
+
+
+class IvfCache:
+    """A `.bntm-ivf-cache-*.bin` file of the reference, mapped and indexed
+    (bn_host_ivf_cache_open); fingerprint 0 accepts any parameters."""
+
+    def __init__(self, path: str, fingerprint: int = 0, n1: int = 128):
+        self.h = None
+        h = vp()
+        check(lib.bn_host_ivf_cache_open(str(path).encode(), fingerprint, N, n1, C.byref(h)))
+        self.h, self.n1 = h, n1
+        nl, dim, rows = u32(0), u32(0), u64(0)
+        lib.bn_host_ivf_cache_info(self.h, C.byref(nl), C.byref(dim), C.byref(rows))
+        self.nlist, self.dim, self.rows = nl.value, dim.value, rows.value
+
+    def lists(self):
+        """(list_offsets, ids, centroids [nlist, dim] f32, h_seeds [nlist, 32] u8)."""
+        off = np.zeros(self.nlist + 1, np.uint64)
+        ids = np.zeros(max(self.rows, 1), np.uint32)
+        cen = np.zeros((max(self.nlist, 1), max(self.dim, 1)), np.float32)
+        hs = np.zeros((max(self.nlist, 1), 32), np.uint8)
+        lib.bn_host_ivf_cache_lists(self.h, ptr(off), ptr(ids), ptr(cen), ptr(hs))
+        return off, ids[: self.rows], cen[: self.nlist, : self.dim], hs[: self.nlist]
+
+    def arrays(self):
+        """Concatenated list-order arrays: m_enc [rows, n], a_l [rows, n1],
+        m_plain [rows, n], h [rows, n1], l_subspace [n, n1]."""
+        r, n1 = self.rows, self.n1
+        me, mp = np.zeros((max(r, 1), N), np.uint64), np.zeros((max(r, 1), N), np.uint64)
+        al, hh = np.zeros((max(r, 1), n1), np.uint64), np.zeros((max(r, 1), n1), np.uint64)
+        L = np.zeros((N, n1), np.uint64)
+        lib.bn_host_ivf_cache_arrays(self.h, ptr(me), ptr(al), ptr(mp), ptr(hh), ptr(L))
+        return {"m_enc": me[:r], "a_l": al[:r], "m_plain": mp[:r], "h": hh[:r], "l_subspace": L}
+
+    def s_lists(self):
+        """S of every list, regenerated from its h_seed (crypto.rs:258-270),
+        concatenated in list order as one CSR (rowptr, idx, sign)."""
+        off, _, _, hs = self.lists()
+        rowptr, idx, sign = [np.zeros(1, np.uint64)], [], []
+        base = 0
+        for c in range(self.nlist):
+            m = int(off[c + 1] - off[c])
+            _, rp, ix, sg = host_regenerate_h_s(hs[c].tobytes(), m, self.n1)
+            rowptr.append(rp[1:] + np.uint64(base))
+            idx.append(ix)
+            sign.append(sg)
+            base += len(ix)
+        cat = lambda xs, t: np.concatenate(xs).astype(t) if xs else np.zeros(0, t)
+        return np.concatenate(rowptr).astype(np.uint64), cat(idx, np.uint32), cat(sign, np.int8)
+
+    def close(self):
+        if self.h:
+            lib.bn_host_ivf_cache_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def ivf_from_cache(ctx, path: str, fingerprint: int = 0, n1: int = 128):
+    """Device IVF handle (server and client state) from a reference cache
+    file: bn_ivf_build on its m_enc / a_l / h and ids, then
+    bn_ivf_attach_client with its L, m_plain and the regenerated S.
+    Returns (Ivf, centroids) -- the centroids route queries
+    (host_probe_route)."""
+    cache = IvfCache(path, fingerprint, n1)
+    off, ids, cen, _ = cache.lists()
+    a = cache.arrays()
+    rp, ix, sg = cache.s_lists()
+    cache.close()
+    v = Ivf.build(ctx, off, ids, a["m_enc"].reshape(-1), a["a_l"].reshape(-1), a["h"].reshape(-1), n1=n1)
+    v.attach_client(a["l_subspace"].reshape(-1), a["m_plain"].reshape(-1), rp, ix, sg)
+    return v, cen
