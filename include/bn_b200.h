@@ -250,6 +250,17 @@ int bn_ivf_decode_dense_terms(bn_ivf* h, uint32_t ci, const uint64_t* g, const u
 /* verify_response for one list and a claimed r (ivf.rs:791-806). */
 int bn_ivf_verify(bn_ivf* h, uint32_t ci, const uint64_t* r, const uint64_t* v_enc, const uint8_t v_seed[32],
                   uint32_t trials, int32_t* failed_trial, uint64_t* ur, uint64_t* zv);
+/* IVF routing on the device (ivf-index/src/ivf.rs:150-164 probe_route) for
+ * a batch: bn_ivf_set_centroids keeps the nlist x d f32 centroids (row-major,
+ * list order; d <= 8192, nlist <= 16384) on the handle; bn_ivf_route writes,
+ * per query of the B x d f32 queries, the min(nprobe, nlist) nearest lists
+ * into probes (B x min(nprobe, nlist)), nearest first.  Distances are the
+ * reference's scalar l2_f32 (distance.rs:30-36: sqrt of the in-order sum of
+ * (x - y)^2, no fused multiply-add), ties to the lower list index, so the
+ * result equals bn_host_probe_route bit for bit; the reference's AVX-512
+ * build sums in 16 lanes and may order near-ties differently. */
+int bn_ivf_set_centroids(bn_ivf* h, const float* centroids, uint32_t d);
+int bn_ivf_route(bn_ivf* h, uint32_t B, const float* queries, uint32_t nprobe, uint32_t* probes);
 /* BnTmIvfScorer::score / score_batch (ivf.rs:746-927, 1199-1366) for B
  * queries with nprobe routed lists each (probes B x nprobe, in probe
  * order): every probed list of every query is scanned, verified, decoded

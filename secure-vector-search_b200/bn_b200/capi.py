@@ -90,6 +90,8 @@ _SIGS = {
     "bn_ivf_build_from_plain": (C.c_int, [vp, u32, vp, vp, vp, u32, u32, vp, vp, SparseCsr, vp]),
     "bn_ivf_destroy": (C.c_int, [vp]),
     "bn_ivf_info": (C.c_int, [vp, vp, vp]),
+    "bn_ivf_set_centroids": (C.c_int, [vp, vp, u32]),
+    "bn_ivf_route": (C.c_int, [vp, u32, vp, u32, vp]),
     "bn_ivf_compute_products": (C.c_int, [vp, u32, vp, vp, vp]),
     "bn_ivf_decode_dense_terms": (C.c_int, [vp, u32, vp, vp, vp, vp]),
     "bn_ivf_verify": (C.c_int, [vp, u32, vp, vp, vp, u32, vp, vp, vp]),
@@ -394,6 +396,21 @@ class Ivf:
         check(lib.bn_ivf_build_from_plain(ctx.h, len(off) - 1, ptr(off), ptr(ids), ptr(m_q), N, n1, ptr(L), ptr(H),
                                           csr, C.byref(out)))
         return cls(ctx, out, off, n1)
+
+    def set_centroids(self, centroids):
+        """bn_ivf_set_centroids: nlist x d f32 centroids for bn_ivf_route."""
+        c = np.ascontiguousarray(centroids, np.float32)
+        check(lib.bn_ivf_set_centroids(self.h, ptr(c), c.shape[1]))
+        self.cent_d = c.shape[1]
+
+    def route(self, queries, nprobe: int) -> np.ndarray:
+        """bn_ivf_route: the min(nprobe, nlist) nearest lists of every query, nearest first."""
+        q = np.ascontiguousarray(queries, np.float32)
+        if q.ndim == 1:
+            q = q[None]
+        out = np.zeros((q.shape[0], max(min(nprobe, self.nlist), 1)), np.uint32)
+        check(lib.bn_ivf_route(self.h, q.shape[0], ptr(q), nprobe, ptr(out)))
+        return out[:, : min(nprobe, self.nlist)]
 
     def attach_client(self, L, m_plain, s_rowptr, s_idx, s_sign):
         L, m_plain = _u64(L), _u64(m_plain)

@@ -324,6 +324,9 @@ struct bn_ivf {
     bn::api::Engine e;
     uint32_t nlist = 0;
     std::vector<uint64_t> offsets;
+    // routing (bn_ivf_set_centroids): centroids dimension-major, [cent_d][nlist] f32
+    bn::api::DevMem cent_t;
+    uint32_t cent_d = 0;
     // block GEMM tiling chosen by the caller (bn_ivf_block_tune; 0 = automatic)
     uint32_t blk_w = 0, blk_stages = 0;
     // stage timing of the host-buffer IVF block entry point (bn_ivf_block_profile)
