@@ -794,7 +794,14 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
         u_count = seg_unit[dq.seg0 + dq.nseg] - u_begin;
     }
     const uint64_t tiles = (u_count + DT_WARPS - 1) / DT_WARPS;
-    for (uint64_t tile = cta; tile < tiles; tile += dq.ctas) {
+    // The buffer is checked (two CTA barriers) every DT_CHECK tiles, not
+    // every tile, so the warps may drift apart within that window; between
+    // checks at most DT_CHECK * 256 rows append, and a check compacts above
+    // CAND_CAP - DT_CHECK * 256 = 1024 >= k entries.
+    constexpr uint32_t DT_CHECK = 4;
+    static_assert(CAND_CAP - DT_CHECK * DT_THREADS >= TOPK_MAX, "candidate buffer too small for the check interval");
+    uint32_t it = 0;
+    for (uint64_t tile = cta; tile < tiles; tile += dq.ctas, ++it) {
         const uint64_t u = tile * DT_WARPS + warp;
         bool valid = false;
         int64_t score = 0;
@@ -834,7 +841,8 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
         const uint32_t th_i = buf.thr_i;
         const int ht = buf.have_thr;
         topk_offer(buf, valid, score, id, th_s, th_i, ht);
-        if (topk_full(buf, CAND_CAP - DT_THREADS)) topk_compact(buf, (int)k);
+        if (it % DT_CHECK == DT_CHECK - 1 && topk_full(buf, CAND_CAP - DT_CHECK * DT_THREADS))
+            topk_compact(buf, (int)k);
     }
     topk_compact(buf, (int)k);
     const int keep = min(buf.cnt, (int)k);
