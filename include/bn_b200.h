@@ -253,7 +253,7 @@ int bn_ivf_verify(bn_ivf* h, uint32_t ci, const uint64_t* r, const uint64_t* v_e
 /* IVF routing on the device (ivf-index/src/ivf.rs:150-164 probe_route) for
  * a batch: bn_ivf_set_centroids keeps the nlist x d f32 centroids (row-major,
  * list order; d <= 8192, nlist <= 16384) on the handle; bn_ivf_route writes,
- * per query of the B x d f32 queries, the min(nprobe, nlist) nearest lists
+ * per query of the B x d f32 queries (B <= 65535), the min(nprobe, nlist) nearest lists
  * into probes (B x min(nprobe, nlist)), nearest first.  Distances are the
  * reference's scalar l2_f32 (distance.rs:30-36: sqrt of the in-order sum of
  * (x - y)^2, no fused multiply-add), ties to the lower list index, so the

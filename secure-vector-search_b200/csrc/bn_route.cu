@@ -98,6 +98,7 @@ int bn_ivf_route(bn_ivf* v, uint32_t B, const float* queries, uint32_t nprobe, u
     if (!queries || !probes) return fail(BN_EINVAL, "null argument");
     if (!v->cent_d) return fail(BN_EINVAL, "no centroids: call bn_ivf_set_centroids first");
     if (nprobe == 0) return fail(BN_EINVAL, "nprobe must be positive");
+    if (B > 65535) return fail(BN_EINVAL, "B = %u exceeds 65535 queries per call", B);
     const uint32_t nlist = v->nlist, d = v->cent_d, np = std::min(nprobe, nlist);
     if (nlist == 0) return BN_OK;
     std::lock_guard<std::mutex> g(v->e.mu);
