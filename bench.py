@@ -350,6 +350,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         "roofline": {"kernel": "tc_fused_kernel (one pass over M_enc: r = M_enc v and z_t = u_t^T M_enc, 20 trials)",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
+                     "frac_of_spec_8tbs": achieved / 8000.0,  # B200 HBM3e data-sheet figure, for context
                      "traffic": FUSED_DRAM_BYTES_PER_ROW * n_rows if FUSED_DRAM_BYTES_PER_ROW else None,
                      "algorithmic_bytes_per_launch": bytes_scan, "launches_timed": int(len(fused_ms)),
                      "scan_only_kernel_step": {"achieved": bytes_scan / scan_s / 1e9,
