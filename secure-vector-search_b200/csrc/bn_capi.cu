@@ -139,21 +139,21 @@ int validate_residues(const uint64_t* a, uint64_t count, const char* what) {
 int build_decode_layout(bn_ctx* ctx, Corpus& c, cudaStream_t s) {
     const uint64_t rows32 = (c.rows + 31) / 32 * 32;
     TRY(c.alh_b.alloc(ctx, rows32 * 2 * c.n1 * 8));
-    TRY(c.m8_b.alloc(ctx, rows32 * N));
+    TRY(c.m8_cm.alloc(ctx, rows32 * N));
     DevMem bad;
     TRY(bad.alloc(ctx, 4));
     launch_decode_layout(c.al_cm.at<uint64_t>(), c.h_cm.at<uint64_t>(), c.mp_cm.at<uint64_t>(), c.rows, c.n1,
-                         c.alh_b.at<uint64_t>(), c.m8_b.at<int8_t>(), bad.at<uint32_t>(), s);
+                         c.alh_b.at<uint64_t>(), c.m8_cm.at<int8_t>(), bad.at<uint32_t>(), s);
     CU(cudaGetLastError());
     uint32_t hb = 0;
     CU(cudaMemcpyAsync(&hb, bad.p, 4, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
-    if (hb) c.m8_b.release();  // M T from the residues
+    if (hb) c.m8_cm.release();  // M T from the residues
     return BN_OK;
 }
 
 DecodeCorpus decode_corpus(const Corpus& c) {
-    return DecodeCorpus{c.alh_b.at<uint64_t>(), c.m8_b.p ? c.m8_b.at<int8_t>() : nullptr, c.mp_cm.at<uint64_t>(),
+    return DecodeCorpus{c.alh_b.at<uint64_t>(), c.m8_cm.p ? c.m8_cm.at<int8_t>() : nullptr, c.mp_cm.at<uint64_t>(),
                         c.s_ell.at<uint16_t>(), c.s_off.at<uint32_t>(), c.s_w.at<uint16_t>(),
                         c.ids.p ? c.ids.at<uint32_t>() : nullptr, c.rows, c.n1};
 }

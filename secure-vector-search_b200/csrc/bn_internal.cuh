@@ -135,7 +135,7 @@ struct Corpus {
     DevMem m_enc, al_cm, h_cm;
     bool client = false;
     DevMem L, mp_cm, s_ell, s_off, s_w, ids;
-    DevMem alh_b, m8_b;  // decode copies in 32-row blocks (bn_kernels.cuh); m8_b only for int8-valued M
+    DevMem alh_b, m8_cm;  // decode copies (bn_kernels.cuh): [AL | H] in 32-row blocks, int8 M column-major
     CUtensorMap tmap_m;  // m_enc as bytes {8192, rows}, 128x128 boxes, 128-byte swizzle
 
     // Byte-planar operands of block scoring (built on first use, see
@@ -154,7 +154,7 @@ struct Corpus {
 
     uint64_t bytes() const {
         return m_enc.bytes + al_cm.bytes + h_cm.bytes + L.bytes + mp_cm.bytes + s_ell.bytes + s_off.bytes + s_w.bytes +
-               ids.bytes + alh_b.bytes + m8_b.bytes + mp8.bytes + alh8.bytes + ms8.bytes + corr.bytes;
+               ids.bytes + alh_b.bytes + m8_cm.bytes + mp8.bytes + alh8.bytes + ms8.bytes + corr.bytes;
     }
 };
 

@@ -456,7 +456,7 @@ __global__ void dense_terms_kernel(const uint64_t* __restrict__ al_cm, const uin
 // bn_kernels.cuh); reads and writes are both coalesced along the rows.
 __global__ void decode_layout_kernel(const uint64_t* __restrict__ al_cm, const uint64_t* __restrict__ h_cm,
                                      const uint64_t* __restrict__ mp_cm, uint64_t rows, uint32_t n1,
-                                     uint64_t* __restrict__ alh_b, int8_t* __restrict__ m8_b, uint32_t* __restrict__ bad) {
+                                     uint64_t* __restrict__ alh_b, int8_t* __restrict__ m8_cm, uint32_t* __restrict__ bad) {
     const uint64_t rows32 = (rows + 31) / 32 * 32;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t n_alh = rows32 * 2 * n1;
@@ -466,15 +466,15 @@ __global__ void decode_layout_kernel(const uint64_t* __restrict__ al_cm, const u
         if (gr < rows) x = col < n1 ? al_cm[col * rows + gr] : h_cm[(col - n1) * rows + gr];
         alh_b[e] = x;
     }
-    if (!m8_b) return;
+    if (!m8_cm) return;
     bool out_of_range = false;
     const uint64_t n_m = rows32 * N;
     for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_m; e += stride) {
-        const uint64_t col = (e >> 5) & (N - 1), gr = (e >> 15) * 32 + (e & 31);
+        const uint64_t col = e / rows32, gr = e - col * rows32;
         int64_t v = 0;
         if (gr < rows) v = to_signed(mp_cm[col * rows + gr]);
         out_of_range |= v < -128 || v > 127;
-        m8_b[e] = (int8_t)v;
+        m8_cm[e] = (int8_t)v;
     }
     if (out_of_range) atomicOr(bad, 1u);
 }
@@ -593,14 +593,16 @@ __device__ __forceinline__ uint32_t sext_pair(uint32_t x, uint32_t sel) {
 
 // M . T for the warp's 32-row block (lane l = row 32 blk + l): the T
 // columns go 32 at a time, one per lane; a lane loads its column's 32 row
-// bytes (one 32-byte run of the int8 block), widens them to 16 signed int16
+// bytes (one 32-byte run of the column-major int8 copy: the warps decoding
+// neighbouring blocks at the same time read neighbouring runs of the same
+// columns, so DRAM pages serve many of them), widens them to 16 signed int16
 // pairs with the entry's sign, and a reduce-scatter over the lanes (lane
 // bit 4 keeps rows 0-15 or 16-31, then bits 3..0) leaves lane l the sum of
 // row l over those 32 columns (|sum| <= 32 * 128, exact in int16).  Four
 // groups of loads are in flight at a time.  Returns the exact integer.
-__device__ __forceinline__ int32_t m_times_t_warp(const int8_t* __restrict__ m8_b, uint64_t blk,
+__device__ __forceinline__ int32_t m_times_t_warp(const int8_t* __restrict__ m8_cm, uint64_t rows32, uint64_t blk,
                                                   const uint32_t* __restrict__ tl, uint32_t tn, uint32_t lane) {
-    const uint4* base = reinterpret_cast<const uint4*>(m8_b + blk * ((uint64_t)N * 32));
+    const int8_t* base = m8_cm + blk * 32;  // column c's run: base + c * rows32, 32-byte aligned
     int32_t acc = 0;
     for (uint32_t g0 = 0; g0 < tn; g0 += 4 * 32) {
         uint4 lo[4], hi[4];
@@ -612,8 +614,9 @@ __device__ __forceinline__ int32_t m_times_t_warp(const int8_t* __restrict__ m8_
             neg[u] = 0;
             if (c < tn) {
                 const uint32_t e = tl[c];
-                lo[u] = __ldg(base + (e & 0x3ffu) * 2);
-                hi[u] = __ldg(base + (e & 0x3ffu) * 2 + 1);
+                const uint4* run = reinterpret_cast<const uint4*>(base + (uint64_t)(e & 0x3ffu) * rows32);
+                lo[u] = __ldg(run);
+                hi[u] = __ldg(run + 1);
                 neg[u] = e >> 31;
             }
         }
@@ -824,13 +827,13 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
                 id = dc.ids ? dc.ids[gr] : (uint32_t)gr;
             }
             uint64_t m_t = 0;
-            if (dc.m8_b) {
-                const int32_t mt = m_times_t_warp(dc.m8_b, blk, tl, tn, lane);
+            if (dc.m8_cm) {
+                const int32_t mt = m_times_t_warp(dc.m8_cm, (dc.rows + 31) & ~31ull, blk, tl, tn, lane);
                 m_t = mt >= 0 ? (uint64_t)mt : P - (uint64_t)(-(int64_t)mt);
             }
             const uint64_t s_v = s_times_v_warp(dc, blk, vs, lane);
             if (valid) {
-                if (!dc.m8_b) m_t = m_times_t_cm(dc.mp_cm, dc.rows, gr, tl, tn);
+                if (!dc.m8_cm) m_t = m_times_t_cm(dc.mp_cm, dc.rows, gr, tl, tn);
                 const uint64_t dense = dense_terms_row(dc.alh_b, n1, gr, dyn_limbs);
                 const uint64_t mv = sub_mod(sub_mod(rv, add_mod(dense, m_t)), s_v);
                 if (mv_out) mv_out[ridx] = mv;
@@ -1199,10 +1202,10 @@ void launch_dense_terms(const uint64_t* d_al_cm, const uint64_t* d_h_cm, uint64_
 }
 
 void launch_decode_layout(const uint64_t* d_al_cm, const uint64_t* d_h_cm, const uint64_t* d_mp_cm, uint64_t rows,
-                          uint32_t n1, uint64_t* d_alh_b, int8_t* d_m8_b, uint32_t* d_bad, cudaStream_t s) {
+                          uint32_t n1, uint64_t* d_alh_b, int8_t* d_m8_cm, uint32_t* d_bad, cudaStream_t s) {
     cudaMemsetAsync(d_bad, 0, 4, s);
     if (!rows) return;
-    decode_layout_kernel<<<148 * 16, 256, 0, s>>>(d_al_cm, d_h_cm, d_mp_cm, rows, n1, d_alh_b, d_m8_b, d_bad);
+    decode_layout_kernel<<<148 * 16, 256, 0, s>>>(d_al_cm, d_h_cm, d_mp_cm, rows, n1, d_alh_b, d_m8_cm, d_bad);
 }
 
 void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanSeg* d_segs, const uint64_t* d_seg_unit,

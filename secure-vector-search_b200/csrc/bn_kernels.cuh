@@ -13,10 +13,11 @@
 // Decode copies of the client state, in blocks of 32 rows (rows32 = rows
 // rounded up to 32; entries past the last row are 0):
 //   alh_b   u64 [rows32/32][2*n1][32]  AL columns then H columns
-//   m8_b    s8  [rows32/32][1024][32]  plaintext M when every entry is
-//           int8-valued (quantised corpora), else absent
-// A warp that decodes 32 consecutive rows reads one 256-byte (u64) or
-// 32-byte (s8) run per column, and a block's columns are contiguous.
+//   m8_cm   s8  [1024][rows32]         plaintext M column-major, when every
+//           entry is int8-valued (quantised corpora), else absent
+// A warp that decodes 32 consecutive rows reads one 256-byte run per column
+// of alh_b (a block's columns are contiguous) and one 32-byte run per T
+// column of m8_cm.
 // Column-major client arrays make the thread-per-row reads of the other
 // kernels coalesced; the row-major m_enc makes the scan's warp-per-row reads
 // coalesced.
@@ -119,7 +120,7 @@ struct TopkScratch {
 // The corpus arrays the decode reads (layouts above).
 struct DecodeCorpus {
     const uint64_t* alh_b;
-    const int8_t* m8_b;     // null: M T from mp_cm
+    const int8_t* m8_cm;    // null: M T from mp_cm
     const uint64_t* mp_cm;
     const uint16_t* s_ell;
     const uint32_t* s_off;
@@ -129,11 +130,11 @@ struct DecodeCorpus {
     uint32_t n1;
 };
 
-// Builds alh_b from al_cm / h_cm and m8_b from mp_cm (m8_b nullable, e.g.
+// Builds alh_b from al_cm / h_cm and m8_cm from mp_cm (m8_cm nullable, e.g.
 // without client state); *d_bad (zeroed here) gets bit 0 if an entry of
-// mp_cm is not int8-valued, in which case m8_b must not be used.
+// mp_cm is not int8-valued, in which case m8_cm must not be used.
 void launch_decode_layout(const uint64_t* d_al_cm, const uint64_t* d_h_cm, const uint64_t* d_mp_cm, uint64_t rows,
-                          uint32_t n1, uint64_t* d_alh_b, int8_t* d_m8_b, uint32_t* d_bad, cudaStream_t s);
+                          uint32_t n1, uint64_t* d_alh_b, int8_t* d_m8_cm, uint32_t* d_bad, cudaStream_t s);
 
 // Decode + fp_to_signed + top-k for every query: each CTA ranks its rows,
 // and the last CTA of a query to finish merges the CTAs' lists into
