@@ -15,14 +15,18 @@ MAGIC = b"\x89SVScach"
 VERSION = 1
 
 
+def fnv1a64_raw(data: bytes) -> int:
+    """FNV-1a 64 of a byte string (offset basis 0xcbf29ce484222325, prime 0x100000001b3)."""
+    h = 0xCBF29CE484222325
+    for b in data:
+        h ^= b
+        h = (h * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
 def fnv1a64(parts) -> int:
     """cache.rs:23-38 fingerprint64: FNV-1a 64 over the u64-LE-length-prefixed parts."""
-    h = 0xCBF29CE484222325
-    for p in parts:
-        for b in struct.pack("<Q", len(p)) + bytes(p):
-            h ^= b
-            h = (h * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
-    return h
+    return fnv1a64_raw(b"".join(struct.pack("<Q", len(p)) + bytes(p) for p in parts))
 
 
 def write_cache(path, parts, centroids, lists, l_subspace, n1=128, fingerprint=None):

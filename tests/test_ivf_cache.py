@@ -68,6 +68,22 @@ def test_fingerprint_matches_cache_rs_restatement():
     assert fp == F.fnv1a64(PARTS) and name == f".bntm-ivf-cache-{fp:016x}.bin"
 
 
+def test_fnv_core_matches_published_vectors():
+    """The FNV-1a 64 core of the restatement, against the algorithm's published test vectors."""
+    assert F.fnv1a64_raw(b"") == 0xCBF29CE484222325
+    assert F.fnv1a64_raw(b"a") == 0xAF63DC4C8601EC8C
+    assert F.fnv1a64_raw(b"foobar") == 0x85944171F73967E8
+
+
+def test_fingerprint_properties_of_cache_rs_tests():
+    """cache.rs:80-100: deterministic, scorer tags differ, part boundaries count."""
+    c = capi()
+    one = [b"plaintext-ivf", bytes([1, 0, 0, 0])]
+    assert c.cache_fingerprint(one) == c.cache_fingerprint(list(one))
+    assert c.cache_fingerprint(one) != c.cache_fingerprint([b"sap-ivf", bytes([1, 0, 0, 0])])
+    assert c.cache_fingerprint([b"ab", b"c"]) != c.cache_fingerprint([b"a", b"bc"])
+
+
 def test_round_trip(small_cache):
     c = capi()
     path, cen, lists, L = small_cache
