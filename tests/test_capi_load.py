@@ -1,5 +1,6 @@
 """CPU checks of the drop-in boundary: the sm_100a library loads and
-exports every entry point that include/bn_b200.h declares."""
+exports every entry point that include/*.h declares (the device ABI
+bn_b200.h and the host-side bn_host.h)."""
 import os
 import re
 
@@ -8,11 +9,14 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_symbols():
-    with open(os.path.join(ROOT, "include", "bn_b200.h")) as f:
-        text = f.read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(bn_[a-z0-9_]+)\s*\(", text)))
+def declared_symbols(headers=("bn_b200.h", "bn_host.h")):
+    syms = set()
+    for h in headers:
+        with open(os.path.join(ROOT, "include", h)) as f:
+            text = f.read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        syms |= set(re.findall(r"\b(bn_[a-z0-9_]+)\s*\(", text))
+    return sorted(syms)
 
 
 def test_header_declares_boundary():
@@ -25,7 +29,9 @@ def test_header_declares_boundary():
 def test_library_exports_every_declared_symbol():
     from bn_b200 import capi
 
-    missing = [s for s in declared_symbols() if not hasattr(capi.lib, s)]
+    syms = declared_symbols()
+    assert "bn_host_encode_query" in syms and "bn_host_ivf_cache_open" in syms and "bn_ivf_route" in syms
+    missing = [s for s in syms if not hasattr(capi.lib, s)]
     assert not missing, missing
 
 
