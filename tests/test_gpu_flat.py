@@ -203,6 +203,30 @@ def test_decode_int8_copy_is_kept_only_for_int8_plaintext(ctx):
     assert a - b == (m + 31) // 32 * 32 * N
 
 
+@pytest.mark.parametrize("n1", [64, 256, 512])
+def test_query_matches_oracle_across_n1(ctx, n1):
+    """The delta sweep of the reference's parameter sets (n1 = 1024 >> k,
+    params.rs:102-120): scan, Protocol 2, decode and top-k at every n1 the
+    ABI accepts (128 is covered above)."""
+    c = capi()
+    m = 1500
+    M = int8_matrix(m, 768, 70 + n1)
+    L = O.generate_subspace(bytes([3]) * 32, n1=n1)
+    cl = O.encrypt_cluster(M.reshape(-1), m, L, O.derive_h_seed(7, 0), n1=n1)
+    f = c.Flat.build(ctx, cl.m_enc, cl.a_l, cl.h_mat, m, n1=n1)
+    f.attach_client(L, M.reshape(-1), cl.s_mat.rowptr, cl.s_mat.idx, cl.s_mat.sign)
+    v = int8_matrix(1, 768, 71 + n1)[0]
+    q_seed = O.derive_h_seed(72, n1)
+    enc = O.encode_query(v, L, q_seed, n1=n1)
+    fo, ids, sc, ro, _ = O.score_flat(cl, L, v, q_seed, 4, 25, want_r=True)
+    mvo = O.decode_scores(ro, cl, L, enc)
+    hits, failed, r, mv = f.query(enc.v_enc[None], enc.g[None], [(enc.t_idx, enc.t_sign)],
+                                  [O.domain_separate(q_seed, b"protocol2")], 4, 25, want_r=True, want_mv=True)
+    assert np.array_equal(r[0], ro) and np.array_equal(mv[0], mvo)
+    assert np.array_equal(hits[0][0], ids) and np.array_equal(hits[0][1], sc)
+    assert failed[0] == fo == -1
+
+
 def test_device_encrypted_handle_matches_host_encrypted(ctx):
     c = capi()
     M, L, cl = cluster(1234, 77)
