@@ -68,6 +68,32 @@ def test_block_query_matches_oracle(ctx, m, B, trials, k):
         assert len(hits[b][0]) == min(k, m)
 
 
+@pytest.mark.parametrize("n1", [64, 512])
+def test_block_query_matches_oracle_across_n1(ctx, n1):
+    """Block scoring at the smallest and largest n1 of the reference's delta
+    sweep: [AL | H] planes of 2 n1 bytes per plane row (one or eight K steps)."""
+    from bnutil import int8_matrix
+
+    c = capi()
+    m, B, trials, k = 900, 6, 3, 12
+    M = int8_matrix(m, 768, 90 + n1)
+    L = O.generate_subspace(bytes([5]) * 32, n1=n1)
+    cl = O.encrypt_cluster(M.reshape(-1), m, L, O.derive_h_seed(9, 0), n1=n1)
+    f = c.Flat.build(ctx, cl.m_enc, cl.a_l, cl.h_mat, m, n1=n1)
+    f.attach_client(L, M.reshape(-1), cl.s_mat.rowptr, cl.s_mat.idx, cl.s_mat.sign)
+    encs = [O.encode_query(int8_matrix(1, 768, 91 + n1 + b)[0], L, O.derive_h_seed(92, b), n1=n1) for b in range(B)]
+    seed = bytes([n1 % 251, 7]) * 16
+    hits, failed, mv = f.query_block(np.stack([e.v_enc for e in encs]), np.stack([e.g for e in encs]),
+                                     [(e.t_idx, e.t_sign) for e in encs], seed, trials, k, want_mv=True)
+    for b, enc in enumerate(encs):
+        r = O.matvec(cl.m_enc, m, N, enc.v_enc)
+        mvo = O.decode_scores(r, cl, L, enc)
+        ids, sc = O.topk(O.to_signed(mvo), k)
+        assert np.array_equal(mv[b], mvo), b
+        assert np.array_equal(hits[b][0], ids) and np.array_equal(hits[b][1], sc), b
+        assert failed[b] == O.verify_response(r, cl.m_enc, m, N, enc.v_enc, trials, seed)[0] == -1
+
+
 @pytest.mark.parametrize("m,B,trials", [(777, 5, 20), (4097, 17, 3), (10000, 2, 29), (1, 1, 1)])
 def test_block_verify_matches_oracle(ctx, m, B, trials):
     """Uniform F_p corpus (no client state needed): every trial's pair per query."""
