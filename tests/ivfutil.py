@@ -8,19 +8,20 @@ from bnutil import N, P, int8_matrix
 
 
 class IvfCase:
-    def __init__(self, sizes, seed=5, d=768, key_seed=bytes([2]) * 32, upload_seed=7):
+    def __init__(self, sizes, seed=5, d=768, key_seed=bytes([2]) * 32, upload_seed=7, n1=128):
         self.sizes = list(sizes)
+        self.n1 = n1
         self.nlist = len(sizes)
         total = sum(sizes)
         self.M = int8_matrix(total, d, seed)
         self.ids = np.random.default_rng(seed).permutation(total).astype(np.uint32)
         self.offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
-        self.L = O.generate_subspace(key_seed)
+        self.L = O.generate_subspace(key_seed, n1=n1)
         self.clusters = []
         for ci, m in enumerate(sizes):
             o = int(self.offsets[ci])
             self.clusters.append(O.encrypt_cluster(self.M[o : o + m].reshape(-1), m, self.L,
-                                                   O.derive_h_seed(upload_seed, ci)) if m else None)
+                                                   O.derive_h_seed(upload_seed, ci), n1=n1) if m else None)
 
     def concat(self):
         cs = [c for c in self.clusters if c is not None]

@@ -144,6 +144,29 @@ def test_verify_block_detects_tampered_response(case, ivf, where):
     assert ur[target][0] != zv[target][0]
 
 
+@pytest.mark.parametrize("n1", [64, 512])
+def test_query_block_across_n1(ctx, n1):
+    """IVF block scoring at the smallest and largest n1 of the reference's
+    delta sweep ([AL | H] pair images of 2 n1 bytes per plane row)."""
+    c = capi()
+    case = IvfCase([40, 0, 300, 7, 129], seed=n1, n1=n1)
+    m_enc, a_l, h, rp, ix, sg = case.concat()
+    v = c.Ivf.build(ctx, case.offsets, case.ids, m_enc, a_l, h, n1=n1)
+    v.attach_client(case.L, case.M.reshape(-1), rp, ix, sg)
+    v.block_prepare()
+    rng = np.random.default_rng(n1)
+    B, nprobe, trials, k = 5, 3, 4, 12
+    probes = np.stack([rng.choice(case.nlist, nprobe, replace=False) for _ in range(B)]).astype(np.uint32)
+    encs = [O.encode_query(int8_matrix(1, 768, 500 + n1 + b)[0], case.L, O.derive_h_seed(n1, b), n1=n1)
+            for b in range(B)]
+    seed = bytes([n1 % 251, 9]) * 16
+    hits, fc, ft = run_block(v, probes, encs, seed, trials, k)
+    for b in range(B):
+        ids, sc = case.oracle_score(list(probes[b]), encs[b], seed, trials, k)
+        assert np.array_equal(hits[b][0], ids) and np.array_equal(hits[b][1], sc), b
+        assert fc[b] == -1 and ft[b] == -1
+
+
 def test_query_block_rejects_bad_input(case, ivf):
     c = capi()
     probes, encs = batch(case, 2, 2, 3)
