@@ -11,8 +11,14 @@ corpus and reported under "block" in the same JSON line.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--block-sizes 8,32,128,512]
 
+Also in the line: a sustained run of 1,000 queries, the reference's default
+3 trials, the reference's own GPU scan kernel timed on the same corpus,
+the CPU baseline (the oracle over the full corpus, compared bit for bit),
+IVF (2M rows, 4096 k-means lists), the serving loop and the N = 100k,
+d = 384 workload.
+
 --impl reference times the reference's CPU path (the CPU restatement under
-oracle/) on the host cores over a bounded sample of the same workload.
+oracle/) on the host cores, one full-size query per timed step.
 Prints one JSON line (rank 0).
 """
 from __future__ import annotations
@@ -33,9 +39,10 @@ sys.path.insert(0, os.path.join(ROOT, "secure-vector-search_b200"))
 
 N_DIM = 1024
 P = (1 << 61) - 1
-# DRAM bytes (read + write) per corpus row of one tc_fused_kernel launch, from
-# the ncu capture in profiles/tc_fused_flat131k.md (131072 rows; the traffic
-# grows in proportion to the rows, so it is scaled to the bench's N).
+# DRAM bytes (read + write) per corpus row of one tc_fused_kernel launch:
+# dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the
+# kernel on a 131,072-row corpus, divided by its rows (the traffic grows in
+# proportion to the rows, so it is scaled to the bench's N).
 FUSED_DRAM_BYTES_PER_ROW = 8628
 METRIC = "BN F_p scan queries/s (flat N=1M, d=768, Freivalds k=20 fused, decode + top-10)"
 
@@ -63,51 +70,109 @@ def to_residues(x8: np.ndarray) -> np.ndarray:
     return out
 
 
-def synth_ivf(rows: int, d: int, nlist: int, seed: int):
+def _int8_rows(x: np.ndarray) -> np.ndarray:
+    """L2-normalise rows in place, then per-row max-abs int8 quantisation."""
+    x /= np.linalg.norm(x, axis=1, keepdims=True)
+    s = 127.0 / np.maximum(np.abs(x).max(axis=1, keepdims=True), 1e-12)
+    return np.clip(np.rint(x * s), -127, 127).astype(np.int8)
+
+
+def kmeans_lists(x8: np.ndarray, nlist: int, seed: int, iters: int = 25, device=None):
+    """Lloyd k-means (ivf-index/src/kmeans.rs:15-132: k-means++ seeding, then
+    assign / recompute until stable or `iters` rounds; an empty cluster's
+    centroid becomes 0) over the int8-valued f32 vectors, run with torch on
+    the GPU as data preparation: 2M x 4096 x 768 distances per round are
+    hours for the host restatement.  Distances are GEMM-form f32 and seeding
+    runs on a 65,536-point sample, so the partition is not the reference's
+    bit for bit (nor could it be: the reference sums in rayon order); it is
+    a real k-means partition of the corpus, fed identically to the GPU path
+    and to the oracle.  Centroid sums are exact (integer data, f64 sums), so
+    the result is reproducible.  Returns (centroids f32 [nlist][d],
+    assignment u32 [rows])."""
+    import torch
+
+    dev = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+    X = torch.from_numpy(x8).to(dev).to(torch.float32)
+    n = X.shape[0]
+    xn = (X * X).sum(1)  # exact: integers below 2^24
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+
+    def assign(C):
+        cn = (C * C).sum(1)
+        out = torch.empty(n, dtype=torch.int64, device=dev)
+        for r0 in range(0, n, 131072):
+            r1 = min(n, r0 + 131072)
+            dist = xn[r0:r1, None] - 2.0 * (X[r0:r1] @ C.T) + cn[None, :]
+            out[r0:r1] = dist.argmin(1)
+        return out
+
+    # k-means++ seeding on a sample: first centre uniform, then each next one
+    # with probability proportional to the squared distance to the nearest
+    # centre chosen so far (kmeans.rs:93-132)
+    samp = X[torch.randperm(n, generator=g, device=dev)[: min(n, 65536)]]
+    sn = (samp * samp).sum(1)
+    first = int(torch.randint(samp.shape[0], (1,), generator=g, device=dev).item())
+    C = torch.empty((nlist, X.shape[1]), dtype=torch.float32, device=dev)
+    C[0] = samp[first]
+    mind = (sn - 2.0 * (samp @ C[0]) + (C[0] * C[0]).sum()).clamp_min(0)
+    for ci in range(1, nlist):
+        pick = torch.multinomial(mind + 1e-12, 1, generator=g)
+        C[ci] = samp[pick[0]]
+        mind = torch.minimum(mind, (sn - 2.0 * (samp @ C[ci]) + (C[ci] * C[ci]).sum()).clamp_min(0))
+    for _ in range(iters):
+        a = assign(C)
+        sums = torch.zeros((nlist, X.shape[1]), dtype=torch.float64, device=dev)
+        for r0 in range(0, n, 262144):
+            sums.index_add_(0, a[r0 : r0 + 262144], X[r0 : r0 + 262144].to(torch.float64))
+        cnt = torch.bincount(a, minlength=nlist).to(torch.float64)
+        newC = torch.where(cnt[:, None] > 0, sums / cnt.clamp_min(1)[:, None], 0.0).to(torch.float32)
+        if torch.equal(newC, C):
+            break
+        C = newC
+    a = assign(C)
+    out = C.cpu().numpy(), a.to(torch.int32).cpu().numpy().astype(np.uint32)
+    del X, C, a
+    torch.cuda.empty_cache()
+    return out
+
+
+def synth_ivf(rows: int, d: int, nlist: int, seed: int, device=None):
     """Gaussian mixture with nlist unit-norm centres and Zipf(1.1) component
     weights; points = centre + 0.3 * N(0, I) / sqrt(d), L2-normalised,
-    int8-quantised per row.  The component of each point is its inverted
-    list (stands in for the k-means partition, which is not pinned to the
-    reference either); lists are stored in list order."""
+    int8-quantised per row (data order: ids are row numbers).  The inverted
+    lists are a k-means partition of those vectors (kmeans_lists, nlist
+    centroids, 25 rounds); rows are stored list by list, members of a list
+    in data order (ivf-index/src/ivf.rs build_index)."""
     rng = np.random.default_rng([seed, 0x1FF])
-    centres = rng.standard_normal((nlist, d), dtype=np.float32)
-    centres /= np.linalg.norm(centres, axis=1, keepdims=True)
+    mix = rng.standard_normal((nlist, d), dtype=np.float32)
+    mix /= np.linalg.norm(mix, axis=1, keepdims=True)
     w = 1.0 / np.arange(1, nlist + 1, dtype=np.float64) ** 1.1
     w /= w.sum()
-    counts = rng.multinomial(rows, w)
-    sizes = np.zeros(nlist, np.int64)
-    sizes[rng.permutation(nlist)] = counts
-    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
-    m8 = np.empty((rows, d), np.int8)
+    w = w[rng.permutation(nlist)]
     sigma = np.float32(0.3 / np.sqrt(d))
-    c0 = 0
-    while c0 < nlist:  # lists in chunks of ~256k rows
-        c1 = c0
-        while c1 < nlist and offsets[c1] - offsets[c0] < 262144:
-            c1 += 1
-        c1 = max(c1, c0 + 1)
-        r0, r1 = int(offsets[c0]), int(offsets[c1])
-        lab = np.repeat(np.arange(c0, c1), sizes[c0:c1])
-        x = centres[lab] + sigma * rng.standard_normal((r1 - r0, d), dtype=np.float32)
-        x /= np.linalg.norm(x, axis=1, keepdims=True)
-        s = 127.0 / np.maximum(np.abs(x).max(axis=1, keepdims=True), 1e-12)
-        m8[r0:r1] = np.clip(np.rint(x * s), -127, 127).astype(np.int8)
-        c0 = c1
-    ids = rng.permutation(rows).astype(np.uint32)
-    return {"centres": centres, "weights": w, "sizes": sizes, "offsets": offsets, "m8": m8, "ids": ids,
-            "sigma": sigma, "seed": seed}
+    x8 = np.empty((rows, d), np.int8)
+    for r0 in range(0, rows, 262144):
+        r1 = min(rows, r0 + 262144)
+        comp = rng.choice(nlist, size=r1 - r0, p=w)
+        x8[r0:r1] = _int8_rows(mix[comp] + sigma * rng.standard_normal((r1 - r0, d), dtype=np.float32))
+    centroids, assign = kmeans_lists(x8, nlist, seed, device=device)
+    order = np.argsort(assign, kind="stable")
+    sizes = np.bincount(assign, minlength=nlist).astype(np.int64)
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    return {"centres": centroids, "mix_centres": mix, "weights": w, "sizes": sizes, "offsets": offsets,
+            "m8": x8[order], "ids": order.astype(np.uint32), "sigma": sigma, "seed": seed}
 
 
 def synth_ivf_queries(data, nq: int, seed: int):
-    """Queries drawn like the corpus points (component by weight): f32 for
-    routing, int8 for encoding."""
+    """Queries drawn like the corpus points (mixture component by weight):
+    the int8 vector, and the same values as f32 for routing (the scorer sees
+    integer-valued f32 vectors, quantisation_q = 1)."""
     rng = np.random.default_rng([seed, 0x9E])
-    nlist, d = data["centres"].shape
-    comp = rng.choice(nlist, size=nq, p=data["sizes"] / data["sizes"].sum())
-    x = data["centres"][comp] + data["sigma"] * rng.standard_normal((nq, d), dtype=np.float32)
-    x /= np.linalg.norm(x, axis=1, keepdims=True)
-    s = 127.0 / np.maximum(np.abs(x).max(axis=1, keepdims=True), 1e-12)
-    return x.astype(np.float32), np.clip(np.rint(x * s), -127, 127).astype(np.int8)
+    nlist, d = data["mix_centres"].shape
+    comp = rng.choice(nlist, size=nq, p=data["weights"])
+    x8 = _int8_rows(data["mix_centres"][comp] + data["sigma"] * rng.standard_normal((nq, d), dtype=np.float32))
+    return x8.astype(np.float32), x8
 
 
 def build_ivf(ctx, data, seed: int):
@@ -176,30 +241,80 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-# ------------------------------------------------------------------ CPU leg
-def cpu_reference(d: int, trials: int, k: int, steps: int, warmup: int, n_total: int, seed: int):
-    """Times the CPU restatement of the reference path (oracle) on a bounded
-    sample of rows of the same generator; returns (qps scaled to n_total,
-    description)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+# ------------------------------------------------------------------ CPU legs
+def oracle_module():
+    """The CPU restatement of the reference path (oracle/): only the
+    cpu_baseline leg and the --impl reference arm run it."""
+    p = os.path.join(ROOT, "oracle")
+    if p not in sys.path:
+        sys.path.insert(0, p)
     import oracle as O
 
-    m = int(os.environ.get("BN_CPU_SAMPLE_ROWS", "16384"))
-    Mu = to_residues(synth_int8(m, d, seed))
+    return O
+
+
+def prefix_cluster(O, cl, rows: int):
+    """The first `rows` rows of an oracle cluster (views, no copies)."""
+    n, n1, s = cl.n, cl.n1, cl.s_mat
+    e = int(s.rowptr[rows])
+    return O.Cluster(rows, n, n1, cl.m_enc[: rows * n], cl.a_l[: rows * n1], cl.m_plain[: rows * n],
+                     cl.h_mat[: rows * n1], O.Sparse(s.rowptr[: rows + 1], s.idx[:e], s.sign[:e]))
+
+
+def cpu_reference_arm(args):
+    """--impl reference: the reference's CPU path restated in C (oracle/;
+    the Rust reference cannot be built here) on the box's host cores, on the
+    bench's own workload: keygen and encryption of the whole corpus on the
+    host (crypto.rs:235-270, 405-478), then every timed step one query over
+    all N rows (BnTmScorer::score, lib.rs:326-475: scan, Protocol 2, decode,
+    top-k).  Warm-up steps query the first 65,536 rows only (they page the
+    code and the corpus in; a CPU has no other warm-up)."""
+    O = oracle_module()
+    n, d, seed = args.rows, 768, 1
+    t0 = time.perf_counter()
+    Mu = to_residues(synth_int8(n, d, seed))
     L = O.generate_subspace(bytes([seed & 0xFF]) * 32)
-    cl = O.encrypt_cluster(Mu.reshape(-1), m, L, O.derive_h_seed(seed, 0))
-    qs = to_residues(synth_int8(warmup + steps, d, seed + 1000))
+    cl = O.encrypt_cluster(Mu.reshape(-1), n, L, O.derive_h_seed(seed, 0))
+    del Mu
+    setup_s = time.perf_counter() - t0
+    qs = to_residues(synth_int8(args.warmup + args.steps, d, seed + 1000))
+    warm = prefix_cluster(O, cl, min(n, 65536))
     times = []
-    for i in range(warmup + steps):
+    for i in range(args.warmup + args.steps):
         q_seed = O.derive_h_seed(seed ^ 0x5155455259, i)
-        t0 = time.perf_counter()
-        f, ids, sc, _, _ = O.score_flat(cl, L, qs[i], q_seed, trials, k, avx512=True)
-        t1 = time.perf_counter()
+        ta = time.perf_counter()
+        f, _, _, _, _ = O.score_flat(warm if i < args.warmup else cl, L, qs[i], q_seed, args.trials, 10)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - ta)
         assert f == -1
-        if i >= warmup:
-            times.append(t1 - t0)
-    per_q = statistics.median(times) * (n_total / m)
-    return 1.0 / per_q, m, O.NTHREADS, O.lib.bno_have_avx512() != 0
+    return len(times) / sum(times), setup_s, O.NTHREADS, O.lib.bno_have_avx512() != 0
+
+
+def cpu_baseline_leg(ctx, flat, Mu, L, H, rp, ix, sg, encs, seeds, q_seeds, qv, trials, k, nq=2):
+    """cpu_baseline of the GPU arm: the oracle on the host cores over the
+    GPU's own corpus (host copies of the device encryption), nq queries of
+    all N rows each, timed; the same queries through bn_flat_query are
+    compared with it bit for bit (every r residue, the top-k, the verdict)."""
+    from bn_b200 import capi
+
+    O = oracle_module()
+    n = flat.m
+    m_enc, a_l = capi.encrypt_cluster(ctx, Mu.reshape(-1), n, L, H, rp, ix, sg)
+    cl = O.Cluster(n, N_DIM, 128, m_enc, a_l, Mu.reshape(-1), H, O.Sparse(rp, ix, sg))
+    times, same = [], []
+    for i in range(nq):
+        ta = time.perf_counter()
+        f, ids, sc, r, _ = O.score_flat(cl, L, qv[i], q_seeds[i], trials, k, want_r=True)
+        times.append(time.perf_counter() - ta)
+        hits, gf, gr, _ = flat.query(encs[i][0][None], encs[i][1][None], [(encs[i][2], encs[i][3])], [seeds[i]],
+                                     trials, k, want_r=True)
+        same.append(bool(np.array_equal(gr[0], r) and np.array_equal(hits[0][0], ids)
+                         and np.array_equal(hits[0][1], sc) and int(gf[0]) == f == -1))
+    del m_enc, a_l, cl
+    return {"value": nq / sum(times), "unit": "queries/s", "cores": O.NTHREADS, "kind": "port",
+            "sample": f"{nq} queries over all {n} rows of the bench corpus (the GPU arm's own encryption, copied "
+                      f"to the host); AVX-512 row dot {'on' if O.lib.bno_have_avx512() else 'off'}",
+            "parity_vs_gpu": {"queries": nq, "r_topk_verdict_bit_exact": all(same)}}
 
 
 # ------------------------------------------------------------------ GPU leg
@@ -225,6 +340,61 @@ def whole_job_rate(units_per_rank: float, world: int, slowest_s: float) -> float
     return world * units_per_rank / slowest_s
 
 
+class QueryBuffers:
+    """Device-resident per-step inputs and outputs of the single-query path
+    (one query per step, B = 1)."""
+
+    def __init__(self, torch, dev, encs, seeds, k):
+        nq = len(encs)
+        t_arr = np.zeros((nq, N_DIM), np.uint32)
+        self.tn = tn = np.zeros(nq, np.uint32)
+        for i, (ve, g, ti, ts) in enumerate(encs):
+            tn[i] = ti.size
+            t_arr[i, : ti.size] = ti | np.where(ts < 0, np.uint32(0x80000000), np.uint32(0))
+        self.v = torch.from_numpy(np.stack([e[0] for e in encs]).view(np.int64)).to(dev)
+        self.g = torch.from_numpy(np.stack([e[1] for e in encs]).view(np.int64)).to(dev)
+        self.t = torch.from_numpy(t_arr.view(np.int32)).to(dev)
+        self.t_nnz = torch.from_numpy(tn.view(np.int32)).to(dev)
+        self.s = torch.from_numpy(np.frombuffer(b"".join(seeds), np.uint8).copy()).to(dev)
+        self.ids = torch.zeros((nq, k), dtype=torch.int32, device=dev)
+        self.sc = torch.zeros((nq, k), dtype=torch.int64, device=dev)
+        self.n = torch.zeros(nq, dtype=torch.int32, device=dev)
+        self.f = torch.full((nq,), 7, dtype=torch.int32, device=dev)
+        self.nq = nq
+
+    def ptrs(self, i):
+        i %= self.nq
+        return (self.v[i].data_ptr(), self.g[i].data_ptr(), self.t[i].data_ptr(), self.t_nnz[i : i + 1].data_ptr(),
+                self.s[32 * i : 32 * (i + 1)].data_ptr(), self.ids[i].data_ptr(), self.sc[i].data_ptr(),
+                self.n[i : i + 1].data_ptr(), self.f[i : i + 1].data_ptr())
+
+
+def make_timer(torch, stream, dist, dev):
+    """timed(fn, warmup, reps): warm-up calls, then reps calls bracketed by a
+    barrier + synchronize and CUDA events on the launch stream; returns the
+    slowest rank's ms."""
+
+    def timed(fn, warmup, reps, arm=None):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for i in range(warmup):
+            fn(i)
+        if arm:
+            arm()
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for i in range(reps):
+            fn(warmup + i)
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        return max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
+
+    return timed
+
+
 def run_gpu(args, rank: int, world: int, local_rank: int):
     import torch
 
@@ -241,72 +411,44 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     H, rp, ix, sg = capi.host_regenerate_h_s(capi.host_derive_h_seed(seed, 0), n_rows)
     ctx = capi.Context(local_rank)
     flat = capi.Flat.build_from_plain(ctx, Mu.reshape(-1), n_rows, L, H, rp, ix, sg)
-    del Mu, H, rp, ix, sg
+    if not (rank == 0 and world == 1 and not args.no_cpu_baseline):
+        del Mu, H, rp, ix, sg  # kept only for the CPU baseline leg
 
-    nq = args.warmup + args.steps
+    nq = max(args.warmup + args.steps, args.sustained)
     qv = to_residues(synth_int8(nq, d, seed + 1000))
-    encs, seeds = [], []
+    encs, seeds, q_seeds = [], [], []
     for i in range(nq):
         q_seed = capi.host_derive_h_seed(seed ^ 0x5155455259, i)
         encs.append(capi.host_encode_query(qv[i], L, q_seed))
         seeds.append(capi.host_domain_separate(q_seed))
+        q_seeds.append(q_seed)
     setup_s = time.perf_counter() - t_setup
 
-    # device-resident per-step inputs
-    t_arr = np.zeros((nq, N_DIM), np.uint32)
-    tn = np.zeros(nq, np.uint32)
-    for i, (ve, g, ti, ts) in enumerate(encs):
-        tn[i] = ti.size
-        t_arr[i, : ti.size] = ti | np.where(ts < 0, np.uint32(0x80000000), np.uint32(0))
-    d_v = torch.from_numpy(np.stack([e[0] for e in encs]).view(np.int64)).to(dev)
-    d_g = torch.from_numpy(np.stack([e[1] for e in encs]).view(np.int64)).to(dev)
-    d_t = torch.from_numpy(t_arr.view(np.int32)).to(dev)
-    d_tn = torch.from_numpy(tn.view(np.int32)).to(dev)
-    d_s = torch.from_numpy(np.frombuffer(b"".join(seeds), np.uint8).copy()).to(dev)
-    d_ids = torch.zeros((nq, k), dtype=torch.int32, device=dev)
-    d_sc = torch.zeros((nq, k), dtype=torch.int64, device=dev)
-    d_n = torch.zeros(nq, dtype=torch.int32, device=dev)
-    d_f = torch.zeros(nq, dtype=torch.int32, device=dev)
+    qb = QueryBuffers(torch, dev, encs, seeds, k)
     d_r = torch.zeros(n_rows, dtype=torch.int64, device=dev)
     stream = torch.cuda.Stream(device=dev)
     sp = stream.cuda_stream
-
-    def ptrs(i):
-        return (d_v[i].data_ptr(), d_g[i].data_ptr(), d_t[i].data_ptr(), d_tn[i : i + 1].data_ptr(),
-                d_s[32 * i : 32 * (i + 1)].data_ptr(), d_ids[i].data_ptr(), d_sc[i].data_ptr(),
-                d_n[i : i + 1].data_ptr(), d_f[i : i + 1].data_ptr())
-
-    plans = {"full": flat.plan(1, trials, k), "noverify": flat.plan(1, 0, k)}
+    plans = {"full": flat.plan(1, trials, k), "noverify": flat.plan(1, 0, k), "trials3": flat.plan(1, 3, k)}
     dist = torch.distributed if world > 1 else None
+    timed = make_timer(torch, stream, dist, dev)
 
-    def timed(fn, reps, arm=None):
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        for i in range(args.warmup):
-            fn(i)
-        if arm:
-            arm()
-        stream.synchronize()
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for i in range(reps):
-            fn(args.warmup + i)
-        ev1.record(stream)
-        ev1.synchronize()
-        torch.cuda.synchronize()
-        return max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
-
-    # the dominant kernel (the one pass over M_enc: fused scan + Protocol 2) is
-    # timed inside every timed step with CUDA events on its launch stream
+    # The clock sampler runs over the sustained run (config 2's 1,000 queries
+    # one at a time) and the K-step window right after it; the dominant
+    # kernel (the one pass over M_enc: fused scan + Protocol 2) is timed
+    # inside every one of the K steps with CUDA events on its launch stream.
     with ClockSampler(local_rank) as clk:
-        full_ms = timed(lambda i: plans["full"].enqueue(*ptrs(i), sp), args.steps,
+        sus_ms = (timed(lambda i: plans["full"].enqueue(*qb.ptrs(i), sp), args.warmup, args.sustained)
+                  if args.sustained else 0.0)
+        full_ms = timed(lambda i: plans["full"].enqueue(*qb.ptrs(i), sp), args.warmup, args.steps,
                         arm=lambda: plans["full"].profile(args.steps))
     fused_ms = plans["full"].profile_read()
-    nov_ms = timed(lambda i: plans["noverify"].enqueue(*ptrs(i), sp), args.steps)
-    scan_ms = timed(lambda i: plans["full"].enqueue_scan(d_v[i].data_ptr(), d_r.data_ptr(), sp), args.steps)
-    ok = d_f[args.warmup :].cpu().numpy()
-    assert np.all(ok == -1), "honest-server verification failed"
+    assert plans["full"].status() == 0
+    assert np.all(qb.f.cpu().numpy() == -1), "honest-server verification failed"
+    nov_ms = timed(lambda i: plans["noverify"].enqueue(*qb.ptrs(i), sp), args.warmup, args.steps)
+    t3_ms = timed(lambda i: plans["trials3"].enqueue(*qb.ptrs(i), sp), args.warmup, args.steps)
+    scan_ms = timed(lambda i: plans["full"].enqueue_scan(qb.v[i % qb.nq].data_ptr(), d_r.data_ptr(), sp),
+                    args.warmup, args.steps)
+    assert np.all(qb.f.cpu().numpy() == -1), "honest-server verification failed"
 
     # e2e through the C ABI with host buffers (H2D of the encoded query, D2H of hits)
     for i in range(min(args.warmup, nq)):
@@ -328,7 +470,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     stages = {"scan_only_step": scan_s, "protocol2_extra": verify_s, "decode_topk": decode_s}
     fused_s = float(np.mean(fused_ms)) / 1e3
     achieved = bytes_scan / fused_s / 1e9
-    h2d = 1024 * 8 + 128 * 8 + 4 * int(np.mean(tn)) + 4 + 32
+    h2d = 1024 * 8 + 128 * 8 + 4 * int(np.mean(qb.tn)) + 4 + 32
     d2h = k * 12 + 8
     res = {
         "metric": METRIC,
@@ -358,14 +500,29 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
         "e2e": {"value": whole_job_rate(args.steps, world, e2e_s), "unit": "queries/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": 9 * args.steps,  # limbs, ugen, query image, fused, rreduce, finish, decide, L^T v, decode + top-k
-        "clocks": clk.summary(),
+        "clocks": dict(clk.summary(), window=f"the {args.sustained}-query sustained run and the K timed steps"),
+        "sustained": {"queries": args.sustained, "qps": whole_job_rate(args.sustained, world, sus_ms / 1e3)
+                      if args.sustained else None, "ms_per_query": sus_ms / max(args.sustained, 1),
+                      "note": "config 2's 1,000 queries one at a time, device-resident inputs, same plan"},
+        "trials3": {"qps": whole_job_rate(args.steps, world, t3_ms / 1e3), "ms_per_step": t3_ms / args.steps,
+                    "note": "the reference's default lambda' = 3 trials (params.rs:198-205), same workload"},
         "setup_s": setup_s,
     }
-    plans["full"].close()
-    plans["noverify"].close()
+    for p in plans.values():
+        p.close()
     progress("single-query leg done")
+    if args.ref_kernel:
+        res["reference_gpu_kernel"] = run_ref_kernel(args, flat, qb, d_r, stream, timed, peak, scan_s, fused_s,
+                                                      nov_ms)
+        progress("reference GPU kernel leg done")
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        res["cpu_baseline"] = cpu_baseline_leg(ctx, flat, Mu, L, H, rp, ix, sg, encs, seeds, q_seeds, qv, trials, k)
+        del Mu, H, rp, ix, sg
+        progress("CPU baseline leg done")
+    del qb, d_r
     if args.block_sizes:
         res["block"] = run_block(args, flat, L, seed, dev, stream, res["value"], dist)
+        res["block_qps"] = {B: round(v["qps"], 1) for B, v in res["block"]["per_B"].items()}
         progress("block leg done")
     if args.ivf_rows:
         res["ivf"], ivf, data = run_ivf(args, ctx, dist)
@@ -375,8 +532,101 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             progress("serving leg done")
         ivf.close()
     flat.close()
+    if args.config1:
+        res["config1"] = run_config1(args, ctx, dev, stream, timed, rank, world)
+        progress("config-1 leg done")
     ctx.close()
     return res
+
+
+def run_ref_kernel(args, flat, qb, d_r, stream, timed, peak, scan_s, fused_s, nov_ms):
+    """The reference's own GPU scan kernel (bntm_compute_products,
+    scorer-bntm/src/gpu/kernels.cu:100-178, compiled from the reference
+    source for sm_100a; one 256-thread CTA per row) timed on the same corpus,
+    stream and queries as the product's kernels, its r checked bit for bit
+    against the product's scan."""
+    import torch
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_gpu
+
+    lib = ref_gpu.load()
+    if lib is None:
+        return {"unavailable": "oracle/_ref/libbnref_gpu.so was not built (no reference checkout at build time)"}
+    m_enc = flat.device_m_enc()
+    r_ref = torch.zeros_like(d_r)
+    sp = stream.cuda_stream
+
+    def ref(i):
+        assert lib.bnref_compute_products(m_enc, qb.v[i % qb.nq].data_ptr(), r_ref.data_ptr(), flat.m, sp) == 0
+
+    ms = timed(ref, args.warmup, args.steps) / args.steps
+    # bit-exact against the product's scan on one query
+    plan = flat.plan(1, 0, 0)
+    with torch.cuda.stream(stream):
+        plan.enqueue_scan(qb.v[0].data_ptr(), d_r.data_ptr(), sp)
+        ref(0)
+    stream.synchronize()
+    same = bool(torch.equal(d_r, r_ref))
+    plan.close()
+    gbs = flat.m * N_DIM * 8 / (ms / 1e3) / 1e9
+    return {"kernel": "bntm_compute_products (reference kernels.cu:100-178, built for sm_100a)",
+            "ms_per_launch": ms, "achieved_gbs": gbs, "frac_of_peak": gbs / peak,
+            "r_equals_product_scan": same,
+            "product_scan_only_ms": scan_s * 1e3, "product_fused_scan_protocol2_ms": fused_s * 1e3,
+            "speedup_scan_only": ms / (scan_s * 1e3), "speedup_fused_incl_20_trials": ms / (fused_s * 1e3)}
+
+
+def run_config1(args, ctx, dev, stream, timed, rank, world):
+    """Config 1 (the reference's CPU case): N = 100,000, d = 384, seed 0,
+    100 queries one at a time, top-10, trials 20 and the reference's default
+    3: the GPU path timed, and the oracle on the host cores over the first 10
+    queries of each, compared bit for bit."""
+    import torch
+
+    from bn_b200 import capi
+
+    n, d, k, seed, nq = 100_000, 384, 10, 0, 100
+    Mu = to_residues(synth_int8(n, d, seed))
+    L = capi.host_generate_subspace(bytes([seed]) * 32)
+    H, rp, ix, sg = capi.host_regenerate_h_s(capi.host_derive_h_seed(seed, 0), n)
+    flat = capi.Flat.build_from_plain(ctx, Mu.reshape(-1), n, L, H, rp, ix, sg)
+    qv = to_residues(synth_int8(nq, d, seed + 1000))
+    encs, seeds, q_seeds = [], [], []
+    for i in range(nq):
+        q_seed = capi.host_derive_h_seed(seed ^ 0x5155455259, i)
+        encs.append(capi.host_encode_query(qv[i], L, q_seed))
+        seeds.append(capi.host_domain_separate(q_seed))
+        q_seeds.append(q_seed)
+    qb = QueryBuffers(torch, dev, encs, seeds, k)
+    sp = stream.cuda_stream
+    out = {"N": n, "d": d, "queries": nq, "k": k, "per_trials": {}}
+    cl = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        O = oracle_module()
+        m_enc, a_l = capi.encrypt_cluster(ctx, Mu.reshape(-1), n, L, H, rp, ix, sg)
+        cl = O.Cluster(n, N_DIM, 128, m_enc, a_l, Mu.reshape(-1), H, O.Sparse(rp, ix, sg))
+    for trials in (20, 3):
+        plan = flat.plan(1, trials, k)
+        ms = timed(lambda i: plan.enqueue(*qb.ptrs(i), sp), 3, nq)
+        assert plan.status() == 0 and np.all(qb.f.cpu().numpy() == -1)
+        rec = {"gpu_qps": whole_job_rate(nq, world, ms / 1e3), "gpu_ms_per_query": ms / nq}
+        if cl is not None:
+            O = oracle_module()
+            ids_g = qb.ids.cpu().numpy().view(np.uint32)
+            sc_g = qb.sc.cpu().numpy()
+            times, same = [], []
+            for i in range(10):
+                ta = time.perf_counter()
+                f, ids, sc, _, _ = O.score_flat(cl, L, qv[i], q_seeds[i], trials, k)
+                times.append(time.perf_counter() - ta)
+                same.append(bool(f == -1 and np.array_equal(ids_g[i], ids) and np.array_equal(sc_g[i], sc)))
+            rec.update({"cpu_qps": 10 / sum(times), "cpu_cores": O.NTHREADS, "cpu_queries": 10,
+                        "gpu_over_cpu": rec["gpu_qps"] / (10 / sum(times)), "topk_verdict_bit_exact": all(same)})
+        out["per_trials"][str(trials)] = rec
+        plan.close()
+    flat.close()
+    return out
 
 
 def run_block(args, flat, L, seed, dev, stream, single_qps, dist):
@@ -663,13 +913,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--rows", type=int, default=1_000_000)
     ap.add_argument("--trials", type=int, default=20)
+    ap.add_argument("--sustained", type=int, default=1000,
+                    help="queries of the sustained single-query run (config 2's 1,000; 0 to skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-kernel", dest="ref_kernel", action="store_false",
+                    help="skip timing the reference's own GPU scan kernel")
+    ap.add_argument("--no-config1", dest="config1", action="store_false",
+                    help="skip the N = 100k, d = 384 workload (the reference's CPU case)")
     ap.add_argument("--block-sizes", default="8,32,128,512",
                     help="block scoring sizes B to time after the single-query metric ('' to skip)")
     ap.add_argument("--no-block-autotune", dest="block_autotune", action="store_false",
                     help="block plans keep the default GEMM tiling (no autotuning launches)")
     ap.add_argument("--ivf-rows", type=int, default=2_000_000, help="IVF corpus rows (0 to skip the IVF legs)")
-    ap.add_argument("--serve-rates", default="2000,10000,50000", help="Poisson arrival rates of the serving leg")
+    ap.add_argument("--serve-rates", default="2000,5000,10000,50000", help="Poisson arrival rates of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=1.5)
     args = ap.parse_args()
 
@@ -680,16 +936,17 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        qps, m, cores, avx = cpu_reference(768, args.trials, 10, args.steps, args.warmup, args.rows, 1)
+        qps, setup_s, cores, avx = cpu_reference_arm(args)
         line = {"metric": METRIC, "value": qps, "unit": "queries/s", "n_gpus": args.gpus, "steps": args.steps,
                 "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "u64 (exact F_p, p=2^61-1)", "data": "synthetic",
-                "config": {"workload": "bn_flat_single_query", "N": args.rows, "d": 768, "freivalds_trials": args.trials,
-                           "k": 10, "B": 1},
+                "config": {"workload": "bn_flat_single_query", "N": args.rows, "d": 768, "n": N_DIM, "n1": 128,
+                           "freivalds_trials": args.trials, "k": 10, "B": 1},
                 "impl": "reference",
                 "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
-                                 "sample": f"{m} rows of the same generator per query, time scaled by N/{m}; "
-                                           f"AVX-512 row dot {'on' if avx else 'off'}"},
+                                 "sample": f"every timed step one query over all {args.rows} rows (warm-up steps: "
+                                           f"the first 65,536 rows); corpus keygen + encryption on the host took "
+                                           f"{setup_s:.0f} s; AVX-512 row dot {'on' if avx else 'off'}"},
                 "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -701,11 +958,6 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600),
                                              device_id=torch.device("cuda", local_rank))
     res = run_gpu(args, rank, world, local_rank)
-    if rank == 0 and not args.no_cpu_baseline:
-        qps, m, cores, avx = cpu_reference(768, args.trials, 10, 6, 1, args.rows, 1)
-        res["cpu_baseline"] = {"value": qps, "unit": "queries/s", "cores": cores, "kind": "port",
-                               "sample": f"{m} rows of the same generator per query (6 queries), time scaled by "
-                                         f"N/{m}; AVX-512 row dot {'on' if avx else 'off'}"}
     if world > 1:
         import torch
 

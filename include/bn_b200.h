@@ -35,7 +35,15 @@ extern "C" {
 #define BN_EBUDGET (-3)      /* payload exceeds budget    (GpuError::BudgetTooSmall) */
 #define BN_ENODEV (-4)       /* no usable CUDA device                                */
 #define BN_EUNSUPPORTED (-5) /* handle lacks the client state this call needs       */
-#define BN_EAGAIN (-6)       /* bn_server_wait: the request is not complete yet      */
+#define BN_EAGAIN (-6)       /* bn_server_wait: the request is not complete yet;
+                                bn_server_submit_*: the queue is full, retry later   */
+/* A Protocol 2 draw equalled p.  The reference rejects that draw and takes
+ * the next one (sample_fp, crypto.rs:155-162), which shifts every later draw
+ * of the stream by one; the kernels here draw by stream position, so the
+ * call reports the event instead of returning a verdict that could differ
+ * from the reference's.  Odds: 2^-61 per draw (about 2^-37 per query at
+ * N = 1M, 20 trials).  Retrying with another seed is the caller's choice. */
+#define BN_EDRAW (-7)
 
 #define BN_TOPK_MAX 1024
 #define BN_MAX_TRIALS 64 /* Protocol 2 trials per call */
@@ -126,10 +134,17 @@ int bn_flat_verify(bn_flat* h, const uint64_t* r, const uint64_t* v_enc, const u
  * could synchronise the device.  Its scratch is a fixed array of about
  * 3 MiB in the library, held on every GPU that loads it until exit; trials
  * must be in 1..=BN_NOALLOC_MAX_TRIALS.  All calls share that array: calls
- * that overlap on the GPU race, so serialise them.  The first call on a
- * device resolves the array's address; make it outside stream capture.
+ * that overlap on the GPU race, so serialise them.  The array and the
+ * kernels this call launches are loaded, and the array's address resolved,
+ * by bn_ctx_create for that device (CUDA loads modules lazily, and loading
+ * one allocates device memory): create the context before the memory budget
+ * is handed out, and this call allocates nothing afterwards.
  *   d_r m, d_v_enc 1024, d_v_seed 32 bytes; outputs d_failed_trial (1),
- *   d_ur / d_zv (trials) as in bn_flat_verify. */
+ *   d_ur / d_zv (trials) as in bn_flat_verify, except that *d_failed_trial
+ *   = -2 when a draw equalled p (the BN_EDRAW event, reported in the output
+ *   because nothing is read back to the host).  An empty corpus gives -1 and
+ *   zero sums, as bn_flat_verify does.  The calling thread's current device
+ *   is left as it was. */
 #define BN_NOALLOC_MAX_TRIALS 24
 int bn_flat_verify_noalloc(bn_flat* h, const uint64_t* d_r, const uint64_t* d_v_enc, const uint8_t* d_v_seed,
                            uint32_t trials, int32_t* d_failed_trial, uint64_t* d_ur, uint64_t* d_zv, void* stream);
@@ -161,9 +176,13 @@ int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v_enc, const uint64_t* d_g, co
                     uint32_t* d_n, int32_t* d_failed, void* stream);
 /* Scan-only enqueue of the same plan: d_r (B x m) = M_enc v_enc. */
 int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v_enc, uint64_t* d_r, void* stream);
-/* Device flags of the last enqueue of this plan (0 = healthy; non-zero when
- * a bounded device-side wait timed out and the outputs must be discarded).
- * Synchronous: call after the enqueued work has completed. */
+/* Device flags of the last enqueue of this plan (0 = healthy).  Bits
+ * 0x1..0x20: a bounded device-side wait timed out; bit 0x1000
+ * (BN_STATUS_DRAW_HIT_P): a Protocol 2 draw equalled p (see BN_EDRAW); block
+ * plans add 0x100 when a T column sum left [-128, 127].  Any bit set means
+ * the outputs must be discarded.  Synchronous: call after the enqueued work
+ * has completed. */
+#define BN_STATUS_DRAW_HIT_P 0x1000u
 int bn_plan_status(bn_plan* p, uint32_t* device_flags);
 /* Kernel timing for measurement: after bn_plan_profile(p, n), the next n
  * enqueues record CUDA events on their stream right before and after the
@@ -364,6 +383,14 @@ int bn_server_wait(bn_server* s, uint64_t ticket, uint32_t timeout_ms, uint32_t*
 int bn_server_stats(bn_server* s, int reset, bn_server_stats_t* out);
 /* Drains queued and in-flight requests, then frees the server. */
 int bn_server_destroy(bn_server* s);
+
+/* ---------------------------------------------------------------- testing
+ * No counterpart in the reference.  While `on` is non-zero, every Protocol 2
+ * run on this context's handles behaves as if one of its draws had equalled
+ * p (BN_EDRAW from the host-buffer calls, BN_STATUS_DRAW_HIT_P in
+ * bn_plan_status, failed_trial = -2 from bn_flat_verify_noalloc), so that a
+ * caller can exercise its handling of that 2^-61 event. */
+int bn_debug_plant_draw_hit(bn_ctx* ctx, int on);
 
 /* ---------------------------------------------------------------- keygen
  * encrypt_cluster (crypto.rs:405-478) on the device with host in/out:

@@ -16,11 +16,12 @@ N = 1024
 P = (1 << 61) - 1
 TOPK_MAX = 1024
 
-BN_OK, BN_EINVAL, BN_ECUDA, BN_EBUDGET, BN_ENODEV, BN_EUNSUPPORTED, BN_EAGAIN = 0, -1, -2, -3, -4, -5, -6
+BN_OK, BN_EINVAL, BN_ECUDA, BN_EBUDGET, BN_ENODEV, BN_EUNSUPPORTED, BN_EAGAIN, BN_EDRAW = 0, -1, -2, -3, -4, -5, -6, -7
+STATUS_DRAW_HIT_P = 0x1000
 ENGINE_TENSOR, ENGINE_CUDA_CORE = 0, 1
 BLOCK_AUTOTUNE = 1
 _NAMES = {BN_EINVAL: "EINVAL", BN_ECUDA: "ECUDA", BN_EBUDGET: "EBUDGET", BN_ENODEV: "ENODEV",
-          BN_EUNSUPPORTED: "EUNSUPPORTED", BN_EAGAIN: "EAGAIN"}
+          BN_EUNSUPPORTED: "EUNSUPPORTED", BN_EAGAIN: "EAGAIN", BN_EDRAW: "EDRAW"}
 
 
 class BnError(RuntimeError):
@@ -60,6 +61,7 @@ _SIGS = {
     "bn_ctx_destroy": (C.c_int, [vp]),
     "bn_ctx_memory": (C.c_int, [vp, vp, vp, vp]),
     "bn_ctx_set_engine": (C.c_int, [vp, C.c_int]),
+    "bn_debug_plant_draw_hit": (C.c_int, [vp, C.c_int]),
     "bn_flat_build": (C.c_int, [vp, vp, vp, vp, u64, u32, u32, vp]),
     "bn_flat_attach_client": (C.c_int, [vp, vp, vp, SparseCsr]),
     "bn_flat_build_from_plain": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, vp]),
@@ -164,6 +166,10 @@ class Context:
 
     def set_engine(self, engine: int):
         check(lib.bn_ctx_set_engine(self.h, engine))
+
+    def plant_draw_hit(self, on: bool):
+        """Testing hook: Protocol 2 runs behave as if a draw had equalled p."""
+        check(lib.bn_debug_plant_draw_hit(self.h, 1 if on else 0))
 
     def memory(self):
         b, u, p = u64(), u64(), u64()

@@ -487,6 +487,7 @@ static void enqueue_verify(BlockPlan& b, const uint64_t* d_v, const uint8_t* d_s
     uint64_t* z = reinterpret_cast<uint64_t*>(d + b.o_z);
     uint64_t* urpart = reinterpret_cast<uint64_t*>(d + b.o_urpart);
     const int sms = b.h->e.ctx->num_sms;
+    if (b.trials && b.h->e.ctx->debug_draw_hit) launch_or_flag(err, DRAW_HIT_P, s);
     for (uint32_t t0 = 0; t0 < b.trials; t0 += TC_MAX_TRIALS) {
         const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, b.trials - t0);
         launch_tc_ugen(vseg, blocks, b.nblocks, reinterpret_cast<const ChaChaKey*>(d_seed), nullptr, t0, tc, b.n_rows,
@@ -636,7 +637,7 @@ int block_query_finish(BlockPlan& b, uint32_t nq, uint32_t* ids, int64_t* scores
     auto at = [&](uint64_t off) { return h + (off - b.o_in); };
     const int32_t* hf = reinterpret_cast<const int32_t*>(h + (b.o_out_end - b.o_in));
     const uint32_t* flags = reinterpret_cast<const uint32_t*>(hf + B);
-    if (flags[0]) return fail(BN_ECUDA, "a device pipeline wait timed out or a draw hit p (flags 0x%x)", flags[0]);
+    TRY(device_flags_status(flags[0]));
     if (flags[1]) return fail(BN_EINVAL, "a T column sum leaves [-128, 127]");
     const uint32_t* hid = reinterpret_cast<const uint32_t*>(at(b.o_out_ids));
     const int64_t* hsc = reinterpret_cast<const int64_t*>(at(b.o_out_sc));
@@ -697,7 +698,7 @@ int block_verify_host(BlockPlan& b, const uint64_t* r, const uint64_t* v_enc, co
     uint32_t flags = 0;
     CU(cudaMemcpyAsync(&flags, d + b.o_err, 4, cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
-    if (flags) return fail(BN_ECUDA, "a device pipeline wait timed out or a draw hit p (flags 0x%x)", flags);
+    TRY(device_flags_status(flags));
     if (failed) memcpy(failed, hf.data(), (uint64_t)B * 4);
     return BN_OK;
 }

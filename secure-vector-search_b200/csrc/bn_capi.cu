@@ -318,6 +318,7 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
     o.ur = L.take<uint64_t>(std::max<uint64_t>(z.nvseg * z.trials, 1));
     o.zv = L.take<uint64_t>(std::max<uint64_t>(z.nvseg * z.trials, 1));
     o.err = L.take<uint32_t>(1);
+    o.flags = L.take<uint32_t>(1);  // DRAW_HIT_P when a Protocol 2 draw equalled p
     o.out_end = L.off;
     o.limbs = L.take<QLimb>((uint64_t)z.B * N);
     o.x = L.take<uint64_t>((uint64_t)z.B * z.n1);
@@ -328,7 +329,6 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
     const uint64_t up = !z.trials ? 1 : tc ? z.nblocks * z.trials : (uint64_t)z.nvseg * z.fp.chunks * z.trials;
     o.z_part = L.take<uint64_t>(std::max<uint64_t>(zp, 1));
     o.ur_part = L.take<uint64_t>(std::max<uint64_t>(up, 1));
-    o.flags = L.take<uint32_t>(1);
     const uint64_t cand = (uint64_t)z.ctas * std::max<uint32_t>(z.k, 1);  // z.ctas: decode CTAs of all queries
     o.cand_s = L.take<int64_t>(cand);
     o.cand_i = L.take<uint32_t>(cand);
@@ -365,12 +365,13 @@ int make_tc_maps(const Sizes& z, const uint8_t* d_u, const uint8_t* d_w, TcMaps&
 int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m, const Inputs& in, const Scratch& sc,
                      const Outputs& out, cudaStream_t s, cudaEvent_t prof0, cudaEvent_t prof1) {
     CU(cudaMemsetAsync(sc.err, 0, 4, s));
+    CU(cudaMemsetAsync(sc.flags, 0, 4, s));
+    if (z.trials && ctx->debug_draw_hit) launch_or_flag(sc.flags, DRAW_HIT_P, s);
     launch_query_limbs(in.v, z.B, sc.limbs, s);
     const ChaChaKey* keys = reinterpret_cast<const ChaChaKey*>(in.seeds);
     if (z.trials && z.engine == BN_ENGINE_TENSOR) {
         // One pass over m_enc yields r and the first <= 20 trials' z (tensor
         // cores); later passes of 20 trials reuse the now-known r.
-        CU(cudaMemsetAsync(sc.flags, 0, 4, s));
         for (uint32_t t0 = 0, ps = 0; t0 < z.trials; t0 += TC_MAX_TRIALS, ++ps) {
             const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, z.trials - t0), nr = pass_rows(tc);
             if (ps == 0) {
@@ -398,7 +399,6 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
                     sc.err, s);
         if (prof1) CU(cudaEventRecord(prof1, s));
         if (z.trials) {
-            CU(cudaMemsetAsync(sc.flags, 0, 4, s));
             launch_freivalds(c.m_enc.at<uint64_t>(), sc.r, m.vsegs, m.nvseg, keys, z.trials, z.fp, sc.z_part, sc.ur_part,
                              sc.flags, s);
             launch_freivalds_finish(sc.z_part, sc.ur_part, in.v, m.vsegs, m.nvseg, z.trials, z.fp, sc.ur, sc.zv,
@@ -564,6 +564,7 @@ int job_launch(Engine& e, QueryJob& j, DevMem& ws, PinnedMem& host, cudaStream_t
     if (hm.segs.empty()) {
         CU(cudaMemsetAsync(out.n, 0, (uint64_t)j.B * 4, s));
         CU(cudaMemsetAsync(sc.err, 0, 4, s));
+        CU(cudaMemsetAsync(sc.flags, 0, 4, s));
     } else {
         TRY(enqueue_pipeline(e.ctx, e.c, j.z, m, in, sc, out, s, nullptr, nullptr));
     }
@@ -578,8 +579,8 @@ int job_finish(const QueryJob& j, const PinnedMem& host, uint32_t* ids, int64_t*
     const HostMeta& hm = *j.hm;
     const RunLayout& o = j.o;
     const char* h = host.at<char>();
-    if (const uint32_t ev = *reinterpret_cast<const uint32_t*>(h + o.err))
-        return fail(BN_ECUDA, "a device pipeline wait timed out (flags 0x%x); results discarded", ev);
+    TRY(device_flags_status(*reinterpret_cast<const uint32_t*>(h + o.err) |
+                            *reinterpret_cast<const uint32_t*>(h + o.flags)));
     const uint32_t k = j.k, ks = std::max<uint32_t>(k, 1);
     const uint32_t* hid = reinterpret_cast<const uint32_t*>(h + o.ids);
     const int64_t* hsc = reinterpret_cast<const int64_t*>(h + o.scores);
@@ -654,6 +655,7 @@ int run_verify(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* r, const
     int32_t* dfail = reinterpret_cast<int32_t*>(d + o.vfailed);
     CU(cudaMemsetAsync(sc.flags, 0, 4, e.stream));
     CU(cudaMemsetAsync(sc.err, 0, 4, e.stream));
+    if (e.ctx->debug_draw_hit) launch_or_flag(sc.flags, DRAW_HIT_P, e.stream);
     if (z.engine == BN_ENGINE_TENSOR) {
         for (uint32_t t0 = 0, ps = 0; t0 < trials; t0 += TC_MAX_TRIALS, ++ps) {
             const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, trials - t0), nr = pass_rows(tc);
@@ -672,8 +674,8 @@ int run_verify(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* r, const
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(h + o.out_begin, d + o.out_begin, o.out_end - o.out_begin, cudaMemcpyDeviceToHost, e.stream));
     CU(cudaStreamSynchronize(e.stream));
-    if (const uint32_t ev = *reinterpret_cast<uint32_t*>(h + o.err))
-        return fail(BN_ECUDA, "a device pipeline wait timed out (flags 0x%x); results discarded", ev);
+    TRY(device_flags_status(*reinterpret_cast<const uint32_t*>(h + o.err) |
+                            *reinterpret_cast<const uint32_t*>(h + o.flags)));
     *failed_trial = *reinterpret_cast<int32_t*>(h + o.vfailed);
     const uint32_t ran = *failed_trial < 0 ? trials : (uint32_t)*failed_trial + 1;
     for (uint32_t t = 0; t < trials; ++t) {
@@ -746,6 +748,10 @@ int run_dense_terms(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* g, 
 }  // namespace api
 }  // namespace bn
 
+// Defined in bn_noalloc.cu: loads the allocation-free verifier's static
+// scratch and kernels on `device` and resolves the scratch address.
+extern "C" int bn_internal_noalloc_setup(int device);
+
 struct bn_plan {
     bn_flat* h = nullptr;
     Sizes z{};
@@ -801,6 +807,9 @@ int bn_ctx_create(int device, uint64_t vram_budget_bytes, bn_ctx** out) {
     if (prop.major < 10) return fail(BN_ENODEV, "device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
     size_t free_b = 0, total_b = 0;
     CU(cudaMemGetInfo(&free_b, &total_b));
+    // the allocation-free verifier's static scratch and kernels are loaded
+    // now, while allocating is still allowed (bn_noalloc.cu)
+    TRY(bn_internal_noalloc_setup(device));
     auto* c = new bn_ctx();
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
@@ -811,6 +820,12 @@ int bn_ctx_create(int device, uint64_t vram_budget_bytes, bn_ctx** out) {
 
 int bn_ctx_destroy(bn_ctx* ctx) {
     delete ctx;
+    return BN_OK;
+}
+
+int bn_debug_plant_draw_hit(bn_ctx* ctx, int on) {
+    if (!ctx) return fail(BN_EINVAL, "null ctx");
+    ctx->debug_draw_hit = on ? 1 : 0;
     return BN_OK;
 }
 
@@ -1055,7 +1070,10 @@ int bn_plan_profile_read(bn_plan* p, float* ms, uint32_t cap, uint32_t* n) {
 int bn_plan_status(bn_plan* p, uint32_t* device_flags) {
     if (!p || !device_flags) return fail(BN_EINVAL, "null argument");
     if (p->block) return block_plan_status(p->block, device_flags);
-    CU(cudaMemcpy(device_flags, p->ws.at<char>() + p->o.err, 4, cudaMemcpyDeviceToHost));
+    uint32_t w[2] = {0, 0};
+    CU(cudaMemcpy(&w[0], p->ws.at<char>() + p->o.err, 4, cudaMemcpyDeviceToHost));
+    CU(cudaMemcpy(&w[1], p->ws.at<char>() + p->o.flags, 4, cudaMemcpyDeviceToHost));
+    *device_flags = w[0] | w[1];
     return BN_OK;
 }
 
@@ -1162,9 +1180,11 @@ static int check_offsets(uint32_t nlist, const uint64_t* off) {
 // Internal hooks for bn_noalloc.cu (not part of the public header).
 int bn_internal_set_error(int code, const char* msg) { return fail(code, "%s", msg); }
 
-int bn_internal_flat_view(const bn_flat* f, int* device, const uint64_t** d_m_enc, uint64_t* rows, int* num_sms) {
+int bn_internal_flat_view(const bn_flat* f, int* device, const uint64_t** d_m_enc, uint64_t* rows, int* num_sms,
+                          int* debug_draw_hit) {
     if (!f) return fail(BN_EINVAL, "null handle");
     *device = f->e.ctx->device;
+    *debug_draw_hit = f->e.ctx->debug_draw_hit;
     *d_m_enc = f->e.c.m_enc.at<uint64_t>();
     *rows = f->m;
     *num_sms = f->e.ctx->num_sms;

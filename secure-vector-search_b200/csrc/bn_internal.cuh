@@ -20,6 +20,7 @@ struct bn_ctx {
     int device = 0;
     int num_sms = 148;
     int engine = BN_ENGINE_TENSOR;  // Protocol 2 engine
+    int debug_draw_hit = 0;         // bn_debug_plant_draw_hit
     uint64_t budget = 0, used = 0, peak = 0;
     std::mutex mu;
 };
@@ -43,6 +44,17 @@ int fail(int code, const char* fmt, ...);
     } while (0)
 
 inline uint64_t align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+
+// Status of a pipeline's device flag word once its stream has drained: a
+// timed-out wait (any bit but DRAW_HIT_P) is BN_ECUDA, a draw that equalled
+// p (and nothing else) BN_EDRAW.
+inline int device_flags_status(uint32_t f) {
+    if (f & ~DRAW_HIT_P) return fail(BN_ECUDA, "a device pipeline wait timed out (flags 0x%x); results discarded", f);
+    if (f & DRAW_HIT_P)
+        return fail(BN_EDRAW, "a Protocol 2 draw equalled p (the reference redraws there, crypto.rs:155-162, shifting "
+                              "every later draw); results discarded");
+    return BN_OK;
+}
 
 
 // Device allocation accounted against the context budget.

@@ -656,6 +656,7 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
     CU(cudaMemcpyAsync(d, h, j.in_end, cudaMemcpyHostToDevice, s));
     uint32_t* err = reinterpret_cast<uint32_t*>(d + j.o_err);
     CU(cudaMemsetAsync(err, 0, 8, s));
+    if (j.trials && e.ctx->debug_draw_hit) launch_or_flag(err, DRAW_HIT_P, s);
     auto U8 = [&](uint64_t o) { return reinterpret_cast<uint8_t*>(d + o); };
     auto U64 = [&](uint64_t o) { return reinterpret_cast<uint64_t*>(d + o); };
     auto U32 = [&](uint64_t o) { return reinterpret_cast<uint32_t*>(d + o); };
@@ -768,7 +769,7 @@ int ivf_block_finish(const IvfBlockJob& j, const PinnedMem& host, uint32_t* ids,
                      int32_t* failed_cluster, int32_t* failed_trial) {
     const char* h = host.at<char>();
     const uint32_t* flags = reinterpret_cast<const uint32_t*>(h + j.o_err);
-    if (flags[0]) return fail(BN_ECUDA, "a device pipeline wait timed out or a draw hit p (flags 0x%x)", flags[0]);
+    TRY(device_flags_status(flags[0]));
     if (flags[1]) return fail(BN_EINVAL, "a T column sum leaves [-128, 127]");
     const uint32_t ks = std::max<uint32_t>(j.k, 1);
     const uint32_t* hid = reinterpret_cast<const uint32_t*>(h + j.o_ids);

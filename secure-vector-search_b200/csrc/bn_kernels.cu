@@ -28,6 +28,8 @@ __device__ __forceinline__ void named_bar(int id, int threads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
 }
 
+__global__ void or_flag_kernel(uint32_t* w, uint32_t bits) { atomicOr(w, bits); }
+
 // ------------------------------------------------------------------ limbs
 __global__ void query_limbs_kernel(const uint64_t* __restrict__ v, uint64_t total, QLimb* __restrict__ out) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -291,7 +293,7 @@ freivalds_kernel(const uint64_t* __restrict__ m_enc, const uint64_t* __restrict_
                     const uint64_t idx = blk * 8 + q;
                     if (idx >= first && idx < first + nt) {
                         uint64_t x = ((uint64_t)w[2 * q] | ((uint64_t)w[2 * q + 1] << 32)) & P;
-                        if (x == P) { atomicOr(flags, 1u); x = 0; }
+                        if (x == P) { atomicOr(flags, DRAW_HIT_P); x = 0; }
                         const uint32_t ii = (uint32_t)(idx - first);
                         Limbs3 b = limbs(x), c = limbs_hi(x);
                         ul[ii][gen_t][0] = b.b0; ul[ii][gen_t][1] = b.b1; ul[ii][gen_t][2] = b.b2;
@@ -1156,6 +1158,22 @@ FreivaldsPlan plan_freivalds(uint64_t max_rows, uint32_t nseg, int num_sms) {
     uint64_t chunks = (max_rows + chunk_rows - 1) / chunk_rows;
     if (chunks < 1) chunks = 1;
     return FreivaldsPlan{(uint32_t)chunks, (uint32_t)chunk_rows};
+}
+
+void launch_or_flag(uint32_t* d_word, uint32_t bits, cudaStream_t s) { or_flag_kernel<<<1, 1, 0, s>>>(d_word, bits); }
+
+cudaError_t preload_freivalds_kernels() {
+    cudaFuncAttributes a;
+    const void* fns[] = {reinterpret_cast<const void*>(freivalds_kernel<24>),
+                         reinterpret_cast<const void*>(freivalds_kernel<8>),
+                         reinterpret_cast<const void*>(freivalds_kernel<4>),
+                         reinterpret_cast<const void*>(freivalds_finish_kernel),
+                         reinterpret_cast<const void*>(or_flag_kernel)};
+    for (const void* f : fns) {
+        const cudaError_t e = cudaFuncGetAttributes(&a, f);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 void launch_freivalds(const uint64_t* d_m_enc, const uint64_t* d_r, const VerifySeg* d_vsegs, uint32_t nseg,

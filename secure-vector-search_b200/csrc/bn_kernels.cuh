@@ -49,9 +49,23 @@ constexpr int SCAN_ROWS = 4;
 
 // Freivalds: per (segment, trial group) the u stream is ChaCha20Rng keyed
 // by v_seed; u_t[i] is draw number t*m_seg + i of that stream (crypto.rs:
-// 1026-1027).  Bit 0 of *flags is set if a draw hit the rejected value p
-// (probability 2^-61 per draw), meaning later draws of the reference
-// stream would be shifted by one.
+// 1026-1027).  DRAW_HIT_P is or-ed into *flags if a draw hit the rejected
+// value p (probability 2^-61 per draw), meaning later draws of the
+// reference stream would be shifted by one (sample_fp redraws,
+// crypto.rs:155-162); the host then fails the call with BN_EDRAW.  The bit
+// is the public BN_STATUS_DRAW_HIT_P and stays clear of the wait-timeout
+// bits (0x1..0x20) and the block path's T-range bit (0x100).
+constexpr uint32_t DRAW_HIT_P = 0x1000u;
+
+// *d_word |= bits on the stream (plants the draw flag for
+// bn_debug_plant_draw_hit).
+void launch_or_flag(uint32_t* d_word, uint32_t bits, cudaStream_t s);
+
+// Loads the kernels launch_freivalds / launch_freivalds_finish use on the
+// current device (CUDA loads modules lazily, on first use, and a load
+// allocates device memory); the allocation-free verifier calls it at
+// context set-up.
+cudaError_t preload_freivalds_kernels();
 struct VerifySeg {
     uint64_t row0;   // first row in m_enc
     uint64_t r0;     // first r value of this segment

@@ -57,7 +57,7 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
                 const uint32_t ii = (uint32_t)(idx - first);
                 uint64_t x = ((uint64_t)w[2 * q] | ((uint64_t)w[2 * q + 1] << 32)) & P;
                 if (ii >= here) x = 0;  // rows past the segment end
-                else if (x == P) { atomicOr(flags, 1u); x = 0; }
+                else if (x == P) { atomicOr(flags, DRAW_HIT_P); x = 0; }
                 us[tl][ug_idx(ii)] = x;
             }
         }
