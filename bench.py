@@ -849,10 +849,12 @@ def run_serving(args, flat, ivf, flat_L, data, dist):
         h, fc, ft = ivf.query(probes[i][None], ienc[i][0][None], ienc[i][1][None], [(ienc[i][2], ienc[i][3])],
                               [iseeds[i]], args.trials, 10)
         ref_i.append((h[0][0], h[0][1], int(ft[0])))
+    qwait = args.serve_queue_wait_ms * 1000
     srv = capi.Server(flat, ivf, max_batch=64, slots=4, mem_budget=24 << 30, max_wait_us=1000, trials=args.trials,
-                      k=10, block_min=2)
+                      k=10, block_min=2, queue_wait_us=qwait)
     out = {"corpora": {"flat_N": flat.m, "ivf_N": int(data["offsets"][-1]), "nlist": int(len(data["sizes"]))},
-           "config": {"max_batch": 64, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 2},
+           "config": {"max_batch": 64, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 2,
+                      "queue_wait_us": qwait},
            "mix": "50% flat / 50% IVF, nprobe uniform in {8, 32, 128}",
            "warmup": "512 requests submitted at once before the timed rates (slots create their plans and "
                      "workspaces), not counted", "rates": {}}
@@ -881,27 +883,35 @@ def run_serving(args, flat, ivf, flat_L, data, dist):
             while time.perf_counter() < due:
                 pass
             i = int(picks[j])
-            if kinds[j]:
-                e = fenc[i]
-                tickets.append(srv.submit_flat(e[0], e[1], e[2], e[3], fseeds[i]))
-            else:
-                e = ienc[i]
-                tickets.append(srv.submit_ivf(probes[i], e[0], e[1], e[2], e[3], iseeds[i]))
+            try:  # refused (BN_EAGAIN) when the queue's expected wait exceeds queue_wait_us
+                if kinds[j]:
+                    e = fenc[i]
+                    tickets.append((j, srv.submit_flat(e[0], e[1], e[2], e[3], fseeds[i])))
+                else:
+                    e = ienc[i]
+                    tickets.append((j, srv.submit_ivf(probes[i], e[0], e[1], e[2], e[3], iseeds[i])))
+            except capi.BnError as err:
+                if err.code != capi.BN_EAGAIN:
+                    raise
         offered = n / (time.perf_counter() - t_start)
         bad = 0
-        for j, t in enumerate(tickets):
+        for j, t in tickets:
             ids, sc, ft, fc, lat = srv.wait(t, 600000)
             ref = ref_f[picks[j]] if kinds[j] else ref_i[picks[j]]
             if not (np.array_equal(ids, ref[0]) and np.array_equal(sc, ref[1]) and ft == ref[2]):
                 bad += 1
         st = srv.stats()
-        out["rates"][str(int(rate))] = {"offered_qps": offered, "requests": n, "served_qps": st["throughput_qps"],
+        out["rates"][str(int(rate))] = {"offered_qps": offered, "requests": n, "admitted": len(tickets),
+                                        "refused": int(st["rejected"]), "served_qps": st["throughput_qps"],
                                         "p50_ms": st["p50_us"] / 1e3, "p99_ms": st["p99_us"] / 1e3,
                                         "max_ms": st["max_us"] / 1e3, "mean_batch": st["mean_batch"],
                                         "block_batches": st["block_batches"],
                                         "peak_workspace_gib": st["peak_workspace_bytes"] / 2**30,
                                         "mismatches_vs_per_query": bad}
     srv.close()
+    ok = [float(r) for r, v in out["rates"].items() if v["p99_ms"] <= 100.0 and v["refused"] == 0]
+    out["max_offered_qps_all_admitted_p99_le_100ms"] = max(ok) if ok else None
+    out["saturated_served_qps"] = max(v["served_qps"] for v in out["rates"].values())
     return out
 
 
@@ -927,6 +937,8 @@ def main():
     ap.add_argument("--ivf-rows", type=int, default=2_000_000, help="IVF corpus rows (0 to skip the IVF legs)")
     ap.add_argument("--serve-rates", default="2000,5000,10000,50000", help="Poisson arrival rates of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=1.5)
+    ap.add_argument("--serve-queue-wait-ms", type=int, default=40,
+                    help="serving admission: refuse a request when the queue's expected wait exceeds this (0: off)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -177,7 +177,7 @@ int bn_plan_enqueue(bn_plan* p, const uint64_t* d_v_enc, const uint64_t* d_g, co
 /* Scan-only enqueue of the same plan: d_r (B x m) = M_enc v_enc. */
 int bn_plan_enqueue_scan(bn_plan* p, const uint64_t* d_v_enc, uint64_t* d_r, void* stream);
 /* Device flags of the last enqueue of this plan (0 = healthy).  Bits
- * 0x1..0x20: a bounded device-side wait timed out; bit 0x1000
+ * 0x1..0x40: a bounded device-side wait timed out; bit 0x1000
  * (BN_STATUS_DRAW_HIT_P): a Protocol 2 draw equalled p (see BN_EDRAW); block
  * plans add 0x100 when a T column sum left [-128, 127].  Any bit set means
  * the outputs must be discarded.  Synchronous: call after the enqueued work
@@ -340,7 +340,17 @@ int bn_ivf_verify_block(bn_ivf* h, uint32_t B, uint32_t nprobe, const uint32_t* 
  * waited max_wait_us.  Admission is by device memory: a batch's workspace
  * plus the workspaces the other slots hold must fit in mem_budget (0 = no
  * limit beyond the context budget); a batch is cut shorter to fit, and a
- * request that cannot fit alone fails with BN_EBUDGET. */
+ * request that cannot fit alone fails with BN_EBUDGET.  Admission is also
+ * by queue: submit returns BN_EAGAIN (nothing queued) when max_queue requests
+ * are waiting, or when the queue's expected wait (waiting requests over the
+ * recent completion rate) exceeds queue_wait_us, so that the latency of
+ * admitted requests stays bounded past saturation.
+ * Hits (ids, scores) equal bn_flat_query / bn_ivf_query on the same inputs,
+ * alone or in any mix.  Protocol 2 of a per-query batch uses each request's
+ * own seed; a block batch (block_min) is verified per block with one seed
+ * derived from all its members' seeds (domain_separate of their XOR with the
+ * tag "serve-block"), so an honest response is accepted in any mix, while
+ * the first failing trial of a rejected one depends on the batch. */
 typedef struct bn_server bn_server;
 #define BN_SERVER_FLAT 0
 #define BN_SERVER_IVF 1
@@ -354,8 +364,10 @@ typedef struct bn_server_config {
     uint32_t block_min;   /* batches of >= block_min requests run as block scoring: flat ones as
                              bn_flat_block_plan (one pass over the corpus for the batch), IVF ones as
                              bn_ivf_query_block (every probed list read once per batch); Protocol 2 per
-                             block (and list) with the first request's seed; 0 = every query verified
-                             with its own seed */
+                             block (and list) with the batch seed; 0 = every query verified with its
+                             own seed */
+    uint32_t max_queue;     /* waiting requests at which submit returns BN_EAGAIN (0: unbounded) */
+    uint32_t queue_wait_us; /* expected queue wait at which submit returns BN_EAGAIN (0: off) */
 } bn_server_config;
 typedef struct bn_server_stats_t {
     uint64_t submitted, completed, batches;
@@ -364,6 +376,7 @@ typedef struct bn_server_stats_t {
     double throughput_qps;             /* completed / (last completion - first submit) */
     uint64_t peak_workspace_bytes;
     uint64_t block_batches;            /* batches (flat or IVF) that ran as block scoring */
+    uint64_t rejected;                 /* submits refused with BN_EAGAIN (queue admission) */
 } bn_server_stats_t;
 /* flat and/or ivf (nullable, not both), with client state, in one context. */
 int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn_server** out);
@@ -391,6 +404,16 @@ int bn_server_destroy(bn_server* s);
  * bn_plan_status, failed_trial = -2 from bn_flat_verify_noalloc), so that a
  * caller can exercise its handling of that 2^-61 event. */
 int bn_debug_plant_draw_hit(bn_ctx* ctx, int on);
+/* No counterpart in the reference.  Every device-side pipeline wait (an
+ * mbarrier wait between the copy, MMA and drain roles of the scan, fused
+ * Protocol 2 and block GEMM kernels) gives up after about a second, records
+ * the event in the launch's status word and winds the kernel down, so a lost
+ * completion cannot hang the GPU.  This sets that limit, in clock cycles,
+ * for later launches on this context's handles (0 restores the default), so
+ * that a test can make the waits run out: the call then returns BN_ECUDA and
+ * bn_plan_status reports the bits.  The wind-down waits for a CTA's own
+ * copies and MMAs keep the full limit. */
+int bn_debug_set_wait_limit(bn_ctx* ctx, uint64_t cycles);
 
 /* ---------------------------------------------------------------- keygen
  * encrypt_cluster (crypto.rs:405-478) on the device with host in/out:

@@ -44,13 +44,14 @@ class SparseCsr(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("max_batch", u32), ("slots", u32), ("mem_budget", u64), ("max_wait_us", u32), ("trials", u32),
-                ("k", u32), ("block_min", u32)]
+                ("k", u32), ("block_min", u32), ("max_queue", u32), ("queue_wait_us", u32)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [("submitted", u64), ("completed", u64), ("batches", u64), ("mean_batch", C.c_double),
                 ("p50_us", C.c_double), ("p99_us", C.c_double), ("max_us", C.c_double),
-                ("throughput_qps", C.c_double), ("peak_workspace_bytes", u64), ("block_batches", u64)]
+                ("throughput_qps", C.c_double), ("peak_workspace_bytes", u64), ("block_batches", u64),
+                ("rejected", u64)]
 
 
 _SIGS = {
@@ -62,6 +63,7 @@ _SIGS = {
     "bn_ctx_memory": (C.c_int, [vp, vp, vp, vp]),
     "bn_ctx_set_engine": (C.c_int, [vp, C.c_int]),
     "bn_debug_plant_draw_hit": (C.c_int, [vp, C.c_int]),
+    "bn_debug_set_wait_limit": (C.c_int, [vp, u64]),
     "bn_flat_build": (C.c_int, [vp, vp, vp, vp, u64, u32, u32, vp]),
     "bn_flat_attach_client": (C.c_int, [vp, vp, vp, SparseCsr]),
     "bn_flat_build_from_plain": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, vp]),
@@ -170,6 +172,10 @@ class Context:
     def plant_draw_hit(self, on: bool):
         """Testing hook: Protocol 2 runs behave as if a draw had equalled p."""
         check(lib.bn_debug_plant_draw_hit(self.h, 1 if on else 0))
+
+    def set_wait_limit(self, cycles: int):
+        """Testing hook: pipeline waits of later launches give up after `cycles` (0 = default)."""
+        check(lib.bn_debug_set_wait_limit(self.h, cycles))
 
     def memory(self):
         b, u, p = u64(), u64(), u64()
@@ -550,9 +556,9 @@ class Server:
     """bn_server: continuous batching of flat and IVF queries over resident corpora."""
 
     def __init__(self, flat=None, ivf=None, max_batch=64, slots=4, mem_budget=0, max_wait_us=200, trials=20, k=10,
-                 block_min=0):
+                 block_min=0, max_queue=0, queue_wait_us=0):
         self.flat, self.ivf, self.k = flat, ivf, k
-        cfg = ServerConfig(max_batch, slots, mem_budget, max_wait_us, trials, k, block_min)
+        cfg = ServerConfig(max_batch, slots, mem_budget, max_wait_us, trials, k, block_min, max_queue, queue_wait_us)
         out = vp()
         check(lib.bn_server_create(flat.h if flat else None, ivf.h if ivf else None, C.byref(cfg), C.byref(out)))
         self.h = out

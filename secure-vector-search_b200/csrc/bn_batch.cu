@@ -100,6 +100,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
     const uint32_t sbase = (su32(bg_dyn) + 1023u) & ~1023u;
     uint8_t* sptr = bg_dyn + (sbase - su32(bg_dyn));
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long wait_limit = p.wait_cycles > 0 ? p.wait_cycles : TC_WAIT_CYCLES;
     constexpr uint32_t A_BYTES = BG_AROWS * BG_KSTEP;
     const uint32_t w_bytes = p.w_tile * BG_KSTEP;
     const uint32_t ksub = p.ksteps2 ? 2u : 1u, kstage = ksub * BG_KSTEP;  // K steps / bytes per stage
@@ -151,7 +152,8 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
             // W tiles of the tile and are reloaded for the next one once the
             // MMAs of its last item have read them)
             uint64_t it = 0;
-            uint32_t t_last = 0xffffffffu;
+            // A loads issued last: slots [0, a_n) for tile a_t, the rest for a_t - 1
+            uint32_t a_t = 0xffffffffu, a_n = 0;
             bool stop = false;
             for (ItemCursor cs(p, items); !stop && cs.have_cur; cs.advance()) {
                 const ItemIdx& ix = cs.cur;
@@ -163,7 +165,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     const uint32_t ks = (k - k0) / BG_KSTEP;
                     if (load_a) {
                         for (uint32_t sub = 0; sub < ksub && !stop; ++sub) {
-                            if (t > 0 && !bar_wait(&aempty_b[ks + sub], (t - 1) & 1)) {
+                            if (t > 0 && !bar_wait(&aempty_b[ks + sub], (t - 1) & 1, wait_limit)) {
                                 abort_s = 1;
                                 atomicOr(err, 4u);
                                 stop = true;
@@ -172,12 +174,13 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                             const uint32_t kq = k + sub * BG_KSTEP;
                             bar_expect_tx(&afull_b[ks + sub], A_BYTES);
                             tma_2d(sptr + (ks + sub) * A_BYTES, &tmap_a, a_x(kq), a_row(ix, kq), &afull_b[ks + sub]);
+                            a_t = t;
+                            a_n = ks + sub + 1;
                         }
                         if (stop) break;
-                        t_last = t;
                     }
                     const uint32_t st = (uint32_t)(it % stages);
-                    if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1))) {
+                    if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1), wait_limit)) {
                         abort_s = 1;
                         atomicOr(err, 4u);
                         stop = true;
@@ -205,8 +208,11 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
             // no copy may still be landing in shared memory when the CTA exits
             for (uint64_t j = it > stages ? it - stages : 0; j < it; ++j)
                 bar_wait(&full_b[j % stages], (uint32_t)((j / stages) & 1));
-            if (t_last != 0xffffffffu)
-                for (uint32_t k = 0; k < a_slots; ++k) bar_wait(&afull_b[k], t_last & 1);
+            if (a_t != 0xffffffffu)
+                for (uint32_t k = 0; k < a_slots; ++k) {
+                    const uint32_t tk = k < a_n ? a_t : a_t - 1;  // the last tile slot k was loaded for
+                    if (k < a_n || a_t > 0) bar_wait(&afull_b[k], tk & 1);
+                }
         }
     } else if (warp == 1) {
         if (lane == 0) {  // ---------------------------------------------- MMA issuer
@@ -222,7 +228,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 const uint32_t t = a_slots ? j / p.w_tiles : 0;
                 const bool last_of_a = a_slots && ix.tw == p.w_tiles - 1;
                 const uint32_t buf = (uint32_t)(n & 1), use = (uint32_t)(n >> 1);
-                if (use > 0 && !bar_wait(&acce_b[buf], (use - 1) & 1)) {
+                if (use > 0 && !bar_wait(&acce_b[buf], (use - 1) & 1, wait_limit)) {
                     abort_s = 1;
                     atomicOr(err, 8u);
                     break;
@@ -235,8 +241,8 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                     const uint32_t st = (uint32_t)(it % stages);
                     const uint32_t ks = (k - k0) / BG_KSTEP;
                     bool a_ok = true;
-                    for (uint32_t sub = 0; a_slots && sub < ksub; ++sub) a_ok = a_ok && bar_wait(&afull_b[ks + sub], t & 1);
-                    if (!a_ok || !bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
+                    for (uint32_t sub = 0; a_slots && sub < ksub; ++sub) a_ok = a_ok && bar_wait(&afull_b[ks + sub], t & 1, wait_limit);
+                    if (!a_ok || !bar_wait(&full_b[st], (uint32_t)((it / stages) & 1), wait_limit) || abort_s) {
                         abort_s = 1;
                         atomicOr(err, 8u);
                         stop = true;
@@ -261,7 +267,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
                 mma_commit(&accf_b[buf]);  // accumulator complete for this item
             }
             mma_commit(&done_b);
-            bar_wait(&done_b, 0);  // every issued MMA has finished before TMEM is freed
+            if (!bar_wait(&done_b, 0)) atomicOr(err, 64u);  // every issued MMA has finished before TMEM is freed
         }
     } else {
         // -------------------------------------------------------------- epilogue
@@ -291,7 +297,7 @@ bgemm_kernel(const __grid_constant__ CUtensorMap tmap_a, const __grid_constant__
 #pragma unroll
                 for (int h = 0; h < 2; ++h) ob_r[k][h] = cr < p.w_tile ? obase(ybase + cr / 8 + h) : 0;
             }
-            const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b[buf], use & 1));  // warp-uniform
+            const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b[buf], use & 1, wait_limit));  // warp-uniform
             if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
             if (__any_sync(FULLMASK, !ok || abort_s)) break;
             tc_after();

@@ -72,11 +72,13 @@ struct BgParams {
     const BgItem* item_tab;
     uint32_t n_items;
     const uint64_t* pair_base;  // grouped outputs: out[pair_base[y] + x]
+    long long wait_cycles;      // limit of the pipeline waits (0 = about a second; shorter only in tests)
 };
 
 // tmap_a: A bytes {k_bytes, A rows}, box {128, 128}; tmap_w: W bytes
 // {k_bytes, W rows}, box {128, w_tile}; both 128-byte swizzle.  stages in
-// [2, BG_MAX_STAGES].  *err: bit 2/3/4 set when a bounded wait timed out.
+// [2, BG_MAX_STAGES].  *err: bit 2/3/4 set when a bounded wait timed out,
+// bit 64 when the wind-down wait for the CTA's own MMAs did.
 // A-resident mode needs k_panel == k_bytes <= BG_MAX_ASLOTS * 128 and
 // bgemm_smem_bytes(p, stages) <= BG_MAX_SMEM.
 // With p.ksteps2: tmap_a2 = the K-blocked A with 256-row boxes (two K steps

@@ -492,7 +492,8 @@ static void enqueue_verify(BlockPlan& b, const uint64_t* d_v, const uint8_t* d_s
         const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, b.trials - t0);
         launch_tc_ugen(vseg, blocks, b.nblocks, reinterpret_cast<const ChaChaKey*>(d_seed), nullptr, t0, tc, b.n_rows,
                        ub, nullptr, b.trials, err, s, b.npad);
-        launch_tc_freivalds(c.tmap_m, b.tm_ub, panels, b.npanels, t0, tc, b.n_rows, b.trials, zpart, err, sms, s, 1);
+        launch_tc_freivalds(c.tmap_m, b.tm_ub, panels, b.npanels, t0, tc, b.n_rows, b.trials, zpart, err, sms, s, 1,
+                            b.h->e.ctx->debug_wait_cycles);
         launch_zsum(zpart, b.npanels, t0, tc, b.trials, z, s);
         BgParams p{};
         p.mode = BG_PLANAR;
@@ -507,6 +508,7 @@ static void enqueue_verify(BlockPlan& b, const uint64_t* d_v, const uint8_t* d_s
         p.out_ld = b.B;
         p.out_pstride = (uint64_t)b.trials * b.B;
         p.order_a_fast = 1;
+        p.wait_cycles = b.h->e.ctx->debug_wait_cycles;
         launch_bgemm(b.tm_rp, b.tm_ub, p, stages_u(b.n_rows), sms, err, s);
     }
     uint64_t* zv = reinterpret_cast<uint64_t*>(d + b.o_zv);
@@ -542,6 +544,7 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     BgParams p = g1_params(b, c);
     p.out = r;
     p.planar_out = rp;
+    p.wait_cycles = b.h->e.ctx->debug_wait_cycles;
     launch_bgemm(c.tmap_mp, b.tm_vp, p, b.stages, sms, err, s, &c.tmap_mp2, &b.tm_vp2);
     // G2: f2 = -(AL g + H x)   (K = 2 n1 bytes per plane row: A tiles stay resident)
     p.k_bytes = c.k_alh;
@@ -567,6 +570,7 @@ int block_enqueue(BlockPlan& b, const uint64_t* d_v, const uint64_t* d_g, const 
     q.order_a_fast = (int)b.order;
     q.a_blocked = 1;
     q.ksteps2 = (int)b.ks2;
+    q.wait_cycles = p.wait_cycles;
     launch_bgemm(c.tmap_ms, b.tm_tv, q, stages_for(q), sms, err, s, &c.tmap_ms2, &b.tm_tv2);
     // Mv = r + f2 - f3 (written over f3 when asked for), fp_to_signed, top-k
     if (b.k || want_mv) {

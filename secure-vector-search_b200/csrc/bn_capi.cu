@@ -380,7 +380,8 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
                 launch_query_wimg(in.v, z.B, sc.wimg, s);
                 if (prof0) CU(cudaEventRecord(prof0, s));
                 launch_tc_fused(c.tmap_m, m.maps->u[ps], m.maps->w, m.tc_panels, m.npanels, m.vsegs, tc, nr,
-                                z.trials, sc.z_part, sc.r_part, z.total_out, sc.err, ctx->num_sms, s);
+                                z.trials, sc.z_part, sc.r_part, z.total_out, sc.err, ctx->num_sms, s,
+                                ctx->debug_wait_cycles);
                 if (prof1) CU(cudaEventRecord(prof1, s));
                 launch_tc_rreduce(m.vsegs, m.tc_blocks, m.nblocks, sc.r_part, z.total_out, tc_groups(nr), sc.u_buf, tc,
                                   nr, z.trials, sc.r, sc.ur_part, s);
@@ -388,7 +389,7 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
                 launch_tc_ugen(m.vsegs, m.tc_blocks, m.nblocks, keys, sc.r, t0, tc, nr, sc.u_buf, sc.ur_part, z.trials,
                                sc.flags, s);
                 launch_tc_freivalds(c.tmap_m, m.maps->u[ps], m.tc_panels, m.npanels, t0, tc, nr, z.trials, sc.z_part,
-                                    sc.err, ctx->num_sms, s);
+                                    sc.err, ctx->num_sms, s, 0, ctx->debug_wait_cycles);
             }
         }
         launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, in.v, m.vsegs, m.nvseg, z.trials, sc.ur,
@@ -396,7 +397,7 @@ int enqueue_pipeline(bn_ctx* ctx, const Corpus& c, const Sizes& z, const Meta& m
     } else {
         if (prof0) CU(cudaEventRecord(prof0, s));
         launch_scan(c.m_enc.at<uint64_t>(), sc.limbs, m.segs, m.seg_blk, m.nseg, m.total_blocks, sc.r, ctx->num_sms,
-                    sc.err, s);
+                    sc.err, s, ctx->debug_wait_cycles);
         if (prof1) CU(cudaEventRecord(prof1, s));
         if (z.trials) {
             launch_freivalds(c.m_enc.at<uint64_t>(), sc.r, m.vsegs, m.nvseg, keys, z.trials, z.fp, sc.z_part, sc.ur_part,
@@ -662,7 +663,7 @@ int run_verify(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* r, const
             launch_tc_ugen(m.vsegs, m.tc_blocks, m.nblocks, keys, sc.r, t0, tc, nr, sc.u_buf, sc.ur_part, trials,
                            sc.flags, e.stream);
             launch_tc_freivalds(e.c.tmap_m, maps.u[ps], m.tc_panels, m.npanels, t0, tc, nr, trials, sc.z_part, sc.err,
-                                e.ctx->num_sms, e.stream);
+                                e.ctx->num_sms, e.stream, 0, e.ctx->debug_wait_cycles);
         }
         launch_tc_finish(sc.z_part, sc.ur_part, m.seg_panel0, m.seg_block0, dv, m.vsegs, 1, trials, sc.ur, sc.zv,
                          sc.zv_chunks, dfail, e.stream);
@@ -710,7 +711,7 @@ int run_scan(Engine& e, uint64_t row0, uint64_t rows, const uint64_t* v_encs, ui
     launch_query_limbs(reinterpret_cast<uint64_t*>(d + o_v), B, reinterpret_cast<QLimb*>(d + o_l), e.stream);
     launch_scan(e.c.m_enc.at<uint64_t>(), reinterpret_cast<QLimb*>(d + o_l), reinterpret_cast<ScanSeg*>(d + o_s),
                 reinterpret_cast<uint64_t*>(d + o_b), B, hm.seg_blk.back(), reinterpret_cast<uint64_t*>(d + o_r),
-                e.ctx->num_sms, reinterpret_cast<uint32_t*>(d + o_e), e.stream);
+                e.ctx->num_sms, reinterpret_cast<uint32_t*>(d + o_e), e.stream, e.ctx->debug_wait_cycles);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(r, d + o_r, (uint64_t)B * rows * 8, cudaMemcpyDeviceToHost, e.stream));
     uint32_t ev = 0;
@@ -826,6 +827,13 @@ int bn_ctx_destroy(bn_ctx* ctx) {
 int bn_debug_plant_draw_hit(bn_ctx* ctx, int on) {
     if (!ctx) return fail(BN_EINVAL, "null ctx");
     ctx->debug_draw_hit = on ? 1 : 0;
+    return BN_OK;
+}
+
+int bn_debug_set_wait_limit(bn_ctx* ctx, uint64_t cycles) {
+    if (!ctx) return fail(BN_EINVAL, "null ctx");
+    if (cycles > 4000000000ull) return fail(BN_EINVAL, "wait limit %llu cycles exceeds the default", (unsigned long long)cycles);
+    ctx->debug_wait_cycles = (long long)cycles;
     return BN_OK;
 }
 

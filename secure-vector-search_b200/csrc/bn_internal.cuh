@@ -21,6 +21,7 @@ struct bn_ctx {
     int num_sms = 148;
     int engine = BN_ENGINE_TENSOR;  // Protocol 2 engine
     int debug_draw_hit = 0;         // bn_debug_plant_draw_hit
+    long long debug_wait_cycles = 0;  // bn_debug_set_wait_limit (0 = the kernels' ~1 s default)
     uint64_t budget = 0, used = 0, peak = 0;
     std::mutex mu;
 };

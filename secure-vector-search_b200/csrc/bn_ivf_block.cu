@@ -699,6 +699,7 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             p.pair_base = U64(j.o_base);
             p.a_blocked = 1;
             p.ksteps2 = 1;  // two K steps per stage: half the producer / MMA handoffs per item
+            p.wait_cycles = e.ctx->debug_wait_cycles;
             launch_bgemm(c.tmap_mp, j.tm_wv, p, j.st_g1, sms, err, s, &c.tmap_mp2, &j.tm_wv2);
             mark(2);
             p.k_bytes = p.k_panel = c.k_alh;
@@ -732,9 +733,9 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, j.trials - t0);
             launch_tc_ugen(vsegs, blocks, j.NB, key, nullptr, t0, tc, j.n_rows, U8(j.o_ub), nullptr, j.trials, err, s);
             launch_tc_freivalds(c.tmap_m, j.tm_u, panels, j.NP_big, t0, tc, j.n_rows, j.trials, U64(j.o_zpart), err,
-                                sms, s);
+                                sms, s, 0, e.ctx->debug_wait_cycles);
             launch_tc_freivalds_small(c.tmap_m, j.tm_u, panels, j.NP_big, j.NP - j.NP_big, t0, tc, j.n_rows, j.trials,
-                                      U64(j.o_zpart), err, sms, s);
+                                      U64(j.o_zpart), err, sms, s, e.ctx->debug_wait_cycles);
             ur_lists_kernel<<<j.NUR, UR_WARPS * 32, 8 * tc * TC_ROWS, s>>>(
                 reinterpret_cast<const IvUrTask*>(d + j.o_urtasks), dpairs, U32(j.o_lmi), U8(j.o_ub), j.n_rows, t0, tc,
                 j.trials, U64(j.o_r), U64(j.o_urpart));

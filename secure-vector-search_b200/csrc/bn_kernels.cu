@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
+
 #include "bn_kernels.cuh"
 
 namespace bn {
@@ -80,11 +82,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// Bounded wait: true when the phase with `parity` completed.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait: true when the phase with `parity` completed within `limit`
+// cycles (pipeline waits take the kernel's wait_limit argument; the drain of
+// the CTA's own copies keeps the full limit).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = WAIT_CYCLES) {
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > WAIT_CYCLES) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -92,6 +96,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// L2 prefetch of a contiguous range (address and size multiples of 16 bytes);
+// nothing is written to shared memory and nothing has to be waited for.
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     asm volatile(
@@ -118,7 +127,7 @@ __device__ __forceinline__ ScanBlock scan_block(const ScanSeg* __restrict__ segs
 __global__ void __launch_bounds__(TS_THREADS, 1)
 scan_tma_kernel(const uint64_t* __restrict__ m_enc, const QLimb* __restrict__ qlimbs, const ScanSeg* __restrict__ segs,
                 const uint64_t* __restrict__ seg_blk, uint32_t nseg, uint64_t total_blocks, uint64_t* __restrict__ r,
-                uint32_t* __restrict__ err) {
+                uint32_t* __restrict__ err, long long wait_limit) {
     extern __shared__ __align__(1024) unsigned char ts_smem[];
     uint4* stage_base = reinterpret_cast<uint4*>(ts_smem);
     __shared__ uint64_t full_bar[TS_STAGES], empty_bar[TS_STAGES];
@@ -145,7 +154,7 @@ scan_tma_kernel(const uint64_t* __restrict__ m_enc, const QLimb* __restrict__ ql
             uint64_t i = 0;
             for (; i < nblk; ++i) {
                 const int s = (int)(i % TS_STAGES);
-                if (i >= TS_STAGES && !mbar_wait(&empty_bar[s], (uint32_t)(((i / TS_STAGES) - 1) & 1))) {
+                if (i >= TS_STAGES && !mbar_wait(&empty_bar[s], (uint32_t)(((i / TS_STAGES) - 1) & 1), wait_limit)) {
                     abort_flag = 1;
                     atomicOr(err, 1u);
                     break;
@@ -184,7 +193,7 @@ scan_tma_kernel(const uint64_t* __restrict__ m_enc, const QLimb* __restrict__ ql
                     c0[2 * k + e] = q.c0; c1[2 * k + e] = q.c1; c2[2 * k + e] = q.c2;
                 }
         }
-        const bool ok = mbar_wait(&full_bar[s], (uint32_t)((i / TS_STAGES) & 1));
+        const bool ok = mbar_wait(&full_bar[s], (uint32_t)((i / TS_STAGES) & 1), wait_limit);
         if (!ok) { abort_flag = 1; atomicOr(err, 2u); }
         uint64_t acc[SCAN_ROWS][3];
         const uint4* base = stage_base + (uint64_t)s * (TS_STAGE_BYTES / 16) + wq * 128 + lane;
@@ -765,7 +774,7 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
                    const uint64_t* __restrict__ vv, const uint64_t* __restrict__ gg, const uint64_t* __restrict__ xx,
                    const uint32_t* __restrict__ t_ent, const uint32_t* __restrict__ t_nnz, uint32_t k, TopkScratch ts,
                    uint64_t* __restrict__ mv_out, uint32_t* __restrict__ out_ids, int64_t* __restrict__ out_scores,
-                   uint32_t* __restrict__ out_n, uint32_t nq) {
+                   uint32_t* __restrict__ out_n, uint32_t nq, uint32_t prefetch) {
     uint32_t lo = 0, hi = nq;  // the query owning this CTA: last one with cta0 <= blockIdx.x
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
@@ -820,6 +829,13 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
             }
             const ScanSeg sg = segs[sa];
             const uint64_t blk = (sg.row0 >> 5) + (gu - seg_unit[sa]);
+            if (prefetch && lane == 0) {
+                // the unit's block-contiguous runs into L2 at once: its [AL | H]
+                // block (2 n1 x 32 words) and its S slice
+                bulk_prefetch_l2(dc.alh_b + blk * (2ull * n1) * 32, 2u * n1 * 32u * 8u);
+                const uint32_t w = dc.s_w[blk];
+                if (w) bulk_prefetch_l2(dc.s_ell + dc.s_off[blk], 64u * w);
+            }
             const uint64_t gr = blk * 32 + lane;
             valid = gr >= sg.row0 && gr < sg.row0 + sg.rows;
             const uint64_t ridx = sg.out0 + (gr - sg.row0);
@@ -1135,16 +1151,14 @@ void launch_query_limbs(const uint64_t* d_v, uint32_t nq, QLimb* d_limbs, cudaSt
 }
 
 void launch_scan(const uint64_t* d_m_enc, const QLimb* d_limbs, const ScanSeg* d_segs, const uint64_t* d_seg_blk,
-                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, uint32_t* d_err, cudaStream_t s) {
+                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, uint32_t* d_err, cudaStream_t s,
+                 long long wait_cycles) {
     if (total_blocks == 0) return;
-    static bool attr_set = false;
     const int smem = TS_STAGES * TS_STAGE_BYTES;
-    if (!attr_set) {
-        cudaFuncSetAttribute(scan_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr_set = true;
-    }
+    cudaFuncSetAttribute(scan_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);  // per device
     unsigned grid = (unsigned)(total_blocks < (uint64_t)num_sms ? total_blocks : (uint64_t)num_sms);
-    scan_tma_kernel<<<grid, TS_THREADS, smem, s>>>(d_m_enc, d_limbs, d_segs, d_seg_blk, nseg, total_blocks, d_r, d_err);
+    scan_tma_kernel<<<grid, TS_THREADS, smem, s>>>(d_m_enc, d_limbs, d_segs, d_seg_blk, nseg, total_blocks, d_r, d_err,
+                                                   wait_cycles > 0 ? wait_cycles : WAIT_CYCLES);
 }
 
 FreivaldsPlan plan_freivalds(uint64_t max_rows, uint32_t nseg, int num_sms) {
@@ -1232,15 +1246,13 @@ void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanS
                         uint64_t* d_mv_out, uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n,
                         cudaStream_t s) {
     if (!nq) return;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(decode_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 2 * 512 * 16);
-        attr_set = true;
-    }
+    cudaFuncSetAttribute(decode_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 2 * 512 * 16);  // per device
+    const char* pf_env = getenv("BN_DECODE_PREFETCH");
+    const uint32_t pf = pf_env ? (uint32_t)atoi(pf_env) : 0u;
     cudaMemsetAsync(scratch.done, 0, (uint64_t)nq * 4, s);
     decode_topk_kernel<<<total_ctas, DT_THREADS, 2 * 2 * dc.n1 * 16, s>>>(d_r, dc, d_segs, d_seg_unit, d_q, d_v, d_g,
                                                                          d_x, d_t, d_t_nnz, k, scratch, d_mv_out,
-                                                                         d_out_ids, d_out_scores, d_out_n, nq);
+                                                                         d_out_ids, d_out_scores, d_out_n, nq, pf);
 }
 
 void launch_topk_rows(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_c, uint64_t ld, uint64_t rows,

@@ -49,12 +49,20 @@ constexpr int SCAN_ROWS = 4;
 
 // Freivalds: per (segment, trial group) the u stream is ChaCha20Rng keyed
 // by v_seed; u_t[i] is draw number t*m_seg + i of that stream (crypto.rs:
-// 1026-1027).  DRAW_HIT_P is or-ed into *flags if a draw hit the rejected
+// 1026-1027).
+struct VerifySeg {
+    uint64_t row0;   // first row in m_enc
+    uint64_t r0;     // first r value of this segment
+    uint32_t rows;   // m of the list / flat corpus
+    uint32_t query;  // index into v_enc / keys arrays
+};
+
+// DRAW_HIT_P is or-ed into a Protocol 2 kernel's flag word if a draw hit the rejected
 // value p (probability 2^-61 per draw), meaning later draws of the
 // reference stream would be shifted by one (sample_fp redraws,
 // crypto.rs:155-162); the host then fails the call with BN_EDRAW.  The bit
 // is the public BN_STATUS_DRAW_HIT_P and stays clear of the wait-timeout
-// bits (0x1..0x20) and the block path's T-range bit (0x100).
+// bits (0x1..0x40) and the block path's T-range bit (0x100).
 constexpr uint32_t DRAW_HIT_P = 0x1000u;
 
 // *d_word |= bits on the stream (plants the draw flag for
@@ -66,12 +74,6 @@ void launch_or_flag(uint32_t* d_word, uint32_t bits, cudaStream_t s);
 // allocates device memory); the allocation-free verifier calls it at
 // context set-up.
 cudaError_t preload_freivalds_kernels();
-struct VerifySeg {
-    uint64_t row0;   // first row in m_enc
-    uint64_t r0;     // first r value of this segment
-    uint32_t rows;   // m of the list / flat corpus
-    uint32_t query;  // index into v_enc / keys arrays
-};
 
 void launch_query_limbs(const uint64_t* d_v, uint32_t nq, QLimb* d_limbs, cudaStream_t s);
 
@@ -79,8 +81,11 @@ void launch_query_limbs(const uint64_t* d_v, uint32_t nq, QLimb* d_limbs, cudaSt
 // seg_blk: exclusive prefix sum over ceil(rows / SCAN_ROWS), nseg + 1 entries.
 // d_err (device u32): bit 0/1 set if a pipeline wait timed out (the scan
 // result is then invalid); the kernel never waits without a bound.
+// wait_cycles: limit of the pipeline waits (0 = about a second; shorter only
+// to test the timeout path).
 void launch_scan(const uint64_t* d_m_enc, const QLimb* d_limbs, const ScanSeg* d_segs, const uint64_t* d_seg_blk,
-                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, uint32_t* d_err, cudaStream_t s);
+                 uint32_t nseg, uint64_t total_blocks, uint64_t* d_r, int num_sms, uint32_t* d_err, cudaStream_t s,
+                 long long wait_cycles = 0);
 
 // Freivalds partial sums for one segment list.  z_part: [nseg][chunks][T][1024],
 // ur_part: [nseg][chunks][T].  chunk_rows: rows per chunk (multiple of 32).

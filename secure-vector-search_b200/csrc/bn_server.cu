@@ -14,8 +14,13 @@
 //     layout for exactly those requests) must fit in mem_budget together with
 //     the workspaces the other slots hold; otherwise it is cut shorter or waits
 //     for a slot to drain (idle slots give their memory back);
-//   - each query's result depends only on its own inputs (its own segments,
-//     seed, decode and top-k), so it is the same alone and in any mix.
+//   - admission is also by queue: a submit is refused with BN_EAGAIN when
+//     max_queue requests wait, or when the expected wait (waiting requests
+//     over the completion rate of the recent batches) exceeds queue_wait_us;
+//   - each query's hits depend only on its own inputs (its own segments,
+//     decode and top-k), so they are the same alone and in any mix; a
+//     per-query batch verifies each query with its own seed, a block batch
+//     with one seed derived from all its members' seeds.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,6 +32,7 @@
 #include <thread>
 #include <unordered_map>
 
+#include "bn_host.h"
 #include "bn_internal.cuh"
 
 using namespace bn;
@@ -98,6 +104,9 @@ struct bn_server {
     bool ivf_block_off = false;  // the same for the IVF corpus
     std::vector<double> lat_us;
     Clock::time_point t_first{}, t_last{};
+    uint64_t rejected = 0;
+    // completion times and sizes of the recent batches (queue admission)
+    std::deque<std::pair<Clock::time_point, uint32_t>> recent;
 };
 
 namespace {
@@ -178,6 +187,27 @@ void complete(bn_server* s, std::vector<Request>& reqs, const std::vector<Result
     }
     s->completed += reqs.size();
     s->t_last = now;
+    s->recent.emplace_back(now, (uint32_t)reqs.size());
+    while (s->recent.size() > 32) s->recent.pop_front();
+}
+
+// Completion rate of the recent batches (queries per second; 0 = unknown).
+double recent_rate(const bn_server* s) {
+    if (s->recent.size() < 4) return 0.0;
+    uint64_t n = 0;
+    for (size_t i = 1; i < s->recent.size(); ++i) n += s->recent[i].second;
+    const double span = std::chrono::duration<double>(s->recent.back().first - s->recent.front().first).count();
+    return span > 0 ? (double)n / span : 0.0;
+}
+
+// The Protocol 2 seed of a block batch: domain_separate of the XOR of its
+// members' seeds, so every member's seed takes part and the seed of the batch
+// is a function of its members alone.
+void block_seed(const std::vector<uint8_t>& seeds, uint32_t B, uint8_t out[32]) {
+    uint8_t x[32] = {0};
+    for (uint32_t b = 0; b < B; ++b)
+        for (int i = 0; i < 32; ++i) x[i] ^= seeds[(uint64_t)b * 32 + i];
+    bn_host_domain_separate(x, "serve-block", out);
 }
 
 // Reads a finished slot's outputs (called with s->mu held).
@@ -246,16 +276,18 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
     const uint32_t bucket = kind == BN_SERVER_FLAT ? block_bucket(s, B) : 0;
     sl.block_run = false;
     sl.ivf_block_run = false;
+    uint8_t bseed[32];
+    block_seed(seeds, B, bseed);
     if (kind == BN_SERVER_IVF && ivf_block(s, B)) {
         // IVF block scoring: the batch's (query, list) pairs grouped by list,
         // every probed list read once; Protocol 2 per block and list with the
-        // first request's seed
+        // batch seed
         if (!sl.ivj) sl.ivj = ivf_block_job_new();
         Engine& e = s->ivf->e;
         rc = ivf_block_plan_reqs(s, sl.reqs.begin(), B, *sl.ivj);
         if (rc == BN_OK)
             rc = ivf_block_pack(e, *sl.ivj, sl.ws, sl.host, v.data(), g.data(), ti.empty() ? nullptr : ti.data(),
-                                ts.empty() ? nullptr : ts.data(), tn.data(), seeds.data());
+                                ts.empty() ? nullptr : ts.data(), tn.data(), bseed);
         if (rc == BN_OK) rc = ivf_block_launch(e, *sl.ivj, sl.ws, sl.host, sl.stream);
         if (rc == BN_OK) {
             sl.ivf_block_run = true;
@@ -264,7 +296,7 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
     }
     if (bucket) {
         // block scoring: the batch's queries share one pass over the corpus;
-        // Protocol 2 runs per block with the first request's seed
+        // Protocol 2 runs per block with the batch seed
         // a slot keeps its largest plan so far (smaller batches pad it with
         // zero queries) and its workspace for per-query / IVF batches:
         // creating plans or freeing device memory mid-stream synchronises the
@@ -279,7 +311,7 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
         if (rc == BN_OK) {
             sl.block_run = true;
             rc = block_query_launch(*sl.bp, B, v.data(), g.data(), ti.empty() ? nullptr : ti.data(),
-                                    ts.empty() ? nullptr : ts.data(), tn.data(), seeds.data(), sl.stream, false);
+                                    ts.empty() ? nullptr : ts.data(), tn.data(), bseed, sl.stream, false);
             if (rc == BN_OK) s->block_batches += 1;
         } else if (rc == BN_EUNSUPPORTED) {
             s->block_off = true;  // e.g. plaintext outside int8: serve flat queries per query from now on
@@ -452,6 +484,19 @@ int validate_request(const bn_server* s, const Engine& e, const uint64_t* v_enc,
 int submit(bn_server* s, int kind, Request&& r, uint64_t* ticket) {
     std::lock_guard<std::mutex> g(s->mu);
     if (s->stop) return fail(BN_EINVAL, "server is stopping");
+    const size_t waiting = s->pending[0].size() + s->pending[1].size();
+    if (s->cfg.max_queue && waiting >= s->cfg.max_queue) {
+        s->rejected += 1;
+        return fail(BN_EAGAIN, "queue full (%zu requests waiting)", waiting);
+    }
+    if (s->cfg.queue_wait_us) {
+        const double rate = recent_rate(s);
+        if (rate > 0 && (double)waiting / rate * 1e6 > (double)s->cfg.queue_wait_us) {
+            s->rejected += 1;
+            return fail(BN_EAGAIN, "expected queue wait %.0f us exceeds %u us", (double)waiting / rate * 1e6,
+                        s->cfg.queue_wait_us);
+        }
+    }
     r.ticket = s->next_ticket++;
     r.t_submit = Clock::now();
     if (s->submitted == 0) s->t_first = r.t_submit;
@@ -576,6 +621,7 @@ int bn_server_stats(bn_server* s, int reset, bn_server_stats_t* out) {
     out->mean_batch = s->batches ? (double)s->batched_queries / (double)s->batches : 0.0;
     out->peak_workspace_bytes = s->peak_mem;
     out->block_batches = s->block_batches;
+    out->rejected = s->rejected;
     std::vector<double> l = s->lat_us;
     if (!l.empty()) {
         std::sort(l.begin(), l.end());
@@ -588,7 +634,7 @@ int bn_server_stats(bn_server* s, int reset, bn_server_stats_t* out) {
     }
     if (reset) {
         s->lat_us.clear();
-        s->batches = s->batched_queries = s->block_batches = 0;
+        s->batches = s->batched_queries = s->block_batches = s->rejected = 0;
         s->submitted = s->completed = 0;
     }
     return BN_OK;

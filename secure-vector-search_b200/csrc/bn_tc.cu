@@ -15,6 +15,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "bn_tc.cuh"
 #include "bn_tcgen05.cuh"
@@ -228,7 +229,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constant__ CUtensorMap tmap_u,
                     const TcPanel* __restrict__ panels, uint32_t npanels, uint32_t t_base, uint32_t t_cnt,
                     uint32_t n_rows, uint32_t trials_total, uint32_t stages, uint32_t stage_bytes,
-                    uint64_t* __restrict__ z_part, uint32_t* __restrict__ err, int u_flat) {
+                    uint64_t* __restrict__ z_part, uint32_t* __restrict__ err, int u_flat, long long wait_limit) {
     extern __shared__ uint8_t tc_dyn[];
     __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b;
     __shared__ uint32_t tmem_base_s;
@@ -276,7 +277,7 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
                     const uint32_t sg = min((uint32_t)S, 64u - g * S);
                     for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                         const uint32_t st = (uint32_t)(it % stages);
-                        if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1))) {
+                        if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1), wait_limit)) {
                             abort_s = 1;
                             atomicOr(err, 4u);
                             stop = true;
@@ -311,7 +312,7 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
                 const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
                 {
                     const uint32_t sg = min((uint32_t)S, 64u - g * S);
-                    if (gc > 0 && !bar_wait(&acce_b, (uint32_t)((gc - 1) & 1))) {
+                    if (gc > 0 && !bar_wait(&acce_b, (uint32_t)((gc - 1) & 1), wait_limit)) {
                         abort_s = 1;
                         atomicOr(err, 8u);
                         stop = true;
@@ -320,7 +321,7 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
                     tc_after();
                     for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                         const uint32_t st = (uint32_t)(it % stages);
-                        if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
+                        if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1), wait_limit) || abort_s) {
                             abort_s = 1;
                             atomicOr(err, 8u);
                             stop = true;
@@ -342,7 +343,7 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
                 }
             }
             mma_commit(&done_b);
-            bar_wait(&done_b, 0);  // every issued MMA has finished before TMEM is freed
+            if (!bar_wait(&done_b, 0)) atomicOr(err, 64u);  // every issued MMA has finished before TMEM is freed
         }
     } else {
         // ---------------------------------------------------------- epilogue
@@ -353,7 +354,7 @@ tc_freivalds_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_con
         for (uint32_t item = blockIdx.x; item < npanels * groups && !stop; item += gridDim.x, ++gc) {
             const uint32_t p = item / groups, g = item % groups;
             const uint32_t sg = min((uint32_t)S, 64u - g * S);
-            const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b, (uint32_t)(gc & 1)));  // warp-uniform
+            const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b, (uint32_t)(gc & 1), wait_limit));  // warp-uniform
             if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
             if (__any_sync(FULLMASK, !ok || abort_s)) { stop = true; break; }
             tc_after();
@@ -393,7 +394,7 @@ __global__ void __launch_bounds__(SM_THREADS, 1)
 tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constant__ CUtensorMap tmap_u,
                           const TcPanel* __restrict__ panels, uint32_t p_first, uint32_t npanels,
                           uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
-                          uint64_t* __restrict__ z_part, uint32_t* __restrict__ err) {
+                          uint64_t* __restrict__ z_part, uint32_t* __restrict__ err, long long wait_limit) {
     extern __shared__ uint8_t tc_dyn[];
     __shared__ uint64_t full_b[SM_STAGES], empty_b[SM_STAGES], accf_b[3], acce_b[3], ufull_b[2], ufree_b[2], done_b;
     __shared__ uint32_t tmem_base_s;
@@ -446,7 +447,7 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
                 const uint32_t nrb = min((pn.rows + TC_ROWS - 1) / TC_ROWS, TC_SMALL_RB);
                 const uint32_t ub = pc & 1;
                 // U region ub is free once the MMAs of panel pc - 2 have read it
-                if (pc >= 2 && !bar_wait(&ufree_b[ub], ((pc >> 1) - 1) & 1)) {
+                if (pc >= 2 && !bar_wait(&ufree_b[ub], ((pc >> 1) - 1) & 1, wait_limit)) {
                     abort_s = 1;
                     atomicOr(err, 4u);
                     break;
@@ -458,7 +459,7 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
                 for (uint32_t s = 0; s < 64 && !stop; ++s)
                     for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                         const uint32_t st = (uint32_t)(it % SM_STAGES);
-                        if (it >= SM_STAGES && !bar_wait(&empty_b[st], (uint32_t)(((it / SM_STAGES) - 1) & 1))) {
+                        if (it >= SM_STAGES && !bar_wait(&empty_b[st], (uint32_t)(((it / SM_STAGES) - 1) & 1), wait_limit)) {
                             abort_s = 1;
                             atomicOr(err, 4u);
                             stop = true;
@@ -487,7 +488,7 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
                 const TcPanel pn = panels[p_first + w];
                 const uint32_t nrb = min((pn.rows + TC_ROWS - 1) / TC_ROWS, TC_SMALL_RB);
                 const uint32_t ub = pc & 1;
-                if (!bar_wait(&ufull_b[ub], (pc >> 1) & 1) || abort_s) {
+                if (!bar_wait(&ufull_b[ub], (pc >> 1) & 1, wait_limit) || abort_s) {
                     abort_s = 1;
                     atomicOr(err, 8u);
                     break;
@@ -495,7 +496,7 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
                 tc_after();
                 for (uint32_t s = 0; s < 64 && !stop; ++s, ++sc) {
                     const uint32_t b = (uint32_t)(sc % 3), use = (uint32_t)(sc / 3);
-                    if (use > 0 && !bar_wait(&acce_b[b], (use - 1) & 1)) {
+                    if (use > 0 && !bar_wait(&acce_b[b], (use - 1) & 1, wait_limit)) {
                         abort_s = 1;
                         atomicOr(err, 8u);
                         stop = true;
@@ -505,7 +506,7 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
                     const uint32_t d = tmem + b * n_rows;
                     for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                         const uint32_t st = (uint32_t)(it % SM_STAGES);
-                        if (!bar_wait(&full_b[st], (uint32_t)((it / SM_STAGES) & 1)) || abort_s) {
+                        if (!bar_wait(&full_b[st], (uint32_t)((it / SM_STAGES) & 1), wait_limit) || abort_s) {
                             abort_s = 1;
                             atomicOr(err, 8u);
                             stop = true;
@@ -527,7 +528,7 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
                 mma_commit(&ufree_b[ub]);  // U region reusable once this panel's MMAs are done
             }
             mma_commit(&done_b);
-            bar_wait(&done_b, 0);  // every issued MMA has finished before TMEM is freed
+            if (!bar_wait(&done_b, 0)) atomicOr(err, 64u);  // every issued MMA has finished before TMEM is freed
         }
     } else {
         // ---------------------------------------------------------- drain
@@ -542,7 +543,7 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
             uint64_t* z_out = z_part + ((uint64_t)p * trials_total + t_base) * N;
             for (uint32_t s = 0; s < 64; ++s, ++sc) {
                 const uint32_t b = (uint32_t)(sc % 3), use = (uint32_t)(sc / 3);
-                const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b[b], use & 1));  // warp-uniform
+                const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b[b], use & 1, wait_limit));  // warp-uniform
                 if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
                 if (__any_sync(FULLMASK, !ok || abort_s)) { stop = true; break; }
                 tc_after();
@@ -594,7 +595,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 const __grid_constant__ CUtensorMap tmap_w, const TcPanel* __restrict__ panels, uint32_t npanels,
                 const VerifySeg* __restrict__ vsegs, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
                 uint32_t stages, uint32_t stage_bytes, uint64_t* __restrict__ z_part, uint64_t* __restrict__ r_part,
-                uint64_t r_stride, uint32_t* __restrict__ err) {
+                uint64_t r_stride, uint32_t* __restrict__ err, long long wait_limit, uint32_t pf_dist) {
     constexpr int S = FU_S;
     extern __shared__ uint8_t tc_dyn[];
     __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b, racc_b[2], rfree_b[2];
@@ -641,6 +642,12 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
         if (lane == 0) {  // ------------------------------------------ TMA producer
             uint64_t it = 0;
             bool stop = false;
+            // L2 prefetch of the m_enc boxes of the load pf_dist loads ahead
+            // (loads past the first `stages`, which go out at once): the
+            // stage ring holds three loads, the prefetches keep pf_dist more
+            // in flight from DRAM.  (pf_item, pf_rb) is load number pf_pos.
+            uint32_t pf_item = blockIdx.x, pf_rb = 0;
+            uint64_t pf_pos = 0;
             for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
                 const uint32_t p = item / groups, g = item % groups;
                 const TcPanel pn = panels[p];
@@ -648,8 +655,20 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
                 const uint32_t sg = min((uint32_t)S, 64u - g * S);
                 for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
+                    while (pf_dist && pf_pos <= it + pf_dist && pf_item < items) {
+                        const uint32_t pp = pf_item / groups, pg = pf_item % groups;
+                        const TcPanel ppn = panels[pp];
+                        if (pf_pos >= stages)
+                            for (uint32_t s = 0; s < min((uint32_t)S, 64u - pg * S); ++s)
+                                tma_prefetch_2d(&tmap_m, (int)((pg * S + s) * 128), (int)(ppn.row0 + pf_rb * TC_ROWS));
+                        ++pf_pos;
+                        if (++pf_rb == (ppn.rows + TC_ROWS - 1) / TC_ROWS) {
+                            pf_rb = 0;
+                            pf_item += gridDim.x;
+                        }
+                    }
                     const uint32_t st = (uint32_t)(it % stages);
-                    if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1))) {
+                    if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1), wait_limit)) {
                         abort_s = 1;
                         atomicOr(err, 4u);
                         stop = true;
@@ -678,7 +697,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 const TcPanel pn = panels[p];
                 const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
                 const uint32_t sg = min((uint32_t)S, 64u - g * S);
-                if (gc > 0 && !bar_wait(&acce_b, (uint32_t)((gc - 1) & 1))) {
+                if (gc > 0 && !bar_wait(&acce_b, (uint32_t)((gc - 1) & 1), wait_limit)) {
                     abort_s = 1;
                     atomicOr(err, 8u);
                     break;
@@ -686,7 +705,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 tc_after();
                 for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                     const uint32_t st = (uint32_t)(it % stages);
-                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s) {
+                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1), wait_limit) || abort_s) {
                         abort_s = 1;
                         atomicOr(err, 8u);
                         stop = true;
@@ -705,7 +724,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 mma_commit(&accf_b);
             }
             mma_commit(&done_b);
-            bar_wait(&done_b, 0);
+            if (!bar_wait(&done_b, 0)) atomicOr(err, 64u);  // every issued MMA has finished
         }
     } else if (warp == FU_R_WARP) {
         if (lane == 0) {  // ------------------------------------------ r MMA issuer
@@ -719,8 +738,8 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 const uint32_t sg = min((uint32_t)S, 64u - g * S);
                 for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                     const uint32_t st = (uint32_t)(it % stages), eb = (uint32_t)(it & 1);
-                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1)) || abort_s ||
-                        (it >= 2 && !bar_wait(&rfree_b[eb], (uint32_t)(((it >> 1) - 1) & 1)))) {
+                    if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1), wait_limit) || abort_s ||
+                        (it >= 2 && !bar_wait(&rfree_b[eb], (uint32_t)(((it >> 1) - 1) & 1), wait_limit))) {
                         abort_s = 1;
                         atomicOr(err, 8u);
                         stop = true;
@@ -738,7 +757,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 }
             }
             mma_commit(&done_b);
-            bar_wait(&done_b, 0);
+            if (!bar_wait(&done_b, 0)) atomicOr(err, 64u);  // every issued MMA has finished
         }
     } else if (warp < 2 + TC_EPI_WARPS) {
         // ---------------------------------------------------------- TMEM epilogue (z)
@@ -748,7 +767,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
         for (uint32_t item = blockIdx.x; item < items; item += gridDim.x, ++gc) {
             const uint32_t p = item / groups, g = item % groups;
             const uint32_t sg = min((uint32_t)S, 64u - g * S);
-            const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b, (uint32_t)(gc & 1)));  // warp-uniform
+            const bool ok = __all_sync(FULLMASK, bar_wait(&accf_b, (uint32_t)(gc & 1), wait_limit));  // warp-uniform
             if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 16u); }
             if (__any_sync(FULLMASK, !ok || abort_s)) break;
             tc_after();
@@ -774,7 +793,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
             const uint64_t r0 = vs.r0 + (pn.row0 - vs.row0);  // r index of the panel's first row
             for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                 const uint32_t eb = (uint32_t)(it & 1);
-                const bool ok = __all_sync(FULLMASK, bar_wait(&racc_b[eb], (uint32_t)((it >> 1) & 1)));
+                const bool ok = __all_sync(FULLMASK, bar_wait(&racc_b[eb], (uint32_t)((it >> 1) & 1), wait_limit));
                 if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 32u); }
                 if (__any_sync(FULLMASK, !ok || abort_s)) { stop = true; break; }
                 tc_after();
@@ -978,8 +997,10 @@ void launch_tc_ugen(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t 
 
 void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
                          uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
-                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s, int u_flat) {
+                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s, int u_flat,
+                         long long wait_cycles) {
     if (!npanels) return;
+    const long long wl = wait_cycles > 0 ? wait_cycles : TC_WAIT_CYCLES;
     const int S = n_rows <= 128 ? 4 : 3;
     const uint32_t stage_bytes = (uint32_t)S * STRIP_BYTES + ((n_rows * TC_ROWS + 1023u) & ~1023u);
     uint32_t stages = (220u * 1024u) / stage_bytes;
@@ -990,24 +1011,25 @@ void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, c
     if (S == 4) {
         cudaFuncSetAttribute(tc_freivalds_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         tc_freivalds_kernel<4><<<grid, TC_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, t_base, t_cnt, n_rows,
-                                                              trials_total, stages, stage_bytes, d_z_part, d_err, u_flat);
+                                                              trials_total, stages, stage_bytes, d_z_part, d_err, u_flat, wl);
     } else {
         cudaFuncSetAttribute(tc_freivalds_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         tc_freivalds_kernel<3><<<grid, TC_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, npanels, t_base, t_cnt, n_rows,
-                                                              trials_total, stages, stage_bytes, d_z_part, d_err, u_flat);
+                                                              trials_total, stages, stage_bytes, d_z_part, d_err, u_flat, wl);
     }
 }
 
 void launch_tc_freivalds_small(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
                                uint32_t p_first, uint32_t npanels, uint32_t t_base, uint32_t t_cnt,
                                uint32_t n_rows, uint32_t trials_total, uint64_t* d_z_part, uint32_t* d_err,
-                               int num_sms, cudaStream_t s) {
+                               int num_sms, cudaStream_t s, long long wait_cycles) {
     if (!npanels) return;
+    const long long wl = wait_cycles > 0 ? wait_cycles : TC_WAIT_CYCLES;
     const int smem = (int)(2 * TC_SMALL_RB * n_rows * TC_ROWS + SM_STAGES * STRIP_BYTES + 1024);
     cudaFuncSetAttribute(tc_freivalds_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     const unsigned grid = npanels < (uint32_t)num_sms ? npanels : (unsigned)num_sms;
     tc_freivalds_small_kernel<<<grid, SM_THREADS, smem, s>>>(tmap_m, tmap_u, d_panels, p_first, npanels, t_base, t_cnt,
-                                                             n_rows, trials_total, d_z_part, d_err);
+                                                             n_rows, trials_total, d_z_part, d_err, wl);
 }
 
 void launch_query_wimg(const uint64_t* d_v, uint32_t nq, uint8_t* d_w, cudaStream_t s) {
@@ -1020,8 +1042,9 @@ void launch_query_wimg(const uint64_t* d_v, uint32_t nq, uint8_t* d_w, cudaStrea
 void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const CUtensorMap& tmap_w,
                      const TcPanel* d_panels, uint32_t npanels, const VerifySeg* d_vsegs, uint32_t t_cnt,
                      uint32_t n_rows, uint32_t trials_total, uint64_t* d_z_part, uint64_t* d_r_part, uint64_t r_stride,
-                     uint32_t* d_err, int num_sms, cudaStream_t s) {
+                     uint32_t* d_err, int num_sms, cudaStream_t s, long long wait_cycles) {
     if (!npanels) return;
+    const long long wl = wait_cycles > 0 ? wait_cycles : TC_WAIT_CYCLES;
     const uint32_t stage_bytes = (uint32_t)FU_S * STRIP_BYTES + ((n_rows * TC_ROWS + 1023u) & ~1023u) +
                                  (uint32_t)FU_S * W_STRIP_BYTES;
     uint32_t stages = (227u * 1024u - 2048u) / stage_bytes;
@@ -1030,9 +1053,11 @@ void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const
     const uint32_t items = npanels * ((64 + FU_S - 1) / FU_S);
     const unsigned grid = items < (uint32_t)num_sms ? items : (unsigned)num_sms;
     cudaFuncSetAttribute(tc_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const char* pf_env = getenv("BN_FUSED_PREFETCH");
+    const uint32_t pf = pf_env ? (uint32_t)atoi(pf_env) : 0u;
     tc_fused_kernel<<<grid, FU_THREADS, smem, s>>>(tmap_m, tmap_u, tmap_w, d_panels, npanels, d_vsegs, t_cnt, n_rows,
                                                    trials_total, stages, stage_bytes, d_z_part, d_r_part, r_stride,
-                                                   d_err);
+                                                   d_err, wl, pf);
 }
 
 void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const uint64_t* d_r_part,

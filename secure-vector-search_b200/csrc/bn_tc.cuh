@@ -66,10 +66,13 @@ void launch_tc_ugen(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t 
 // tmap_u: U bytes {128, nblocks * n_rows}, box {128, n_rows}, swizzle 128B
 // (u_flat = 0), or the flat image {row pitch, n_rows}, box {128, n_rows}
 // (u_flat = 1; panel rb0 = first row / 128).
-// *err: bit 2/3/4 set when a bounded pipeline wait timed out.
+// *err: bit 2/3/4 set when a bounded pipeline wait timed out, bit 64 when
+// the wind-down wait for the CTA's own MMAs did.  wait_cycles: limit of the
+// pipeline waits (0 = about a second; shorter only to test the timeout path).
 void launch_tc_freivalds(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
                          uint32_t npanels, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
-                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s, int u_flat = 0);
+                         uint64_t* d_z_part, uint32_t* d_err, int num_sms, cudaStream_t s, int u_flat = 0,
+                         long long wait_cycles = 0);
 
 // The same for panels [p_first, p_first + npanels) of at most
 // TC_SMALL_PANEL_ROWS rows (short IVF lists): whole panels per CTA, the
@@ -79,7 +82,7 @@ constexpr uint32_t TC_SMALL_PANEL_ROWS = 3 * 128;
 void launch_tc_freivalds_small(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const TcPanel* d_panels,
                                uint32_t p_first, uint32_t npanels, uint32_t t_base, uint32_t t_cnt,
                                uint32_t n_rows, uint32_t trials_total, uint64_t* d_z_part, uint32_t* d_err,
-                               int num_sms, cudaStream_t s);
+                               int num_sms, cudaStream_t s, long long wait_cycles = 0);
 
 // Fused single pass over m_enc for the first <= 20 trials, both products on
 // the tensor cores: z_part as above plus r_part[group][r index] (3-strip
@@ -89,7 +92,7 @@ void launch_tc_freivalds_small(const CUtensorMap& tmap_m, const CUtensorMap& tma
 void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const CUtensorMap& tmap_w,
                      const TcPanel* d_panels, uint32_t npanels, const VerifySeg* d_vsegs, uint32_t t_cnt,
                      uint32_t n_rows, uint32_t trials_total, uint64_t* d_z_part, uint64_t* d_r_part, uint64_t r_stride,
-                     uint32_t* d_err, int num_sms, cudaStream_t s);
+                     uint32_t* d_err, int num_sms, cudaStream_t s, long long wait_cycles = 0);
 inline uint32_t tc_groups(uint32_t) { return 22u; }  // strip groups of the fused pass (3 strips each)
 constexpr uint32_t WIMG_BYTES_PER_QUERY = 64u * 16u * 128u;
 constexpr uint32_t WIMG_BOX_ROWS = 48;  // one strip group's diagonal rows

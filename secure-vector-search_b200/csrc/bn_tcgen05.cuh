@@ -26,10 +26,14 @@ static __device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-static __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity) {
+// Bounded wait for the phase with `parity`: false after `limit` cycles.
+// Pipeline waits take the kernel's wait_limit argument (TC_WAIT_CYCLES unless
+// a test shortens it, bn_debug_set_wait_limit); the wind-down waits for a
+// CTA's own copies and MMAs always keep the full limit.
+static __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, long long limit = TC_WAIT_CYCLES) {
     const long long t0 = clock64();
     while (!bar_try(b, parity))
-        if (clock64() - t0 > TC_WAIT_CYCLES) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 static __device__ __forceinline__ void bar_arrive(uint64_t* b) {
@@ -51,6 +55,12 @@ static __device__ __forceinline__ void tma_3d(void* dst, const CUtensorMap* map,
             su32(dst)),
         "l"(map), "r"(x), "r"(y), "r"(z), "r"(su32(b))
         : "memory");
+}
+// L2 prefetch of one box of a 2-D tensor map: no shared memory is written
+// and nothing completes, so nothing has to be waited for.
+static __device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
+    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(map), "r"(x), "r"(y)
+                 : "memory");
 }
 static __device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 static __device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }

@@ -241,3 +241,49 @@ def test_ivf_block_batches_match_per_query(corpora):
     st = srv.stats()
     assert st["block_batches"] > 0 and st["completed"] == len(reqs)
     srv.close()
+
+
+def test_queue_admission_refuses_with_eagain(corpora):
+    """A bounded queue: with max_queue waiting requests a submit is refused
+    with BN_EAGAIN (nothing queued); every admitted request is served and
+    equals the per-query path."""
+    c = capi()
+    flat, L, ivf, case = corpora
+    reqs = requests(L, case, 24, 8100)
+    want = [direct(flat, ivf, r) for r in reqs]
+    srv = c.Server(flat, ivf, max_batch=4, slots=1, max_wait_us=200000, trials=TRIALS, k=K, max_queue=6)
+    tickets, refused = [], 0
+    for i, r in enumerate(reqs):
+        try:
+            tickets.append((submit(srv, r), i))
+        except c.BnError as e:
+            assert e.code == c.BN_EAGAIN and "queue full" in str(e)
+            refused += 1
+    for t, i in tickets:
+        assert same(srv.wait(t)[:4], want[i])
+    st = srv.stats()
+    srv.close()
+    assert refused > 0 and st["rejected"] == refused and st["completed"] == len(tickets)
+
+
+def test_queue_wait_admission(corpora):
+    """Latency-aware admission: once completions give a service rate, a
+    submit whose expected queue wait exceeds queue_wait_us is refused."""
+    c = capi()
+    flat, L, ivf, case = corpora
+    reqs = [r for r in requests(L, case, 80, 8300) if r[0] == "flat"]
+    srv = c.Server(flat, ivf, max_batch=2, slots=1, max_wait_us=0, trials=TRIALS, k=K, queue_wait_us=1)
+    for r in reqs[:10]:  # completions give the server its service rate
+        srv.wait(submit(srv, r))
+    refused, tickets = 0, []
+    for r in reqs[10:]:
+        try:
+            tickets.append(submit(srv, r))
+        except c.BnError as e:
+            assert e.code == c.BN_EAGAIN and "expected queue wait" in str(e)
+            refused += 1
+    for t in tickets:
+        srv.wait(t)
+    st = srv.stats()
+    srv.close()
+    assert refused > 0 and st["rejected"] == refused
