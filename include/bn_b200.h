@@ -163,6 +163,25 @@ int bn_flat_query(bn_flat* h, uint32_t B, const uint64_t* v_enc, const uint64_t*
                   uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed_trial, uint64_t* r_out,
                   uint64_t* mv_out);
 
+/* One row shard of a flat corpus split over several GPUs (one process per
+ * GPU).  No counterpart in the reference, whose GPU backend serves one card
+ * per process.  The handle holds rows [shard_row0, shard_row0 + m) of a
+ * corpus of total_rows rows; the call runs bn_flat_query's pipeline on them
+ * with the Protocol 2 draws at those rows' positions in the whole corpus
+ * (u_t[i] = draw t * total_rows + i of the query's stream, crypto.rs:1021-
+ * 1036), and returns what the ranks exchange instead of a verdict:
+ *   ids / scores / n_hits  the shard's top-k (ids are global row numbers);
+ *   ur, zv (B x trials)    this shard's u_t . r and z_t . v_enc, canonical.
+ * Summed over the shards (mod p), ur and zv are verify_response's two sides
+ * for the whole corpus (z . v is linear in z), so query b is accepted iff
+ * every trial's sums agree; the union of the shards' top-k lists holds the
+ * global top-k.  The merge and the exact sums are the caller's
+ * (bn_b200/shard.py does them over torch.distributed). */
+int bn_flat_query_shard(bn_flat* h, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                        const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds, uint32_t trials,
+                        uint32_t k, uint64_t shard_row0, uint64_t total_rows, uint32_t* ids, int64_t* scores,
+                        uint32_t* n_hits, uint64_t* ur, uint64_t* zv);
+
 /* Prepared, device-resident form of bn_flat_query for a fixed (B, trials,
  * k): bn_plan_enqueue only enqueues kernels on `stream` (no host work, no
  * allocation, no synchronisation), so it can be captured in a CUDA graph.

@@ -496,6 +496,33 @@ int32_t bno_verify_response(const uint64_t* r, const uint64_t* M_enc, uint64_t m
     return fail;
 }
 
+/* Protocol 2 split over row shards (no counterpart in the reference): the
+ * shard rows [row0, row0 + rows) of a corpus of `total` rows, every trial's
+ * two partial sums u_t . r_shard and (u_t^T M_shard) . v_enc, where u_t is
+ * verify_response's draw vector for the whole corpus (crypto.rs:1021-1036:
+ * total draws per trial from one stream, rejection included) restricted to
+ * the shard.  All trials, no early exit: the verdict needs every shard's
+ * sums.  Summed over the shards mod p they are verify_response's ur / zv. */
+void bno_verify_shard_partials(const uint64_t* r_shard, const uint64_t* M_shard, uint64_t rows, uint32_t n,
+                               const uint64_t* v_enc, uint32_t trials, const uint8_t v_seed[32], uint64_t row0,
+                               uint64_t total, uint64_t* ur, uint64_t* zv, int nthreads) {
+    bno_rng rng;
+    bno_rng_from_seed(&rng, v_seed);
+    uint64_t* u = (uint64_t*)malloc(sizeof(uint64_t) * (rows ? rows : 1));
+    uint64_t* z = (uint64_t*)malloc(sizeof(uint64_t) * n);
+    for (uint32_t t = 0; t < trials; ++t) {
+        for (uint64_t i = 0; i < total; ++i) {
+            const uint64_t x = bno_sample_fp(&rng);
+            if (i >= row0 && i < row0 + rows) u[i - row0] = x;
+        }
+        ur[t] = bno_dot_product(u, r_shard, rows);
+        bno_matvec_transpose(M_shard, rows, n, u, z, nthreads);
+        zv[t] = bno_dot_product(z, v_enc, n);
+    }
+    free(u);
+    free(z);
+}
+
 /* ------------------------------------------------------------------ */
 /* Decode -- crypto.rs:837-940                                         */
 /* ------------------------------------------------------------------ */

@@ -111,6 +111,9 @@ uint64_t bno_dot_product(const uint64_t* a, const uint64_t* b, uint64_t len);
  * v_seed = domain_separate(q_seed, "protocol2").  Returns -1 when every
  * trial passes, else the first failing trial.  ur/zv (nullable) receive
  * the two sides of each trial that ran. */
+void bno_verify_shard_partials(const uint64_t* r_shard, const uint64_t* M_shard, uint64_t rows, uint32_t n,
+                               const uint64_t* v_enc, uint32_t trials, const uint8_t v_seed[32], uint64_t row0,
+                               uint64_t total, uint64_t* ur, uint64_t* zv, int nthreads);
 int32_t bno_verify_response(const uint64_t* r, const uint64_t* M_enc, uint64_t m, uint32_t n,
                             const uint64_t* v_enc, uint32_t trials, const uint8_t v_seed[32],
                             uint64_t* ur, uint64_t* zv, int nthreads);

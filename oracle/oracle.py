@@ -66,6 +66,8 @@ def _load():
         "bno_matvec_batch": (None, [_u64p, u64, u32, _u64p, u32, _u64p, C.c_int]),
         "bno_dot_product": (u64, [_u64p, _u64p, u64]),
         "bno_verify_response": (i32, [_u64p, _u64p, u64, u32, _u64p, u32, _u8p, vp, vp, C.c_int]),
+        "bno_verify_shard_partials": (None, [_u64p, _u64p, u64, u32, _u64p, u32, _u8p, u64, u64, _u64p, _u64p,
+                                              C.c_int]),
         "bno_l_transpose_times_vec": (None, [_u64p, u32, u32, _u64p, _u64p]),
         "bno_decode_scores": (None, [_u64p, _u64p, _u64p, _u64p, _u64p, _u32p, _i8p, _u64p, _u64p,
                                      _u64p, _u32p, _i8p, u32, u64, u32, u32, _u64p, C.c_int]),
@@ -265,6 +267,18 @@ def verify_response(r, m_enc, m, n, v_enc, trials, v_seed, threads=None):
                                 _ptr(ur), _ptr(zv), threads or NTHREADS)
     ran = trials if f < 0 else f + 1
     return int(f), ur[:ran], zv[:ran]
+
+
+def verify_shard_partials(r_shard, m_shard, rows, n, v_enc, trials, v_seed, row0, total, threads=None):
+    """(ur, zv) partial sums of every trial for rows [row0, row0 + rows) of a
+    corpus of `total` rows (verify_response's draws restricted to the shard)."""
+    ur = np.zeros(max(trials, 1), np.uint64)
+    zv = np.zeros(max(trials, 1), np.uint64)
+    lib.bno_verify_shard_partials(np.ascontiguousarray(r_shard, np.uint64) if rows else np.zeros(1, np.uint64),
+                                  np.ascontiguousarray(m_shard, np.uint64).reshape(-1) if rows else np.zeros(1, np.uint64),
+                                  rows, n, np.ascontiguousarray(v_enc, np.uint64), trials, _seed(v_seed), row0, total,
+                                  ur, zv, threads or NTHREADS)
+    return ur[:trials], zv[:trials]
 
 
 # ---------------------------------------------------------------- decode

@@ -76,6 +76,7 @@ _SIGS = {
     "bn_flat_verify": (C.c_int, [vp, vp, vp, vp, u32, vp, vp, vp]),
     "bn_flat_verify_noalloc": (C.c_int, [vp, vp, vp, vp, u32, vp, vp, vp, vp]),
     "bn_flat_query": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp, vp]),
+    "bn_flat_query_shard": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, vp, u32, u32, u64, u64, vp, vp, vp, vp, vp]),
     "bn_flat_plan": (C.c_int, [vp, u32, u32, u32, vp]),
     "bn_plan_enqueue": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "bn_plan_enqueue_scan": (C.c_int, [vp, vp, vp, vp]),
@@ -282,6 +283,26 @@ class Flat:
                                 ptr(tn), ptr(seeds), trials, k, ptr(ids), ptr(sc), ptr(nh), ptr(fl), ptr(r), ptr(mv)))
         hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
         return hits, fl, (r[:, : self.m] if want_r else None), (mv[:, : self.m] if want_mv else None)
+
+    def query_shard(self, v_enc, g, t_list, v_seeds, trials, k, shard_row0: int, total_rows: int):
+        """bn_flat_query_shard: this handle is rows [shard_row0, shard_row0 + m) of a corpus of total_rows.
+        Returns (hits with global ids, ur, zv) with ur / zv of shape (B, trials)."""
+        v = _u64(v_enc).reshape(-1, N)
+        B = v.shape[0]
+        gg = _u64(g).reshape(B, self.n1)
+        ti, ts, tn = _t_concat(t_list)
+        seeds = None if v_seeds is None else np.frombuffer(b"".join(bytes(s) for s in v_seeds), np.uint8).copy()
+        kk = max(k, 1)
+        ids = np.zeros((B, kk), np.uint32)
+        sc = np.zeros((B, kk), np.int64)
+        nh = np.zeros(B, np.uint32)
+        ur = np.zeros((B, max(trials, 1)), np.uint64)
+        zv = np.zeros((B, max(trials, 1)), np.uint64)
+        check(lib.bn_flat_query_shard(self.h, B, ptr(v), ptr(gg), ptr(ti) if ti.size else None,
+                                      ptr(ts) if ts.size else None, ptr(tn), ptr(seeds), trials, k, shard_row0,
+                                      total_rows, ptr(ids), ptr(sc), ptr(nh), ptr(ur), ptr(zv)))
+        hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
+        return hits, ur[:, :trials], zv[:, :trials]
 
     def plan(self, B: int, trials: int, k: int) -> "Plan":
         out = vp()

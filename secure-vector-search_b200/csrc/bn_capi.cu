@@ -982,6 +982,48 @@ int bn_flat_query(bn_flat* f, uint32_t B, const uint64_t* v_enc, const uint64_t*
     return BN_OK;
 }
 
+int bn_flat_query_shard(bn_flat* f, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                        const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds, uint32_t trials,
+                        uint32_t k, uint64_t shard_row0, uint64_t total_rows, uint32_t* ids, int64_t* scores,
+                        uint32_t* n_hits, uint64_t* ur, uint64_t* zv) {
+    if (!f) return fail(BN_EINVAL, "null handle");
+    if (B == 0) return BN_OK;
+    if (!f->m) return fail(BN_EINVAL, "empty shard");
+    if (shard_row0 > total_rows || f->m > total_rows - shard_row0)
+        return fail(BN_EINVAL, "shard rows [%llu, %llu) exceed the corpus of %llu rows", (unsigned long long)shard_row0,
+                    (unsigned long long)(shard_row0 + f->m), (unsigned long long)total_rows);
+    if (shard_row0 + f->m > 0xffffffffull) return fail(BN_EINVAL, "global row ids must fit in u32");
+    if (trials && (!ur || !zv)) return fail(BN_EINVAL, "ur / zv are required when trials > 0");
+    std::lock_guard<std::mutex> gd(f->e.mu);
+    HostMeta hm;
+    flat_meta(f->m, B, hm);
+    for (VerifySeg& vs : hm.vsegs) {  // draw positions of these rows within the whole corpus
+        vs.draw_stride = total_rows;
+        vs.draw_base = shard_row0;
+    }
+    QueryJob j;
+    j.hm = &hm;
+    j.B = B;
+    j.trials = trials;
+    j.k = k;
+    Engine& e = f->e;
+    TRY(job_prepare(e, j, e.ws, e.host, v_enc, g, t_idx, t_sign, t_nnz, v_seeds));
+    TRY(job_launch(e, j, e.ws, e.host, e.stream, nullptr, nullptr));
+    CU(cudaStreamSynchronize(e.stream));
+    std::vector<int32_t> vf;  // local verdicts: meaningless for a shard (decided on the sums)
+    TRY(job_finish(j, e.host, ids, scores, n_hits, vf));
+    if (k && ids)
+        for (uint32_t b = 0; b < B; ++b)
+            for (uint32_t i = 0; i < (n_hits ? n_hits[b] : std::min<uint64_t>(k, f->m)); ++i)
+                ids[(uint64_t)b * k + i] += (uint32_t)shard_row0;
+    if (trials) {
+        const char* h = e.host.at<char>();
+        memcpy(ur, h + j.o.ur, (uint64_t)B * trials * 8);
+        memcpy(zv, h + j.o.zv, (uint64_t)B * trials * 8);
+    }
+    return BN_OK;
+}
+
 int bn_flat_plan(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k, bn_plan** out) {
     if (!f || !out) return fail(BN_EINVAL, "null argument");
     *out = nullptr;

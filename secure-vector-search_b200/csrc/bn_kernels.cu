@@ -292,7 +292,7 @@ freivalds_kernel(const uint64_t* __restrict__ m_enc, const uint64_t* __restrict_
         const uint32_t nt = (uint32_t)min((uint64_t)FV_TILE, row_end - tile);
         __syncthreads();
         if (gen_t < t_cnt) {
-            const uint64_t first = (uint64_t)(t_base + gen_t) * vs.rows + tile;  // draw index of row `tile`
+            const uint64_t first = draw_index(vs, t_base + gen_t, tile);  // draw index of row `tile`
             const uint64_t blk = first / 8 + gen_b;
             if (blk * 8 < first + nt) {
                 uint32_t w[16];

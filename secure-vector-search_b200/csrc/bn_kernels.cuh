@@ -49,13 +49,19 @@ constexpr int SCAN_ROWS = 4;
 
 // Freivalds: per (segment, trial group) the u stream is ChaCha20Rng keyed
 // by v_seed; u_t[i] is draw number t*m_seg + i of that stream (crypto.rs:
-// 1026-1027).
+// 1026-1027).  A row shard of a larger corpus (bn_flat_query_shard) draws
+// at its rows' positions in the whole corpus: t * draw_stride + draw_base + i.
 struct VerifySeg {
-    uint64_t row0;   // first row in m_enc
-    uint64_t r0;     // first r value of this segment
-    uint32_t rows;   // m of the list / flat corpus
-    uint32_t query;  // index into v_enc / keys arrays
+    uint64_t row0;         // first row in m_enc
+    uint64_t r0;           // first r value of this segment
+    uint32_t rows;         // m of the list / flat corpus
+    uint32_t query;        // index into v_enc / keys arrays
+    uint64_t draw_stride;  // draws per trial (0: rows)
+    uint64_t draw_base;    // draw position of the segment's first row within a trial
 };
+__host__ __device__ __forceinline__ uint64_t draw_index(const VerifySeg& vs, uint32_t t, uint64_t i) {
+    return (uint64_t)t * (vs.draw_stride ? vs.draw_stride : vs.rows) + vs.draw_base + i;
+}
 
 // DRAW_HIT_P is or-ed into a Protocol 2 kernel's flag word if a draw hit the rejected
 // value p (probability 2^-61 per draw), meaning later draws of the

@@ -46,7 +46,7 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
     // draws: 128 consecutive indices per trial span at most 17 keystream blocks
     for (uint32_t item = threadIdx.x; item < t_cnt * 17; item += blockDim.x) {
         const uint32_t tl = item / 17, bi = item % 17;
-        const uint64_t first = (uint64_t)(t_base + tl) * vs.rows + tb.i0;
+        const uint64_t first = draw_index(vs, t_base + tl, tb.i0);
         const uint64_t kb = first / 8 + bi;
         if (kb * 8 >= first + TC_ROWS) continue;
         uint32_t w[16];
