@@ -339,7 +339,7 @@ RunLayout make_layout(const Sizes& z, bool want_mv) {
                    ? L.take<uint64_t>((uint64_t)tc_groups(pass_rows(std::min<uint32_t>(TC_MAX_TRIALS, z.trials))) *
                                       std::max<uint64_t>(z.total_out, 1))
                    : 0;
-    o.zv_chunks = L.take<uint64_t>(std::max<uint64_t>(z.nvseg * z.trials * 8, 1));
+    o.zv_chunks = L.take<uint64_t>(std::max<uint64_t>(tc_finish_words((uint32_t)z.nvseg, z.trials), 1));
     o.wimg = (tc && z.trials) ? L.take<uint8_t>((uint64_t)z.B * WIMG_BYTES_PER_QUERY) : 0;
     o.total = L.off + 1024;
     return o;

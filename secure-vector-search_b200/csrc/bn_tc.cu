@@ -895,17 +895,20 @@ tc_rreduce_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict
     }
 }
 
-// CTA (trial t, y, segment): y < 8 sums z over the segment's panels for the
-// 128 columns [128y, 128y+128) and writes that chunk's share of z_t . v;
-// y == 8 sums the u_t . r partials of the segment's row blocks.
+// CTA (trial t, y, segment, split sp): y < 8 sums z over every split-th
+// panel of the segment (from its sp-th) for the 128 columns [128y, 128y+128)
+// and writes that share of z_t . v (z . v is linear in z, so the shares of
+// the splits add up); y == 8 sums every split-th row block's u_t . r
+// partial.  Splitting the panels over more CTAs keeps enough loads in flight
+// when a launch has few segments (one query: 245 panels at N = 1M).
 constexpr int FIN_CHUNKS = N / 128;
 
 __global__ void __launch_bounds__(128)
 tc_finish_kernel(const uint64_t* __restrict__ z_part, const uint64_t* __restrict__ ur_part,
                  const uint32_t* __restrict__ seg_panel0, const uint32_t* __restrict__ seg_block0,
                  const uint64_t* __restrict__ v_enc, const VerifySeg* __restrict__ vsegs, uint32_t trials,
-                 uint64_t* __restrict__ ur, uint64_t* __restrict__ zv_chunks) {
-    const uint32_t t = blockIdx.x, y = blockIdx.y, seg = blockIdx.z;
+                 uint32_t split, uint64_t* __restrict__ chunks) {
+    const uint32_t t = blockIdx.x, y = blockIdx.y, seg = blockIdx.z / split, sp = blockIdx.z % split;
     __shared__ uint64_t sh[4];
     uint64_t part = 0;
     if (y < FIN_CHUNKS) {
@@ -913,35 +916,55 @@ tc_finish_kernel(const uint64_t* __restrict__ z_part, const uint64_t* __restrict
         const uint32_t j = y * 128 + threadIdx.x;
         const uint32_t p0 = seg_panel0[seg], p1 = seg_panel0[seg + 1];
         uint64_t z = 0;
-        for (uint32_t p = p0; p < p1; ++p) z = add_mod(z, z_part[((uint64_t)p * trials + t) * N + j]);
+#pragma unroll 4
+        for (uint32_t p = p0 + sp; p < p1; p += split) z = add_mod(z, z_part[((uint64_t)p * trials + t) * N + j]);
         part = mul_mod(z, v_enc[(uint64_t)vs.query * N + j]);
     } else {
         const uint32_t b0 = seg_block0[seg], b1 = seg_block0[seg + 1];
-        for (uint32_t b = b0 + threadIdx.x; b < b1; b += blockDim.x) part = add_mod(part, ur_part[(uint64_t)b * trials + t]);
+        for (uint32_t b = b0 + sp + split * threadIdx.x; b < b1; b += split * blockDim.x)
+            part = add_mod(part, ur_part[(uint64_t)b * trials + t]);
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) part = add_mod(part, __shfl_xor_sync(FULLMASK, part, off));
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = part;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint64_t tot = add_mod(add_mod(sh[0], sh[1]), add_mod(sh[2], sh[3]));
-        if (y < FIN_CHUNKS) zv_chunks[((uint64_t)seg * trials + t) * FIN_CHUNKS + y] = tot;
-        else ur[(uint64_t)seg * trials + t] = tot;
-    }
+    if (threadIdx.x == 0)
+        chunks[(((uint64_t)seg * trials + t) * (FIN_CHUNKS + 1) + y) * split + sp] =
+            add_mod(add_mod(sh[0], sh[1]), add_mod(sh[2], sh[3]));
 }
 
-__global__ void tc_decide_kernel(const uint64_t* __restrict__ ur, const uint64_t* __restrict__ zv_chunks,
-                                 uint32_t nseg, uint32_t trials, uint64_t* __restrict__ zv, int32_t* __restrict__ failed) {
-    const uint32_t seg = blockIdx.x * blockDim.x + threadIdx.x;
-    if (seg >= nseg) return;
-    int32_t f = -1;
-    for (uint32_t t = 0; t < trials; ++t) {
-        uint64_t z = 0;
-        for (int c = 0; c < FIN_CHUNKS; ++c) z = add_mod(z, zv_chunks[((uint64_t)seg * trials + t) * FIN_CHUNKS + c]);
-        zv[(uint64_t)seg * trials + t] = z;
-        if (f < 0 && ur[(uint64_t)seg * trials + t] != z) f = (int32_t)t;
+// One CTA per segment, a warp per trial: ur_t and zv_t from the finish
+// kernel's shares, then the first trial whose sides differ (-1 if none).
+constexpr int DECIDE_WARPS = 8;
+
+__global__ void __launch_bounds__(DECIDE_WARPS * 32)
+tc_decide_kernel(const uint64_t* __restrict__ chunks, uint32_t trials, uint32_t split, uint64_t* __restrict__ ur,
+                 uint64_t* __restrict__ zv, int32_t* __restrict__ failed) {
+    const uint32_t seg = blockIdx.x, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ int32_t first;
+    if (threadIdx.x == 0) first = 0x7fffffff;
+    __syncthreads();
+    const uint32_t per = (FIN_CHUNKS + 1) * split;  // shares per trial; the last split of them are u . r
+    for (uint32_t t = warp; t < trials; t += DECIDE_WARPS) {
+        const uint64_t* c = chunks + ((uint64_t)seg * trials + t) * per;
+        uint64_t a = 0, b = 0;
+        for (uint32_t i = lane; i < per; i += 32) {
+            if (i < FIN_CHUNKS * split) b = add_mod(b, c[i]);
+            else a = add_mod(a, c[i]);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            a = add_mod(a, __shfl_xor_sync(FULLMASK, a, off));
+            b = add_mod(b, __shfl_xor_sync(FULLMASK, b, off));
+        }
+        if (lane == 0) {
+            ur[(uint64_t)seg * trials + t] = a;
+            zv[(uint64_t)seg * trials + t] = b;
+            if (a != b) atomicMin(&first, (int32_t)t);
+        }
     }
-    failed[seg] = f;
+    __syncthreads();
+    if (threadIdx.x == 0) failed[seg] = first == 0x7fffffff ? -1 : first;
 }
 
 }  // namespace
@@ -1070,18 +1093,18 @@ void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32
 
 void launch_tc_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint32_t* d_seg_panel0,
                       const uint32_t* d_seg_block0, const uint64_t* d_v_enc, const VerifySeg* d_vsegs, uint32_t nseg,
-                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, uint64_t* d_zv_chunks, int32_t* d_failed,
+                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, uint64_t* d_chunks, int32_t* d_failed,
                       cudaStream_t s) {
     if (!nseg || !trials) return;
-    // zv chunk partials go to the z_part tail region reserved by the caller
-    uint64_t* zv_chunks = d_zv_chunks;
-    for (uint32_t s0 = 0; s0 < nseg; s0 += 65535u) {  // grid.z limit
-        const uint32_t ns = nseg - s0 < 65535u ? nseg - s0 : 65535u;
-        tc_finish_kernel<<<dim3(trials, FIN_CHUNKS + 1, ns), 128, 0, s>>>(
-            d_z_part, d_ur_part, d_seg_panel0 + s0, d_seg_block0 + s0, d_v_enc, d_vsegs + s0, trials,
-            d_ur + (uint64_t)s0 * trials, zv_chunks + (uint64_t)s0 * trials * FIN_CHUNKS);
+    const uint32_t split = tc_finish_split(nseg);
+    const uint32_t per_launch = 65535u / split;  // grid.z limit
+    for (uint32_t s0 = 0; s0 < nseg; s0 += per_launch) {
+        const uint32_t ns = nseg - s0 < per_launch ? nseg - s0 : per_launch;
+        tc_finish_kernel<<<dim3(trials, FIN_CHUNKS + 1, ns * split), 128, 0, s>>>(
+            d_z_part, d_ur_part, d_seg_panel0 + s0, d_seg_block0 + s0, d_v_enc, d_vsegs + s0, trials, split,
+            d_chunks + (uint64_t)s0 * trials * (FIN_CHUNKS + 1) * split);
     }
-    tc_decide_kernel<<<(nseg + 127) / 128, 128, 0, s>>>(d_ur, zv_chunks, nseg, trials, d_zv, d_failed);
+    tc_decide_kernel<<<nseg, DECIDE_WARPS * 32, 0, s>>>(d_chunks, trials, split, d_ur, d_zv, d_failed);
 }
 
 }  // namespace bn

@@ -107,10 +107,16 @@ void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32
 
 // Per segment: z_t = sum of its panels' partials, zv_t = z_t . v, ur_t =
 // sum of its blocks' partials; failed = first t with ur_t != zv_t or -1.
-// d_zv_chunks: scratch of nseg * trials * 8 words (per 128-column share of zv).
+// d_chunks: scratch of tc_finish_words(nseg, trials) words (the shares of z . v
+// and u . r that the finish kernel's CTAs write and the decide kernel sums).
+// With few segments each one's panels are split over tc_finish_split CTAs.
+inline uint32_t tc_finish_split(uint32_t nseg) { return nseg <= 4 ? 16u : 1u; }
+inline uint64_t tc_finish_words(uint32_t nseg, uint32_t trials) {
+    return (uint64_t)nseg * trials * (N / 128 + 1) * tc_finish_split(nseg);
+}
 void launch_tc_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part, const uint32_t* d_seg_panel0,
                       const uint32_t* d_seg_block0, const uint64_t* d_v_enc, const VerifySeg* d_vsegs, uint32_t nseg,
-                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, uint64_t* d_zv_chunks, int32_t* d_failed,
+                      uint32_t trials, uint64_t* d_ur, uint64_t* d_zv, uint64_t* d_chunks, int32_t* d_failed,
                       cudaStream_t s);
 
 }  // namespace bn
