@@ -850,10 +850,11 @@ def run_serving(args, flat, ivf, flat_L, data, dist):
                               [iseeds[i]], args.trials, 10)
         ref_i.append((h[0][0], h[0][1], int(ft[0])))
     qwait = args.serve_queue_wait_ms * 1000
-    srv = capi.Server(flat, ivf, max_batch=64, slots=4, mem_budget=24 << 30, max_wait_us=1000, trials=args.trials,
+    mb = args.serve_max_batch
+    srv = capi.Server(flat, ivf, max_batch=mb, slots=4, mem_budget=24 << 30, max_wait_us=1000, trials=args.trials,
                       k=10, block_min=2, queue_wait_us=qwait)
     out = {"corpora": {"flat_N": flat.m, "ivf_N": int(data["offsets"][-1]), "nlist": int(len(data["sizes"]))},
-           "config": {"max_batch": 64, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 2,
+           "config": {"max_batch": mb, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 2,
                       "queue_wait_us": qwait},
            "mix": "50% flat / 50% IVF, nprobe uniform in {8, 32, 128}",
            "warmup": "512 requests submitted at once before the timed rates (slots create their plans and "
@@ -937,6 +938,7 @@ def main():
     ap.add_argument("--ivf-rows", type=int, default=2_000_000, help="IVF corpus rows (0 to skip the IVF legs)")
     ap.add_argument("--serve-rates", default="2000,5000,10000,50000", help="Poisson arrival rates of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=1.5)
+    ap.add_argument("--serve-max-batch", type=int, default=256, help="serving: most queries per launched batch")
     ap.add_argument("--serve-queue-wait-ms", type=int, default=40,
                     help="serving admission: refuse a request when the queue's expected wait exceeds this (0: off)")
     args = ap.parse_args()

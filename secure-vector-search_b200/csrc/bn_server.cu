@@ -78,6 +78,10 @@ struct Slot {
     // block scoring of IVF batches (pairs grouped by list), in ws / host
     IvfBlockJob* ivj = nullptr;
     bool ivf_block_run = false;
+    // ivj holds the host plan of these requests (the first one's ticket and
+    // the count): planned while sizing the batch, reused by its launch
+    uint64_t ivj_ticket0 = 0;
+    size_t ivj_count = 0;
     ~Slot() {
         if (bp) block_plan_free(bp);
         if (ivj) ivf_block_job_free(ivj);
@@ -162,14 +166,25 @@ int ivf_block_plan_reqs(bn_server* s, It first, size_t count, IvfBlockJob& j) {
 }
 
 // Device workspace of a batch made of the first `count` requests of q (a
-// block plan's workspace when the batch runs as a block).
-uint64_t batch_bytes(bn_server* s, int kind, const std::deque<Request>& q, size_t count) {
+// block plan's workspace when the batch runs as a block).  An IVF block's
+// host plan is made in `me`'s job and kept for the launch.
+uint64_t batch_bytes(bn_server* s, int kind, const std::deque<Request>& q, size_t count, Slot* me) {
     if (kind == BN_SERVER_FLAT)
         if (const uint32_t bucket = block_bucket(s, count))
             return block_plan_estimate(s->flat, bucket, s->cfg.trials, s->cfg.k);
     if (kind == BN_SERVER_IVF && ivf_block(s, count)) {
-        std::unique_ptr<IvfBlockJob, void (*)(IvfBlockJob*)> j(ivf_block_job_new(), ivf_block_job_free);
-        if (ivf_block_plan_reqs(s, q.begin(), count, *j) == BN_OK) return ivf_block_job_bytes(j.get());
+        if (me) {
+            if (!me->ivj) me->ivj = ivf_block_job_new();
+            me->ivj_count = 0;
+            if (ivf_block_plan_reqs(s, q.begin(), count, *me->ivj) == BN_OK) {
+                me->ivj_ticket0 = q.front().ticket;
+                me->ivj_count = count;
+                return ivf_block_job_bytes(me->ivj);
+            }
+        } else {
+            std::unique_ptr<IvfBlockJob, void (*)(IvfBlockJob*)> j(ivf_block_job_new(), ivf_block_job_free);
+            if (ivf_block_plan_reqs(s, q.begin(), count, *j) == BN_OK) return ivf_block_job_bytes(j.get());
+        }
     }
     HostMeta hm;
     batch_meta(s, kind, q.begin(), q.begin() + count, hm);
@@ -284,7 +299,9 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
         // batch seed
         if (!sl.ivj) sl.ivj = ivf_block_job_new();
         Engine& e = s->ivf->e;
-        rc = ivf_block_plan_reqs(s, sl.reqs.begin(), B, *sl.ivj);
+        if (!(sl.ivj_count == B && sl.ivj_ticket0 == sl.reqs.front().ticket))  // not planned while sizing
+            rc = ivf_block_plan_reqs(s, sl.reqs.begin(), B, *sl.ivj);
+        sl.ivj_count = 0;
         if (rc == BN_OK)
             rc = ivf_block_pack(e, *sl.ivj, sl.ws, sl.host, v.data(), g.data(), ti.empty() ? nullptr : ti.data(),
                                 ts.empty() ? nullptr : ts.data(), tn.data(), bseed);
@@ -385,7 +402,7 @@ std::vector<Request> take_batch(bn_server* s, Slot& me, int& kind_out, bool& rej
     auto need = [&](size_t cnt) -> uint64_t {
         const uint32_t bucket = kind == BN_SERVER_FLAT ? block_bucket(s, cnt) : 0;
         if (bucket && me.bp && me.bp_B >= bucket) return me.ws.bytes + block_plan_bytes(me.bp);
-        const uint64_t own = batch_bytes(s, kind, q, cnt);
+        const uint64_t own = batch_bytes(s, kind, q, cnt, &me);
         return own + (bucket ? me.ws.bytes : (me.bp ? block_plan_bytes(me.bp) : 0));
     };
     size_t count = std::min<size_t>(q.size(), s->cfg.max_batch);
@@ -401,7 +418,7 @@ std::vector<Request> take_batch(bn_server* s, Slot& me, int& kind_out, bool& rej
                 sl->bp = nullptr;
                 sl->bp_B = 0;
             }
-            if (batch_bytes(s, kind, q, 1) + held_bytes(s) > budget) {
+            if (batch_bytes(s, kind, q, 1, nullptr) + held_bytes(s) > budget) {
                 reject_front = true;  // this request alone exceeds the budget
                 reject_kind = kind;
             } else {
