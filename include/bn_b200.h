@@ -438,6 +438,27 @@ int bn_debug_set_wait_limit(bn_ctx* ctx, uint64_t cycles);
  * encrypt_cluster (crypto.rs:405-478) on the device with host in/out:
  * m_enc = m_q + H L^T + S, a_l = m_q L.  Used to cross-check the device
  * encryption against a CPU restatement. */
+/* Key generation on the device (regenerate_h_s, crypto.rs:258-270): H
+ * (m x n1, row-major) and S (CSR) drawn from the cluster's h_seed with the
+ * same ChaCha20 stream positions as bn_host_regenerate_h_s, which they equal
+ * bit for bit; S is parsed in parallel (the column / sign draw structure
+ * scanned as a two-state machine).  S must fit in s_cap entries (*nnz gets
+ * the count either way; BN_EINVAL when it does not fit).  BN_EDRAW when an H
+ * draw equalled p (the reference redraws there; odds 2^-61 per draw): use the
+ * host keygen for that seed. */
+int bn_keygen_h_s(bn_ctx* ctx, const uint8_t h_seed[32], uint64_t m, uint32_t n1, uint64_t* H, uint64_t* s_rowptr,
+                  uint32_t* s_idx, int8_t* s_sign, uint64_t s_cap, uint64_t* nnz);
+/* bn_flat_build_from_plain with the keys drawn on the device from h_seed
+ * instead of passed in (BnTmScorer::upload_cluster, lib.rs:223-324 +
+ * crypto.rs:405-478, with only the plaintext and L crossing the bus). */
+int bn_flat_build_keygen(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1,
+                         const uint64_t* l_subspace, const uint8_t h_seed[32], bn_flat** out);
+/* bn_ivf_build_from_plain with every list's keys drawn on the device from
+ * its own h_seed = derive_h_seed(upload_seed, list) (ivf.rs:258-264,
+ * 627-653). */
+int bn_ivf_build_keygen(bn_ctx* ctx, uint32_t nlist, const uint64_t* list_offsets, const uint32_t* ids,
+                        const uint64_t* m_q, uint32_t n, uint32_t n1, const uint64_t* l_subspace,
+                        uint64_t upload_seed, bn_ivf** out);
 int bn_encrypt_cluster(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1,
                        const uint64_t* l_subspace, const uint64_t* h, bn_sparse_csr s_mat, uint64_t* m_enc,
                        uint64_t* a_l);

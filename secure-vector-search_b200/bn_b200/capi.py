@@ -108,6 +108,9 @@ _SIGS = {
     "bn_ivf_block_profile_read": (C.c_int, [vp, vp, u32, vp]),
     "bn_ivf_verify_block": (C.c_int, [vp, u32, u32, vp, vp, u64, vp, vp, u32, vp, vp, vp, vp]),
     "bn_encrypt_cluster": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, vp, vp]),
+    "bn_keygen_h_s": (C.c_int, [vp, vp, u64, u32, vp, vp, vp, vp, u64, vp]),
+    "bn_flat_build_keygen": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, vp]),
+    "bn_ivf_build_keygen": (C.c_int, [vp, u32, vp, vp, vp, u32, u32, vp, u64, vp]),
     "bn_server_create": (C.c_int, [vp, vp, C.POINTER(ServerConfig), vp]),
     "bn_server_submit_flat": (C.c_int, [vp, vp, vp, vp, vp, u32, vp, vp]),
     "bn_server_submit_ivf": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, u32, vp, vp]),
@@ -211,6 +214,15 @@ class Flat:
         m_enc, a_l, h = _u64(m_enc), _u64(a_l), _u64(h)
         out = vp()
         check(lib.bn_flat_build(ctx.h, ptr(m_enc), ptr(a_l), ptr(h), m, N, n1, C.byref(out)))
+        return cls(ctx, out, m, n1)
+
+    @classmethod
+    def build_keygen(cls, ctx, m_q, m, L, h_seed: bytes, n1=128):
+        """bn_flat_build_keygen: keys drawn on the device from h_seed."""
+        m_q, L = _u64(m_q), _u64(L)
+        seed = np.frombuffer(bytes(h_seed), np.uint8).copy()
+        out = vp()
+        check(lib.bn_flat_build_keygen(ctx.h, ptr(m_q), m, N, n1, ptr(L), ptr(seed), C.byref(out)))
         return cls(ctx, out, m, n1)
 
     @classmethod
@@ -420,6 +432,17 @@ class Ivf:
         return cls(ctx, out, off, n1)
 
     @classmethod
+    def build_keygen(cls, ctx, offsets, ids, m_q, L, upload_seed: int, n1=128):
+        """bn_ivf_build_keygen: every list's keys drawn on the device from derive_h_seed(upload_seed, list)."""
+        off = _u64(offsets)
+        ids = np.ascontiguousarray(ids, np.uint32)
+        m_q, L = _u64(m_q), _u64(L)
+        out = vp()
+        check(lib.bn_ivf_build_keygen(ctx.h, len(off) - 1, ptr(off), ptr(ids), ptr(m_q), N, n1, ptr(L), upload_seed,
+                                      C.byref(out)))
+        return cls(ctx, out, off, n1)
+
+    @classmethod
     def build_from_plain(cls, ctx, offsets, ids, m_q, L, H, s_rowptr, s_idx, s_sign, n1=128):
         off = _u64(offsets)
         ids = np.ascontiguousarray(ids, np.uint32)
@@ -626,6 +649,24 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def keygen_h_s(ctx, h_seed: bytes, m: int, n1: int = 128):
+    """bn_keygen_h_s: (H, rowptr, idx, sign) drawn on the device."""
+    seed = np.frombuffer(bytes(h_seed), np.uint8).copy()
+    H = np.zeros(max(m * n1, 1), np.uint64)
+    rowptr = np.zeros(m + 1, np.uint64)
+    cap = max(m * 160, 1024)
+    nnz = u64(0)
+    while True:
+        idx = np.zeros(cap, np.uint32)
+        sign = np.zeros(cap, np.int8)
+        rc = lib.bn_keygen_h_s(ctx.h, ptr(seed), m, n1, ptr(H), ptr(rowptr), ptr(idx), ptr(sign), cap, C.byref(nnz))
+        if rc == BN_EINVAL and nnz.value > cap:
+            cap = nnz.value
+            continue
+        check(rc)
+        return H[: m * n1], rowptr, idx[: nnz.value], sign[: nnz.value]
 
 
 def encrypt_cluster(ctx, m_q, m, L, H, s_rowptr, s_idx, s_sign, n1=128):

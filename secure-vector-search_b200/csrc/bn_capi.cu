@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "bn_b200.h"
+#include "bn_host.h"
 #include "bn_internal.cuh"
 #include "bn_kernels.cuh"
 #include "bn_tc.cuh"
@@ -80,6 +81,36 @@ int device_colmajor(bn_ctx* ctx, const uint64_t* d_src, uint64_t rows, uint32_t 
     TRY(dst.alloc(ctx, rows * cols * 8));
     if (rows) launch_transpose_u64(d_src, rows, cols, dst.at<uint64_t>(), rows, s);
     CU(cudaGetLastError());
+    return BN_OK;
+}
+
+// Sliced ELL of S from its row pointers (host, for the slice widths) and
+// its entries already on the device.
+int ell_from_device_csr(bn_ctx* ctx, const uint64_t* h_rowptr, const uint64_t* d_rowptr, const uint32_t* d_idx,
+                        const int8_t* d_sign, uint64_t rows, Corpus& c, cudaStream_t s) {
+    const uint64_t slices = (rows + 31) / 32;
+    std::vector<uint16_t> w(std::max<uint64_t>(slices, 1), 0);
+    std::vector<uint32_t> off(std::max<uint64_t>(slices, 1), 0);
+    uint64_t total = 0;
+    for (uint64_t sl = 0; sl < slices; ++sl) {
+        uint64_t mx = 0;
+        for (uint64_t i = sl * 32; i < std::min(rows, sl * 32 + 32); ++i) mx = std::max<uint64_t>(mx, h_rowptr[i + 1] - h_rowptr[i]);
+        if (mx > N) return fail(BN_EINVAL, "S row with %llu entries exceeds n", (unsigned long long)mx);
+        w[sl] = (uint16_t)mx;
+        off[sl] = (uint32_t)total;
+        total += mx * 32;
+        if (total > 0xffffffffull) return fail(BN_EINVAL, "S too large for the sliced-ELL layout");
+    }
+    TRY(c.s_ell.alloc(ctx, std::max<uint64_t>(total, 1) * 2));
+    TRY(c.s_off.alloc(ctx, off.size() * 4));
+    TRY(c.s_w.alloc(ctx, w.size() * 2));
+    CU(cudaMemcpyAsync(c.s_off.p, off.data(), off.size() * 4, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(c.s_w.p, w.data(), w.size() * 2, cudaMemcpyHostToDevice, s));
+    if (rows)
+        launch_csr_to_ell(d_rowptr, d_idx, d_sign, rows, c.s_off.at<uint32_t>(), c.s_w.at<uint16_t>(),
+                          c.s_ell.at<uint16_t>(), s);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(s));
     return BN_OK;
 }
 
@@ -174,6 +205,23 @@ int attach_client(bn_ctx* ctx, Corpus& c, const uint64_t* L, const uint64_t* m_p
 
 // Device encryption: m_enc = m_q + H L^T + S (row-major, stays on device in
 // `m_enc`), AL = m_q L (row-major in `al_rm`).  crypto.rs:405-478.
+int device_encrypt_dev(bn_ctx* ctx, const uint64_t* d_mq, uint64_t rows, uint32_t n1, const uint64_t* d_L,
+                       const uint64_t* d_H, const uint64_t* d_rowptr, const uint32_t* d_idx, const int8_t* d_sign,
+                       DevMem& m_enc, DevMem& al_rm, cudaStream_t s) {
+    TRY(m_enc.alloc(ctx, rows * N * 8));
+    TRY(al_rm.alloc(ctx, rows * n1 * 8));
+    if (!rows) return BN_OK;
+    launch_gemm_abt(d_H, d_L, d_mq, rows, N, n1, m_enc.at<uint64_t>(), s);  // H L^T + M
+    launch_apply_sparse(d_rowptr, d_idx, d_sign, rows, N, m_enc.at<uint64_t>(), s);  // + S
+    DevMem lt;  // AL = M L: B operand is L^T (n1 x n), K = n
+    TRY(lt.alloc(ctx, (uint64_t)n1 * N * 8));
+    launch_transpose_u64(d_L, N, n1, lt.at<uint64_t>(), N, s);
+    launch_gemm_abt(d_mq, lt.at<uint64_t>(), nullptr, rows, n1, N, al_rm.at<uint64_t>(), s);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(s));
+    return BN_OK;
+}
+
 int device_encrypt(bn_ctx* ctx, const uint64_t* d_mq, uint64_t rows, uint32_t n1, const uint64_t* d_L,
                    const uint64_t* d_H, bn_sparse_csr S, DevMem& m_enc, DevMem& al_rm, cudaStream_t s) {
     TRY(m_enc.alloc(ctx, rows * N * 8));
@@ -245,6 +293,100 @@ int build_corpus_from_plain(bn_ctx* ctx, Corpus& c, const uint64_t* m_q, uint64_
     CU(cudaStreamSynchronize(s));
     TRY(build_decode_layout(ctx, c, s));
     c.client = true;
+    return BN_OK;
+}
+
+// The sparsity threshold of sample_sparse_pm1 (crypto.rs:207-223): mu 2^32
+// in f64, truncated, as the host keygen computes it.
+uint32_t sparse_threshold() {
+    const double t = bn_host_mu() * 4294967296.0;
+    const uint64_t u = t <= 0.0 ? 0 : (uint64_t)t;
+    return (uint32_t)std::min<uint64_t>(u, 0xffffffffull);
+}
+
+// H and S of one cluster from its h_seed on the device (bn_keygen.cu):
+// H -> d_H (rows x n1), S -> d_rowptr (rows + 1, from 0), d_idx / d_sign
+// (at most cap entries); *nnz = S's entries.
+int device_keygen(bn_ctx* ctx, const uint8_t seed[32], uint64_t rows, uint32_t n1, uint64_t* d_H, uint64_t* d_rowptr,
+                  uint32_t* d_idx, int8_t* d_sign, uint64_t cap, DevMem& scratch, DevMem& status, uint64_t* nnz,
+                  cudaStream_t s) {
+    *nnz = 0;
+    if (!rows) return BN_OK;
+    TRY(scratch.reserve(ctx, keygen_s_scratch_bytes(rows, N)));
+    TRY(status.reserve(ctx, 16));
+    CU(cudaMemsetAsync(status.p, 0, 16, s));
+    uint32_t* st = status.at<uint32_t>();
+    launch_keygen_h(seed, rows * n1, d_H, st + 2, ctx->num_sms, s);
+    launch_keygen_s(seed, rows, N, n1, sparse_threshold(), scratch.p, cap, d_idx, d_sign, d_rowptr, st, s);
+    CU(cudaGetLastError());
+    uint32_t h[3];
+    CU(cudaMemcpyAsync(h, st, 12, cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(nnz, d_rowptr + rows, 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    if (!h[0] || h[1]) return fail(BN_EINVAL, "S has more entries than the keygen sizes for (m n / 4)");
+    if (h[2] & DRAW_HIT_P)
+        return fail(BN_EDRAW, "an H draw equalled p (regenerate_h_s redraws there, crypto.rs:155-162); draw this "
+                              "cluster's keys on the host (bn_host_regenerate_h_s)");
+    return BN_OK;
+}
+
+// Corpus from the plaintext with H and S already on the device: encryption,
+// client arrays and decode layouts (the device-resident form of
+// build_corpus_from_plain).
+int build_corpus_device_keys(bn_ctx* ctx, Corpus& c, const uint64_t* m_q, uint64_t rows, uint32_t n1,
+                             const uint64_t* L, DevMem& d_H, const uint64_t* h_rowptr, DevMem& d_rowptr, DevMem& d_idx,
+                             DevMem& d_sign, cudaStream_t s) {
+    c.rows = rows;
+    c.n1 = n1;
+    DevMem d_mq, d_L, al_rm;
+    TRY(d_mq.alloc(ctx, rows * N * 8));
+    TRY(d_L.alloc(ctx, (uint64_t)N * n1 * 8));
+    if (rows) CU(cudaMemcpyAsync(d_mq.p, m_q, rows * N * 8, cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(d_L.p, L, (uint64_t)N * n1 * 8, cudaMemcpyHostToDevice, s));
+    TRY(device_encrypt_dev(ctx, d_mq.at<uint64_t>(), rows, n1, d_L.at<uint64_t>(), d_H.at<uint64_t>(),
+                           d_rowptr.at<uint64_t>(), d_idx.at<uint32_t>(), d_sign.at<int8_t>(), c.m_enc, al_rm, s));
+    TRY(corpus_tmap(c));
+    TRY(device_colmajor(ctx, al_rm.at<uint64_t>(), rows, n1, c.al_cm, s));
+    TRY(device_colmajor(ctx, d_H.at<uint64_t>(), rows, n1, c.h_cm, s));
+    TRY(device_colmajor(ctx, d_mq.at<uint64_t>(), rows, N, c.mp_cm, s));
+    CU(cudaStreamSynchronize(s));
+    TRY(c.L.alloc(ctx, (uint64_t)N * n1 * 8));
+    CU(cudaMemcpyAsync(c.L.p, L, (uint64_t)N * n1 * 8, cudaMemcpyHostToDevice, s));
+    TRY(ell_from_device_csr(ctx, h_rowptr, d_rowptr.at<uint64_t>(), d_idx.at<uint32_t>(), d_sign.at<int8_t>(), rows, c,
+                            s));
+    TRY(build_decode_layout(ctx, c, s));
+    c.client = true;
+    return BN_OK;
+}
+
+// Keys of `lists` clusters (list c owns rows [off[c], off[c+1]) and has
+// seed seeds[c]) drawn on the device into one H and one concatenated CSR.
+int keygen_lists(bn_ctx* ctx, uint32_t lists, const uint64_t* off, const uint8_t* seeds, uint32_t n1, DevMem& H,
+                 DevMem& rowptr, DevMem& idx, DevMem& sign, std::vector<uint64_t>& h_rowptr, cudaStream_t s) {
+    const uint64_t rows = off[lists];
+    const uint64_t cap = rows * N / 4 + 1024;
+    TRY(H.alloc(ctx, std::max<uint64_t>(rows * n1, 1) * 8));
+    TRY(rowptr.alloc(ctx, (rows + 1) * 8));
+    TRY(idx.alloc(ctx, cap * 4));
+    TRY(sign.alloc(ctx, cap));
+    DevMem scratch, status, local;
+    uint64_t base = 0, max_rows = 0;
+    for (uint32_t c = 0; c < lists; ++c) max_rows = std::max(max_rows, off[c + 1] - off[c]);
+    TRY(local.alloc(ctx, (max_rows + 1) * 8));
+    CU(cudaMemsetAsync(rowptr.p, 0, 8, s));
+    for (uint32_t c = 0; c < lists; ++c) {
+        const uint64_t o = off[c], m = off[c + 1] - o;
+        if (!m) continue;
+        uint64_t nnz = 0;
+        TRY(device_keygen(ctx, seeds + 32ull * c, m, n1, H.at<uint64_t>() + o * n1, local.at<uint64_t>(),
+                          idx.at<uint32_t>() + base, sign.at<int8_t>() + base, cap - base, scratch, status, &nnz, s));
+        launch_rowptr_shift(local.at<uint64_t>(), m + 1, base, rowptr.at<uint64_t>() + o, s);
+        base += nnz;
+    }
+    CU(cudaGetLastError());
+    h_rowptr.resize(rows + 1);
+    CU(cudaMemcpyAsync(h_rowptr.data(), rowptr.p, (rows + 1) * 8, cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
     return BN_OK;
 }
 
@@ -1429,6 +1571,104 @@ int bn_ivf_query(bn_ivf* v, uint32_t B, uint32_t nprobe, const uint32_t* probes,
 }
 
 // ---------------------------------------------------------------- keygen
+int bn_keygen_h_s(bn_ctx* ctx, const uint8_t* h_seed, uint64_t m, uint32_t n1, uint64_t* H, uint64_t* s_rowptr,
+                  uint32_t* s_idx, int8_t* s_sign, uint64_t s_cap, uint64_t* nnz) {
+    if (!ctx || !h_seed || !nnz || (m && (!H || !s_rowptr))) return fail(BN_EINVAL, "null argument");
+    TRY(check_shape(N, n1));
+    *nnz = 0;
+    if (!m) {
+        if (s_rowptr) s_rowptr[0] = 0;
+        return BN_OK;
+    }
+    CU(cudaSetDevice(ctx->device));
+    cudaStream_t s;
+    CU(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int rc = BN_OK;
+    {
+        DevMem dH, rp, ix, sg;
+        std::vector<uint64_t> hrp;
+        const uint64_t off[2] = {0, m};
+        rc = keygen_lists(ctx, 1, off, h_seed, n1, dH, rp, ix, sg, hrp, s);
+        if (rc == BN_OK) {
+            *nnz = hrp[m];
+            if (hrp[m] > s_cap) {
+                rc = fail(BN_EINVAL, "S has %llu entries, more than s_cap = %llu", (unsigned long long)hrp[m],
+                          (unsigned long long)s_cap);
+            } else {
+                memcpy(s_rowptr, hrp.data(), (m + 1) * 8);
+                cudaError_t e = cudaMemcpyAsync(H, dH.p, m * n1 * 8, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess && hrp[m]) e = cudaMemcpyAsync(s_idx, ix.p, hrp[m] * 4, cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess && hrp[m]) e = cudaMemcpyAsync(s_sign, sg.p, hrp[m], cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                if (e != cudaSuccess) rc = fail(BN_ECUDA, "keygen copy-back: %s", cudaGetErrorString(e));
+            }
+        }
+    }
+    cudaStreamDestroy(s);
+    return rc;
+}
+
+int bn_flat_build_keygen(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1, const uint64_t* L,
+                         const uint8_t* h_seed, bn_flat** out) {
+    if (!ctx || !out || !h_seed || !L || (m && !m_q)) return fail(BN_EINVAL, "null argument");
+    *out = nullptr;
+    TRY(check_shape(n, n1));
+    if (m > 0xffffffffull) return fail(BN_EINVAL, "cluster size must fit in u32");
+    TRY(validate_residues(m_q, m * N, "m_q"));
+    TRY(validate_residues(L, (uint64_t)N * n1, "l_subspace"));
+    auto* f = new bn_flat();
+    int rc = engine_init(f->e, ctx);
+    f->m = m;
+    if (rc == BN_OK) {
+        DevMem H, rp, ix, sg;
+        std::vector<uint64_t> hrp;
+        const uint64_t off[2] = {0, m};
+        rc = keygen_lists(ctx, 1, off, h_seed, n1, H, rp, ix, sg, hrp, f->e.stream);
+        if (rc == BN_OK) rc = build_corpus_device_keys(ctx, f->e.c, m_q, m, n1, L, H, hrp.data(), rp, ix, sg, f->e.stream);
+    }
+    if (rc != BN_OK) {
+        engine_free(f->e);
+        delete f;
+        return rc;
+    }
+    *out = f;
+    return BN_OK;
+}
+
+int bn_ivf_build_keygen(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const uint32_t* ids, const uint64_t* m_q,
+                        uint32_t n, uint32_t n1, const uint64_t* L, uint64_t upload_seed, bn_ivf** out) {
+    if (!ctx || !out || !L) return fail(BN_EINVAL, "null argument");
+    *out = nullptr;
+    TRY(check_shape(n, n1));
+    TRY(check_offsets(nlist, off));
+    const uint64_t rows = off[nlist];
+    if (rows && (!ids || !m_q)) return fail(BN_EINVAL, "null corpus array");
+    TRY(validate_residues(m_q, rows * N, "m_q"));
+    TRY(validate_residues(L, (uint64_t)N * n1, "l_subspace"));
+    std::vector<uint8_t> seeds(32ull * std::max<uint32_t>(nlist, 1));
+    for (uint32_t c = 0; c < nlist; ++c) derive_h_seed(upload_seed, c, &seeds[32ull * c]);  // ivf.rs:258-264
+    auto* v = new bn_ivf();
+    int rc = engine_init(v->e, ctx);
+    v->nlist = nlist;
+    v->offsets.assign(off, off + nlist + 1);
+    if (rc == BN_OK) {
+        DevMem H, rp, ix, sg;
+        std::vector<uint64_t> hrp;
+        rc = keygen_lists(ctx, nlist, off, seeds.data(), n1, H, rp, ix, sg, hrp, v->e.stream);
+        if (rc == BN_OK) rc = build_corpus_device_keys(ctx, v->e.c, m_q, rows, n1, L, H, hrp.data(), rp, ix, sg, v->e.stream);
+    }
+    if (rc == BN_OK) rc = v->e.c.ids.alloc(ctx, std::max<uint64_t>(rows, 1) * 4);
+    if (rc == BN_OK && rows && cudaMemcpy(v->e.c.ids.p, ids, rows * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = fail(BN_ECUDA, "upload ids failed");
+    if (rc != BN_OK) {
+        engine_free(v->e);
+        delete v;
+        return rc;
+    }
+    *out = v;
+    return BN_OK;
+}
+
 int bn_encrypt_cluster(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1, const uint64_t* L,
                        const uint64_t* H, bn_sparse_csr S, uint64_t* m_enc, uint64_t* a_l) {
     if (!ctx) return fail(BN_EINVAL, "null ctx");

@@ -190,6 +190,22 @@ void launch_topk_segs(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* 
                       uint32_t nq, const uint32_t* d_ids, uint32_t k, int ctas_per_query, TopkScratch scratch,
                       uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n, cudaStream_t s);
 
+// Keygen on the device (regenerate_h_s, crypto.rs:258-270) from a cluster's
+// h_seed: H = the first `count` = m * n1 draws (sample_fp; DRAW_HIT_P in
+// *d_flags if one equalled p), row-major.
+void launch_keygen_h(const uint8_t seed[32], uint64_t count, uint64_t* d_H, uint32_t* d_flags, int num_sms,
+                     cudaStream_t s);
+// S as CSR: d_rowptr (m + 1, from 0), d_idx / d_sign (at most cap entries,
+// in row order, columns ascending).  d_scratch: keygen_s_scratch_bytes(m, n).
+// d_status[0] = 1 when the scanned keystream held all m * n column draws,
+// d_status[1] = 1 when S had more than cap entries (both zeroed by the caller).
+uint64_t keygen_s_scratch_bytes(uint64_t m, uint32_t n);
+void launch_keygen_s(const uint8_t seed[32], uint64_t m, uint32_t n, uint32_t n1, uint32_t thr, void* d_scratch,
+                     uint64_t cap, uint32_t* d_idx, int8_t* d_sign, uint64_t* d_rowptr, uint32_t* d_status,
+                     cudaStream_t s);
+// d_dst[i] = base + d_src[i], i < count (one list's row pointers in a concatenated CSR).
+void launch_rowptr_shift(const uint64_t* d_src, uint64_t count, uint64_t base, uint64_t* d_dst, cudaStream_t s);
+
 // Keygen-side dense F_p GEMM: C[i][j] = sum_k A[i][k] * B[j][k]  (A: rows x K,
 // B: cols x K, both row-major), optionally C += D (same shape, row-major).
 // K must be a multiple of 16 and at most 1024.
