@@ -176,19 +176,19 @@ def synth_ivf_queries(data, nq: int, seed: int):
 
 
 def build_ivf(ctx, data, seed: int):
-    """BN-encrypts every list on the device (per-list h_seed, ivf.rs:258-264)."""
+    """Keys (per-list h_seed, ivf.rs:258-264) and encryption of every list on
+    the device (bn_ivf_build_keygen)."""
     from bn_b200 import capi
 
     rows = int(data["offsets"][-1])
     L = capi.host_generate_subspace(bytes([seed & 0xFF, 0x1F]) * 16)
     data["L"] = L
-    H, rp, ix, sg = capi.host_regenerate_h_s_lists(seed, data["offsets"])
     mq = np.zeros((rows, N_DIM), np.uint64)
     blk = 1 << 18
     for r0 in range(0, rows, blk):
         mq[r0 : r0 + blk] = to_residues(data["m8"][r0 : r0 + blk])
-    ivf = capi.Ivf.build_from_plain(ctx, data["offsets"], data["ids"], mq.reshape(-1), L, H, rp, ix, sg)
-    del mq, H, rp, ix, sg
+    ivf = capi.Ivf.build_keygen(ctx, data["offsets"], data["ids"], mq.reshape(-1), L, seed)
+    del mq
     return ivf
 
 
