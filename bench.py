@@ -864,10 +864,17 @@ def run_serving(args, flat, ivf, flat_L, data, dist):
     warm = []
     for j in range(512):
         i = j % pool
-        if j & 1:
-            warm.append(srv.submit_flat(fenc[i][0], fenc[i][1], fenc[i][2], fenc[i][3], fseeds[i]))
-        else:
-            warm.append(srv.submit_ivf(probes[i], ienc[i][0], ienc[i][1], ienc[i][2], ienc[i][3], iseeds[i]))
+        while True:  # a refused submit (queue admission) waits for the oldest request, then retries
+            try:
+                if j & 1:
+                    warm.append(srv.submit_flat(fenc[i][0], fenc[i][1], fenc[i][2], fenc[i][3], fseeds[i]))
+                else:
+                    warm.append(srv.submit_ivf(probes[i], ienc[i][0], ienc[i][1], ienc[i][2], ienc[i][3], iseeds[i]))
+                break
+            except capi.BnError as err:
+                if err.code != capi.BN_EAGAIN or not warm:
+                    raise
+                srv.wait(warm.pop(0), 600000)
     for t in warm:
         srv.wait(t, 600000)
     for rate in [float(r) for r in args.serve_rates.split(",") if r]:

@@ -192,7 +192,10 @@ class Context:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
 
 
 def _t_concat(enc_list):
@@ -365,7 +368,10 @@ class Flat:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
 
 
 class Plan:
@@ -411,7 +417,10 @@ class Plan:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
 
 
 class Ivf:
@@ -593,7 +602,10 @@ class Ivf:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
 
 
 class Server:
@@ -648,7 +660,10 @@ class Server:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
 
 
 def keygen_h_s(ctx, h_seed: bytes, m: int, n1: int = 128):
@@ -863,7 +878,10 @@ class IvfCache:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
 
 
 def ivf_from_cache(ctx, path: str, fingerprint: int = 0, n1: int = 128):

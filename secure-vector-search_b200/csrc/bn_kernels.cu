@@ -16,8 +16,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <cstdlib>
-
 #include "bn_kernels.cuh"
 
 namespace bn {
@@ -87,20 +85,30 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // the CTA's own copies keeps the full limit).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit = WAIT_CYCLES) {
     const long long t0 = clock64();
-    while (!mbar_try_wait(bar, parity))
+    if (limit >= WAIT_CYCLES) {
+        while (!mbar_try_wait(bar, parity))
+            if (clock64() - t0 > limit) return false;
+        return true;
+    }
+    // a shortened (test) limit also bounds each try_wait's suspension (its
+    // suspendTimeHint, in ns), which could otherwise outlast the limit
+    const uint32_t ns = (uint32_t)(limit / 2 > 1 ? limit / 2 : 1);
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+            : "memory");
+        if (ok) return true;
         if (clock64() - t0 > limit) return false;
-    return true;
+    }
 }
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-// L2 prefetch of a contiguous range (address and size multiples of 16 bytes);
-// nothing is written to shared memory and nothing has to be waited for.
-__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     asm volatile(
@@ -774,7 +782,7 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
                    const uint64_t* __restrict__ vv, const uint64_t* __restrict__ gg, const uint64_t* __restrict__ xx,
                    const uint32_t* __restrict__ t_ent, const uint32_t* __restrict__ t_nnz, uint32_t k, TopkScratch ts,
                    uint64_t* __restrict__ mv_out, uint32_t* __restrict__ out_ids, int64_t* __restrict__ out_scores,
-                   uint32_t* __restrict__ out_n, uint32_t nq, uint32_t prefetch) {
+                   uint32_t* __restrict__ out_n, uint32_t nq) {
     uint32_t lo = 0, hi = nq;  // the query owning this CTA: last one with cta0 <= blockIdx.x
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
@@ -829,13 +837,6 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
             }
             const ScanSeg sg = segs[sa];
             const uint64_t blk = (sg.row0 >> 5) + (gu - seg_unit[sa]);
-            if (prefetch && lane == 0) {
-                // the unit's block-contiguous runs into L2 at once: its [AL | H]
-                // block (2 n1 x 32 words) and its S slice
-                bulk_prefetch_l2(dc.alh_b + blk * (2ull * n1) * 32, 2u * n1 * 32u * 8u);
-                const uint32_t w = dc.s_w[blk];
-                if (w) bulk_prefetch_l2(dc.s_ell + dc.s_off[blk], 64u * w);
-            }
             const uint64_t gr = blk * 32 + lane;
             valid = gr >= sg.row0 && gr < sg.row0 + sg.rows;
             const uint64_t ridx = sg.out0 + (gr - sg.row0);
@@ -1247,12 +1248,10 @@ void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanS
                         cudaStream_t s) {
     if (!nq) return;
     cudaFuncSetAttribute(decode_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 2 * 512 * 16);  // per device
-    const char* pf_env = getenv("BN_DECODE_PREFETCH");
-    const uint32_t pf = pf_env ? (uint32_t)atoi(pf_env) : 0u;
     cudaMemsetAsync(scratch.done, 0, (uint64_t)nq * 4, s);
     decode_topk_kernel<<<total_ctas, DT_THREADS, 2 * 2 * dc.n1 * 16, s>>>(d_r, dc, d_segs, d_seg_unit, d_q, d_v, d_g,
                                                                          d_x, d_t, d_t_nnz, k, scratch, d_mv_out,
-                                                                         d_out_ids, d_out_scores, d_out_n, nq, pf);
+                                                                         d_out_ids, d_out_scores, d_out_n, nq);
 }
 
 void launch_topk_rows(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_c, uint64_t ld, uint64_t rows,

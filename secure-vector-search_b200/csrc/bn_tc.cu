@@ -15,7 +15,6 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
-#include <cstdlib>
 
 #include "bn_tc.cuh"
 #include "bn_tcgen05.cuh"
@@ -595,10 +594,10 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 const __grid_constant__ CUtensorMap tmap_w, const TcPanel* __restrict__ panels, uint32_t npanels,
                 const VerifySeg* __restrict__ vsegs, uint32_t t_cnt, uint32_t n_rows, uint32_t trials_total,
                 uint32_t stages, uint32_t stage_bytes, uint64_t* __restrict__ z_part, uint64_t* __restrict__ r_part,
-                uint64_t r_stride, uint32_t* __restrict__ err, long long wait_limit, uint32_t pf_dist) {
+                uint64_t r_stride, uint32_t* __restrict__ err, long long wait_limit) {
     constexpr int S = FU_S;
     extern __shared__ uint8_t tc_dyn[];
-    __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b, racc_b[2], rfree_b[2];
+    __shared__ uint64_t full_b[4], empty_b[4], accf_b, acce_b, done_b, racc_b[2], rfree_b[2], wfull_b[2], wfree_b[2];
     __shared__ uint32_t tmem_base_s;
     __shared__ volatile int abort_s;
 
@@ -607,8 +606,11 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t u_off = S * STRIP_BYTES;
     const uint32_t u_bytes = n_rows * TC_ROWS;
-    const uint32_t w_off = u_off + u_bytes;  // 1024-aligned: n_rows is a multiple of 16
+    // the query's diagonal image of an item's strip group: loaded once per item
+    // into one of two buffers behind the stage ring (1024-aligned: stage_bytes
+    // and w_bytes are multiples of 1024)
     const uint32_t w_bytes = S * W_STRIP_BYTES;
+    const uint32_t w_ring = stages * stage_bytes;
     const uint32_t groups = (64 + S - 1) / S;
     const uint32_t items = npanels * groups;
 
@@ -623,6 +625,8 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
         for (int e = 0; e < 2; ++e) {
             bar_init(&racc_b[e], 1);
             bar_init(&rfree_b[e], FU_DRAIN_WARPS);
+            bar_init(&wfull_b[e], 1);
+            bar_init(&wfree_b[e], 1);
         }
         abort_s = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -641,32 +645,25 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
     if (warp == 0) {
         if (lane == 0) {  // ------------------------------------------ TMA producer
             uint64_t it = 0;
+            uint32_t ic = 0, w_issued = 0;  // items started, W images loaded
             bool stop = false;
-            // L2 prefetch of the m_enc boxes of the load pf_dist loads ahead
-            // (loads past the first `stages`, which go out at once): the
-            // stage ring holds three loads, the prefetches keep pf_dist more
-            // in flight from DRAM.  (pf_item, pf_rb) is load number pf_pos.
-            uint32_t pf_item = blockIdx.x, pf_rb = 0;
-            uint64_t pf_pos = 0;
-            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
+            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x, ++ic) {
                 const uint32_t p = item / groups, g = item % groups;
                 const TcPanel pn = panels[p];
                 const uint32_t query = vsegs[pn.seg].query;
                 const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
                 const uint32_t sg = min((uint32_t)S, 64u - g * S);
+                const uint32_t ib = ic & 1;  // W buffer of this item: free once item ic - 2's r MMAs are done
+                if (ic >= 2 && !bar_wait(&wfree_b[ib], ((ic >> 1) - 1) & 1, wait_limit)) {
+                    abort_s = 1;
+                    atomicOr(err, 4u);
+                    break;
+                }
+                if (abort_s) break;
+                bar_expect_tx(&wfull_b[ib], w_bytes);
+                tma_2d(ring + w_ring + ib * w_bytes, &tmap_w, 0, (int)((query * 64 + g * S) * 16), &wfull_b[ib]);
+                ++w_issued;
                 for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
-                    while (pf_dist && pf_pos <= it + pf_dist && pf_item < items) {
-                        const uint32_t pp = pf_item / groups, pg = pf_item % groups;
-                        const TcPanel ppn = panels[pp];
-                        if (pf_pos >= stages)
-                            for (uint32_t s = 0; s < min((uint32_t)S, 64u - pg * S); ++s)
-                                tma_prefetch_2d(&tmap_m, (int)((pg * S + s) * 128), (int)(ppn.row0 + pf_rb * TC_ROWS));
-                        ++pf_pos;
-                        if (++pf_rb == (ppn.rows + TC_ROWS - 1) / TC_ROWS) {
-                            pf_rb = 0;
-                            pf_item += gridDim.x;
-                        }
-                    }
                     const uint32_t st = (uint32_t)(it % stages);
                     if (it >= stages && !bar_wait(&empty_b[st], (uint32_t)(((it / stages) - 1) & 1), wait_limit)) {
                         abort_s = 1;
@@ -676,16 +673,19 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                     }
                     if (abort_s) { stop = true; break; }
                     uint8_t* sb = ring + (uint64_t)st * stage_bytes;
-                    bar_expect_tx(&full_b[st], sg * STRIP_BYTES + u_bytes + w_bytes);
+                    bar_expect_tx(&full_b[st], sg * STRIP_BYTES + u_bytes);
                     for (uint32_t s = 0; s < sg; ++s)
                         tma_2d(sb + s * STRIP_BYTES, &tmap_m, (int)((g * S + s) * 128), (int)(pn.row0 + rb * TC_ROWS),
                                &full_b[st]);
                     tma_2d(sb + u_off, &tmap_u, 0, (int)((pn.rb0 + rb) * n_rows), &full_b[st]);
-                    tma_2d(sb + w_off, &tmap_w, 0, (int)((query * 64 + g * S) * 16), &full_b[st]);
                 }
             }
+            // no copy may still be landing in shared memory when the CTA exits:
+            // the last ring stages and the W images of the last two items
             for (uint64_t j = it > stages ? it - stages : 0; j < it; ++j)
                 bar_wait(&full_b[j % stages], (uint32_t)((j / stages) & 1));
+            for (uint32_t x = w_issued > 2 ? w_issued - 2 : 0; x < w_issued; ++x)
+                bar_wait(&wfull_b[x & 1], (x >> 1) & 1);
         }
     } else if (warp == 1) {
         if (lane == 0) {  // ------------------------------------------ z MMA issuer
@@ -730,12 +730,20 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
         if (lane == 0) {  // ------------------------------------------ r MMA issuer
             const uint32_t idesc_r = (2u << 4) | ((16u >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
             uint64_t it = 0;
+            uint32_t ic = 0;
             bool stop = false;
-            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x) {
+            for (uint32_t item = blockIdx.x; item < items && !stop; item += gridDim.x, ++ic) {
                 const uint32_t p = item / groups, g = item % groups;
                 const TcPanel pn = panels[p];
                 const uint32_t nrb = (pn.rows + TC_ROWS - 1) / TC_ROWS;
                 const uint32_t sg = min((uint32_t)S, 64u - g * S);
+                const uint32_t ib = ic & 1;
+                if (!bar_wait(&wfull_b[ib], (ic >> 1) & 1, wait_limit) || abort_s) {
+                    abort_s = 1;
+                    atomicOr(err, 8u);
+                    break;
+                }
+                const uint32_t wb = base + w_ring + ib * w_bytes;
                 for (uint32_t rb = 0; rb < nrb; ++rb, ++it) {
                     const uint32_t st = (uint32_t)(it % stages), eb = (uint32_t)(it & 1);
                     if (!bar_wait(&full_b[st], (uint32_t)((it / stages) & 1), wait_limit) || abort_s ||
@@ -751,10 +759,12 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
 #pragma unroll
                         for (uint32_t ks = 0; ks < TC_ROWS / 32; ++ks)  // strip read K-major
                             mma_i8(tmem + FU_E_COL + 16 * eb, sdesc(sb + s * STRIP_BYTES + ks * 32u, 16, 1024),
-                                   sdesc(sb + w_off + s * W_STRIP_BYTES + ks * 32u, 16, 1024), idesc_r, (s | ks) != 0);
+                                   sdesc(wb + s * W_STRIP_BYTES + ks * 32u, 16, 1024), idesc_r, (s | ks) != 0);
                     mma_commit(&empty_b[st]);
                     mma_commit(&racc_b[eb]);  // the stage's row products are ready for the drain warps
                 }
+                if (stop) break;
+                mma_commit(&wfree_b[ib]);  // W buffer reusable once this item's r MMAs have read it
             }
             mma_commit(&done_b);
             if (!bar_wait(&done_b, 0)) atomicOr(err, 64u);  // every issued MMA has finished
@@ -1068,19 +1078,17 @@ void launch_tc_fused(const CUtensorMap& tmap_m, const CUtensorMap& tmap_u, const
                      uint32_t* d_err, int num_sms, cudaStream_t s, long long wait_cycles) {
     if (!npanels) return;
     const long long wl = wait_cycles > 0 ? wait_cycles : TC_WAIT_CYCLES;
-    const uint32_t stage_bytes = (uint32_t)FU_S * STRIP_BYTES + ((n_rows * TC_ROWS + 1023u) & ~1023u) +
-                                 (uint32_t)FU_S * W_STRIP_BYTES;
-    uint32_t stages = (227u * 1024u - 2048u) / stage_bytes;
+    const uint32_t stage_bytes = (uint32_t)FU_S * STRIP_BYTES + ((n_rows * TC_ROWS + 1023u) & ~1023u);
+    const uint32_t w_two = 2u * FU_S * W_STRIP_BYTES;  // the two per-item W buffers
+    uint32_t stages = (227u * 1024u - 2048u - w_two) / stage_bytes;
     stages = stages < 2 ? 2 : (stages > 4 ? 4 : stages);
-    const int smem = (int)(stages * stage_bytes + 1024);
+    const int smem = (int)(stages * stage_bytes + w_two + 1024);
     const uint32_t items = npanels * ((64 + FU_S - 1) / FU_S);
     const unsigned grid = items < (uint32_t)num_sms ? items : (unsigned)num_sms;
     cudaFuncSetAttribute(tc_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    const char* pf_env = getenv("BN_FUSED_PREFETCH");
-    const uint32_t pf = pf_env ? (uint32_t)atoi(pf_env) : 0u;
     tc_fused_kernel<<<grid, FU_THREADS, smem, s>>>(tmap_m, tmap_u, tmap_w, d_panels, npanels, d_vsegs, t_cnt, n_rows,
                                                    trials_total, stages, stage_bytes, d_z_part, d_r_part, r_stride,
-                                                   d_err, wl, pf);
+                                                   d_err, wl);
 }
 
 void launch_tc_rreduce(const VerifySeg* d_vsegs, const TcBlock* d_blocks, uint32_t nblocks, const uint64_t* d_r_part,

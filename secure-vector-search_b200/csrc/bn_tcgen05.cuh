@@ -26,13 +26,31 @@ static __device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// try_wait whose suspension is bounded by `ns` nanoseconds (its
+// suspendTimeHint) instead of the system-dependent window.
+static __device__ __forceinline__ bool bar_try_hint(uint64_t* b, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(su32(b)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
 // Bounded wait for the phase with `parity`: false after `limit` cycles.
 // Pipeline waits take the kernel's wait_limit argument (TC_WAIT_CYCLES unless
 // a test shortens it, bn_debug_set_wait_limit); the wind-down waits for a
-// CTA's own copies and MMAs always keep the full limit.
+// CTA's own copies and MMAs always keep the full limit.  A shortened limit
+// also bounds each try_wait's suspension, which could otherwise outlast it.
 static __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, long long limit = TC_WAIT_CYCLES) {
     const long long t0 = clock64();
-    while (!bar_try(b, parity))
+    if (limit >= TC_WAIT_CYCLES) {
+        while (!bar_try(b, parity))
+            if (clock64() - t0 > limit) return false;
+        return true;
+    }
+    const uint32_t ns = (uint32_t)(limit / 2 > 1 ? limit / 2 : 1);  // ~2 cycles per ns
+    while (!bar_try_hint(b, parity, ns))
         if (clock64() - t0 > limit) return false;
     return true;
 }
@@ -55,12 +73,6 @@ static __device__ __forceinline__ void tma_3d(void* dst, const CUtensorMap* map,
             su32(dst)),
         "l"(map), "r"(x), "r"(y), "r"(z), "r"(su32(b))
         : "memory");
-}
-// L2 prefetch of one box of a 2-D tensor map: no shared memory is written
-// and nothing completes, so nothing has to be waited for.
-static __device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int x, int y) {
-    asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(map), "r"(x), "r"(y)
-                 : "memory");
 }
 static __device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 static __device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
