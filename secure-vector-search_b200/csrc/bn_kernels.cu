@@ -90,15 +90,14 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long l
             if (clock64() - t0 > limit) return false;
         return true;
     }
-    // a shortened (test) limit also bounds each try_wait's suspension (its
-    // suspendTimeHint, in ns), which could otherwise outlast the limit
-    const uint32_t ns = (uint32_t)(limit / 2 > 1 ? limit / 2 : 1);
+    // a shortened (test) limit polls with test_wait: try_wait may stay
+    // suspended until the phase completes, which would outlast the limit
     for (;;) {
         uint32_t ok;
         asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+            "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(ok)
-            : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+            : "r"(smem_u32(bar)), "r"(parity)
             : "memory");
         if (ok) return true;
         if (clock64() - t0 > limit) return false;

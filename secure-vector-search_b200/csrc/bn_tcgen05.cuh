@@ -26,22 +26,22 @@ static __device__ __forceinline__ bool bar_try(uint64_t* b, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// try_wait whose suspension is bounded by `ns` nanoseconds (its
-// suspendTimeHint) instead of the system-dependent window.
-static __device__ __forceinline__ bool bar_try_hint(uint64_t* b, uint32_t parity, uint32_t ns) {
+// Non-blocking test of the phase with `parity` (test_wait never suspends).
+static __device__ __forceinline__ bool bar_test(uint64_t* b, uint32_t parity) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(su32(b)), "r"(parity), "r"(ns)
+        : "r"(su32(b)), "r"(parity)
         : "memory");
     return ok != 0;
 }
 // Bounded wait for the phase with `parity`: false after `limit` cycles.
 // Pipeline waits take the kernel's wait_limit argument (TC_WAIT_CYCLES unless
 // a test shortens it, bn_debug_set_wait_limit); the wind-down waits for a
-// CTA's own copies and MMAs always keep the full limit.  A shortened limit
-// also bounds each try_wait's suspension, which could otherwise outlast it.
+// CTA's own copies and MMAs always keep the full limit.  Under a shortened
+// limit the wait polls with test_wait: try_wait may stay suspended until the
+// phase completes, which would outlast a limit of a few hundred cycles.
 static __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, long long limit = TC_WAIT_CYCLES) {
     const long long t0 = clock64();
     if (limit >= TC_WAIT_CYCLES) {
@@ -49,8 +49,7 @@ static __device__ __forceinline__ bool bar_wait(uint64_t* b, uint32_t parity, lo
             if (clock64() - t0 > limit) return false;
         return true;
     }
-    const uint32_t ns = (uint32_t)(limit / 2 > 1 ? limit / 2 : 1);  // ~2 cycles per ns
-    while (!bar_try_hint(b, parity, ns))
+    while (!bar_test(b, parity))
         if (clock64() - t0 > limit) return false;
     return true;
 }
