@@ -539,6 +539,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     if args.config1:
         res["config1"] = run_config1(args, ctx, dev, stream, timed, rank, world)
         progress("config-1 leg done")
+    if args.stream_rows:
+        res["stream"] = run_stream(args, ctx)
+        progress("streaming leg done")
     ctx.close()
     return res
 
@@ -630,6 +633,61 @@ def run_config1(args, ctx, dev, stream, timed, rank, world):
         out["per_trials"][str(trials)] = rec
         plan.close()
     flat.close()
+    return out
+
+
+def run_stream(args, ctx):
+    """A flat corpus streamed through device memory (bn_stream): N rows in
+    chunks of C rows with a budget of S chunk slots, B queries per call.  A
+    call scores every chunk: the resident ones first while the others are
+    uploaded from pinned host memory into the slots of chunks already scored.
+    Timed end to end on the host clock (host inputs and outputs, every copy
+    inside); the first call's hits and verdicts are compared with a resident
+    flat corpus built from the same data."""
+    from bn_b200 import capi
+
+    n, d, seed, k, trials = args.stream_rows, 768, 11, 10, args.trials
+    chunk, slots = args.stream_chunk_rows, args.stream_slots
+    Mu = to_residues(synth_int8(n, d, seed))
+    L = capi.host_generate_subspace(bytes([seed]) * 32)
+    H, rp, ix, sg = capi.keygen_h_s(ctx, capi.host_derive_h_seed(seed, 0), n, 128)
+    # slot size from a one-chunk probe (+4 % for chunks with wider ELL slices)
+    probe = capi.Stream.build_from_plain(ctx, Mu[:chunk].reshape(-1), chunk, L, H[: chunk * 128], rp[: chunk + 1],
+                                         ix, sg, chunk, 1 << 42)
+    budget = int(slots * probe.info()["slot_bytes"] * 1.04)
+    probe.close()
+    t0 = time.perf_counter()
+    st = capi.Stream.build_from_plain(ctx, Mu.reshape(-1), n, L, H, rp, ix, sg, chunk, budget)
+    build_s = time.perf_counter() - t0
+    info = st.info()
+    nq = 64
+    x8 = synth_int8(nq, d, seed + 500)
+    encs, seeds = encode_pool(L, nq, x8, seed + 500)
+    out = {"N": n, "chunk_rows": chunk, "chunks": info["chunks"], "slots": info["slots"],
+           "slot_gib": info["slot_bytes"] / 2**30, "host_image_gib": info["host_bytes"] / 2**30,
+           "corpus_over_budget": info["chunks"] / max(info["slots"], 1), "build_s": build_s, "per_B": {}}
+    flat = capi.Flat.build_from_plain(ctx, Mu.reshape(-1), n, L, H, rp, ix, sg)
+    for B in (1, 16, 64):
+        a = (np.stack([e[0] for e in encs[:B]]), np.stack([e[1] for e in encs[:B]]),
+             [(e[2], e[3]) for e in encs[:B]], seeds[:B], trials, k)
+        got, gf = st.query(*a)  # warm-up call, checked against the resident corpus
+        want, wf, _, _ = flat.query(*a)
+        same = bool(np.array_equal(gf, wf) and np.all(gf == -1) and
+                    all(np.array_equal(got[b][0], want[b][0]) and np.array_equal(got[b][1], want[b][1])
+                        for b in range(B)))
+        st.stats(reset=True)
+        calls = 3
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            st.query(*a)
+        dt = time.perf_counter() - t0
+        s = st.stats()
+        out["per_B"][str(B)] = {"qps": B * calls / dt, "ms_per_call": dt / calls * 1e3,
+                                "uploads_per_call": s["uploads"] / calls,
+                                "gib_uploaded_per_call": s["bytes_uploaded"] / calls / 2**30,
+                                "h2d_gbs": s["bytes_uploaded"] / dt / 1e9, "hits_verdicts_equal_resident": same}
+    flat.close()
+    st.close()
     return out
 
 
@@ -861,10 +919,11 @@ def run_serving(args, flat, ivf, flat_L, data, dist):
            "config": {"max_batch": mb, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 2,
                       "queue_wait_us": qwait},
            "mix": "50% flat / 50% IVF, nprobe uniform in {8, 32, 128}",
-           "warmup": "512 requests submitted at once before the timed rates (slots create their plans and "
-                     "workspaces), not counted", "rates": {}}
-    # warm-up: the slots grow their block plans and workspaces to the largest
-    # batches once, as a service does at start-up
+           "warmup": "the server creates one flat block plan per block size at start-up; 512 requests "
+                     "submitted at once before the timed rates (the slots grow their workspaces), not counted",
+           "rates": {}}
+    # warm-up: the slots grow their workspaces to the largest batches once,
+    # as a service does at start-up
     warm = []
     for j in range(512):
         i = j % pool
@@ -882,7 +941,7 @@ def run_serving(args, flat, ivf, flat_L, data, dist):
     for t in warm:
         srv.wait(t, 600000)
     for rate in [float(r) for r in args.serve_rates.split(",") if r]:
-        n = int(min(max(rate * args.serve_seconds, 200), 8000))
+        n = int(min(max(rate * args.serve_seconds, 200), 16000))
         kinds = rng.random(n) < 0.5
         picks = rng.integers(0, pool, size=n)
         gaps = rng.exponential(1.0 / rate, size=n)
@@ -947,8 +1006,13 @@ def main():
     ap.add_argument("--no-block-autotune", dest="block_autotune", action="store_false",
                     help="block plans keep the default GEMM tiling (no autotuning launches)")
     ap.add_argument("--ivf-rows", type=int, default=2_000_000, help="IVF corpus rows (0 to skip the IVF legs)")
-    ap.add_argument("--serve-rates", default="2000,5000,10000,50000", help="Poisson arrival rates of the serving leg")
+    ap.add_argument("--serve-rates", default="1000,2000,4000,6000,8000,50000",
+                    help="Poisson arrival rates of the serving leg")
     ap.add_argument("--serve-seconds", type=float, default=1.5)
+    ap.add_argument("--stream-rows", type=int, default=262_144,
+                    help="rows of the streamed corpus (bn_stream, larger than its budget; 0 to skip)")
+    ap.add_argument("--stream-chunk-rows", type=int, default=32_768)
+    ap.add_argument("--stream-slots", type=int, default=3, help="chunk slots the streamed corpus's budget holds")
     ap.add_argument("--serve-max-batch", type=int, default=64, help="serving: most queries per launched batch")
     ap.add_argument("--serve-queue-wait-ms", type=int, default=40,
                     help="serving admission: refuse a request when the queue's expected wait exceeds this (0: off)")

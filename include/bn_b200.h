@@ -463,6 +463,58 @@ int bn_encrypt_cluster(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n,
                        const uint64_t* l_subspace, const uint64_t* h, bn_sparse_csr s_mat, uint64_t* m_enc,
                        uint64_t* a_l);
 
+/* ---------------------------------------------------------------- corpora larger than device memory
+ * Replaces the streaming cluster store (ClusterStore::get_or_upload,
+ * scorer-gpu-common/src/store.rs:247-395) as the flat scorer uses it
+ * (FlatGpuState, scorer-bntm/src/gpu/mod.rs:279-376): the corpus is cut
+ * into chunks of chunk_rows rows (a multiple of 32) whose device images stay
+ * in pinned host memory; device memory holds budget_bytes / slot_bytes chunk
+ * slots, kept least-recently-used, and a query uploads the chunks it misses
+ * on an upload stream while the resident ones are scored.  Results (hits,
+ * failed_trial) equal bn_flat_query's on the same corpus bit for bit: every
+ * chunk is scored as a row shard with its rows' Protocol 2 draw positions in
+ * the whole corpus.  BN_EBUDGET when the budget holds no slot (the
+ * reference's BudgetTooSmall).  Calls on one handle are serialised. */
+typedef struct bn_stream bn_stream;
+/* The store's counters (store.rs:36-80 ClusterStoreStats; gets counts one
+ * per chunk visited, uploads / bytes_uploaded the chunk images copied in). */
+typedef struct bn_store_stats {
+    uint64_t gets, uploads, evictions, bytes_uploaded;
+    uint64_t resident_bytes, budget_bytes;
+} bn_store_stats;
+/* From the encrypted corpus and the client state, as bn_flat_build followed
+ * by bn_flat_attach_client. */
+int bn_stream_build(bn_ctx* ctx, const uint64_t* m_enc, const uint64_t* a_l, const uint64_t* h, uint64_t m,
+                    uint32_t n, uint32_t n1, const uint64_t* l_subspace, const uint64_t* m_plain, bn_sparse_csr s_mat,
+                    uint64_t chunk_rows, uint64_t budget_bytes, bn_stream** out);
+/* From the quantised plaintext and the keys, as bn_flat_build_from_plain
+ * (each chunk encrypted on the device). */
+int bn_stream_build_from_plain(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1,
+                               const uint64_t* l_subspace, const uint64_t* h, bn_sparse_csr s_mat,
+                               uint64_t chunk_rows, uint64_t budget_bytes, bn_stream** out);
+int bn_stream_info(const bn_stream* st, uint64_t* rows, uint32_t* chunks, uint32_t* slots, uint64_t* slot_bytes,
+                   uint64_t* host_bytes);
+/* bn_flat_query over the streamed corpus (same arguments and outputs). */
+int bn_stream_query(bn_stream* st, uint32_t B, const uint64_t* v_enc, const uint64_t* g, const uint32_t* t_idx,
+                    const int8_t* t_sign, const uint32_t* t_nnz, const uint8_t* v_seeds, uint32_t trials, uint32_t k,
+                    uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed_trial);
+int bn_stream_stats(bn_stream* st, int reset, bn_store_stats* out);
+int bn_stream_destroy(bn_stream* st);
+
+/* The store's LRU bookkeeping alone, with no CUDA (the reference's LruInner,
+ * store.rs:133-245): touch bumps an entry's recency (hit = 1) or reports a
+ * miss; pre_evict pops least-recently-used entries until `bytes` fits on top
+ * of the resident total (BN_EBUDGET, nothing evicted, when bytes exceeds the
+ * budget); insert adds an entry (inserted = 0 when the id is resident, which
+ * keeps the existing entry, as on the reference's insert race). */
+typedef struct bn_lru bn_lru;
+int bn_lru_create(uint64_t budget_bytes, bn_lru** out);
+int bn_lru_touch(bn_lru* l, uint64_t id, int* hit);
+int bn_lru_pre_evict(bn_lru* l, uint64_t bytes, uint64_t* evicted, uint32_t cap, uint32_t* n_evicted);
+int bn_lru_insert(bn_lru* l, uint64_t id, uint64_t bytes, int* inserted);
+int bn_lru_stats(const bn_lru* l, bn_store_stats* out);
+int bn_lru_destroy(bn_lru* l);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,11 @@ class ServerStats(C.Structure):
                 ("rejected", u64)]
 
 
+class StoreStats(C.Structure):
+    _fields_ = [("gets", u64), ("uploads", u64), ("evictions", u64), ("bytes_uploaded", u64),
+                ("resident_bytes", u64), ("budget_bytes", u64)]
+
+
 _SIGS = {
     "bn_last_error": (C.c_char_p, []),
     "bn_build_info": (C.c_char_p, []),
@@ -117,6 +122,18 @@ _SIGS = {
     "bn_server_wait": (C.c_int, [vp, u64, u32, vp, vp, vp, vp, vp, vp]),
     "bn_server_stats": (C.c_int, [vp, C.c_int, C.POINTER(ServerStats)]),
     "bn_server_destroy": (C.c_int, [vp]),
+    "bn_stream_build": (C.c_int, [vp, vp, vp, vp, u64, u32, u32, vp, vp, SparseCsr, u64, u64, vp]),
+    "bn_stream_build_from_plain": (C.c_int, [vp, vp, u64, u32, u32, vp, vp, SparseCsr, u64, u64, vp]),
+    "bn_stream_info": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "bn_stream_query": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp]),
+    "bn_stream_stats": (C.c_int, [vp, C.c_int, C.POINTER(StoreStats)]),
+    "bn_stream_destroy": (C.c_int, [vp]),
+    "bn_lru_create": (C.c_int, [u64, vp]),
+    "bn_lru_touch": (C.c_int, [vp, u64, vp]),
+    "bn_lru_pre_evict": (C.c_int, [vp, u64, vp, u32, vp]),
+    "bn_lru_insert": (C.c_int, [vp, u64, u64, vp]),
+    "bn_lru_stats": (C.c_int, [vp, C.POINTER(StoreStats)]),
+    "bn_lru_destroy": (C.c_int, [vp]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)
@@ -898,3 +915,116 @@ def ivf_from_cache(ctx, path: str, fingerprint: int = 0, n1: int = 128):
     v = Ivf.build(ctx, off, ids, a["m_enc"].reshape(-1), a["a_l"].reshape(-1), a["h"].reshape(-1), n1=n1)
     v.attach_client(a["l_subspace"].reshape(-1), a["m_plain"].reshape(-1), rp, ix, sg)
     return v, cen
+
+
+def _store_stats(st: StoreStats) -> dict:
+    return {f: getattr(st, f) for f, _ in StoreStats._fields_}
+
+
+class Stream:
+    """bn_stream: a flat corpus streamed through device memory in chunks
+    (the reference's ClusterStore, scorer-gpu-common/src/store.rs:247-395)."""
+
+    def __init__(self, ctx: Context, handle, m: int, n1: int):
+        self.ctx, self.h, self.m, self.n1 = ctx, handle, m, n1
+
+    @classmethod
+    def build(cls, ctx, m_enc, a_l, h, m, L, m_plain, s_rowptr, s_idx, s_sign, chunk_rows, budget_bytes, n1=128):
+        m_enc, a_l, h, L, m_plain = _u64(m_enc), _u64(a_l), _u64(h), _u64(L), _u64(m_plain)
+        csr, keep = _csr(s_rowptr, s_idx, s_sign)
+        out = vp()
+        check(lib.bn_stream_build(ctx.h, ptr(m_enc), ptr(a_l), ptr(h), m, N, n1, ptr(L), ptr(m_plain), csr,
+                                  chunk_rows, budget_bytes, C.byref(out)))
+        return cls(ctx, out, m, n1)
+
+    @classmethod
+    def build_from_plain(cls, ctx, m_q, m, L, H, s_rowptr, s_idx, s_sign, chunk_rows, budget_bytes, n1=128):
+        m_q, L, H = _u64(m_q), _u64(L), _u64(H)
+        csr, keep = _csr(s_rowptr, s_idx, s_sign)
+        out = vp()
+        check(lib.bn_stream_build_from_plain(ctx.h, ptr(m_q), m, N, n1, ptr(L), ptr(H), csr, chunk_rows,
+                                             budget_bytes, C.byref(out)))
+        return cls(ctx, out, m, n1)
+
+    def info(self) -> dict:
+        rows, chunks, slots, sb, hb = u64(), u32(), u32(), u64(), u64()
+        check(lib.bn_stream_info(self.h, C.byref(rows), C.byref(chunks), C.byref(slots), C.byref(sb), C.byref(hb)))
+        return {"rows": rows.value, "chunks": chunks.value, "slots": slots.value, "slot_bytes": sb.value,
+                "host_bytes": hb.value}
+
+    def query(self, v_enc, g, t_list, v_seeds, trials, k):
+        """Same arguments as Flat.query; returns (hits, failed_trial)."""
+        v = _u64(v_enc).reshape(-1, N)
+        B = v.shape[0]
+        gg = _u64(g).reshape(B, self.n1)
+        ti, ts, tn = _t_concat(t_list)
+        seeds = None if v_seeds is None else np.frombuffer(b"".join(bytes(s) for s in v_seeds), np.uint8).copy()
+        kk = max(k, 1)
+        ids = np.zeros((B, kk), np.uint32)
+        sc = np.zeros((B, kk), np.int64)
+        nh = np.zeros(B, np.uint32)
+        fl = np.zeros(B, np.int32)
+        check(lib.bn_stream_query(self.h, B, ptr(v), ptr(gg), ptr(ti) if ti.size else None,
+                                  ptr(ts) if ts.size else None, ptr(tn), ptr(seeds), trials, k, ptr(ids), ptr(sc),
+                                  ptr(nh), ptr(fl)))
+        hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
+        return hits, fl
+
+    def stats(self, reset=False) -> dict:
+        st = StoreStats()
+        check(lib.bn_stream_stats(self.h, 1 if reset else 0, C.byref(st)))
+        return _store_stats(st)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.bn_stream_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
+
+
+class Lru:
+    """bn_lru: the store's CUDA-free LRU bookkeeping (LruInner, store.rs:133-245)."""
+
+    def __init__(self, budget_bytes: int):
+        out = vp()
+        check(lib.bn_lru_create(budget_bytes, C.byref(out)))
+        self.h = out
+
+    def touch(self, cid: int) -> bool:
+        hit = C.c_int(0)
+        check(lib.bn_lru_touch(self.h, cid, C.byref(hit)))
+        return bool(hit.value)
+
+    def pre_evict(self, nbytes: int) -> list:
+        """Evicted ids, least recently used first; BnError(BN_EBUDGET) when nbytes cannot fit."""
+        cap = 4096
+        ev = np.zeros(cap, np.uint64)
+        n = u32(0)
+        check(lib.bn_lru_pre_evict(self.h, nbytes, ptr(ev), cap, C.byref(n)))
+        return [int(x) for x in ev[: n.value]]
+
+    def insert(self, cid: int, nbytes: int) -> bool:
+        ins = C.c_int(0)
+        check(lib.bn_lru_insert(self.h, cid, nbytes, C.byref(ins)))
+        return bool(ins.value)
+
+    def stats(self) -> dict:
+        st = StoreStats()
+        check(lib.bn_lru_stats(self.h, C.byref(st)))
+        return _store_stats(st)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.bn_lru_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except (AttributeError, TypeError):
+            pass

@@ -539,9 +539,9 @@ __global__ void ms8_s_kernel(const uint16_t* __restrict__ s_ell, const uint32_t*
         int rs = 0;
         for (uint32_t cc = 0; cc < wdt; ++cc) {
             const uint16_t f = s_ell[off + (uint64_t)cc * 32 + sl];
-            if (f == 0xffffu) continue;
-            const int sgn = (f & 0x8000u) ? -1 : 1;
-            int8_t* e = dst + blk_off(pi, N + (f & 0x3ffu), KS);
+            if (f == ELL_PAD) continue;
+            const int sgn = f >= ELL_NEG ? -1 : 1;
+            int8_t* e = dst + blk_off(pi, N + (f >= ELL_NEG ? f - ELL_NEG : f), KS);
             const int nv = (int)*e + sgn;
             if (nv < -128 || nv > 127) atomicOr(bad, 1u);
             *e = (int8_t)nv;

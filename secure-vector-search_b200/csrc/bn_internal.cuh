@@ -377,6 +377,10 @@ uint64_t block_plan_estimate(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k
 int block_prepare_engine(Engine& e, const std::vector<uint64_t>* offsets);
 int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms);
 int validate_residues(const uint64_t* a, uint64_t count, const char* what);
+int engine_init(Engine& e, bn_ctx* ctx);
+void engine_free(Engine& e);
+int corpus_tmap(Corpus& c);
+int check_shape(uint32_t n, uint32_t n1);
 int block_verify_host(BlockPlan& b, const uint64_t* r, const uint64_t* v_enc, const uint8_t* seed, int32_t* failed,
                       uint64_t* ur, uint64_t* zv);
 }  // namespace api

@@ -601,9 +601,9 @@ __device__ __forceinline__ uint64_t dense_terms_row(const uint64_t* __restrict__
     return combine3(a0, a1, a2);
 }
 
-// Two sign-extended int16 halves from bytes 0, 1 (sel 0x9180) or 2, 3
-// (sel 0xB3A2) of x: prmt's selector msb replicates the byte's sign.
-__device__ __forceinline__ uint32_t sext_pair(uint32_t x, uint32_t sel) {
+// Two zero-extended 16-bit halves from bytes 0, 1 (sel 0x4140) or 2, 3
+// (sel 0x4342) of x (selector nibble 4 picks a zero byte).
+__device__ __forceinline__ uint32_t zext_pair(uint32_t x, uint32_t sel) {
     uint32_t d;
     asm("prmt.b32 %0, %1, 0, %2;" : "=r"(d) : "r"(x), "r"(sel));
     return d;
@@ -613,44 +613,46 @@ __device__ __forceinline__ uint32_t sext_pair(uint32_t x, uint32_t sel) {
 // columns go 32 at a time, one per lane; a lane loads its column's 32 row
 // bytes (one 32-byte run of the column-major int8 copy: the warps decoding
 // neighbouring blocks at the same time read neighbouring runs of the same
-// columns, so DRAM pages serve many of them), widens them to 16 signed int16
-// pairs with the entry's sign, and a reduce-scatter over the lanes (lane
-// bit 4 keeps rows 0-15 or 16-31, then bits 3..0) leaves lane l the sum of
-// row l over those 32 columns (|sum| <= 32 * 128, exact in int16).  Four
-// groups of loads are in flight at a time.  Returns the exact integer.
+// columns, so DRAM pages serve many of them).  Each byte m becomes the
+// unsigned m + 128 (xor 0x80) for a +1 entry or 127 - m (xor 0x7f) for a -1
+// entry, widened to 16-bit halves; a reduce-scatter over the lanes (lane bit
+// 4 keeps rows 0-15 or 16-31, then bits 3..0) with plain 32-bit adds (32
+// terms <= 255 stay below 2^16, so no carry crosses a half) leaves lane l
+// the biased sum of row l over those 32 columns.  The bias, 128 per +1
+// entry and 127 per -1 entry, is taken off at the end.  Four groups of
+// loads are in flight at a time.  Returns the exact integer.
 __device__ __forceinline__ int32_t m_times_t_warp(const int8_t* __restrict__ m8_cm, uint64_t rows32, uint64_t blk,
                                                   const uint32_t* __restrict__ tl, uint32_t tn, uint32_t lane) {
     const int8_t* base = m8_cm + blk * 32;  // column c's run: base + c * rows32, 32-byte aligned
-    int32_t acc = 0;
+    int32_t acc = 0, bias = 0;
     for (uint32_t g0 = 0; g0 < tn; g0 += 4 * 32) {
         uint4 lo[4], hi[4];
-        uint32_t neg[4];
+        uint32_t mask[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const uint32_t c = g0 + u * 32 + lane;
             lo[u] = hi[u] = make_uint4(0u, 0u, 0u, 0u);
-            neg[u] = 0;
+            mask[u] = 0;  // past tn: zero bytes, no bias
             if (c < tn) {
                 const uint32_t e = tl[c];
                 const uint4* run = reinterpret_cast<const uint4*>(base + (uint64_t)(e & 0x3ffu) * rows32);
                 lo[u] = __ldg(run);
                 hi[u] = __ldg(run + 1);
-                neg[u] = e >> 31;
+                mask[u] = (e >> 31) ? 0x7f7f7f7fu : 0x80808080u;
             }
+            const uint32_t pos = __ballot_sync(FULL, mask[u] == 0x80808080u), neg = __ballot_sync(FULL, mask[u] == 0x7f7f7f7fu);
+            bias += 128 * __popc(pos) + 127 * __popc(neg);
         }
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             if (g0 + u * 32 >= tn) break;  // warp-uniform
-            const uint32_t wds[8] = {lo[u].x, lo[u].y, lo[u].z, lo[u].w, hi[u].x, hi[u].y, hi[u].z, hi[u].w};
+            const uint32_t wds[8] = {lo[u].x ^ mask[u], lo[u].y ^ mask[u], lo[u].z ^ mask[u], lo[u].w ^ mask[u],
+                                     hi[u].x ^ mask[u], hi[u].y ^ mask[u], hi[u].z ^ mask[u], hi[u].w ^ mask[u]};
             uint32_t v[16];  // v[w]: rows 2w (low half), 2w + 1 (high half)
 #pragma unroll
             for (int i = 0; i < 8; ++i) {
-                v[2 * i] = sext_pair(wds[i], 0x9180u);
-                v[2 * i + 1] = sext_pair(wds[i], 0xB3A2u);
-            }
-            if (neg[u]) {
-#pragma unroll
-                for (int w = 0; w < 16; ++w) v[w] = __vsub2(0u, v[w]);
+                v[2 * i] = zext_pair(wds[i], 0x4140u);
+                v[2 * i + 1] = zext_pair(wds[i], 0x4342u);
             }
             // reduce-scatter: after the step over lane bit b the lane keeps
             // the half of its words that its bit b selects
@@ -658,30 +660,30 @@ __device__ __forceinline__ int32_t m_times_t_warp(const int8_t* __restrict__ m8_
             for (int w = 0; w < 8; ++w) {
                 const bool up = lane & 16;
                 const uint32_t send = up ? v[w] : v[w + 8], keep = up ? v[w + 8] : v[w];
-                v[w] = __vadd2(keep, __shfl_xor_sync(FULL, send, 16));
+                v[w] = keep + __shfl_xor_sync(FULL, send, 16);
             }
 #pragma unroll
             for (int w = 0; w < 4; ++w) {
                 const bool up = lane & 8;
                 const uint32_t send = up ? v[w] : v[w + 4], keep = up ? v[w + 4] : v[w];
-                v[w] = __vadd2(keep, __shfl_xor_sync(FULL, send, 8));
+                v[w] = keep + __shfl_xor_sync(FULL, send, 8);
             }
 #pragma unroll
             for (int w = 0; w < 2; ++w) {
                 const bool up = lane & 4;
                 const uint32_t send = up ? v[w] : v[w + 2], keep = up ? v[w + 2] : v[w];
-                v[w] = __vadd2(keep, __shfl_xor_sync(FULL, send, 4));
+                v[w] = keep + __shfl_xor_sync(FULL, send, 4);
             }
             {
                 const bool up = lane & 2;
                 const uint32_t send = up ? v[0] : v[1], keep = up ? v[1] : v[0];
-                v[0] = __vadd2(keep, __shfl_xor_sync(FULL, send, 2));
+                v[0] = keep + __shfl_xor_sync(FULL, send, 2);
             }
-            const uint32_t pair = __vadd2(v[0], __shfl_xor_sync(FULL, v[0], 1));
-            acc += (lane & 1) ? (int32_t)(int16_t)(pair >> 16) : (int32_t)(int16_t)(pair & 0xffffu);
+            const uint32_t pair = v[0] + __shfl_xor_sync(FULL, v[0], 1);
+            acc += (int32_t)((lane & 1) ? (pair >> 16) : (pair & 0xffffu));
         }
     }
-    return acc;
+    return acc - bias;
 }
 
 // M_i . T from the column-major residues (plaintext not int8-valued): one
@@ -714,34 +716,37 @@ __device__ __forceinline__ uint64_t m_times_t_cm(const uint64_t* __restrict__ mp
 // j = lane + 32 i holding entries of column slot j / 4 for rows 8 (j % 4) ..
 // + 7, so a lane always sees the same 8 rows (8 (lane % 4) + 0..7) and
 // keeps 8 partial sums; a reduce-scatter over lane bits 4, 3, 2 then leaves
-// one row's sum per lane, and a shuffle hands row l to lane l.
-__device__ __forceinline__ uint64_t s_times_v_warp(const DecodeCorpus& dc, uint64_t blk, const uint64_t* __restrict__ vs,
+// one row's sum per lane, and a shuffle hands row l to lane l.  Every entry
+// is an index into vt = [v_enc, 0, p - v_enc] (ELL_NEG, ELL_PAD), so a term
+// is one shared load and one add; the sums fold every 4 terms (4 terms
+// below 2^61 on top of a folded value stay below 2^64).
+__device__ __forceinline__ uint64_t s_times_v_warp(const DecodeCorpus& dc, uint64_t blk, const uint64_t* __restrict__ vt,
                                                    uint32_t lane) {
     const uint32_t off = dc.s_off[blk], wdt = dc.s_w[blk];
     const uint4* base = reinterpret_cast<const uint4*>(dc.s_ell + off);  // slice data is 64 * wdt bytes
     const uint32_t chunks = wdt * 4;
+    constexpr uint32_t PAD2 = ELL_PAD | (ELL_PAD << 16);
     uint64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t j0 = 0; j0 < chunks; j0 += 8 * 32) {
         uint4 ch[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const uint32_t j = j0 + u * 32 + lane;
-            ch[u] = j < chunks ? __ldg(base + j) : make_uint4(0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu);
+            ch[u] = j < chunks ? __ldg(base + j) : make_uint4(PAD2, PAD2, PAD2, PAD2);
         }
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
             const uint32_t w[4] = {ch[u].x, ch[u].y, ch[u].z, ch[u].w};
 #pragma unroll
-            for (int h = 0; h < 8; ++h) {
-                const uint32_t f = (w[h >> 1] >> (16 * (h & 1))) & 0xffffu;
-                const uint64_t y = f == 0xffffu ? 0 : signed_term(vs[f & 0x3ffu], f & 0x8000u);
-                acc[h] = fold(acc[h]) + y;
+            for (int h = 0; h < 8; ++h)  // clamped into the table (ELL_TABLE - 1 holds 0)
+                acc[h] += vt[min((h & 1) ? (w[h >> 1] >> 16) : (w[h >> 1] & 0xffffu), ELL_TABLE - 1)];
+            if ((u & 3) == 3) {
+#pragma unroll
+                for (int h = 0; h < 8; ++h) acc[h] = fold(acc[h]);
             }
         }
     }
     // each step adds two values below 2^61 + 8 and folds the sum
-#pragma unroll
-    for (int h = 0; h < 8; ++h) acc[h] = fold(acc[h]);
 #pragma unroll
     for (int h = 0; h < 4; ++h) {  // lane bit 4: keep rows h + 4 * bit
         const bool up = lane & 16;
@@ -793,7 +798,7 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
     const uint32_t n1 = dc.n1;
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     extern __shared__ uint4 dyn_limbs[];  // 2 x uint4 per column: g's n1 columns, then x's
-    __shared__ uint64_t vs[N];
+    __shared__ uint64_t vt[ELL_TABLE];  // [v_enc, 0, p - v_enc, 0]: the S . v table
     __shared__ uint32_t tl[N];
     __shared__ TopkBuf buf;
     __shared__ int last_s;
@@ -804,7 +809,12 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
         dyn_limbs[2 * kk] = make_uint4(b.b0, b.b1, b.b2, c.b0);
         dyn_limbs[2 * kk + 1] = make_uint4(c.b1, c.b2, 0u, 0u);
     }
-    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) vs[j] = vv[(uint64_t)q * N + j];
+    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
+        const uint64_t x = vv[(uint64_t)q * N + j];
+        vt[j] = x;
+        vt[ELL_NEG + j] = x ? P - x : 0;
+    }
+    if (threadIdx.x == 0) vt[ELL_PAD] = vt[ELL_TABLE - 1] = 0;
     for (uint32_t c = threadIdx.x; c < tn; c += blockDim.x) tl[c] = t_ent[(uint64_t)q * N + c];
     if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
     __syncthreads();
@@ -849,7 +859,7 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
                 const int32_t mt = m_times_t_warp(dc.m8_cm, (dc.rows + 31) & ~31ull, blk, tl, tn, lane);
                 m_t = mt >= 0 ? (uint64_t)mt : P - (uint64_t)(-(int64_t)mt);
             }
-            const uint64_t s_v = s_times_v_warp(dc, blk, vs, lane);
+            const uint64_t s_v = s_times_v_warp(dc, blk, vt, lane);
             if (valid) {
                 if (!dc.m8_cm) m_t = m_times_t_cm(dc.mp_cm, dc.rows, gr, tl, tn);
                 const uint64_t dense = dense_terms_row(dc.alh_b, n1, gr, dyn_limbs);
@@ -1123,13 +1133,16 @@ __global__ void transpose_u64_kernel(const uint64_t* __restrict__ in, uint64_t r
 __global__ void csr_to_ell_kernel(const uint64_t* __restrict__ rowptr, const uint32_t* __restrict__ idx,
                                   const int8_t* __restrict__ sign, uint64_t rows, const uint32_t* __restrict__ s_off,
                                   const uint16_t* __restrict__ s_w, uint16_t* __restrict__ ell) {
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += (uint64_t)gridDim.x * blockDim.x) {
+    // every row position of every slice is written: the positions past the
+    // last row of the last slice hold padding
+    const uint64_t rows32 = (rows + 31) & ~31ull;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < rows32; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t slice = i >> 5;
         const uint32_t sl = (uint32_t)(i & 31), off = s_off[slice], w = s_w[slice];
-        const uint64_t b = rowptr[i], e = rowptr[i + 1];
+        const uint64_t b = i < rows ? rowptr[i] : 0, e = i < rows ? rowptr[i + 1] : 0;
         for (uint32_t c = 0; c < w; ++c) {
-            uint16_t v = 0xffffu;
-            if (b + c < e) v = (uint16_t)(idx[b + c] | (sign[b + c] < 0 ? 0x8000u : 0u));
+            uint16_t v = (uint16_t)ELL_PAD;
+            if (b + c < e) v = (uint16_t)(idx[b + c] + (sign[b + c] < 0 ? ELL_NEG : 0u));
             ell[off + (uint64_t)c * 32 + sl] = v;
         }
     }
@@ -1295,7 +1308,8 @@ void launch_transpose_u64(const uint64_t* d_in, uint64_t rows, uint32_t cols, ui
 
 void launch_csr_to_ell(const uint64_t* d_rowptr, const uint32_t* d_idx, const int8_t* d_sign, uint64_t rows,
                        const uint32_t* d_s_off, const uint16_t* d_s_w, uint16_t* d_s_ell, cudaStream_t s) {
-    csr_to_ell_kernel<<<grid_for(rows, 256, 148 * 16), 256, 0, s>>>(d_rowptr, d_idx, d_sign, rows, d_s_off, d_s_w, d_s_ell);
+    csr_to_ell_kernel<<<grid_for((rows + 31) & ~31ull, 256, 148 * 16), 256, 0, s>>>(d_rowptr, d_idx, d_sign, rows, d_s_off,
+                                                                                   d_s_w, d_s_ell);
 }
 
 }  // namespace bn

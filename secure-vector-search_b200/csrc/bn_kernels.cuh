@@ -6,9 +6,10 @@
 //   al_cm   u64 [128][rows]    AL, column-major           (client state)
 //   h_cm    u64 [128][rows]    H,  column-major
 //   mp_cm   u64 [1024][rows]   plaintext M, column-major  (M*T column sums)
-//   s_ell   u16 sliced-ELL of S: 32-row slices, entry = col | 0x8000 for -1,
-//           0xFFFF = padding; s_off[slice] = u32 offset of the slice's data,
-//           s_w[slice] = width
+//   s_ell   u16 sliced-ELL of S: 32-row slices, entry = col for +1,
+//           ELL_NEG + col for -1, ELL_PAD = padding (an index into the
+//           signed table [v, 0, p - v] of a query); s_off[slice] = u32
+//           offset of the slice's data, s_w[slice] = width
 //   ids     u32 [rows]         global vector id of each row (IVF), or null
 // Decode copies of the client state, in blocks of 32 rows (rows32 = rows
 // rounded up to 32; entries past the last row are 0):
@@ -29,6 +30,10 @@
 #include "bn_fp.cuh"
 
 namespace bn {
+
+// Sliced-ELL entries of S (layout note above); ELL_TABLE entries of the
+// decode's signed table, the last one a zero past every valid entry.
+constexpr uint32_t ELL_PAD = 1024, ELL_NEG = 1025, ELL_TABLE = 2 * 1024 + 2;
 
 // Per-query operand limbs for the scan: v = b0 + b1 2^21 + b2 2^42 and the
 // same split of v * 2^32 mod p (c0..c2), padded to 32 bytes.

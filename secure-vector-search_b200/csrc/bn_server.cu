@@ -10,10 +10,13 @@
 //     queued requests of one corpus (IVF requests with different nprobe share
 //     a batch: every probed list of every query is its own segment), after
 //     waiting at most max_wait_us for the batch to fill;
+//   - flat block plans are pooled across slots, one per block size and
+//     concurrent use, and kept, so a small batch runs a small block;
 //   - admission is by device memory: a batch's workspace (the pipeline's
-//     layout for exactly those requests) must fit in mem_budget together with
-//     the workspaces the other slots hold; otherwise it is cut shorter or waits
-//     for a slot to drain (idle slots give their memory back);
+//     layout for exactly those requests, or a new block plan) must fit in
+//     mem_budget together with what the slots and the plan pool hold;
+//     otherwise it is cut shorter or waits for a slot to drain (idle slots and
+//     plans give their memory back);
 //   - admission is also by queue: a submit is refused with BN_EAGAIN when
 //     max_queue requests wait, or when the expected wait (waiting requests
 //     over the completion rate of the recent batches) exceeds queue_wait_us;
@@ -71,9 +74,8 @@ struct Slot {
     std::vector<Request> reqs;
     HostMeta hm;
     QueryJob job;
-    // block scoring of flat batches: a plan for blocks of bp_B queries
-    BlockPlan* bp = nullptr;
-    uint32_t bp_B = 0;
+    // block scoring of flat batches: the index of the pooled plan in use
+    int plan = -1;
     bool block_run = false;
     // block scoring of IVF batches (pairs grouped by list), in ws / host
     IvfBlockJob* ivj = nullptr;
@@ -83,9 +85,16 @@ struct Slot {
     uint64_t ivj_ticket0 = 0;
     size_t ivj_count = 0;
     ~Slot() {
-        if (bp) block_plan_free(bp);
         if (ivj) ivf_block_job_free(ivj);
     }
+};
+
+// A block plan of the server's pool: one per block size (8, 16, 32, ...)
+// and concurrent use, lent to a slot for one batch.
+struct PooledPlan {
+    BlockPlan* bp = nullptr;
+    uint32_t B = 0;
+    bool busy = false;
 };
 
 }  // namespace
@@ -99,6 +108,7 @@ struct bn_server {
     std::deque<Request> pending[2];
     std::unordered_map<uint64_t, Result> results;
     std::vector<std::unique_ptr<Slot>> slots;
+    std::vector<PooledPlan> plans;
     uint64_t next_ticket = 1;
     bool stop = false;
     std::thread sched;
@@ -111,6 +121,9 @@ struct bn_server {
     uint64_t rejected = 0;
     // completion times and sizes of the recent batches (queue admission)
     std::deque<std::pair<Clock::time_point, uint32_t>> recent;
+    ~bn_server() {
+        for (PooledPlan& pp : plans) block_plan_free(pp.bp);
+    }
 };
 
 namespace {
@@ -147,6 +160,8 @@ void batch_meta(bn_server* s, int kind, It first, It last, HostMeta& hm) {
 }
 
 uint32_t block_bucket(bn_server* s, size_t count);
+uint64_t held_bytes(bn_server* s);
+int pool_find(const bn_server* s, uint32_t bucket, bool exact);
 
 // IVF batches of at least block_min requests run as IVF block scoring.
 bool ivf_block(const bn_server* s, size_t count) {
@@ -235,7 +250,7 @@ void harvest(bn_server* s, Slot& sl) {
     int rc = cudaEventSynchronize(sl.done) == cudaSuccess ? BN_OK : fail(BN_ECUDA, "batch failed on the device");
     std::vector<int32_t> bf(B, -1), bc(B, -1);
     if (rc == BN_OK)
-        rc = sl.block_run       ? block_query_finish(*sl.bp, B, ids.data(), sc.data(), nh.data(), bf.data())
+        rc = sl.block_run       ? block_query_finish(*s->plans[sl.plan].bp, B, ids.data(), sc.data(), nh.data(), bf.data())
              : sl.ivf_block_run ? ivf_block_finish(*sl.ivj, sl.host, ids.data(), sc.data(), nh.data(), bc.data(),
                                                    bf.data())
                                 : job_finish(sl.job, sl.host, ids.data(), sc.data(), nh.data(), vf);
@@ -264,6 +279,8 @@ void harvest(bn_server* s, Slot& sl) {
     complete(s, sl.reqs, res);
     sl.reqs.clear();
     sl.busy = false;
+    if (sl.plan >= 0) s->plans[sl.plan].busy = false;
+    sl.plan = -1;
 }
 
 // Packs and launches one batch on a free slot (called with s->mu held; the
@@ -313,21 +330,28 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
     }
     if (bucket) {
         // block scoring: the batch's queries share one pass over the corpus;
-        // Protocol 2 runs per block with the batch seed
-        // a slot keeps its largest plan so far (smaller batches pad it with
-        // zero queries) and its workspace for per-query / IVF batches:
-        // creating plans or freeing device memory mid-stream synchronises the
-        // device and stalls every slot
-        if (!sl.bp || sl.bp_B < bucket) {
-            if (sl.bp) block_plan_free(sl.bp);
-            sl.bp = nullptr;
-            sl.bp_B = 0;
-            rc = block_plan_create(s->flat, bucket, s->cfg.trials, s->cfg.k, 0, &sl.bp);
-            if (rc == BN_OK) sl.bp_B = bucket;
+        // Protocol 2 runs per block with the batch seed.  Plans are pooled
+        // and kept (creating plans or freeing device memory mid-stream
+        // synchronises the device and stalls every slot): an idle plan of
+        // the batch's own size, else a new one, else, when the budget has no
+        // room for it, an idle larger one padded with zero queries.
+        int pi = pool_find(s, bucket, true);
+        if (pi < 0 && s->cfg.mem_budget &&
+            held_bytes(s) + block_plan_estimate(s->flat, bucket, s->cfg.trials, s->cfg.k) > s->cfg.mem_budget)
+            pi = pool_find(s, bucket, false);
+        if (pi < 0) {
+            BlockPlan* bp = nullptr;
+            rc = block_plan_create(s->flat, bucket, s->cfg.trials, s->cfg.k, 0, &bp);
+            if (rc == BN_OK) {
+                s->plans.push_back(PooledPlan{bp, bucket, false});
+                pi = (int)s->plans.size() - 1;
+            }
         }
         if (rc == BN_OK) {
             sl.block_run = true;
-            rc = block_query_launch(*sl.bp, B, v.data(), g.data(), ti.empty() ? nullptr : ti.data(),
+            sl.plan = pi;
+            s->plans[pi].busy = true;
+            rc = block_query_launch(*s->plans[pi].bp, B, v.data(), g.data(), ti.empty() ? nullptr : ti.data(),
                                     ts.empty() ? nullptr : ts.data(), tn.data(), bseed, sl.stream, false);
             if (rc == BN_OK) s->block_batches += 1;
         } else if (rc == BN_EUNSUPPORTED) {
@@ -363,12 +387,23 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
     return BN_OK;
 }
 
-uint64_t slot_bytes(const Slot& sl) { return sl.ws.bytes + (sl.bp ? block_plan_bytes(sl.bp) : 0); }
-
 uint64_t held_bytes(bn_server* s) {
     uint64_t t = 0;
-    for (auto& sl : s->slots) t += slot_bytes(*sl);
+    for (auto& sl : s->slots) t += sl->ws.bytes;
+    for (const PooledPlan& pp : s->plans) t += block_plan_bytes(pp.bp);
     return t;
+}
+
+// An idle pooled plan for blocks of `bucket` queries (exact) or of the
+// fewest queries at least `bucket` (not exact); -1 if none.
+int pool_find(const bn_server* s, uint32_t bucket, bool exact) {
+    int best = -1;
+    for (size_t i = 0; i < s->plans.size(); ++i) {
+        const PooledPlan& pp = s->plans[i];
+        if (pp.busy || pp.B < bucket || (exact && pp.B != bucket)) continue;
+        if (best < 0 || pp.B < s->plans[best].B) best = (int)i;
+    }
+    return best;
 }
 
 // Block size a flat batch of `count` requests runs as (0: per-query path).
@@ -393,17 +428,21 @@ std::vector<Request> take_batch(bn_server* s, Slot& me, int& kind_out, bool& rej
     const double age_us = std::chrono::duration<double, std::micro>(Clock::now() - q.front().t_submit).count();
     if (q.size() < s->cfg.max_batch && age_us < s->cfg.max_wait_us) return {};
     // memory admission: the largest prefix whose workspace fits beside the
-    // other slots' memory and what this slot keeps besides the batch's own
-    // (its block plan while it runs a per-query or IVF batch, its workspace
-    // while it runs a flat block; a kept plan at least the batch's bucket is
-    // reused, so it is the batch's own)
-    const uint64_t others = held_bytes(s) - slot_bytes(me);
+    // memory held by the other slots and the plan pool.  A flat block reuses
+    // an idle pooled plan of its size, else needs a new one (or, when that
+    // does not fit, pads into an idle larger one) and keeps this slot's
+    // workspace; a per-query or IVF batch grows this slot's workspace.
+    const uint64_t others = held_bytes(s) - me.ws.bytes;
     const uint64_t budget = s->cfg.mem_budget;
     auto need = [&](size_t cnt) -> uint64_t {
         const uint32_t bucket = kind == BN_SERVER_FLAT ? block_bucket(s, cnt) : 0;
-        if (bucket && me.bp && me.bp_B >= bucket) return me.ws.bytes + block_plan_bytes(me.bp);
-        const uint64_t own = batch_bytes(s, kind, q, cnt, &me);
-        return own + (bucket ? me.ws.bytes : (me.bp ? block_plan_bytes(me.bp) : 0));
+        if (bucket) {
+            if (pool_find(s, bucket, true) >= 0) return me.ws.bytes;
+            const uint64_t fresh = me.ws.bytes + batch_bytes(s, kind, q, cnt, &me);
+            if (budget && others + fresh > budget && pool_find(s, bucket, false) >= 0) return me.ws.bytes;
+            return fresh;
+        }
+        return std::max(batch_bytes(s, kind, q, cnt, &me), me.ws.bytes);
     };
     size_t count = std::min<size_t>(q.size(), s->cfg.max_batch);
     while (count > 0 && budget && others + need(count) > budget) count = count > 8 ? count / 2 : count - 1;
@@ -411,13 +450,10 @@ std::vector<Request> take_batch(bn_server* s, Slot& me, int& kind_out, bool& rej
         bool any_busy = false;
         for (auto& sl : s->slots) any_busy |= sl->busy;
         if (!any_busy) {
-            // idle slots keep their memory: give it back (this slot's too), then retry once
-            for (auto& sl : s->slots) {
-                sl->ws.release();
-                if (sl->bp) block_plan_free(sl->bp);
-                sl->bp = nullptr;
-                sl->bp_B = 0;
-            }
+            // idle slots and plans keep their memory: give it back, then retry once
+            for (auto& sl : s->slots) sl->ws.release();
+            for (PooledPlan& pp : s->plans) block_plan_free(pp.bp);
+            s->plans.clear();
             if (batch_bytes(s, kind, q, 1, nullptr) + held_bytes(s) > budget) {
                 reject_front = true;  // this request alone exceeds the budget
                 reject_kind = kind;
@@ -578,6 +614,20 @@ int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn
         // (plaintext outside int8) is served per query
         if (flat && block_prepare(flat) == BN_EUNSUPPORTED) s->block_off = true;
         if (ivf && ivf_block_prepare(ivf) == BN_EUNSUPPORTED) s->ivf_block_off = true;
+        // one pooled plan per block size now, smallest first, while the
+        // budget has room for it (at most half of it): creating one later
+        // stalls the device while batches are in flight
+        if (flat && !s->block_off) {
+            uint64_t held = 0;
+            for (uint32_t b = block_bucket(s, cfg->block_min); b && b <= block_bucket(s, cfg->max_batch); b <<= 1) {
+                const uint64_t need = block_plan_estimate(flat, b, cfg->trials, cfg->k);
+                if (cfg->mem_budget && 2 * (held + need) > cfg->mem_budget) break;
+                BlockPlan* bp = nullptr;
+                if (block_plan_create(flat, b, cfg->trials, cfg->k, 0, &bp) != BN_OK) break;
+                s->plans.push_back(PooledPlan{bp, b, false});
+                held += block_plan_bytes(bp);
+            }
+        }
     }
     s->sched = std::thread(scheduler, s);
     *out = s;
