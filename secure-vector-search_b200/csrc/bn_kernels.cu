@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 #include "bn_kernels.cuh"
 
 namespace bn {
@@ -770,16 +772,66 @@ __device__ __forceinline__ uint64_t s_times_v_warp(const DecodeCorpus& dc, uint6
     return canon(__shfl_sync(FULL, acc[0], src));
 }
 
+// A warp's running top-k (k <= 32) as a list sorted best first across the
+// lanes: lane i holds the i-th best (score, id), lanes >= k the empty entry
+// (INT64_MIN never occurs as a score: fp_to_signed lies in (-p/2, p/2)).
+// Every lane offers one candidate; those better than the k-th best are
+// inserted one at a time, each at the rank the ballot of the list entries
+// better than it gives, the entries below it moving down one lane.  No
+// shared memory and no block barrier.
+constexpr int WARP_TOPK_MAX = 32;
+
+__device__ __forceinline__ void warp_topk_offer(int64_t& ls, uint32_t& li, int k, bool valid, int64_t s, uint32_t id,
+                                                uint32_t lane) {
+    const int64_t ts = __shfl_sync(FULL, ls, k - 1);
+    const uint32_t ti = __shfl_sync(FULL, li, k - 1);
+    uint32_t m = __ballot_sync(FULL, valid && better(s, id, ts, ti));
+    while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const int64_t cs = __shfl_sync(FULL, s, src);
+        const uint32_t ci = __shfl_sync(FULL, id, src);
+        const int pos = __popc(__ballot_sync(FULL, (int)lane < k && better(ls, li, cs, ci)));
+        const int64_t up_s = __shfl_up_sync(FULL, ls, 1);
+        const uint32_t up_i = __shfl_up_sync(FULL, li, 1);
+        if (pos < k) {  // warp-uniform
+            if ((int)lane > pos) { ls = up_s; li = up_i; }
+            if ((int)lane == pos) { ls = cs; li = ci; }
+            if ((int)lane >= k) { ls = INT64_MIN; li = 0xffffffffu; }
+        }
+    }
+}
+
+// Merges n (score, id) entries of shared memory into every warp's list
+// (entry e goes to warp e / 32 % warps), then the warps' lists into warp 0
+// through `xs`, `xi` (32 * warps entries).  Returns in warp 0's lanes.
+__device__ __forceinline__ void warp_topk_reduce(int64_t& ls, uint32_t& li, int k, int64_t* xs, uint32_t* xi,
+                                                 uint32_t warp, uint32_t lane) {
+    xs[warp * 32 + lane] = ls;
+    xi[warp * 32 + lane] = li;
+    __syncthreads();
+    if (warp == 0) {
+        for (uint32_t w = 1; w < DT_THREADS / 32; ++w) {
+            const int64_t s = xs[w * 32 + lane];
+            const uint32_t id = xi[w * 32 + lane];
+            warp_topk_offer(ls, li, k, s != INT64_MIN, s, id, lane);
+        }
+    }
+    __syncthreads();
+}
+
 // A warp decodes one unit: a segment's rows inside one aligned 32-row block
 // of the corpus (lane l = row 32 blk + l; lanes outside the segment idle in
 // the row work but join the block-wide M T and S v).  A CTA takes tiles of
 // 8 units of its query in turn (the host gives each query CTAs in
 // proportion to its units).  Mv = r - (AL g + H x) - M T - S v, ranked by
-// fp_to_signed into the CTA's candidate buffer; the CTA's best k go to the
-// scratch lists, and the last CTA of the query to finish (a ticket taken
-// after a device-scope fence, no waiting) merges them.
+// fp_to_signed into the CTA's candidate buffer (WARP_LISTS: k <= 32, every
+// warp's own list, merged at the end with no barrier in the loop); the CTA's
+// best k go to the scratch lists, and the last CTA of the query to finish (a
+// ticket taken after a device-scope fence, no waiting) merges them.
 constexpr uint32_t DT_WARPS = DT_THREADS / 32;
 
+template <bool WARP_LISTS>
 __global__ void __launch_bounds__(DT_THREADS, DECODE_CTAS_PER_SM)
 decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSeg* __restrict__ segs,
                    const uint64_t* __restrict__ seg_unit, const DecodeQuery* __restrict__ queries,
@@ -800,7 +852,11 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
     extern __shared__ uint4 dyn_limbs[];  // 2 x uint4 per column: g's n1 columns, then x's
     __shared__ uint64_t vt[ELL_TABLE];  // [v_enc, 0, p - v_enc, 0]: the S . v table
     __shared__ uint32_t tl[N];
-    __shared__ TopkBuf buf;
+    struct WarpXchg {  // the warps' lists on their way to warp 0
+        int64_t s[DT_THREADS];
+        uint32_t id[DT_THREADS];
+    };
+    __shared__ typename std::conditional<WARP_LISTS, WarpXchg, TopkBuf>::type buf;
     __shared__ int last_s;
     const uint32_t tn = min(t_nnz[q], (uint32_t)N);
     for (uint32_t kk = threadIdx.x; kk < 2 * n1; kk += blockDim.x) {
@@ -816,8 +872,11 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
     }
     if (threadIdx.x == 0) vt[ELL_PAD] = vt[ELL_TABLE - 1] = 0;
     for (uint32_t c = threadIdx.x; c < tn; c += blockDim.x) tl[c] = t_ent[(uint64_t)q * N + c];
-    if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
+    if constexpr (!WARP_LISTS)
+        if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
     __syncthreads();
+    int64_t ls = INT64_MIN;  // WARP_LISTS: this warp's list (lane i: i-th best)
+    uint32_t li = 0xffffffffu;
 
     uint64_t u_begin = 0, u_count = 0;  // nseg == 0: every probed list of this query was empty
     if (dq.nseg) {
@@ -868,22 +927,38 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
                 score = to_signed(mv);
             }
         }
-        const int64_t th_s = buf.thr_s;
-        const uint32_t th_i = buf.thr_i;
-        const int ht = buf.have_thr;
-        topk_offer(buf, valid, score, id, th_s, th_i, ht);
-        if (it % DT_CHECK == DT_CHECK - 1 && topk_full(buf, CAND_CAP - DT_CHECK * DT_THREADS))
-            topk_compact(buf, (int)k);
+        if constexpr (WARP_LISTS) {
+            warp_topk_offer(ls, li, (int)k, valid, score, id, lane);
+        } else {
+            const int64_t th_s = buf.thr_s;
+            const uint32_t th_i = buf.thr_i;
+            const int ht = buf.have_thr;
+            topk_offer(buf, valid, score, id, th_s, th_i, ht);
+            if (it % DT_CHECK == DT_CHECK - 1 && topk_full(buf, CAND_CAP - DT_CHECK * DT_THREADS))
+                topk_compact(buf, (int)k);
+        }
     }
-    topk_compact(buf, (int)k);
-    const int keep = min(buf.cnt, (int)k);
     const uint32_t ctas = dq.ctas;
     const uint64_t slot = blockIdx.x;
-    for (int i = threadIdx.x; i < keep; i += blockDim.x) {
-        ts.cand_s[slot * k + i] = buf.s[i];
-        ts.cand_i[slot * k + i] = buf.id[i];
+    if constexpr (WARP_LISTS) {
+        warp_topk_reduce(ls, li, (int)k, buf.s, buf.id, warp, lane);
+        if (warp == 0) {
+            const uint32_t keep = __popc(__ballot_sync(FULL, lane < k && ls != INT64_MIN));
+            if (lane < keep) {
+                ts.cand_s[slot * k + lane] = ls;
+                ts.cand_i[slot * k + lane] = li;
+            }
+            if (lane == 0) ts.cand_n[slot] = keep;
+        }
+    } else {
+        topk_compact(buf, (int)k);
+        const int keep = min(buf.cnt, (int)k);
+        for (int i = threadIdx.x; i < keep; i += blockDim.x) {
+            ts.cand_s[slot * k + i] = buf.s[i];
+            ts.cand_i[slot * k + i] = buf.id[i];
+        }
+        if (threadIdx.x == 0) ts.cand_n[slot] = (uint32_t)keep;
     }
-    if (threadIdx.x == 0) ts.cand_n[slot] = (uint32_t)keep;
     __threadfence();  // this CTA's lists are visible device-wide before its ticket
     __syncthreads();
     if (threadIdx.x == 0) last_s = atomicAdd(&ts.done[q], 1u) == ctas - 1;
@@ -892,12 +967,46 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
 
     // ---------------------------------------------------------- merge (last CTA of the query)
     __threadfence();
-    if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
-    __syncthreads();
+    const uint64_t total = (uint64_t)ctas * k;
+    if constexpr (WARP_LISTS) {
+        // warp w takes entries w * 32 + lane + 256 i into its list; then warp 0 merges the lists
+        ls = INT64_MIN;
+        li = 0xffffffffu;
+        for (uint64_t t0 = (uint64_t)warp * 32; t0 < total; t0 += DT_THREADS) {
+            const uint64_t e = t0 + lane;
+            bool v = false;
+            int64_t sc = 0;
+            uint32_t id = 0;
+            if (e < total) {
+                const uint64_t sl = (uint64_t)dq.cta0 + e / k;
+                const uint32_t i = (uint32_t)(e % k);
+                v = i < __ldcg(ts.cand_n + sl);
+                if (v) {
+                    sc = __ldcg(ts.cand_s + sl * k + i);
+                    id = __ldcg(ts.cand_i + sl * k + i);
+                }
+            }
+            warp_topk_offer(ls, li, (int)k, v, sc, id, lane);
+        }
+        warp_topk_reduce(ls, li, (int)k, buf.s, buf.id, warp, lane);
+        if (warp == 0) {
+            const uint32_t keep = __popc(__ballot_sync(FULL, lane < k && ls != INT64_MIN));
+            if (lane < keep) {
+                out_ids[(uint64_t)q * k + lane] = li;
+                out_scores[(uint64_t)q * k + lane] = ls;
+            }
+            if (lane == 0) {
+                out_n[q] = keep;
+                ts.done[q] = 0;
+            }
+        }
+        return;
+    } else {
+        if (threadIdx.x == 0) { buf.cnt = 0; buf.have_thr = 0; buf.thr_s = INT64_MIN; buf.thr_i = 0xffffffffu; }
+        __syncthreads();
     // Four tiles of entries per round: their loads (written by other CTAs
     // during this launch, so read through L2) are all in flight before the
     // offers; entries past a list's count are loaded and ignored.
-    const uint64_t total = (uint64_t)ctas * k;
     for (uint64_t t0 = 0; t0 < total; t0 += 4 * DT_THREADS) {
         bool valid[4];
         int64_t sc[4];
@@ -935,6 +1044,7 @@ decode_topk_kernel(const uint64_t* __restrict__ r, DecodeCorpus dc, const ScanSe
     if (threadIdx.x == 0) {
         out_n[q] = (uint32_t)out_keep;
         ts.done[q] = 0;
+    }
     }
 }
 
@@ -1259,11 +1369,19 @@ void launch_decode_topk(const uint64_t* d_r, const DecodeCorpus& dc, const ScanS
                         uint64_t* d_mv_out, uint32_t* d_out_ids, int64_t* d_out_scores, uint32_t* d_out_n,
                         cudaStream_t s) {
     if (!nq) return;
-    cudaFuncSetAttribute(decode_topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 2 * 512 * 16);  // per device
     cudaMemsetAsync(scratch.done, 0, (uint64_t)nq * 4, s);
-    decode_topk_kernel<<<total_ctas, DT_THREADS, 2 * 2 * dc.n1 * 16, s>>>(d_r, dc, d_segs, d_seg_unit, d_q, d_v, d_g,
-                                                                         d_x, d_t, d_t_nnz, k, scratch, d_mv_out,
-                                                                         d_out_ids, d_out_scores, d_out_n, nq);
+    const unsigned dyn = 2 * 2 * dc.n1 * 16;
+    if (k >= 1 && k <= (uint32_t)WARP_TOPK_MAX) {  // every warp keeps its own list
+        cudaFuncSetAttribute(decode_topk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 2 * 512 * 16);
+        decode_topk_kernel<true><<<total_ctas, DT_THREADS, dyn, s>>>(d_r, dc, d_segs, d_seg_unit, d_q, d_v, d_g, d_x,
+                                                                     d_t, d_t_nnz, k, scratch, d_mv_out, d_out_ids,
+                                                                     d_out_scores, d_out_n, nq);
+    } else {
+        cudaFuncSetAttribute(decode_topk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 2 * 512 * 16);
+        decode_topk_kernel<false><<<total_ctas, DT_THREADS, dyn, s>>>(d_r, dc, d_segs, d_seg_unit, d_q, d_v, d_g, d_x,
+                                                                      d_t, d_t_nnz, k, scratch, d_mv_out, d_out_ids,
+                                                                      d_out_scores, d_out_n, nq);
+    }
 }
 
 void launch_topk_rows(const uint64_t* d_a, const uint64_t* d_b, const uint64_t* d_c, uint64_t ld, uint64_t rows,
