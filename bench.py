@@ -41,9 +41,9 @@ N_DIM = 1024
 P = (1 << 61) - 1
 # DRAM bytes (read + write) per corpus row of one tc_fused_kernel launch:
 # dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of the
-# kernel on a 131,072-row corpus, divided by its rows (the traffic grows in
+# kernel on a 262,144-row corpus, divided by its rows (the traffic grows in
 # proportion to the rows, so it is scaled to the bench's N).
-FUSED_DRAM_BYTES_PER_ROW = 8628
+FUSED_DRAM_BYTES_PER_ROW = 8670
 METRIC = "BN F_p scan queries/s (flat N=1M, d=768, Freivalds k=20 fused, decode + top-10)"
 
 

@@ -665,7 +665,7 @@ int job_prepare(Engine& e, QueryJob& j, DevMem& ws, PinnedMem& host, const uint6
     j.z = sizes_for(e, hm, B, trials, k);
     j.o = make_layout(j.z, j.want_mv);
     const RunLayout& o = j.o;
-    TRY(ws.reserve(e.ctx, o.total));
+    TRY(ws.reserve_grow(e.ctx, o.total));
     TRY(host.reserve(o.out_end));
     char* d = ws.at<char>();
     TRY(make_tc_maps(j.z, reinterpret_cast<uint8_t*>(d + o.u_buf), reinterpret_cast<uint8_t*>(d + o.wimg), j.maps));

@@ -58,11 +58,16 @@ inline int device_flags_status(uint32_t f) {
 }
 
 
-// Device allocation accounted against the context budget.
+// Device allocation accounted against the context budget.  With `stream`
+// set the buffer is allocated and freed in that stream's order
+// (cudaMallocAsync / cudaFreeAsync): growing it then synchronises nothing,
+// where cudaFree waits for the whole device (the serving loop's slot
+// workspaces, which grow while other slots' batches are in flight).
 struct DevMem {
     bn_ctx* ctx = nullptr;
     void* p = nullptr;
     uint64_t bytes = 0;
+    cudaStream_t stream = nullptr;
 
     DevMem() = default;
     DevMem(const DevMem&) = delete;
@@ -71,7 +76,8 @@ struct DevMem {
 
     void release() {
         if (p) {
-            cudaFree(p);
+            if (stream) cudaFreeAsync(p, stream);
+            else cudaFree(p);
             std::lock_guard<std::mutex> g(ctx->mu);
             ctx->used -= bytes;
         }
@@ -90,7 +96,7 @@ struct DevMem {
             c->used += b;
             c->peak = std::max(c->peak, c->used);
         }
-        cudaError_t e = cudaMalloc(&p, b);
+        cudaError_t e = stream ? cudaMallocAsync(&p, b, stream) : cudaMalloc(&p, b);
         if (e != cudaSuccess) {
             std::lock_guard<std::mutex> g(c->mu);
             c->used -= b;
@@ -102,6 +108,19 @@ struct DevMem {
     }
     // Grow-only reallocation (contents not kept).
     int reserve(bn_ctx* c, uint64_t b) { return (p && bytes >= b) ? BN_OK : alloc(c, b); }
+    // The size reserve_grow makes room for: at least `need`, and half again
+    // the current size when it grows at all, so a stream of slowly growing
+    // requests reallocates (and so synchronises the device) a few times, not
+    // every time.
+    static uint64_t grown(uint64_t have, uint64_t need) {
+        return have >= need ? have : (need > have + have / 2 ? need : have + have / 2);
+    }
+    int reserve_grow(bn_ctx* c, uint64_t b) {
+        if (p && bytes >= b) return BN_OK;
+        const uint64_t g = grown(bytes, b);
+        const int rc = alloc(c, g);
+        return rc == BN_EBUDGET && g > b ? alloc(c, b) : rc;  // the headroom is optional
+    }
     template <class T>
     T* at(uint64_t off = 0) const {
         return reinterpret_cast<T*>(static_cast<char*>(p) + off);
@@ -114,13 +133,15 @@ struct PinnedMem {
     ~PinnedMem() {
         if (p) cudaFreeHost(p);
     }
+    // Grows by half again at least (cudaFreeHost synchronises the device).
     int reserve(uint64_t b) {
         if (p && bytes >= b) return BN_OK;
+        const uint64_t g = b > bytes + bytes / 2 ? b : bytes + bytes / 2;
         if (p) cudaFreeHost(p);
         p = nullptr;
         bytes = 0;
-        CU(cudaMallocHost(&p, b));
-        bytes = b;
+        CU(cudaMallocHost(&p, g));
+        bytes = g;
         return BN_OK;
     }
     template <class T>

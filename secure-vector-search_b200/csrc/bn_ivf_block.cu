@@ -540,7 +540,7 @@ int ivf_block_pack(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, const
     if (!v_enc) return fail(BN_EINVAL, "null v_enc");
     if (j.trials && !seed) return fail(BN_EINVAL, "block_seed is required when trials > 0");
     TRY(validate_residues(v_enc, (uint64_t)B * N, "v_enc"));
-    TRY(ws.reserve(e.ctx, j.total));
+    TRY(ws.reserve_grow(e.ctx, j.total));
     TRY(host.reserve(j.out_end));  // inputs, then the outputs read back at the same offsets
     char* h = host.at<char>();
     memcpy(h + j.o_v, v_enc, (uint64_t)B * N * 8);

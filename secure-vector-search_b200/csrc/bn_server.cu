@@ -11,7 +11,9 @@
 //     a batch: every probed list of every query is its own segment), after
 //     waiting at most max_wait_us for the batch to fill;
 //   - flat block plans are pooled across slots, one per block size and
-//     concurrent use, and kept, so a small batch runs a small block;
+//     concurrent use, and kept, so a small batch runs a small block (or
+//     pads into an idle larger one rather than creating a plan while
+//     batches are in flight);
 //   - admission is by device memory: a batch's workspace (the pipeline's
 //     layout for exactly those requests, or a new block plan) must fit in
 //     mem_budget together with what the slots and the plan pool hold;
@@ -333,12 +335,10 @@ int launch(bn_server* s, Slot& sl, int kind, std::vector<Request>&& reqs) {
         // Protocol 2 runs per block with the batch seed.  Plans are pooled
         // and kept (creating plans or freeing device memory mid-stream
         // synchronises the device and stalls every slot): an idle plan of
-        // the batch's own size, else a new one, else, when the budget has no
-        // room for it, an idle larger one padded with zero queries.
+        // the batch's own size, else an idle larger one padded with zero
+        // queries, else a new one.
         int pi = pool_find(s, bucket, true);
-        if (pi < 0 && s->cfg.mem_budget &&
-            held_bytes(s) + block_plan_estimate(s->flat, bucket, s->cfg.trials, s->cfg.k) > s->cfg.mem_budget)
-            pi = pool_find(s, bucket, false);
+        if (pi < 0) pi = pool_find(s, bucket, false);
         if (pi < 0) {
             BlockPlan* bp = nullptr;
             rc = block_plan_create(s->flat, bucket, s->cfg.trials, s->cfg.k, 0, &bp);
@@ -437,12 +437,10 @@ std::vector<Request> take_batch(bn_server* s, Slot& me, int& kind_out, bool& rej
     auto need = [&](size_t cnt) -> uint64_t {
         const uint32_t bucket = kind == BN_SERVER_FLAT ? block_bucket(s, cnt) : 0;
         if (bucket) {
-            if (pool_find(s, bucket, true) >= 0) return me.ws.bytes;
-            const uint64_t fresh = me.ws.bytes + batch_bytes(s, kind, q, cnt, &me);
-            if (budget && others + fresh > budget && pool_find(s, bucket, false) >= 0) return me.ws.bytes;
-            return fresh;
+            if (pool_find(s, bucket, false) >= 0) return me.ws.bytes;  // an idle plan of this size or larger
+            return me.ws.bytes + batch_bytes(s, kind, q, cnt, &me);
         }
-        return std::max(batch_bytes(s, kind, q, cnt, &me), me.ws.bytes);
+        return DevMem::grown(me.ws.bytes, batch_bytes(s, kind, q, cnt, &me));  // reserve_grow's size
     };
     size_t count = std::min<size_t>(q.size(), s->cfg.max_batch);
     while (count > 0 && budget && others + need(count) > budget) count = count > 8 ? count / 2 : count - 1;
@@ -607,6 +605,7 @@ int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn
             return fail(BN_ECUDA, "stream / event creation failed");
         }
         sl->ws.ctx = ctx;
+        sl->ws.stream = sl->stream;  // grows in the slot's stream order, with no device-wide sync
     }
     if (cfg->block_min) {
         // byte-planar corpus copies of block scoring, built now rather than
@@ -614,19 +613,25 @@ int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn
         // (plaintext outside int8) is served per query
         if (flat && block_prepare(flat) == BN_EUNSUPPORTED) s->block_off = true;
         if (ivf && ivf_block_prepare(ivf) == BN_EUNSUPPORTED) s->ivf_block_off = true;
-        // one pooled plan per block size now, smallest first, while the
-        // budget has room for it (at most half of it): creating one later
-        // stalls the device while batches are in flight
+        // pooled plans now: one per block size, smallest first, then more
+        // of the largest size until every slot could run one, while they fit
+        // in half the budget; creating one later stalls the device while
+        // batches are in flight
         if (flat && !s->block_off) {
             uint64_t held = 0;
-            for (uint32_t b = block_bucket(s, cfg->block_min); b && b <= block_bucket(s, cfg->max_batch); b <<= 1) {
+            const uint32_t top = block_bucket(s, cfg->max_batch);
+            auto add = [&](uint32_t b) {
                 const uint64_t need = block_plan_estimate(flat, b, cfg->trials, cfg->k);
-                if (cfg->mem_budget && 2 * (held + need) > cfg->mem_budget) break;
+                if (cfg->mem_budget && 2 * (held + need) > cfg->mem_budget) return false;
                 BlockPlan* bp = nullptr;
-                if (block_plan_create(flat, b, cfg->trials, cfg->k, 0, &bp) != BN_OK) break;
+                if (block_plan_create(flat, b, cfg->trials, cfg->k, 0, &bp) != BN_OK) return false;
                 s->plans.push_back(PooledPlan{bp, b, false});
                 held += block_plan_bytes(bp);
-            }
+                return true;
+            };
+            bool ok = true;
+            for (uint32_t b = block_bucket(s, cfg->block_min); ok && b && b <= top; b <<= 1) ok = add(b);
+            for (uint32_t i = 1; ok && top && i < cfg->slots; ++i) ok = add(top);
         }
     }
     s->sched = std::thread(scheduler, s);
@@ -716,6 +721,8 @@ int bn_server_destroy(bn_server* s) {
     }
     if (s->sched.joinable()) s->sched.join();  // drains queued and in-flight batches
     for (auto& sl : s->slots) {
+        sl->ws.release();  // freed in its stream's order, before the stream goes
+        if (sl->stream) cudaStreamSynchronize(sl->stream);
         if (sl->stream) cudaStreamDestroy(sl->stream);
         if (sl->done) cudaEventDestroy(sl->done);
     }

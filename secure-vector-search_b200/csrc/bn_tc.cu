@@ -30,6 +30,18 @@ constexpr int UG_THREADS = 352;  // >= 20 trials x 17 keystream blocks: one bloc
 constexpr int UG_PAD = TC_ROWS + TC_ROWS / 16;  // one pad word per 16 keeps lanes off shared banks
 __device__ __forceinline__ uint32_t ug_idx(uint32_t i) { return i + (i >> 4); }
 
+// Byte transpose of four words: o_b = byte b of w[0], w[1], w[2], w[3] (in
+// that order, low byte first), by byte permutes.
+__device__ __forceinline__ void transpose_bytes4(const uint32_t w[4], uint32_t& o0, uint32_t& o1, uint32_t& o2,
+                                                 uint32_t& o3) {
+    const uint32_t t0 = __byte_perm(w[0], w[1], 0x5140), t1 = __byte_perm(w[2], w[3], 0x5140);
+    const uint32_t t2 = __byte_perm(w[0], w[1], 0x7362), t3 = __byte_perm(w[2], w[3], 0x7362);
+    o0 = __byte_perm(t0, t1, 0x5410);
+    o1 = __byte_perm(t0, t1, 0x7632);
+    o2 = __byte_perm(t2, t3, 0x5410);
+    o3 = __byte_perm(t2, t3, 0x7632);
+}
+
 __global__ void __launch_bounds__(UG_THREADS)
 tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ blocks, const ChaChaKey* __restrict__ keys,
                const uint64_t* __restrict__ r, uint32_t t_base, uint32_t t_cnt, uint32_t n_rows,
@@ -71,16 +83,23 @@ tc_ugen_kernel(const VerifySeg* __restrict__ vsegs, const TcBlock* __restrict__ 
     uint8_t* dst = u_row_pitch ? u_out + vs.r0 + tb.i0 : u_out + (uint64_t)blk * n_rows * TC_ROWS;
     for (uint32_t c = threadIdx.x; c < t_cnt * (TC_ROWS / 16); c += blockDim.x) {
         const uint32_t tl = c / (TC_ROWS / 16), ch = c % (TC_ROWS / 16);
-        uint64_t x[16];
+        uint32_t pl[8][4];  // pl[b][j]: byte b of draws 4j .. 4j + 3
 #pragma unroll
-        for (int q = 0; q < 16; ++q) x[q] = us[tl][ug_idx(ch * 16 + q)];
+        for (int j = 0; j < 4; ++j) {
+            uint32_t lo[4], hi[4];
 #pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            uint32_t wv[4] = {0, 0, 0, 0};
-#pragma unroll
-            for (int q = 0; q < 16; ++q) wv[q >> 2] |= (uint32_t)((x[q] >> (8 * b)) & 0xffu) << (8 * (q & 3));
-            reinterpret_cast<uint4*>(dst + (uint64_t)(tl * 8 + b) * pitch)[ch] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+            for (int q = 0; q < 4; ++q) {
+                const uint64_t x = us[tl][ug_idx(ch * 16 + 4 * j + q)];
+                lo[q] = (uint32_t)x;
+                hi[q] = (uint32_t)(x >> 32);
+            }
+            transpose_bytes4(lo, pl[0][j], pl[1][j], pl[2][j], pl[3][j]);
+            transpose_bytes4(hi, pl[4][j], pl[5][j], pl[6][j], pl[7][j]);
         }
+#pragma unroll
+        for (int b = 0; b < 8; ++b)
+            reinterpret_cast<uint4*>(dst + (uint64_t)(tl * 8 + b) * pitch)[ch] =
+                make_uint4(pl[b][0], pl[b][1], pl[b][2], pl[b][3]);
     }
     for (uint32_t c = threadIdx.x; c < (n_rows - 8 * t_cnt) * (TC_ROWS / 16); c += blockDim.x) {  // zero pad rows
         const uint32_t row = 8 * t_cnt + c / (TC_ROWS / 16), ch = c % (TC_ROWS / 16);
