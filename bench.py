@@ -688,6 +688,60 @@ def run_stream(args, ctx):
                                 "h2d_gbs": s["bytes_uploaded"] / dt / 1e9, "hits_verdicts_equal_resident": same}
     flat.close()
     st.close()
+    out["ivf"] = run_stream_ivf(args, ctx)
+    return out
+
+
+def run_stream_ivf(args, ctx):
+    """The IVF form (bn_ivf_stream): a k-means-partitioned corpus of N rows
+    and 512 lists in chunks of whole lists, a budget of S chunk slots,
+    batches of 64 queries routed to nprobe lists; a call uploads only the
+    chunks holding a probed list.  The first call's hits and verdicts are
+    compared with a resident IVF corpus built from the same data."""
+    from bn_b200 import capi
+
+    n, nlist, seed, k, trials = args.stream_rows, 512, 12, 10, args.trials
+    chunk, slots = args.stream_chunk_rows, args.stream_slots
+    data = synth_ivf(n, 768, nlist, seed)
+    L = capi.host_generate_subspace(bytes([seed & 0xFF, 0x1F]) * 16)
+    mq = to_residues(data["m8"])
+    probe = capi.IvfStream.build_keygen(ctx, data["offsets"], data["ids"], mq.reshape(-1), L, seed, chunk, 1 << 42)
+    budget = slots * probe.info()["slot_bytes"]
+    probe.close()
+    t0 = time.perf_counter()
+    st = capi.IvfStream.build_keygen(ctx, data["offsets"], data["ids"], mq.reshape(-1), L, seed, chunk, budget)
+    build_s = time.perf_counter() - t0
+    res = capi.Ivf.build_keygen(ctx, data["offsets"], data["ids"], mq.reshape(-1), L, seed)
+    del mq
+    info = st.info()
+    B = 64
+    qx, q8 = synth_ivf_queries(data, B, seed + 1)
+    encs, seeds = encode_pool(L, B, q8, seed + 1)
+    out = {"N": n, "nlist": nlist, "chunk_rows": chunk, "chunks": info["chunks"], "slots": info["slots"],
+           "slot_gib": info["slot_bytes"] / 2**30, "host_image_gib": info["host_bytes"] / 2**30,
+           "build_s": build_s, "B": B, "per_nprobe": {}}
+    for nprobe in (8, 32):
+        probes = np.stack([capi.host_probe_route(data["centres"], qx[i], nprobe)[0] for i in range(B)])
+        a = (probes, np.stack([e[0] for e in encs]), np.stack([e[1] for e in encs]),
+             [(e[2], e[3]) for e in encs], seeds, trials, k)
+        got, gc, gt = st.query(*a)  # warm-up call, checked against the resident corpus
+        want, wc, wt = res.query(*a)
+        same = bool(np.array_equal(gc, wc) and np.array_equal(gt, wt) and np.all(gt == -1) and
+                    all(np.array_equal(got[b][0], want[b][0]) and np.array_equal(got[b][1], want[b][1])
+                        for b in range(B)))
+        st.stats(reset=True)
+        calls = 3
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            st.query(*a)
+        dt = time.perf_counter() - t0
+        s = st.stats()
+        out["per_nprobe"][str(nprobe)] = {
+            "qps": B * calls / dt, "ms_per_call": dt / calls * 1e3, "chunks_needed_per_call": s["gets"] / calls,
+            "uploads_per_call": s["uploads"] / calls, "gib_uploaded_per_call": s["bytes_uploaded"] / calls / 2**30,
+            "h2d_gbs": s["bytes_uploaded"] / dt / 1e9, "hits_verdicts_equal_resident": same}
+    res.close()
+    st.close()
     return out
 
 

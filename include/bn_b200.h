@@ -500,6 +500,28 @@ int bn_stream_query(bn_stream* st, uint32_t B, const uint64_t* v_enc, const uint
                     uint32_t* ids, int64_t* scores, uint32_t* n_hits, int32_t* failed_trial);
 int bn_stream_stats(bn_stream* st, int reset, bn_store_stats* out);
 int bn_stream_destroy(bn_stream* st);
+/* The IVF form (the reference's per-cluster uploads, IvfGpuState,
+ * gpu/mod.rs:423-577): chunks of whole lists up to chunk_rows rows (a
+ * longer list is a chunk of its own); a call uploads only the chunks that
+ * hold a probed list.  Arguments and results as bn_ivf_build +
+ * bn_ivf_attach_client, bn_ivf_build_keygen and bn_ivf_query (failed_cluster
+ * / failed_trial: the first failing list in probe order). */
+typedef struct bn_ivf_stream bn_ivf_stream;
+int bn_ivf_stream_build(bn_ctx* ctx, uint32_t nlist, const uint64_t* list_offsets, const uint32_t* ids,
+                        const uint64_t* m_enc, const uint64_t* a_l, const uint64_t* h, uint32_t n, uint32_t n1,
+                        const uint64_t* l_subspace, const uint64_t* m_plain, bn_sparse_csr s_mat, uint64_t chunk_rows,
+                        uint64_t budget_bytes, bn_ivf_stream** out);
+int bn_ivf_stream_build_keygen(bn_ctx* ctx, uint32_t nlist, const uint64_t* list_offsets, const uint32_t* ids,
+                               const uint64_t* m_q, uint32_t n, uint32_t n1, const uint64_t* l_subspace,
+                               uint64_t upload_seed, uint64_t chunk_rows, uint64_t budget_bytes, bn_ivf_stream** out);
+int bn_ivf_stream_info(const bn_ivf_stream* st, uint64_t* rows, uint32_t* chunks, uint32_t* slots,
+                       uint64_t* slot_bytes, uint64_t* host_bytes);
+int bn_ivf_stream_query(bn_ivf_stream* st, uint32_t B, uint32_t nprobe, const uint32_t* probes, const uint64_t* v_enc,
+                        const uint64_t* g, const uint32_t* t_idx, const int8_t* t_sign, const uint32_t* t_nnz,
+                        const uint8_t* v_seeds, uint32_t trials, uint32_t k, uint32_t* ids, int64_t* scores,
+                        uint32_t* n_hits, int32_t* failed_cluster, int32_t* failed_trial);
+int bn_ivf_stream_stats(bn_ivf_stream* st, int reset, bn_store_stats* out);
+int bn_ivf_stream_destroy(bn_ivf_stream* st);
 
 /* The store's LRU bookkeeping alone, with no CUDA (the reference's LruInner,
  * store.rs:133-245): touch bumps an entry's recency (hit = 1) or reports a

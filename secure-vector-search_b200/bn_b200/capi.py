@@ -128,6 +128,12 @@ _SIGS = {
     "bn_stream_query": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp]),
     "bn_stream_stats": (C.c_int, [vp, C.c_int, C.POINTER(StoreStats)]),
     "bn_stream_destroy": (C.c_int, [vp]),
+    "bn_ivf_stream_build": (C.c_int, [vp, u32, vp, vp, vp, vp, vp, u32, u32, vp, vp, SparseCsr, u64, u64, vp]),
+    "bn_ivf_stream_build_keygen": (C.c_int, [vp, u32, vp, vp, vp, u32, u32, vp, u64, u64, u64, vp]),
+    "bn_ivf_stream_info": (C.c_int, [vp, vp, vp, vp, vp, vp]),
+    "bn_ivf_stream_query": (C.c_int, [vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, u32, u32, vp, vp, vp, vp, vp]),
+    "bn_ivf_stream_stats": (C.c_int, [vp, C.c_int, C.POINTER(StoreStats)]),
+    "bn_ivf_stream_destroy": (C.c_int, [vp]),
     "bn_lru_create": (C.c_int, [u64, vp]),
     "bn_lru_touch": (C.c_int, [vp, u64, vp]),
     "bn_lru_pre_evict": (C.c_int, [vp, u64, vp, u32, vp]),
@@ -978,6 +984,79 @@ class Stream:
     def close(self):
         if getattr(self, "h", None):
             lib.bn_stream_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except (AttributeError, TypeError):  # interpreter shutdown: the library is already unloaded
+            pass
+
+
+class IvfStream:
+    """bn_ivf_stream: an IVF corpus streamed through device memory in chunks of
+    whole lists (the reference's per-cluster ClusterStore uploads)."""
+
+    def __init__(self, ctx: Context, handle, nlist: int, n1: int):
+        self.ctx, self.h, self.nlist, self.n1 = ctx, handle, nlist, n1
+
+    @classmethod
+    def build(cls, ctx, offsets, ids, m_enc, a_l, h, L, m_plain, s_rowptr, s_idx, s_sign, chunk_rows, budget_bytes,
+              n1=128):
+        off = np.ascontiguousarray(offsets, np.uint64)
+        ids = np.ascontiguousarray(ids, np.uint32)
+        m_enc, a_l, h, L, m_plain = _u64(m_enc), _u64(a_l), _u64(h), _u64(L), _u64(m_plain)
+        csr, keep = _csr(s_rowptr, s_idx, s_sign)
+        out = vp()
+        check(lib.bn_ivf_stream_build(ctx.h, off.size - 1, ptr(off), ptr(ids), ptr(m_enc), ptr(a_l), ptr(h), N, n1,
+                                      ptr(L), ptr(m_plain), csr, chunk_rows, budget_bytes, C.byref(out)))
+        return cls(ctx, out, off.size - 1, n1)
+
+    @classmethod
+    def build_keygen(cls, ctx, offsets, ids, m_q, L, upload_seed: int, chunk_rows, budget_bytes, n1=128):
+        off = np.ascontiguousarray(offsets, np.uint64)
+        ids = np.ascontiguousarray(ids, np.uint32)
+        m_q, L = _u64(m_q), _u64(L)
+        out = vp()
+        check(lib.bn_ivf_stream_build_keygen(ctx.h, off.size - 1, ptr(off), ptr(ids), ptr(m_q), N, n1, ptr(L),
+                                             upload_seed, chunk_rows, budget_bytes, C.byref(out)))
+        return cls(ctx, out, off.size - 1, n1)
+
+    def info(self) -> dict:
+        rows, chunks, slots, sb, hb = u64(), u32(), u32(), u64(), u64()
+        check(lib.bn_ivf_stream_info(self.h, C.byref(rows), C.byref(chunks), C.byref(slots), C.byref(sb),
+                                     C.byref(hb)))
+        return {"rows": rows.value, "chunks": chunks.value, "slots": slots.value, "slot_bytes": sb.value,
+                "host_bytes": hb.value}
+
+    def query(self, probes, v_enc, g, t_list, v_seeds, trials, k):
+        """Same arguments as Ivf.query; returns (hits, failed_cluster, failed_trial)."""
+        pr = np.ascontiguousarray(probes, np.uint32)
+        B, nprobe = pr.shape
+        v = _u64(v_enc).reshape(B, N)
+        gg = _u64(g).reshape(B, self.n1)
+        ti, ts, tn = _t_concat(t_list)
+        seeds = None if v_seeds is None else np.frombuffer(b"".join(bytes(s) for s in v_seeds), np.uint8).copy()
+        kk = max(k, 1)
+        ids = np.zeros((B, kk), np.uint32)
+        sc = np.zeros((B, kk), np.int64)
+        nh = np.zeros(B, np.uint32)
+        fc = np.zeros(B, np.int32)
+        ft = np.zeros(B, np.int32)
+        check(lib.bn_ivf_stream_query(self.h, B, nprobe, ptr(pr), ptr(v), ptr(gg), ptr(ti) if ti.size else None,
+                                      ptr(ts) if ts.size else None, ptr(tn), ptr(seeds), trials, k, ptr(ids), ptr(sc),
+                                      ptr(nh), ptr(fc), ptr(ft)))
+        hits = [(ids[b, : nh[b]].copy(), sc[b, : nh[b]].copy()) for b in range(B)]
+        return hits, fc, ft
+
+    def stats(self, reset=False) -> dict:
+        st = StoreStats()
+        check(lib.bn_ivf_stream_stats(self.h, 1 if reset else 0, C.byref(st)))
+        return _store_stats(st)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib.bn_ivf_stream_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -1637,6 +1637,17 @@ int bn_flat_build_keygen(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t 
 
 int bn_ivf_build_keygen(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const uint32_t* ids, const uint64_t* m_q,
                         uint32_t n, uint32_t n1, const uint64_t* L, uint64_t upload_seed, bn_ivf** out) {
+    return bn::api::ivf_build_keygen_from(ctx, nlist, off, ids, m_q, n, n1, L, upload_seed, 0, out);
+}
+
+}  // extern "C"
+
+namespace bn {
+namespace api {
+
+int ivf_build_keygen_from(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const uint32_t* ids, const uint64_t* m_q,
+                          uint32_t n, uint32_t n1, const uint64_t* L, uint64_t upload_seed, uint32_t list0,
+                          bn_ivf** out) {
     if (!ctx || !out || !L) return fail(BN_EINVAL, "null argument");
     *out = nullptr;
     TRY(check_shape(n, n1));
@@ -1646,7 +1657,7 @@ int bn_ivf_build_keygen(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const 
     TRY(validate_residues(m_q, rows * N, "m_q"));
     TRY(validate_residues(L, (uint64_t)N * n1, "l_subspace"));
     std::vector<uint8_t> seeds(32ull * std::max<uint32_t>(nlist, 1));
-    for (uint32_t c = 0; c < nlist; ++c) derive_h_seed(upload_seed, c, &seeds[32ull * c]);  // ivf.rs:258-264
+    for (uint32_t c = 0; c < nlist; ++c) derive_h_seed(upload_seed, list0 + c, &seeds[32ull * c]);  // ivf.rs:258-264
     auto* v = new bn_ivf();
     int rc = engine_init(v->e, ctx);
     v->nlist = nlist;
@@ -1668,6 +1679,11 @@ int bn_ivf_build_keygen(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const 
     *out = v;
     return BN_OK;
 }
+
+}  // namespace api
+}  // namespace bn
+
+extern "C" {
 
 int bn_encrypt_cluster(bn_ctx* ctx, const uint64_t* m_q, uint64_t m, uint32_t n, uint32_t n1, const uint64_t* L,
                        const uint64_t* H, bn_sparse_csr S, uint64_t* m_enc, uint64_t* a_l) {

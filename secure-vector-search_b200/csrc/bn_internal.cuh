@@ -398,6 +398,11 @@ uint64_t block_plan_estimate(bn_flat* f, uint32_t B, uint32_t trials, uint32_t k
 int block_prepare_engine(Engine& e, const std::vector<uint64_t>* offsets);
 int pick_ctas(uint64_t max_rows_per_query, uint32_t B, int sms);
 int validate_residues(const uint64_t* a, uint64_t count, const char* what);
+// bn_ivf_build_keygen over lists whose global indices start at list0 (the
+// keys of list c are drawn from derive_h_seed(upload_seed, list0 + c)).
+int ivf_build_keygen_from(bn_ctx* ctx, uint32_t nlist, const uint64_t* off, const uint32_t* ids, const uint64_t* m_q,
+                          uint32_t n, uint32_t n1, const uint64_t* L, uint64_t upload_seed, uint32_t list0,
+                          bn_ivf** out);
 int engine_init(Engine& e, bn_ctx* ctx);
 void engine_free(Engine& e);
 int corpus_tmap(Corpus& c);

@@ -396,17 +396,19 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
     j.qp0[B] = (uint32_t)j.pairs.size();
     j.R = R;
     j.P = (uint32_t)j.pairs.size();
-    // groups: pairs sorted by (list, pair), so a list's queries stay in batch order
-    std::vector<uint64_t> keys(j.P);
-    for (uint32_t i = 0; i < j.P; ++i) keys[i] = ((uint64_t)j.pairs[i].list << 32) | i;
-    std::sort(keys.begin(), keys.end());
+    // groups: pairs ordered by (list, pair), so a list's queries stay in
+    // batch order (a counting sort over the lists: O(pairs + nlist))
+    std::vector<uint32_t> keys(j.P), start(v.nlist + 1, 0);
+    for (uint32_t i = 0; i < j.P; ++i) ++start[j.pairs[i].list + 1];
+    for (uint32_t c = 0; c < v.nlist; ++c) start[c + 1] += start[c];
+    for (uint32_t i = 0; i < j.P; ++i) keys[start[j.pairs[i].list]++] = i;
     j.order.resize(j.P);
     j.groups.clear();
     j.block0.clear();
     j.panel0.clear();
     uint32_t nb = 0, np = 0, nch = 0;
     for (uint32_t lp = 0; lp < j.P; ++lp) {
-        const uint32_t i = (uint32_t)keys[lp];
+        const uint32_t i = keys[lp];
         j.order[lp] = i;
         IvPair& pr = j.pairs[i];
         if (lp == 0 || j.pairs[j.order[lp - 1]].list != pr.list) {

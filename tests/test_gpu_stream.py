@@ -124,3 +124,70 @@ def test_stream_non_int8_plaintext(ctx):
     fo, ids, sc, _, _ = O.score_flat(cl, L, v, q_seed, 20, 10)
     assert gf[0] == fo and np.array_equal(got[0][0], ids) and np.array_equal(got[0][1], sc)
     st.close()
+
+
+# ---------------------------------------------------------------- IVF
+
+def ivf_args(case, B, nprobe, trials, k, seed):
+    rng = np.random.default_rng(seed)
+    probes = np.stack([rng.choice(case.nlist, nprobe, replace=False) for _ in range(B)]).astype(np.uint32)
+    encs = [O.encode_query(case.M[(7 * b) % case.M.shape[0]], case.L, bytes([90 + b]) * 32) for b in range(B)]
+    seeds = [O.domain_separate(bytes([90 + b]) * 32, b"protocol2") for b in range(B)]
+    return probes, encs, seeds, (probes, np.stack([e.v_enc for e in encs]), np.stack([e.g for e in encs]),
+                                 [(e.t_idx, e.t_sign) for e in encs], seeds, trials, k)
+
+
+@pytest.mark.parametrize("chunk_rows,slots", [(256, 1), (256, 2), (700, 2), (100000, 1)])
+def test_ivf_stream_equals_resident_and_oracle(ctx, chunk_rows, slots):
+    """Lists larger than a chunk (400 rows at chunk 256), empty lists, chunks
+    that hold several lists; repeated calls go through the LRU."""
+    from ivfutil import IvfCase
+
+    c = capi()
+    case = IvfCase([50, 0, 3, 200, 1, 0, 97, 400, 33, 120, 64, 9])
+    m_enc, a_l, h, rp, ix, sg = case.concat()
+    res = c.Ivf.build(ctx, case.offsets, case.ids, m_enc, a_l, h)
+    res.attach_client(case.L, case.M.reshape(-1), rp, ix, sg)
+    probe = c.IvfStream.build(ctx, case.offsets, case.ids, m_enc, a_l, h, case.L, case.M.reshape(-1), rp, ix, sg,
+                              chunk_rows, 1 << 40)
+    slot = probe.info()["slot_bytes"]
+    probe.close()
+    st = c.IvfStream.build(ctx, case.offsets, case.ids, m_enc, a_l, h, case.L, case.M.reshape(-1), rp, ix, sg,
+                           chunk_rows, slots * slot)
+    info = st.info()
+    assert info["rows"] == int(case.offsets[-1]) and info["slots"] == min(slots, info["chunks"])
+    for call in range(3):
+        probes, encs, seeds, a = ivf_args(case, 5, 4, 20, 10, 70 + call)
+        want, wc, wt = res.query(*a)
+        got, gc, gt = st.query(*a)
+        assert np.array_equal(gc, wc) and np.array_equal(gt, wt) and np.all(gt == -1)
+        for b in range(5):
+            assert np.array_equal(got[b][0], want[b][0]) and np.array_equal(got[b][1], want[b][1])
+            o = case.oracle_score(probes[b], encs[b], seeds[b], 20, 10)
+            assert np.array_equal(got[b][0], o[0]) and np.array_equal(got[b][1], o[1])
+    s = st.stats()
+    assert s["gets"] >= s["uploads"] >= 1 and s["resident_bytes"] <= slots * slot
+    st.close()
+    res.close()
+
+
+def test_ivf_stream_keygen_equals_resident_keygen(ctx):
+    """Chunks built by device keygen draw each list's keys from its global
+    list index (derive_h_seed(upload_seed, list), ivf.rs:258-264)."""
+    from ivfutil import IvfCase
+
+    c = capi()
+    case = IvfCase([50, 0, 3, 200, 1, 0, 97, 400, 33], upload_seed=7)
+    res = c.Ivf.build_keygen(ctx, case.offsets, case.ids, case.M.reshape(-1), case.L, 7)
+    st = c.IvfStream.build_keygen(ctx, case.offsets, case.ids, case.M.reshape(-1), case.L, 7, 256, 1 << 40)
+    assert st.info()["chunks"] >= 3
+    probes, encs, seeds, a = ivf_args(case, 4, 5, 3, 20, 81)
+    want, wc, wt = res.query(*a)
+    got, gc, gt = st.query(*a)
+    assert np.array_equal(gc, wc) and np.array_equal(gt, wt)
+    for b in range(4):
+        assert np.array_equal(got[b][0], want[b][0]) and np.array_equal(got[b][1], want[b][1])
+        o = case.oracle_score(probes[b], encs[b], seeds[b], 3, 20)
+        assert np.array_equal(got[b][0], o[0]) and np.array_equal(got[b][1], o[1])
+    st.close()
+    res.close()
