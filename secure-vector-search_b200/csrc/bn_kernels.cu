@@ -16,9 +16,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cooperative_groups.h>
 #include <type_traits>
 
 #include "bn_kernels.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace bn {
 
@@ -398,34 +401,42 @@ freivalds_finish_kernel(const uint64_t* __restrict__ z_part, const uint64_t* __r
 }
 
 // ------------------------------------------------------------------ L^T v
-// One CTA of 1024 threads per query: column k = tid % n1, rows j = slice,
-// slice + slices, ... with v_j's limbs in shared memory, so each term is six
-// multiply-adds into three accumulators and the column loads are
-// independent (batches of 16 in flight).  Each thread sums at most 512
-// terms below 2^53.2 (hi < 2^29), so the accumulators stay below 2^64.
-__global__ void __launch_bounds__(1024)
+// A cluster of 8 CTAs of 1024 threads per query (one CTA per query kept a
+// single SM busy for ~34 us): column k = tid % n1, rows j of the CTA's
+// range, slice, slice + slices, ... with v_j's limbs in shared memory, so
+// each term is six multiply-adds into three accumulators and the column
+// loads are independent (batches of 8 in flight).  Each thread sums at most
+// 64 terms below 2^53.2 (hi < 2^29), so the accumulators stay below 2^64.
+constexpr uint32_t LT_SPLIT = 8;  // CTAs per query (one cluster), N / LT_SPLIT terms each
+
+__global__ void __cluster_dims__(1, LT_SPLIT, 1) __launch_bounds__(1024)
 lt_times_v_kernel(const uint64_t* __restrict__ L, uint32_t n1, const uint64_t* __restrict__ v, uint64_t* __restrict__ x) {
-    const uint32_t q = blockIdx.x;
+    // CTA (q, s) of the query's cluster sums the terms j in [s N/8, (s+1) N/8)
+    // for every output k; CTA 0 adds the 8 partial rows through distributed
+    // shared memory.  A thread takes one k and every slices-th term of the range.
+    constexpr uint32_t TERMS = N / LT_SPLIT;
+    const uint32_t q = blockIdx.x, s = blockIdx.y;
     const uint32_t k = threadIdx.x % n1, slices = blockDim.x / n1, sl = threadIdx.x / n1;
-    __shared__ uint4 vl[2 * N];
+    __shared__ uint4 vl[2 * TERMS];
     __shared__ uint64_t part[1024];
-    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
-        const uint64_t w = v[(uint64_t)q * N + j];
+    __shared__ uint64_t row[512];  // this CTA's partial x (n1 <= 512)
+    for (uint32_t jj = threadIdx.x; jj < TERMS; jj += blockDim.x) {
+        const uint64_t w = v[(uint64_t)q * N + s * TERMS + jj];
         const Limbs3 b = limbs(w), c = limbs_hi(w);
-        vl[2 * j] = make_uint4(b.b0, b.b1, b.b2, c.b0);
-        vl[2 * j + 1] = make_uint4(c.b1, c.b2, 0u, 0u);
+        vl[2 * jj] = make_uint4(b.b0, b.b1, b.b2, c.b0);
+        vl[2 * jj + 1] = make_uint4(c.b1, c.b2, 0u, 0u);
     }
     __syncthreads();
     uint64_t a0 = 0, a1 = 0, a2 = 0;
-    const uint32_t terms = N / slices;  // multiple of 16: slices <= 16
-    for (uint32_t i0 = 0; i0 < terms; i0 += 16) {
-        uint64_t xs[16];
+    const uint32_t terms = TERMS / slices;  // n1 / 8: a multiple of 8 for n1 >= 64
+    for (uint32_t i0 = 0; i0 < terms; i0 += 8) {
+        uint64_t xs[8];
 #pragma unroll
-        for (int ii = 0; ii < 16; ++ii) xs[ii] = __ldg(L + (uint64_t)(sl + (i0 + ii) * slices) * n1 + k);
+        for (int ii = 0; ii < 8; ++ii) xs[ii] = __ldg(L + (uint64_t)(s * TERMS + sl + (i0 + ii) * slices) * n1 + k);
 #pragma unroll
-        for (int ii = 0; ii < 16; ++ii) {
-            const uint32_t j = sl + (i0 + ii) * slices;
-            const uint4 l0 = vl[2 * j], l1 = vl[2 * j + 1];
+        for (int ii = 0; ii < 8; ++ii) {
+            const uint32_t jj = sl + (i0 + ii) * slices;
+            const uint4 l0 = vl[2 * jj], l1 = vl[2 * jj + 1];
             const uint32_t xl = (uint32_t)xs[ii], xh = (uint32_t)(xs[ii] >> 32);
             a0 = mac(mac(a0, xl, l0.x), xh, l0.w);
             a1 = mac(mac(a1, xl, l0.y), xh, l1.x);
@@ -435,10 +446,18 @@ lt_times_v_kernel(const uint64_t* __restrict__ L, uint32_t n1, const uint64_t* _
     part[threadIdx.x] = combine3(a0, a1, a2);
     __syncthreads();
     if (threadIdx.x < n1) {
-        uint64_t s = 0;
-        for (uint32_t i = 0; i < slices; ++i) s = add_mod(s, part[i * n1 + threadIdx.x]);
-        x[(uint64_t)q * n1 + threadIdx.x] = s;
+        uint64_t t = 0;
+        for (uint32_t i = 0; i < slices; ++i) t = add_mod(t, part[i * n1 + threadIdx.x]);
+        row[threadIdx.x] = t;
     }
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();  // every CTA's row is written
+    if (s == 0 && threadIdx.x < n1) {
+        uint64_t t = 0;
+        for (uint32_t r = 0; r < LT_SPLIT; ++r) t = add_mod(t, cluster.map_shared_rank(row, r)[threadIdx.x]);
+        x[(uint64_t)q * n1 + threadIdx.x] = t;
+    }
+    cluster.sync();  // no CTA leaves while CTA 0 still reads its row
 }
 
 // ------------------------------------------------------------------ decode
@@ -1348,7 +1367,7 @@ void launch_freivalds_finish(const uint64_t* d_z_part, const uint64_t* d_ur_part
 
 void launch_lt_times_v(const uint64_t* d_L, uint32_t n1, const uint64_t* d_v, uint32_t nq, uint64_t* d_x,
                        cudaStream_t s) {
-    lt_times_v_kernel<<<nq, (1024 / n1) * n1, 0, s>>>(d_L, n1, d_v, d_x);
+    lt_times_v_kernel<<<dim3(nq, LT_SPLIT), (1024 / n1) * n1, 0, s>>>(d_L, n1, d_v, d_x);
 }
 
 void launch_dense_terms(const uint64_t* d_al_cm, const uint64_t* d_h_cm, uint64_t rows, uint32_t n1,
