@@ -1111,11 +1111,16 @@ int bn_flat_query(bn_flat* f, uint32_t B, const uint64_t* v_enc, const uint64_t*
     if (!f) return fail(BN_EINVAL, "null handle");
     if (B == 0) return BN_OK;
     std::lock_guard<std::mutex> gd(f->e.mu);
-    HostMeta hm;
-    if (f->m) flat_meta(f->m, B, hm);
-    else {
-        for (uint32_t b = 0; b < B; ++b) hm.dq.push_back(DecodeQuery{0, 0});
-        finish_meta(hm);
+    HostMeta& hm = f->query_meta;  // reused while B stays the same
+    if (f->query_meta_B != B) {
+        f->query_meta_B = 0;
+        hm = HostMeta();
+        if (f->m) flat_meta(f->m, B, hm);
+        else {
+            for (uint32_t b = 0; b < B; ++b) hm.dq.push_back(DecodeQuery{0, 0});
+            finish_meta(hm);
+        }
+        f->query_meta_B = B;
     }
     std::vector<int32_t> vf;
     TRY(run_query(f->e, hm, B, v_enc, g, t_idx, t_sign, t_nnz, v_seeds, trials, k, ids, scores, n_hits, vf, r_out, mv_out));

@@ -345,6 +345,10 @@ int ivf_block_prepare(bn_ivf* v);
 struct bn_flat {
     bn::api::Engine e;
     uint64_t m = 0;
+    // segment metadata of the last bn_flat_query batch size (rebuilding it
+    // walks every 128-row block of the corpus: tens of us per call at 1M rows)
+    bn::api::HostMeta query_meta;
+    uint32_t query_meta_B = 0;
     // block plan cached by the host-buffer block entry points
     bn::api::BlockPlan* block_cache = nullptr;
     uint32_t cache_B = 0, cache_trials = 0, cache_k = 0, cache_flags = 0;
