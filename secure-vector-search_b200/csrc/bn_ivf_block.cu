@@ -221,28 +221,53 @@ __global__ void zsum_lists_kernel(const uint64_t* __restrict__ z_part, const IvZ
     }
 }
 
-// zv[i][t] = z_t^{list(i)} . v_{q(i)}, list u's z at zbase + zoff[u] (its
-// single panel's z_part, or its panel sum); blocks visit the pairs list by
-// list (lm_pair) so that a list's z stays in L2 across its queries
-__global__ void __launch_bounds__(128) zv_pairs_kernel(const uint64_t* __restrict__ zbase,
+// zv[i][t] = z_t^u . v_{q(i)} for every pair i of list u = blockIdx.x and
+// trials [ZV_TRIALS * blockIdx.y, + ZV_TRIALS): list u's z (at zbase +
+// zoff[u]: its single panel's z_part, or its panel sum) is read once into
+// registers (thread x holds elements x + 128 e) and serves all the list's
+// pairs, whose v rows come from L2.  8 products (< 2^122 each) per thread and
+// trial are summed in 128 bits.
+constexpr uint32_t ZV_TRIALS = 4;
+__global__ void __launch_bounds__(128) zv_lists_kernel(const uint64_t* __restrict__ zbase,
                                                        const uint64_t* __restrict__ zoff,
                                                        const uint64_t* __restrict__ v,
                                                        const IvPair* __restrict__ pairs,
-                                                       const uint32_t* __restrict__ lm_pair, uint32_t trials,
+                                                       const IvGroup* __restrict__ groups,
+                                                       const uint32_t* __restrict__ lmi, uint32_t trials,
                                                        uint64_t* __restrict__ zv) {
-    const uint32_t i = lm_pair[blockIdx.x], t = blockIdx.y;
-    const IvPair pr = pairs[i];
-    const uint64_t* zr = zbase + zoff[pr.u] + (uint64_t)t * N;
-    const uint64_t* vr = v + (uint64_t)pr.q * N;
-    uint64_t lo = 0, hi = 0;
-    for (uint32_t j = threadIdx.x; j < N; j += 128) mac128(lo, hi, zr[j], vr[j]);  // 8 products per thread
-    uint64_t x = reduce128(lo, hi);
+    const uint32_t u = blockIdx.x, t0 = blockIdx.y * ZV_TRIALS;
+    const uint32_t tn = min(ZV_TRIALS, trials - t0);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const IvGroup g = groups[u];
+    const uint64_t* zr = zbase + zoff[u] + (uint64_t)t0 * N;
+    uint64_t z[ZV_TRIALS][N / 128];
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) x = add_mod(x, __shfl_xor_sync(0xffffffffu, x, off));
-    __shared__ uint64_t sh[4];
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = x;
-    __syncthreads();
-    if (threadIdx.x == 0) zv[(uint64_t)i * trials + t] = add_mod(add_mod(sh[0], sh[1]), add_mod(sh[2], sh[3]));
+    for (uint32_t tt = 0; tt < ZV_TRIALS; ++tt)
+#pragma unroll
+        for (uint32_t e = 0; e < N / 128; ++e) z[tt][e] = tt < tn ? zr[(uint64_t)tt * N + threadIdx.x + 128 * e] : 0;
+    __shared__ uint64_t sh[4][ZV_TRIALS];
+    for (uint32_t k = 0; k < g.n; ++k) {
+        const uint32_t i = lmi[g.lp0 + k];
+        const uint64_t* vr = v + (uint64_t)pairs[i].q * N;
+        uint64_t vv[N / 128];
+#pragma unroll
+        for (uint32_t e = 0; e < N / 128; ++e) vv[e] = vr[threadIdx.x + 128 * e];
+#pragma unroll
+        for (uint32_t tt = 0; tt < ZV_TRIALS; ++tt) {
+            uint64_t lo = 0, hi = 0;
+#pragma unroll
+            for (uint32_t e = 0; e < N / 128; ++e) mac128(lo, hi, z[tt][e], vv[e]);
+            uint64_t x = reduce128(lo, hi);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) x = add_mod(x, __shfl_xor_sync(0xffffffffu, x, off));
+            if (lane == 0) sh[warp][tt] = x;
+        }
+        __syncthreads();
+        if (threadIdx.x < tn)
+            zv[(uint64_t)i * trials + t0 + threadIdx.x] =
+                add_mod(add_mod(sh[0][threadIdx.x], sh[1][threadIdx.x]), add_mod(sh[2][threadIdx.x], sh[3][threadIdx.x]));
+        __syncthreads();  // sh is rewritten by the next pair
+    }
 }
 
 // First failing trial of each pair (-1: accepted); ur_out (nullable) [i][t].
@@ -756,8 +781,9 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             zsum_lists_kernel<<<j.NZ * j.trials, 256, 0, s>>>(U64(j.o_zpart),
                                                               reinterpret_cast<const IvZsum*>(d + j.o_zsum), j.trials,
                                                               U64(j.o_z));
-        zv_pairs_kernel<<<dim3(j.P, j.trials), 128, 0, s>>>(U64(j.o_zpart), U64(j.o_zoff), dv, dpairs, U32(j.o_lmi),
-                                                           j.trials, U64(j.o_zv));
+        zv_lists_kernel<<<dim3(j.U, (j.trials + ZV_TRIALS - 1) / ZV_TRIALS), 128, 0, s>>>(
+            U64(j.o_zpart), U64(j.o_zoff), dv, dpairs, reinterpret_cast<const IvGroup*>(d + j.o_groups), U32(j.o_lmi),
+            j.trials, U64(j.o_zv));
         pair_decide_kernel<<<(j.P + 3) / 4, 128, 0, s>>>(dpairs, j.P, U64(j.o_urpart), U64(j.o_zv), j.trials,
                                                              reinterpret_cast<int32_t*>(d + j.o_pfail),
                                                              j.verify_only ? U64(j.o_urout) : nullptr);
