@@ -599,8 +599,8 @@ tc_freivalds_small_kernel(const __grid_constant__ CUtensorMap tmap_m, const __gr
 //      column 480 alternate, and four drain warps turn each into r partials
 //      r_part[group][r index] while the next stage accumulates.
 // The z and r MMAs are issued by two warps (1 and FU_R_WARP), so neither
-// instruction stream waits for the other; a stage is free once both have
-// committed.  TMEM: z in columns [0, 3 n_rows) (n_rows <= 160), E in [480, 512).
+// instruction stream waits for the other; a stage is free once the z issuer
+// has committed and a drain warp has seen the stage's r MMAs complete.  TMEM: z in columns [0, 3 n_rows) (n_rows <= 160), E in [480, 512).
 constexpr int FU_S = 3;
 constexpr int FU_DRAIN_WARPS = 4;
 constexpr int FU_R_WARP = 2 + TC_EPI_WARPS + FU_DRAIN_WARPS;           // issues the r MMAs
@@ -636,7 +636,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < stages; ++s) {
             bar_init(&full_b[s], 1);
-            bar_init(&empty_b[s], 2);  // z issuer + r issuer
+            bar_init(&empty_b[s], 2);  // z issuer's commit + r drain's arrival
         }
         bar_init(&accf_b, 1);
         bar_init(&acce_b, TC_EPI_WARPS);
@@ -779,8 +779,7 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                         for (uint32_t ks = 0; ks < TC_ROWS / 32; ++ks)  // strip read K-major
                             mma_i8(tmem + FU_E_COL + 16 * eb, sdesc(sb + s * STRIP_BYTES + ks * 32u, 16, 1024),
                                    sdesc(wb + s * W_STRIP_BYTES + ks * 32u, 16, 1024), idesc_r, (s | ks) != 0);
-                    mma_commit(&empty_b[st]);
-                    mma_commit(&racc_b[eb]);  // the stage's row products are ready for the drain warps
+                    mma_commit(&racc_b[eb]);  // the stage's row products are ready (and its strips read)
                 }
                 if (stop) break;
                 mma_commit(&wfree_b[ib]);  // W buffer reusable once this item's r MMAs have read it
@@ -825,6 +824,10 @@ tc_fused_kernel(const __grid_constant__ CUtensorMap tmap_m, const __grid_constan
                 const bool ok = __all_sync(FULLMASK, bar_wait(&racc_b[eb], (uint32_t)((it >> 1) & 1), wait_limit));
                 if (!ok && lane == 0) { abort_s = 1; atomicOr(err, 32u); }
                 if (__any_sync(FULLMASK, !ok || abort_s)) { stop = true; break; }
+                // the r MMAs of stage it have completed, so they no longer read its
+                // strips: the r side's release of the stage (one commit fewer per
+                // stage for the r issuer)
+                if (q == 0 && lane == 0) bar_arrive(&empty_b[it % stages]);
                 tc_after();
                 uint32_t v[16];
                 tmem_ld16(tmem + ((q * 32) << 16) + FU_E_COL + 16 * eb, v);
