@@ -332,9 +332,11 @@ int bn_ivf_query_block(bn_ivf* h, uint32_t B, uint32_t nprobe, const uint32_t* p
  * (2..=12, capped by shared memory); 0 = chosen per batch from its groups. */
 int bn_ivf_block_tune(bn_ivf* h, uint32_t w_tile, uint32_t stages);
 /* Stage timing of later bn_ivf_query_block calls (enable = 1) and its read:
- * ms[0] = host planning and packing, ms[1..8] = device time of the stages
- * (H2D + operand images, G1, G2, G3, top-k, Protocol 2 passes, z . v and
- * verdicts, D2H) of the last call; *n = 0 before the first profiled call. */
+ * ms[0] = host planning and packing, ms[1..10] = device time of the stages
+ * (H2D + operand images, G1, G2, G3, top-k, Protocol 2's u draws, z passes
+ * and u . r sums, z . v and verdicts, D2H) of the last call; with more than
+ * 32 trials the earlier trial chunks count in the u draws; *n = 0 before the
+ * first profiled call. */
 int bn_ivf_block_profile(bn_ivf* h, int enable);
 int bn_ivf_block_profile_read(bn_ivf* h, float* ms, uint32_t cap, uint32_t* n);
 /* Protocol 2 of the block form over claimed responses: r holds every

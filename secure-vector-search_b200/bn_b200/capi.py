@@ -575,7 +575,7 @@ class Ivf:
         return hits, fc, ft
 
     IVF_BLOCK_STAGES = ("host_plan_pack", "h2d_operand_images", "g1_r", "g2_al_h", "g3_m_t_s_v", "topk",
-                        "protocol2_passes", "zv_decide", "d2h")
+                        "protocol2_u_draws", "protocol2_z_passes", "protocol2_u_dot_r", "zv_decide", "d2h")
 
     def block_tune(self, w_tile=0, stages=0):
         """GEMM tiling of later block calls: W rows per tile, pipeline stages (0 = automatic)."""

@@ -368,7 +368,7 @@ struct bn_ivf {
     // block GEMM tiling chosen by the caller (bn_ivf_block_tune; 0 = automatic)
     uint32_t blk_w = 0, blk_stages = 0;
     // stage timing of the host-buffer IVF block entry point (bn_ivf_block_profile)
-    static constexpr int PROF_EVENTS = 9;
+    static constexpr int PROF_EVENTS = 11;
     bool prof = false, prof_have = false;
     cudaEvent_t prof_ev[PROF_EVENTS] = {};
     float prof_host_ms = 0.f;

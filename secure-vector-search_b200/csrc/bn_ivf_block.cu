@@ -767,16 +767,19 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
         const auto* key = reinterpret_cast<const ChaChaKey*>(d + j.o_seed);
         for (uint32_t t0 = 0; t0 < j.trials; t0 += TC_MAX_TRIALS) {
             const uint32_t tc = std::min<uint32_t>(TC_MAX_TRIALS, j.trials - t0);
+            const bool last_chunk = t0 + tc == j.trials;  // stage marks: the last trial chunk
             launch_tc_ugen(vsegs, blocks, j.NB, key, nullptr, t0, tc, j.n_rows, U8(j.o_ub), nullptr, j.trials, err, s);
+            if (last_chunk) mark(6);
             launch_tc_freivalds(c.tmap_m, j.tm_u, panels, j.NP_big, t0, tc, j.n_rows, j.trials, U64(j.o_zpart), err,
                                 sms, s, 0, e.ctx->debug_wait_cycles);
             launch_tc_freivalds_small(c.tmap_m, j.tm_u, panels, j.NP_big, j.NP - j.NP_big, t0, tc, j.n_rows, j.trials,
                                       U64(j.o_zpart), err, sms, s, e.ctx->debug_wait_cycles);
+            if (last_chunk) mark(7);
             ur_lists_kernel<<<j.NUR, UR_WARPS * 32, 8 * tc * TC_ROWS, s>>>(
                 reinterpret_cast<const IvUrTask*>(d + j.o_urtasks), dpairs, U32(j.o_lmi), U8(j.o_ub), j.n_rows, t0, tc,
                 j.trials, U64(j.o_r), U64(j.o_urpart));
         }
-        mark(6);
+        mark(8);
         if (j.NZ)
             zsum_lists_kernel<<<j.NZ * j.trials, 256, 0, s>>>(U64(j.o_zpart),
                                                               reinterpret_cast<const IvZsum*>(d + j.o_zsum), j.trials,
@@ -795,10 +798,10 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
         CU(cudaMemsetAsync(d + j.o_fc, 0xff, (uint64_t)B * 4, s));
         CU(cudaMemsetAsync(d + j.o_ft, 0xff, (uint64_t)B * 4, s));
     }
-    mark(7);
+    mark(9);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(h + j.o_ids, d + j.o_ids, j.out_end - j.o_ids, cudaMemcpyDeviceToHost, s));
-    mark(8);
+    mark(10);
     return BN_OK;
 }
 
@@ -907,7 +910,7 @@ int bn_ivf_block_profile_read(bn_ivf* v, float* ms, uint32_t cap, uint32_t* n) {
     std::lock_guard<std::mutex> gd(v->e.mu);
     *n = 0;
     if (!v->prof_have) return BN_OK;
-    const uint32_t total = bn_ivf::PROF_EVENTS;  // host plan + pack, then the 8 device stages
+    const uint32_t total = bn_ivf::PROF_EVENTS;  // host plan + pack, then the 10 device stages
     for (uint32_t i = 0; i < total && i < cap; ++i) {
         if (i == 0) {
             ms[0] = v->prof_host_ms;

@@ -181,3 +181,20 @@ def test_query_block_rejects_bad_input(case, ivf):
     with pytest.raises(c.BnError) as e:
         ivf.query_block(probes, v, np.stack([e.g for e in encs]), [(e.t_idx, e.t_sign) for e in encs], bytes(32), 2, 10)
     assert e.value.code == c.BN_EINVAL
+
+
+def test_block_profile_stages(case, ivf):
+    """Stage timing of a profiled block call: one non-negative time per named
+    stage (host plan, H2D, G1-G3, top-k, the three Protocol 2 steps, verdicts,
+    D2H), and the same hits as an unprofiled call."""
+    probes, encs = batch(case, 6, 4, 61)
+    want = run_block(ivf, probes, encs, bytes([6]) * 32, 20, 10)
+    ivf.block_profile(True)
+    got = run_block(ivf, probes, encs, bytes([6]) * 32, 20, 10)
+    st = ivf.block_profile_read()
+    ivf.block_profile(False)
+    assert list(st) == list(capi().Ivf.IVF_BLOCK_STAGES) and len(st) == 11
+    assert all(x >= 0 for x in st.values()) and st["protocol2_z_passes"] > 0 and st["g1_r"] > 0
+    for a, b in zip(want[0], got[0]):
+        assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    assert np.array_equal(want[1], got[1])
