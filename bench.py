@@ -974,17 +974,21 @@ def run_serving(args, flat, ivf, flat_L, data, dist):
            "config": {"max_batch": mb, "slots": 4, "mem_budget_gib": 24, "max_wait_us": 1000, "block_min": 2,
                       "queue_wait_us": qwait},
            "mix": "50% flat / 50% IVF, nprobe uniform in {8, 32, 128}",
-           "warmup": "the server creates one flat block plan per block size at start-up; 512 requests "
-                     "submitted at once before the timed rates (the slots grow their workspaces), not counted",
+           "warmup": "the server creates one flat block plan per block size at start-up; before the timed "
+                     "rates, 256 flat requests, 256 IVF requests at nprobe 128 and 512 mixed ones submitted at "
+                     "once (the slots grow their workspaces and staging buffers), not counted",
            "rates": {}}
     # warm-up: the slots grow their workspaces to the largest batches once,
-    # as a service does at start-up
+    # as a service does at start-up: full flat batches, full IVF batches of
+    # the widest probes (nprobe 128), then the mix
+    heavy = [i for i in range(pool) if nps[i] == 128] or list(range(pool))
+    order = ([(1, j % pool) for j in range(256)] + [(0, heavy[j % len(heavy)]) for j in range(256)] +
+             [(j & 1, j % pool) for j in range(512)])
     warm = []
-    for j in range(512):
-        i = j % pool
+    for is_flat, i in order:
         while True:  # a refused submit (queue admission) waits for the oldest request, then retries
             try:
-                if j & 1:
+                if is_flat:
                     warm.append(srv.submit_flat(fenc[i][0], fenc[i][1], fenc[i][2], fenc[i][3], fseeds[i]))
                 else:
                     warm.append(srv.submit_ivf(probes[i], ienc[i][0], ienc[i][1], ienc[i][2], ienc[i][3], iseeds[i]))

@@ -130,14 +130,23 @@ struct DevMem {
 struct PinnedMem {
     void* p = nullptr;
     uint64_t bytes = 0;
+    // cudaFreeHost synchronises the whole device: a buffer that other streams
+    // keep busy (a serving slot's) sets keep_retired, and the buffers it grows
+    // out of are freed with it instead of at each growth.
+    bool keep_retired = false;
+    std::vector<void*> retired;
     ~PinnedMem() {
         if (p) cudaFreeHost(p);
+        for (void* x : retired) cudaFreeHost(x);
     }
-    // Grows by half again at least (cudaFreeHost synchronises the device).
+    // Grows by half again at least.
     int reserve(uint64_t b) {
         if (p && bytes >= b) return BN_OK;
         const uint64_t g = b > bytes + bytes / 2 ? b : bytes + bytes / 2;
-        if (p) cudaFreeHost(p);
+        if (p) {
+            if (keep_retired) retired.push_back(p);
+            else cudaFreeHost(p);
+        }
         p = nullptr;
         bytes = 0;
         CU(cudaMallocHost(&p, g));

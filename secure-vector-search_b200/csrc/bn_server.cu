@@ -606,6 +606,7 @@ int bn_server_create(bn_flat* flat, bn_ivf* ivf, const bn_server_config* cfg, bn
         }
         sl->ws.ctx = ctx;
         sl->ws.stream = sl->stream;  // grows in the slot's stream order, with no device-wide sync
+        sl->host.keep_retired = true;  // and its staging buffer without a cudaFreeHost while batches run
     }
     if (cfg->block_min) {
         // byte-planar corpus copies of block scoring, built now rather than

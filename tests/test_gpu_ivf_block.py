@@ -198,3 +198,28 @@ def test_block_profile_stages(case, ivf):
     for a, b in zip(want[0], got[0]):
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     assert np.array_equal(want[1], got[1])
+
+
+def test_verify_block_many_short_lists(ctx):
+    """More short lists (1 to 384 rows: panels of 1, 2 and 3 row blocks, in
+    random order) than SMs, so that CTAs of the short-list Protocol 2 kernel
+    take several panels in turn: every pair's u_t . r and z_t . v equal
+    verify_response's, trial by trial."""
+    c = capi()
+    rng = np.random.default_rng(77)
+    sizes = rng.integers(1, 385, 320).tolist()
+    big = IvfCase(sizes, seed=77)
+    m_enc, a_l, h, _, _, _ = big.concat()
+    v = c.Ivf.build(ctx, big.offsets, big.ids, m_enc, a_l, h)
+    probes = np.stack([rng.choice(big.nlist, size=64, replace=False) for _ in range(6)]).astype(np.uint32)
+    assert len(np.unique(probes)) > 200
+    encs = [O.encode_query(int8_matrix(1, 768, 7700 + b)[0], big.L, O.derive_h_seed(77, b)) for b in range(6)]
+    rs = pair_responses(big, v, probes, encs)
+    seed = bytes([77]) * 32
+    fc, ft, ur, zv = v.verify_block(probes, np.concatenate(rs), np.stack([e.v_enc for e in encs]), seed, 20)
+    assert np.all(fc == -1) and np.all(ft == -1)
+    for i, (q, ci, m) in enumerate(v.pairs(probes)):
+        cl = big.clusters[ci]
+        fo, uro, zvo = O.verify_response(rs[i], cl.m_enc, m, N, encs[q].v_enc, 20, seed)
+        assert fo == -1 and np.array_equal(ur[i], uro) and np.array_equal(zv[i], zvo), i
+    v.close()
