@@ -927,12 +927,15 @@ def run_ivf(args, ctx, dist):
         for w_tile, st in ((32, 0), (64, 0), (128, 0), (256, 0), (64, 6)):
             ivf.block_tune(w_tile, st)
             ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
-            g1 = []
+            g1, wall = [], []
             for _ in range(3):
+                ta = time.perf_counter()
                 ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
+                wall.append(time.perf_counter() - ta)
                 g1.append(ivf.block_profile_read())
-            sweep[f"w{w_tile}_s{st}"] = {k: round(statistics.median(x[k] for x in g1), 3)
-                                         for k in ("g1_r", "g2_al_h", "g3_m_t_s_v")}
+            sweep[f"w{w_tile}_s{st}"] = dict({k: round(statistics.median(x[k] for x in g1), 3)
+                                              for k in ("g1_r", "g2_al_h", "g3_m_t_s_v")},
+                                             call_ms=round(statistics.median(wall) * 1e3, 3))
         ivf.block_tune(0, 0)
         ivf.block_profile(False)
         res["block"] = {"qps": bq / db, "ms_per_batch": db * 1e3, "hits_equal_per_query": bool(same),
