@@ -71,3 +71,41 @@ def test_shard_rows_out_of_range(ctx):
         f.query_shard(enc.v_enc[None], enc.g[None], [(enc.t_idx, enc.t_sign)], [bytes(32)], 3, 5, 100, 120)
     assert e.value.code == capi.BN_EINVAL
     f.close()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_ivf_list_shards_equal_one_handle(ctx, world):
+    """An IVF corpus split by whole lists (shard.split_lists) into one handle
+    per rank (here all on one GPU): each rank's bn_ivf_query over the probes
+    that name its lists, merged on the host (top-k by score and id, the
+    earliest failing probe), equals one handle holding every list and the
+    oracle's BnTmIvfScorer::score (ivf.rs:778-823)."""
+    from bn_b200 import capi, shard
+    from ivfutil import IvfCase
+    from test_shard import IVF_SIZES, ivf_batch
+
+    case = IvfCase(IVF_SIZES, seed=81)
+    m_enc, a_l, h, rp, ix, sg = case.concat()
+    client = (case.L, case.M.reshape(-1), rp, ix, sg)
+    one = capi.Ivf.build(ctx, case.offsets, case.ids, m_enc, a_l, h)
+    one.attach_client(*client)
+    owner = shard.split_lists(case.sizes, world)
+    ranks = []
+    for g in range(world):
+        v, lists = shard.build_ivf_shard(capi, ctx, case.offsets, case.ids, m_enc, a_l, h, owner, g, client)
+        ranks.append(shard.ShardedIvf(v, lists, owner, g, dist=None))
+    probes, encs, seeds = ivf_batch(case, 5, 6, 82)
+    args = (np.stack([e.v_enc for e in encs]), np.stack([e.g for e in encs]), [(e.t_idx, e.t_sign) for e in encs],
+            seeds, TRIALS, K)
+    want, wc, wt = one.query(probes.astype(np.uint32), *args)
+    parts = [r.local(probes, *args) for r in ranks]
+    fc, ft = shard.merge_verdicts([p[1] for p in parts])
+    assert np.array_equal(fc, wc) and np.array_equal(ft, wt) and np.all(fc == -1)
+    for b in range(len(probes)):
+        ids, sc = shard.merge_topk([p[0][b] for p in parts], K)
+        assert np.array_equal(ids, want[b][0]) and np.array_equal(sc, want[b][1])
+        o = case.oracle_score(probes[b], encs[b], seeds[b], TRIALS, K)
+        assert np.array_equal(ids, o[0]) and np.array_equal(sc, o[1])
+    for r in ranks:
+        r.ivf.close()
+    one.close()
