@@ -921,6 +921,7 @@ def run_ivf(args, ctx, dist):
             ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
             t.append(time.perf_counter() - ta)
         db = statistics.median(t)
+        t_first = t
         ivf.block_profile(True)  # one more call with stage events (not part of the timing above)
         ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
         stages = ivf.block_profile_read()
@@ -940,6 +941,14 @@ def run_ivf(args, ctx, dist):
                                              call_ms=round(statistics.median(wall) * 1e3, 3))
         ivf.block_tune(0, 0)
         ivf.block_profile(False)
+        # the same five timed calls again after the sweep
+        t_late = []
+        for _ in range(reps):
+            ta = time.perf_counter()
+            ivf.query_block(pr, vb, gb, tb, bseed, args.trials, 10)
+            t_late.append(time.perf_counter() - ta)
+        res["block_repeat"] = {"calls_ms_first": [round(x * 1e3, 3) for x in t_first],
+                               "calls_ms_after_sweep": [round(x * 1e3, 3) for x in t_late]}
         res["block"] = {"qps": bq / db, "ms_per_batch": db * 1e3, "hits_equal_per_query": bool(same),
                         "distinct_rows_gbs": rows_u * N_DIM * 8 / db / 1e9, "stages_ms": stages,
                         "tiling_sweep_ms": sweep}
