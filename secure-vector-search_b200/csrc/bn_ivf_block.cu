@@ -364,15 +364,13 @@ namespace {
 // the tile minimising sum over groups of A tiles x W tiles x (A + W rows +
 // a fixed per-item cost).
 uint32_t pick_w_tile(const std::vector<IvGroup>& groups, uint32_t B) {
-    // Measured on 2M rows / 4096 k-means lists, batches of 64: where the
-    // lists take few of the batch's queries (nprobe 8 and 32: 1.6 and 2.8 on
-    // average), W = 128 ran the whole batch 5 % and 11 % faster than the W = 64
-    // the item-count model below picks there; at nprobe 128 (6.3 per list) it
-    // ran 18 % slower, so the model keeps those and batches too small to fill
-    // 128 W rows.
-    uint64_t pairs = 0;
-    for (const IvGroup& g : groups) pairs += g.n;
-    if (B >= 16 && !groups.empty() && pairs <= 4 * (uint64_t)groups.size()) return 128;
+    // Measured on 2M rows / 4096 k-means lists, batches of 64 (whole-batch
+    // call times of each tiling in the same run): W = 128 ran nprobe 8 and 32
+    // (1.6 and 2.8 queries per list on average) 5 % and 11 % faster than the
+    // W = 64 the item-count model below picks there, and nprobe 128 (6.3 per
+    // list) 2 % faster than the model's choice in three runs out of four; the
+    // model keeps the batches too small to fill 128 W rows.
+    if (B >= 16 && !groups.empty()) return 128;
     uint32_t best_w = 64;
     double best = 1e300;
     for (uint32_t w : {16u, 32u, 64u, 128u, 256u}) {
