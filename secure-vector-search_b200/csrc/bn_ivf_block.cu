@@ -221,13 +221,15 @@ __global__ void zsum_lists_kernel(const uint64_t* __restrict__ z_part, const IvZ
     }
 }
 
-// zv[i][t] = z_t^u . v_{q(i)} for every pair i of list u = blockIdx.x and
-// trials [ZV_TRIALS * blockIdx.y, + ZV_TRIALS): list u's z (at zbase +
-// zoff[u]: its single panel's z_part, or its panel sum) is read once into
-// registers (thread x holds elements x + 128 e) and serves all the list's
-// pairs, whose v rows come from L2.  8 products (< 2^122 each) per thread and
-// trial are summed in 128 bits.
+// zv[i][t] = z_t^u . v_{q(i)} for pairs ZV_PAIRS * blockIdx.z, ... of list
+// u = blockIdx.x and trials [ZV_TRIALS * blockIdx.y, + ZV_TRIALS): list u's z
+// (at zbase + zoff[u]: its single panel's z_part, or its panel sum) is read
+// into registers (thread x holds elements x + 128 e) and serves up to
+// ZV_PAIRS of the list's pairs, whose v rows come from L2 (a list probed by
+// many queries of the batch spreads over several CTAs).  8 products (< 2^122
+// each) per thread and trial are summed in 128 bits.
 constexpr uint32_t ZV_TRIALS = 4;
+constexpr uint32_t ZV_PAIRS = 8;
 __global__ void __launch_bounds__(128) zv_lists_kernel(const uint64_t* __restrict__ zbase,
                                                        const uint64_t* __restrict__ zoff,
                                                        const uint64_t* __restrict__ v,
@@ -235,10 +237,12 @@ __global__ void __launch_bounds__(128) zv_lists_kernel(const uint64_t* __restric
                                                        const IvGroup* __restrict__ groups,
                                                        const uint32_t* __restrict__ lmi, uint32_t trials,
                                                        uint64_t* __restrict__ zv) {
-    const uint32_t u = blockIdx.x, t0 = blockIdx.y * ZV_TRIALS;
+    const uint32_t u = blockIdx.x, t0 = blockIdx.y * ZV_TRIALS, k0 = blockIdx.z * ZV_PAIRS;
     const uint32_t tn = min(ZV_TRIALS, trials - t0);
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const IvGroup g = groups[u];
+    if (k0 >= g.n) return;  // CTA-uniform: this list has fewer pairs
+    const uint32_t k1 = min(g.n, k0 + ZV_PAIRS);
     const uint64_t* zr = zbase + zoff[u] + (uint64_t)t0 * N;
     uint64_t z[ZV_TRIALS][N / 128];
 #pragma unroll
@@ -246,7 +250,7 @@ __global__ void __launch_bounds__(128) zv_lists_kernel(const uint64_t* __restric
 #pragma unroll
         for (uint32_t e = 0; e < N / 128; ++e) z[tt][e] = tt < tn ? zr[(uint64_t)tt * N + threadIdx.x + 128 * e] : 0;
     __shared__ uint64_t sh[4][ZV_TRIALS];
-    for (uint32_t k = 0; k < g.n; ++k) {
+    for (uint32_t k = k0; k < k1; ++k) {
         const uint32_t i = lmi[g.lp0 + k];
         const uint64_t* vr = v + (uint64_t)pairs[i].q * N;
         uint64_t vv[N / 128];
@@ -330,6 +334,7 @@ struct IvfBlockJob {
     uint32_t B = 0, trials = 0, k = 0;
     bool verify_only = false;
     uint32_t P = 0, U = 0, NB = 0, NP = 0, NCH = 0, n_pl = 0, n_s8 = 0, NZ = 0;
+    uint32_t max_n = 0;   // most pairs of one list
     uint32_t NP_big = 0;  // panels [0, NP_big) belong to lists longer than TC_SMALL_PANEL_ROWS
     uint32_t NUR = 0;     // u . r tasks (list chunk x pair slab)
     uint64_t R = 0, max_q_rows = 0;
@@ -460,6 +465,8 @@ int ivf_block_plan(const bn_ivf& v, IvfBlockJob& j, uint32_t B, const uint32_t* 
         ++g.n;
     }
     j.U = (uint32_t)j.groups.size();
+    j.max_n = 0;
+    for (const IvGroup& g : j.groups) j.max_n = std::max(j.max_n, g.n);
     // z panels: the long lists' first (tc_freivalds_kernel), then the short
     // lists' single panels (tc_freivalds_small_kernel)
     j.panel0.assign(j.U, 0);
@@ -782,7 +789,8 @@ int ivf_block_launch(Engine& e, IvfBlockJob& j, DevMem& ws, PinnedMem& host, cud
             zsum_lists_kernel<<<j.NZ * j.trials, 256, 0, s>>>(U64(j.o_zpart),
                                                               reinterpret_cast<const IvZsum*>(d + j.o_zsum), j.trials,
                                                               U64(j.o_z));
-        zv_lists_kernel<<<dim3(j.U, (j.trials + ZV_TRIALS - 1) / ZV_TRIALS), 128, 0, s>>>(
+        zv_lists_kernel<<<dim3(j.U, (j.trials + ZV_TRIALS - 1) / ZV_TRIALS, (j.max_n + ZV_PAIRS - 1) / ZV_PAIRS), 128,
+                          0, s>>>(
             U64(j.o_zpart), U64(j.o_zoff), dv, dpairs, reinterpret_cast<const IvGroup*>(d + j.o_groups), U32(j.o_lmi),
             j.trials, U64(j.o_zv));
         pair_decide_kernel<<<(j.P + 3) / 4, 128, 0, s>>>(dpairs, j.P, U64(j.o_urpart), U64(j.o_zv), j.trials,
