@@ -282,3 +282,20 @@ def test_ivf_gloo_two_ranks_equal_the_whole_corpus(tmp_path):
         h, v = ivf_local(case, probes[b], encs[b], seeds[b], 20, K, set(range(case.nlist)), tl if b == 2 else None)
         assert got[0]["ids"][b] == h[0].tolist() and got[0]["scores"][b] == h[1].tolist()
         assert (got[0]["fc"][b], got[0]["ft"][b]) == (v[1], v[2])
+
+
+def test_ivf_shard_edge_cases():
+    """More ranks than lists (a rank owns nothing and pads every query with
+    its empty list), a batch whose probes miss a rank, k = 0, and a verdict
+    from the only shard that failed."""
+    from bn_b200 import shard
+
+    owner = shard.split_lists([5, 3], 3)
+    assert sorted(owner.tolist()) == [0, 1] and shard.shard_lists(owner, 2).size == 0
+    lp, pos = shard.local_probes(np.array([[0, 1], [1, 0]]), owner, 2)
+    assert lp.tolist() == [[0], [0]] and pos.tolist() == [[-1], [-1]]  # the empty list only
+    assert shard.shard_offsets([0, 5, 8], shard.shard_lists(owner, 2)).tolist() == [0, 0]
+    ids, sc = shard.merge_topk([(np.zeros(0, np.uint32), np.zeros(0, np.int64))] * 3, 0)
+    assert ids.size == 0 and sc.size == 0
+    fc, ft = shard.merge_verdicts([np.array([[-1, -1, -1]]), np.array([[3, 17, 2]])])
+    assert fc.tolist() == [17] and ft.tolist() == [2]
